@@ -1,0 +1,332 @@
+"""Benchmark: forward + adjoint PM N-body throughput on B200.
+
+Workload (default): 512^3 particles, 1024^3 force mesh, 1024 Mpc/h box,
+32 log-spaced kick-drift-kick steps from a = 0.1 to a = 1, forward pass plus
+the hand-written reverse sweep (the differentiable-run configuration).  One
+bench step = one full forward + adjoint run; the metric counts
+particles x 32 macro steps per second.  Initial state: the Lagrangian lattice
+displaced by a seeded Gaussian field (sigma 0.3 cells), zero velocity;
+random-normal final-state cotangents (seed 2).  Inputs are larger than L2.
+
+``--impl reference`` times the CPU oracle (NumPy restatement of PM++, the
+reference's own JAX stack is not installable here) on the host cores, on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+METRIC = "particle-steps/s at 512³/1024³ fwd+adj; learned-128³ vs plain-384³ time at 1% P(k)"
+UNIT = "particle-steps/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--ptcl", type=int, default=512)
+    p.add_argument("--mesh", type=int, default=2)
+    p.add_argument("--nsteps", type=int, default=32)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-ptcl", type=int, default=128)
+    return p.parse_args()
+
+
+# --------------------------------------------------------------------------
+# distributed plumbing (replicas only: every rank runs its own simulation)
+# --------------------------------------------------------------------------
+def dist_init(n):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------
+# clocks sampled during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace('.', '', 1).isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace('.', '', 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# --------------------------------------------------------------------------
+# algorithmic bytes per launch (the roofline numerator)
+# --------------------------------------------------------------------------
+def algorithmic_bytes(stage, N, M):
+    Mc = M // 2  # ~ nx*ny*(nz/2+1) for large nz
+    return {
+        "sort": 18 * N + 20 * N,               # read pmid+disp, write records+permutation
+        "scatter": 18 * N + 4 * M,             # particle positions in, density mesh out
+        "gather": 18 * N + 12 * N + 12 * M,    # positions, acc out, 3 force meshes in
+        "green_gradient": 8 * Mc + 24 * Mc,    # 1 spectrum in, 3 out
+        "fft_r2c": 4 * M + 8 * Mc,
+        "fft_c2r": 3 * (8 * Mc + 4 * M),
+        "gather_adjoint": 18 * N + 12 * N + 12 * N + 12 * M,
+        "scatter3": 18 * N + 12 * N + 12 * M,
+        "scatter_adjoint": 18 * N + 12 * N + 4 * M,
+    }.get(stage)
+
+
+def load_peaks():
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the oracle on a bounded sample
+# --------------------------------------------------------------------------
+def cpu_sample_rate(ptcl=128, mesh=2, nsteps=1, seed=0):
+    """One forward + adjoint macro step of the oracle at ptcl^3 / (mesh*ptcl)^3."""
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from oracle import cosmology as ocos
+    from oracle import pm as opm
+    opm.set_fft_workers(os.cpu_count() or 1)
+    box = 1024.0 * ptcl / 512
+    a = np.geomspace(0.1, 1.0, 33)[:nsteps + 1]
+    co = opm.Conf(box / ptcl, (ptcl, ) * 3, mesh_shape=mesh, a_start=0.1, a_custom=a)
+    oc = opm.boltzmann(ocos.Cosmo(), co)
+    pmid, disp = opm.gen_grid(co)
+    rng = np.random.default_rng(seed)
+    disp = (disp + rng.normal(0, 0.3 * co.cell_size, size=disp.shape)).astype(np.float32)
+    vel = np.zeros_like(disp)
+    t0 = time.perf_counter()
+    d, v, acc = opm.nbody(pmid, disp, vel, co, oc)
+    cot = rng.normal(size=disp.shape).astype(np.float32)
+    opm.nbody_adj(pmid, d, v, acc, cot, cot, np.zeros_like(cot), co, oc, om_grads=False)
+    dt = time.perf_counter() - t0
+    n = ptcl**3
+    return n * nsteps / dt, dt, f"oracle fwd+adj, {ptcl}^3 particles / {mesh * ptcl}^3 mesh, {nsteps} step(s), {dt:.1f}s"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    rates = []
+    for i in range(args.warmup + args.steps):
+        r, dt, sample = cpu_sample_rate(args.cpu_ptcl, args.mesh, 1, seed=i)
+        if i >= args.warmup:
+            rates.append(r)
+    v = float(np.mean(rates))
+    cores = os.cpu_count() or 1
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * (args.cpu_ptcl**3) / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"CPU oracle sample of the {args.ptcl}^3/{args.mesh * args.ptcl}^3 fwd+adj run",
+                   "sample_ptcl": args.cpu_ptcl, "sample_mesh": args.mesh * args.cpu_ptcl},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_init(args.gpus)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    import pmpp_b200 as pb
+    from pmpp_b200 import _lib
+    from pmpp_b200.runtime import StageTimer
+
+    n1 = args.ptcl
+    box = 1024.0 * n1 / 512
+    a = np.geomspace(0.1, 1.0, args.nsteps + 1)
+    conf = pb.Configuration(box / n1, (n1, ) * 3, args.mesh, a_start=0.1, a_custom=a, device=dev)
+    cos = pb.boltzmann(pb.SimpleLCDM(conf))
+    N = conf.ptcl_num
+    M = conf.mesh_size
+    g = torch.Generator(device=dev).manual_seed(1 + rank)
+    base = pb.Particles.gen_grid(conf, vel=True, device=dev)
+    base.disp += 0.3 * conf.cell_size * torch.randn(base.disp.shape, generator=g, device=dev)
+    g2 = torch.Generator(device=dev).manual_seed(2)
+    dcot = torch.randn((N, 3), generator=g2, device=dev)
+    run = pb.NBodyRun(conf, cos)
+
+    def step(p0, cot_d):
+        out = run.forward(p0)
+        cot = pb.Particles(conf, p0.pmid, cot_d, torch.zeros_like(cot_d), torch.zeros_like(cot_d))
+        return run.adjoint(out, cot)
+
+    for _ in range(args.warmup):
+        step(base, dcot)
+    torch.cuda.synchronize()
+    _lib.reset_launch_count()
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        with StageTimer() as timer:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.steps):
+                res = step(base, dcot)
+            e1.record()
+            torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches = _lib.launch_count()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(ms, world)
+    stages = timer.totals()
+    counts = dict(timer.counts)
+    value = world * N * args.nsteps / (ms * 1e-3)
+
+    # end to end: pinned host inputs in, cotangents out, every step
+    pin = lambda t: t.cpu().pin_memory()
+    h_pmid, h_disp, h_vel, h_cot = pin(base.pmid), pin(base.disp), pin(base.vel), pin(dcot)
+    h_out_d = torch.empty_like(h_disp).pin_memory()
+    h_out_v = torch.empty_like(h_disp).pin_memory()
+    barrier(world)
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record()
+    for _ in range(args.steps):
+        p = pb.Particles(conf, h_pmid.to(dev, non_blocking=True), h_disp.to(dev, non_blocking=True),
+                         h_vel.to(dev, non_blocking=True))
+        c = h_cot.to(dev, non_blocking=True)
+        _, pc, om = step(p, c)
+        h_out_d.copy_(pc.disp, non_blocking=True)
+        h_out_v.copy_(pc.vel, non_blocking=True)
+    e3.record()
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(e2.elapsed_time(e3) / args.steps, world)
+    h2d = int(h_pmid.numel() * 2 + h_disp.numel() * 4 * 2 + h_cot.numel() * 4)
+    d2h = int(h_out_d.numel() * 4 * 2)
+
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    peak, peak_kind = load_peaks()
+    ours = {k: v for k, v in stages.items() if not k.startswith("fft")}
+    dom = max(ours, key=ours.get)
+    per_launch_ms = ours[dom] / counts[dom]
+    alg = algorithmic_bytes(dom, N, M)
+    achieved = alg / (per_launch_ms * 1e-3) / 1e9
+    breakdown = {k: {"ms_total": round(v, 3), "launches": counts[k], "share": round(v / sum(stages.values()), 4)}
+                 for k, v in sorted(stages.items(), key=lambda kv: -kv[1])}
+    cpu = None
+    if not args.no_cpu_baseline:
+        r, dt, sample = cpu_sample_rate(args.cpu_ptcl, args.mesh, 1)
+        cpu = {"value": r, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port", "sample": sample}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{n1}^3 particles / {args.mesh * n1}^3 mesh, {box:.0f} Mpc/h, {args.nsteps} log KDK "
+                               f"steps a=0.1->1, forward + adjoint per step", "particles": N, "mesh": M,
+                   "kdk_steps": args.nsteps, "parallelism": f"replicas x{world}", "l2": "inputs larger than L2"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms},
+        "breakdown": breakdown,
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * N * args.nsteps / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,154 @@
+/*
+ * pmb200.h -- C ABI of the PM++ B200 particle-mesh kernels (libpmb200.so).
+ *
+ * Every entry point only enqueues work on the CUDA stream it is given; it
+ * never synchronises, never creates streams and never allocates device
+ * memory: buffers and scratch come from the caller (the same ownership rules
+ * as the reference's XLA FFI handlers, cuda/route_kernels.cu:1-7).  All
+ * pointers are device pointers unless stated otherwise.  Return value: 0 on
+ * success, a negative pmb status otherwise (-1 invalid argument, -2 CUDA
+ * error, -3 cuFFT error, -4 unsupported shape, -5 scratch too small); the
+ * message of the last failure on the calling thread is pmb_last_error().
+ *
+ * Layouts (C order): pmid int16 (n,3); disp/vel/acc float (n,3); meshes float
+ * (C,nx,ny,nz) planar channels; spectra float2 (C,nx,ny,nz/2+1).
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the PM++ source tree).
+ */
+#ifndef PMB200_H
+#define PMB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Version of this ABI; bumped on any signature change. */
+int pmb_abi_version(void);
+/* Message of the last failed call on this thread (never NULL). */
+const char* pmb_last_error(void);
+
+/* ---------------- particle sort by cell ----------------------------------
+ * Replaces the key computation of core/utils.py:292-326 and the per-cell
+ * ordering that cuda/route_kernels.cu:131-145, 615-724 maintain, using the
+ * binning of cic/enmesh.py:139-147.  Particles are counting-sorted by the
+ * mesh row (x, y) of their lower CIC corner; `sorted` receives 16-byte
+ * records (fx, fy, fz, raveled cell key), the permutation (uint32) and the
+ * row offsets (uint32, nx*ny+1).  With vel != NULL the drift
+ * disp += vel * drift (nbody/integrator.py:223-225) is applied first and
+ * written back to disp. */
+int64_t pmb_sorted_bytes(int64_t n, int nx, int ny, int nz);
+int64_t pmb_sort_scratch_bytes(int64_t n, int nx, int ny, int nz);
+int pmb_sort_rows(const int16_t* pmid, float* disp, const float* vel, float drift, int64_t n, int nx, int ny, int nz,
+                  float cell, void* sorted, void* scratch, int64_t scratch_bytes, void* stream);
+/* Stable per-cell order of the reference key ((x*My+y)*Mz+z), ties keep
+ * source order: keys_out[n] (uint32) and perm_out[n] (uint32). */
+int pmb_sort_by_cell(const int16_t* pmid, const float* disp, int64_t n, int nx, int ny, int nz, float cell,
+                     uint32_t* keys_out, uint32_t* perm_out, void* scratch, int64_t scratch_bytes, void* stream);
+int64_t pmb_sort_by_cell_scratch_bytes(int64_t n, int nx, int ny, int nz);
+
+/* ---------------- CIC on sorted particles --------------------------------
+ * Deterministic scatter (cic/scatter.py:315-338, cic/pallas.py:268-303):
+ * out[c] = sum_p val[p,c] * w_p.  val (n,C) or NULL for the constant
+ * val_const.  mode 0 writes the sum; mode 1 writes (sum - 1) * src_mul (the
+ * Poisson source of nbody/gravity.py:628-630).  scratch: 16 bytes. */
+int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* val, float val_const,
+                     int mode, float src_mul, float* out, void* scratch16, void* stream);
+/* Gather (cic/gather.py:452-472, cic/pallas.py:305-318): out[p,c]; with
+ * vel != NULL also vel += out * kick (nbody/integrator.py:536). */
+int pmb_gather_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh, float* out,
+                    float* vel, float kick, void* stream);
+/* Position term of the CIC adjoints (cic/gather.py:495-502,
+ * cic/scatter.py:366-373): disp_cot[p] (+)= sum_b (sum_c u[p,c] mesh_c[i_b])
+ * grad w_b / cell; optional wsum[p,c] = sum_b mesh_c[i_b] w_b. */
+int pmb_interp_grad_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh,
+                         const float* u, float u_const, float cell, int accumulate, float* disp_cot, float* wsum,
+                         void* stream);
+
+/* ---------------- spectral ------------------------------------------------
+ * 3-D R2C / C2R (numpy convention: forward unnormalised, the inverse is NOT
+ * divided by nx*ny*nz here), batch meshes back to back.  These stand in for
+ * jnp.fft.rfftn / irfftn at nbody/gravity.py:425, 528. */
+int64_t pmb_fft_work_bytes(int nx, int ny, int nz, int batch);
+int pmb_rfft3(int nx, int ny, int nz, int batch, float* in, void* out, void* work, void* stream);
+int pmb_irfft3(int nx, int ny, int nz, int batch, void* in, float* out, void* work, void* stream);
+/* tables: float [kx(nx) ky(ny) kz(nz/2+1) cx(nx) cy(ny) cz(nz/2+1)] plus,
+ * when has_masks, [mx(nx) my(ny) mz(nz/2+1)] (core/configuration.py:301-307,
+ * 365-376; core/utils.py:15-37).  green_kernel 0 = continuum -1/k^2
+ * (gravity.py:283-285), 1 = discrete Laplacian (gravity.py:122-171, 345-352;
+ * pass the effective k tables).  transfer: optional real multiplier per
+ * half-spectrum cell (corrections/core.py:333-334); radial: optional table
+ * indexed by integer |n|^2.  grad_hat = 3 spectra (i c_d) K S_hat * post_scale
+ * (gravity.py:389-399, 506-543). */
+int pmb_green_gradient(const void* src_hat, void* grad_hat, int nx, int ny, int nz, const float* tables, int has_masks,
+                       int green_kernel, const float* transfer, const float* radial, int radial_len, float post_scale,
+                       void* stream);
+/* Adjoint of pmb_green_gradient: src_cot_hat = K sum_d conj(i c_d) A_d * post_scale. */
+int pmb_green_gradient_adjoint(const void* grad_cot_hat, void* src_cot_hat, int nx, int ny, int nz,
+                               const float* tables, int has_masks, int green_kernel, const float* transfer,
+                               const float* radial, int radial_len, float post_scale, void* stream);
+
+/* ---------------- fused PM force ------------------------------------------
+ * One PM force evaluation (nbody/gravity.py:786-814 -> _gravity_from_density
+ * :626-633 -> _streamed_acceleration_from_potential :506-543): optional
+ * drift, cell sort, deterministic scatter to the Poisson source, R2C, Green x
+ * gradient, batched C2R into force_meshes (3,nx,ny,nz), 3-channel gather into
+ * acc (n,3), optional fused half-kick vel_kick += acc * kick. */
+int64_t pmb_force_workspace_bytes(int64_t n, int nx, int ny, int nz);
+int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float drift, int64_t n, int nx, int ny, int nz,
+              float cell, float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
+              const float* transfer, const float* radial, int radial_len, float* force_meshes, float* acc,
+              float* vel_kick, float kick, void* workspace, int64_t workspace_bytes, void* stream);
+/* Transpose of pmb_force w.r.t. disp given force_meshes at the same disp
+ * (the force VJP of nbody/integrator.py:620-686): disp_cot (n,3) +=
+ * gather-adjoint position term + scatter-adjoint term of the density. */
+int64_t pmb_force_vjp_workspace_bytes(int64_t n, int nx, int ny, int nz);
+int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int ny, int nz, float cell,
+                  float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
+                  const float* transfer, const float* radial, int radial_len, const float* force_meshes,
+                  const float* acc_cot, float* disp_cot, void* workspace, int64_t workspace_bytes, void* stream);
+
+/* ---------------- time integration ---------------------------------------
+ * y += x * f in float (drift integrator.py:225, kick :536). */
+int pmb_axpy(float* y, const float* x, int64_t n, float f, void* stream);
+/* Kick adjoint (integrator.py:566-580); dot (double, device) += sum vel_cot*acc. */
+int pmb_kick_adj(float* vel, const float* acc, const float* vel_cot, float* acc_cot, int64_t n, float kick,
+                 double* dot, void* stream);
+/* Drift adjoint (integrator.py:459-474); dot += sum disp_cot*vel. */
+int pmb_drift_adj(float* disp, const float* vel, const float* disp_cot, float* vel_cot, int64_t n, float drift,
+                  double* dot, void* stream);
+/* dot (double, device) += sum a*b. */
+int pmb_dot(const float* a, const float* b, int64_t n, double* dot, void* stream);
+
+/* ---------------- host-side FP64 cosmology (no device work) ---------------
+ * Growth table [order 1..2][deriv 0..2][na] from the growth ODE integrated
+ * with the adaptive Dormand-Prince scheme of numerics/ode.py:304-422 at the
+ * scale factors growth_a (cosmology/boltzmann.py:177-249); dtable_dom
+ * (optional) receives d table / d Omega_m by complex-step differentiation. */
+int pmb_growth_table(double omega_m, double omega_k, double w0, double wa, const double* growth_a, int na,
+                     double a_lpt_step, double rtol, double atol, double dt0, double* table, double* dtable_dom);
+/* kind 0: drift factor (integrator.py:125-146) for (a_vel, a_prev, a_next);
+ * kind 1: kick factor (integrator.py:149-170) for (a_acc, a_prev, a_next).
+ * dfactor_dom (optional) needs dtable_dom. */
+int pmb_time_factor(int kind, double a0, double a1, double a2, double omega_m, double omega_k, double w0, double wa,
+                    const double* growth_a, int na, const double* table, const double* dtable_dom, double* factor,
+                    double* dfactor_dom);
+/* LPT growth factors at a (initial_conditions/lpt.py:412-417): out[m-1][0..2]
+ * = (D_m, dD_m/dlna, a^2 H dD_m/dlna) for m = 1, 2; dout = d/d Omega_m. */
+int pmb_lpt_factors(double a, double omega_m, double omega_k, double w0, double wa, const double* growth_a, int na,
+                    const double* table, const double* dtable_dom, double* out, double* dout);
+/* Eisenstein & Hu transfer fit (cosmology/boltzmann.py:33-137). */
+int pmb_transfer_fit(const double* k, int64_t nk, double omega_m, double omega_b, double h, double T_cmb,
+                     int nowiggle, double* out);
+/* Linear power without growth (cosmology/boltzmann.py:428-484) from a
+ * tabulated transfer function (tk, tt). */
+int pmb_linear_power(const double* k, int64_t nk, const double* tk, const double* tt, int ntab, double A_s,
+                     double n_s, double omega_m, double h, double k_pivot_Mpc, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PMB200_H */

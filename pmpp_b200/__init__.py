@@ -1,0 +1,24 @@
+"""B200-native rebuild of PM++'s single-GPU particle-mesh path.
+
+The hot path runs hand-written sm_100a CUDA kernels from libpmb200.so (C ABI,
+include/pmb200.h); this package is the host-side mirror of PM++'s Python API:
+
+* Configuration, Cosmology / SimpleLCDM / boltzmann, Particles
+* cic.scatter / cic.gather and their adjoints
+* gravity, nbody (forward) and nbody_adj (hand-written reverse sweep)
+* lpt, white_noise_nested, linear_modes
+* delta_to_pk / density_to_pk / particles_to_pk
+"""
+from .configuration import Configuration
+from .cosmology import Cosmology, SimpleLCDM, boltzmann, growth, linear_power
+from .particles import Particles
+from . import cic
+from .cic import scatter, gather, scatter_vjp, gather_vjp
+from .gravity import gravity, gravity_vjp
+from .nbody import nbody, nbody_adj, integrate, kick, drift, NBodyRun
+
+__all__ = [
+    "Configuration", "Cosmology", "SimpleLCDM", "boltzmann", "growth", "linear_power", "Particles", "cic", "scatter",
+    "gather", "scatter_vjp", "gather_vjp", "gravity", "gravity_vjp", "nbody", "nbody_adj", "integrate", "kick",
+    "drift", "NBodyRun"
+]

@@ -1,0 +1,106 @@
+"""ctypes binding of libpmb200.so (include/pmb200.h).
+
+The library must have been built in-tree (``python -m pmpp_b200.build``); a
+missing library is an error, never a silent fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpmb200.so")
+
+c_int, c_i64, c_f, c_d, c_p = ctypes.c_int, ctypes.c_int64, ctypes.c_float, ctypes.c_double, ctypes.c_void_p
+
+_SIGS = {
+    "pmb_abi_version": (c_int, []),
+    "pmb_last_error": (ctypes.c_char_p, []),
+    "pmb_sorted_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
+    "pmb_sort_scratch_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
+    "pmb_sort_rows": (c_int, [c_p, c_p, c_p, c_f, c_i64, c_int, c_int, c_int, c_f, c_p, c_p, c_i64, c_p]),
+    "pmb_sort_by_cell": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_f, c_p, c_p, c_p, c_i64, c_p]),
+    "pmb_sort_by_cell_scratch_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
+    "pmb_scatter_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_f, c_int, c_f, c_p, c_p, c_p]),
+    "pmb_gather_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_f, c_p]),
+    "pmb_interp_grad_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_p, c_f, c_f, c_int, c_p, c_p,
+                                     c_p]),
+    "pmb_fft_work_bytes": (c_i64, [c_int, c_int, c_int, c_int]),
+    "pmb_rfft3": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
+    "pmb_irfft3": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
+    "pmb_green_gradient": (c_int, [c_p, c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p, c_int, c_f, c_p]),
+    "pmb_green_gradient_adjoint": (c_int, [c_p, c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p, c_int, c_f,
+                                           c_p]),
+    "pmb_force_workspace_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
+    "pmb_force": (c_int, [c_p, c_p, c_p, c_f, c_i64, c_int, c_int, c_int, c_f, c_f, c_f, c_p, c_int, c_int, c_p, c_p,
+                          c_int, c_p, c_p, c_p, c_f, c_p, c_i64, c_p]),
+    "pmb_force_vjp_workspace_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
+    "pmb_force_vjp": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_f, c_f, c_f, c_p, c_int, c_int, c_p, c_p, c_int,
+                              c_p, c_p, c_p, c_p, c_i64, c_p]),
+    "pmb_axpy": (c_int, [c_p, c_p, c_i64, c_f, c_p]),
+    "pmb_kick_adj": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_p, c_p]),
+    "pmb_drift_adj": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_p, c_p]),
+    "pmb_dot": (c_int, [c_p, c_p, c_i64, c_p, c_p]),
+    "pmb_growth_table": (c_int, [c_d, c_d, c_d, c_d, c_p, c_int, c_d, c_d, c_d, c_d, c_p, c_p]),
+    "pmb_time_factor": (c_int, [c_int, c_d, c_d, c_d, c_d, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p]),
+    "pmb_lpt_factors": (c_int, [c_d, c_d, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p]),
+    "pmb_transfer_fit": (c_int, [c_p, c_i64, c_d, c_d, c_d, c_d, c_int, c_p]),
+    "pmb_linear_power": (c_int, [c_p, c_i64, c_p, c_p, c_int, c_d, c_d, c_d, c_d, c_d, c_p]),
+}
+
+_lib = None
+
+
+class PMBError(RuntimeError):
+    """A libpmb200 entry point returned a non-zero status."""
+
+
+def lib():
+    """Load libpmb200.so once; raise if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m pmpp_b200.build`")
+        L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return sorted(_SIGS)
+
+
+def check(status, what):
+    if status != 0:
+        msg = lib().pmb_last_error().decode(errors="replace")
+        raise PMBError(f"{what} failed with status {status}: {msg}")
+
+
+# Hand-written kernels launched per entry point (cuFFT's own kernels excluded).
+_KERNELS = {
+    "pmb_sort_rows": 5, "pmb_gather_rows": 1, "pmb_interp_grad_rows": 1, "pmb_green_gradient": 1,
+    "pmb_green_gradient_adjoint": 1, "pmb_axpy": 1, "pmb_kick_adj": 1, "pmb_drift_adj": 1, "pmb_dot": 1,
+    "pmb_force": 9, "pmb_force_vjp": 11,
+}
+_launches = [0]
+
+
+def reset_launch_count():
+    _launches[0] = 0
+
+
+def launch_count():
+    return _launches[0]
+
+
+def call(name, *args):
+    """Call an entry point that returns a status and raise on failure."""
+    check(getattr(lib(), name)(*args), name)
+    if name == "pmb_scatter_rows":
+        _launches[0] += 2 if args[6] is None else 3
+    else:
+        _launches[0] += _KERNELS.get(name, 0)

@@ -1,0 +1,183 @@
+"""Run configuration (the fields of PM++'s ``Configuration`` the PM path reads).
+
+Mirrors core/configuration.py:172-575: geometry (ptcl_spacing,
+ptcl_grid_shape, mesh_shape as a scale or a shape), time schedules (a_start,
+a_stop, a_custom, symp_splits), LPT order, growth-ODE tolerances and the
+transfer-function k grid.  The cached spectral operators (kvec, the
+Nyquist-zeroed derivative factors and the particle-Nyquist masks) are built
+here once with the reference formulas and uploaded as one device table.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+
+def _fftfreq(shape, spacing):
+    """Angular wavevectors per axis (numerics/fft.py:4-44), float32."""
+    period = 2 * np.pi / spacing
+    ks = [(np.fft.fftfreq(s) * period).astype(np.float32) for s in shape[:-1]]
+    ks.append((np.fft.rfftfreq(shape[-1]) * period).astype(np.float32))
+    return ks
+
+
+class Configuration:
+    """PM configuration; see core/configuration.py:22-243 for field meanings."""
+
+    def __init__(self, ptcl_spacing, ptcl_grid_shape, mesh_shape=1, *, a_start=1 / 64, a_stop=1.0,
+                 a_lpt_maxstep=1 / 128, a_nbody_maxstep=1 / 64, a_custom=None,
+                 symp_splits=((0, 0.5), (1, 0.5)), lpt_order=2, growth_rtol=None, growth_atol=None,
+                 growth_inistep=(1, None), transfer_fit=True, transfer_fit_nowiggle=False, transfer_lgk_min=-4,
+                 transfer_lgk_max=3, transfer_lgk_maxstep=1 / 128, T_cmb=2.7255, k_pivot_Mpc=0.05,
+                 float_dtype="float32", device=None):
+        self.ptcl_spacing = float(ptcl_spacing)
+        self.ptcl_grid_shape = tuple(int(s) for s in ptcl_grid_shape)
+        if isinstance(mesh_shape, (int, float)):
+            mesh_shape = tuple(round(s * mesh_shape) for s in self.ptcl_grid_shape)
+        self.mesh_shape = tuple(int(s) for s in mesh_shape)
+        if len(self.ptcl_grid_shape) != 3 or len(self.mesh_shape) != 3:
+            raise ValueError("only three spatial dimensions are supported")
+        if any(sm < sp for sp, sm in zip(self.ptcl_grid_shape, self.mesh_shape)):
+            raise ValueError('mesh grid cannot be smaller than particle grid')
+        if any(self.ptcl_grid_shape[0] * sm != self.mesh_shape[0] * sp
+               for sp, sm in zip(self.ptcl_grid_shape[1:], self.mesh_shape[1:])):
+            raise ValueError('particle and mesh grid aspect ratios differ')
+        if str(float_dtype).replace("torch.", "") != "float32":
+            raise NotImplementedError("the B200 kernels compute in float32")
+        self.float_dtype = torch.float32
+        self.a_start = float(a_start)
+        self.a_stop = float(a_stop)
+        self.a_lpt_maxstep = a_lpt_maxstep
+        self.a_nbody_maxstep = a_nbody_maxstep
+        self.a_custom = None if a_custom is None else tuple(float(a) for a in np.asarray(a_custom).tolist())
+        if any(len(s) != 2 for s in symp_splits):
+            raise ValueError(f'symp_splits={symp_splits} not supported')
+        if tuple(sum(s) for s in zip(*symp_splits)) != (1, 1):
+            raise ValueError('sum of symplectic splits != (1, 1)')
+        self.symp_splits = tuple(tuple(s) for s in symp_splits)
+        if lpt_order not in (0, 1, 2):
+            raise ValueError(f'lpt_order={lpt_order} not supported')
+        self.lpt_order = lpt_order
+        tol = math.sqrt(np.finfo(np.float64).eps)
+        self.growth_rtol = tol if growth_rtol is None else growth_rtol
+        self.growth_atol = tol if growth_atol is None else growth_atol
+        self.growth_inistep = growth_inistep
+        if not transfer_fit:
+            raise NotImplementedError('only the Eisenstein-Hu transfer fit is available')
+        self.transfer_fit_nowiggle = bool(transfer_fit_nowiggle)
+        self.transfer_lgk_min = transfer_lgk_min
+        self.transfer_lgk_max = transfer_lgk_max
+        self.transfer_lgk_maxstep = transfer_lgk_maxstep
+        self.T_cmb = T_cmb
+        self.k_pivot_Mpc = k_pivot_Mpc
+        self.device = torch.device(device if device is not None else ("cuda" if torch.cuda.is_available() else "cpu"))
+        # cached spectral operators (configuration.py:301-307, 365-376)
+        self.kvec = _fftfreq(self.mesh_shape, self.cell_size)
+        self.kvec_spacing = _fftfreq(self.ptcl_grid_shape, self.ptcl_spacing)
+        self.neg_k = tuple(self._neg_k(k, self.cell_size) for k in self.kvec)
+        self._tables = {}
+
+    @staticmethod
+    def _neg_k(k, spacing):
+        nyquist = np.float32(np.pi / spacing)
+        eps = nyquist * np.finfo(np.float32).eps
+        return np.where(np.abs(np.abs(k) - nyquist) <= eps, np.float32(0), -k).astype(np.float32)
+
+    # ---- derived quantities (configuration.py:437-563) ----
+    @property
+    def dim(self):
+        return 3
+
+    @property
+    def ptcl_num(self):
+        return math.prod(self.ptcl_grid_shape)
+
+    @property
+    def mesh_size(self):
+        return math.prod(self.mesh_shape)
+
+    @property
+    def cell_size(self):
+        return self.ptcl_spacing * self.ptcl_grid_shape[0] / self.mesh_shape[0]
+
+    @property
+    def ptcl_cell_vol(self):
+        return self.ptcl_spacing**3
+
+    @property
+    def box_size(self):
+        return tuple(self.ptcl_spacing * s for s in self.ptcl_grid_shape)
+
+    @property
+    def box_vol(self):
+        return float(np.prod(self.box_size))
+
+    @property
+    def transfer_k_num(self):
+        return 1 + math.ceil((self.transfer_lgk_max - self.transfer_lgk_min) / self.transfer_lgk_maxstep) + 1
+
+    @property
+    def transfer_k(self):
+        k = np.logspace(self.transfer_lgk_min, self.transfer_lgk_max, num=self.transfer_k_num - 1)
+        return np.concatenate(([0.0], k))
+
+    @property
+    def a_lpt_num(self):
+        return math.ceil(self.a_start / self.a_lpt_maxstep)
+
+    @property
+    def a_lpt_step(self):
+        return self.a_start / self.a_lpt_num
+
+    @property
+    def a_nbody_num(self):
+        return math.ceil((self.a_stop - self.a_start) / self.a_nbody_maxstep)
+
+    @property
+    def a_lpt(self):
+        return np.linspace(0, self.a_start, num=self.a_lpt_num + 1)
+
+    @property
+    def a_nbody(self):
+        if self.a_custom is not None:
+            return np.array(self.a_custom, dtype=np.float64)
+        return np.linspace(self.a_start, self.a_stop, num=1 + self.a_nbody_num)
+
+    @property
+    def growth_a(self):
+        return np.concatenate((self.a_lpt, self.a_nbody[1:]))
+
+    @property
+    def has_particle_nyquist_masks(self):
+        return self.mesh_shape != self.ptcl_grid_shape
+
+    def particle_nyquist_masks(self):
+        """Per-axis masks of modes resolvable on the particle grid (core/utils.py:15-37)."""
+        kn = np.float32(np.pi / self.ptcl_spacing)
+        limit = kn + kn * np.float32(8 * np.finfo(np.float32).eps)
+        return tuple((np.abs(k) <= limit).astype(np.float32) for k in self.kvec)
+
+    def spectral_tables(self, which="mesh", device=None, green_kernel=0):
+        """Device table [kx ky kz cx cy cz (mx my mz)] for pmb_green_gradient.
+
+        which="mesh" uses the force mesh (kvec, cell_size); "particle" the
+        particle grid (kvec_spacing, ptcl_spacing).  green_kernel=1 replaces
+        k by the discrete-Laplacian wavenumber 2 sin(k dx/2)/dx
+        (gravity.py:122-171)."""
+        device = self.device if device is None else torch.device(device)
+        key = (which, str(device), green_kernel)
+        if key not in self._tables:
+            if which == "mesh":
+                ks, spacing, masks = self.kvec, self.cell_size, (self.particle_nyquist_masks()
+                                                                 if self.has_particle_nyquist_masks else ())
+            else:
+                ks, spacing, masks = self.kvec_spacing, self.ptcl_spacing, ()
+            cs = [self._neg_k(k, spacing) for k in ks]
+            if green_kernel == 1:
+                c = np.float32(spacing)
+                ks = [(np.float32(2) * np.sin(k * c / np.float32(2)) / c).astype(np.float32) for k in ks]
+            parts = list(ks) + cs + list(masks)
+            self._tables[key] = torch.from_numpy(np.concatenate(parts).astype(np.float32)).to(device)
+        return self._tables[key]

@@ -1,0 +1,563 @@
+// Cell sort, deterministic CIC scatter, CIC gather and their adjoints.
+//
+// Reference semantics: cic/enmesh.py:34-165 (binning, weights, weight
+// gradients), cic/scatter.py:315-437 and cic/gather.py:452-548 (forward and
+// hand-written VJPs), cic/pallas.py:268-409 (the GPU kernels this replaces).
+//
+// B200 design:
+//  * particles are counting-sorted by the mesh row (x, y) of their lower CIC
+//    corner.  Bin order is the reference's raveled cell-key order
+//    ((x*My + y)*Mz + z, core/utils.py:292-326) at row granularity;
+//  * the scatter is a pull kernel: one CTA owns an RX x RY block of output
+//    rows, reads the particles of the (RX+1) x (RY+1) source rows that can
+//    reach it, and accumulates in shared memory in 64-bit fixed point.  The
+//    result is independent of accumulation order (bit-deterministic), every
+//    output cell is written exactly once with coalesced stores, and no
+//    global atomics or mesh zero-fill pass are needed;
+//  * gathers and adjoint position terms walk particles in sorted order so the
+//    eight corner loads of neighbouring threads hit the same cache lines.
+#include <cstdio>
+
+#include "pmb_common.cuh"
+#include "pmb_kernels.cuh"
+
+namespace pmb {
+
+// ---------------------------------------------------------------------------
+// Binning
+// ---------------------------------------------------------------------------
+struct Binned {
+  int cx, cy, cz;
+  float fx, fy, fz;
+};
+
+__device__ __forceinline__ Binned bin_particle(const int16_t* __restrict__ pmid, const float d0, const float d1,
+                                               const float d2, int64_t i, Mesh3 m, float cell) {
+  Binned b;
+  float q0 = __fdiv_rn(d0, cell), q1 = __fdiv_rn(d1, cell), q2 = __fdiv_rn(d2, cell);
+  float l0 = floorf(q0), l1 = floorf(q1), l2 = floorf(q2);
+  b.fx = __fsub_rn(q0, l0);
+  b.fy = __fsub_rn(q1, l1);
+  b.fz = __fsub_rn(q2, l2);
+  b.cx = pmod((int)pmid[3 * i + 0] + (int)l0, m.nx);
+  b.cy = pmod((int)pmid[3 * i + 1] + (int)l1, m.ny);
+  b.cz = pmod((int)pmid[3 * i + 2] + (int)l2, m.nz);
+  return b;
+}
+
+// Count particles per row.  Optionally applies the drift disp += vel * D
+// first (integrator.py:223-225, two roundings as in the reference) and writes
+// the drifted displacement back.  Ranks come from warp-aggregated atomics.
+__global__ void bin_count_kernel(const int16_t* __restrict__ pmid, float* __restrict__ disp,
+                                 const float* __restrict__ vel, float drift, int64_t n, Mesh3 m, float cell,
+                                 uint32_t* __restrict__ counts, uint32_t* __restrict__ row_of,
+                                 uint32_t* __restrict__ rank_of) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = i < n;
+  uint32_t row = 0xFFFFFFFFu;
+  if (active) {
+    float d0 = disp[3 * i], d1 = disp[3 * i + 1], d2 = disp[3 * i + 2];
+    if (vel != nullptr) {
+      d0 = __fadd_rn(d0, __fmul_rn(vel[3 * i], drift));
+      d1 = __fadd_rn(d1, __fmul_rn(vel[3 * i + 1], drift));
+      d2 = __fadd_rn(d2, __fmul_rn(vel[3 * i + 2], drift));
+      disp[3 * i] = d0;
+      disp[3 * i + 1] = d1;
+      disp[3 * i + 2] = d2;
+    }
+    Binned b = bin_particle(pmid, d0, d1, d2, i, m, cell);
+    row = (uint32_t)((int64_t)b.cx * m.ny + b.cy);
+  }
+  unsigned full = __ballot_sync(0xFFFFFFFFu, active);
+  if (!active) return;
+  unsigned peers = __match_any_sync(full, row);
+  int leader = __ffs(peers) - 1;
+  int lane = threadIdx.x & 31;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(&counts[row], (uint32_t)__popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  row_of[i] = row;
+  rank_of[i] = base + __popc(peers & ((1u << lane) - 1u));
+}
+
+__global__ void bin_place_kernel(const int16_t* __restrict__ pmid, const float* __restrict__ disp, int64_t n,
+                                 Mesh3 m, float cell, const uint32_t* __restrict__ offs,
+                                 const uint32_t* __restrict__ row_of, const uint32_t* __restrict__ rank_of,
+                                 Rec* __restrict__ rec, uint32_t* __restrict__ perm) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Binned b = bin_particle(pmid, disp[3 * i], disp[3 * i + 1], disp[3 * i + 2], i, m, cell);
+  uint32_t dst = offs[row_of[i]] + rank_of[i];
+  Rec r;
+  r.fx = b.fx;
+  r.fy = b.fy;
+  r.fz = b.fz;
+  r.key = (uint32_t)(((int64_t)b.cx * m.ny + b.cy) * m.nz + b.cz);
+  rec[dst] = r;
+  perm[dst] = (uint32_t)i;
+}
+
+// Exclusive scan of row counts, three phases over tiles of 4096 entries.
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 4;
+constexpr int kScanTile = kScanThreads * kScanPer;
+
+__device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* sh, uint32_t* total) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < (blockDim.x >> 5) ? sh[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+      if (lane >= o) w += y;
+    }
+    sh[lane] = w;
+  }
+  __syncthreads();
+  uint32_t warp_off = warp ? sh[warp - 1] : 0;
+  if (total) *total = sh[(blockDim.x >> 5) - 1];
+  uint32_t r = warp_off + x - v;
+  __syncthreads();
+  return r;
+}
+
+__global__ void scan_tiles_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int64_t n,
+                                  uint32_t* __restrict__ tile_sums) {
+  __shared__ uint32_t sh[32];
+  int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanPer;
+  uint32_t v[kScanPer];
+  uint32_t s = 0;
+  for (int j = 0; j < kScanPer; ++j) {
+    v[j] = (base + j < n) ? in[base + j] : 0u;
+    s += v[j];
+  }
+  uint32_t total;
+  uint32_t off = block_exclusive_scan(s, sh, &total);
+  for (int j = 0; j < kScanPer; ++j) {
+    if (base + j < n) out[base + j] = off;
+    off += v[j];
+  }
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void scan_sums_kernel(uint32_t* __restrict__ sums, int64_t ntiles, uint32_t* __restrict__ grand) {
+  __shared__ uint32_t sh[32];
+  uint32_t carry = 0;
+  for (int64_t b = 0; b < ntiles; b += blockDim.x) {
+    int64_t i = b + threadIdx.x;
+    uint32_t v = i < ntiles ? sums[i] : 0u;
+    uint32_t total;
+    uint32_t off = block_exclusive_scan(v, sh, &total);
+    if (i < ntiles) sums[i] = carry + off;
+    carry += total;
+  }
+  if (threadIdx.x == 0) *grand = carry;
+}
+
+__global__ void scan_add_kernel(uint32_t* __restrict__ out, int64_t n, const uint32_t* __restrict__ sums) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] += sums[i / kScanTile];
+}
+
+int64_t scan_tmp_elems(int64_t len) { return (len + kScanTile - 1) / kScanTile + 1; }
+
+// Exclusive scan of len uint32 values (in == out allowed); tile_sums needs
+// scan_tmp_elems(len) entries.
+int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t len, uint32_t* tile_sums, cudaStream_t s) {
+  if (len <= 0) return kOk;
+  const int64_t ntiles = (len + kScanTile - 1) / kScanTile;
+  scan_tiles_kernel<<<(unsigned)ntiles, kScanThreads, 0, s>>>(in, out, len, tile_sums);
+  scan_sums_kernel<<<1, 1024, 0, s>>>(tile_sums, ntiles, tile_sums + ntiles);
+  scan_add_kernel<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(out, len, tile_sums);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int64_t bin_scratch_bytes(int64_t n, Mesh3 m) {
+  int64_t rows = m.rows();
+  int64_t ntiles = (rows + 1 + kScanTile - 1) / kScanTile;
+  return align_up(4 * (rows + 1), 256) * 2 + align_up(4 * n, 256) * 2 + align_up(4 * (ntiles + 1), 256);
+}
+
+// Sort particles by lower-corner row.  Outputs rec[n], perm[n] and
+// offs[rows + 1] (offs lives inside the caller's scratch, returned pointer).
+int bin_particles(const int16_t* pmid, float* disp, const float* vel, float drift, int64_t n, Mesh3 m, float cell,
+                  Rec* rec, uint32_t* perm, uint32_t* offs, void* scratch, cudaStream_t s) {
+  int64_t rows = m.rows();
+  char* p = (char*)scratch;
+  uint32_t* counts = (uint32_t*)p;
+  p += align_up(4 * (rows + 1), 256);
+  uint32_t* row_of = (uint32_t*)p;
+  p += align_up(4 * n, 256);
+  uint32_t* rank_of = (uint32_t*)p;
+  p += align_up(4 * n, 256);
+  uint32_t* tile_sums = (uint32_t*)p;
+  int64_t len = rows + 1;
+  int64_t ntiles = (len + kScanTile - 1) / kScanTile;
+  PMB_CUDA_CHECK(cudaMemsetAsync(counts, 0, 4 * len, s));
+  if (n > 0) {
+    int th = 256;
+    bin_count_kernel<<<(unsigned)((n + th - 1) / th), th, 0, s>>>(pmid, disp, vel, drift, n, m, cell, counts, row_of,
+                                                                    rank_of);
+  }
+  (void)ntiles;
+  int st = exclusive_scan_u32(counts, offs, len, tile_sums, s);
+  if (st != kOk) return st;
+  if (n > 0) {
+    int th = 256;
+    bin_place_kernel<<<(unsigned)((n + th - 1) / th), th, 0, s>>>(pmid, disp, n, m, cell, offs, row_of, rank_of,
+                                                                    rec, perm);
+  }
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// Fixed-point scale for the deterministic scatter
+// ---------------------------------------------------------------------------
+// Contributions val*w are converted to int64 units of 1/scale with
+// scale = 2^e / max|val|, e = 62 - ceil(log2(n + 1)), so that the sum of up to
+// n contributions of magnitude <= max|val| cannot overflow.
+__global__ void absmax_kernel(const float* __restrict__ v, int64_t count, unsigned int* __restrict__ out) {
+  float mx = 0.f;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+    float a = fabsf(v[i]);
+    if (a > mx || a != a) mx = (a != a) ? __int_as_float(0x7f800000) : a;
+  }
+  for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(mx));
+}
+
+__global__ void scale_from_absmax_kernel(const unsigned int* __restrict__ bits, double pow2e, double* __restrict__ scale) {
+  float mx = __uint_as_float(*bits);
+  // A non-finite maximum leaves no usable scale: flag it with a NaN scale.
+  if (!(mx < __int_as_float(0x7f800000))) {
+    *scale = __longlong_as_double(0x7ff8000000000000ll);
+    return;
+  }
+  *scale = mx > 0.f ? pow2e / (double)mx : 1.0;
+}
+
+double fixed_point_pow2(int64_t n) {
+  int e = 62;
+  int64_t t = n + 1;
+  int lg = 0;
+  while ((int64_t(1) << lg) < t) ++lg;
+  e -= lg;
+  if (e > 52) e = 52;
+  return ldexp(1.0, e);
+}
+
+int compute_scale(const float* val, int64_t count, int64_t n, double* scale_dev, unsigned int* tmp, cudaStream_t s) {
+  PMB_CUDA_CHECK(cudaMemsetAsync(tmp, 0, sizeof(unsigned int), s));
+  if (count > 0) {
+    int blocks = (int)((count + 255) / 256);
+    if (blocks > 4096) blocks = 4096;
+    absmax_kernel<<<blocks, 256, 0, s>>>(val, count, tmp);
+  }
+  scale_from_absmax_kernel<<<1, 1, 0, s>>>(tmp, fixed_point_pow2(n), scale_dev);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// Pull scatter
+// ---------------------------------------------------------------------------
+// Epilogue: mode 0 writes the density sum, mode 1 writes the Poisson source
+// (rho - 1) * src_mul (gravity.py:628-630), both in float.
+template <int C>
+__global__ void __launch_bounds__(256) scatter_pull_kernel(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm,
+                                                           const uint32_t* __restrict__ offs, Mesh3 m, int RX, int RY,
+                                                           const float* __restrict__ val, float val_const,
+                                                           const double* __restrict__ scale_dev, int mode,
+                                                           float src_mul, float* __restrict__ out) {
+  extern __shared__ long long acc[];  // [RX][RY][C][nz]
+  const int nby = (m.ny + RY - 1) / RY;
+  const int x0 = (int)(blockIdx.x / nby) * RX;
+  const int y0 = (int)(blockIdx.x % nby) * RY;
+  const int nz = m.nz;
+  const int64_t total = (int64_t)RX * RY * C * nz;
+  for (int64_t t = threadIdx.x; t < total; t += blockDim.x) acc[t] = 0;
+  __syncthreads();
+  const double scale = *scale_dev;
+  for (int sx = -1; sx < RX; ++sx) {
+    const int px = pmod(x0 + sx, m.nx);
+    for (int sy = -1; sy < RY; ++sy) {
+      const int py = pmod(y0 + sy, m.ny);
+      const int64_t row = (int64_t)px * m.ny + py;
+      const uint32_t beg = offs[row], end = offs[row + 1];
+      for (uint32_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+        const Rec r = rec[i];
+        const int cz = (int)(r.key % (uint32_t)nz);
+        float v[C];
+        if (val != nullptr) {
+          const uint32_t src = perm[i];
+#pragma unroll
+          for (int c = 0; c < C; ++c) v[c] = val[(int64_t)src * C + c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < C; ++c) v[c] = val_const;
+        }
+#pragma unroll
+        for (int bx = 0; bx < 2; ++bx) {
+          const int lx = sx + bx;
+          if (lx < 0 || lx >= RX || x0 + lx >= m.nx) continue;
+          const float wx = axis_weight(r.fx, bx);
+#pragma unroll
+          for (int by = 0; by < 2; ++by) {
+            const int ly = sy + by;
+            if (ly < 0 || ly >= RY || y0 + ly >= m.ny) continue;
+            const float wxy = __fmul_rn(wx, axis_weight(r.fy, by));
+#pragma unroll
+            for (int bz = 0; bz < 2; ++bz) {
+              int z = cz + bz;
+              if (z >= nz) z -= nz;
+              const float w = __fmul_rn(wxy, axis_weight(r.fz, bz));
+#pragma unroll
+              for (int c = 0; c < C; ++c) {
+                const float contrib = __fmul_rn(v[c], w);
+                const long long q = __double2ll_rn((double)contrib * scale);
+                atomicAdd((unsigned long long*)&acc[(((int64_t)lx * RY + ly) * C + c) * nz + z],
+                          (unsigned long long)q);
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  const double inv = 1.0 / scale;
+  const int64_t cells = m.cells();
+  for (int64_t t = threadIdx.x; t < total; t += blockDim.x) {
+    const int z = (int)(t % nz);
+    int64_t rest = t / nz;
+    const int c = (int)(rest % C);
+    rest /= C;
+    const int ly = (int)(rest % RY);
+    const int lx = (int)(rest / RY);
+    if (x0 + lx >= m.nx || y0 + ly >= m.ny) continue;
+    float rho = (float)((double)acc[t] * inv);
+    if (mode == 1) rho = __fmul_rn(__fsub_rn(rho, 1.0f), src_mul);
+    out[(int64_t)c * cells + ((int64_t)(x0 + lx) * m.ny + (y0 + ly)) * nz + z] = rho;
+  }
+}
+
+void scatter_block_shape(Mesh3 m, int C, int* RX, int* RY) {
+  // Keep the fixed-point accumulator at <= 96 KB so two CTAs fit per SM.
+  const int64_t budget = 96 * 1024;
+  int rx = 2, ry = 4;
+  while ((int64_t)rx * ry * C * m.nz * 8 > budget && (rx > 1 || ry > 1)) {
+    if (ry > rx) ry /= 2; else rx /= 2;
+  }
+  *RX = rx < m.nx ? rx : m.nx;
+  *RY = ry < m.ny ? ry : m.ny;
+}
+
+int scatter_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, Mesh3 m, int C, const float* val,
+                   float val_const, const double* scale_dev, int mode, float src_mul, float* out, cudaStream_t s) {
+  int RX, RY;
+  scatter_block_shape(m, C, &RX, &RY);
+  const size_t smem = (size_t)RX * RY * C * m.nz * sizeof(long long);
+  if (smem > 200 * 1024) return kUnsupported;
+  const int nbx = (m.nx + RX - 1) / RX, nby = (m.ny + RY - 1) / RY;
+  const unsigned grid = (unsigned)((int64_t)nbx * nby);
+#define PMB_LAUNCH_SCATTER(CC)                                                                                   \
+  do {                                                                                                           \
+    static bool attr_##CC = false;                                                                               \
+    if (!attr_##CC) {                                                                                            \
+      PMB_CUDA_CHECK(cudaFuncSetAttribute(scatter_pull_kernel<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                          200 * 1024));                                                         \
+      attr_##CC = true;                                                                                          \
+    }                                                                                                            \
+    scatter_pull_kernel<CC><<<grid, 256, smem, s>>>(rec, perm, offs, m, RX, RY, val, val_const, scale_dev, mode, \
+                                                     src_mul, out);                                             \
+  } while (0)
+  switch (C) {
+    case 1: PMB_LAUNCH_SCATTER(1); break;
+    case 2: PMB_LAUNCH_SCATTER(2); break;
+    case 3: PMB_LAUNCH_SCATTER(3); break;
+    case 4: PMB_LAUNCH_SCATTER(4); break;
+    default: return kUnsupported;
+  }
+#undef PMB_LAUNCH_SCATTER
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// Gather and adjoint position terms
+// ---------------------------------------------------------------------------
+struct Corners {
+  int64_t idx[8];
+  float w[8];
+};
+
+__device__ __forceinline__ void corners_of(const Rec& r, Mesh3 m, Corners& k) {
+  const uint32_t key = r.key;
+  const int cz = (int)(key % (uint32_t)m.nz);
+  const uint32_t rowk = key / (uint32_t)m.nz;
+  const int cy = (int)(rowk % (uint32_t)m.ny);
+  const int cx = (int)(rowk / (uint32_t)m.ny);
+  const int x1 = cx + 1 == m.nx ? 0 : cx + 1;
+  const int y1 = cy + 1 == m.ny ? 0 : cy + 1;
+  const int z1 = cz + 1 == m.nz ? 0 : cz + 1;
+  const float wx[2] = {axis_weight(r.fx, 0), axis_weight(r.fx, 1)};
+  const float wy[2] = {axis_weight(r.fy, 0), axis_weight(r.fy, 1)};
+  const float wz[2] = {axis_weight(r.fz, 0), axis_weight(r.fz, 1)};
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int bx = c & 1, by = (c >> 1) & 1, bz = (c >> 2) & 1;
+    const int x = bx ? x1 : cx, y = by ? y1 : cy, z = bz ? z1 : cz;
+    k.idx[c] = ((int64_t)x * m.ny + y) * m.nz + z;
+    k.w[c] = __fmul_rn(__fmul_rn(wx[bx], wy[by]), wz[bz]);
+  }
+}
+
+// out[src, c] = sum_b mesh_c[i_b] w_b (gather.py:452-472, pallas.py:305-318).
+// With kick != 0 the second half-kick vel += out * kick is applied in place
+// (integrator.py:536), saving a pass over the particles.
+template <int C>
+__global__ void gather_kernel(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm, int64_t n, Mesh3 m,
+                              const float* __restrict__ mesh, float* __restrict__ out, float* __restrict__ vel,
+                              float kick) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Rec r = rec[i];
+  const uint32_t src = perm[i];
+  Corners k;
+  corners_of(r, m, k);
+  const int64_t cells = m.cells();
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const float* mc = mesh + (int64_t)c * cells;
+    float a = 0.f;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) a = __fadd_rn(a, __fmul_rn(__ldg(mc + k.idx[b]), k.w[b]));
+    out[(int64_t)src * C + c] = a;
+    if (vel != nullptr) vel[(int64_t)src * C + c] = __fadd_rn(vel[(int64_t)src * C + c], __fmul_rn(a, kick));
+  }
+}
+
+int gather_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int C, const float* mesh, float* out,
+                  float* vel, float kick, cudaStream_t s) {
+  if (n == 0) return kOk;
+  const int th = 256;
+  const unsigned g = (unsigned)((n + th - 1) / th);
+  switch (C) {
+    case 1: gather_kernel<1><<<g, th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick); break;
+    case 2: gather_kernel<2><<<g, th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick); break;
+    case 3: gather_kernel<3><<<g, th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick); break;
+    case 4: gather_kernel<4><<<g, th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick); break;
+    default: return kUnsupported;
+  }
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+// Position term of the CIC adjoints.  With per-particle weights u (N, C) or a
+// constant u_const:
+//   inner_b = sum_c u_c * mesh_c[i_b]
+//   disp_cot[src] (+)= (sum_b inner_b * grad w_b) / cell
+// This is gather.py:495-502 (u = val_cot) and scatter.py:366-370 (u = val).
+// Optionally also emits wsum[src, c] = sum_b mesh_c[i_b] w_b (the scatter
+// adjoint's val cotangent, scatter.py:372-373) and accumulates
+// dot = sum_src sum_c u_c * extra[src, c] in FP64 (used for cosmology
+// cotangents).
+template <int C>
+__global__ void interp_grad_kernel(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm, int64_t n, Mesh3 m,
+                                   const float* __restrict__ mesh, const float* __restrict__ u, float u_const,
+                                   float cell, int accumulate, float* __restrict__ disp_cot,
+                                   float* __restrict__ wsum) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Rec r = rec[i];
+  const uint32_t src = perm[i];
+  const uint32_t key = r.key;
+  const int cz = (int)(key % (uint32_t)m.nz);
+  const uint32_t rowk = key / (uint32_t)m.nz;
+  const int cy = (int)(rowk % (uint32_t)m.ny);
+  const int cx = (int)(rowk / (uint32_t)m.ny);
+  const int x1 = cx + 1 == m.nx ? 0 : cx + 1;
+  const int y1 = cy + 1 == m.ny ? 0 : cy + 1;
+  const int z1 = cz + 1 == m.nz ? 0 : cz + 1;
+  const float f[3] = {r.fx, r.fy, r.fz};
+  float wa[3][2], sg[3][2];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    wa[a][0] = axis_weight(f[a], 0);
+    wa[a][1] = axis_weight(f[a], 1);
+    sg[a][0] = axis_sign(f[a], 0);
+    sg[a][1] = axis_sign(f[a], 1);
+  }
+  float uu[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) uu[c] = u ? u[(int64_t)src * C + c] : u_const;
+  const int64_t cells = m.cells();
+  float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+  float ws[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) ws[c] = 0.f;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const int bx = b & 1, by = (b >> 1) & 1, bz = (b >> 2) & 1;
+    const int64_t idx = ((int64_t)(bx ? x1 : cx) * m.ny + (by ? y1 : cy)) * m.nz + (bz ? z1 : cz);
+    float inner = 0.f;
+    const float w = __fmul_rn(__fmul_rn(wa[0][bx], wa[1][by]), wa[2][bz]);
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const float mv = __ldg(mesh + (int64_t)c * cells + idx);
+      inner = __fadd_rn(inner, __fmul_rn(uu[c], mv));
+      ws[c] = __fadd_rn(ws[c], __fmul_rn(mv, w));
+    }
+    // grad_i = sign_i * w_{i+1} * w_{i+2} (enmesh.py:155-160)
+    const float gx = __fmul_rn(__fmul_rn(sg[0][bx], wa[1][by]), wa[2][bz]);
+    const float gy = __fmul_rn(__fmul_rn(sg[1][by], wa[2][bz]), wa[0][bx]);
+    const float gz = __fmul_rn(__fmul_rn(sg[2][bz], wa[0][bx]), wa[1][by]);
+    g0 = __fadd_rn(g0, __fmul_rn(inner, gx));
+    g1 = __fadd_rn(g1, __fmul_rn(inner, gy));
+    g2 = __fadd_rn(g2, __fmul_rn(inner, gz));
+  }
+  g0 = __fdiv_rn(g0, cell);
+  g1 = __fdiv_rn(g1, cell);
+  g2 = __fdiv_rn(g2, cell);
+  float* dc = disp_cot + 3 * (int64_t)src;
+  if (accumulate) {
+    dc[0] = __fadd_rn(dc[0], g0);
+    dc[1] = __fadd_rn(dc[1], g1);
+    dc[2] = __fadd_rn(dc[2], g2);
+  } else {
+    dc[0] = g0;
+    dc[1] = g1;
+    dc[2] = g2;
+  }
+  if (wsum != nullptr) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) wsum[(int64_t)src * C + c] = ws[c];
+  }
+}
+
+int interp_grad_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int C, const float* mesh,
+                       const float* u, float u_const, float cell, int accumulate, float* disp_cot, float* wsum,
+                       cudaStream_t s) {
+  if (n == 0) return kOk;
+  const int th = 256;
+  const unsigned g = (unsigned)((n + th - 1) / th);
+  switch (C) {
+    case 1: interp_grad_kernel<1><<<g, th, 0, s>>>(rec, perm, n, m, mesh, u, u_const, cell, accumulate, disp_cot, wsum); break;
+    case 2: interp_grad_kernel<2><<<g, th, 0, s>>>(rec, perm, n, m, mesh, u, u_const, cell, accumulate, disp_cot, wsum); break;
+    case 3: interp_grad_kernel<3><<<g, th, 0, s>>>(rec, perm, n, m, mesh, u, u_const, cell, accumulate, disp_cot, wsum); break;
+    case 4: interp_grad_kernel<4><<<g, th, 0, s>>>(rec, perm, n, m, mesh, u, u_const, cell, accumulate, disp_cot, wsum); break;
+    default: return kUnsupported;
+  }
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+}  // namespace pmb

@@ -1,0 +1,93 @@
+// Shared definitions for the PM++ B200 kernels.
+//
+// Layout conventions (all C order, row-major):
+//   pmid   int16  (N, 3)       anchor mesh cell of each particle
+//   disp   float  (N, 3)       comoving displacement from pmid * cell
+//   vel/acc float (N, 3)
+//   mesh   float  (C, Mx, My, Mz)          planar channels
+//   spec   float2 (C, Mx, My, Mz/2 + 1)    rFFT half spectra
+// A "row" is the z-line (x, y) of the mesh; the cell sort bins particles by
+// the row of their lower CIC corner, so bin order equals raveled-cell order.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pmb {
+
+// Status codes returned by every C-ABI entry point.
+enum Status : int {
+  kOk = 0,
+  kInvalidArgument = -1,
+  kCudaError = -2,
+  kCufftError = -3,
+  kUnsupported = -4,
+  kScratchTooSmall = -5,
+};
+
+struct Mesh3 {
+  int nx, ny, nz;
+  __host__ __device__ int64_t rows() const { return (int64_t)nx * ny; }
+  __host__ __device__ int64_t cells() const { return (int64_t)nx * ny * nz; }
+  __host__ __device__ int64_t half_cells() const { return (int64_t)nx * ny * (nz / 2 + 1); }
+};
+
+__host__ __device__ inline int pmod(int a, int m) {
+  int r = a % m;
+  return r < 0 ? r + m : r;
+}
+
+__host__ __device__ inline int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+
+// Particle binning shared by every CIC kernel.  Restates the float32
+// arithmetic of the reference enmesh (cic/enmesh.py:139-149) and the Pallas
+// coordinate helper (cic/pallas.py:225-256): d = disp / cell in IEEE float
+// (no fast-math), lower corner i = pmid + floor(d), fraction f = d - floor(d)
+// (exact in float).  The per-axis corner weight is 1 - |f - b| evaluated in
+// float, which reproduces 1 - |d - (floor(d) + b)| bit for bit.
+__device__ __forceinline__ float axis_weight(float f, int b) {
+  return __fsub_rn(1.0f, fabsf(b ? __fsub_rn(f, 1.0f) : f));
+}
+// sign(-(f - b)) as in enmesh.py:155 (0 exactly at f == b).
+__device__ __forceinline__ float axis_sign(float f, int b) {
+  float d = b ? __fsub_rn(f, 1.0f) : f;
+  return d < 0.0f ? 1.0f : (d > 0.0f ? -1.0f : 0.0f);
+}
+
+// Sorted particle record: fractions along x, y, z and the raveled lower cell.
+struct __align__(16) Rec {
+  float fx, fy, fz;
+  uint32_t key;
+};
+
+// Spectral description of one mesh: per-axis wavenumbers, the derivative
+// factors c (neg_ik = i c, Nyquist zeroed) and the optional particle-Nyquist
+// masks, all in float precision, built on the host with the reference
+// formulas (numerics/fft.py:4-44, core/configuration.py:365-376,
+// core/utils.py:15-37).
+struct SpecTables {
+  const float* kx;
+  const float* ky;
+  const float* kz;
+  const float* cx;
+  const float* cy;
+  const float* cz;
+  const float* mx;  // may be null (mesh == particle grid)
+  const float* my;
+  const float* mz;
+};
+
+}  // namespace pmb
+
+#define PMB_CUDA_CHECK(expr)                         \
+  do {                                               \
+    cudaError_t _e = (expr);                         \
+    if (_e != cudaSuccess) {                         \
+      pmb::set_last_error(cudaGetErrorString(_e));   \
+      return pmb::kCudaError;                        \
+    }                                                \
+  } while (0)
+
+namespace pmb {
+void set_last_error(const char* msg);
+}

@@ -1,0 +1,44 @@
+// Internal (C++) interfaces between the kernel files and the C-ABI layer.
+#pragma once
+
+#include <cufft.h>
+
+#include "pmb_common.cuh"
+
+namespace pmb {
+
+// cic.cu
+int64_t scan_tmp_elems(int64_t len);
+int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t len, uint32_t* tile_sums, cudaStream_t s);
+int64_t bin_scratch_bytes(int64_t n, Mesh3 m);
+int bin_particles(const int16_t* pmid, float* disp, const float* vel, float drift, int64_t n, Mesh3 m, float cell,
+                  Rec* rec, uint32_t* perm, uint32_t* offs, void* scratch, cudaStream_t s);
+double fixed_point_pow2(int64_t n);
+int compute_scale(const float* val, int64_t count, int64_t n, double* scale_dev, unsigned int* tmp, cudaStream_t s);
+int scatter_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, Mesh3 m, int C, const float* val,
+                   float val_const, const double* scale_dev, int mode, float src_mul, float* out, cudaStream_t s);
+int gather_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int C, const float* mesh, float* out,
+                  float* vel, float kick, cudaStream_t s);
+int interp_grad_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int C, const float* mesh,
+                       const float* u, float u_const, float cell, int accumulate, float* disp_cot, float* wsum,
+                       cudaStream_t s);
+
+// spectral.cu
+int fft_r2c(Mesh3 m, int batch, float* in, float2* out, void* work, cudaStream_t s);
+int fft_c2r(Mesh3 m, int batch, float2* in, float* out, void* work, cudaStream_t s);
+int64_t fft_work_bytes(Mesh3 m, int batch);
+// Gravity spectral multipliers (see spectral.cu for the exact semantics).
+struct GreenParams {
+  int green_kernel;     // 0 continuum -1/k^2, 1 discrete Laplacian
+  float cell;           // mesh cell size (discrete Laplacian)
+  const float* transfer;  // optional real transfer per half-spectrum cell, may be null
+  const float* radial;    // optional radial table indexed by integer n^2, may be null
+  int radial_len;
+  float post_scale;       // applied last (1/M folds the inverse-FFT normalisation in)
+};
+int green_gradient(const float2* src_hat, float2* grad_hat, Mesh3 m, SpecTables t, GreenParams g, cudaStream_t s);
+int green_gradient_adjoint(const float2* grad_cot_hat, float2* src_cot_hat, Mesh3 m, SpecTables t, GreenParams g,
+                           cudaStream_t s);
+int scale_real(float* x, int64_t count, float a, float b, cudaStream_t s);
+
+}  // namespace pmb

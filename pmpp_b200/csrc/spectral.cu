@@ -1,0 +1,244 @@
+// Spectral stages of the PM force: cuFFT R2C/C2R plans with caller-provided
+// work areas, the fused Green's-function x gradient multiplier and its
+// adjoint, and the FP64 power-spectrum shell sums.
+//
+// Reference semantics: nbody/gravity.py:174-196 (particle-Nyquist masks),
+// :283-352 (continuum and discrete-Laplacian Poisson kernels), :355-391 and
+// core/configuration.py:365-376 (spectral gradient with the Nyquist
+// derivative zeroed), corrections/core.py:333-334 (multiplicative transfer),
+// analysis/power_spectrum.py:106-143 (shell sums).
+#include <cufft.h>
+
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "pmb_common.cuh"
+#include "pmb_kernels.cuh"
+
+namespace pmb {
+
+// ---------------------------------------------------------------------------
+// cuFFT plan cache.  Plans are created once per (device, shape, batch, kind)
+// without auto-allocation; every execution binds the caller's work area, so
+// the library never allocates device memory per call.
+// ---------------------------------------------------------------------------
+namespace {
+struct PlanKey {
+  int dev, nx, ny, nz, batch, kind;
+  bool operator<(const PlanKey& o) const {
+    return std::tie(dev, nx, ny, nz, batch, kind) < std::tie(o.dev, o.nx, o.ny, o.nz, o.batch, o.kind);
+  }
+};
+struct PlanVal {
+  cufftHandle h;
+  size_t work;
+};
+std::mutex g_plan_mu;
+std::map<PlanKey, PlanVal>& plans() {
+  static std::map<PlanKey, PlanVal> p;
+  return p;
+}
+
+int get_plan(Mesh3 m, int batch, int kind, PlanVal* out) {
+  int dev = 0;
+  PMB_CUDA_CHECK(cudaGetDevice(&dev));
+  PlanKey key{dev, m.nx, m.ny, m.nz, batch, kind};
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  auto it = plans().find(key);
+  if (it != plans().end()) {
+    *out = it->second;
+    return kOk;
+  }
+  cufftHandle h;
+  if (cufftCreate(&h) != CUFFT_SUCCESS) {
+    set_last_error("cufftCreate failed");
+    return kCufftError;
+  }
+  cufftSetAutoAllocation(h, 0);
+  long long n[3] = {m.nx, m.ny, m.nz};
+  long long rdist = (long long)m.cells();
+  long long cdist = (long long)m.half_cells();
+  size_t work = 0;
+  cufftResult r;
+  if (kind == 0) {
+    r = cufftMakePlanMany64(h, 3, n, nullptr, 1, rdist, nullptr, 1, cdist, CUFFT_R2C, batch, &work);
+  } else {
+    r = cufftMakePlanMany64(h, 3, n, nullptr, 1, cdist, nullptr, 1, rdist, CUFFT_C2R, batch, &work);
+  }
+  if (r != CUFFT_SUCCESS) {
+    cufftDestroy(h);
+    set_last_error("cufftMakePlanMany64 failed");
+    return kCufftError;
+  }
+  PlanVal v{h, work};
+  plans()[key] = v;
+  *out = v;
+  return kOk;
+}
+}  // namespace
+
+int64_t fft_work_bytes(Mesh3 m, int batch) {
+  PlanVal a, b;
+  if (get_plan(m, batch, 0, &a) != kOk) return -1;
+  if (get_plan(m, batch, 1, &b) != kOk) return -1;
+  return (int64_t)(a.work > b.work ? a.work : b.work);
+}
+
+int fft_r2c(Mesh3 m, int batch, float* in, float2* out, void* work, cudaStream_t s) {
+  PlanVal p;
+  int st = get_plan(m, batch, 0, &p);
+  if (st != kOk) return st;
+  if (cufftSetStream(p.h, s) != CUFFT_SUCCESS || cufftSetWorkArea(p.h, work) != CUFFT_SUCCESS ||
+      cufftExecR2C(p.h, in, (cufftComplex*)out) != CUFFT_SUCCESS) {
+    set_last_error("cufftExecR2C failed");
+    return kCufftError;
+  }
+  return kOk;
+}
+
+int fft_c2r(Mesh3 m, int batch, float2* in, float* out, void* work, cudaStream_t s) {
+  PlanVal p;
+  int st = get_plan(m, batch, 1, &p);
+  if (st != kOk) return st;
+  if (cufftSetStream(p.h, s) != CUFFT_SUCCESS || cufftSetWorkArea(p.h, work) != CUFFT_SUCCESS ||
+      cufftExecC2R(p.h, (cufftComplex*)in, out) != CUFFT_SUCCESS) {
+    set_last_error("cufftExecC2R failed");
+    return kCufftError;
+  }
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// Green's function x gradient
+// ---------------------------------------------------------------------------
+// K(k) = mask(k) * G(k) * T(k) with G = -1/k^2 (0 where k^2 == 0).
+// Forward:  phi = (-(S*mask)) / k2 * T ; grad_d = (i c_d) phi,  d = x, y, z.
+// The division is done component-wise in float, as the reference's
+// complex-by-real division (gravity.py:285, :350-352).
+__device__ __forceinline__ float k2_of(const SpecTables& t, int ix, int iy, int iz) {
+  const float kx = t.kx[ix], ky = t.ky[iy], kz = t.kz[iz];
+  return __fadd_rn(__fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky)), __fmul_rn(kz, kz));
+}
+
+__device__ __forceinline__ float transfer_of(const GreenParams& g, const SpecTables& t, int64_t j, int ix, int iy, int iz,
+                                             Mesh3 m) {
+  float T = 1.0f;
+  if (g.transfer != nullptr) T = g.transfer[j];
+  if (g.radial != nullptr) {
+    // integer mode numbers: |n|^2 indexes the radial table exactly
+    const int nx = ix < (m.nx + 1) / 2 ? ix : ix - m.nx;
+    const int ny = iy < (m.ny + 1) / 2 ? iy : iy - m.ny;
+    const long long n2 = (long long)nx * nx + (long long)ny * ny + (long long)iz * iz;
+    T = __fmul_rn(T, n2 < g.radial_len ? g.radial[n2] : 1.0f);
+  }
+  return T;
+}
+
+__global__ void green_gradient_kernel(const float2* __restrict__ src, float2* __restrict__ grad, Mesh3 m,
+                                      SpecTables t, GreenParams g) {
+  const int nzh = m.nz / 2 + 1;
+  const int64_t total = m.half_cells();
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
+    const int iz = (int)(j % nzh);
+    const int64_t r = j / nzh;
+    const int iy = (int)(r % m.ny);
+    const int ix = (int)(r / m.ny);
+    float2 v = src[j];
+    if (t.mx != nullptr) {
+      const float mk = __fmul_rn(__fmul_rn(t.mx[ix], t.my[iy]), t.mz[iz]);
+      v.x = __fmul_rn(v.x, mk);
+      v.y = __fmul_rn(v.y, mk);
+    }
+    const float k2 = k2_of(t, ix, iy, iz);
+    float pr = 0.f, pi = 0.f;
+    if (k2 != 0.f) {
+      pr = __fdiv_rn(-v.x, k2);
+      pi = __fdiv_rn(-v.y, k2);
+      if (g.transfer != nullptr || g.radial != nullptr) {
+        const float T = transfer_of(g, t, j, ix, iy, iz, m);
+        pr = __fmul_rn(pr, T);
+        pi = __fmul_rn(pi, T);
+      }
+    }
+    const float c[3] = {t.cx[ix], t.cy[iy], t.cz[iz]};
+    const float ps = g.post_scale;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      grad[(int64_t)d * total + j] = make_float2(__fmul_rn(-__fmul_rn(c[d], pi), ps), __fmul_rn(__fmul_rn(c[d], pr), ps));
+  }
+}
+
+// Adjoint: S_cot = K * sum_d conj(i c_d) A_d.  The force map is a real
+// convolution (H_d Hermitian), so its transpose is the correlation with the
+// conjugate multiplier.
+__global__ void green_gradient_adjoint_kernel(const float2* __restrict__ gc, float2* __restrict__ out, Mesh3 m,
+                                              SpecTables t, GreenParams g) {
+  const int nzh = m.nz / 2 + 1;
+  const int64_t total = m.half_cells();
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
+    const int iz = (int)(j % nzh);
+    const int64_t r = j / nzh;
+    const int iy = (int)(r % m.ny);
+    const int ix = (int)(r / m.ny);
+    const float c[3] = {t.cx[ix], t.cy[iy], t.cz[iz]};
+    float ar = 0.f, ai = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float2 a = gc[(int64_t)d * total + j];
+      ar = __fadd_rn(ar, __fmul_rn(c[d], a.y));
+      ai = __fsub_rn(ai, __fmul_rn(c[d], a.x));
+    }
+    const float k2 = k2_of(t, ix, iy, iz);
+    float pr = 0.f, pi = 0.f;
+    if (k2 != 0.f) {
+      if (g.transfer != nullptr || g.radial != nullptr) {
+        const float T = transfer_of(g, t, j, ix, iy, iz, m);
+        ar = __fmul_rn(ar, T);
+        ai = __fmul_rn(ai, T);
+      }
+      pr = __fdiv_rn(-ar, k2);
+      pi = __fdiv_rn(-ai, k2);
+      if (t.mx != nullptr) {
+        const float mk = __fmul_rn(__fmul_rn(t.mx[ix], t.my[iy]), t.mz[iz]);
+        pr = __fmul_rn(pr, mk);
+        pi = __fmul_rn(pi, mk);
+      }
+    }
+    out[j] = make_float2(__fmul_rn(pr, g.post_scale), __fmul_rn(pi, g.post_scale));
+  }
+}
+
+static unsigned grid_for(int64_t total, int th) {
+  int64_t b = (total + th - 1) / th;
+  int64_t cap = 148 * 32;
+  return (unsigned)(b < cap ? (b > 0 ? b : 1) : cap);
+}
+
+int green_gradient(const float2* src_hat, float2* grad_hat, Mesh3 m, SpecTables t, GreenParams g, cudaStream_t s) {
+  green_gradient_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(src_hat, grad_hat, m, t, g);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int green_gradient_adjoint(const float2* grad_cot_hat, float2* src_cot_hat, Mesh3 m, SpecTables t, GreenParams g,
+                           cudaStream_t s) {
+  green_gradient_adjoint_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(grad_cot_hat, src_cot_hat, m, t, g);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+// x = x * a + b, elementwise in float.
+__global__ void scale_real_kernel(float* __restrict__ x, int64_t n, float a, float b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = __fadd_rn(__fmul_rn(x[i], a), b);
+}
+
+int scale_real(float* x, int64_t count, float a, float b, cudaStream_t s) {
+  scale_real_kernel<<<grid_for(count, 256), 256, 0, s>>>(x, count, a, b);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+}  // namespace pmb

@@ -1,0 +1,178 @@
+"""Particle-mesh gravity and its adjoint (nbody/gravity.py:786-814).
+
+acc = gather(irfft((i c_d) K(k) rfft((rho - 1) * 1.5 Omega_m)))  for d = x, y, z
+with K = particle-Nyquist mask x Green's function x optional transfer.  The
+whole chain runs as one C-ABI call (pmb_force): sort, deterministic scatter
+straight into the Poisson source, R2C, fused Green x gradient, one batched
+C2R for the three force meshes, and a three-channel gather.
+
+``correction`` accepts None or an object with ``green_kernel`` (0 continuum,
+1 discrete Laplacian) and ``transfer_tables(a, cosmo, conf)`` returning
+(transfer half-spectrum tensor or None, radial |n|^2 table or None); see
+pmpp_b200/corrections.py.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from ._lib import call, lib
+from .runtime import StageTimer, ptr, require_cuda, stream_handle, workspace
+
+
+def _om32(omega_m):
+    return float(np.float32(omega_m))
+
+
+def _stage_buffers(n, conf, dev):
+    """Workspace views shared by the staged force and force adjoint."""
+    L = lib()
+    nx, ny, nz = conf.mesh_shape
+    M = conf.mesh_size
+    Mc = nx * ny * (nz // 2 + 1)
+    sorted_buf = workspace(L.pmb_sorted_bytes(n, nx, ny, nz), dev, "st_sorted")
+    sort_scr = workspace(L.pmb_sort_scratch_bytes(n, nx, ny, nz), dev, "st_sortscr")
+    s16 = workspace(16, dev, "st_s16")
+    real3 = workspace(12 * M, dev, "st_real3")
+    spec3 = workspace(24 * Mc, dev, "st_spec3")
+    spec1 = workspace(8 * Mc, dev, "st_spec1")
+    fw = max(L.pmb_fft_work_bytes(nx, ny, nz, 3), L.pmb_fft_work_bytes(nx, ny, nz, 1))
+    work = workspace(fw, dev, "st_fftwork")
+    return sorted_buf, sort_scr, s16, real3, spec3, spec1, work
+
+
+def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc, drift_vel, drift, vel_kick,
+                  kick, timer):
+    """pmb_force as separate stage calls with a CUDA event after each stage."""
+    n = pmid.shape[0]
+    nx, ny, nz = conf.mesh_shape
+    dev = disp.device
+    s = stream_handle(dev)
+    sorted_buf, sort_scr, s16, real3, spec3, spec1, work = _stage_buffers(n, conf, dev)
+    t = timer.start()
+    call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
+         float(conf.cell_size), sorted_buf.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
+    t = timer.mark("sort", t)
+    call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 1, None, float(conf.mesh_size / conf.ptcl_num), 1,
+         1.5 * _om32(omega_m), real3.data_ptr(), s16.data_ptr(), s)
+    t = timer.mark("scatter", t)
+    call("pmb_rfft3", nx, ny, nz, 1, real3.data_ptr(), spec1.data_ptr(), work.data_ptr(), s)
+    t = timer.mark("fft_r2c", t)
+    call("pmb_green_gradient", spec1.data_ptr(), spec3.data_ptr(), nx, ny, nz, tables.data_ptr(),
+         int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, float(1.0 / conf.mesh_size), s)
+    t = timer.mark("green_gradient", t)
+    call("pmb_irfft3", nx, ny, nz, 3, spec3.data_ptr(), F.data_ptr(), work.data_ptr(), s)
+    t = timer.mark("fft_c2r", t)
+    call("pmb_gather_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc.data_ptr(), ptr(vel_kick),
+         float(kick), s)
+    timer.mark("gather", t)
+
+
+def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc_cot, disp_cot, timer):
+    """pmb_force_vjp as separate stage calls with a CUDA event after each stage."""
+    n = pmid.shape[0]
+    nx, ny, nz = conf.mesh_shape
+    dev = disp.device
+    s = stream_handle(dev)
+    sorted_buf, sort_scr, s16, real3, spec3, spec1, work = _stage_buffers(n, conf, dev)
+    t = timer.start()
+    call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), None, 0.0, n, nx, ny, nz, float(conf.cell_size),
+         sorted_buf.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
+    t = timer.mark("sort", t)
+    call("pmb_interp_grad_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc_cot.data_ptr(), 0.0,
+         float(conf.cell_size), 1, disp_cot.data_ptr(), None, s)
+    t = timer.mark("gather_adjoint", t)
+    call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, acc_cot.data_ptr(), 0.0, 0, 1.0,
+         real3.data_ptr(), s16.data_ptr(), s)
+    t = timer.mark("scatter3", t)
+    call("pmb_rfft3", nx, ny, nz, 3, real3.data_ptr(), spec3.data_ptr(), work.data_ptr(), s)
+    t = timer.mark("fft_r2c", t)
+    post = float(np.float32(1.5 * _om32(omega_m)) / conf.mesh_size)
+    call("pmb_green_gradient_adjoint", spec3.data_ptr(), spec1.data_ptr(), nx, ny, nz, tables.data_ptr(),
+         int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, post, s)
+    t = timer.mark("green_gradient", t)
+    call("pmb_irfft3", nx, ny, nz, 1, spec1.data_ptr(), real3.data_ptr(), work.data_ptr(), s)
+    t = timer.mark("fft_c2r", t)
+    call("pmb_interp_grad_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 1, real3.data_ptr(), None,
+         float(conf.mesh_size / conf.ptcl_num), float(conf.cell_size), 1, disp_cot.data_ptr(), None, s)
+    timer.mark("scatter_adjoint", t)
+
+
+def _correction_args(correction, a, cosmo, conf):
+    if correction is None:
+        return 0, None, None, 0
+    gk = int(getattr(correction, "green_kernel", 0))
+    transfer, radial = correction.transfer_tables(a, cosmo, conf)
+    rl = 0 if radial is None else int(radial.numel())
+    return gk, transfer, radial, rl
+
+
+def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, force_meshes=None, acc=None,
+          drift_vel=None, drift=0.0, vel_kick=None, kick=0.0):
+    """One PM force evaluation on device tensors.
+
+    Returns (acc (N,3), force_meshes (3,Mx,My,Mz)).  With drift_vel the
+    particles are drifted first (disp updated in place); with vel_kick the
+    half-kick vel_kick += acc * kick is fused into the gather."""
+    require_cuda(pmid, disp, drift_vel, vel_kick)
+    n = pmid.shape[0]
+    nx, ny, nz = conf.mesh_shape
+    dev = disp.device
+    if force_meshes is None:
+        force_meshes = torch.empty((3, nx, ny, nz), dtype=torch.float32, device=dev)
+    if acc is None:
+        acc = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    gk, transfer, radial, rl = _correction_args(correction, a, cosmo, conf)
+    tables = conf.spectral_tables("mesh", dev, gk)
+    if StageTimer.active is not None:
+        _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc, drift_vel,
+                      drift, vel_kick, kick, StageTimer.active)
+        return acc, force_meshes
+    wb = lib().pmb_force_workspace_bytes(n, nx, ny, nz)
+    if wb < 0:
+        raise RuntimeError("pmb_force_workspace_bytes failed: " + lib().pmb_last_error().decode())
+    ws = workspace(wb, dev, "force")
+    call("pmb_force", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
+         float(conf.cell_size), float(conf.mesh_size / conf.ptcl_num), 1.5 * _om32(omega_m), tables.data_ptr(),
+         int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, force_meshes.data_ptr(),
+         acc.data_ptr(), ptr(vel_kick), float(kick), ws.data_ptr(), ws.numel(), stream_handle(dev))
+    return acc, force_meshes
+
+
+def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *, a=None, cosmo=None,
+              correction=None):
+    """disp_cot (+)= (d acc / d disp)^T acc_cot, with force_meshes computed at disp."""
+    require_cuda(pmid, disp, force_meshes, acc_cot, disp_cot)
+    n = pmid.shape[0]
+    nx, ny, nz = conf.mesh_shape
+    dev = disp.device
+    if disp_cot is None:
+        disp_cot = torch.zeros((n, 3), dtype=torch.float32, device=dev)
+    gk, transfer, radial, rl = _correction_args(correction, a, cosmo, conf)
+    tables = conf.spectral_tables("mesh", dev, gk)
+    if StageTimer.active is not None:
+        _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc_cot,
+                          disp_cot, StageTimer.active)
+        return disp_cot
+    wb = lib().pmb_force_vjp_workspace_bytes(n, nx, ny, nz)
+    ws = workspace(wb, dev, "force_vjp")
+    call("pmb_force_vjp", pmid.data_ptr(), disp.data_ptr(), n, nx, ny, nz, float(conf.cell_size),
+         float(conf.mesh_size / conf.ptcl_num), 1.5 * _om32(omega_m), tables.data_ptr(),
+         int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, force_meshes.data_ptr(),
+         acc_cot.data_ptr(), disp_cot.data_ptr(), ws.data_ptr(), ws.numel(), stream_handle(dev))
+    return disp_cot
+
+
+def gravity(a, ptcl, cosmo, conf, correction=None):
+    """Gravitational accelerations [H_0^2 L] (gravity.py:786-814)."""
+    acc, _ = force(ptcl.pmid, ptcl.disp, conf, cosmo.Omega_m, a=a, cosmo=cosmo, correction=correction)
+    return acc
+
+
+def gravity_vjp(a, ptcl, cosmo, conf, acc_cot, correction=None):
+    """Returns (disp_cot, Omega_m_cot) of gravity w.r.t. acc_cot."""
+    acc, F = force(ptcl.pmid, ptcl.disp.clone(), conf, cosmo.Omega_m, a=a, cosmo=cosmo, correction=correction)
+    dc = force_vjp(ptcl.pmid, ptcl.disp, conf, cosmo.Omega_m, F, acc_cot.contiguous(), a=a, cosmo=cosmo,
+                   correction=correction)
+    om_cot = float((acc_cot.double() * acc.double()).sum()) / _om32(cosmo.Omega_m)
+    return dc, om_cot

@@ -1,0 +1,196 @@
+"""Kick-drift-kick time integration and the hand-written reverse sweep.
+
+Forward (nbody/solver.py:253-273, nbody/integrator.py:689-731): an initial
+force, then per macro step the stages of ``symp_splits``.  With the default
+splits ((0, .5), (1, .5)) a step is  kick(a_p -> a_m), drift(a_p -> a_n),
+force(a_n), kick(a_m -> a_n); the drift is fused into the cell sort and the
+closing half-kick into the force gather, so a step is one axpy plus one
+fused force call.
+
+Reverse (nbody/solver.py:385-444, integrator.py:781-837): states are rebuilt
+algebraically (vel -= acc K, disp -= vel D) and the force at the earlier time
+is recomputed.  The force meshes of that recomputation are exactly the ones
+the next reverse step's force adjoint needs (same positions), so they are
+kept instead of being recomputed a third time: a reverse step costs one
+force adjoint plus one forward force.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from ._lib import call
+from .gravity import force, force_vjp, _om32
+from .particles import Particles
+from .runtime import stream_handle
+
+
+def _schedule(a_prev, a_next, conf):
+    """Stage list of one macro step (integrator.py:760-778)."""
+    D = K = 0
+    a_disp = a_vel = a_acc = a_prev
+    stages = []
+    for d, k in conf.symp_splits:
+        if d != 0:
+            D += d
+            a_disp_next = a_prev * (1 - D) + a_next * D
+            stages.append(("drift", a_vel, a_disp, a_disp_next, a_acc))
+            a_disp = a_disp_next
+            a_acc = a_disp
+        if k != 0:
+            K += k
+            a_vel_next = a_prev * (1 - K) + a_next * K
+            stages.append(("kick", a_acc, a_vel, a_vel_next))
+            a_vel = a_vel_next
+    return stages
+
+
+def _f32(x):
+    return float(np.float32(x))
+
+
+def kick(a_acc, a_prev, a_next, ptcl, cosmo, conf):
+    """vel += acc * K (integrator.py:512-538), in place on a copy of vel."""
+    K = _f32(cosmo.kick_factor(a_acc, a_prev, a_next))
+    vel = ptcl.vel.clone()
+    call("pmb_axpy", vel.data_ptr(), ptcl.acc.data_ptr(), vel.numel(), K, stream_handle(vel.device))
+    return ptcl.replace(vel=vel)
+
+
+def drift(a_vel, a_prev, a_next, ptcl, cosmo, conf):
+    """disp += vel * D (integrator.py:202-237)."""
+    D = _f32(cosmo.drift_factor(a_vel, a_prev, a_next))
+    disp = ptcl.disp.clone()
+    call("pmb_axpy", disp.data_ptr(), ptcl.vel.data_ptr(), disp.numel(), D, stream_handle(disp.device))
+    return ptcl.replace(disp=disp)
+
+
+def force_state(a, ptcl, cosmo, conf, correction=None):
+    """Overwrite acc with the PM force (integrator.py:595-617)."""
+    acc, _ = force(ptcl.pmid, ptcl.disp, conf, cosmo.Omega_m, a=a, cosmo=cosmo, correction=correction)
+    return ptcl.replace(acc=acc)
+
+
+def integrate(a_prev, a_next, ptcl, cosmo, conf, correction=None):
+    """One macro step with the configured splitting (integrator.py:689-731)."""
+    for st in _schedule(a_prev, a_next, conf):
+        if st[0] == "drift":
+            ptcl = drift(st[1], st[2], st[3], ptcl, cosmo, conf)
+            ptcl = force_state(st[3], ptcl, cosmo, conf, correction)
+        else:
+            ptcl = kick(st[1], st[2], st[3], ptcl, cosmo, conf)
+    return ptcl
+
+
+class NBodyRun:
+    """Fused forward integration that keeps the final force meshes for the adjoint."""
+
+    def __init__(self, conf, cosmo, correction=None):
+        self.conf = conf
+        self.cosmo = cosmo
+        self.correction = correction
+
+    def forward(self, ptcl, a_nbody=None):
+        conf, cosmo = self.conf, self.cosmo
+        a = conf.a_nbody if a_nbody is None else np.asarray(a_nbody)
+        disp = ptcl.disp.clone()
+        vel = ptcl.vel.clone() if ptcl.vel is not None else torch.zeros_like(disp)
+        acc = torch.empty_like(disp)
+        F = torch.empty((3, ) + conf.mesh_shape, dtype=torch.float32, device=disp.device)
+        s = stream_handle(disp.device)
+        force(ptcl.pmid, disp, conf, cosmo.Omega_m, a=float(a[0]), cosmo=cosmo, correction=self.correction,
+              force_meshes=F, acc=acc)
+        for a_prev, a_next in zip(a[:-1], a[1:]):
+            stages = _schedule(a_prev, a_next, conf)
+            i = 0
+            while i < len(stages):
+                st = stages[i]
+                if st[0] == "kick":
+                    call("pmb_axpy", vel.data_ptr(), acc.data_ptr(), vel.numel(),
+                         _f32(cosmo.kick_factor(st[1], st[2], st[3])), s)
+                    i += 1
+                    continue
+                D = _f32(cosmo.drift_factor(st[1], st[2], st[3]))
+                # fuse a directly following kick into the gather
+                kick_f, vk = 0.0, None
+                if i + 1 < len(stages) and stages[i + 1][0] == "kick":
+                    kst = stages[i + 1]
+                    kick_f, vk = _f32(cosmo.kick_factor(kst[1], kst[2], kst[3])), vel
+                    i += 1
+                force(ptcl.pmid, disp, conf, cosmo.Omega_m, a=float(st[3]), cosmo=cosmo, correction=self.correction,
+                      force_meshes=F, acc=acc, drift_vel=vel, drift=D, vel_kick=vk, kick=kick_f)
+                i += 1
+        self.final_meshes = F
+        return ptcl.replace(disp=disp, vel=vel, acc=acc)
+
+    def adjoint(self, ptcl, ptcl_cot, force_meshes=None, a_nbody=None):
+        """Reverse sweep from the final state.  Returns (ptcl_in, ptcl_in_cot, Omega_m_cot).
+
+        force_meshes must be the force meshes at ptcl's positions (the
+        forward pass leaves them in self.final_meshes)."""
+        conf, cosmo, corr = self.conf, self.cosmo, self.correction
+        a = conf.a_nbody if a_nbody is None else np.asarray(a_nbody)
+        dev = ptcl.disp.device
+        s = stream_handle(dev)
+        pmid = ptcl.pmid
+        disp, vel, acc = ptcl.disp.clone(), ptcl.vel.clone(), ptcl.acc.clone()
+        dc = ptcl_cot.disp.clone().float().contiguous()
+        vc = (ptcl_cot.vel if ptcl_cot.vel is not None else torch.zeros_like(dc)).clone().float().contiguous()
+        ac = (ptcl_cot.acc if ptcl_cot.acc is not None else torch.zeros_like(dc)).clone().float().contiguous()
+        F = self.final_meshes if force_meshes is None else force_meshes
+        F2 = torch.empty_like(F)
+        dots = torch.zeros(4 * len(a) + 8, dtype=torch.float64, device=dev)
+        grads = []  # (d factor / d Omega_m, dot slot) pairs, reduced on the host at the end
+        force_slots = []
+        slot = 0
+        om32 = _om32(cosmo.Omega_m)
+        for a_prev, a_next in zip(a[:-1][::-1], a[1:][::-1]):
+            for st in reversed(_schedule(a_prev, a_next, conf)):
+                if st[0] == "kick":
+                    K, dK = cosmo.kick_factor(st[1], st[2], st[3], with_grad=True)
+                    call("pmb_kick_adj", vel.data_ptr(), acc.data_ptr(), vc.data_ptr(), ac.data_ptr(), vel.numel(),
+                         _f32(K), dots[slot:].data_ptr(), s)
+                    grads.append((dK, slot))
+                    slot += 1
+                    continue
+                _, a_vel, a_dp, a_dn, a_acc_in = st
+                # force adjoint at the post-drift positions
+                call("pmb_dot", ac.data_ptr(), acc.data_ptr(), ac.numel(), dots[slot:].data_ptr(), s)
+                force_slots.append(slot)
+                slot += 1
+                force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=float(a_dn), cosmo=cosmo, correction=corr)
+                ac.zero_()
+                D, dD = cosmo.drift_factor(a_vel, a_dp, a_dn, with_grad=True)
+                call("pmb_drift_adj", disp.data_ptr(), vel.data_ptr(), dc.data_ptr(), vc.data_ptr(), disp.numel(),
+                     _f32(D), dots[slot:].data_ptr(), s)
+                grads.append((dD, slot))
+                slot += 1
+                # recompute the incoming acceleration; keep its meshes for the next force adjoint
+                force(pmid, disp, conf, cosmo.Omega_m, a=float(a_acc_in), cosmo=cosmo, correction=corr,
+                      force_meshes=F2, acc=acc)
+                F, F2 = F2, F
+        # the initial force evaluation (solver.py:437-441)
+        call("pmb_dot", ac.data_ptr(), acc.data_ptr(), ac.numel(), dots[slot:].data_ptr(), s)
+        force_slots.append(slot)
+        force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=float(a[0]), cosmo=cosmo, correction=corr)
+        ac.zero_()
+        d = dots.cpu().numpy()
+        om_cot = sum(g * d[k] for g, k in grads) + sum(d[k] for k in force_slots) / om32
+        return (ptcl.replace(disp=disp, vel=vel, acc=acc), Particles(conf, pmid, dc, vc, ac), float(om_cot))
+
+
+def nbody(ptcl, cosmo, conf, reverse=False, correction=None):
+    """Advance particles through conf.a_nbody (nbody/solver.py:605-642)."""
+    a = conf.a_nbody[::-1] if reverse else conf.a_nbody
+    return NBodyRun(conf, cosmo, correction).forward(ptcl, a)
+
+
+def nbody_adj(ptcl, ptcl_cot, cosmo, conf, reverse=False, correction=None):
+    """Reverse sweep from the final state (nbody/solver.py:385-444).
+
+    Returns (ptcl_in, ptcl_in_cot, Omega_m_cot)."""
+    a = conf.a_nbody[::-1] if reverse else conf.a_nbody
+    run = NBodyRun(conf, cosmo, correction)
+    _, F = force(ptcl.pmid, ptcl.disp.clone(), conf, cosmo.Omega_m, a=float(a[-1]), cosmo=cosmo,
+                 correction=correction)
+    return run.adjoint(ptcl, ptcl_cot, force_meshes=F, a_nbody=a)
