@@ -232,8 +232,11 @@ def run_ours(args):
         cot = pb.Particles(conf, p0.pmid, cot_d, torch.zeros_like(cot_d), torch.zeros_like(cot_d))
         return run.adjoint(out, cot)
 
-    for _ in range(args.warmup):
-        step(base, dcot)
+    # all device work runs through the staged entry points so a single set of
+    # workspaces is allocated
+    with StageTimer():
+        for _ in range(args.warmup):
+            step(base, dcot)
     torch.cuda.synchronize()
     _lib.reset_launch_count()
     barrier(world)
@@ -265,15 +268,16 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
-    e2.record()
-    for _ in range(args.steps):
-        p = pb.Particles(conf, h_pmid.to(dev, non_blocking=True), h_disp.to(dev, non_blocking=True),
-                         h_vel.to(dev, non_blocking=True))
-        c = h_cot.to(dev, non_blocking=True)
-        _, pc, om = step(p, c)
-        h_out_d.copy_(pc.disp, non_blocking=True)
-        h_out_v.copy_(pc.vel, non_blocking=True)
-    e3.record()
+    with StageTimer():
+        e2.record()
+        for _ in range(args.steps):
+            p = pb.Particles(conf, h_pmid.to(dev, non_blocking=True), h_disp.to(dev, non_blocking=True),
+                             h_vel.to(dev, non_blocking=True))
+            c = h_cot.to(dev, non_blocking=True)
+            _, pc, om = step(p, c)
+            h_out_d.copy_(pc.disp, non_blocking=True)
+            h_out_v.copy_(pc.vel, non_blocking=True)
+        e3.record()
     torch.cuda.synchronize()
     ms_e2e = max_over_ranks(e2.elapsed_time(e3) / args.steps, world)
     h2d = int(h_pmid.numel() * 2 + h_disp.numel() * 4 * 2 + h_cot.numel() * 4)

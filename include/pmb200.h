@@ -121,6 +121,59 @@ int pmb_drift_adj(float* disp, const float* vel, const float* disp_cot, float* v
                   double* dot, void* stream);
 /* dot (double, device) += sum a*b. */
 int pmb_dot(const float* a, const float* b, int64_t n, double* dot, void* stream);
+/* out (double, device) += sum a. */
+int pmb_sum(const float* a, int64_t n, double* out, void* stream);
+
+/* ---------------- initial conditions --------------------------------------
+ * Nested white noise (initial_conditions/modes.py:223-268): hashed Gaussian
+ * rFFT modes (gx, gy, gz/2+1) identical for shared low-k modes across
+ * resolutions.  hashes_out (optional, uint32 [2 x cells]) receives the real /
+ * imaginary stream hashes (modes.py:205-208). */
+int pmb_white_noise_nested(uint32_t seed, int gx, int gy, int gz, void* modes_out, uint32_t* hashes_out,
+                           void* stream);
+/* Linear modes delta = omega sqrt(V P_lin(|k|)) (modes.py:397-454): ktables =
+ * float [kx ky kz] of the particle grid; P_lin from the tabulated transfer
+ * function (FP64, cosmology/boltzmann.py:428-484) times growth2 = D(a)^2 (1
+ * without growth).  modes_in may be NULL to only write the amplitude
+ * amp_out (float per half-spectrum cell, optional). */
+int pmb_linear_modes(const void* modes_in, void* modes_out, float* amp_out, int gx, int gy, int gz,
+                     const float* ktables, const double* transfer_k, const double* transfer, int ntab, double A_s,
+                     double n_s, double omega_m, double k_pivot, double growth2, double box_vol, void* stream);
+/* 1LPT/2LPT displacements and velocities (initial_conditions/lpt.py:337-449):
+ * modes = linear modes on the particle grid; tables = float [kx ky kz cx cy
+ * cz] of the particle grid; (D1, V1, D2, V2) = growth factors D_m and
+ * a^2 H dD_m/dlna at a_start.  disp/vel (n,3) are updated in place for
+ * particles at pmid/disp (lattice positions); fields (6, gx, gy, gz) receive
+ * the sampled gradient fields and index_out (int64, n) the grid index of each
+ * particle, both reused by pmb_lpt_vjp. */
+int64_t pmb_lpt_workspace_bytes(int gx, int gy, int gz);
+int pmb_lpt(const void* modes, int gx, int gy, int gz, float spacing, float cell_vol, const float* tables, int order,
+            float D1, float V1, float D2, float V2, const int16_t* pmid, float* disp, float* vel, int64_t n,
+            float cell, float* fields, int64_t* index_out, void* workspace, int64_t workspace_bytes, void* stream);
+/* Adjoint of pmb_lpt w.r.t. the modes (the hand-written transpose of
+ * lpt.py:379-431; packed d/dRe + i d/dIm convention, the complex conjugate of
+ * JAX's gradient convention).  amp (optional) chains through the linear-mode
+ * amplitude.  dots (double[4], device, accumulated): sum g_m . disp_cot and
+ * sum g_m . vel_cot for m = 1, 2 (growth-factor cotangents). */
+int64_t pmb_lpt_vjp_workspace_bytes(int gx, int gy, int gz);
+int pmb_lpt_vjp(const void* modes, int gx, int gy, int gz, float cell_vol, const float* tables, int order, float D1,
+                float V1, float D2, float V2, const int64_t* index, const float* fields, const float* disp_cot,
+                const float* vel_cot, int64_t n, const float* amp, void* modes_cot, double* dots, void* workspace,
+                int64_t workspace_bytes, void* stream);
+
+/* ---------------- power spectrum ------------------------------------------
+ * FP64 shell sums of |d|^2 * mult * W^-2p over integer-radius shells
+ * (analysis/power_spectrum.py:120-176); sinc_tab = float sinc(n/M) per axis
+ * [nx ny nz/2+1].  With spec_b, also the auto sums of b and the cross sums. */
+int pmb_pk_shells(const void* spec, int nx, int ny, int nz, const float* sinc_tab, int mas_power, int num_shells,
+                  double* sums, const void* spec_b, double* sums_b, double* sums_x, void* stream);
+/* Mode counts and sum of |n| * mult per shell (power_spectrum.py:46-74). */
+int pmb_shell_stats(int nx, int ny, int nz, int num_shells, double* counts, double* ksum, void* stream);
+/* Adjoint of the shell power: out = 2 spec W^-2p wshell[shell] * post. */
+int pmb_pk_shells_adjoint(const void* spec, int nx, int ny, int nz, const float* sinc_tab, int mas_power,
+                          int num_shells, const double* wshell, float post, void* out, void* stream);
+/* delta = rho / (total / n) - 1 (power_spectrum.py:371-374). */
+int pmb_overdensity(const float* rho, float* delta, int64_t n, const double* total, void* stream);
 
 /* ---------------- host-side FP64 cosmology (no device work) ---------------
  * Growth table [order 1..2][deriv 0..2][na] from the growth ODE integrated

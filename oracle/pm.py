@@ -686,6 +686,32 @@ def _strain_ops(conf):
     return ops
 
 
+def lpt_source(pot_m, conf, pot_n=None):
+    """Quadratic LPT source, lpt.py:239-301:
+    sum_{i<j} phi_ii psi_jj (symmetrised when pot_n is given) - phi_ij psi_ji."""
+    shape = conf.ptcl_grid_shape
+    ops = _strain_ops(conf)
+    same = pot_n is None
+    pot_n = pot_m if same else pot_n
+    dm = [np.fft.irfftn(ops[(i, i)] * pot_m, s=shape) for i in range(3)]
+    dn = dm if same else [np.fft.irfftn(ops[(i, i)] * pot_n, s=shape) for i in range(3)]
+    L = np.zeros(shape)
+    for i in range(3):
+        for j in range(2, i, -1):
+            L += dm[i] * dn[j]
+        if not same:
+            for j in range(i - 1, -1, -1):
+                L += dm[i] * dn[j]
+    if not same:
+        L *= 0.5
+    for i in range(2):
+        for j in range(i + 1, 3):
+            sm = np.fft.irfftn(ops[(i, j)] * pot_m, s=shape)
+            sn = sm if same else np.fft.irfftn(ops[(i, j)] * pot_n, s=shape)
+            L -= sm * sn
+    return L
+
+
 def lpt_fields(modes, cosmo, conf):
     """1LPT/2LPT gradient fields on the particle grid, lpt.py:239-449.
 
@@ -693,16 +719,7 @@ def lpt_fields(modes, cosmo, conf):
     shape = conf.ptcl_grid_shape
     G = green(conf, "continuum", conf.kvec_spacing)
     pot1 = modes.astype(np.complex128) / conf.ptcl_cell_vol * G
-    ops = _strain_ops(conf)
-    diag = [np.fft.irfftn(ops[(i, i)] * pot1, s=shape) for i in range(3)]
-    L = np.zeros(shape)
-    for i in range(3):
-        for j in range(2, i, -1):
-            L += diag[i] * diag[j]
-    for i in range(2):
-        for j in range(i + 1, 3):
-            s = np.fft.irfftn(ops[(i, j)] * pot1, s=shape)
-            L -= s * s
+    L = lpt_source(pot1, conf)
     pot2 = np.fft.rfftn(L) * G
     c = [np.where(np.abs(np.abs(k.astype(np.float64)) - np.pi / conf.ptcl_spacing) <= np.pi / conf.ptcl_spacing *
                   np.finfo(conf.float_dtype).eps, 0.0, -k.astype(np.float64)) for k in conf.kvec_spacing]
@@ -799,6 +816,24 @@ def delta_to_pk(delta, conf, mas_power=2):
 def density_to_pk(density, conf, mas_power=2):
     """power_spectrum.py:348-374."""
     return delta_to_pk(density / density.mean() - 1, conf, mas_power)
+
+
+def delta_to_cross_correlation(da, db, conf, mas_power=2, eps=1e-30):
+    """power_spectrum.py:146-176, 259-267, 308-345: (k, r, P_ab, P_aa, P_bb, nmodes)."""
+    sa, sb = np.fft.rfftn(da), np.fft.rfftn(db)
+    k, pa, n = delta_to_pk(da, conf, mas_power)
+    _, pb, _ = delta_to_pk(db, conf, mas_power)
+    cross = (sa * np.conj(sb)).real
+    mx = np.fft.fftfreq(conf.mesh_shape[0]) * conf.mesh_shape[0]
+    my = np.fft.fftfreq(conf.mesh_shape[1]) * conf.mesh_shape[1]
+    mz = np.arange(conf.mesh_shape[2] // 2 + 1)
+    _, shell, mult = shell_sums(sa, conf.mesh_shape, mas_power)
+    w = (np.sinc(mx / conf.mesh_shape[0])[:, None, None] * np.sinc(my / conf.mesh_shape[1])[None, :, None] *
+         np.sinc(mz / conf.mesh_shape[2])[None, None, :])**(-2 * mas_power)
+    xs = np.bincount(shell.ravel(), weights=(cross * w * mult).ravel(), minlength=len(pa) + 1)
+    px = xs[1:len(pa) + 1] / n * (conf.cell_size**3 / conf.mesh_size)
+    r = px / np.sqrt(np.maximum(pa * pb, eps))
+    return k, r, px, pa, pb, n
 
 
 def log_bins(k, pk, nmodes, nbins=32, kmin=None, kmax=None):

@@ -41,6 +41,20 @@ _SIGS = {
     "pmb_kick_adj": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_p, c_p]),
     "pmb_drift_adj": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_p, c_p]),
     "pmb_dot": (c_int, [c_p, c_p, c_i64, c_p, c_p]),
+    "pmb_sum": (c_int, [c_p, c_i64, c_p, c_p]),
+    "pmb_white_noise_nested": (c_int, [ctypes.c_uint32, c_int, c_int, c_int, c_p, c_p, c_p]),
+    "pmb_linear_modes": (c_int, [c_p, c_p, c_p, c_int, c_int, c_int, c_p, c_p, c_p, c_int, c_d, c_d, c_d, c_d, c_d,
+                                 c_d, c_p]),
+    "pmb_lpt_workspace_bytes": (c_i64, [c_int, c_int, c_int]),
+    "pmb_lpt": (c_int, [c_p, c_int, c_int, c_int, c_f, c_f, c_p, c_int, c_f, c_f, c_f, c_f, c_p, c_p, c_p, c_i64, c_f,
+                        c_p, c_p, c_p, c_i64, c_p]),
+    "pmb_lpt_vjp_workspace_bytes": (c_i64, [c_int, c_int, c_int]),
+    "pmb_lpt_vjp": (c_int, [c_p, c_int, c_int, c_int, c_f, c_p, c_int, c_f, c_f, c_f, c_f, c_p, c_p, c_p, c_p, c_i64,
+                            c_p, c_p, c_p, c_p, c_i64, c_p]),
+    "pmb_pk_shells": (c_int, [c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p, c_p, c_p, c_p]),
+    "pmb_shell_stats": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p]),
+    "pmb_pk_shells_adjoint": (c_int, [c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_f, c_p, c_p]),
+    "pmb_overdensity": (c_int, [c_p, c_p, c_i64, c_p, c_p]),
     "pmb_growth_table": (c_int, [c_d, c_d, c_d, c_d, c_p, c_int, c_d, c_d, c_d, c_d, c_p, c_p]),
     "pmb_time_factor": (c_int, [c_int, c_d, c_d, c_d, c_d, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p]),
     "pmb_lpt_factors": (c_int, [c_d, c_d, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p]),
@@ -84,7 +98,9 @@ def check(status, what):
 _KERNELS = {
     "pmb_sort_rows": 5, "pmb_gather_rows": 1, "pmb_interp_grad_rows": 1, "pmb_green_gradient": 1,
     "pmb_green_gradient_adjoint": 1, "pmb_axpy": 1, "pmb_kick_adj": 1, "pmb_drift_adj": 1, "pmb_dot": 1,
-    "pmb_force": 9, "pmb_force_vjp": 11,
+    "pmb_force": 9, "pmb_force_vjp": 11, "pmb_sum": 1, "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,
+    "pmb_lpt": 4, "pmb_lpt_vjp": 6, "pmb_pk_shells": 1, "pmb_shell_stats": 1, "pmb_pk_shells_adjoint": 1,
+    "pmb_overdensity": 1,
 }
 _launches = [0]
 

@@ -5,6 +5,7 @@
 
 #include "../../include/pmb200.h"
 #include "pmb_common.cuh"
+#include "pmb_ic.cuh"
 #include "pmb_integrate.cuh"
 #include "pmb_kernels.cuh"
 #include "pmb_sort.cuh"
@@ -333,6 +334,185 @@ int pmb_drift_adj(float* disp, const float* vel, const float* disp_cot, float* v
 int pmb_dot(const float* a, const float* b, int64_t n, double* out, void* stream) {
   PMB_REQUIRE(out != nullptr, "pmb_dot: output required");
   return dot(a, b, n, out, S(stream));
+}
+
+int pmb_sum(const float* a, int64_t n, double* out, void* stream) {
+  PMB_REQUIRE(out != nullptr, "pmb_sum: output required");
+  return sum(a, n, out, S(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Initial conditions
+// ---------------------------------------------------------------------------
+int pmb_white_noise_nested(uint32_t seed, int gx, int gy, int gz, void* modes_out, uint32_t* hashes_out,
+                           void* stream) {
+  PMB_REQUIRE(gx > 0 && gy > 0 && gz > 0, "pmb_white_noise_nested: bad grid");
+  return white_noise(seed, Mesh3{gx, gy, gz}, (float2*)modes_out, hashes_out, S(stream));
+}
+
+int pmb_linear_modes(const void* modes_in, void* modes_out, float* amp_out, int gx, int gy, int gz,
+                     const float* ktables, const double* transfer_k, const double* transfer, int ntab, double A_s,
+                     double n_s, double omega_m, double k_pivot, double growth2, double box_vol, void* stream) {
+  PMB_REQUIRE(gx > 0 && gy > 0 && gz > 0 && ntab >= 2, "pmb_linear_modes: bad arguments");
+  const double c_light = 299792458.0 / 1e5;
+  LinearPowerParams p;
+  p.coef = 0.32 * A_s * k_pivot;
+  p.k_pivot = k_pivot;
+  p.n_s = n_s;
+  p.pi_c2_over_om = M_PI * c_light * c_light / omega_m;
+  p.growth2 = growth2;
+  p.box_vol = (float)box_vol;
+  return linear_modes((const float2*)modes_in, (float2*)modes_out, amp_out, Mesh3{gx, gy, gz}, ktables, transfer_k,
+                      transfer, ntab, p, S(stream));
+}
+
+static int64_t lpt_layout(Mesh3 g, void* ws, int64_t cap, float2** pot1, float2** spec6, float** real6, float** L,
+                          float2** Lhat, void** work) {
+  Carve c(ws, cap);
+  const int64_t ng = g.cells(), mc = g.half_cells();
+  *pot1 = (float2*)c.take(8 * mc);
+  *spec6 = (float2*)c.take(48 * mc);
+  *real6 = (float*)c.take(24 * ng);
+  *L = (float*)c.take(4 * ng);
+  *Lhat = (float2*)c.take(8 * mc);
+  int64_t w6 = fft_work_bytes(g, 6), w1 = fft_work_bytes(g, 1);
+  if (w6 < 0 || w1 < 0) return -1;
+  *work = c.take(w6 > w1 ? w6 : w1);
+  return c.off;
+}
+
+int64_t pmb_lpt_workspace_bytes(int gx, int gy, int gz) {
+  float2 *a, *b, *d;
+  float *r, *l;
+  void* w;
+  return lpt_layout(Mesh3{gx, gy, gz}, nullptr, 0, &a, &b, &r, &l, &d, &w);
+}
+
+int pmb_lpt(const void* modes, int gx, int gy, int gz, float spacing, float cell_vol, const float* tables, int order,
+            float D1, float V1, float D2, float V2, const int16_t* pmid, float* disp, float* vel, int64_t n,
+            float cell, float* fields, int64_t* index_out, void* workspace, int64_t workspace_bytes, void* stream) {
+  Mesh3 g{gx, gy, gz};
+  PMB_REQUIRE(gx > 0 && gy > 0 && gz > 0, "pmb_lpt: bad grid");
+  PMB_REQUIRE(order >= 0 && order <= 2, "pmb_lpt: order must be 0, 1 or 2");
+  float2 *pot1, *spec6, *Lhat;
+  float *real6, *L;
+  void* work;
+  int64_t need = lpt_layout(g, workspace, workspace_bytes, &pot1, &spec6, &real6, &L, &Lhat, &work);
+  PMB_REQUIRE(need >= 0, "pmb_lpt: cuFFT plan creation failed");
+  if (need > workspace_bytes) {
+    set_last_error("pmb_lpt: workspace too small");
+    return kScratchTooSmall;
+  }
+  cudaStream_t s = S(stream);
+  const float inv_n = (float)(1.0 / (double)g.cells());
+  PMB_TRY(lpt_strains((const float2*)modes, 1.0f / cell_vol, pot1, spec6, g, tables, inv_n, s));
+  const float2* Lh = nullptr;
+  if (order >= 2) {
+    PMB_TRY(fft_c2r(g, 6, spec6, real6, work, s));
+    PMB_TRY(lpt_source(real6, L, g.cells(), s));
+    PMB_TRY(fft_r2c(g, 1, L, Lhat, work, s));
+    Lh = Lhat;
+  }
+  PMB_TRY(lpt_gradients(pot1, Lh, spec6, g, tables, inv_n, s));
+  PMB_TRY(fft_c2r(g, 6, spec6, fields, work, s));
+  return lpt_displace(pmid, disp, vel, n, g, cell, spacing, fields, order, D1, V1, D2, V2, index_out, s);
+}
+
+static int64_t lpt_vjp_layout(Mesh3 g, void* ws, int64_t cap, float** cot6, float2** F6, float2** Lhat, float** L,
+                              float2** pot1, float2** spec6, float** real6, void** work) {
+  Carve c(ws, cap);
+  const int64_t ng = g.cells(), mc = g.half_cells();
+  *cot6 = (float*)c.take(24 * ng);
+  *F6 = (float2*)c.take(48 * mc);
+  *Lhat = (float2*)c.take(8 * mc);
+  *L = (float*)c.take(4 * ng);
+  *pot1 = (float2*)c.take(8 * mc);
+  *spec6 = (float2*)c.take(48 * mc);
+  *real6 = (float*)c.take(24 * ng);
+  int64_t w6 = fft_work_bytes(g, 6), w1 = fft_work_bytes(g, 1);
+  if (w6 < 0 || w1 < 0) return -1;
+  *work = c.take(w6 > w1 ? w6 : w1);
+  return c.off;
+}
+
+int64_t pmb_lpt_vjp_workspace_bytes(int gx, int gy, int gz) {
+  float *a, *l, *r;
+  float2 *f, *lh, *p, *sp;
+  void* w;
+  return lpt_vjp_layout(Mesh3{gx, gy, gz}, nullptr, 0, &a, &f, &lh, &l, &p, &sp, &r, &w);
+}
+
+int pmb_lpt_vjp(const void* modes, int gx, int gy, int gz, float cell_vol, const float* tables, int order, float D1,
+                float V1, float D2, float V2, const int64_t* index, const float* fields, const float* disp_cot,
+                const float* vel_cot, int64_t n, const float* amp, void* modes_cot, double* dots, void* workspace,
+                int64_t workspace_bytes, void* stream) {
+  Mesh3 g{gx, gy, gz};
+  PMB_REQUIRE(gx > 0 && gy > 0 && gz > 0, "pmb_lpt_vjp: bad grid");
+  PMB_REQUIRE(order >= 1 && order <= 2, "pmb_lpt_vjp: order must be 1 or 2");
+  PMB_REQUIRE(dots != nullptr, "pmb_lpt_vjp: dots required");
+  float *cot6, *L, *real6;
+  float2 *F6, *Lhat, *pot1, *spec6;
+  void* work;
+  int64_t need = lpt_vjp_layout(g, workspace, workspace_bytes, &cot6, &F6, &Lhat, &L, &pot1, &spec6, &real6, &work);
+  PMB_REQUIRE(need >= 0, "pmb_lpt_vjp: cuFFT plan creation failed");
+  if (need > workspace_bytes) {
+    set_last_error("pmb_lpt_vjp: workspace too small");
+    return kScratchTooSmall;
+  }
+  cudaStream_t s = S(stream);
+  const int64_t ng = g.cells();
+  const float inv_n = (float)(1.0 / (double)ng);
+  PMB_CUDA_CHECK(cudaMemsetAsync(cot6, 0, 24 * ng, s));
+  PMB_TRY(lpt_field_cot(index, disp_cot, vel_cot, n, ng, fields, order, D1, V1, D2, V2, cot6, dots, s));
+  PMB_TRY(fft_r2c(g, 6, cot6, F6, work, s));
+  const float2* FS = nullptr;
+  if (order >= 2) {
+    PMB_TRY(lpt_grad2_adjoint(F6 + 3 * g.half_cells(), Lhat, g, tables, inv_n, s));
+    PMB_TRY(fft_c2r(g, 1, Lhat, L, work, s));
+    PMB_TRY(lpt_strains((const float2*)modes, 1.0f / cell_vol, pot1, spec6, g, tables, inv_n, s));
+    PMB_TRY(fft_c2r(g, 6, spec6, real6, work, s));
+    PMB_TRY(lpt_source_adjoint(real6, L, cot6, ng, s));
+    PMB_TRY(fft_r2c(g, 6, cot6, spec6, work, s));
+    FS = spec6;
+  }
+  const float scale = (float)(1.0 / ((double)cell_vol * (double)ng));
+  return lpt_modes_adjoint(F6, FS, amp, (float2*)modes_cot, g, tables, scale, s);
+}
+
+// ---------------------------------------------------------------------------
+// Power spectrum
+// ---------------------------------------------------------------------------
+int pmb_pk_shells(const void* spec, int nx, int ny, int nz, const float* sinc_tab, int mas_power, int num_shells,
+                  double* sums, const void* spec_b, double* sums_b, double* sums_x, void* stream) {
+  PMB_REQUIRE(nx > 0 && ny > 0 && nz > 0 && num_shells > 0, "pmb_pk_shells: bad arguments");
+  PMB_REQUIRE(spec_b == nullptr || (sums_b != nullptr && sums_x != nullptr), "pmb_pk_shells: cross sums missing");
+  cudaStream_t s = S(stream);
+  PMB_CUDA_CHECK(cudaMemsetAsync(sums, 0, sizeof(double) * num_shells, s));
+  if (spec_b != nullptr) {
+    PMB_CUDA_CHECK(cudaMemsetAsync(sums_b, 0, sizeof(double) * num_shells, s));
+    PMB_CUDA_CHECK(cudaMemsetAsync(sums_x, 0, sizeof(double) * num_shells, s));
+  }
+  return pk_shells((const float2*)spec, Mesh3{nx, ny, nz}, sinc_tab, mas_power, num_shells, sums,
+                   (const float2*)spec_b, sums_b, sums_x, s);
+}
+
+int pmb_shell_stats(int nx, int ny, int nz, int num_shells, double* counts, double* ksum, void* stream) {
+  PMB_REQUIRE(nx > 0 && ny > 0 && nz > 0 && num_shells > 0, "pmb_shell_stats: bad arguments");
+  cudaStream_t s = S(stream);
+  PMB_CUDA_CHECK(cudaMemsetAsync(counts, 0, sizeof(double) * num_shells, s));
+  PMB_CUDA_CHECK(cudaMemsetAsync(ksum, 0, sizeof(double) * num_shells, s));
+  return shell_stats(Mesh3{nx, ny, nz}, num_shells, counts, ksum, s);
+}
+
+int pmb_pk_shells_adjoint(const void* spec, int nx, int ny, int nz, const float* sinc_tab, int mas_power,
+                          int num_shells, const double* wshell, float post, void* out, void* stream) {
+  PMB_REQUIRE(nx > 0 && ny > 0 && nz > 0 && num_shells > 0, "pmb_pk_shells_adjoint: bad arguments");
+  return pk_shells_adjoint((const float2*)spec, Mesh3{nx, ny, nz}, sinc_tab, mas_power, num_shells, wshell, post,
+                           (float2*)out, S(stream));
+}
+
+int pmb_overdensity(const float* rho, float* delta, int64_t n, const double* total, void* stream) {
+  return overdensity(rho, delta, n, total, S(stream));
 }
 
 // ---------------------------------------------------------------------------

@@ -269,6 +269,7 @@ int compute_scale(const float* val, int64_t count, int64_t n, double* scale_dev,
 // ---------------------------------------------------------------------------
 // Pull scatter
 // ---------------------------------------------------------------------------
+constexpr int kMaxSrcRows = 25;  // (RX+1)*(RY+1) with RX, RY <= 4
 // Epilogue: mode 0 writes the density sum, mode 1 writes the Poisson source
 // (rho - 1) * src_mul (gravity.py:628-630), both in float.
 template <int C>
@@ -278,21 +279,45 @@ __global__ void __launch_bounds__(256) scatter_pull_kernel(const Rec* __restrict
                                                            const double* __restrict__ scale_dev, int mode,
                                                            float src_mul, float* __restrict__ out) {
   extern __shared__ long long acc[];  // [RX][RY][C][nz]
+  __shared__ uint32_t seg_beg[kMaxSrcRows];
+  __shared__ uint32_t seg_pre[kMaxSrcRows + 1];
   const int nby = (m.ny + RY - 1) / RY;
   const int x0 = (int)(blockIdx.x / nby) * RX;
   const int y0 = (int)(blockIdx.x % nby) * RY;
   const int nz = m.nz;
-  const int64_t total = (int64_t)RX * RY * C * nz;
-  for (int64_t t = threadIdx.x; t < total; t += blockDim.x) acc[t] = 0;
+  const int nsrc = (RX + 1) * (RY + 1);
+  const int total = RX * RY * C * nz;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) acc[t] = 0;
+  // source-row segments of the (RX+1) x (RY+1) rows that reach this block,
+  // flattened so all threads stay busy regardless of per-row counts
+  if (threadIdx.x < nsrc) {
+    const int k = threadIdx.x;
+    const int px = pmod(x0 + k / (RY + 1) - 1, m.nx), py = pmod(y0 + k % (RY + 1) - 1, m.ny);
+    const int64_t row = (int64_t)px * m.ny + py;
+    const uint32_t b = offs[row];
+    seg_beg[k] = b;
+    seg_pre[k + 1] = offs[row + 1] - b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (int k = 0; k < nsrc; ++k) {
+      const uint32_t c = seg_pre[k + 1];
+      seg_pre[k] = run;
+      run += c;
+    }
+    seg_pre[nsrc] = run;
+  }
   __syncthreads();
   const double scale = *scale_dev;
-  for (int sx = -1; sx < RX; ++sx) {
-    const int px = pmod(x0 + sx, m.nx);
-    for (int sy = -1; sy < RY; ++sy) {
-      const int py = pmod(y0 + sy, m.ny);
-      const int64_t row = (int64_t)px * m.ny + py;
-      const uint32_t beg = offs[row], end = offs[row + 1];
-      for (uint32_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+  const uint32_t ntot = seg_pre[nsrc];
+  for (uint32_t idx = threadIdx.x; idx < ntot; idx += blockDim.x) {
+    {
+      int k = 0;
+      while (idx >= seg_pre[k + 1]) ++k;
+      const int sx = k / (RY + 1) - 1, sy = k % (RY + 1) - 1;
+      const uint32_t i = seg_beg[k] + (idx - seg_pre[k]);
+      {
         const Rec r = rec[i];
         const int cz = (int)(r.key % (uint32_t)nz);
         float v[C];
@@ -323,8 +348,7 @@ __global__ void __launch_bounds__(256) scatter_pull_kernel(const Rec* __restrict
               for (int c = 0; c < C; ++c) {
                 const float contrib = __fmul_rn(v[c], w);
                 const long long q = __double2ll_rn((double)contrib * scale);
-                atomicAdd((unsigned long long*)&acc[(((int64_t)lx * RY + ly) * C + c) * nz + z],
-                          (unsigned long long)q);
+                atomicAdd((unsigned long long*)&acc[((lx * RY + ly) * C + c) * nz + z], (unsigned long long)q);
               }
             }
           }
@@ -335,17 +359,22 @@ __global__ void __launch_bounds__(256) scatter_pull_kernel(const Rec* __restrict
   __syncthreads();
   const double inv = 1.0 / scale;
   const int64_t cells = m.cells();
-  for (int64_t t = threadIdx.x; t < total; t += blockDim.x) {
-    const int z = (int)(t % nz);
-    int64_t rest = t / nz;
-    const int c = (int)(rest % C);
-    rest /= C;
-    const int ly = (int)(rest % RY);
-    const int lx = (int)(rest / RY);
-    if (x0 + lx >= m.nx || y0 + ly >= m.ny) continue;
-    float rho = (float)((double)acc[t] * inv);
-    if (mode == 1) rho = __fmul_rn(__fsub_rn(rho, 1.0f), src_mul);
-    out[(int64_t)c * cells + ((int64_t)(x0 + lx) * m.ny + (y0 + ly)) * nz + z] = rho;
+  for (int lx = 0; lx < RX; ++lx) {
+    if (x0 + lx >= m.nx) break;
+    for (int ly = 0; ly < RY; ++ly) {
+      if (y0 + ly >= m.ny) break;
+      const int64_t row_off = ((int64_t)(x0 + lx) * m.ny + (y0 + ly)) * nz;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const long long* a = acc + ((lx * RY + ly) * C + c) * nz;
+        float* o = out + (int64_t)c * cells + row_off;
+        for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+          float rho = (float)((double)a[z] * inv);
+          if (mode == 1) rho = __fmul_rn(__fsub_rn(rho, 1.0f), src_mul);
+          o[z] = rho;
+        }
+      }
+    }
   }
 }
 
