@@ -22,3 +22,7 @@ __all__ = [
     "gather", "scatter_vjp", "gather_vjp", "gravity", "gravity_vjp", "nbody", "nbody_adj", "integrate", "kick",
     "drift", "NBodyRun"
 ]
+from . import modes, lpt, power_spectrum, pipeline  # noqa: E402
+from .modes import white_noise_nested, linear_modes  # noqa: E402
+from .lpt import lpt as lpt_displacements  # noqa: E402
+from .power_spectrum import delta_to_pk, density_to_pk, particles_to_pk  # noqa: E402

@@ -64,7 +64,7 @@ def test_linear_modes_matches_oracle():
     w = pm.white_noise_nested(3, conf)
     lm = pm.linear_modes(w, cos, conf).cpu().numpy()
     ref = opm.linear_modes(w.cpu().numpy(), oc, co)
-    assert rel_err(np.abs(lm - ref), np.abs(ref)) < 2e-5
+    assert np.abs(lm - ref).max() < 2e-5 * np.abs(ref).max()
 
 
 @pytest.mark.parametrize("order", [1, 2])
@@ -148,6 +148,9 @@ def test_pk_loss_gradient_vs_finite_differences():
 
     np.testing.assert_allclose(loss, L(disp.astype(np.float64)), rtol=1e-4)
     direction = rng.normal(size=disp.shape)
-    eps = 1e-3
-    fd = (L(disp + eps * direction) - L(disp - eps * direction)) / (2 * eps)
+    # CIC is piecewise linear: keep the step far below the distance at which
+    # a particle crosses a cell boundary
+    eps = 1e-5
+    d64 = disp.astype(np.float64)
+    fd = (L(d64 + eps * direction) - L(d64 - eps * direction)) / (2 * eps)
     np.testing.assert_allclose(float((g * direction).sum()), fd, rtol=2e-3)
