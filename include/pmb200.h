@@ -43,6 +43,18 @@ int64_t pmb_sorted_bytes(int64_t n, int nx, int ny, int nz);
 int64_t pmb_sort_scratch_bytes(int64_t n, int nx, int ny, int nz);
 int pmb_sort_rows(const int16_t* pmid, float* disp, const float* vel, float drift, int64_t n, int nx, int ny, int nz,
                   float cell, void* sorted, void* scratch, int64_t scratch_bytes, void* stream);
+/* Density scatter that allocates nothing and takes no workspace.  No
+ * counterpart in the reference: it exists for callers that may not allocate
+ * device memory (framework plugins whose host program owns every allocation
+ * and hands them no scratch).  Same result as pmb_sort_rows +
+ * pmb_scatter_rows (mode 0, constant val).  Its scratch is a fixed 32 MiB
+ * device array inside the library (held on every GPU that loads it until
+ * exit); problems needing more (28 B per particle + ~8 B per mesh row) are
+ * rejected.  Calls share that array, so calls that overlap on the GPU race;
+ * the first call on a device resolves the array's address and should come
+ * before any stream capture. */
+int pmb_scatter_density_noalloc(const int16_t* pmid, const float* disp, int64_t n, int nx, int ny, int nz, float cell,
+                                float val, float* out, void* stream);
 /* Stable per-cell order of the reference key ((x*My+y)*Mz+z), ties keep
  * source order: keys_out[n] (uint32) and perm_out[n] (uint32). */
 int pmb_sort_by_cell(const int16_t* pmid, const float* disp, int64_t n, int nx, int ny, int nz, float cell,

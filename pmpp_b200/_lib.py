@@ -55,6 +55,7 @@ _SIGS = {
     "pmb_shell_stats": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p]),
     "pmb_pk_shells_adjoint": (c_int, [c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_f, c_p, c_p]),
     "pmb_overdensity": (c_int, [c_p, c_p, c_i64, c_p, c_p]),
+    "pmb_scatter_density_noalloc": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_f, c_f, c_p, c_p]),
     "pmb_growth_table": (c_int, [c_d, c_d, c_d, c_d, c_p, c_int, c_d, c_d, c_d, c_d, c_p, c_p]),
     "pmb_time_factor": (c_int, [c_int, c_d, c_d, c_d, c_d, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p]),
     "pmb_lpt_factors": (c_int, [c_d, c_d, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p]),
