@@ -187,6 +187,26 @@ int pmb_pk_shells_adjoint(const void* spec, int nx, int ny, int nz, const float*
 /* delta = rho / (total / n) - 1 (power_spectrum.py:371-374). */
 int pmb_overdensity(const float* rho, float* delta, int64_t n, const double* total, void* stream);
 
+/* ---------------- learned Green's-function correction ----------------------
+ * A width-64 sin-MLP T(|k|, a, Omega_m, sigma8) = 1 + f(x) multiplying the
+ * Green's function (the potential-transfer hook of corrections/core.py:
+ * 286-334; cf. the radial filter of corrections/radial.py:29-216).  Weights
+ * bf16 [W1 (64x4) W2 (64x64) W3 (64x64) W4 (64)], biases float [b1 b2 b3 (64
+ * each) b4]; FP32 accumulation.  pmb_mlp_table evaluates T on the table of
+ * integer |n|^2 = 0..len-1 (|k|/k_Ny = sqrt(n^2) * kscale) that
+ * pmb_green_gradient reads as `radial`. */
+int pmb_mlp_param_counts(int* n_weights, int* n_biases);
+int pmb_mlp_table(const void* weights_bf16, const float* biases, float kscale, float a, float omega_m, float sigma8,
+                  int len, float* table, void* stream);
+/* grad (float, weights then biases) += d/dparams sum_n table_cot[n] T[n]. */
+int pmb_mlp_backward(const void* weights_bf16, const float* biases, float kscale, float a, float omega_m,
+                     float sigma8, int len, const double* table_cot, float* grad, void* stream);
+/* out[n^2] += dL/dT for one force adjoint: grad_cot_hat = rFFT of the three
+ * force-mesh cotangents, src_hat = rFFT of the Poisson source at the same
+ * positions. */
+int pmb_transfer_cot(const void* grad_cot_hat, const void* src_hat, int nx, int ny, int nz, const float* tables,
+                     int has_masks, int len, double* out, void* stream);
+
 /* ---------------- host-side FP64 cosmology (no device work) ---------------
  * Growth table [order 1..2][deriv 0..2][na] from the growth ODE integrated
  * with the adaptive Dormand-Prince scheme of numerics/ode.py:304-422 at the

@@ -517,15 +517,16 @@ def nbody(pmid, disp, vel, conf, cosmo, kernel=None, acc=None):
     """nbody/solver.py:253-273 forward (init force + scan of integrate)."""
     ft = conf.float_dtype
     a = conf.a_nbody
+    K = kernel if callable(kernel) else (lambda _a: kernel)
     disp = disp.astype(ft).copy()
     vel = vel.astype(ft).copy()
-    acc = gravity(pmid, disp, conf, cosmo.Omega_m, kernel).astype(ft)
+    acc = gravity(pmid, disp, conf, cosmo.Omega_m, K(a[0])).astype(ft)
     for a_prev, a_next in zip(a[:-1], a[1:]):
         for st in stage_schedule(a_prev, a_next, conf):
             if st[0] == "drift":
                 f = ft.type(drift_factor(st[1], st[2], st[3], cosmo, conf))
                 disp = (disp + vel * f).astype(ft)
-                acc = gravity(pmid, disp, conf, cosmo.Omega_m, kernel).astype(ft)
+                acc = gravity(pmid, disp, conf, cosmo.Omega_m, K(st[3])).astype(ft)
             else:
                 f = ft.type(kick_factor(st[1], st[2], st[3], cosmo, conf))
                 vel = (vel + acc * f).astype(ft)
@@ -834,6 +835,48 @@ def delta_to_cross_correlation(da, db, conf, mas_power=2, eps=1e-30):
     px = xs[1:len(pa) + 1] / n * (conf.cell_size**3 / conf.mesh_size)
     r = px / np.sqrt(np.maximum(pa * pb, eps))
     return k, r, px, pa, pb, n
+
+
+# --------------------------------------------------------------------------
+# Learned Green's-function correction (test reference for csrc/mlp.cu)
+# --------------------------------------------------------------------------
+def bf16_round(x):
+    """Round float32 values to bfloat16 (round to nearest even), returned as float64."""
+    u = np.asarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def mlp_unpack(w, b, H=64):
+    w = np.asarray(w, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    W1 = w[:4 * H].reshape(H, 4)
+    W2 = w[4 * H:4 * H + H * H].reshape(H, H)
+    W3 = w[4 * H + H * H:4 * H + 2 * H * H].reshape(H, H)
+    W4 = w[4 * H + 2 * H * H:]
+    return W1, W2, W3, W4, b[:H], b[H:2 * H], b[2 * H:3 * H], b[3 * H]
+
+
+def mlp_table(w, b, kscale, a, om, s8, length):
+    """T[n2] = 1 + f(sqrt(n2) kscale, a, Om, s8), T[0] = 1 (width-64 sin-MLP)."""
+    W1, W2, W3, W4, b1, b2, b3, b4 = mlp_unpack(w, b)
+    n2 = np.arange(length, dtype=np.float64)
+    x = np.stack([np.sqrt(n2) * kscale, np.full_like(n2, a), np.full_like(n2, om), np.full_like(n2, s8)], 1)
+    h = np.sin(x @ W1.T + b1)
+    h = np.sin(h @ W2.T + b2)
+    h = np.sin(h @ W3.T + b3)
+    T = 1.0 + h @ W4 + b4
+    T[0] = 1.0
+    return T
+
+
+def radial_transfer(table, conf):
+    """Expand a |n|^2-indexed table onto the half spectrum (cubic mesh)."""
+    mx = np.fft.fftfreq(conf.mesh_shape[0]) * conf.mesh_shape[0]
+    my = np.fft.fftfreq(conf.mesh_shape[1]) * conf.mesh_shape[1]
+    mz = np.arange(conf.mesh_shape[2] // 2 + 1)
+    n2 = (mx[:, None, None]**2 + my[None, :, None]**2 + mz[None, None, :]**2).astype(np.int64)
+    return np.asarray(table)[n2]
 
 
 def log_bins(k, pk, nmodes, nbins=32, kmin=None, kmax=None):

@@ -56,6 +56,10 @@ _SIGS = {
     "pmb_pk_shells_adjoint": (c_int, [c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_f, c_p, c_p]),
     "pmb_overdensity": (c_int, [c_p, c_p, c_i64, c_p, c_p]),
     "pmb_scatter_density_noalloc": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_f, c_f, c_p, c_p]),
+    "pmb_mlp_param_counts": (c_int, [c_p, c_p]),
+    "pmb_mlp_table": (c_int, [c_p, c_p, c_f, c_f, c_f, c_f, c_int, c_p, c_p]),
+    "pmb_mlp_backward": (c_int, [c_p, c_p, c_f, c_f, c_f, c_f, c_int, c_p, c_p, c_p]),
+    "pmb_transfer_cot": (c_int, [c_p, c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p]),
     "pmb_growth_table": (c_int, [c_d, c_d, c_d, c_d, c_p, c_int, c_d, c_d, c_d, c_d, c_p, c_p]),
     "pmb_time_factor": (c_int, [c_int, c_d, c_d, c_d, c_d, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p]),
     "pmb_lpt_factors": (c_int, [c_d, c_d, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p]),

@@ -1,0 +1,162 @@
+"""Potential corrections applied inside the PM force.
+
+* ``PMWindowCompensation`` -- the analytic CIC-window compensation
+  (corrections/window.py:23-265): gain = W(k)^(-order*windows*alpha) capped at
+  max_gain, tapered to 1 between taper_start and taper_stop of the particle
+  Nyquist wavenumber, with the discrete-Laplacian Green's function.  Evaluated
+  once per configuration into a device transfer table.
+* ``LearnedGreen`` -- a width-64 sin-MLP T(|k|, a, Omega_m, sigma8) = 1 + f(x)
+  (bf16 weights, FP32 accumulation) evaluated by pmb_mlp_table on the table of
+  integer |n|^2 each force evaluation and trained through the hand-written
+  adjoints (pmb_transfer_cot + pmb_mlp_backward), Adam in FP32.  The reference's
+  learned radial filter (corrections/radial.py:29-216) is a spline whose knots
+  come from a sin-MLP of a only; this network takes the cosmology as input.
+
+Both follow the protocol pmpp_b200.gravity expects: ``green_kernel`` and
+``transfer_tables(a, cosmo, conf) -> (transfer or None, radial or None)``.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from ._lib import call, lib
+from .runtime import stream_handle
+
+
+class PMWindowCompensation:
+    green_kernel = 1  # discrete Laplacian (window.py:100-108 default)
+
+    def __init__(self, alpha=0.48, max_gain=4.0, assignment_order=2, windows=2, taper_start=0.75, taper_stop=1.0,
+                 green_kernel="discrete_laplacian"):
+        self.alpha = alpha
+        self.max_gain = max_gain
+        self.assignment_order = assignment_order
+        self.windows = windows
+        self.taper_start = taper_start
+        self.taper_stop = taper_stop
+        self.green_kernel = 1 if green_kernel == "discrete_laplacian" else 0
+        self._cache = {}
+
+    def transfer_tables(self, a, cosmo, conf):
+        dev = conf.device
+        key = (conf.mesh_shape, conf.cell_size, conf.ptcl_spacing, str(dev))
+        if key not in self._cache:
+            kx, ky, kz = [torch.from_numpy(k.astype(np.float32)).to(dev) for k in conf.kvec]
+            c = np.float32(conf.cell_size)
+            two_pi = np.float32(2 * np.pi)
+            sinc = lambda x: torch.where(x == 0, torch.ones_like(x), torch.sin(np.pi * x) / (np.pi * x))
+            sx = sinc(kx * c / two_pi)[:, None, None]
+            sy = sinc(ky * c / two_pi)[None, :, None]
+            sz = sinc(kz * c / two_pi)[None, None, :]
+            base = torch.clamp((sx * sy * sz).abs(), min=1e-6)
+            gain = base**(-float(self.assignment_order * self.windows * self.alpha))
+            if self.max_gain is not None and self.max_gain > 0:
+                gain = torch.clamp(gain, max=float(self.max_gain))
+            if self.taper_stop > self.taper_start:
+                kn = np.float32(np.pi / conf.ptcl_spacing)
+                q = torch.maximum(torch.maximum(kx.abs()[:, None, None], ky.abs()[None, :, None]),
+                                  kz.abs()[None, None, :]) / kn
+                t = torch.clamp((q - self.taper_start) / (self.taper_stop - self.taper_start), 0.0, 1.0)
+                gain = 1.0 + (gain - 1.0) * (1.0 - t * t * (3.0 - 2.0 * t))
+            self._cache[key] = gain.to(torch.float32).contiguous()
+        return self._cache[key], None
+
+
+def radial_table_len(conf):
+    nx, ny, nz = conf.mesh_shape
+    return (nx // 2)**2 + (ny // 2)**2 + (nz // 2)**2 + 1
+
+
+class LearnedGreen:
+    """Trainable multiplicative Green's-function correction."""
+
+    green_kernel = 0
+    trainable = True
+
+    def __init__(self, device="cuda", seed=0, sigma8=0.8, init_scale=1.0):
+        nw, nb = ctypes.c_int(), ctypes.c_int()
+        call("pmb_mlp_param_counts", ctypes.byref(nw), ctypes.byref(nb))
+        self.n_weights, self.n_biases = nw.value, nb.value
+        H = 64
+        g = torch.Generator().manual_seed(seed)
+        u = lambda shape, fan: (torch.rand(shape, generator=g) * 2 - 1) * math.sqrt(6.0 / fan) * init_scale
+        W1 = u((H, 4), 4)
+        W2 = u((H, H), H)
+        W3 = u((H, H), H)
+        W4 = torch.zeros(H)  # T = 1 at initialisation: starts from the plain Green's function
+        self.w = torch.cat([W1.reshape(-1), W2.reshape(-1), W3.reshape(-1), W4]).to(device)
+        self.b = torch.cat([u((H, ), 4), u((H, ), H), u((H, ), H), torch.zeros(1)]).to(device)
+        assert self.w.numel() == self.n_weights and self.b.numel() == self.n_biases
+        self.device = torch.device(device)
+        self.sigma8 = sigma8
+        self.grad = torch.zeros(self.n_weights + self.n_biases, dtype=torch.float32, device=device)
+        self._adam = None
+        self._sync_bf16()
+
+    def _sync_bf16(self):
+        self.w16 = self.w.to(torch.bfloat16).contiguous()
+
+    def parameters(self):
+        return torch.cat([self.w, self.b])
+
+    def load_parameters(self, p):
+        p = p.to(self.device, torch.float32)
+        self.w = p[:self.n_weights].clone()
+        self.b = p[self.n_weights:].clone()
+        self._sync_bf16()
+
+    def _kscale(self, conf):
+        return 2.0 / conf.mesh_shape[0]
+
+    def _cond(self, a, cosmo, conf):
+        s8 = cosmo.__dict__.get("_sigma8_cached")
+        if s8 is None:
+            s8 = float(cosmo.sigma8) if cosmo.transfer is not None and cosmo.growth is not None else self.sigma8
+            object.__setattr__(cosmo, "_sigma8_cached", s8)
+        return float(self._kscale(conf)), float(a), float(cosmo.Omega_m), float(s8)
+
+    def table(self, a, cosmo, conf):
+        L = radial_table_len(conf)
+        out = torch.empty(L, dtype=torch.float32, device=self.device)
+        ks, aa, om, s8 = self._cond(a, cosmo, conf)
+        call("pmb_mlp_table", self.w16.data_ptr(), self.b.data_ptr(), ks, aa, om, s8, L, out.data_ptr(),
+             stream_handle(self.device))
+        return out
+
+    def transfer_tables(self, a, cosmo, conf):
+        if conf.mesh_shape[0] != conf.mesh_shape[1] or conf.mesh_shape[0] != conf.mesh_shape[2]:
+            raise ValueError("LearnedGreen needs a cubic force mesh")
+        return None, self.table(a, cosmo, conf)
+
+    def accumulate(self, a, cosmo, conf, table_cot):
+        """grad += d(sum_n table_cot[n] T_n) / d params for one force evaluation."""
+        ks, aa, om, s8 = self._cond(a, cosmo, conf)
+        call("pmb_mlp_backward", self.w16.data_ptr(), self.b.data_ptr(), ks, aa, om, s8, int(table_cot.numel()),
+             table_cot.data_ptr(), self.grad.data_ptr(), stream_handle(self.device))
+
+    def zero_grad(self):
+        self.grad.zero_()
+
+    def adam_step(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8, clip=None):
+        """Adam in FP32 on the master parameters; bf16 copies refreshed after."""
+        p = self.parameters()
+        g = self.grad.clone()
+        if clip is not None:
+            n = float(g.norm())
+            if n > clip:
+                g *= clip / n
+        if self._adam is None:
+            self._adam = [torch.zeros_like(p), torch.zeros_like(p), 0]
+        m, v, t = self._adam
+        t += 1
+        m.mul_(b1).add_(g, alpha=1 - b1)
+        v.mul_(b2).addcmul_(g, g, value=1 - b2)
+        mh = m / (1 - b1**t)
+        vh = v / (1 - b2**t)
+        p = p - lr * mh / (vh.sqrt() + eps)
+        self._adam = [m, v, t]
+        self.load_parameters(p)

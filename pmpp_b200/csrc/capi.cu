@@ -8,6 +8,7 @@
 #include "pmb_ic.cuh"
 #include "pmb_integrate.cuh"
 #include "pmb_kernels.cuh"
+#include "pmb_mlp.cuh"
 #include "pmb_sort.cuh"
 
 namespace pmb {
@@ -513,6 +514,37 @@ int pmb_pk_shells_adjoint(const void* spec, int nx, int ny, int nz, const float*
 
 int pmb_overdensity(const float* rho, float* delta, int64_t n, const double* total, void* stream) {
   return overdensity(rho, delta, n, total, S(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Learned Green's-function correction
+// ---------------------------------------------------------------------------
+int pmb_mlp_param_counts(int* n_weights, int* n_biases) {
+  if (n_weights) *n_weights = kMlpWeights;
+  if (n_biases) *n_biases = kMlpBiases;
+  return kOk;
+}
+
+int pmb_mlp_table(const void* weights_bf16, const float* biases, float kscale, float a, float omega_m, float sigma8,
+                  int len, float* table, void* stream) {
+  PMB_REQUIRE(weights_bf16 != nullptr && biases != nullptr && table != nullptr && len > 0,
+              "pmb_mlp_table: bad arguments");
+  return mlp_table(weights_bf16, biases, MlpCond{kscale, a, omega_m, sigma8}, len, table, S(stream));
+}
+
+int pmb_mlp_backward(const void* weights_bf16, const float* biases, float kscale, float a, float omega_m,
+                     float sigma8, int len, const double* table_cot, float* grad, void* stream) {
+  PMB_REQUIRE(weights_bf16 != nullptr && biases != nullptr && table_cot != nullptr && grad != nullptr && len > 0,
+              "pmb_mlp_backward: bad arguments");
+  return mlp_backward(weights_bf16, biases, MlpCond{kscale, a, omega_m, sigma8}, len, table_cot, grad, S(stream));
+}
+
+int pmb_transfer_cot(const void* grad_cot_hat, const void* src_hat, int nx, int ny, int nz, const float* tables,
+                     int has_masks, int len, double* out, void* stream) {
+  Mesh3 m{nx, ny, nz};
+  PMB_REQUIRE(nx > 0 && ny > 0 && nz > 0 && len > 0, "pmb_transfer_cot: bad arguments");
+  return transfer_cot((const float2*)grad_cot_hat, (const float2*)src_hat, m, make_tables(tables, m, has_masks), len,
+                      out, S(stream));
 }
 
 // ---------------------------------------------------------------------------

@@ -41,14 +41,28 @@ def _stage_buffers(n, conf, dev):
     return sorted_buf, sort_scr, s16, real3, spec3, spec1, work
 
 
+class _NoTimer:
+    def start(self):
+        return None
+
+    def mark(self, name, start):
+        return None
+
+
 def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc, drift_vel, drift, vel_kick,
-                  kick, timer):
-    """pmb_force as separate stage calls with a CUDA event after each stage."""
+                  kick, timer, src_hat_out=None):
+    """pmb_force as separate stage calls with a CUDA event after each stage.
+
+    With src_hat_out (complex64, half spectrum) the rFFT of the Poisson source
+    is kept there (the learned correction's adjoint needs it)."""
     n = pmid.shape[0]
     nx, ny, nz = conf.mesh_shape
     dev = disp.device
     s = stream_handle(dev)
     sorted_buf, sort_scr, s16, real3, spec3, spec1, work = _stage_buffers(n, conf, dev)
+    if src_hat_out is not None:
+        spec1 = src_hat_out
+    timer = _NoTimer() if timer is None else timer
     t = timer.start()
     call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
          float(conf.cell_size), sorted_buf.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
@@ -68,13 +82,19 @@ def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F
     timer.mark("gather", t)
 
 
-def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc_cot, disp_cot, timer):
-    """pmb_force_vjp as separate stage calls with a CUDA event after each stage."""
+def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc_cot, disp_cot, timer,
+                      src_hat=None, transfer_cot_out=None):
+    """pmb_force_vjp as separate stage calls with a CUDA event after each stage.
+
+    With src_hat (the source spectrum at the same positions) and
+    transfer_cot_out (float64, radial table length) also accumulates dL/dT per
+    integer |n|^2 (pmb_transfer_cot)."""
     n = pmid.shape[0]
     nx, ny, nz = conf.mesh_shape
     dev = disp.device
     s = stream_handle(dev)
     sorted_buf, sort_scr, s16, real3, spec3, spec1, work = _stage_buffers(n, conf, dev)
+    timer = _NoTimer() if timer is None else timer
     t = timer.start()
     call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), None, 0.0, n, nx, ny, nz, float(conf.cell_size),
          sorted_buf.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
@@ -87,6 +107,9 @@ def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, r
     t = timer.mark("scatter3", t)
     call("pmb_rfft3", nx, ny, nz, 3, real3.data_ptr(), spec3.data_ptr(), work.data_ptr(), s)
     t = timer.mark("fft_r2c", t)
+    if transfer_cot_out is not None:
+        call("pmb_transfer_cot", spec3.data_ptr(), src_hat.data_ptr(), nx, ny, nz, tables.data_ptr(),
+             int(conf.has_particle_nyquist_masks), int(transfer_cot_out.numel()), transfer_cot_out.data_ptr(), s)
     post = float(np.float32(1.5 * _om32(omega_m)) / conf.mesh_size)
     call("pmb_green_gradient_adjoint", spec3.data_ptr(), spec1.data_ptr(), nx, ny, nz, tables.data_ptr(),
          int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, post, s)
@@ -108,7 +131,7 @@ def _correction_args(correction, a, cosmo, conf):
 
 
 def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, force_meshes=None, acc=None,
-          drift_vel=None, drift=0.0, vel_kick=None, kick=0.0):
+          drift_vel=None, drift=0.0, vel_kick=None, kick=0.0, src_hat_out=None):
     """One PM force evaluation on device tensors.
 
     Returns (acc (N,3), force_meshes (3,Mx,My,Mz)).  With drift_vel the
@@ -124,9 +147,9 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
         acc = torch.empty((n, 3), dtype=torch.float32, device=dev)
     gk, transfer, radial, rl = _correction_args(correction, a, cosmo, conf)
     tables = conf.spectral_tables("mesh", dev, gk)
-    if StageTimer.active is not None:
+    if StageTimer.active is not None or src_hat_out is not None:
         _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc, drift_vel,
-                      drift, vel_kick, kick, StageTimer.active)
+                      drift, vel_kick, kick, StageTimer.active, src_hat_out)
         return acc, force_meshes
     wb = lib().pmb_force_workspace_bytes(n, nx, ny, nz)
     if wb < 0:
@@ -140,7 +163,7 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
 
 
 def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *, a=None, cosmo=None,
-              correction=None):
+              correction=None, src_hat=None, transfer_cot_out=None):
     """disp_cot (+)= (d acc / d disp)^T acc_cot, with force_meshes computed at disp."""
     require_cuda(pmid, disp, force_meshes, acc_cot, disp_cot)
     n = pmid.shape[0]
@@ -150,9 +173,9 @@ def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *
         disp_cot = torch.zeros((n, 3), dtype=torch.float32, device=dev)
     gk, transfer, radial, rl = _correction_args(correction, a, cosmo, conf)
     tables = conf.spectral_tables("mesh", dev, gk)
-    if StageTimer.active is not None:
+    if StageTimer.active is not None or transfer_cot_out is not None:
         _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc_cot,
-                          disp_cot, StageTimer.active)
+                          disp_cot, StageTimer.active, src_hat, transfer_cot_out)
         return disp_cot
     wb = lib().pmb_force_vjp_workspace_bytes(n, nx, ny, nz)
     ws = workspace(wb, dev, "force_vjp")

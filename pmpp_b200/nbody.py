@@ -98,8 +98,9 @@ class NBodyRun:
         acc = torch.empty_like(disp)
         F = torch.empty((3, ) + conf.mesh_shape, dtype=torch.float32, device=disp.device)
         s = stream_handle(disp.device)
+        S = self._src_hat_buffer(disp.device)
         force(ptcl.pmid, disp, conf, cosmo.Omega_m, a=float(a[0]), cosmo=cosmo, correction=self.correction,
-              force_meshes=F, acc=acc)
+              force_meshes=F, acc=acc, src_hat_out=S)
         for a_prev, a_next in zip(a[:-1], a[1:]):
             stages = _schedule(a_prev, a_next, conf)
             i = 0
@@ -118,12 +119,35 @@ class NBodyRun:
                     kick_f, vk = _f32(cosmo.kick_factor(kst[1], kst[2], kst[3])), vel
                     i += 1
                 force(ptcl.pmid, disp, conf, cosmo.Omega_m, a=float(st[3]), cosmo=cosmo, correction=self.correction,
-                      force_meshes=F, acc=acc, drift_vel=vel, drift=D, vel_kick=vk, kick=kick_f)
+                      force_meshes=F, acc=acc, drift_vel=vel, drift=D, vel_kick=vk, kick=kick_f, src_hat_out=S)
                 i += 1
         self.final_meshes = F
+        self.final_src_hat = S
         return ptcl.replace(disp=disp, vel=vel, acc=acc)
 
-    def adjoint(self, ptcl, ptcl_cot, force_meshes=None, a_nbody=None):
+    def _trainable(self):
+        return self.correction is not None and getattr(self.correction, "trainable", False)
+
+    def _src_hat_buffer(self, device):
+        """Source-spectrum buffer, only when a trainable correction needs it in the adjoint."""
+        if not self._trainable():
+            return None
+        nx, ny, nz = self.conf.mesh_shape
+        return torch.empty((nx, ny, nz // 2 + 1), dtype=torch.complex64, device=device)
+
+    def _force_adjoint(self, pmid, disp, F, S, ac, dc, a):
+        """Force adjoint; with a trainable correction also its parameter gradient."""
+        conf, cosmo, corr = self.conf, self.cosmo, self.correction
+        if self._trainable():
+            from .corrections import radial_table_len
+            tc = torch.zeros(radial_table_len(conf), dtype=torch.float64, device=disp.device)
+            force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=corr, src_hat=S,
+                      transfer_cot_out=tc)
+            corr.accumulate(a, cosmo, conf, tc)
+        else:
+            force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=corr)
+
+    def adjoint(self, ptcl, ptcl_cot, force_meshes=None, a_nbody=None, src_hat=None):
         """Reverse sweep from the final state.  Returns (ptcl_in, ptcl_in_cot, Omega_m_cot).
 
         force_meshes must be the force meshes at ptcl's positions (the
@@ -139,6 +163,8 @@ class NBodyRun:
         ac = (ptcl_cot.acc if ptcl_cot.acc is not None else torch.zeros_like(dc)).clone().float().contiguous()
         F = self.final_meshes if force_meshes is None else force_meshes
         F2 = torch.empty_like(F)
+        S = (self.final_src_hat if src_hat is None else src_hat) if self._trainable() else None
+        S2 = self._src_hat_buffer(dev)
         dots = torch.zeros(4 * len(a) + 8, dtype=torch.float64, device=dev)
         grads = []  # (d factor / d Omega_m, dot slot) pairs, reduced on the host at the end
         force_slots = []
@@ -158,7 +184,7 @@ class NBodyRun:
                 call("pmb_dot", ac.data_ptr(), acc.data_ptr(), ac.numel(), dots[slot:].data_ptr(), s)
                 force_slots.append(slot)
                 slot += 1
-                force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=float(a_dn), cosmo=cosmo, correction=corr)
+                self._force_adjoint(pmid, disp, F, S, ac, dc, float(a_dn))
                 ac.zero_()
                 D, dD = cosmo.drift_factor(a_vel, a_dp, a_dn, with_grad=True)
                 call("pmb_drift_adj", disp.data_ptr(), vel.data_ptr(), dc.data_ptr(), vc.data_ptr(), disp.numel(),
@@ -167,12 +193,13 @@ class NBodyRun:
                 slot += 1
                 # recompute the incoming acceleration; keep its meshes for the next force adjoint
                 force(pmid, disp, conf, cosmo.Omega_m, a=float(a_acc_in), cosmo=cosmo, correction=corr,
-                      force_meshes=F2, acc=acc)
+                      force_meshes=F2, acc=acc, src_hat_out=S2)
                 F, F2 = F2, F
+                S, S2 = S2, S
         # the initial force evaluation (solver.py:437-441)
         call("pmb_dot", ac.data_ptr(), acc.data_ptr(), ac.numel(), dots[slot:].data_ptr(), s)
         force_slots.append(slot)
-        force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=float(a[0]), cosmo=cosmo, correction=corr)
+        self._force_adjoint(pmid, disp, F, S, ac, dc, float(a[0]))
         ac.zero_()
         d = dots.cpu().numpy()
         om_cot = sum(g * d[k] for g, k in grads) + sum(d[k] for k in force_slots) / om32

@@ -157,7 +157,7 @@ def log_binned(k, pk, nmodes, nbins=32, kmin=None, kmax=None):
     return kb, pb, w
 
 
-def pk_loss(ptcl, conf, pk_target, mas="CIC", grad=True):
+def pk_loss(ptcl, conf, pk_target, mas="CIC", grad=True, kmax=None):
     """L = mean_s (log P_s / P_target,s)^2 over shells with modes, and dL/d disp.
 
     Forward: scatter -> delta = rho/mean - 1 -> rFFT -> FP64 shell sums.
@@ -178,6 +178,8 @@ def pk_loss(ptcl, conf, pk_target, mas="CIC", grad=True):
     k, pk, nmodes = _finalize(sums, conf)
     tgt = np.asarray(pk_target, dtype=np.float64)
     valid = (nmodes > 0) & (pk > 0) & (tgt > 0)
+    if kmax is not None:
+        valid &= k <= kmax
     lr = np.where(valid, np.log(np.where(valid, pk, 1.0) / np.where(valid, tgt, 1.0)), 0.0)
     nv = max(int(valid.sum()), 1)
     loss = float((lr**2).sum() / nv)
