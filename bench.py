@@ -38,6 +38,7 @@ def parse():
     p.add_argument("--mesh", type=int, default=2)
     p.add_argument("--nsteps", type=int, default=32)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-learned", action="store_true")
     p.add_argument("--cpu-ptcl", type=int, default=128)
     return p.parse_args()
 
@@ -298,6 +299,14 @@ def run_ours(args):
     counts["other (kick/drift adjoints, LPT, P(k), host)"] = args.steps
     breakdown = {k: {"ms_total": round(v, 3), "launches": counts[k], "share": round(v / (ms * args.steps), 4)}
                  for k, v in sorted(stages.items(), key=lambda kv: -kv[1])}
+    learned = None
+    wpath = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pmpp_b200", "data", "learned_green_c3.npy")
+    if world == 1 and not args.no_learned and os.path.exists(wpath):
+        # second half of the metric: learned 128^3-mesh run vs plain 384^3-mesh run
+        # (128^3 particles, 256 Mpc/h, 20 KDK steps), committed weights trained by
+        # `python -m pmpp_b200.learned`, evaluated on held-out seeds 64..79
+        from pmpp_b200 import learned as pl
+        learned = pl.evaluate(wpath)
     cpu = None
     if not args.no_cpu_baseline:
         r, dt, sample = cpu_sample_rate(args.cpu_ptcl, args.mesh, 1)
@@ -319,6 +328,7 @@ def run_ours(args):
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
+        "learned": learned,
     }
     print(json.dumps(line), flush=True)
     if world > 1:

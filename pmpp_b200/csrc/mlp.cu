@@ -99,17 +99,79 @@ __device__ float forward_one(const SmemW& s, const float x[kIn], float z1[H], fl
 }
 }  // namespace
 
-__global__ void __launch_bounds__(128) mlp_table_kernel(const __nv_bfloat16* __restrict__ w,
+// Table evaluation, tile-parallel: a block evaluates kTE entries; thread
+// (group g, unit j) computes hidden unit j for entries g, g+4, ... so every
+// layer is a (kTE x 64) x (64 x 64) product from shared memory.  Weights are
+// kept transposed ([in][out]) so a warp reads 32 consecutive output units.
+constexpr int kTE = 32;
+
+__global__ void __launch_bounds__(256) mlp_table_kernel(const __nv_bfloat16* __restrict__ w,
                                                         const float* __restrict__ b, MlpCond cond, int len,
                                                         float* __restrict__ table) {
-  __shared__ SmemW s;
-  load_weights(s, unpack(w, b));
-  __syncthreads();
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < len; e += gridDim.x * blockDim.x) {
-    float x[kIn], z1[H], z2[H], z3[H];
-    features(e, cond, x);
-    const float y = forward_one(s, x, z1, z2, z3);
-    table[e] = e == 0 ? 1.0f : 1.0f + y;  // T(|k| = 0) = 1 (corrections/radial.py:193-194)
+  __shared__ __nv_bfloat16 W2t[H * H], W3t[H * H];  // [in][out]
+  __shared__ float W1t[kIn * H], W4[H], b1[H], b2[H], b3[H];
+  __shared__ float xin[kTE][kIn];
+  __shared__ float act[2][kTE][H];
+  const MlpW p = unpack(w, b);
+  for (int q = threadIdx.x; q < H * H; q += blockDim.x) {
+    const int o = q / H, i = q % H;
+    W2t[i * H + o] = p.W2[q];
+    W3t[i * H + o] = p.W3[q];
+  }
+  for (int q = threadIdx.x; q < H * kIn; q += blockDim.x) W1t[(q % kIn) * H + q / kIn] = __bfloat162float(p.W1[q]);
+  for (int q = threadIdx.x; q < H; q += blockDim.x) {
+    W4[q] = __bfloat162float(p.W4[q]);
+    b1[q] = p.b1[q];
+    b2[q] = p.b2[q];
+    b3[q] = p.b3[q];
+  }
+  const float b4 = p.b4[0];
+  const int j = threadIdx.x % H;   // hidden unit
+  const int g0 = threadIdx.x / H;  // entry group 0..3
+  constexpr int kPer = kTE / 4;    // entries per thread
+  for (int tile = blockIdx.x * kTE; tile < len; tile += gridDim.x * kTE) {
+    __syncthreads();
+    if (threadIdx.x < kTE) {
+      float x[kIn];
+      features(tile + threadIdx.x, cond, x);
+#pragma unroll
+      for (int i = 0; i < kIn; ++i) xin[threadIdx.x][i] = x[i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int e = g0 + 4 * k;
+      float acc = b1[j];
+#pragma unroll
+      for (int i = 0; i < kIn; ++i) acc = fmaf(W1t[i * H + j], xin[e][i], acc);
+      act[0][e][j] = sinf(acc);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+      const __nv_bfloat16* Wt = l == 0 ? W2t : W3t;
+      const float* bl = l == 0 ? b2 : b3;
+      float acc[kPer];
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) acc[k] = bl[j];
+      for (int i = 0; i < H; ++i) {
+        const float wv = __bfloat162float(Wt[i * H + j]);
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) acc[k] = fmaf(wv, act[l][g0 + 4 * k][i], acc[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) act[l ^ 1][g0 + 4 * k][j] = sinf(acc[k]);
+      __syncthreads();
+    }
+    // output y_e = b4 + sum_j W4[j] h3[e][j]: one warp per entry
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    for (int e = warp; e < kTE; e += blockDim.x / 32) {
+      float v = W4[lane] * act[0][e][lane] + W4[lane + 32] * act[0][e][lane + 32];
+      for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+      const int idx = tile + e;
+      // T(|k| = 0) = 1 (corrections/radial.py:193-194)
+      if (lane == 0 && idx < len) table[idx] = idx == 0 ? 1.0f : 1.0f + (b4 + v);
+    }
   }
 }
 
@@ -266,8 +328,9 @@ __global__ void transfer_cot_kernel(const float2* __restrict__ R3, const float2*
 }
 
 int mlp_table(const void* w, const float* b, MlpCond c, int len, float* table, cudaStream_t s) {
-  int blocks = (len + 127) / 128;
-  mlp_table_kernel<<<blocks > 0 ? blocks : 1, 128, 0, s>>>((const __nv_bfloat16*)w, b, c, len, table);
+  int blocks = (len + kTE - 1) / kTE;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  mlp_table_kernel<<<blocks > 0 ? blocks : 1, 256, 0, s>>>((const __nv_bfloat16*)w, b, c, len, table);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }

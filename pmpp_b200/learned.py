@@ -83,6 +83,40 @@ def density(disp, coarse):
     return SortedParticles(grid.pmid, disp, coarse).scatter()[0]
 
 
+def graphed_runs(smp, coarse, fine, model):
+    """CUDA-graph-captured forward runs: learned 128^3 mesh and plain 384^3 mesh."""
+    from .graphs import GraphedForward
+    pc = Particles(coarse, Particles.gen_grid(coarse, device=smp.ic.disp.device).pmid, smp.ic.disp, smp.ic.vel)
+    pf = Particles(fine, Particles.gen_grid(fine, device=smp.ic.disp.device).pmid, smp.ic.disp, smp.ic.vel)
+    return GraphedForward(coarse, smp.cos_c, pc, model), GraphedForward(fine, smp.cos_f, pf)
+
+
+def evaluate(params_path, test_seeds=range(64, 80), nsteps=20, kmax=0.5):
+    """Held-out evaluation with stored parameters (float32 .npy of weights then biases).
+
+    Returns plain / learned max |P/P_fine - 1| (k <= kmax) averaged over the
+    seeds and the CUDA-graph times of a learned 128^3 and a plain 384^3 run."""
+    coarse, fine = configs(nsteps)
+    model = LearnedGreen("cuda", seed=0)
+    model.load_parameters(torch.from_numpy(np.load(params_path)))
+    ep, el = [], []
+    for s in test_seeds:
+        smp = Sample(s, coarse, fine)
+        _, out_f = run_forward(smp, fine, smp.cos_f)
+        tgt = pk_of(out_f.disp, coarse)
+        sel = tgt[0] <= kmax
+        _, plain = run_forward(smp, coarse, smp.cos_c)
+        _, learn = run_forward(smp, coarse, smp.cos_c, model)
+        ep.append(float(np.max(np.abs(pk_of(plain.disp, coarse)[1][sel] / tgt[1][sel] - 1))))
+        el.append(float(np.max(np.abs(pk_of(learn.disp, coarse)[1][sel] / tgt[1][sel] - 1))))
+    g_learn, g_fine = graphed_runs(smp, coarse, fine, model)
+    tl = gpu_time(g_learn, reps=10)
+    tf = gpu_time(g_fine, reps=5)
+    return {"seeds": len(ep), "max_pk_err_plain_128": float(np.mean(ep)), "max_pk_err_learned_128": float(np.mean(el)),
+            "worst_pk_err_learned_128": float(np.max(el)), "kmax": kmax, "time_ms_learned_128": tl,
+            "time_ms_plain_384": tf, "speedup": tf / tl}
+
+
 def gpu_time(fn, reps=3):
     fn()
     torch.cuda.synchronize()
@@ -146,6 +180,9 @@ def main(argv=None):
     smp = samples[args.train]
     t_learn = gpu_time(lambda: run_forward(smp, coarse, smp.cos_c, model))
     t_fine = gpu_time(lambda: run_forward(smp, fine, smp.cos_f))
+    g_learn, g_fine = graphed_runs(smp, coarse, fine, model)
+    tg_learn = gpu_time(g_learn, reps=10)
+    tg_fine = gpu_time(g_fine, reps=5)
     res = {
         "config": {"particles": NP**3, "box": BOX, "coarse_mesh": coarse.mesh_shape[0], "fine_mesh": fine.mesh_shape[0],
                    "kdk_steps": args.nsteps, "train_seeds": args.train, "test_seeds": args.test,
@@ -154,13 +191,14 @@ def main(argv=None):
         "test": evals,
         "test_mean_max_pk_err": {"plain": float(np.mean([e["plain_max_pk_err"] for e in evals])),
                                  "learned": float(np.mean([e["learned_max_pk_err"] for e in evals]))},
-        "time_ms": {"learned_128": t_learn, "plain_384": t_fine, "speedup": t_fine / t_learn},
+        "time_ms": {"learned_128": t_learn, "plain_384": t_fine, "speedup": t_fine / t_learn,
+                    "graphed_learned_128": tg_learn, "graphed_plain_384": tg_fine, "graphed_speedup": tg_fine / tg_learn},
         "wall_s": {"data": t_data, "train": t_train},
     }
     if args.out:
         with open(args.out, "w") as f:
             json.dump(res, f, indent=1)
-        torch.save(model.parameters().cpu(), args.out.replace(".json", "_params.pt"))
+        np.save(args.out.replace(".json", "_params.npy"), model.parameters().cpu().numpy().astype(np.float32))
     print(json.dumps({k: res[k] for k in ("test_mean_max_pk_err", "time_ms", "wall_s", "train_loss_first",
                                           "train_loss_last")}))
     return res
