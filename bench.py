@@ -124,24 +124,6 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-# --------------------------------------------------------------------------
-# algorithmic bytes per launch (the roofline numerator)
-# --------------------------------------------------------------------------
-def algorithmic_bytes(stage, N, M):
-    Mc = M // 2  # ~ nx*ny*(nz/2+1) for large nz
-    return {
-        "sort": 18 * N + 20 * N,               # read pmid+disp, write records+permutation
-        "scatter": 18 * N + 4 * M,             # particle positions in, density mesh out
-        "gather": 18 * N + 12 * N + 12 * M,    # positions, acc out, 3 force meshes in
-        "green_gradient": 8 * Mc + 24 * Mc,    # 1 spectrum in, 3 out
-        "fft_r2c": 4 * M + 8 * Mc,
-        "fft_c2r": 3 * (8 * Mc + 4 * M),
-        "gather_adjoint": 18 * N + 12 * N + 12 * N + 12 * M,
-        "scatter3": 18 * N + 12 * N + 12 * M,
-        "scatter_adjoint": 18 * N + 12 * N + 4 * M,
-    }.get(stage)
-
-
 def load_peaks():
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
     try:
@@ -293,7 +275,9 @@ def run_ours(args):
     ours = {k: v for k, v in stages.items() if not k.startswith("fft")}
     dom = max(ours, key=ours.get)
     per_launch_ms = ours[dom] / counts[dom]
-    alg = algorithmic_bytes(dom, N, M)
+    from pmpp_b200.roofline import algorithmic_bytes
+    nx, ny, nz = conf.mesh_shape
+    alg = algorithmic_bytes(dom, N, M, Mc=nx * ny * (nz // 2 + 1), R=nx * ny)
     achieved = alg / (per_launch_ms * 1e-3) / 1e9
     stages["other (kick/drift adjoints, LPT, P(k), host)"] = max(ms * args.steps - sum(stages.values()), 0.0)
     counts["other (kick/drift adjoints, LPT, P(k), host)"] = args.steps

@@ -1,0 +1,165 @@
+"""PM stage microbenchmark: 256^3 particles on a 512^3 mesh, unit masses.
+
+Two position sets:
+
+* U -- uniform random positions in the box (numpy PCG64, seed 1);
+* K -- the final positions of the 64^3 / 128^3-mesh, 256 Mpc/h, sigma8 = 0.8
+  run (2LPT at a = 0.1, 10 KDK steps to a = 1, noise seed 0) tiled 4 x 4 x 4
+  onto the 256^3 lattice (clustered, same particle spacing).
+
+Timed per stage with CUDA events on the launching stream (mean over
+``reps`` launches after warm-up): row sort, density scatter, R2C, Green x
+gradient, 3 x C2R, 3-channel gather, and the adjoints -- scatter VJP (position
+term against an N(0,1) mesh cotangent), gather VJP (position term + 3-channel
+scatter against N(0,1) particle cotangents, seed 2), and the spectral adjoint
+(3 x R2C, Green adjoint, C2R).  Every stage reports algorithmic bytes per
+launch (pmpp_b200.roofline, with the measured count of touched cells) and
+the fraction of the measured HBM copy bandwidth.
+
+    python -m pmpp_b200.microbench --ptcl 256 --mesh 2 --reps 10
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+
+import numpy as np
+import torch
+
+from . import lpt as _lpt
+from . import modes as _modes
+from ._lib import call, lib
+from .cic import SortedParticles
+from .configuration import Configuration
+from .cosmology import Cosmology
+from .nbody import nbody
+from .particles import Particles
+from .roofline import algorithmic_bytes
+from .runtime import stream_handle, workspace
+
+
+def uniform_positions(conf, seed=1):
+    """Set U: disp such that pmid * cell + disp is uniform in the box."""
+    grid = Particles.gen_grid(conf)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pos = rng.uniform(0.0, conf.box_size[0], size=(conf.ptcl_num, 3)).astype(np.float64)
+    base = grid.pmid.cpu().numpy().astype(np.float64) * conf.cell_size
+    disp = torch.from_numpy((pos - base).astype(np.float32)).to(grid.disp.device)
+    return Particles(conf, grid.pmid, disp)
+
+
+def clustered_positions(conf, seed=0):
+    """Set K: the 64^3 run's final displacements tiled onto conf's lattice."""
+    n1 = conf.ptcl_grid_shape[0]
+    mesh = conf.mesh_shape[0] // n1
+    a = np.linspace(0.1, 1.0, 11)
+    small = Configuration(conf.ptcl_spacing, (64, 64, 64), mesh, a_start=0.1, a_custom=a, device=conf.device)
+    cos = Cosmology.from_sigma8(small, 0.8, n_s=0.96, Omega_m=0.3, Omega_b=0.05, h=0.7)
+    lin = _modes.linear_modes(_modes.white_noise_nested(seed, small), cos, small)
+    out = nbody(_lpt.lpt(lin, cos, small), cos, small)
+    rep = n1 // 64
+    d = out.disp.reshape(64, 64, 64, 3).repeat(rep, rep, rep, 1).reshape(-1, 3).contiguous()
+    grid = Particles.gen_grid(conf)
+    return Particles(conf, grid.pmid, d)
+
+
+def _time(fn, reps):
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_set(ptcl, conf, reps, peak):
+    dev = ptcl.disp.device
+    L = lib()
+    s = stream_handle(dev)
+    n = conf.ptcl_num
+    nx, ny, nz = conf.mesh_shape
+    M = conf.mesh_size
+    Mc = nx * ny * (nz // 2 + 1)
+    tables = conf.spectral_tables("mesh", dev, 0)
+    rng = torch.Generator(device="cpu").manual_seed(2)
+    acc_cot = torch.randn((n, 3), generator=rng).to(dev)
+    mesh_cot = torch.randn((1, nx, ny, nz), generator=rng).to(dev)
+    rho = torch.empty((1, nx, ny, nz), dtype=torch.float32, device=dev)
+    F = torch.empty((3, nx, ny, nz), dtype=torch.float32, device=dev)
+    F3 = torch.empty_like(F)
+    spec1 = torch.empty((nx, ny, nz // 2 + 1), dtype=torch.complex64, device=dev)
+    spec3 = torch.empty((3, nx, ny, nz // 2 + 1), dtype=torch.complex64, device=dev)
+    acc = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    dcot = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    fw = max(L.pmb_fft_work_bytes(nx, ny, nz, 3), L.pmb_fft_work_bytes(nx, ny, nz, 1))
+    work = workspace(fw, dev, "micro_fft")
+    sp = SortedParticles(ptcl.pmid, ptcl.disp, conf)
+    vc = float(M / n)
+    inv_m = float(1.0 / M)
+
+    stages = {
+        "sort": lambda: SortedParticles(ptcl.pmid, ptcl.disp, conf),
+        "scatter": lambda: sp.scatter(out=rho, mode=1, src_mul=0.45),
+        "fft_r2c": lambda: call("pmb_rfft3", nx, ny, nz, 1, rho.data_ptr(), spec1.data_ptr(), work.data_ptr(), s),
+        "green_gradient": lambda: call("pmb_green_gradient", spec1.data_ptr(), spec3.data_ptr(), nx, ny, nz,
+                                       tables.data_ptr(), int(conf.has_particle_nyquist_masks), 0, None, None, 0,
+                                       inv_m, s),
+        "fft_c2r_x3": lambda: call("pmb_irfft3", nx, ny, nz, 3, spec3.data_ptr(), F.data_ptr(), work.data_ptr(), s),
+        "gather": lambda: sp.gather(F, out=acc),
+        "scatter_adjoint": lambda: sp.interp_grad(mesh_cot, u_const=vc, disp_cot=dcot, accumulate=True),
+        "gather_adjoint": lambda: sp.interp_grad(F, u=acc_cot, disp_cot=dcot, accumulate=True),
+        "scatter3": lambda: sp.scatter(val=acc_cot, channels=3, out=F3),
+        "fft_r2c_x3": lambda: call("pmb_rfft3", nx, ny, nz, 3, F3.data_ptr(), spec3.data_ptr(), work.data_ptr(), s),
+        "green_gradient_adjoint": lambda: call("pmb_green_gradient_adjoint", spec3.data_ptr(), spec1.data_ptr(), nx,
+                                               ny, nz, tables.data_ptr(), int(conf.has_particle_nyquist_masks), 0,
+                                               None, None, 0, 0.45 * inv_m, s),
+        "fft_c2r": lambda: call("pmb_irfft3", nx, ny, nz, 1, spec1.data_ptr(), rho.data_ptr(), work.data_ptr(), s),
+    }
+    # distinct touched cells: nonzero cells of the unit-mass density
+    T = int((sp.scatter() != 0).sum())
+    out = {"touched_cells": T}
+    for name, fn in stages.items():
+        ms = _time(fn, reps)
+        alg = algorithmic_bytes(name, n, M, Mc=Mc, R=nx * ny, T=T)
+        gbs = alg / (ms * 1e-3) / 1e9
+        out[name] = {"ms": round(ms, 4), "algorithmic_bytes": alg, "GB/s": round(gbs, 1), "frac_hbm": round(gbs / peak, 4)}
+    return out
+
+
+def load_peak():
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ptcl", type=int, default=256)
+    ap.add_argument("--mesh", type=int, default=2)
+    ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--sets", default="U,K")
+    args = ap.parse_args(argv)
+    if args.ptcl % 64:
+        raise ValueError("--ptcl must be a multiple of 64 (set K tiles the 64^3 run)")
+    conf = Configuration(4.0, (args.ptcl, ) * 3, args.mesh, a_start=0.1, device="cuda")
+    peak, kind = load_peak()
+    res = {"config": {"particles": conf.ptcl_num, "mesh": conf.mesh_size, "box": conf.box_size[0], "reps": args.reps},
+           "peak_gbs": peak, "peak_kind": kind}
+    for name in args.sets.split(","):
+        ptcl = uniform_positions(conf) if name == "U" else clustered_positions(conf)
+        res[name] = run_set(ptcl, conf, args.reps, peak)
+        del ptcl
+        torch.cuda.empty_cache()
+    print(json.dumps(res))
+    return res
+
+
+if __name__ == "__main__":
+    main()
