@@ -232,6 +232,59 @@ int pmb_transfer_fit(const double* k, int64_t nk, double omega_m, double omega_b
 int pmb_linear_power(const double* k, int64_t nk, const double* tk, const double* tt, int ntab, double A_s,
                      double n_s, double omega_m, double h, double k_pivot_Mpc, double* out);
 
+/* ---------------- ensembles of independent simulations --------------------
+ * No single counterpart in the reference, which advances one simulation per
+ * call (nbody/solver.py:253-273) and batches only by a Python loop or a vmap
+ * over equal shapes.  An ensemble advances many PM simulations of uneven
+ * sizes together, one persistent launch per PM stage over all of them; each
+ * simulation gets exactly the single-simulation arithmetic of pmb_sort_rows /
+ * pmb_scatter_rows (mode 1) / pmb_green_gradient / pmb_gather_rows / pmb_axpy.
+ *
+ * pmb_ens_create (host only): nsims descriptions -- particle counts,
+ * mesh_shapes[3*s], mesh cell sizes, deposit per particle (mesh cells /
+ * particles), Poisson source factor 1.5*Omega_m, particle-Nyquist mask flag --
+ * and the number of kick-drift-kick steps whose factors it stores.
+ * Simulations with equal mesh shape must be consecutive (one batched FFT per
+ * shape); ordering them by decreasing mesh size balances the persistent
+ * scatter.  The handle owns host memory only.
+ * pmb_ens_workspace_bytes: device workspace for pmb_ens_bind (256-byte
+ * aligned).  pmb_ens_size: 0 particles, 1 mesh cells, 2 half-spectrum cells,
+ * 3 scatter tiles, 4 distinct mesh shapes.
+ * pmb_ens_bind: concatenated particle arrays (simulation order), the
+ * concatenated Poisson source meshes rho (sum of cells), their spectra
+ * (sum of half cells), three gradient spectra and three force meshes per
+ * simulation ([3][cells] each, simulation after simulation), the spectral
+ * tables of every mesh (pmb_green_gradient layout) at table_offsets[s] floats
+ * into `tables` (host array of offsets).  Enqueues the descriptor upload.
+ * pmb_ens_set_factors: host table [nsteps][nsims][3] of float factors
+ * (opening kick K1, drift D, closing kick K2 of each step,
+ * nbody/integrator.py:125-170).  pmb_ens_set_step: device step counter.
+ * pmb_ens_force: sort (with drift: disp += vel*D of the current step), scatter
+ * of the Poisson source, R2C, Green x gradient, 3 x C2R, gather into acc
+ * (with kick: vel += acc*K2 of the current step).
+ * pmb_ens_step: vel += acc*K1, pmb_ens_force(drift, kick), step += 1 -- a
+ * kick-drift-kick step that a CUDA graph can capture once and replay.
+ * pmb_ens_stage: one stage alone (0 kick, 1 sort, 2 scatter, 3 R2C, 4 Green,
+ * 5 C2R, 6 gather) for tuning.  pmb_ens_set_tiles: per-simulation scatter
+ * tile rows (rx, ry <= 4); pmb_ens_set_launch: threads and CTAs per SM of a
+ * particle or cell stage.  Changes of tiles take effect at the next
+ * uncaptured call. */
+int pmb_ens_create(int nsims, const int64_t* counts, const int32_t* mesh_shapes, const float* cells,
+                   const float* vals, const float* src_muls, const int32_t* has_masks, int max_steps, void** handle);
+int pmb_ens_destroy(void* handle);
+int64_t pmb_ens_workspace_bytes(const void* handle);
+int64_t pmb_ens_size(const void* handle, int which);
+int pmb_ens_bind(void* handle, const int16_t* pmid, float* disp, float* vel, float* acc, float* rho, void* rho_hat,
+                 void* grad_hat, float* force, const float* tables, const int64_t* table_offsets, void* workspace,
+                 int64_t workspace_bytes, void* stream);
+int pmb_ens_set_tiles(void* handle, const int32_t* rx, const int32_t* ry);
+int pmb_ens_set_launch(void* handle, int stage, int threads, int ctas_per_sm);
+int pmb_ens_set_factors(void* handle, int nsteps, const float* factors, void* stream);
+int pmb_ens_set_step(void* handle, int step, void* stream);
+int pmb_ens_stage(void* handle, int stage, int drift, int kick, void* stream);
+int pmb_ens_force(void* handle, int drift, int kick, void* stream);
+int pmb_ens_step(void* handle, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,6 +65,18 @@ _SIGS = {
     "pmb_lpt_factors": (c_int, [c_d, c_d, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p]),
     "pmb_transfer_fit": (c_int, [c_p, c_i64, c_d, c_d, c_d, c_d, c_int, c_p]),
     "pmb_linear_power": (c_int, [c_p, c_i64, c_p, c_p, c_int, c_d, c_d, c_d, c_d, c_d, c_p]),
+    "pmb_ens_create": (c_int, [c_int, c_p, c_p, c_p, c_p, c_p, c_p, c_int, c_p]),
+    "pmb_ens_destroy": (c_int, [c_p]),
+    "pmb_ens_workspace_bytes": (c_i64, [c_p]),
+    "pmb_ens_size": (c_i64, [c_p, c_int]),
+    "pmb_ens_bind": (c_int, [c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_i64, c_p]),
+    "pmb_ens_set_tiles": (c_int, [c_p, c_p, c_p]),
+    "pmb_ens_set_launch": (c_int, [c_p, c_int, c_int, c_int]),
+    "pmb_ens_set_factors": (c_int, [c_p, c_int, c_p, c_p]),
+    "pmb_ens_set_step": (c_int, [c_p, c_int, c_p]),
+    "pmb_ens_stage": (c_int, [c_p, c_int, c_int, c_int, c_p]),
+    "pmb_ens_force": (c_int, [c_p, c_int, c_int, c_p]),
+    "pmb_ens_step": (c_int, [c_p, c_p]),
 }
 
 _lib = None
@@ -105,7 +117,7 @@ _KERNELS = {
     "pmb_green_gradient_adjoint": 1, "pmb_axpy": 1, "pmb_kick_adj": 1, "pmb_drift_adj": 1, "pmb_dot": 1,
     "pmb_force": 9, "pmb_force_vjp": 11, "pmb_sum": 1, "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,
     "pmb_lpt": 4, "pmb_lpt_vjp": 6, "pmb_pk_shells": 1, "pmb_shell_stats": 1, "pmb_pk_shells_adjoint": 1,
-    "pmb_overdensity": 1,
+    "pmb_overdensity": 1, "pmb_ens_force": 7, "pmb_ens_step": 9, "pmb_ens_set_step": 1,
 }
 _launches = [0]
 

@@ -63,24 +63,7 @@ SortedView sorted_view(void* sorted, int64_t n) {
 
 int64_t sorted_bytes(int64_t n, Mesh3 m) { return align_up(16 * n, 256) + align_up(4 * n, 256) + align_up(4 * (m.rows() + 1), 256); }
 
-SpecTables make_tables(const float* t, Mesh3 m, int has_masks) {
-  const int nzh = m.nz / 2 + 1;
-  SpecTables s;
-  s.kx = t;
-  s.ky = s.kx + m.nx;
-  s.kz = s.ky + m.ny;
-  s.cx = s.kz + nzh;
-  s.cy = s.cx + m.nx;
-  s.cz = s.cy + m.ny;
-  if (has_masks) {
-    s.mx = s.cz + nzh;
-    s.my = s.mx + m.nx;
-    s.mz = s.my + m.ny;
-  } else {
-    s.mx = s.my = s.mz = nullptr;
-  }
-  return s;
-}
+SpecTables make_tables(const float* t, Mesh3 m, int has_masks) { return spec_tables_from(t, m, has_masks); }
 
 GreenParams make_green(int green_kernel, const float* transfer, const float* radial, int radial_len, float post_scale) {
   GreenParams g;

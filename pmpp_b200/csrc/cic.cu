@@ -18,6 +18,7 @@
 //    eight corner loads of neighbouring threads hit the same cache lines.
 #include <cstdio>
 
+#include "pmb_cic_device.cuh"
 #include "pmb_common.cuh"
 #include "pmb_kernels.cuh"
 
@@ -26,25 +27,6 @@ namespace pmb {
 // ---------------------------------------------------------------------------
 // Binning
 // ---------------------------------------------------------------------------
-struct Binned {
-  int cx, cy, cz;
-  float fx, fy, fz;
-};
-
-__device__ __forceinline__ Binned bin_particle(const int16_t* __restrict__ pmid, const float d0, const float d1,
-                                               const float d2, int64_t i, Mesh3 m, float cell) {
-  Binned b;
-  float q0 = __fdiv_rn(d0, cell), q1 = __fdiv_rn(d1, cell), q2 = __fdiv_rn(d2, cell);
-  float l0 = floorf(q0), l1 = floorf(q1), l2 = floorf(q2);
-  b.fx = __fsub_rn(q0, l0);
-  b.fy = __fsub_rn(q1, l1);
-  b.fz = __fsub_rn(q2, l2);
-  b.cx = pmod((int)pmid[3 * i + 0] + (int)l0, m.nx);
-  b.cy = pmod((int)pmid[3 * i + 1] + (int)l1, m.ny);
-  b.cz = pmod((int)pmid[3 * i + 2] + (int)l2, m.nz);
-  return b;
-}
-
 // Count particles per row.  Optionally applies the drift disp += vel * D
 // first (integrator.py:223-225, two roundings as in the reference) and writes
 // the drifted displacement back.  Ranks come from warp-aggregated atomics.
@@ -269,7 +251,6 @@ int compute_scale(const float* val, int64_t count, int64_t n, double* scale_dev,
 // ---------------------------------------------------------------------------
 // Pull scatter
 // ---------------------------------------------------------------------------
-constexpr int kMaxSrcRows = 25;  // (RX+1)*(RY+1) with RX, RY <= 4
 // Epilogue: mode 0 writes the density sum, mode 1 writes the Poisson source
 // (rho - 1) * src_mul (gravity.py:628-630), both in float.
 template <int C>
@@ -279,103 +260,11 @@ __global__ void __launch_bounds__(256) scatter_pull_kernel(const Rec* __restrict
                                                            const double* __restrict__ scale_dev, int mode,
                                                            float src_mul, float* __restrict__ out) {
   extern __shared__ long long acc[];  // [RX][RY][C][nz]
-  __shared__ uint32_t seg_beg[kMaxSrcRows];
-  __shared__ uint32_t seg_pre[kMaxSrcRows + 1];
+  __shared__ ScatterSmem sm;
   const int nby = (m.ny + RY - 1) / RY;
   const int x0 = (int)(blockIdx.x / nby) * RX;
   const int y0 = (int)(blockIdx.x % nby) * RY;
-  const int nz = m.nz;
-  const int nsrc = (RX + 1) * (RY + 1);
-  const int total = RX * RY * C * nz;
-  for (int t = threadIdx.x; t < total; t += blockDim.x) acc[t] = 0;
-  // source-row segments of the (RX+1) x (RY+1) rows that reach this block,
-  // flattened so all threads stay busy regardless of per-row counts
-  if (threadIdx.x < nsrc) {
-    const int k = threadIdx.x;
-    const int px = pmod(x0 + k / (RY + 1) - 1, m.nx), py = pmod(y0 + k % (RY + 1) - 1, m.ny);
-    const int64_t row = (int64_t)px * m.ny + py;
-    const uint32_t b = offs[row];
-    seg_beg[k] = b;
-    seg_pre[k + 1] = offs[row + 1] - b;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t run = 0;
-    for (int k = 0; k < nsrc; ++k) {
-      const uint32_t c = seg_pre[k + 1];
-      seg_pre[k] = run;
-      run += c;
-    }
-    seg_pre[nsrc] = run;
-  }
-  __syncthreads();
-  const double scale = *scale_dev;
-  const uint32_t ntot = seg_pre[nsrc];
-  for (uint32_t idx = threadIdx.x; idx < ntot; idx += blockDim.x) {
-    {
-      int k = 0;
-      while (idx >= seg_pre[k + 1]) ++k;
-      const int sx = k / (RY + 1) - 1, sy = k % (RY + 1) - 1;
-      const uint32_t i = seg_beg[k] + (idx - seg_pre[k]);
-      {
-        const Rec r = rec[i];
-        const int cz = (int)(r.key % (uint32_t)nz);
-        float v[C];
-        if (val != nullptr) {
-          const uint32_t src = perm[i];
-#pragma unroll
-          for (int c = 0; c < C; ++c) v[c] = val[(int64_t)src * C + c];
-        } else {
-#pragma unroll
-          for (int c = 0; c < C; ++c) v[c] = val_const;
-        }
-#pragma unroll
-        for (int bx = 0; bx < 2; ++bx) {
-          const int lx = sx + bx;
-          if (lx < 0 || lx >= RX || x0 + lx >= m.nx) continue;
-          const float wx = axis_weight(r.fx, bx);
-#pragma unroll
-          for (int by = 0; by < 2; ++by) {
-            const int ly = sy + by;
-            if (ly < 0 || ly >= RY || y0 + ly >= m.ny) continue;
-            const float wxy = __fmul_rn(wx, axis_weight(r.fy, by));
-#pragma unroll
-            for (int bz = 0; bz < 2; ++bz) {
-              int z = cz + bz;
-              if (z >= nz) z -= nz;
-              const float w = __fmul_rn(wxy, axis_weight(r.fz, bz));
-#pragma unroll
-              for (int c = 0; c < C; ++c) {
-                const float contrib = __fmul_rn(v[c], w);
-                const long long q = __double2ll_rn((double)contrib * scale);
-                atomicAdd((unsigned long long*)&acc[((lx * RY + ly) * C + c) * nz + z], (unsigned long long)q);
-              }
-            }
-          }
-        }
-      }
-    }
-  }
-  __syncthreads();
-  const double inv = 1.0 / scale;
-  const int64_t cells = m.cells();
-  for (int lx = 0; lx < RX; ++lx) {
-    if (x0 + lx >= m.nx) break;
-    for (int ly = 0; ly < RY; ++ly) {
-      if (y0 + ly >= m.ny) break;
-      const int64_t row_off = ((int64_t)(x0 + lx) * m.ny + (y0 + ly)) * nz;
-#pragma unroll
-      for (int c = 0; c < C; ++c) {
-        const long long* a = acc + ((lx * RY + ly) * C + c) * nz;
-        float* o = out + (int64_t)c * cells + row_off;
-        for (int z = threadIdx.x; z < nz; z += blockDim.x) {
-          float rho = (float)((double)a[z] * inv);
-          if (mode == 1) rho = __fmul_rn(__fsub_rn(rho, 1.0f), src_mul);
-          o[z] = rho;
-        }
-      }
-    }
-  }
+  scatter_tile<C>(rec, perm, offs, m, RX, RY, x0, y0, val, val_const, *scale_dev, mode, src_mul, out, acc, sm);
 }
 
 void scatter_block_shape(Mesh3 m, int C, int* RX, int* RY) {
@@ -423,32 +312,6 @@ int scatter_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, M
 // ---------------------------------------------------------------------------
 // Gather and adjoint position terms
 // ---------------------------------------------------------------------------
-struct Corners {
-  int64_t idx[8];
-  float w[8];
-};
-
-__device__ __forceinline__ void corners_of(const Rec& r, Mesh3 m, Corners& k) {
-  const uint32_t key = r.key;
-  const int cz = (int)(key % (uint32_t)m.nz);
-  const uint32_t rowk = key / (uint32_t)m.nz;
-  const int cy = (int)(rowk % (uint32_t)m.ny);
-  const int cx = (int)(rowk / (uint32_t)m.ny);
-  const int x1 = cx + 1 == m.nx ? 0 : cx + 1;
-  const int y1 = cy + 1 == m.ny ? 0 : cy + 1;
-  const int z1 = cz + 1 == m.nz ? 0 : cz + 1;
-  const float wx[2] = {axis_weight(r.fx, 0), axis_weight(r.fx, 1)};
-  const float wy[2] = {axis_weight(r.fy, 0), axis_weight(r.fy, 1)};
-  const float wz[2] = {axis_weight(r.fz, 0), axis_weight(r.fz, 1)};
-#pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const int bx = c & 1, by = (c >> 1) & 1, bz = (c >> 2) & 1;
-    const int x = bx ? x1 : cx, y = by ? y1 : cy, z = bz ? z1 : cz;
-    k.idx[c] = ((int64_t)x * m.ny + y) * m.nz + z;
-    k.w[c] = __fmul_rn(__fmul_rn(wx[bx], wy[by]), wz[bz]);
-  }
-}
-
 // out[src, c] = sum_b mesh_c[i_b] w_b (gather.py:452-472, pallas.py:305-318).
 // With kick != 0 the second half-kick vel += out * kick is applied in place
 // (integrator.py:536), saving a pass over the particles.
@@ -458,20 +321,7 @@ __global__ void gather_kernel(const Rec* __restrict__ rec, const uint32_t* __res
                               float kick) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const Rec r = rec[i];
-  const uint32_t src = perm[i];
-  Corners k;
-  corners_of(r, m, k);
-  const int64_t cells = m.cells();
-#pragma unroll
-  for (int c = 0; c < C; ++c) {
-    const float* mc = mesh + (int64_t)c * cells;
-    float a = 0.f;
-#pragma unroll
-    for (int b = 0; b < 8; ++b) a = __fadd_rn(a, __fmul_rn(__ldg(mc + k.idx[b]), k.w[b]));
-    out[(int64_t)src * C + c] = a;
-    if (vel != nullptr) vel[(int64_t)src * C + c] = __fadd_rn(vel[(int64_t)src * C + c], __fmul_rn(a, kick));
-  }
+  gather_one<C>(rec[i], perm[i], m, mesh, out, vel, kick);
 }
 
 int gather_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int C, const float* mesh, float* out,

@@ -1,0 +1,191 @@
+// Device-side CIC building blocks shared by the single-simulation kernels
+// (cic.cu) and the persistent ensemble kernels (ensemble.cu).
+//
+// Reference semantics: cic/enmesh.py:34-165 (binning and weights),
+// cic/scatter.py:315-338 and cic/gather.py:452-472 (deposit / interpolation).
+#pragma once
+
+#include "pmb_common.cuh"
+
+namespace pmb {
+
+struct Binned {
+  int cx, cy, cz;
+  float fx, fy, fz;
+};
+
+// Lower CIC corner and fractions of one particle: d = disp / cell in IEEE
+// float, corner = pmid + floor(d) (periodic), fraction = d - floor(d).
+__device__ __forceinline__ Binned bin_particle(const int16_t* __restrict__ pmid, const float d0, const float d1,
+                                               const float d2, int64_t i, Mesh3 m, float cell) {
+  Binned b;
+  float q0 = __fdiv_rn(d0, cell), q1 = __fdiv_rn(d1, cell), q2 = __fdiv_rn(d2, cell);
+  float l0 = floorf(q0), l1 = floorf(q1), l2 = floorf(q2);
+  b.fx = __fsub_rn(q0, l0);
+  b.fy = __fsub_rn(q1, l1);
+  b.fz = __fsub_rn(q2, l2);
+  b.cx = pmod((int)pmid[3 * i + 0] + (int)l0, m.nx);
+  b.cy = pmod((int)pmid[3 * i + 1] + (int)l1, m.ny);
+  b.cz = pmod((int)pmid[3 * i + 2] + (int)l2, m.nz);
+  return b;
+}
+
+constexpr int kMaxSrcRows = 25;  // (RX+1)*(RY+1) with RX, RY <= 4
+
+// Shared-memory bookkeeping of one scatter tile.
+struct ScatterSmem {
+  uint32_t seg_beg[kMaxSrcRows];
+  uint32_t seg_pre[kMaxSrcRows + 1];
+};
+
+// One RX x RY block of output rows at (x0, y0) of mesh m: pulls the
+// particles of the (RX+1) x (RY+1) source rows that reach the block
+// (offs[row] .. offs[row+1] in the sorted records; offs points at this
+// mesh's first row), accumulates val * w in 64-bit fixed point (units of
+// 1/scale) in acc[RX][RY][C][nz], and writes every output cell once:
+// mode 0 the deposit, mode 1 the Poisson source (rho - 1) * src_mul
+// (gravity.py:628-630).  The fixed-point sum is independent of the order in
+// which particles arrive, so the result is bit-deterministic.  Must be
+// called by all threads of the block; leaves the block synchronised.
+template <int C>
+__device__ __forceinline__ void scatter_tile(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm,
+                                             const uint32_t* __restrict__ offs, Mesh3 m, int RX, int RY, int x0,
+                                             int y0, const float* __restrict__ val, float val_const, double scale,
+                                             int mode, float src_mul, float* __restrict__ out, long long* acc,
+                                             ScatterSmem& sm) {
+  const int nz = m.nz;
+  const int nsrc = (RX + 1) * (RY + 1);
+  const int total = RX * RY * C * nz;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) acc[t] = 0;
+  if (threadIdx.x < nsrc) {
+    const int k = threadIdx.x;
+    const int px = pmod(x0 + k / (RY + 1) - 1, m.nx), py = pmod(y0 + k % (RY + 1) - 1, m.ny);
+    const int64_t row = (int64_t)px * m.ny + py;
+    const uint32_t b = offs[row];
+    sm.seg_beg[k] = b;
+    sm.seg_pre[k + 1] = offs[row + 1] - b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (int k = 0; k < nsrc; ++k) {
+      const uint32_t c = sm.seg_pre[k + 1];
+      sm.seg_pre[k] = run;
+      run += c;
+    }
+    sm.seg_pre[nsrc] = run;
+  }
+  __syncthreads();
+  const uint32_t ntot = sm.seg_pre[nsrc];
+  for (uint32_t idx = threadIdx.x; idx < ntot; idx += blockDim.x) {
+    int k = 0;
+    while (idx >= sm.seg_pre[k + 1]) ++k;
+    const int sx = k / (RY + 1) - 1, sy = k % (RY + 1) - 1;
+    const uint32_t i = sm.seg_beg[k] + (idx - sm.seg_pre[k]);
+    const Rec r = rec[i];
+    const int cz = (int)(r.key % (uint32_t)nz);
+    float v[C];
+    if (val != nullptr) {
+      const uint32_t src = perm[i];
+#pragma unroll
+      for (int c = 0; c < C; ++c) v[c] = val[(int64_t)src * C + c];
+    } else {
+#pragma unroll
+      for (int c = 0; c < C; ++c) v[c] = val_const;
+    }
+#pragma unroll
+    for (int bx = 0; bx < 2; ++bx) {
+      const int lx = sx + bx;
+      if (lx < 0 || lx >= RX || x0 + lx >= m.nx) continue;
+      const float wx = axis_weight(r.fx, bx);
+#pragma unroll
+      for (int by = 0; by < 2; ++by) {
+        const int ly = sy + by;
+        if (ly < 0 || ly >= RY || y0 + ly >= m.ny) continue;
+        const float wxy = __fmul_rn(wx, axis_weight(r.fy, by));
+#pragma unroll
+        for (int bz = 0; bz < 2; ++bz) {
+          int z = cz + bz;
+          if (z >= nz) z -= nz;
+          const float w = __fmul_rn(wxy, axis_weight(r.fz, bz));
+#pragma unroll
+          for (int c = 0; c < C; ++c) {
+            const float contrib = __fmul_rn(v[c], w);
+            const long long q = __double2ll_rn((double)contrib * scale);
+            atomicAdd((unsigned long long*)&acc[((lx * RY + ly) * C + c) * nz + z], (unsigned long long)q);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  const double inv = 1.0 / scale;
+  const int64_t cells = m.cells();
+  for (int lx = 0; lx < RX; ++lx) {
+    if (x0 + lx >= m.nx) break;
+    for (int ly = 0; ly < RY; ++ly) {
+      if (y0 + ly >= m.ny) break;
+      const int64_t row_off = ((int64_t)(x0 + lx) * m.ny + (y0 + ly)) * nz;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const long long* a = acc + ((lx * RY + ly) * C + c) * nz;
+        float* o = out + (int64_t)c * cells + row_off;
+        for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+          float rho = (float)((double)a[z] * inv);
+          if (mode == 1) rho = __fmul_rn(__fsub_rn(rho, 1.0f), src_mul);
+          o[z] = rho;
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+struct Corners {
+  int64_t idx[8];
+  float w[8];
+};
+
+// Raveled indices and weights of the eight CIC corners of a sorted record;
+// corner c moves +1 along axis a when bit a of c is set.
+__device__ __forceinline__ void corners_of(const Rec& r, Mesh3 m, Corners& k) {
+  const uint32_t key = r.key;
+  const int cz = (int)(key % (uint32_t)m.nz);
+  const uint32_t rowk = key / (uint32_t)m.nz;
+  const int cy = (int)(rowk % (uint32_t)m.ny);
+  const int cx = (int)(rowk / (uint32_t)m.ny);
+  const int x1 = cx + 1 == m.nx ? 0 : cx + 1;
+  const int y1 = cy + 1 == m.ny ? 0 : cy + 1;
+  const int z1 = cz + 1 == m.nz ? 0 : cz + 1;
+  const float wx[2] = {axis_weight(r.fx, 0), axis_weight(r.fx, 1)};
+  const float wy[2] = {axis_weight(r.fy, 0), axis_weight(r.fy, 1)};
+  const float wz[2] = {axis_weight(r.fz, 0), axis_weight(r.fz, 1)};
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int bx = c & 1, by = (c >> 1) & 1, bz = (c >> 2) & 1;
+    const int x = bx ? x1 : cx, y = by ? y1 : cy, z = bz ? z1 : cz;
+    k.idx[c] = ((int64_t)x * m.ny + y) * m.nz + z;
+    k.w[c] = __fmul_rn(__fmul_rn(wx[bx], wy[by]), wz[bz]);
+  }
+}
+
+// out[src, c] = sum_b mesh_c[i_b] w_b for one sorted record; with vel the
+// half-kick vel += out * kick is applied in place (integrator.py:536).
+template <int C>
+__device__ __forceinline__ void gather_one(const Rec& r, uint32_t src, Mesh3 m, const float* __restrict__ mesh,
+                                           float* __restrict__ out, float* __restrict__ vel, float kick) {
+  Corners k;
+  corners_of(r, m, k);
+  const int64_t cells = m.cells();
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const float* mc = mesh + (int64_t)c * cells;
+    float a = 0.f;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) a = __fadd_rn(a, __fmul_rn(__ldg(mc + k.idx[b]), k.w[b]));
+    out[(int64_t)src * C + c] = a;
+    if (vel != nullptr) vel[(int64_t)src * C + c] = __fadd_rn(vel[(int64_t)src * C + c], __fmul_rn(a, kick));
+  }
+}
+
+}  // namespace pmb

@@ -77,6 +77,33 @@ struct SpecTables {
   const float* mz;
 };
 
+// Table layout [kx ky kz cx cy cz (mx my mz)] (kz, cz, mz of length nz/2+1)
+// as built by the host configuration.
+inline SpecTables spec_tables_from(const float* t, Mesh3 m, int has_masks) {
+  const int nzh = m.nz / 2 + 1;
+  SpecTables s;
+  s.kx = t;
+  s.ky = s.kx + m.nx;
+  s.kz = s.ky + m.ny;
+  s.cx = s.kz + nzh;
+  s.cy = s.cx + m.nx;
+  s.cz = s.cy + m.ny;
+  if (has_masks) {
+    s.mx = s.cz + nzh;
+    s.my = s.mx + m.nx;
+    s.mz = s.my + m.ny;
+  } else {
+    s.mx = s.my = s.mz = nullptr;
+  }
+  return s;
+}
+
+// Floats in one spectral table of mesh m.
+inline int64_t spec_table_len(Mesh3 m, int has_masks) {
+  const int64_t nzh = m.nz / 2 + 1;
+  return (has_masks ? 3 : 2) * ((int64_t)m.nx + m.ny + nzh);
+}
+
 }  // namespace pmb
 
 #define PMB_CUDA_CHECK(expr)                         \

@@ -16,6 +16,7 @@
 
 #include "pmb_common.cuh"
 #include "pmb_kernels.cuh"
+#include "pmb_spectral_device.cuh"
 
 namespace pmb {
 
@@ -113,61 +114,11 @@ int fft_c2r(Mesh3 m, int batch, float2* in, float* out, void* work, cudaStream_t
 // ---------------------------------------------------------------------------
 // Green's function x gradient
 // ---------------------------------------------------------------------------
-// K(k) = mask(k) * G(k) * T(k) with G = -1/k^2 (0 where k^2 == 0).
-// Forward:  phi = (-(S*mask)) / k2 * T ; grad_d = (i c_d) phi,  d = x, y, z.
-// The division is done component-wise in float, as the reference's
-// complex-by-real division (gravity.py:285, :350-352).
-__device__ __forceinline__ float k2_of(const SpecTables& t, int ix, int iy, int iz) {
-  const float kx = t.kx[ix], ky = t.ky[iy], kz = t.kz[iz];
-  return __fadd_rn(__fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky)), __fmul_rn(kz, kz));
-}
-
-__device__ __forceinline__ float transfer_of(const GreenParams& g, const SpecTables& t, int64_t j, int ix, int iy, int iz,
-                                             Mesh3 m) {
-  float T = 1.0f;
-  if (g.transfer != nullptr) T = g.transfer[j];
-  if (g.radial != nullptr) {
-    // integer mode numbers: |n|^2 indexes the radial table exactly
-    const int nx = ix < (m.nx + 1) / 2 ? ix : ix - m.nx;
-    const int ny = iy < (m.ny + 1) / 2 ? iy : iy - m.ny;
-    const long long n2 = (long long)nx * nx + (long long)ny * ny + (long long)iz * iz;
-    T = __fmul_rn(T, n2 < g.radial_len ? g.radial[n2] : 1.0f);
-  }
-  return T;
-}
-
 __global__ void green_gradient_kernel(const float2* __restrict__ src, float2* __restrict__ grad, Mesh3 m,
                                       SpecTables t, GreenParams g) {
-  const int nzh = m.nz / 2 + 1;
   const int64_t total = m.half_cells();
-  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
-    const int iz = (int)(j % nzh);
-    const int64_t r = j / nzh;
-    const int iy = (int)(r % m.ny);
-    const int ix = (int)(r / m.ny);
-    float2 v = src[j];
-    if (t.mx != nullptr) {
-      const float mk = __fmul_rn(__fmul_rn(t.mx[ix], t.my[iy]), t.mz[iz]);
-      v.x = __fmul_rn(v.x, mk);
-      v.y = __fmul_rn(v.y, mk);
-    }
-    const float k2 = k2_of(t, ix, iy, iz);
-    float pr = 0.f, pi = 0.f;
-    if (k2 != 0.f) {
-      pr = __fdiv_rn(-v.x, k2);
-      pi = __fdiv_rn(-v.y, k2);
-      if (g.transfer != nullptr || g.radial != nullptr) {
-        const float T = transfer_of(g, t, j, ix, iy, iz, m);
-        pr = __fmul_rn(pr, T);
-        pi = __fmul_rn(pi, T);
-      }
-    }
-    const float c[3] = {t.cx[ix], t.cy[iy], t.cz[iz]};
-    const float ps = g.post_scale;
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-      grad[(int64_t)d * total + j] = make_float2(__fmul_rn(-__fmul_rn(c[d], pi), ps), __fmul_rn(__fmul_rn(c[d], pr), ps));
-  }
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x)
+    green_gradient_at(src, grad, j, total, m, t, g);
 }
 
 // Adjoint: S_cot = K * sum_d conj(i c_d) A_d.  The force map is a real

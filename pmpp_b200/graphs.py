@@ -7,12 +7,15 @@ captured once into a CUDA graph and replayed: replay removes the per-launch
 host work that dominates small meshes.  Inputs are copied into the graph's
 static buffers before each replay.  cuFFT plans and workspaces are created by
 a warm-up run before capture (plan creation allocates and must not happen
-inside a capture).
+inside a capture).  The graph keeps references to every workspace buffer
+that existed at capture time: a later run that grows a shared workspace slot
+replaces the slot's tensor, and the captured pointers must stay valid.
 """
 from __future__ import annotations
 
 import torch
 
+from . import runtime
 from .nbody import NBodyRun
 from .particles import Particles
 
@@ -35,6 +38,7 @@ class GraphedForward:
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph):
             self.out = self.run.forward(self.static_in, self.a)
+        self._workspaces = runtime.workspace_refs()
 
     def __call__(self, disp=None, vel=None):
         if disp is not None:

@@ -25,6 +25,12 @@ def workspace(nbytes, device, slot="default"):
     return buf
 
 
+def workspace_refs():
+    """References to every current workspace buffer (a captured CUDA graph
+    holds these so that its baked-in pointers outlive slot growth)."""
+    return list(_ws.values())
+
+
 def release_workspaces():
     _ws.clear()
 

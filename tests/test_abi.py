@@ -39,3 +39,35 @@ def test_invalid_arguments_fail_loudly():
     with pytest.raises(_lib.PMBError):
         _lib.call("pmb_sort_rows", None, None, None, 0.0, 10, 0, 4, 4, 1.0, None, None, 0, None)
     assert b"unsupported mesh" in _lib.lib().pmb_last_error()
+
+
+def test_ensemble_create_rejects_bad_layouts_without_device_work():
+    """Descriptions are validated on the host before any CUDA call."""
+    import ctypes
+
+    import numpy as np
+
+    from pmpp_b200 import _lib
+    L = _lib.lib()
+
+    def create(shapes, counts=None, cells=None):
+        n = len(shapes)
+        counts = np.array(counts or [8] * n, np.int64)
+        sh = np.array(shapes, np.int32).reshape(-1)
+        cells = np.array(cells or [1.0] * n, np.float32)
+        vals = np.ones(n, np.float32)
+        muls = np.full(n, 0.45, np.float32)
+        masks = np.zeros(n, np.int32)
+        h = ctypes.c_void_p()
+        p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        return L.pmb_ens_create(n, p(counts), p(sh), p(cells), p(vals), p(muls), p(masks), 4, ctypes.byref(h)), h
+
+    st, h = create([(8, 8, 8), (4, 4, 4), (8, 8, 8)])
+    assert st == -1 and not h.value
+    assert b"consecutive" in L.pmb_last_error()
+    st, _ = create([(8, 8, 8)], cells=[0.0])
+    assert st == -1
+    st, _ = create([(8, 8, 8)], counts=[-1])
+    assert st == -1
+    st, _ = create([(8, 8, 0)])
+    assert st == -1

@@ -1,0 +1,60 @@
+"""Ensembles of uneven simulations against single-simulation runs.
+
+With one member per mesh shape every batched FFT is a batch-1 plan, so an
+ensemble run must equal NBodyRun.forward of every member bit for bit; with
+several members per shape the batched cuFFT plans may round differently, so
+members agree within float32 round-off carried over a few steps.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _members(specs, nsteps=4):
+    import pmpp_b200 as pb
+    from pmpp_b200 import lpt as pl, modes as pm
+    a = np.geomspace(0.1, 1.0, nsteps + 1)
+    confs, coss, ics = [], [], []
+    for k, (n, mesh, box, om) in enumerate(specs):
+        conf = pb.Configuration(box / n, (n, ) * 3, mesh, a_start=0.1, a_custom=a, device="cuda")
+        cos = pb.boltzmann(pb.SimpleLCDM(conf, Omega_m=om))
+        ic = pl.lpt(pm.linear_modes(pm.white_noise_nested(k, conf), cos, conf), cos, conf)
+        confs.append(conf)
+        coss.append(cos)
+        ics.append(ic)
+    return confs, coss, ics
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_one_member_per_shape_is_bitwise_single_runs(graph):
+    import pmpp_b200 as pb
+    from pmpp_b200.ensemble import Ensemble
+    confs, coss, ics = _members([(16, 2, 64.0, 0.3), (24, 2, 100.0, 0.27), (8, 2, 50.0, 0.33), (12, 1, 80.0, 0.31)])
+    ens = Ensemble(confs, coss)
+    outs = ens.forward(ics, graph=graph)
+    for conf, cos, ic, out in zip(confs, coss, ics, outs):
+        ref = pb.NBodyRun(conf, cos).forward(ic)
+        for name in ("disp", "vel", "acc"):
+            assert torch.equal(getattr(out, name), getattr(ref, name)), name
+
+
+def test_batched_shapes_autotune_and_replay():
+    import pmpp_b200 as pb
+    from pmpp_b200.ensemble import Ensemble
+    specs = [(16, 2, 64.0, 0.3), (16, 2, 90.0, 0.26), (8, 2, 40.0, 0.34), (16, 2, 70.0, 0.29), (8, 2, 60.0, 0.3)]
+    confs, coss, ics = _members(specs)
+    ens = Ensemble(confs, coss)
+    first = ens.forward(ics, graph=False)
+    tuning = ens.autotune(reps=2)
+    assert set(tuning["tiles"]) == {str((32, 32, 32)), str((16, 16, 16))}
+    again = ens.forward(ics, graph=True)
+    replay = ens.forward(ics, graph=True)
+    for a, b, c in zip(first, again, replay):
+        # tile and launch shapes change no arithmetic; graph replays are deterministic
+        assert torch.equal(a.disp, b.disp) and torch.equal(b.disp, c.disp)
+    for conf, cos, ic, out in zip(confs, coss, ics, first):
+        ref = pb.NBodyRun(conf, cos).forward(ic)
+        scale = float(ref.disp.abs().max())
+        assert float((out.disp - ref.disp).abs().max()) < 1e-4 * scale
