@@ -64,20 +64,24 @@ int64_t pmb_sort_by_cell_scratch_bytes(int64_t n, int nx, int ny, int nz);
 /* ---------------- CIC on sorted particles --------------------------------
  * Deterministic scatter (cic/scatter.py:315-338, cic/pallas.py:268-303):
  * out[c] = sum_p val[p,c] * w_p.  val (n,C) or NULL for the constant
- * val_const.  mode 0 writes the sum; mode 1 writes (sum - 1) * src_mul (the
- * Poisson source of nbody/gravity.py:628-630).  scratch: 16 bytes. */
-int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* val, float val_const,
-                     int mode, float src_mul, float* out, void* scratch16, void* stream);
+ * val_const; val is in particle order, or in sorted order when val_sorted
+ * (as pmb_interp_grad_rows writes it to u_sorted).  mode 0 writes the sum;
+ * mode 1 writes (sum - 1) * src_mul (the Poisson source of
+ * nbody/gravity.py:628-630).  The sum is exact in 64-bit fixed point, so the
+ * result does not depend on particle order.  scratch: 16 bytes. */
+int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* val, int val_sorted,
+                     float val_const, int mode, float src_mul, float* out, void* scratch16, void* stream);
 /* Gather (cic/gather.py:452-472, cic/pallas.py:305-318): out[p,c]; with
  * vel != NULL also vel += out * kick (nbody/integrator.py:536). */
 int pmb_gather_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh, float* out,
                     float* vel, float kick, void* stream);
 /* Position term of the CIC adjoints (cic/gather.py:495-502,
  * cic/scatter.py:366-373): disp_cot[p] (+)= sum_b (sum_c u[p,c] mesh_c[i_b])
- * grad w_b / cell; optional wsum[p,c] = sum_b mesh_c[i_b] w_b. */
+ * grad w_b / cell; optional wsum[p,c] = sum_b mesh_c[i_b] w_b and
+ * u_sorted (n,C) = u in sorted order (input of a val_sorted scatter). */
 int pmb_interp_grad_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh,
                          const float* u, float u_const, float cell, int accumulate, float* disp_cot, float* wsum,
-                         void* stream);
+                         float* u_sorted, void* stream);
 
 /* ---------------- spectral ------------------------------------------------
  * 3-D R2C / C2R (numpy convention: forward unnormalised, the inverse is NOT

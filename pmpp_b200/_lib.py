@@ -21,10 +21,10 @@ _SIGS = {
     "pmb_sort_rows": (c_int, [c_p, c_p, c_p, c_f, c_i64, c_int, c_int, c_int, c_f, c_p, c_p, c_i64, c_p]),
     "pmb_sort_by_cell": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_f, c_p, c_p, c_p, c_i64, c_p]),
     "pmb_sort_by_cell_scratch_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
-    "pmb_scatter_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_f, c_int, c_f, c_p, c_p, c_p]),
+    "pmb_scatter_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_int, c_f, c_int, c_f, c_p, c_p, c_p]),
     "pmb_gather_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_f, c_p]),
     "pmb_interp_grad_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_p, c_f, c_f, c_int, c_p, c_p,
-                                     c_p]),
+                                     c_p, c_p]),
     "pmb_fft_work_bytes": (c_i64, [c_int, c_int, c_int, c_int]),
     "pmb_rfft3": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
     "pmb_irfft3": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),

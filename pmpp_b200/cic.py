@@ -37,7 +37,9 @@ class SortedParticles:
         call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), self.n, nx, ny, nz,
              float(conf.cell_size), self.buf.data_ptr(), scratch.data_ptr(), scratch.numel(), stream_handle(dev))
 
-    def scatter(self, val=None, val_const=None, channels=1, mode=0, src_mul=1.0, out=None):
+    def scatter(self, val=None, val_const=None, channels=1, mode=0, src_mul=1.0, out=None, val_sorted=False):
+        """Deposit; val (n, channels) is in particle order, or in sorted order
+        with val_sorted (as written by interp_grad's u_sorted)."""
         nx, ny, nz = self.shape
         dev = self.buf.device
         if out is None:
@@ -45,8 +47,8 @@ class SortedParticles:
         s16 = workspace(16, dev, "scale16")
         vc = float(self.conf.mesh_size / self.conf.ptcl_num) if (val is None and val_const is None) else (
             0.0 if val_const is None else float(val_const))
-        call("pmb_scatter_rows", self.buf.data_ptr(), self.n, nx, ny, nz, channels, ptr(val), vc, mode,
-             float(src_mul), out.data_ptr(), s16.data_ptr(), stream_handle(dev))
+        call("pmb_scatter_rows", self.buf.data_ptr(), self.n, nx, ny, nz, channels, ptr(val), int(val_sorted), vc,
+             mode, float(src_mul), out.data_ptr(), s16.data_ptr(), stream_handle(dev))
         return out
 
     def gather(self, mesh_planar, out=None, vel=None, kick=0.0):
@@ -58,7 +60,7 @@ class SortedParticles:
              ptr(vel), float(kick), stream_handle(mesh_planar.device))
         return out
 
-    def interp_grad(self, mesh_planar, u=None, u_const=0.0, disp_cot=None, accumulate=False, wsum=False):
+    def interp_grad(self, mesh_planar, u=None, u_const=0.0, disp_cot=None, accumulate=False, wsum=False, u_sorted=None):
         nx, ny, nz = self.shape
         C = mesh_planar.shape[0]
         dev = mesh_planar.device
@@ -67,7 +69,7 @@ class SortedParticles:
             accumulate = False
         ws = torch.empty((self.n, C), dtype=torch.float32, device=dev) if wsum else None
         call("pmb_interp_grad_rows", self.buf.data_ptr(), self.n, nx, ny, nz, C, mesh_planar.data_ptr(), ptr(u),
-             float(u_const), float(self.conf.cell_size), int(accumulate), disp_cot.data_ptr(), ptr(ws),
+             float(u_const), float(self.conf.cell_size), int(accumulate), disp_cot.data_ptr(), ptr(ws), ptr(u_sorted),
              stream_handle(dev))
         return disp_cot, ws
 

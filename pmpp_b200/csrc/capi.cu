@@ -94,7 +94,7 @@ struct Carve {
 
 extern "C" {
 
-int pmb_abi_version(void) { return 1; }
+int pmb_abi_version(void) { return 2; }
 
 const char* pmb_last_error(void) { return g_last_error.c_str(); }
 
@@ -113,8 +113,8 @@ int pmb_sort_rows(const int16_t* pmid, float* disp, const float* vel, float drif
   return bin_particles(pmid, disp, vel, drift, n, m, cell, v.rec, v.perm, v.offs, scratch, S(stream));
 }
 
-int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* val, float val_const,
-                     int mode, float src_mul, float* out, void* scratch16, void* stream) {
+int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* val, int val_sorted,
+                     float val_const, int mode, float src_mul, float* out, void* scratch16, void* stream) {
   Mesh3 m{nx, ny, nz};
   PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_scatter_rows: unsupported mesh shape");
   PMB_REQUIRE(C >= 1 && C <= 4, "pmb_scatter_rows: 1..4 channels supported");
@@ -129,7 +129,8 @@ int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int 
     PMB_REQUIRE(a < INFINITY, "pmb_scatter_rows: non-finite value");
     PMB_TRY(set_double(scale, a > 0.f ? fixed_point_pow2(n) / (double)a : 1.0, S(stream)));
   }
-  return scatter_sorted(v.rec, v.perm, v.offs, m, C, val, val_const, scale, mode, src_mul, out, S(stream));
+  return scatter_sorted(v.rec, v.perm, v.offs, m, C, val, val_sorted, val_const, scale, mode, src_mul, out,
+                        S(stream));
 }
 
 int pmb_gather_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh, float* out,
@@ -143,12 +144,13 @@ int pmb_gather_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C
 
 int pmb_interp_grad_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh,
                          const float* u, float u_const, float cell, int accumulate, float* disp_cot, float* wsum,
-                         void* stream) {
+                         float* u_sorted, void* stream) {
   Mesh3 m{nx, ny, nz};
   PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_interp_grad_rows: unsupported mesh shape");
   PMB_REQUIRE(C >= 1 && C <= 4, "pmb_interp_grad_rows: 1..4 channels supported");
   SortedView v = sorted_view((void*)sorted, n);
-  return interp_grad_sorted(v.rec, v.perm, n, m, C, mesh, u, u_const, cell, accumulate, disp_cot, wsum, S(stream));
+  return interp_grad_sorted(v.rec, v.perm, n, m, C, mesh, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted,
+                            S(stream));
 }
 
 int64_t pmb_fft_work_bytes(int nx, int ny, int nz, int batch) { return fft_work_bytes(Mesh3{nx, ny, nz}, batch); }
@@ -229,7 +231,7 @@ int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float dr
   }
   cudaStream_t s = S(stream);
   PMB_TRY(pmb_sort_rows(pmid, disp, drift_vel, drift, n, nx, ny, nz, cell, sorted, bins, bin_scratch_bytes(n, m), stream));
-  PMB_TRY(pmb_scatter_rows(sorted, n, nx, ny, nz, 1, nullptr, val_const, 1, src_mul, src, scale16, stream));
+  PMB_TRY(pmb_scatter_rows(sorted, n, nx, ny, nz, 1, nullptr, 0, val_const, 1, src_mul, src, scale16, stream));
   PMB_TRY(fft_r2c(m, 1, src, src_hat, work, s));
   const float inv_m = (float)(1.0 / (double)m.cells());
   PMB_TRY(green_gradient(src_hat, grad_hat, m, make_tables(tables, m, has_masks),
@@ -240,11 +242,13 @@ int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float dr
 }
 
 static int64_t force_vjp_layout(int64_t n, Mesh3 m, void* ws, int64_t cap, void** sorted, void** bins, void** scale16,
-                                float** mesh_cot, float2** spec3, float2** src_hat, float** src_cot, void** work) {
+                                float** cot_sorted, float** mesh_cot, float2** spec3, float2** src_hat, float** src_cot,
+                                void** work) {
   Carve c(ws, cap);
   *sorted = c.take(sorted_bytes(n, m));
   *bins = c.take(bin_scratch_bytes(n, m));
   *scale16 = c.take(16);
+  *cot_sorted = (float*)c.take(12 * n);
   *mesh_cot = (float*)c.take(12 * m.cells());
   *spec3 = (float2*)c.take(24 * m.half_cells());
   *src_hat = (float2*)c.take(8 * m.half_cells());
@@ -258,9 +262,9 @@ static int64_t force_vjp_layout(int64_t n, Mesh3 m, void* ws, int64_t cap, void*
 
 int64_t pmb_force_vjp_workspace_bytes(int64_t n, int nx, int ny, int nz) {
   void *a, *b, *c, *w;
-  float *mc, *sc;
+  float *cs, *mc, *sc;
   float2 *s3, *sh;
-  return force_vjp_layout(n, Mesh3{nx, ny, nz}, nullptr, 0, &a, &b, &c, &mc, &s3, &sh, &sc, &w);
+  return force_vjp_layout(n, Mesh3{nx, ny, nz}, nullptr, 0, &a, &b, &c, &cs, &mc, &s3, &sh, &sc, &w);
 }
 
 int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int ny, int nz, float cell,
@@ -272,10 +276,10 @@ int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int
   PMB_REQUIRE(n >= 0 && n < 4294967295ll, "pmb_force_vjp: particle count out of range");
   PMB_REQUIRE(cell > 0.f, "pmb_force_vjp: cell size must be positive");
   void *sorted, *bins, *scale16, *work;
-  float *mesh_cot, *src_cot;
+  float *cot_sorted, *mesh_cot, *src_cot;
   float2 *spec3, *src_hat;
-  int64_t need = force_vjp_layout(n, m, workspace, workspace_bytes, &sorted, &bins, &scale16, &mesh_cot, &spec3,
-                                  &src_hat, &src_cot, &work);
+  int64_t need = force_vjp_layout(n, m, workspace, workspace_bytes, &sorted, &bins, &scale16, &cot_sorted, &mesh_cot,
+                                  &spec3, &src_hat, &src_cot, &work);
   PMB_REQUIRE(need >= 0, "pmb_force_vjp: cuFFT plan creation failed");
   if (need > workspace_bytes) {
     set_last_error("pmb_force_vjp: workspace too small");
@@ -286,8 +290,9 @@ int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int
                         stream));
   SortedView v = sorted_view(sorted, n);
   // gather adjoint: position term and the 3-channel scatter of acc_cot
-  PMB_TRY(interp_grad_sorted(v.rec, v.perm, n, m, 3, force_meshes, acc_cot, 0.f, cell, 1, disp_cot, nullptr, s));
-  PMB_TRY(pmb_scatter_rows(sorted, n, nx, ny, nz, 3, acc_cot, 0.f, 0, 1.f, mesh_cot, scale16, stream));
+  PMB_TRY(interp_grad_sorted(v.rec, v.perm, n, m, 3, force_meshes, acc_cot, 0.f, cell, 1, disp_cot, nullptr,
+                             cot_sorted, s));
+  PMB_TRY(pmb_scatter_rows(sorted, n, nx, ny, nz, 3, cot_sorted, 1, 0.f, 0, 1.f, mesh_cot, scale16, stream));
   // transposes of the C2R, gradient, Green and R2C stages
   PMB_TRY(fft_r2c(m, 3, mesh_cot, spec3, work, s));
   const float post = (float)((double)src_mul / (double)m.cells());
@@ -295,7 +300,8 @@ int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int
                                  make_green(green_kernel, transfer, radial, radial_len, post), s));
   PMB_TRY(fft_c2r(m, 1, src_hat, src_cot, work, s));
   // scatter adjoint of the density (constant particle value)
-  return interp_grad_sorted(v.rec, v.perm, n, m, 1, src_cot, nullptr, val_const, cell, 1, disp_cot, nullptr, s);
+  return interp_grad_sorted(v.rec, v.perm, n, m, 1, src_cot, nullptr, val_const, cell, 1, disp_cot, nullptr, nullptr,
+                            s);
 }
 
 // ---------------------------------------------------------------------------

@@ -256,33 +256,35 @@ int compute_scale(const float* val, int64_t count, int64_t n, double* scale_dev,
 template <int C>
 __global__ void __launch_bounds__(256) scatter_pull_kernel(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm,
                                                            const uint32_t* __restrict__ offs, Mesh3 m, int RX, int RY,
-                                                           const float* __restrict__ val, float val_const,
-                                                           const double* __restrict__ scale_dev, int mode,
-                                                           float src_mul, float* __restrict__ out) {
-  extern __shared__ long long acc[];  // [RX][RY][C][nz]
+                                                           const float* __restrict__ val, int val_sorted,
+                                                           float val_const, const double* __restrict__ scale_dev,
+                                                           int mode, float src_mul, float* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned int acc_smem[];  // ScatterSmem::acc_bytes(RX, RY, C, nz)
   __shared__ ScatterSmem sm;
   const int nby = (m.ny + RY - 1) / RY;
   const int x0 = (int)(blockIdx.x / nby) * RX;
   const int y0 = (int)(blockIdx.x % nby) * RY;
-  scatter_tile<C>(rec, perm, offs, m, RX, RY, x0, y0, val, val_const, *scale_dev, mode, src_mul, out, acc, sm);
+  scatter_tile<C>(rec, perm, offs, m, RX, RY, x0, y0, val, val_sorted, val_const, *scale_dev, mode, src_mul, out,
+                  acc_smem, sm);
 }
 
 void scatter_block_shape(Mesh3 m, int C, int* RX, int* RY) {
-  // Keep the fixed-point accumulator at <= 96 KB so two CTAs fit per SM.
-  const int64_t budget = 96 * 1024;
-  int rx = 2, ry = 4;
-  while ((int64_t)rx * ry * C * m.nz * 8 > budget && (rx > 1 || ry > 1)) {
-    if (ry > rx) ry /= 2; else rx /= 2;
-  }
+  // Largest of 2x2, 1x2, 1x1 output rows whose accumulator fits in 100 KB
+  // (two or more CTAs per SM).
+  const int64_t budget = 100 * 1024;
+  int rx = 2, ry = 2;
+  if (ScatterSmem::acc_bytes(rx, ry, C, m.nz) > budget) rx = 1;
+  if (ScatterSmem::acc_bytes(rx, ry, C, m.nz) > budget) ry = 1;
   *RX = rx < m.nx ? rx : m.nx;
   *RY = ry < m.ny ? ry : m.ny;
 }
 
 int scatter_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, Mesh3 m, int C, const float* val,
-                   float val_const, const double* scale_dev, int mode, float src_mul, float* out, cudaStream_t s) {
+                   int val_sorted, float val_const, const double* scale_dev, int mode, float src_mul, float* out,
+                   cudaStream_t s) {
   int RX, RY;
   scatter_block_shape(m, C, &RX, &RY);
-  const size_t smem = (size_t)RX * RY * C * m.nz * sizeof(long long);
+  const int64_t smem = ScatterSmem::acc_bytes(RX, RY, C, m.nz);
   if (smem > 200 * 1024) return kUnsupported;
   const int nbx = (m.nx + RX - 1) / RX, nby = (m.ny + RY - 1) / RY;
   const unsigned grid = (unsigned)((int64_t)nbx * nby);
@@ -294,8 +296,8 @@ int scatter_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, M
                                           200 * 1024));                                                         \
       attr_##CC = true;                                                                                          \
     }                                                                                                            \
-    scatter_pull_kernel<CC><<<grid, 256, smem, s>>>(rec, perm, offs, m, RX, RY, val, val_const, scale_dev, mode, \
-                                                     src_mul, out);                                             \
+    scatter_pull_kernel<CC><<<grid, 256, (size_t)smem, s>>>(rec, perm, offs, m, RX, RY, val, val_sorted,         \
+                                                             val_const, scale_dev, mode, src_mul, out);         \
   } while (0)
   switch (C) {
     case 1: PMB_LAUNCH_SCATTER(1); break;
@@ -346,14 +348,14 @@ int gather_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int 
 //   disp_cot[src] (+)= (sum_b inner_b * grad w_b) / cell
 // This is gather.py:495-502 (u = val_cot) and scatter.py:366-370 (u = val).
 // Optionally also emits wsum[src, c] = sum_b mesh_c[i_b] w_b (the scatter
-// adjoint's val cotangent, scatter.py:372-373) and accumulates
-// dot = sum_src sum_c u_c * extra[src, c] in FP64 (used for cosmology
-// cotangents).
+// adjoint's val cotangent, scatter.py:372-373) and u_sorted[i, c] =
+// u[src, c] (the weights in sorted order, so a following scatter of u reads
+// them coalesced instead of through the permutation).
 template <int C>
 __global__ void interp_grad_kernel(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm, int64_t n, Mesh3 m,
                                    const float* __restrict__ mesh, const float* __restrict__ u, float u_const,
                                    float cell, int accumulate, float* __restrict__ disp_cot,
-                                   float* __restrict__ wsum) {
+                                   float* __restrict__ wsum, float* __restrict__ u_sorted) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Rec r = rec[i];
@@ -378,6 +380,10 @@ __global__ void interp_grad_kernel(const Rec* __restrict__ rec, const uint32_t* 
   float uu[C];
 #pragma unroll
   for (int c = 0; c < C; ++c) uu[c] = u ? u[(int64_t)src * C + c] : u_const;
+  if (u_sorted != nullptr) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) u_sorted[i * C + c] = uu[c];
+  }
   const int64_t cells = m.cells();
   float g0 = 0.f, g1 = 0.f, g2 = 0.f;
   float ws[C];
@@ -424,15 +430,15 @@ __global__ void interp_grad_kernel(const Rec* __restrict__ rec, const uint32_t* 
 
 int interp_grad_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int C, const float* mesh,
                        const float* u, float u_const, float cell, int accumulate, float* disp_cot, float* wsum,
-                       cudaStream_t s) {
+                       float* u_sorted, cudaStream_t s) {
   if (n == 0) return kOk;
   const int th = 256;
   const unsigned g = (unsigned)((n + th - 1) / th);
   switch (C) {
-    case 1: interp_grad_kernel<1><<<g, th, 0, s>>>(rec, perm, n, m, mesh, u, u_const, cell, accumulate, disp_cot, wsum); break;
-    case 2: interp_grad_kernel<2><<<g, th, 0, s>>>(rec, perm, n, m, mesh, u, u_const, cell, accumulate, disp_cot, wsum); break;
-    case 3: interp_grad_kernel<3><<<g, th, 0, s>>>(rec, perm, n, m, mesh, u, u_const, cell, accumulate, disp_cot, wsum); break;
-    case 4: interp_grad_kernel<4><<<g, th, 0, s>>>(rec, perm, n, m, mesh, u, u_const, cell, accumulate, disp_cot, wsum); break;
+    case 1: interp_grad_kernel<1><<<g, th, 0, s>>>(rec, perm, n, m, mesh, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted); break;
+    case 2: interp_grad_kernel<2><<<g, th, 0, s>>>(rec, perm, n, m, mesh, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted); break;
+    case 3: interp_grad_kernel<3><<<g, th, 0, s>>>(rec, perm, n, m, mesh, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted); break;
+    case 4: interp_grad_kernel<4><<<g, th, 0, s>>>(rec, perm, n, m, mesh, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted); break;
     default: return kUnsupported;
   }
   PMB_CUDA_CHECK(cudaGetLastError());

@@ -165,7 +165,7 @@ __global__ void ens_bin_place_kernel(EnsDev d) {
 // Persistent deterministic scatter: CTAs pull scatter tiles from the work
 // counter until every tile of every simulation is written.
 __global__ void __launch_bounds__(256) ens_scatter_kernel(EnsDev d) {
-  extern __shared__ long long acc[];
+  extern __shared__ __align__(16) unsigned int acc_smem[];
   __shared__ ScatterSmem sm;
   __shared__ long long item_sh;
   for (;;) {
@@ -180,8 +180,8 @@ __global__ void __launch_bounds__(256) ens_scatter_kernel(EnsDev d) {
     const int64_t local = item - d.tile_start[s];
     const int nby = (m.ny + ry - 1) / ry;
     const int x0 = (int)(local / nby) * rx, y0 = (int)(local % nby) * ry;
-    scatter_tile<1>(d.rec, d.perm, d.offs + sim.row0, m, rx, ry, x0, y0, nullptr, sim.val, sim.scale, 1, sim.src_mul,
-                    sim.rho, acc, sm);
+    scatter_tile<1>(d.rec, d.perm, d.offs + sim.row0, m, rx, ry, x0, y0, nullptr, 0, sim.val, sim.scale, 1,
+                    sim.src_mul, sim.rho, acc_smem, sm);
   }
 }
 
@@ -287,7 +287,7 @@ void recount_tiles(Ensemble* e) {
 size_t scatter_smem_of(const Ensemble* e) {
   size_t mx = 0;
   for (const EnsSim& s : e->sims) {
-    const size_t b = (size_t)s.rx * s.ry * s.m.nz * sizeof(long long);
+    const size_t b = (size_t)ScatterSmem::acc_bytes(s.rx, s.ry, 1, s.m.nz);
     if (b > mx) mx = b;
   }
   return mx;
@@ -589,7 +589,7 @@ int pmb_ens_set_tiles(void* handle, const int32_t* rx, const int32_t* ry) {
   for (int i = 0; i < e->nsims; ++i) {
     const EnsSim& q = e->sims[i];
     ENS_REQUIRE(rx[i] >= 1 && ry[i] >= 1 && (rx[i] + 1) * (ry[i] + 1) <= kMaxSrcRows && rx[i] <= q.m.nx &&
-                    ry[i] <= q.m.ny && (int64_t)rx[i] * ry[i] * q.m.nz * 8 <= 200 * 1024,
+                    ry[i] <= q.m.ny && ScatterSmem::acc_bytes(rx[i], ry[i], 1, q.m.nz) <= 200 * 1024,
                 "pmb_ens_set_tiles: tile shape out of range");
   }
   for (int i = 0; i < e->nsims; ++i) {

@@ -110,5 +110,5 @@ extern "C" int pmb_scatter_density_noalloc(const int16_t* pmid, const float* dis
   }
   st = set_double(scale, a > 0.f ? fixed_point_pow2(n) / (double)a : 1.0, s);
   if (st != kOk) return st;
-  return scatter_sorted(rec, perm, offs, m, 1, nullptr, val, scale, 0, 1.f, out, s);
+  return scatter_sorted(rec, perm, offs, m, 1, nullptr, 0, val, scale, 0, 1.f, out, s);
 }

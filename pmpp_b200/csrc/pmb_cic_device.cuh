@@ -36,27 +36,40 @@ constexpr int kMaxSrcRows = 25;  // (RX+1)*(RY+1) with RX, RY <= 4
 struct ScatterSmem {
   uint32_t seg_beg[kMaxSrcRows];
   uint32_t seg_pre[kMaxSrcRows + 1];
+  // dynamic accumulator bytes of an RX x RY block with C channels
+  static constexpr int64_t acc_bytes(int RX, int RY, int C, int nz) { return (int64_t)12 * RX * RY * C * nz; }
 };
 
 // One RX x RY block of output rows at (x0, y0) of mesh m: pulls the
 // particles of the (RX+1) x (RY+1) source rows that reach the block
 // (offs[row] .. offs[row+1] in the sorted records; offs points at this
-// mesh's first row), accumulates val * w in 64-bit fixed point (units of
-// 1/scale) in acc[RX][RY][C][nz], and writes every output cell once:
+// mesh's first row), accumulates val * w as 64-bit fixed-point integers
+// (units of 1/scale) in shared memory, and writes every output cell once:
 // mode 0 the deposit, mode 1 the Poisson source (rho - 1) * src_mul
-// (gravity.py:628-630).  The fixed-point sum is independent of the order in
-// which particles arrive, so the result is bit-deterministic.  Must be
-// called by all threads of the block; leaves the block synchronised.
+// (gravity.py:628-630).  val (C values per particle, may be null for the
+// constant val_const) is indexed by source particle (perm) or, with
+// val_sorted, by sorted position.
+//
+// Integer sums do not depend on the order in which particles arrive, so the
+// result is bit-deterministic.  Accumulator: 12 bytes per output cell-channel
+// (ScatterSmem::acc_bytes).  When the block's source segments hold fewer than
+// 2^16 particles, each 64-bit contribution q = a*2^32 + b*2^16 + c (a signed,
+// 0 <= b, c < 2^16) is added as three 32-bit shared atomics on separate
+// planes: the b and c sums stay below 2^32 and the a sum below 2^31, so the
+// recombined total is exactly the 64-bit sum, while 32-bit atomics tolerate
+// many particles per cell (clustering) far better than 64-bit ones.  Larger
+// blocks use 64-bit atomics on the first 8 bytes per cell.  Must be called by
+// all threads of the block; leaves the block synchronised.
 template <int C>
 __device__ __forceinline__ void scatter_tile(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm,
                                              const uint32_t* __restrict__ offs, Mesh3 m, int RX, int RY, int x0,
-                                             int y0, const float* __restrict__ val, float val_const, double scale,
-                                             int mode, float src_mul, float* __restrict__ out, long long* acc,
-                                             ScatterSmem& sm) {
+                                             int y0, const float* __restrict__ val, int val_sorted, float val_const,
+                                             double scale, int mode, float src_mul, float* __restrict__ out,
+                                             unsigned int* acc, ScatterSmem& sm) {
   const int nz = m.nz;
   const int nsrc = (RX + 1) * (RY + 1);
-  const int total = RX * RY * C * nz;
-  for (int t = threadIdx.x; t < total; t += blockDim.x) acc[t] = 0;
+  const int cells = RX * RY * C * nz;
+  for (int t = threadIdx.x; t < 3 * cells; t += blockDim.x) acc[t] = 0u;
   if (threadIdx.x < nsrc) {
     const int k = threadIdx.x;
     const int px = pmod(x0 + k / (RY + 1) - 1, m.nx), py = pmod(y0 + k % (RY + 1) - 1, m.ny);
@@ -77,6 +90,8 @@ __device__ __forceinline__ void scatter_tile(const Rec* __restrict__ rec, const 
   }
   __syncthreads();
   const uint32_t ntot = sm.seg_pre[nsrc];
+  const bool split = ntot < 65536u;
+  unsigned long long* acc64 = reinterpret_cast<unsigned long long*>(acc);
   for (uint32_t idx = threadIdx.x; idx < ntot; idx += blockDim.x) {
     int k = 0;
     while (idx >= sm.seg_pre[k + 1]) ++k;
@@ -86,9 +101,9 @@ __device__ __forceinline__ void scatter_tile(const Rec* __restrict__ rec, const 
     const int cz = (int)(r.key % (uint32_t)nz);
     float v[C];
     if (val != nullptr) {
-      const uint32_t src = perm[i];
+      const int64_t src = val_sorted ? (int64_t)i : (int64_t)perm[i];
 #pragma unroll
-      for (int c = 0; c < C; ++c) v[c] = val[(int64_t)src * C + c];
+      for (int c = 0; c < C; ++c) v[c] = val[src * C + c];
     } else {
 #pragma unroll
       for (int c = 0; c < C; ++c) v[c] = val_const;
@@ -112,7 +127,14 @@ __device__ __forceinline__ void scatter_tile(const Rec* __restrict__ rec, const 
           for (int c = 0; c < C; ++c) {
             const float contrib = __fmul_rn(v[c], w);
             const long long q = __double2ll_rn((double)contrib * scale);
-            atomicAdd((unsigned long long*)&acc[((lx * RY + ly) * C + c) * nz + z], (unsigned long long)q);
+            const int a = ((lx * RY + ly) * C + c) * nz + z;
+            if (split) {
+              atomicAdd(&acc[a], (unsigned int)(q >> 32));
+              atomicAdd(&acc[cells + a], (unsigned int)((q >> 16) & 0xFFFF));
+              atomicAdd(&acc[2 * cells + a], (unsigned int)(q & 0xFFFF));
+            } else {
+              atomicAdd(&acc64[a], (unsigned long long)q);
+            }
           }
         }
       }
@@ -120,7 +142,7 @@ __device__ __forceinline__ void scatter_tile(const Rec* __restrict__ rec, const 
   }
   __syncthreads();
   const double inv = 1.0 / scale;
-  const int64_t cells = m.cells();
+  const int64_t mcells = m.cells();
   for (int lx = 0; lx < RX; ++lx) {
     if (x0 + lx >= m.nx) break;
     for (int ly = 0; ly < RY; ++ly) {
@@ -128,10 +150,15 @@ __device__ __forceinline__ void scatter_tile(const Rec* __restrict__ rec, const 
       const int64_t row_off = ((int64_t)(x0 + lx) * m.ny + (y0 + ly)) * nz;
 #pragma unroll
       for (int c = 0; c < C; ++c) {
-        const long long* a = acc + ((lx * RY + ly) * C + c) * nz;
-        float* o = out + (int64_t)c * cells + row_off;
+        const int a0 = ((lx * RY + ly) * C + c) * nz;
+        float* o = out + (int64_t)c * mcells + row_off;
         for (int z = threadIdx.x; z < nz; z += blockDim.x) {
-          float rho = (float)((double)a[z] * inv);
+          const int a = a0 + z;
+          const long long sum = split ? (long long)(((unsigned long long)acc[a] << 32) +
+                                                    ((unsigned long long)acc[cells + a] << 16) +
+                                                    (unsigned long long)acc[2 * cells + a])
+                                      : (long long)acc64[a];
+          float rho = (float)((double)sum * inv);
           if (mode == 1) rho = __fmul_rn(__fsub_rn(rho, 1.0f), src_mul);
           o[z] = rho;
         }

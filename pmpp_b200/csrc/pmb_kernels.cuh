@@ -16,12 +16,13 @@ int bin_particles(const int16_t* pmid, float* disp, const float* vel, float drif
 double fixed_point_pow2(int64_t n);
 int compute_scale(const float* val, int64_t count, int64_t n, double* scale_dev, unsigned int* tmp, cudaStream_t s);
 int scatter_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, Mesh3 m, int C, const float* val,
-                   float val_const, const double* scale_dev, int mode, float src_mul, float* out, cudaStream_t s);
+                   int val_sorted, float val_const, const double* scale_dev, int mode, float src_mul, float* out,
+                   cudaStream_t s);
 int gather_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int C, const float* mesh, float* out,
                   float* vel, float kick, cudaStream_t s);
 int interp_grad_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int C, const float* mesh,
                        const float* u, float u_const, float cell, int accumulate, float* disp_cot, float* wsum,
-                       cudaStream_t s);
+                       float* u_sorted, cudaStream_t s);
 
 // spectral.cu
 int fft_r2c(Mesh3 m, int batch, float* in, float2* out, void* work, cudaStream_t s);

@@ -237,7 +237,7 @@ class Ensemble:
         for ms in shapes:
             best = None
             for rx, ry in TILE_CANDIDATES:
-                if rx > ms[0] or ry > ms[1] or rx * ry * ms[2] * 8 > 200 * 1024:
+                if rx > ms[0] or ry > ms[1] or rx * ry * ms[2] * 12 > 200 * 1024:
                     continue
                 trial = dict(tiles)
                 trial[str(ms)] = (rx, ry)

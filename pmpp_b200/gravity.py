@@ -67,8 +67,8 @@ def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F
     call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
          float(conf.cell_size), sorted_buf.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
     t = timer.mark("sort", t)
-    call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 1, None, float(conf.mesh_size / conf.ptcl_num), 1,
-         1.5 * _om32(omega_m), real3.data_ptr(), s16.data_ptr(), s)
+    call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 1, None, 0, float(conf.mesh_size / conf.ptcl_num),
+         1, 1.5 * _om32(omega_m), real3.data_ptr(), s16.data_ptr(), s)
     t = timer.mark("scatter", t)
     call("pmb_rfft3", nx, ny, nz, 1, real3.data_ptr(), spec1.data_ptr(), work.data_ptr(), s)
     t = timer.mark("fft_r2c", t)
@@ -99,10 +99,11 @@ def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, r
     call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), None, 0.0, n, nx, ny, nz, float(conf.cell_size),
          sorted_buf.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
     t = timer.mark("sort", t)
+    cot_sorted = workspace(12 * n, dev, "st_cot_sorted")
     call("pmb_interp_grad_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc_cot.data_ptr(), 0.0,
-         float(conf.cell_size), 1, disp_cot.data_ptr(), None, s)
+         float(conf.cell_size), 1, disp_cot.data_ptr(), None, cot_sorted.data_ptr(), s)
     t = timer.mark("gather_adjoint", t)
-    call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, acc_cot.data_ptr(), 0.0, 0, 1.0,
+    call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, cot_sorted.data_ptr(), 1, 0.0, 0, 1.0,
          real3.data_ptr(), s16.data_ptr(), s)
     t = timer.mark("scatter3", t)
     call("pmb_rfft3", nx, ny, nz, 3, real3.data_ptr(), spec3.data_ptr(), work.data_ptr(), s)
@@ -117,7 +118,7 @@ def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, r
     call("pmb_irfft3", nx, ny, nz, 1, spec1.data_ptr(), real3.data_ptr(), work.data_ptr(), s)
     t = timer.mark("fft_c2r", t)
     call("pmb_interp_grad_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 1, real3.data_ptr(), None,
-         float(conf.mesh_size / conf.ptcl_num), float(conf.cell_size), 1, disp_cot.data_ptr(), None, s)
+         float(conf.mesh_size / conf.ptcl_num), float(conf.cell_size), 1, disp_cot.data_ptr(), None, None, s)
     timer.mark("scatter_adjoint", t)
 
 

@@ -11,7 +11,8 @@ Timed per stage with CUDA events on the launching stream (mean over
 ``reps`` launches after warm-up): row sort, density scatter, R2C, Green x
 gradient, 3 x C2R, 3-channel gather, and the adjoints -- scatter VJP (position
 term against an N(0,1) mesh cotangent), gather VJP (position term + 3-channel
-scatter against N(0,1) particle cotangents, seed 2), and the spectral adjoint
+scatter against N(0,1) particle cotangents, seed 2, the position term also
+writing the cotangents in sorted order for the scatter), and the spectral adjoint
 (3 x R2C, Green adjoint, C2R).  Every stage reports algorithmic bytes per
 launch (pmpp_b200.roofline, with the measured count of touched cells) and
 the fraction of the measured HBM copy bandwidth.
@@ -95,6 +96,7 @@ def run_set(ptcl, conf, reps, peak):
     spec3 = torch.empty((3, nx, ny, nz // 2 + 1), dtype=torch.complex64, device=dev)
     acc = torch.empty((n, 3), dtype=torch.float32, device=dev)
     dcot = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    cot_sorted = torch.empty((n, 3), dtype=torch.float32, device=dev)
     fw = max(L.pmb_fft_work_bytes(nx, ny, nz, 3), L.pmb_fft_work_bytes(nx, ny, nz, 1))
     work = workspace(fw, dev, "micro_fft")
     sp = SortedParticles(ptcl.pmid, ptcl.disp, conf)
@@ -111,8 +113,8 @@ def run_set(ptcl, conf, reps, peak):
         "fft_c2r_x3": lambda: call("pmb_irfft3", nx, ny, nz, 3, spec3.data_ptr(), F.data_ptr(), work.data_ptr(), s),
         "gather": lambda: sp.gather(F, out=acc),
         "scatter_adjoint": lambda: sp.interp_grad(mesh_cot, u_const=vc, disp_cot=dcot, accumulate=True),
-        "gather_adjoint": lambda: sp.interp_grad(F, u=acc_cot, disp_cot=dcot, accumulate=True),
-        "scatter3": lambda: sp.scatter(val=acc_cot, channels=3, out=F3),
+        "gather_adjoint": lambda: sp.interp_grad(F, u=acc_cot, disp_cot=dcot, accumulate=True, u_sorted=cot_sorted),
+        "scatter3": lambda: sp.scatter(val=cot_sorted, channels=3, out=F3, val_sorted=True),
         "fft_r2c_x3": lambda: call("pmb_rfft3", nx, ny, nz, 3, F3.data_ptr(), spec3.data_ptr(), work.data_ptr(), s),
         "green_gradient_adjoint": lambda: call("pmb_green_gradient_adjoint", spec3.data_ptr(), spec1.data_ptr(), nx,
                                                ny, nz, tables.data_ptr(), int(conf.has_particle_nyquist_masks), 0,

@@ -22,7 +22,7 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in declared_symbols() if not hasattr(L, s)]
     assert not missing, missing
     assert set(declared_symbols()) <= set(_lib.exported_symbols()) | {"pmb_last_error"}
-    assert L.pmb_abi_version() == 1
+    assert L.pmb_abi_version() == 2
 
 
 def test_workspace_queries_without_device():

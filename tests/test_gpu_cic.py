@@ -126,3 +126,53 @@ def test_row_bins_match_reference_binning():
     assert np.array_equal(np.sort(perm), np.arange(n))
     rows = keys // co.mesh_shape[2]
     assert np.all(np.diff(rows) >= 0)
+
+
+def _exact_case(concentrate, seed=5):
+    """2^17 particles on an 8^3 mesh; with concentrate, 100000 of them in one
+    mesh row, so the scatter blocks next to it hold more than 2^16 particles
+    (64-bit accumulation) and the others fewer (split 32-bit accumulation)."""
+    import pmpp_b200 as pb
+    co = opm.Conf(2.0, (8, 8, 8), mesh_shape=1)
+    conf = pb.Configuration(2.0, (8, 8, 8), 1, device="cuda")
+    rng = np.random.default_rng(seed)
+    n = 1 << 17
+    pmid = rng.integers(0, 8, size=(n, 3)).astype(np.int16)
+    disp = rng.uniform(-3.0, 3.0, size=(n, 3)).astype(np.float32)
+    if concentrate:
+        pmid[:100000, 0] = 3
+        pmid[:100000, 1] = 3
+        disp[:100000, :2] = rng.uniform(0.0, 1.99, size=(100000, 2)).astype(np.float32)
+    return pb, co, conf, pmid, disp
+
+
+@pytest.mark.parametrize("concentrate", [False, True])
+def test_scatter_bit_exact_fixed_point(concentrate):
+    from pmpp_b200.cic import SortedParticles
+    from tests.helpers import fixed_point_scatter
+    pb, co, conf, pmid, disp = _exact_case(concentrate)
+    sp = SortedParticles(torch.from_numpy(pmid).cuda(), torch.from_numpy(disp).cuda(), conf)
+    got = sp.scatter(val_const=1.75)[0].cpu().numpy()
+    ref = fixed_point_scatter(pmid, disp, co, np.full(len(pmid), 1.75, np.float32))
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.parametrize("concentrate", [False, True])
+def test_scatter_sorted_values_bit_exact(concentrate):
+    """3-channel signed values: particle-order and sorted-order inputs give the
+    same bits, equal to the fixed-point restatement."""
+    from pmpp_b200.cic import SortedParticles
+    from tests.helpers import fixed_point_scatter
+    pb, co, conf, pmid, disp = _exact_case(concentrate, seed=6)
+    rng = np.random.default_rng(7)
+    vals = rng.normal(size=(len(pmid), 3)).astype(np.float32)
+    sp = SortedParticles(torch.from_numpy(pmid).cuda(), torch.from_numpy(disp).cuda(), conf)
+    v = torch.from_numpy(vals).cuda()
+    mesh = torch.from_numpy(rng.normal(size=(3, 8, 8, 8)).astype(np.float32)).cuda()
+    u_sorted = torch.empty_like(v)
+    sp.interp_grad(mesh, u=v, u_sorted=u_sorted)
+    a = sp.scatter(val=v, channels=3).cpu().numpy()
+    b = sp.scatter(val=u_sorted, channels=3, val_sorted=True).cpu().numpy()
+    ref = fixed_point_scatter(pmid, disp, co, vals)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.array_equal(a.view(np.uint32), ref.view(np.uint32))

@@ -37,7 +37,7 @@ def _reference_scatter(pmid, disp, dims, cell, val):
     s = stream_handle()
     _lib.call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), None, 0.0, n, nx, ny, nz, cell,
               sorted_buf.data_ptr(), scratch.data_ptr(), scratch.numel(), s)
-    _lib.call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 1, None, val, 0, 1.0, out.data_ptr(),
+    _lib.call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 1, None, 0, val, 0, 1.0, out.data_ptr(),
               s16.data_ptr(), s)
     return out
 
