@@ -83,6 +83,18 @@ int pmb_interp_grad_rows(const void* sorted, int64_t n, int nx, int ny, int nz, 
                          const float* u, float u_const, float cell, int accumulate, float* disp_cot, float* wsum,
                          float* u_sorted, void* stream);
 
+/* Mesh-row staging of pmb_gather_rows / pmb_interp_grad_rows (process-wide):
+ * 0 (default) direct corner loads; 1 stage the rows a tile of particle rows
+ * touches into shared memory with bulk asynchronous copies when the tile
+ * holds enough particles to repay the copies; 2 stage every non-empty tile.
+ * All modes give bit-identical results; staging is faster for spread-out
+ * particles and slower for clustered ones. */
+int pmb_set_gather_staging(int mode);
+/* Count of bounded device waits (bulk-copy completions in the staged
+ * gathers) that gave up since the library was loaded; 0 in a healthy run.
+ * Synchronous: reads a device counter. */
+int pmb_wait_timeouts(uint32_t* count);
+
 /* ---------------- spectral ------------------------------------------------
  * 3-D R2C / C2R (numpy convention: forward unnormalised, the inverse is NOT
  * divided by nx*ny*nz here), batch meshes back to back.  These stand in for

@@ -25,6 +25,8 @@ _SIGS = {
     "pmb_gather_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_f, c_p]),
     "pmb_interp_grad_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_p, c_f, c_f, c_int, c_p, c_p,
                                      c_p, c_p]),
+    "pmb_wait_timeouts": (c_int, [c_p]),
+    "pmb_set_gather_staging": (c_int, [c_int]),
     "pmb_fft_work_bytes": (c_i64, [c_int, c_int, c_int, c_int]),
     "pmb_rfft3": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
     "pmb_irfft3": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
@@ -120,6 +122,13 @@ _KERNELS = {
     "pmb_overdensity": 1, "pmb_ens_force": 7, "pmb_ens_step": 9, "pmb_ens_set_step": 1,
 }
 _launches = [0]
+
+
+def wait_timeouts():
+    """Bounded device waits that gave up since the library was loaded."""
+    v = ctypes.c_uint32()
+    check(lib().pmb_wait_timeouts(ctypes.byref(v)), "pmb_wait_timeouts")
+    return v.value
 
 
 def reset_launch_count():

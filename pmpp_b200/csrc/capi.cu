@@ -139,7 +139,7 @@ int pmb_gather_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C
   PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_gather_rows: unsupported mesh shape");
   PMB_REQUIRE(C >= 1 && C <= 4, "pmb_gather_rows: 1..4 channels supported");
   SortedView v = sorted_view((void*)sorted, n);
-  return gather_sorted(v.rec, v.perm, n, m, C, mesh, out, vel, kick, S(stream));
+  return gather_sorted(v.rec, v.perm, v.offs, n, m, C, mesh, out, vel, kick, S(stream));
 }
 
 int pmb_interp_grad_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh,
@@ -149,8 +149,19 @@ int pmb_interp_grad_rows(const void* sorted, int64_t n, int nx, int ny, int nz, 
   PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_interp_grad_rows: unsupported mesh shape");
   PMB_REQUIRE(C >= 1 && C <= 4, "pmb_interp_grad_rows: 1..4 channels supported");
   SortedView v = sorted_view((void*)sorted, n);
-  return interp_grad_sorted(v.rec, v.perm, n, m, C, mesh, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted,
-                            S(stream));
+  return interp_grad_sorted(v.rec, v.perm, v.offs, n, m, C, mesh, u, u_const, cell, accumulate, disp_cot, wsum,
+                            u_sorted, S(stream));
+}
+
+int pmb_set_gather_staging(int mode) {
+  PMB_REQUIRE(mode >= 0 && mode <= 2, "pmb_set_gather_staging: mode must be 0, 1 or 2");
+  set_gather_staging(mode);
+  return kOk;
+}
+
+int pmb_wait_timeouts(uint32_t* count) {
+  PMB_REQUIRE(count != nullptr, "pmb_wait_timeouts: null output");
+  return wait_timeouts(count);
 }
 
 int64_t pmb_fft_work_bytes(int nx, int ny, int nz, int batch) { return fft_work_bytes(Mesh3{nx, ny, nz}, batch); }
@@ -238,7 +249,7 @@ int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float dr
                          make_green(green_kernel, transfer, radial, radial_len, inv_m), s));
   PMB_TRY(fft_c2r(m, 3, grad_hat, force_meshes, work, s));
   SortedView v = sorted_view(sorted, n);
-  return gather_sorted(v.rec, v.perm, n, m, 3, force_meshes, acc, vel_kick, kick, s);
+  return gather_sorted(v.rec, v.perm, v.offs, n, m, 3, force_meshes, acc, vel_kick, kick, s);
 }
 
 static int64_t force_vjp_layout(int64_t n, Mesh3 m, void* ws, int64_t cap, void** sorted, void** bins, void** scale16,
@@ -290,7 +301,7 @@ int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int
                         stream));
   SortedView v = sorted_view(sorted, n);
   // gather adjoint: position term and the 3-channel scatter of acc_cot
-  PMB_TRY(interp_grad_sorted(v.rec, v.perm, n, m, 3, force_meshes, acc_cot, 0.f, cell, 1, disp_cot, nullptr,
+  PMB_TRY(interp_grad_sorted(v.rec, v.perm, v.offs, n, m, 3, force_meshes, acc_cot, 0.f, cell, 1, disp_cot, nullptr,
                              cot_sorted, s));
   PMB_TRY(pmb_scatter_rows(sorted, n, nx, ny, nz, 3, cot_sorted, 1, 0.f, 0, 1.f, mesh_cot, scale16, stream));
   // transposes of the C2R, gradient, Green and R2C stages
@@ -300,8 +311,8 @@ int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int
                                  make_green(green_kernel, transfer, radial, radial_len, post), s));
   PMB_TRY(fft_c2r(m, 1, src_hat, src_cot, work, s));
   // scatter adjoint of the density (constant particle value)
-  return interp_grad_sorted(v.rec, v.perm, n, m, 1, src_cot, nullptr, val_const, cell, 1, disp_cot, nullptr, nullptr,
-                            s);
+  return interp_grad_sorted(v.rec, v.perm, v.offs, n, m, 1, src_cot, nullptr, val_const, cell, 1, disp_cot, nullptr,
+                            nullptr, s);
 }
 
 // ---------------------------------------------------------------------------

@@ -21,6 +21,7 @@
 #include "pmb_cic_device.cuh"
 #include "pmb_common.cuh"
 #include "pmb_kernels.cuh"
+#include "pmb_tma.cuh"
 
 namespace pmb {
 
@@ -269,12 +270,18 @@ __global__ void __launch_bounds__(256) scatter_pull_kernel(const Rec* __restrict
 }
 
 void scatter_block_shape(Mesh3 m, int C, int* RX, int* RY) {
-  // Largest of 2x2, 1x2, 1x1 output rows whose accumulator fits in 100 KB
-  // (two or more CTAs per SM).
+  // First of 2x2, 1x2, 1x1 output rows whose accumulator fits in 100 KB
+  // (two or more CTAs per SM; larger blocks measured slower).
   const int64_t budget = 100 * 1024;
-  int rx = 2, ry = 2;
-  if (ScatterSmem::acc_bytes(rx, ry, C, m.nz) > budget) rx = 1;
-  if (ScatterSmem::acc_bytes(rx, ry, C, m.nz) > budget) ry = 1;
+  static const int shapes[3][2] = {{2, 2}, {1, 2}, {1, 1}};
+  int rx = 1, ry = 1;
+  for (const auto& sh : shapes) {
+    if (ScatterSmem::acc_bytes(sh[0], sh[1], C, m.nz) <= budget) {
+      rx = sh[0];
+      ry = sh[1];
+      break;
+    }
+  }
   *RX = rx < m.nx ? rx : m.nx;
   *RY = ry < m.ny ? ry : m.ny;
 }
@@ -326,9 +333,188 @@ __global__ void gather_kernel(const Rec* __restrict__ rec, const uint32_t* __res
   gather_one<C>(rec[i], perm[i], m, mesh, out, vel, kick);
 }
 
-int gather_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int C, const float* mesh, float* out,
-                  float* vel, float kick, cudaStream_t s) {
+// ---------------------------------------------------------------------------
+// Staged gathers: the mesh rows a tile of particle rows touches are copied
+// into shared memory with bulk asynchronous copies, then every particle of
+// the tile interpolates from shared memory.
+// ---------------------------------------------------------------------------
+__device__ unsigned int g_wait_timeouts_cic = 0;
+
+// 0: direct corner loads (default); 1: stage the rows of tiles with enough
+// particles; 2: stage every non-empty tile.  Staging wins on spread-out
+// particles and loses on clustered ones, whose corner loads already hit in
+// L1/L2, so it is opt-in.
+static int g_gather_staging = 0;
+
+void set_gather_staging(int mode) { g_gather_staging = mode; }
+
+constexpr int kStageMaxRX = 4;
+constexpr int64_t kStageBudget = 110 * 1024;
+
+// Shared bytes of the staged rows of an RX x RY tile with C channels.
+inline int64_t stage_bytes(int RX, int RY, int C, int nz) { return (int64_t)(RX + 1) * (RY + 1) * C * nz * 4; }
+
+// Tile of particle rows whose staged mesh rows fit the budget; false when the
+// mesh rows cannot be bulk-copied (nz % 4 != 0 or a misaligned mesh).
+bool stage_shape(Mesh3 m, int C, const float* mesh, int* RX, int* RY) {
+  if (g_gather_staging == 0 || m.nz % 4 != 0 || ((uintptr_t)mesh & 15) != 0) return false;
+  static const int shapes[5][2] = {{4, 4}, {2, 4}, {2, 2}, {1, 2}, {1, 1}};
+  for (const auto& sh : shapes) {
+    if (sh[0] <= m.nx && sh[1] <= m.ny && stage_bytes(sh[0], sh[1], C, m.nz) <= kStageBudget) {
+      *RX = sh[0];
+      *RY = sh[1];
+      return true;
+    }
+  }
+  return false;
+}
+
+// Tiles with fewer particles than this load their corners directly: staging
+// costs the tile's rows, a direct gather about one 32-byte sector per corner
+// and channel of every particle.
+inline uint32_t stage_threshold(int64_t smem, int C) {
+  return g_gather_staging == 2 ? 1u : (uint32_t)(smem / (8 * 32 * C));
+}
+
+// Copies the (RX+1) x (RY+1) mesh rows (periodic) of C channels starting at
+// row (x0, y0) into stage[c][ix][iy][nz].  Returns false (after flagging the
+// timeout) when the copies do not complete.
+__device__ __forceinline__ bool stage_mesh_rows(float* stage, const float* __restrict__ mesh, Mesh3 m, int C, int x0,
+                                                int y0, int RX, int RY, uint64_t* bar) {
+  const int SX = RX + 1, SY = RY + 1;
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    const uint32_t row_bytes = (uint32_t)m.nz * 4u;
+    mbar_expect_tx(bar, row_bytes * (uint32_t)(SX * SY * C));
+    const int64_t cells = m.cells();
+    for (int c = 0; c < C; ++c)
+      for (int ix = 0; ix < SX; ++ix) {
+        const int x = x0 + ix >= m.nx ? x0 + ix - m.nx : x0 + ix;
+        for (int iy = 0; iy < SY; ++iy) {
+          const int y = y0 + iy >= m.ny ? y0 + iy - m.ny : y0 + iy;
+          bulk_copy_g2s(stage + ((c * SX + ix) * SY + iy) * m.nz, mesh + c * cells + ((int64_t)x * m.ny + y) * m.nz,
+                        row_bytes, bar);
+        }
+      }
+  }
+  __syncthreads();
+  return mbar_wait_or_flag(bar, 0, &g_wait_timeouts_cic);
+}
+
+// Particle segments of the tile: rows (x0 + k, y0 .. y0+RY-1) are contiguous
+// in the sorted records for each k.  Returns the particle count.
+__device__ __forceinline__ uint32_t tile_segments(const uint32_t* __restrict__ offs, Mesh3 m, int x0, int y0, int RX,
+                                                  int RY, uint32_t* seg_b, uint32_t* seg_n) {
+  if (threadIdx.x < RX) {
+    const int x = x0 + threadIdx.x;
+    uint32_t b = 0, c = 0;
+    if (x < m.nx) {
+      const int y1 = y0 + RY < m.ny ? y0 + RY : m.ny;
+      b = offs[(int64_t)x * m.ny + y0];
+      c = offs[(int64_t)x * m.ny + y1] - b;
+    }
+    seg_b[threadIdx.x] = b;
+    seg_n[threadIdx.x] = c;
+  }
+  __syncthreads();
+  uint32_t total = 0;
+  for (int k = 0; k < RX; ++k) total += seg_n[k];
+  return total;
+}
+
+// Sorted index and tile-local row (k, iy) of the j-th particle of the tile.
+__device__ __forceinline__ uint32_t tile_particle(uint32_t j, const uint32_t* seg_b, const uint32_t* seg_n, int* k) {
+  int kk = 0;
+  while (j >= seg_n[kk]) {
+    j -= seg_n[kk];
+    ++kk;
+  }
+  *k = kk;
+  return seg_b[kk] + j;
+}
+
+// Same arithmetic as gather_one, reading the staged rows.
+template <int C>
+__global__ void __launch_bounds__(256) gather_staged_kernel(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm,
+                                                            const uint32_t* __restrict__ offs, Mesh3 m, int RX, int RY,
+                                                            uint32_t min_stage, const float* __restrict__ mesh,
+                                                            float* __restrict__ out, float* __restrict__ vel,
+                                                            float kick) {
+  extern __shared__ __align__(16) float stage[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t seg_b[kStageMaxRX], seg_n[kStageMaxRX];
+  const int nby = (m.ny + RY - 1) / RY;
+  const int x0 = (int)(blockIdx.x / nby) * RX, y0 = (int)(blockIdx.x % nby) * RY;
+  const uint32_t total = tile_segments(offs, m, x0, y0, RX, RY, seg_b, seg_n);
+  if (total == 0) return;
+  if (total < min_stage) {
+    // too few particles to pay for staging the rows: load corners directly
+    for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
+      int k;
+      const uint32_t i = tile_particle(j, seg_b, seg_n, &k);
+      gather_one<C>(rec[i], perm[i], m, mesh, out, vel, kick);
+    }
+    return;
+  }
+  if (!stage_mesh_rows(stage, mesh, m, C, x0, y0, RX, RY, &bar)) return;
+  const int SX = RX + 1, SY = RY + 1, nz = m.nz;
+  for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
+    int k;
+    const uint32_t i = tile_particle(j, seg_b, seg_n, &k);
+    const Rec r = rec[i];
+    const uint32_t row = r.key / (uint32_t)nz;
+    const int cz = (int)(r.key - row * (uint32_t)nz);
+    const int iy = (int)(row - (uint32_t)(x0 + k) * (uint32_t)m.ny) - y0;
+    const int z1 = cz + 1 == nz ? 0 : cz + 1;
+    const float wx[2] = {axis_weight(r.fx, 0), axis_weight(r.fx, 1)};
+    const float wy[2] = {axis_weight(r.fy, 0), axis_weight(r.fy, 1)};
+    const float wz[2] = {axis_weight(r.fz, 0), axis_weight(r.fz, 1)};
+    const uint32_t src = perm[i];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      float a = 0.f;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const int bx = b & 1, by = (b >> 1) & 1, bz = (b >> 2) & 1;
+        const float v = stage[((c * SX + k + bx) * SY + iy + by) * nz + (bz ? z1 : cz)];
+        a = __fadd_rn(a, __fmul_rn(v, __fmul_rn(__fmul_rn(wx[bx], wy[by]), wz[bz])));
+      }
+      out[(int64_t)src * C + c] = a;
+      if (vel != nullptr) vel[(int64_t)src * C + c] = __fadd_rn(vel[(int64_t)src * C + c], __fmul_rn(a, kick));
+    }
+  }
+}
+
+int gather_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, int64_t n, Mesh3 m, int C,
+                  const float* mesh, float* out, float* vel, float kick, cudaStream_t s) {
   if (n == 0) return kOk;
+  int RX, RY;
+  if (offs != nullptr && stage_shape(m, C, mesh, &RX, &RY)) {
+    const int64_t smem = stage_bytes(RX, RY, C, m.nz);
+    const uint32_t min_stage = stage_threshold(smem, C);
+    const unsigned grid = (unsigned)((int64_t)((m.nx + RX - 1) / RX) * ((m.ny + RY - 1) / RY));
+#define PMB_LAUNCH_GS(CC)                                                                                      \
+  do {                                                                                                         \
+    static bool attr_##CC = false;                                                                             \
+    if (!attr_##CC) {                                                                                          \
+      PMB_CUDA_CHECK(cudaFuncSetAttribute(gather_staged_kernel<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                          (int)kStageBudget));                                                \
+      attr_##CC = true;                                                                                        \
+    }                                                                                                          \
+    gather_staged_kernel<CC><<<grid, 256, (size_t)smem, s>>>(rec, perm, offs, m, RX, RY, min_stage, mesh, out, vel, \
+                                                              kick);                                            \
+  } while (0)
+    switch (C) {
+      case 1: PMB_LAUNCH_GS(1); break;
+      case 2: PMB_LAUNCH_GS(2); break;
+      case 3: PMB_LAUNCH_GS(3); break;
+      case 4: PMB_LAUNCH_GS(4); break;
+      default: return kUnsupported;
+    }
+#undef PMB_LAUNCH_GS
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return kOk;
+  }
   const int th = 256;
   const unsigned g = (unsigned)((n + th - 1) / th);
   switch (C) {
@@ -342,6 +528,11 @@ int gather_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int 
   return kOk;
 }
 
+int wait_timeouts(unsigned int* count) {
+  PMB_CUDA_CHECK(cudaMemcpyFromSymbol(count, g_wait_timeouts_cic, sizeof(unsigned int)));
+  return kOk;
+}
+
 // Position term of the CIC adjoints.  With per-particle weights u (N, C) or a
 // constant u_const:
 //   inner_b = sum_c u_c * mesh_c[i_b]
@@ -351,23 +542,13 @@ int gather_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int 
 // adjoint's val cotangent, scatter.py:372-373) and u_sorted[i, c] =
 // u[src, c] (the weights in sorted order, so a following scatter of u reads
 // them coalesced instead of through the permutation).
-template <int C>
-__global__ void interp_grad_kernel(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm, int64_t n, Mesh3 m,
-                                   const float* __restrict__ mesh, const float* __restrict__ u, float u_const,
-                                   float cell, int accumulate, float* __restrict__ disp_cot,
-                                   float* __restrict__ wsum, float* __restrict__ u_sorted) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const Rec r = rec[i];
-  const uint32_t src = perm[i];
-  const uint32_t key = r.key;
-  const int cz = (int)(key % (uint32_t)m.nz);
-  const uint32_t rowk = key / (uint32_t)m.nz;
-  const int cy = (int)(rowk % (uint32_t)m.ny);
-  const int cx = (int)(rowk / (uint32_t)m.ny);
-  const int x1 = cx + 1 == m.nx ? 0 : cx + 1;
-  const int y1 = cy + 1 == m.ny ? 0 : cy + 1;
-  const int z1 = cz + 1 == m.nz ? 0 : cz + 1;
+// Per-particle body shared by the direct and staged kernels; fetch(c, b)
+// returns channel c of corner b (bit a of b: +1 along axis a).
+template <int C, class Fetch>
+__device__ __forceinline__ void interp_grad_one(const Rec& r, uint32_t src, int64_t i, const Fetch& fetch,
+                                                const float* __restrict__ u, float u_const, float cell, int accumulate,
+                                                float* __restrict__ disp_cot, float* __restrict__ wsum,
+                                                float* __restrict__ u_sorted) {
   const float f[3] = {r.fx, r.fy, r.fz};
   float wa[3][2], sg[3][2];
 #pragma unroll
@@ -384,7 +565,6 @@ __global__ void interp_grad_kernel(const Rec* __restrict__ rec, const uint32_t* 
 #pragma unroll
     for (int c = 0; c < C; ++c) u_sorted[i * C + c] = uu[c];
   }
-  const int64_t cells = m.cells();
   float g0 = 0.f, g1 = 0.f, g2 = 0.f;
   float ws[C];
 #pragma unroll
@@ -392,12 +572,11 @@ __global__ void interp_grad_kernel(const Rec* __restrict__ rec, const uint32_t* 
 #pragma unroll
   for (int b = 0; b < 8; ++b) {
     const int bx = b & 1, by = (b >> 1) & 1, bz = (b >> 2) & 1;
-    const int64_t idx = ((int64_t)(bx ? x1 : cx) * m.ny + (by ? y1 : cy)) * m.nz + (bz ? z1 : cz);
     float inner = 0.f;
     const float w = __fmul_rn(__fmul_rn(wa[0][bx], wa[1][by]), wa[2][bz]);
 #pragma unroll
     for (int c = 0; c < C; ++c) {
-      const float mv = __ldg(mesh + (int64_t)c * cells + idx);
+      const float mv = fetch(c, b);
       inner = __fadd_rn(inner, __fmul_rn(uu[c], mv));
       ws[c] = __fadd_rn(ws[c], __fmul_rn(mv, w));
     }
@@ -428,10 +607,96 @@ __global__ void interp_grad_kernel(const Rec* __restrict__ rec, const uint32_t* 
   }
 }
 
-int interp_grad_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int C, const float* mesh,
-                       const float* u, float u_const, float cell, int accumulate, float* disp_cot, float* wsum,
-                       float* u_sorted, cudaStream_t s) {
+template <int C>
+__global__ void interp_grad_kernel(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm, int64_t n, Mesh3 m,
+                                   const float* __restrict__ mesh, const float* __restrict__ u, float u_const,
+                                   float cell, int accumulate, float* __restrict__ disp_cot,
+                                   float* __restrict__ wsum, float* __restrict__ u_sorted) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Rec r = rec[i];
+  Corners k;
+  corners_of(r, m, k);
+  const int64_t cells = m.cells();
+  auto fetch = [&](int c, int b) { return __ldg(mesh + (int64_t)c * cells + k.idx[b]); };
+  interp_grad_one<C>(r, perm[i], i, fetch, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted);
+}
+
+template <int C>
+__global__ void __launch_bounds__(256) interp_grad_staged_kernel(
+    const Rec* __restrict__ rec, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ offs, Mesh3 m, int RX,
+    int RY, uint32_t min_stage, const float* __restrict__ mesh, const float* __restrict__ u, float u_const, float cell,
+    int accumulate, float* __restrict__ disp_cot, float* __restrict__ wsum, float* __restrict__ u_sorted) {
+  extern __shared__ __align__(16) float stage[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t seg_b[kStageMaxRX], seg_n[kStageMaxRX];
+  const int nby = (m.ny + RY - 1) / RY;
+  const int x0 = (int)(blockIdx.x / nby) * RX, y0 = (int)(blockIdx.x % nby) * RY;
+  const uint32_t total = tile_segments(offs, m, x0, y0, RX, RY, seg_b, seg_n);
+  if (total == 0) return;
+  if (total < min_stage) {
+    const int64_t cells = m.cells();
+    for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
+      int k;
+      const uint32_t i = tile_particle(j, seg_b, seg_n, &k);
+      const Rec r = rec[i];
+      Corners kc;
+      corners_of(r, m, kc);
+      auto fetch = [&](int c, int b) { return __ldg(mesh + (int64_t)c * cells + kc.idx[b]); };
+      interp_grad_one<C>(r, perm[i], i, fetch, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted);
+    }
+    return;
+  }
+  if (!stage_mesh_rows(stage, mesh, m, C, x0, y0, RX, RY, &bar)) return;
+  const int SX = RX + 1, SY = RY + 1, nz = m.nz;
+  for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
+    int k;
+    const uint32_t i = tile_particle(j, seg_b, seg_n, &k);
+    const Rec r = rec[i];
+    const uint32_t row = r.key / (uint32_t)nz;
+    const int cz = (int)(r.key - row * (uint32_t)nz);
+    const int iy = (int)(row - (uint32_t)(x0 + k) * (uint32_t)m.ny) - y0;
+    const int z1 = cz + 1 == nz ? 0 : cz + 1;
+    auto fetch = [&](int c, int b) {
+      const int bx = b & 1, by = (b >> 1) & 1, bz = (b >> 2) & 1;
+      return stage[((c * SX + k + bx) * SY + iy + by) * nz + (bz ? z1 : cz)];
+    };
+    interp_grad_one<C>(r, perm[i], i, fetch, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted);
+  }
+}
+
+int interp_grad_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, int64_t n, Mesh3 m, int C,
+                       const float* mesh, const float* u, float u_const, float cell, int accumulate, float* disp_cot,
+                       float* wsum, float* u_sorted, cudaStream_t s) {
   if (n == 0) return kOk;
+  int RX, RY;
+  if (offs != nullptr && stage_shape(m, C, mesh, &RX, &RY)) {
+    const int64_t smem = stage_bytes(RX, RY, C, m.nz);
+    const uint32_t min_stage = stage_threshold(smem, C);
+    const unsigned grid = (unsigned)((int64_t)((m.nx + RX - 1) / RX) * ((m.ny + RY - 1) / RY));
+#define PMB_LAUNCH_IS(CC)                                                                                       \
+  do {                                                                                                          \
+    static bool attr_##CC = false;                                                                              \
+    if (!attr_##CC) {                                                                                           \
+      PMB_CUDA_CHECK(cudaFuncSetAttribute(interp_grad_staged_kernel<CC>,                                        \
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBudget));     \
+      attr_##CC = true;                                                                                         \
+    }                                                                                                           \
+    interp_grad_staged_kernel<CC><<<grid, 256, (size_t)smem, s>>>(rec, perm, offs, m, RX, RY, min_stage, mesh, u, \
+                                                                   u_const, cell, accumulate, disp_cot, wsum,   \
+                                                                   u_sorted);                                   \
+  } while (0)
+    switch (C) {
+      case 1: PMB_LAUNCH_IS(1); break;
+      case 2: PMB_LAUNCH_IS(2); break;
+      case 3: PMB_LAUNCH_IS(3); break;
+      case 4: PMB_LAUNCH_IS(4); break;
+      default: return kUnsupported;
+    }
+#undef PMB_LAUNCH_IS
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return kOk;
+  }
   const int th = 256;
   const unsigned g = (unsigned)((n + th - 1) / th);
   switch (C) {

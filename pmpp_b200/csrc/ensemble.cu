@@ -185,6 +185,8 @@ __global__ void __launch_bounds__(256) ens_scatter_kernel(EnsDev d) {
   }
 }
 
+// Flat loop over the half spectra of all members; local cell coordinates
+// from 32-bit index arithmetic (members have fewer than 2^31 half cells).
 __global__ void ens_green_kernel(EnsDev d) {
   __shared__ int64_t ss[kEnsMaxSims + 1];
   load_starts(ss, d.spec_start, d.nsims);
@@ -201,7 +203,11 @@ __global__ void ens_green_kernel(EnsDev d) {
     g.post_scale = sim.post;
     const Mesh3 m = sim.m;
     const SpecTables t = sim.t;
-    green_gradient_at(sim.rho_hat, sim.grad_hat, jg - ss[s], m.half_cells(), m, t, g);
+    const uint32_t nzh = (uint32_t)(m.nz / 2 + 1), ny = (uint32_t)m.ny;
+    const uint32_t j = (uint32_t)(jg - ss[s]);
+    const uint32_t r = j / nzh, ix = r / ny;
+    green_gradient_at(sim.rho_hat, sim.grad_hat, (int64_t)j, m.half_cells(), (int)ix, (int)(r - ix * ny),
+                      (int)(j - r * nzh), m, t, g);
   }
 }
 
@@ -440,7 +446,8 @@ int pmb_ens_create(int nsims, const int64_t* counts, const int32_t* mesh_shapes,
     std::memset(&q, 0, sizeof(q));
     q.m = Mesh3{mesh_shapes[3 * s], mesh_shapes[3 * s + 1], mesh_shapes[3 * s + 2]};
     const bool ok_mesh = q.m.nx >= 1 && q.m.ny >= 1 && q.m.nz >= 1 && q.m.nz <= 4096 &&
-                         (double)q.m.nx * q.m.ny * q.m.nz < 4294967296.0;
+                         (double)q.m.nx * q.m.ny * q.m.nz < 4294967296.0 &&
+                         (double)q.m.nx * q.m.ny * (q.m.nz / 2 + 1) < 2147483648.0;
     if (!ok_mesh || counts[s] < 0 || !(cells[s] > 0.f) || !std::isfinite(vals[s])) {
       delete e;
       set_last_error("pmb_ens_create: invalid simulation description");
@@ -575,6 +582,7 @@ int pmb_ens_bind(void* handle, const int16_t* pmid, float* disp, float* vel, flo
   PMB_CUDA_CHECK(cudaMemcpyAsync((void*)d.p_start, e->p_start.data(), 8 * (e->nsims + 1), cudaMemcpyHostToDevice, s));
   PMB_CUDA_CHECK(
       cudaMemcpyAsync((void*)d.spec_start, e->spec_start.data(), 8 * (e->nsims + 1), cudaMemcpyHostToDevice, s));
+
   PMB_CUDA_CHECK(cudaMemsetAsync((void*)d.fac, 0, 4 * 3 * (int64_t)e->nsims * (e->max_steps + 1), s));
   ens_set_step_kernel<<<1, 1, 0, s>>>((int*)d.step, 0);
   PMB_CUDA_CHECK(cudaGetLastError());

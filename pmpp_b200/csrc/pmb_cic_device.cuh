@@ -52,13 +52,14 @@ struct ScatterSmem {
 //
 // Integer sums do not depend on the order in which particles arrive, so the
 // result is bit-deterministic.  Accumulator: 12 bytes per output cell-channel
-// (ScatterSmem::acc_bytes).  When the block's source segments hold fewer than
-// 2^16 particles, each 64-bit contribution q = a*2^32 + b*2^16 + c (a signed,
-// 0 <= b, c < 2^16) is added as three 32-bit shared atomics on separate
-// planes: the b and c sums stay below 2^32 and the a sum below 2^31, so the
-// recombined total is exactly the 64-bit sum, while 32-bit atomics tolerate
-// many particles per cell (clustering) far better than 64-bit ones.  Larger
-// blocks use 64-bit atomics on the first 8 bytes per cell.  Must be called by
+// (ScatterSmem::acc_bytes).  When the block's source segments hold fewer
+// than 2^16 particles, each 64-bit contribution q = a*2^32 + b*2^16 + c (a
+// signed, 0 <= b, c < 2^16) is added as three 32-bit shared atomics on
+// separate planes: the b and c sums stay below 2^32 and the a sum below 2^31,
+// so the recombined total is exactly the 64-bit sum, while 32-bit atomics
+// tolerate many particles per cell (clustering) far better than 64-bit ones.
+// Larger blocks use one 64-bit atomic per contribution on the first 8 bytes
+// per cell.  Either way the result is the same exact sum.  Must be called by
 // all threads of the block; leaves the block synchronised.
 template <int C>
 __device__ __forceinline__ void scatter_tile(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm,
@@ -69,7 +70,12 @@ __device__ __forceinline__ void scatter_tile(const Rec* __restrict__ rec, const 
   const int nz = m.nz;
   const int nsrc = (RX + 1) * (RY + 1);
   const int cells = RX * RY * C * nz;
-  for (int t = threadIdx.x; t < 3 * cells; t += blockDim.x) acc[t] = 0u;
+  {
+    uint4* a4 = reinterpret_cast<uint4*>(acc);
+    const int n4 = (3 * cells) >> 2;
+    for (int t = threadIdx.x; t < n4; t += blockDim.x) a4[t] = make_uint4(0u, 0u, 0u, 0u);
+    for (int t = 4 * n4 + threadIdx.x; t < 3 * cells; t += blockDim.x) acc[t] = 0u;
+  }
   if (threadIdx.x < nsrc) {
     const int k = threadIdx.x;
     const int px = pmod(x0 + k / (RY + 1) - 1, m.nx), py = pmod(y0 + k % (RY + 1) - 1, m.ny);

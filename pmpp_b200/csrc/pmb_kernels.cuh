@@ -18,11 +18,14 @@ int compute_scale(const float* val, int64_t count, int64_t n, double* scale_dev,
 int scatter_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, Mesh3 m, int C, const float* val,
                    int val_sorted, float val_const, const double* scale_dev, int mode, float src_mul, float* out,
                    cudaStream_t s);
-int gather_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int C, const float* mesh, float* out,
-                  float* vel, float kick, cudaStream_t s);
-int interp_grad_sorted(const Rec* rec, const uint32_t* perm, int64_t n, Mesh3 m, int C, const float* mesh,
-                       const float* u, float u_const, float cell, int accumulate, float* disp_cot, float* wsum,
-                       float* u_sorted, cudaStream_t s);
+// offs (row offsets, may be null) enables the staged kernels.
+int gather_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, int64_t n, Mesh3 m, int C,
+                  const float* mesh, float* out, float* vel, float kick, cudaStream_t s);
+int interp_grad_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, int64_t n, Mesh3 m, int C,
+                       const float* mesh, const float* u, float u_const, float cell, int accumulate, float* disp_cot,
+                       float* wsum, float* u_sorted, cudaStream_t s);
+int wait_timeouts(unsigned int* count);
+void set_gather_staging(int mode);
 
 // spectral.cu
 int fft_r2c(Mesh3 m, int batch, float* in, float2* out, void* work, cudaStream_t s);

@@ -34,15 +34,12 @@ __device__ __forceinline__ float transfer_of(const GreenParams& g, const SpecTab
   return T;
 }
 
-// Half-spectrum cell j of the forward multiplier: three gradient spectra
-// (channel stride `total`) from one source spectrum.
+// Half-spectrum cell j = (ix*ny + iy)*(nz/2+1) + iz of the forward
+// multiplier: three gradient spectra (channel stride `total`) from one
+// source spectrum.
 __device__ __forceinline__ void green_gradient_at(const float2* __restrict__ src, float2* __restrict__ grad, int64_t j,
-                                                  int64_t total, Mesh3 m, const SpecTables& t, const GreenParams& g) {
-  const int nzh = m.nz / 2 + 1;
-  const int iz = (int)(j % nzh);
-  const int64_t r = j / nzh;
-  const int iy = (int)(r % m.ny);
-  const int ix = (int)(r / m.ny);
+                                                  int64_t total, int ix, int iy, int iz, Mesh3 m, const SpecTables& t,
+                                                  const GreenParams& g) {
   float2 v = src[j];
   if (t.mx != nullptr) {
     const float mk = __fmul_rn(__fmul_rn(t.mx[ix], t.my[iy]), t.mz[iz]);
@@ -65,6 +62,39 @@ __device__ __forceinline__ void green_gradient_at(const float2* __restrict__ src
 #pragma unroll
   for (int d = 0; d < 3; ++d)
     grad[(int64_t)d * total + j] = make_float2(__fmul_rn(-__fmul_rn(c[d], pi), ps), __fmul_rn(__fmul_rn(c[d], pr), ps));
+}
+
+// Adjoint at half-spectrum cell j: S_cot = K * sum_d conj(i c_d) A_d.  The
+// force map is a real convolution (H_d Hermitian), so its transpose is the
+// correlation with the conjugate multiplier.
+__device__ __forceinline__ void green_gradient_adjoint_at(const float2* __restrict__ gc, float2* __restrict__ out,
+                                                          int64_t j, int64_t total, int ix, int iy, int iz, Mesh3 m,
+                                                          const SpecTables& t, const GreenParams& g) {
+  const float c[3] = {t.cx[ix], t.cy[iy], t.cz[iz]};
+  float ar = 0.f, ai = 0.f;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float2 a = gc[(int64_t)d * total + j];
+    ar = __fadd_rn(ar, __fmul_rn(c[d], a.y));
+    ai = __fsub_rn(ai, __fmul_rn(c[d], a.x));
+  }
+  const float k2 = k2_of(t, ix, iy, iz);
+  float pr = 0.f, pi = 0.f;
+  if (k2 != 0.f) {
+    if (g.transfer != nullptr || g.radial != nullptr) {
+      const float T = transfer_of(g, t, j, ix, iy, iz, m);
+      ar = __fmul_rn(ar, T);
+      ai = __fmul_rn(ai, T);
+    }
+    pr = __fdiv_rn(-ar, k2);
+    pi = __fdiv_rn(-ai, k2);
+    if (t.mx != nullptr) {
+      const float mk = __fmul_rn(__fmul_rn(t.mx[ix], t.my[iy]), t.mz[iz]);
+      pr = __fmul_rn(pr, mk);
+      pi = __fmul_rn(pi, mk);
+    }
+  }
+  out[j] = make_float2(__fmul_rn(pr, g.post_scale), __fmul_rn(pi, g.post_scale));
 }
 
 }  // namespace pmb

@@ -114,50 +114,33 @@ int fft_c2r(Mesh3 m, int batch, float2* in, float* out, void* work, cudaStream_t
 // ---------------------------------------------------------------------------
 // Green's function x gradient
 // ---------------------------------------------------------------------------
+// Flat grid-stride loops over the half spectrum; the cell coordinates come
+// from 32-bit index arithmetic (Index = uint32_t) whenever the spectrum has
+// fewer than 2^31 cells (the loop index then cannot wrap), which keeps the
+// multipliers memory-bound.
+template <class Index>
 __global__ void green_gradient_kernel(const float2* __restrict__ src, float2* __restrict__ grad, Mesh3 m,
                                       SpecTables t, GreenParams g) {
-  const int64_t total = m.half_cells();
-  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x)
-    green_gradient_at(src, grad, j, total, m, t, g);
+  const Index nzh = (Index)(m.nz / 2 + 1), ny = (Index)m.ny;
+  const Index total = (Index)m.half_cells();
+  for (Index j = (Index)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (Index)gridDim.x * blockDim.x) {
+    const Index r = j / nzh;
+    const Index ix = r / ny;
+    green_gradient_at(src, grad, (int64_t)j, (int64_t)total, (int)ix, (int)(r - ix * ny), (int)(j - r * nzh), m, t,
+                      g);
+  }
 }
 
-// Adjoint: S_cot = K * sum_d conj(i c_d) A_d.  The force map is a real
-// convolution (H_d Hermitian), so its transpose is the correlation with the
-// conjugate multiplier.
+template <class Index>
 __global__ void green_gradient_adjoint_kernel(const float2* __restrict__ gc, float2* __restrict__ out, Mesh3 m,
                                               SpecTables t, GreenParams g) {
-  const int nzh = m.nz / 2 + 1;
-  const int64_t total = m.half_cells();
-  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
-    const int iz = (int)(j % nzh);
-    const int64_t r = j / nzh;
-    const int iy = (int)(r % m.ny);
-    const int ix = (int)(r / m.ny);
-    const float c[3] = {t.cx[ix], t.cy[iy], t.cz[iz]};
-    float ar = 0.f, ai = 0.f;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const float2 a = gc[(int64_t)d * total + j];
-      ar = __fadd_rn(ar, __fmul_rn(c[d], a.y));
-      ai = __fsub_rn(ai, __fmul_rn(c[d], a.x));
-    }
-    const float k2 = k2_of(t, ix, iy, iz);
-    float pr = 0.f, pi = 0.f;
-    if (k2 != 0.f) {
-      if (g.transfer != nullptr || g.radial != nullptr) {
-        const float T = transfer_of(g, t, j, ix, iy, iz, m);
-        ar = __fmul_rn(ar, T);
-        ai = __fmul_rn(ai, T);
-      }
-      pr = __fdiv_rn(-ar, k2);
-      pi = __fdiv_rn(-ai, k2);
-      if (t.mx != nullptr) {
-        const float mk = __fmul_rn(__fmul_rn(t.mx[ix], t.my[iy]), t.mz[iz]);
-        pr = __fmul_rn(pr, mk);
-        pi = __fmul_rn(pi, mk);
-      }
-    }
-    out[j] = make_float2(__fmul_rn(pr, g.post_scale), __fmul_rn(pi, g.post_scale));
+  const Index nzh = (Index)(m.nz / 2 + 1), ny = (Index)m.ny;
+  const Index total = (Index)m.half_cells();
+  for (Index j = (Index)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (Index)gridDim.x * blockDim.x) {
+    const Index r = j / nzh;
+    const Index ix = r / ny;
+    green_gradient_adjoint_at(gc, out, (int64_t)j, (int64_t)total, (int)ix, (int)(r - ix * ny), (int)(j - r * nzh), m,
+                              t, g);
   }
 }
 
@@ -168,14 +151,22 @@ static unsigned grid_for(int64_t total, int th) {
 }
 
 int green_gradient(const float2* src_hat, float2* grad_hat, Mesh3 m, SpecTables t, GreenParams g, cudaStream_t s) {
-  green_gradient_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(src_hat, grad_hat, m, t, g);
+  const unsigned grid = grid_for(m.half_cells(), 256);
+  if (m.half_cells() < 2147483648ll)
+    green_gradient_kernel<uint32_t><<<grid, 256, 0, s>>>(src_hat, grad_hat, m, t, g);
+  else
+    green_gradient_kernel<int64_t><<<grid, 256, 0, s>>>(src_hat, grad_hat, m, t, g);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }
 
 int green_gradient_adjoint(const float2* grad_cot_hat, float2* src_cot_hat, Mesh3 m, SpecTables t, GreenParams g,
                            cudaStream_t s) {
-  green_gradient_adjoint_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(grad_cot_hat, src_cot_hat, m, t, g);
+  const unsigned grid = grid_for(m.half_cells(), 256);
+  if (m.half_cells() < 2147483648ll)
+    green_gradient_adjoint_kernel<uint32_t><<<grid, 256, 0, s>>>(grad_cot_hat, src_cot_hat, m, t, g);
+  else
+    green_gradient_adjoint_kernel<int64_t><<<grid, 256, 0, s>>>(grad_cot_hat, src_cot_hat, m, t, g);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }

@@ -65,6 +65,14 @@ def clustered_positions(conf, seed=0):
     return Particles(conf, grid.pmid, d)
 
 
+def _staged(fn):
+    call("pmb_set_gather_staging", 1)
+    try:
+        fn()
+    finally:
+        call("pmb_set_gather_staging", 0)
+
+
 def _time(fn, reps):
     fn()
     torch.cuda.synchronize()
@@ -120,13 +128,17 @@ def run_set(ptcl, conf, reps, peak):
                                                ny, nz, tables.data_ptr(), int(conf.has_particle_nyquist_masks), 0,
                                                None, None, 0, 0.45 * inv_m, s),
         "fft_c2r": lambda: call("pmb_irfft3", nx, ny, nz, 1, spec1.data_ptr(), rho.data_ptr(), work.data_ptr(), s),
+        # the same gathers with mesh rows staged in shared memory (opt-in mode)
+        "gather@staged": lambda: _staged(lambda: sp.gather(F, out=acc)),
+        "gather_adjoint@staged": lambda: _staged(
+            lambda: sp.interp_grad(F, u=acc_cot, disp_cot=dcot, accumulate=True, u_sorted=cot_sorted)),
     }
     # distinct touched cells: nonzero cells of the unit-mass density
     T = int((sp.scatter() != 0).sum())
     out = {"touched_cells": T}
     for name, fn in stages.items():
         ms = _time(fn, reps)
-        alg = algorithmic_bytes(name, n, M, Mc=Mc, R=nx * ny, T=T)
+        alg = algorithmic_bytes(name.split("@")[0], n, M, Mc=Mc, R=nx * ny, T=T)
         gbs = alg / (ms * 1e-3) / 1e9
         out[name] = {"ms": round(ms, 4), "algorithmic_bytes": alg, "GB/s": round(gbs, 1), "frac_hbm": round(gbs / peak, 4)}
     return out

@@ -11,7 +11,8 @@ def test_microbench_small():
     for s in ("U", "K"):
         stages = {k: v for k, v in res[s].items() if k != "touched_cells"}
         assert set(stages) == {"sort", "scatter", "fft_r2c", "green_gradient", "fft_c2r_x3", "gather", "scatter_adjoint",
-                               "gather_adjoint", "scatter3", "fft_r2c_x3", "green_gradient_adjoint", "fft_c2r"}
+                               "gather_adjoint", "scatter3", "fft_r2c_x3", "green_gradient_adjoint", "fft_c2r",
+                               "gather@staged", "gather_adjoint@staged"}
         assert all(v["ms"] > 0 for v in stages.values())
         assert 0 < res[s]["touched_cells"] <= 128**3
 
