@@ -124,6 +124,17 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per particle of one launch, from an ncu
+# --set full capture of the same kernels at 256^3 particles / 512^3 mesh (mesh cells = 8 particles);
+# traffic scales with particles at a fixed cells-per-particle ratio.
+MEASURED_TRAFFIC_PER_PARTICLE = {
+    "gather": (1.949 + 0.198) * 1e9 / 256**3,
+    "scatter3": (0.472 + 1.556) * 1e9 / 256**3,
+    "scatter": (0.270 + 0.484) * 1e9 / 256**3,
+    "scatter_adjoint": (1.075 + 0.189) * 1e9 / 256**3,
+}
+
+
 def load_peaks():
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
     try:
@@ -304,7 +315,10 @@ def run_ours(args):
                    "particles": N, "mesh": M,
                    "kdk_steps": args.nsteps, "parallelism": f"replicas x{world}", "l2": "inputs larger than L2"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": (MEASURED_TRAFFIC_PER_PARTICLE[dom] * N
+                                 if dom in MEASURED_TRAFFIC_PER_PARTICLE and M == 8 * N else None),
+                     "traffic_source": "ncu capture at 256^3/512^3 scaled by particles",
                      "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms},
         "breakdown": breakdown,
         "cpu_baseline": cpu,
