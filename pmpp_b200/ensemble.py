@@ -25,6 +25,7 @@ import os
 import numpy as np
 import torch
 
+from . import modes as _modes
 from ._lib import call, lib
 from .gravity import _om32
 from .nbody import _schedule
@@ -150,6 +151,88 @@ class Ensemble:
         sl = self._slot(i)
         c = (lambda t: t.clone()) if clone else (lambda t: t)
         return Particles(self.confs[i], c(self.pmid[sl]), c(self.disp[sl]), c(self.vel[sl]), c(self.acc[sl]))
+
+    # ---- initial conditions ---------------------------------------------------
+    def _prepare_ics(self):
+        """Device tables, lattices and scratch of the per-member 2LPT sequence."""
+        dev = self.device
+        L = lib()
+        self._ic = []
+        half = max(c.ptcl_grid_shape[0] * c.ptcl_grid_shape[1] * (c.ptcl_grid_shape[2] // 2 + 1) for c in self.confs)
+        cells = max(c.ptcl_num for c in self.confs)
+        wsb = max(int(L.pmb_lpt_workspace_bytes(*c.ptcl_grid_shape)) for c in self.confs)
+        self._ic_modes = torch.empty((2, half), dtype=torch.complex64, device=dev)
+        self._ic_fields = torch.empty((6, cells), dtype=torch.float32, device=dev)
+        self._ic_ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+        for i, (conf, cos) in enumerate(zip(self.confs, self.cosmos)):
+            lat = Particles.gen_grid(conf, device=dev)
+            fac, _ = cos.lpt_factors(conf.a_start)
+            self._ic.append({
+                "lin": _modes._Tables(cos, conf, dev), "pmid": lat.pmid, "disp": lat.disp,
+                "ptab": conf.spectral_tables("particle", dev),
+                "fac": tuple(_f32(x) for x in (fac[0, 0], fac[0, 2], fac[1, 0], fac[1, 2])),
+            })
+        self._ic_graph = None
+
+    def _ic_sequence(self, seeds):
+        s = stream_handle(self.device)
+        ma, mb = self._ic_modes[0], self._ic_modes[1]
+        for i, (conf, cos) in enumerate(zip(self.confs, self.cosmos)):
+            d = self._ic[i]
+            gx, gy, gz = conf.ptcl_grid_shape
+            sl = self._slot(i)
+            self.pmid[sl].copy_(d["pmid"])
+            self.disp[sl].copy_(d["disp"])
+            self.vel[sl].zero_()
+            call("pmb_white_noise_nested", int(seeds[i]) & 0xFFFFFFFF, gx, gy, gz, ma.data_ptr(), None, s)
+            tb = d["lin"]
+            call("pmb_linear_modes", ma.data_ptr(), mb.data_ptr(), None, gx, gy, gz, tb.k.data_ptr(), tb.tk.data_ptr(),
+                 tb.tt.data_ptr(), int(tb.tk.numel()), float(cos.A_s), float(cos.n_s), float(cos.Omega_m),
+                 float(cos.k_pivot), 1.0, float(conf.box_vol), s)
+            D1, V1, D2, V2 = d["fac"]
+            p0 = self.pmid[sl]
+            call("pmb_lpt", mb.data_ptr(), gx, gy, gz, float(conf.ptcl_spacing), float(conf.ptcl_cell_vol),
+                 d["ptab"].data_ptr(), int(conf.lpt_order), D1, V1, D2, V2, p0.data_ptr(), self.disp[sl].data_ptr(),
+                 self.vel[sl].data_ptr(), conf.ptcl_num, float(conf.cell_size), self._ic_fields.data_ptr(), None,
+                 self._ic_ws.data_ptr(), self._ic_ws.numel(), s)
+
+    def initial_conditions(self, seeds, graph=True):
+        """2LPT initial conditions of every member (nested white noise with the
+        member's seed -> linear modes -> 2LPT at a_start), written straight into
+        the ensemble's particle buffers.  The per-member kernel sequence is the
+        single-simulation one (so members equal ``lpt(linear_modes(
+        white_noise_nested(seed)))`` bit for bit); with graph it is captured once
+        in a CUDA graph per seed list and replayed."""
+        seeds = tuple(int(x) for x in seeds)
+        if len(seeds) != len(self.confs):
+            raise ValueError("one seed per member")
+        if not hasattr(self, "_ic"):
+            self._prepare_ics()
+        if not graph:
+            self._ic_sequence(seeds)
+            return
+        if self._ic_graph is None or self._ic_graph[0] != seeds:
+            self._ic_sequence(seeds)  # uncaptured first: cuFFT plans exist before capture
+            torch.cuda.synchronize(self.device)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._ic_sequence(seeds)
+            self._ic_graph = (seeds, g)
+        self._ic_graph[1].replay()
+
+    def run(self, seeds, graph=True):
+        """Initial conditions plus the N-body run; returns the final Particles."""
+        self.initial_conditions(seeds, graph=graph)
+        if graph and self.graph is None:
+            self.capture()
+        self.set_step(0)
+        self.force()
+        for _ in range(self.nsteps):
+            if graph:
+                self.graph.replay()
+            else:
+                self.step()
+        return [self.particles(i) for i in range(len(self.confs))]
 
     # ---- stages -------------------------------------------------------------
     def stage(self, name, drift=0, kick=0):

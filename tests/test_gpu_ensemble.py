@@ -58,3 +58,25 @@ def test_batched_shapes_autotune_and_replay():
         ref = pb.NBodyRun(conf, cos).forward(ic)
         scale = float(ref.disp.abs().max())
         assert float((out.disp - ref.disp).abs().max()) < 1e-4 * scale
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_ensemble_initial_conditions_bitwise(graph):
+    """Batched 2LPT initial conditions equal the per-member sequence bit for bit."""
+    import pmpp_b200 as pb
+    from pmpp_b200 import lpt as pl, modes as pm
+    from pmpp_b200.ensemble import Ensemble
+    confs, coss, _ = _members([(16, 2, 64.0, 0.3), (8, 2, 50.0, 0.33), (16, 1, 90.0, 0.27)])
+    seeds = [5, 9, 13]
+    ens = Ensemble(confs, coss)
+    for _ in range(2):  # the second call replays the captured sequence
+        ens.initial_conditions(seeds, graph=graph)
+    for i, (conf, cos, seed) in enumerate(zip(confs, coss, seeds)):
+        ref = pl.lpt(pm.linear_modes(pm.white_noise_nested(seed, conf), cos, conf), cos, conf)
+        got = ens.particles(i)
+        assert torch.equal(got.disp, ref.disp) and torch.equal(got.vel, ref.vel)
+        assert torch.equal(got.pmid, ref.pmid)
+    outs = ens.run(seeds, graph=graph)
+    ref = pb.NBodyRun(confs[0], coss[0]).forward(
+        pl.lpt(pm.linear_modes(pm.white_noise_nested(seeds[0], confs[0]), coss[0], confs[0]), coss[0], confs[0]))
+    assert torch.equal(outs[0].disp, ref.disp)
