@@ -66,3 +66,53 @@ def test_pipeline_forward_and_gradients():
     fd_as = (_oracle_loss(om64, co64, target, As=2.0 + 1e-5)[0] -
              _oracle_loss(om64, co64, target, As=2.0 - 1e-5)[0]) / 2e-5
     np.testing.assert_allclose(grads["A_s_1e9"], fd_as, rtol=2e-2)
+
+
+def test_gradients_sixteen_modes_and_sigma8():
+    """Reverse pass against float64 central differences of the oracle pipeline:
+    16 random single white-noise coefficients, sigma8 at fixed Omega_m and
+    Omega_m at fixed sigma8 (sigma8_chain); 16^3 particles / 32^3 mesh, 6 steps."""
+    import pmpp_b200 as pb
+    from pmpp_b200 import modes as pm, pipeline
+    a = np.linspace(0.1, 1.0, 7)
+    kw = dict(n_s=0.96, Omega_b=0.05, h=0.7)
+    conf = pb.Configuration(4.0, (16, 16, 16), 2, a_start=0.1, a_custom=a, device="cuda")
+    co64 = opm.Conf(4.0, (16, 16, 16), mesh_shape=2, a_start=0.1, a_custom=a, float_dtype=np.float64)
+    cos = pb.Cosmology.from_sigma8(conf, 0.8, Omega_m=0.3, **kw)
+    omega = pm.white_noise_nested(3, conf)
+    model = pipeline.ForwardModel(conf, cos)
+    model.forward(omega)
+    _, pk0, _ = pb.power_spectrum.particles_to_pk(model.final, conf)
+    target = pk0 * (1.0 + 0.1 * np.sin(np.arange(len(pk0))))
+    loss, g = model.loss(target)
+    grads = model.backward(g)
+    d_s8, d_om = pipeline.sigma8_chain(grads, cos, conf)
+    om64 = omega.cpu().numpy().astype(np.complex128)
+
+    def oracle(w, s8=0.8, Om=0.3):
+        c = opm.cosmo_from_sigma8(co64, s8, Omega_m=Om, **kw)
+        lin = opm.linear_modes(w, c, co64)
+        pmid, d, v = opm.lpt(lin, c, co64)
+        d2, _, _ = opm.nbody(pmid, d, v, co64, c)
+        _, p, _ = opm.density_to_pk(opm.scatter(pmid, d2, co64), co64)
+        return float((np.log(p / target)**2).mean())
+
+    np.testing.assert_allclose(loss, oracle(om64), rtol=2e-3)
+    rng = np.random.default_rng(21)
+    mc = grads["modes"].cpu().numpy()
+    ad, fd = [], []
+    eps = 1e-4
+    for _ in range(16):
+        ix, iy, iz = rng.integers(0, 16), rng.integers(0, 16), rng.integers(1, 8)
+        imag = bool(rng.integers(0, 2))
+        e = np.zeros_like(om64)
+        e[ix, iy, iz] = 1j if imag else 1.0
+        fd.append((oracle(om64 + eps * e) - oracle(om64 - eps * e)) / (2 * eps))
+        ad.append(mc[ix, iy, iz].imag if imag else mc[ix, iy, iz].real)
+    ad, fd = np.array(ad), np.array(fd)
+    assert np.linalg.norm(ad - fd) < 3e-2 * np.linalg.norm(fd)
+    h = 1e-4
+    fd_s8 = (oracle(om64, s8=0.8 + h) - oracle(om64, s8=0.8 - h)) / (2 * h)
+    np.testing.assert_allclose(d_s8, fd_s8, rtol=2e-2)
+    fd_om = (oracle(om64, Om=0.3 + h) - oracle(om64, Om=0.3 - h)) / (2 * h)
+    np.testing.assert_allclose(d_om, fd_om, rtol=3e-2)
