@@ -248,6 +248,42 @@ int pmb_transfer_fit(const double* k, int64_t nk, double omega_m, double omega_b
 int pmb_linear_power(const double* k, int64_t nk, const double* tk, const double* tt, int ntab, double A_s,
                      double n_s, double omega_m, double h, double k_pivot_Mpc, double* out);
 
+/* ---------------- float64 build ---------------------------------------------
+ * The reference's x64 configuration (jax_enable_x64): the same operations in
+ * double precision with cuFFT D2Z / Z2D, for float64 parity.  Not the
+ * optimised path: the deposit uses double atomics without a sort.
+ * pmb_force64: optional drift disp += drift_vel * drift, CIC deposit of val,
+ * source (rho - 1) * src_mul, D2Z, Green x gradient (tables: float64
+ * [kx ky kz cx cy cz (mx my mz)]), 3 x Z2D into force_meshes (3, nx, ny, nz),
+ * gather into acc with optional vel_kick += acc * kick (nbody/gravity.py:
+ * 786-814, nbody/integrator.py:202-238, 512-538).  pmb_deposit64: the density
+ * alone (cic/scatter.py:315-338).  pmb_lpt64 / pmb_linear_modes64 /
+ * pmb_white_noise_nested64 / pmb_pk_shells64 / pmb_overdensity64: float64
+ * versions of the float32 entry points of the same names. */
+int64_t pmb_force64_workspace_bytes(int nx, int ny, int nz);
+int pmb_force64(const int16_t* pmid, double* disp, const double* drift_vel, double drift, int64_t n, int nx, int ny,
+                int nz, double cell, double val, double src_mul, const double* tables, int has_masks,
+                double* force_meshes, double* acc, double* vel_kick, double kick, void* workspace,
+                int64_t workspace_bytes, void* stream);
+int pmb_deposit64(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz, double cell, double val,
+                  double* rho, void* stream);
+int pmb_axpy64(double* y, const double* x, int64_t n, double f, void* stream);
+int pmb_sum64(const double* a, int64_t n, double* out, void* stream);
+int64_t pmb_fft64_work_bytes(int nx, int ny, int nz, int batch);
+int pmb_rfft3_64(int nx, int ny, int nz, int batch, double* in, void* out, void* work, void* stream);
+int pmb_irfft3_64(int nx, int ny, int nz, int batch, void* in, double* out, void* work, void* stream);
+int pmb_white_noise_nested64(uint32_t seed, int gx, int gy, int gz, void* out, void* stream);
+int pmb_linear_modes64(const void* modes_in, void* modes_out, int gx, int gy, int gz, const double* kvec,
+                       const double* tk, const double* tt, int ntab, double A_s, double n_s, double omega_m,
+                       double k_pivot, double growth2, double box_vol, void* stream);
+int64_t pmb_lpt64_workspace_bytes(int gx, int gy, int gz);
+int pmb_lpt64(const void* modes, int gx, int gy, int gz, double spacing, double cell_vol, const double* tables,
+              int order, double D1, double V1, double D2, double V2, const int16_t* pmid, double* disp, double* vel,
+              int64_t n, double cell, double* fields, void* workspace, int64_t workspace_bytes, void* stream);
+int pmb_pk_shells64(const void* spec, int nx, int ny, int nz, const double* sinc_tab, int mas_power, int num_shells,
+                    double* sums, void* stream);
+int pmb_overdensity64(const double* rho, double* delta, int64_t n, const double* total, void* stream);
+
 /* ---------------- ensembles of independent simulations --------------------
  * No single counterpart in the reference, which advances one simulation per
  * call (nbody/solver.py:253-273) and batches only by a Python loop or a vmap

@@ -67,6 +67,23 @@ _SIGS = {
     "pmb_lpt_factors": (c_int, [c_d, c_d, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p]),
     "pmb_transfer_fit": (c_int, [c_p, c_i64, c_d, c_d, c_d, c_d, c_int, c_p]),
     "pmb_linear_power": (c_int, [c_p, c_i64, c_p, c_p, c_int, c_d, c_d, c_d, c_d, c_d, c_p]),
+    "pmb_force64_workspace_bytes": (c_i64, [c_int, c_int, c_int]),
+    "pmb_force64": (c_int, [c_p, c_p, c_p, c_d, c_i64, c_int, c_int, c_int, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p,
+                            c_d, c_p, c_i64, c_p]),
+    "pmb_deposit64": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_d, c_d, c_p, c_p]),
+    "pmb_axpy64": (c_int, [c_p, c_p, c_i64, c_d, c_p]),
+    "pmb_sum64": (c_int, [c_p, c_i64, c_p, c_p]),
+    "pmb_fft64_work_bytes": (c_i64, [c_int, c_int, c_int, c_int]),
+    "pmb_rfft3_64": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
+    "pmb_irfft3_64": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
+    "pmb_white_noise_nested64": (c_int, [ctypes.c_uint32, c_int, c_int, c_int, c_p, c_p]),
+    "pmb_linear_modes64": (c_int, [c_p, c_p, c_int, c_int, c_int, c_p, c_p, c_p, c_int, c_d, c_d, c_d, c_d, c_d, c_d,
+                                   c_p]),
+    "pmb_lpt64_workspace_bytes": (c_i64, [c_int, c_int, c_int]),
+    "pmb_lpt64": (c_int, [c_p, c_int, c_int, c_int, c_d, c_d, c_p, c_int, c_d, c_d, c_d, c_d, c_p, c_p, c_p, c_i64, c_d,
+                          c_p, c_p, c_i64, c_p]),
+    "pmb_pk_shells64": (c_int, [c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p]),
+    "pmb_overdensity64": (c_int, [c_p, c_p, c_i64, c_p, c_p]),
     "pmb_ens_create": (c_int, [c_int, c_p, c_p, c_p, c_p, c_p, c_p, c_int, c_p]),
     "pmb_ens_destroy": (c_int, [c_p]),
     "pmb_ens_workspace_bytes": (c_i64, [c_p]),
@@ -120,6 +137,8 @@ _KERNELS = {
     "pmb_force": 9, "pmb_force_vjp": 11, "pmb_sum": 1, "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,
     "pmb_lpt": 4, "pmb_lpt_vjp": 6, "pmb_pk_shells": 1, "pmb_shell_stats": 1, "pmb_pk_shells_adjoint": 1,
     "pmb_overdensity": 1, "pmb_ens_force": 7, "pmb_ens_step": 9, "pmb_ens_set_step": 1,
+    "pmb_force64": 5, "pmb_deposit64": 1, "pmb_axpy64": 1, "pmb_sum64": 1, "pmb_white_noise_nested64": 1,
+    "pmb_linear_modes64": 1, "pmb_lpt64": 4, "pmb_pk_shells64": 1, "pmb_overdensity64": 1,
 }
 _launches = [0]
 

@@ -100,6 +100,12 @@ def _val_array(val, n, device):
 
 def scatter(ptcl, conf, mesh=None, val=None, offset=0, cell_size=None):
     """CIC deposit (cic/scatter.py:235-275); val defaults to mesh_size/ptcl_num."""
+    if conf.float_dtype == torch.float64:
+        if mesh is not None or offset not in (0, 0.0) or cell_size is not None or (val is not None and
+                                                                                     not isinstance(val, float)):
+            raise NotImplementedError("the float64 build deposits a constant value on the configuration mesh")
+        from . import x64
+        return x64.scatter(ptcl, conf, val)
     if (offset not in (0, 0.0)) or cell_size is not None:
         raise NotImplementedError("only offset=0 and the configuration cell size are supported")
     sp = SortedParticles(ptcl.pmid, ptcl.disp, conf)

@@ -15,11 +15,11 @@ import numpy as np
 import torch
 
 
-def _fftfreq(shape, spacing):
-    """Angular wavevectors per axis (numerics/fft.py:4-44), float32."""
+def _fftfreq(shape, spacing, dtype=np.float32):
+    """Angular wavevectors per axis (numerics/fft.py:4-44) in the working precision."""
     period = 2 * np.pi / spacing
-    ks = [(np.fft.fftfreq(s) * period).astype(np.float32) for s in shape[:-1]]
-    ks.append((np.fft.rfftfreq(shape[-1]) * period).astype(np.float32))
+    ks = [(np.fft.fftfreq(s) * period).astype(dtype) for s in shape[:-1]]
+    ks.append((np.fft.rfftfreq(shape[-1]) * period).astype(dtype))
     return ks
 
 
@@ -44,9 +44,12 @@ class Configuration:
         if any(self.ptcl_grid_shape[0] * sm != self.mesh_shape[0] * sp
                for sp, sm in zip(self.ptcl_grid_shape[1:], self.mesh_shape[1:])):
             raise ValueError('particle and mesh grid aspect ratios differ')
-        if str(float_dtype).replace("torch.", "") != "float32":
-            raise NotImplementedError("the B200 kernels compute in float32")
-        self.float_dtype = torch.float32
+        name = str(np.dtype(str(float_dtype).replace("torch.", "")))
+        if name not in ("float32", "float64"):
+            raise NotImplementedError("float32 (optimised kernels) and float64 (x64 build) are supported")
+        # float32: the optimised kernels; float64: the x64 build (forward path only)
+        self.float_dtype = torch.float32 if name == "float32" else torch.float64
+        self.np_dtype = np.dtype(name)
         self.a_start = float(a_start)
         self.a_stop = float(a_stop)
         self.a_lpt_maxstep = a_lpt_maxstep
@@ -74,16 +77,17 @@ class Configuration:
         self.k_pivot_Mpc = k_pivot_Mpc
         self.device = torch.device(device if device is not None else ("cuda" if torch.cuda.is_available() else "cpu"))
         # cached spectral operators (configuration.py:301-307, 365-376)
-        self.kvec = _fftfreq(self.mesh_shape, self.cell_size)
-        self.kvec_spacing = _fftfreq(self.ptcl_grid_shape, self.ptcl_spacing)
+        self.kvec = _fftfreq(self.mesh_shape, self.cell_size, self.np_dtype)
+        self.kvec_spacing = _fftfreq(self.ptcl_grid_shape, self.ptcl_spacing, self.np_dtype)
         self.neg_k = tuple(self._neg_k(k, self.cell_size) for k in self.kvec)
         self._tables = {}
 
     @staticmethod
     def _neg_k(k, spacing):
-        nyquist = np.float32(np.pi / spacing)
-        eps = nyquist * np.finfo(np.float32).eps
-        return np.where(np.abs(np.abs(k) - nyquist) <= eps, np.float32(0), -k).astype(np.float32)
+        f = k.dtype.type
+        nyquist = f(np.pi / spacing)
+        eps = nyquist * np.finfo(k.dtype).eps
+        return np.where(np.abs(np.abs(k) - nyquist) <= eps, f(0), -k).astype(k.dtype)
 
     # ---- derived quantities (configuration.py:437-563) ----
     @property
@@ -155,9 +159,10 @@ class Configuration:
 
     def particle_nyquist_masks(self):
         """Per-axis masks of modes resolvable on the particle grid (core/utils.py:15-37)."""
-        kn = np.float32(np.pi / self.ptcl_spacing)
-        limit = kn + kn * np.float32(8 * np.finfo(np.float32).eps)
-        return tuple((np.abs(k) <= limit).astype(np.float32) for k in self.kvec)
+        f = self.np_dtype.type
+        kn = f(np.pi / self.ptcl_spacing)
+        limit = kn + kn * f(8 * np.finfo(self.np_dtype).eps)
+        return tuple((np.abs(k) <= limit).astype(self.np_dtype) for k in self.kvec)
 
     def spectral_tables(self, which="mesh", device=None, green_kernel=0):
         """Device table [kx ky kz cx cy cz (mx my mz)] for pmb_green_gradient.
@@ -176,8 +181,9 @@ class Configuration:
                 ks, spacing, masks = self.kvec_spacing, self.ptcl_spacing, ()
             cs = [self._neg_k(k, spacing) for k in ks]
             if green_kernel == 1:
-                c = np.float32(spacing)
-                ks = [(np.float32(2) * np.sin(k * c / np.float32(2)) / c).astype(np.float32) for k in ks]
+                f = self.np_dtype.type
+                c = f(spacing)
+                ks = [(f(2) * np.sin(k * c / f(2)) / c).astype(self.np_dtype) for k in ks]
             parts = list(ks) + cs + list(masks)
-            self._tables[key] = torch.from_numpy(np.concatenate(parts).astype(np.float32)).to(device)
+            self._tables[key] = torch.from_numpy(np.concatenate(parts).astype(self.np_dtype)).to(device)
         return self._tables[key]

@@ -61,7 +61,10 @@ __device__ __forceinline__ bool self_inverse(int k, int n) { return k == 0 || ((
 // ---------------------------------------------------------------------------
 // Nested white noise (modes.py:181-220)
 // ---------------------------------------------------------------------------
-__global__ void white_noise_kernel(uint32_t seed, Mesh3 m, float2* __restrict__ out, uint32_t* __restrict__ hashes) {
+template <class T>
+__global__ void white_noise_kernel(uint32_t seed, Mesh3 m, typename Real<T>::T2* __restrict__ out,
+                                   uint32_t* __restrict__ hashes) {
+  using R = Real<T>;
   const int64_t total = m.half_cells();
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
     const Idx3 q = unravel_half(j, m);
@@ -80,17 +83,17 @@ __global__ void white_noise_kernel(uint32_t seed, Mesh3 m, float2* __restrict__ 
       hashes[2 * j] = hr;
       hashes[2 * j + 1] = hi;
     }
-    // Box-Muller on bin-centred uniforms (modes.py:132-152), float arithmetic
-    const float scale = 2.3283064365386963e-10f;
-    const float u1 = __fmul_rn(__fadd_rn((float)hr, 0.5f), scale);
-    const float u2 = __fmul_rn(__fadd_rn((float)hi, 0.5f), scale);
-    const float r = sqrtf(__fmul_rn(-2.0f, logf(u1)));
-    const float th = __fmul_rn(6.2831853071795865f, u2);
-    const float gr = __fmul_rn(r, cosf(th)), gi = __fmul_rn(r, sinf(th));
-    const float sq = 0.7071067811865476f;
-    float2 c = make_float2(__fmul_rn(gr, sq), __fmul_rn(gi, sq));
+    // Box-Muller on bin-centred uniforms (modes.py:132-152) in the working precision
+    const T scale = (T)2.3283064365386963e-10;
+    const T u1 = R::mul(R::add((T)hr, (T)0.5), scale);
+    const T u2 = R::mul(R::add((T)hi, (T)0.5), scale);
+    const T r = R::sqrt_(R::mul((T)-2.0, R::log_(u1)));
+    const T th = R::mul((T)6.2831853071795865, u2);
+    const T gr = R::mul(r, R::cos_(th)), gi = R::mul(r, R::sin_(th));
+    const T sq = (T)0.7071067811865476;
+    typename R::T2 c = R::make2(R::mul(gr, sq), R::mul(gi, sq));
     if (plane) {
-      if (self_point) c = make_float2(gr, 0.0f);
+      if (self_point) c = R::make2(gr, (T)0);
       if (!keep) c.y = -c.y;
     }
     out[j] = c;
@@ -98,7 +101,13 @@ __global__ void white_noise_kernel(uint32_t seed, Mesh3 m, float2* __restrict__ 
 }
 
 int white_noise(uint32_t seed, Mesh3 m, float2* out, uint32_t* hashes, cudaStream_t s) {
-  white_noise_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(seed, m, out, hashes);
+  white_noise_kernel<float><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(seed, m, out, hashes);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int white_noise64(uint32_t seed, Mesh3 m, double2* out, cudaStream_t s) {
+  white_noise_kernel<double><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(seed, m, out, nullptr);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }
@@ -120,24 +129,26 @@ __device__ double interp_table(double x, const double* __restrict__ xp, const do
   return fp[lo] + (x - xp[lo]) * (fp[hi] - fp[lo]) / (xp[hi] - xp[lo]);
 }
 
-__global__ void linear_modes_kernel(const float2* __restrict__ in, float2* __restrict__ out, float* __restrict__ amp_out,
-                                    Mesh3 m, const float* __restrict__ kx, const float* __restrict__ ky,
-                                    const float* __restrict__ kz, const double* __restrict__ tk,
+template <class T>
+__global__ void linear_modes_kernel(const typename Real<T>::T2* __restrict__ in, typename Real<T>::T2* __restrict__ out,
+                                    T* __restrict__ amp_out, Mesh3 m, const T* __restrict__ kx,
+                                    const T* __restrict__ ky, const T* __restrict__ kz, const double* __restrict__ tk,
                                     const double* __restrict__ tt, int ntab, LinearPowerParams p) {
+  using R = Real<T>;
   const int64_t total = m.half_cells();
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
     const Idx3 q = unravel_half(j, m);
-    const float a = kx[q.ix], b = ky[q.iy], c = kz[q.iz];
-    const float k = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c)));
+    const T a = kx[q.ix], b = ky[q.iy], c = kz[q.iz];
+    const T k = R::sqrt_(R::add(R::add(R::mul(a, a), R::mul(b, b)), R::mul(c, c)));
     const double kd = (double)k;
-    const double T = interp_table(kd, tk, tt, ntab);
-    const double amp = p.pi_c2_over_om * T;
+    const double Tk = interp_table(kd, tk, tt, ntab);
+    const double amp = p.pi_c2_over_om * Tk;
     const double P = kd > 0.0 ? p.coef * pow(kd / p.k_pivot, p.n_s) * amp * amp * p.growth2 : 0.0;
-    const float A = sqrtf(__fmul_rn((float)P, p.box_vol));
+    const T A = R::sqrt_(R::mul((T)P, (T)p.box_vol));
     if (amp_out != nullptr) amp_out[j] = A;
     if (in != nullptr) {
-      const float2 v = in[j];
-      out[j] = make_float2(__fmul_rn(v.x, A), __fmul_rn(v.y, A));
+      const typename R::T2 v = in[j];
+      out[j] = R::make2(R::mul(v.x, A), R::mul(v.y, A));
     }
   }
 }
@@ -147,7 +158,19 @@ int linear_modes(const float2* in, float2* out, float* amp, Mesh3 m, const float
   const float* kx = ktab;
   const float* ky = kx + m.nx;
   const float* kz = ky + m.ny;
-  linear_modes_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(in, out, amp, m, kx, ky, kz, tk, tt, ntab, p);
+  linear_modes_kernel<float><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(in, out, amp, m, kx, ky, kz, tk, tt, ntab,
+                                                                           p);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int linear_modes64(const double2* in, double2* out, Mesh3 m, const double* ktab, const double* tk, const double* tt,
+                   int ntab, LinearPowerParams p, cudaStream_t s) {
+  const double* kx = ktab;
+  const double* ky = kx + m.nx;
+  const double* kz = ky + m.ny;
+  linear_modes_kernel<double><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(in, out, nullptr, m, kx, ky, kz, tk, tt,
+                                                                            ntab, p);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }
@@ -156,11 +179,13 @@ int linear_modes(const float2* in, float2* out, float* amp, Mesh3 m, const float
 // 2LPT spectral stages (lpt.py:17-43, 239-301, 379-431)
 // ---------------------------------------------------------------------------
 // tables: [kx ky kz cx cy cz] of the particle grid (c = Nyquist-zeroed -k).
+template <class T>
 struct LptTables {
-  const float *kx, *ky, *kz, *cx, *cy, *cz;
+  const T *kx, *ky, *kz, *cx, *cy, *cz;
 };
-__device__ __forceinline__ LptTables lpt_tables(const float* t, Mesh3 m) {
-  LptTables r;
+template <class T>
+__device__ __forceinline__ LptTables<T> lpt_tables(const T* t, Mesh3 m) {
+  LptTables<T> r;
   const int nzh = m.nz / 2 + 1;
   r.kx = t;
   r.ky = r.kx + m.nx;
@@ -172,78 +197,90 @@ __device__ __forceinline__ LptTables lpt_tables(const float* t, Mesh3 m) {
 }
 
 // pot1 = -(modes / cell_vol) / k^2 (lpt.py:379, 390; gravity.py:283-285)
-__device__ __forceinline__ float2 pot_from(float2 v, float k2) {
-  if (k2 == 0.f) return make_float2(0.f, 0.f);
-  return make_float2(__fdiv_rn(-v.x, k2), __fdiv_rn(-v.y, k2));
+template <class T>
+__device__ __forceinline__ typename Real<T>::T2 pot_from(typename Real<T>::T2 v, T k2) {
+  using R = Real<T>;
+  if (k2 == (T)0) return R::make2((T)0, (T)0);
+  return R::make2(R::div(-v.x, k2), R::div(-v.y, k2));
 }
 
-__device__ __forceinline__ float k2_at(const LptTables& t, const Idx3& q) {
-  const float a = t.kx[q.ix], b = t.ky[q.iy], c = t.kz[q.iz];
-  return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
+template <class T>
+__device__ __forceinline__ T k2_at(const LptTables<T>& t, const Idx3& q) {
+  using R = Real<T>;
+  const T a = t.kx[q.ix], b = t.ky[q.iy], c = t.kz[q.iz];
+  return R::add(R::add(R::mul(a, a), R::mul(b, b)), R::mul(c, c));
 }
 
 // Six strain spectra -k_i k_j pot1 * inv_n in the order (00, 11, 22, 01, 02,
 // 12); off-diagonal factors use the Nyquist-zeroed wavenumbers (lpt.py:31-35).
 // Also writes pot1 (times inv_n) for the first-order gradient.
-__global__ void lpt_strain_kernel(const float2* __restrict__ modes, float inv_cell_vol, float2* __restrict__ pot1,
-                                  float2* __restrict__ strains, Mesh3 m, const float* __restrict__ tab, float inv_n) {
-  const LptTables t = lpt_tables(tab, m);
+template <class T>
+__global__ void lpt_strain_kernel(const typename Real<T>::T2* __restrict__ modes, T inv_cell_vol,
+                                  typename Real<T>::T2* __restrict__ pot1, typename Real<T>::T2* __restrict__ strains,
+                                  Mesh3 m, const T* __restrict__ tab, T inv_n) {
+  using R = Real<T>;
+  const LptTables<T> t = lpt_tables(tab, m);
   const int64_t total = m.half_cells();
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
     const Idx3 q = unravel_half(j, m);
-    float2 v = modes[j];
-    v.x = __fmul_rn(v.x, inv_cell_vol);
-    v.y = __fmul_rn(v.y, inv_cell_vol);
-    const float2 p = pot_from(v, k2_at(t, q));
+    typename R::T2 v = modes[j];
+    v.x = R::mul(v.x, inv_cell_vol);
+    v.y = R::mul(v.y, inv_cell_vol);
+    const typename R::T2 p = pot_from<T>(v, k2_at(t, q));
     pot1[j] = p;
-    const float k[3] = {t.kx[q.ix], t.ky[q.iy], t.kz[q.iz]};
+    const T k[3] = {t.kx[q.ix], t.ky[q.iy], t.kz[q.iz]};
     // Nyquist-zeroed k is -c
-    const float kz0[3] = {-t.cx[q.ix], -t.cy[q.iy], -t.cz[q.iz]};
+    const T kz0[3] = {-t.cx[q.ix], -t.cy[q.iy], -t.cz[q.iz]};
     const int pi[6] = {0, 1, 2, 0, 0, 1}, pj[6] = {0, 1, 2, 1, 2, 2};
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
-      const float ki = s < 3 ? k[pi[s]] : kz0[pi[s]];
-      const float kj = s < 3 ? k[pj[s]] : kz0[pj[s]];
-      const float f = __fmul_rn(__fmul_rn(-ki, kj), inv_n);
-      strains[(int64_t)s * total + j] = make_float2(__fmul_rn(p.x, f), __fmul_rn(p.y, f));
+      const T ki = s < 3 ? k[pi[s]] : kz0[pi[s]];
+      const T kj = s < 3 ? k[pj[s]] : kz0[pj[s]];
+      const T f = R::mul(R::mul(-ki, kj), inv_n);
+      strains[(int64_t)s * total + j] = R::make2(R::mul(p.x, f), R::mul(p.y, f));
     }
   }
 }
 
-// 2LPT source sum_{i<j} phi_ii phi_jj - phi_ij^2 (lpt.py:263-299), float,
-// summation order of the reference loops.
-__global__ void lpt_source_kernel(const float* __restrict__ s6, float* __restrict__ L, int64_t n) {
+// 2LPT source sum_{i<j} phi_ii phi_jj - phi_ij^2 (lpt.py:263-299), summation
+// order of the reference loops.
+template <class T>
+__global__ void lpt_source_kernel(const T* __restrict__ s6, T* __restrict__ L, int64_t n) {
+  using R = Real<T>;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const float d0 = s6[i], d1 = s6[n + i], d2 = s6[2 * n + i];
-    const float s01 = s6[3 * n + i], s02 = s6[4 * n + i], s12 = s6[5 * n + i];
-    float l = 0.f;
-    l = __fadd_rn(l, __fmul_rn(d0, d2));
-    l = __fadd_rn(l, __fmul_rn(d0, d1));
-    l = __fadd_rn(l, __fmul_rn(d1, d2));
-    l = __fsub_rn(l, __fmul_rn(s01, s01));
-    l = __fsub_rn(l, __fmul_rn(s02, s02));
-    l = __fsub_rn(l, __fmul_rn(s12, s12));
+    const T d0 = s6[i], d1 = s6[n + i], d2 = s6[2 * n + i];
+    const T s01 = s6[3 * n + i], s02 = s6[4 * n + i], s12 = s6[5 * n + i];
+    T l = (T)0;
+    l = R::add(l, R::mul(d0, d2));
+    l = R::add(l, R::mul(d0, d1));
+    l = R::add(l, R::mul(d1, d2));
+    l = R::sub(l, R::mul(s01, s01));
+    l = R::sub(l, R::mul(s02, s02));
+    l = R::sub(l, R::mul(s12, s12));
     L[i] = l;
   }
 }
 
 // pot2 = -L_hat / k^2, then the six gradient spectra (i c_d) pot_m * inv_n
 // for m = 1 (from pot1) and m = 2 (from pot2), layout [m][d].
-__global__ void lpt_gradient_kernel(const float2* __restrict__ pot1, const float2* __restrict__ L_hat,
-                                    float2* __restrict__ grads, Mesh3 m, const float* __restrict__ tab, float inv_n) {
-  const LptTables t = lpt_tables(tab, m);
+template <class T>
+__global__ void lpt_gradient_kernel(const typename Real<T>::T2* __restrict__ pot1,
+                                    const typename Real<T>::T2* __restrict__ L_hat,
+                                    typename Real<T>::T2* __restrict__ grads, Mesh3 m, const T* __restrict__ tab,
+                                    T inv_n) {
+  using R = Real<T>;
+  const LptTables<T> t = lpt_tables(tab, m);
   const int64_t total = m.half_cells();
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
     const Idx3 q = unravel_half(j, m);
-    const float2 p1 = pot1[j];
-    const float2 p2 = L_hat != nullptr ? pot_from(L_hat[j], k2_at(t, q)) : make_float2(0.f, 0.f);
-    const float c[3] = {t.cx[q.ix], t.cy[q.iy], t.cz[q.iz]};
+    const typename R::T2 p1 = pot1[j];
+    const typename R::T2 p2 = L_hat != nullptr ? pot_from<T>(L_hat[j], k2_at(t, q)) : R::make2((T)0, (T)0);
+    const T c[3] = {t.cx[q.ix], t.cy[q.iy], t.cz[q.iz]};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      grads[(int64_t)d * total + j] =
-          make_float2(__fmul_rn(-__fmul_rn(c[d], p1.y), inv_n), __fmul_rn(__fmul_rn(c[d], p1.x), inv_n));
+      grads[(int64_t)d * total + j] = R::make2(R::mul(-R::mul(c[d], p1.y), inv_n), R::mul(R::mul(c[d], p1.x), inv_n));
       grads[(int64_t)(3 + d) * total + j] =
-          make_float2(__fmul_rn(-__fmul_rn(c[d], p2.y), inv_n), __fmul_rn(__fmul_rn(c[d], p2.x), inv_n));
+          R::make2(R::mul(-R::mul(c[d], p2.y), inv_n), R::mul(R::mul(c[d], p2.x), inv_n));
     }
   }
 }
@@ -251,27 +288,29 @@ __global__ void lpt_gradient_kernel(const float2* __restrict__ pot1, const float
 // Sample the gradient fields at the particles' Lagrangian grid points
 // (lpt.py:46-62: rint((pmid*cell + disp)/spacing) mod grid) and apply
 // disp += D_m g_m, vel += a^2 H D'_m g_m for m = 1..order (lpt.py:412-431).
-__global__ void lpt_displace_kernel(const int16_t* __restrict__ pmid, float* __restrict__ disp, float* __restrict__ vel,
-                                    int64_t n, Mesh3 g, float cell, float spacing, const float* __restrict__ fields,
-                                    int order, float D1, float V1, float D2, float V2, int64_t* __restrict__ index_out) {
+template <class T>
+__global__ void lpt_displace_kernel(const int16_t* __restrict__ pmid, T* __restrict__ disp, T* __restrict__ vel,
+                                    int64_t n, Mesh3 g, T cell, T spacing, const T* __restrict__ fields, int order,
+                                    T D1, T V1, T D2, T V2, int64_t* __restrict__ index_out) {
+  using R = Real<T>;
   const int64_t ng = g.cells();
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
     int c[3];
     const int dims[3] = {g.nx, g.ny, g.nz};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float x = __fadd_rn(__fmul_rn((float)pmid[3 * p + a], cell), disp[3 * p + a]);
-      c[a] = pmod((int)rintf(__fdiv_rn(x, spacing)), dims[a]);
+      const T x = R::add(R::mul((T)pmid[3 * p + a], cell), disp[3 * p + a]);
+      c[a] = pmod((int)R::rint_(R::div(x, spacing)), dims[a]);
     }
     const int64_t idx = ((int64_t)c[0] * g.ny + c[1]) * g.nz + c[2];
     if (index_out != nullptr) index_out[p] = idx;
-    const float Ds[2] = {D1, D2}, Vs[2] = {V1, V2};
+    const T Ds[2] = {D1, D2}, Vs[2] = {V1, V2};
     for (int mo = 0; mo < order; ++mo) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const float gv = fields[(int64_t)(3 * mo + d) * ng + idx];
-        disp[3 * p + d] = __fadd_rn(disp[3 * p + d], __fmul_rn(Ds[mo], gv));
-        vel[3 * p + d] = __fadd_rn(vel[3 * p + d], __fmul_rn(Vs[mo], gv));
+        const T gv = fields[(int64_t)(3 * mo + d) * ng + idx];
+        disp[3 * p + d] = R::add(disp[3 * p + d], R::mul(Ds[mo], gv));
+        vel[3 * p + d] = R::add(vel[3 * p + d], R::mul(Vs[mo], gv));
       }
     }
   }
@@ -279,20 +318,21 @@ __global__ void lpt_displace_kernel(const int16_t* __restrict__ pmid, float* __r
 
 int lpt_strains(const float2* modes, float inv_cell_vol, float2* pot1, float2* strains, Mesh3 m, const float* tab,
                 float inv_n, cudaStream_t s) {
-  lpt_strain_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(modes, inv_cell_vol, pot1, strains, m, tab, inv_n);
+  lpt_strain_kernel<float><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(modes, inv_cell_vol, pot1, strains, m, tab,
+                                                                         inv_n);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }
 
 int lpt_source(const float* s6, float* L, int64_t n, cudaStream_t s) {
-  lpt_source_kernel<<<grid_for(n, 256), 256, 0, s>>>(s6, L, n);
+  lpt_source_kernel<float><<<grid_for(n, 256), 256, 0, s>>>(s6, L, n);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }
 
 int lpt_gradients(const float2* pot1, const float2* L_hat, float2* grads, Mesh3 m, const float* tab, float inv_n,
                   cudaStream_t s) {
-  lpt_gradient_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(pot1, L_hat, grads, m, tab, inv_n);
+  lpt_gradient_kernel<float><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(pot1, L_hat, grads, m, tab, inv_n);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }
@@ -300,8 +340,37 @@ int lpt_gradients(const float2* pot1, const float2* L_hat, float2* grads, Mesh3 
 int lpt_displace(const int16_t* pmid, float* disp, float* vel, int64_t n, Mesh3 g, float cell, float spacing,
                  const float* fields, int order, float D1, float V1, float D2, float V2, int64_t* index_out,
                  cudaStream_t s) {
-  lpt_displace_kernel<<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, vel, n, g, cell, spacing, fields, order, D1, V1,
-                                                        D2, V2, index_out);
+  lpt_displace_kernel<float><<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, vel, n, g, cell, spacing, fields, order, D1,
+                                                               V1, D2, V2, index_out);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int lpt_strains64(const double2* modes, double inv_cell_vol, double2* pot1, double2* strains, Mesh3 m,
+                  const double* tab, double inv_n, cudaStream_t s) {
+  lpt_strain_kernel<double><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(modes, inv_cell_vol, pot1, strains, m, tab,
+                                                                          inv_n);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int lpt_source64(const double* s6, double* L, int64_t n, cudaStream_t s) {
+  lpt_source_kernel<double><<<grid_for(n, 256), 256, 0, s>>>(s6, L, n);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int lpt_gradients64(const double2* pot1, const double2* L_hat, double2* grads, Mesh3 m, const double* tab,
+                    double inv_n, cudaStream_t s) {
+  lpt_gradient_kernel<double><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(pot1, L_hat, grads, m, tab, inv_n);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int lpt_displace64(const int16_t* pmid, double* disp, double* vel, int64_t n, Mesh3 g, double cell, double spacing,
+                   const double* fields, int order, double D1, double V1, double D2, double V2, cudaStream_t s) {
+  lpt_displace_kernel<double><<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, vel, n, g, cell, spacing, fields, order,
+                                                                D1, V1, D2, V2, nullptr);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }
@@ -342,7 +411,7 @@ __global__ void lpt_field_cot_kernel(const int64_t* __restrict__ index, const fl
 // second-order gradient stage; F2 = rFFT of the order-2 field cotangents.
 __global__ void lpt_grad2_adjoint_kernel(const float2* __restrict__ F2, float2* __restrict__ out, Mesh3 m,
                                          const float* __restrict__ tab, float post) {
-  const LptTables t = lpt_tables(tab, m);
+  const LptTables<float> t = lpt_tables(tab, m);
   const int64_t total = m.half_cells();
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
     const Idx3 q = unravel_half(j, m);
@@ -354,7 +423,7 @@ __global__ void lpt_grad2_adjoint_kernel(const float2* __restrict__ F2, float2* 
       ar = __fadd_rn(ar, __fmul_rn(c[d], a.y));
       ai = __fsub_rn(ai, __fmul_rn(c[d], a.x));
     }
-    const float2 p = pot_from(make_float2(ar, ai), k2_at(t, q));
+    const float2 p = pot_from<float>(make_float2(ar, ai), k2_at(t, q));
     out[j] = make_float2(__fmul_rn(p.x, post), __fmul_rn(p.y, post));
   }
 }
@@ -380,7 +449,7 @@ __global__ void lpt_source_adjoint_kernel(const float* __restrict__ s6, const fl
 __global__ void lpt_modes_adjoint_kernel(const float2* __restrict__ F1, const float2* __restrict__ FS,
                                          const float* __restrict__ amp, float2* __restrict__ out, Mesh3 m,
                                          const float* __restrict__ tab, float scale) {
-  const LptTables t = lpt_tables(tab, m);
+  const LptTables<float> t = lpt_tables(tab, m);
   const int64_t total = m.half_cells();
   const int nzh = m.nz / 2 + 1;
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
@@ -410,7 +479,7 @@ __global__ void lpt_modes_adjoint_kernel(const float2* __restrict__ F1, const fl
       }
     }
     const float mult = (q.iz == 0 || ((m.nz % 2 == 0) && q.iz == nzh - 1)) ? 1.0f : 2.0f;
-    float2 p = pot_from(make_float2(ar, ai), k2_at(t, q));
+    float2 p = pot_from<float>(make_float2(ar, ai), k2_at(t, q));
     float f = __fmul_rn(scale, mult);
     if (amp != nullptr) f = __fmul_rn(f, amp[j]);
     out[j] = make_float2(__fmul_rn(p.x, f), __fmul_rn(p.y, f));
@@ -450,10 +519,12 @@ int lpt_modes_adjoint(const float2* F1, const float2* FS, const float* amp, floa
 // ---------------------------------------------------------------------------
 // shell = floor(sqrt(n^2) + 1e-9) clipped, weight = |d|^2 * W^-2p * mult in
 // float (W = product of per-axis sinc(n/M) tables), summed in FP64.
-__global__ void pk_shells_kernel(const float2* __restrict__ spec, Mesh3 m, const float* __restrict__ sinc_tab,
+template <class T>
+__global__ void pk_shells_kernel(const typename Real<T>::T2* __restrict__ spec, Mesh3 m, const T* __restrict__ sinc_tab,
                                  int mas_power, int num_shells, double* __restrict__ sums,
-                                 const float2* __restrict__ spec_b, double* __restrict__ sums_b,
+                                 const typename Real<T>::T2* __restrict__ spec_b, double* __restrict__ sums_b,
                                  double* __restrict__ sums_x) {
+  using R = Real<T>;
   extern __shared__ double sh[];
   double* shA = sh;
   double* shB = sh + num_shells;
@@ -462,9 +533,9 @@ __global__ void pk_shells_kernel(const float2* __restrict__ spec, Mesh3 m, const
   const int nsh = cross ? 3 * num_shells : num_shells;
   for (int t = threadIdx.x; t < nsh; t += blockDim.x) sh[t] = 0.0;
   __syncthreads();
-  const float* sx = sinc_tab;
-  const float* sy = sx + m.nx;
-  const float* sz = sy + m.ny;
+  const T* sx = sinc_tab;
+  const T* sy = sx + m.nx;
+  const T* sz = sy + m.ny;
   const int64_t total = m.half_cells();
   const int nzh = m.nz / 2 + 1;
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
@@ -473,21 +544,21 @@ __global__ void pk_shells_kernel(const float2* __restrict__ spec, Mesh3 m, const
     const long long n2 = mx * mx + my * my + mz * mz;
     int shell = (int)floor(sqrt((double)n2) + 1e-9);
     if (shell > num_shells - 1) shell = num_shells - 1;
-    const float mult = (q.iz == 0 || ((m.nz % 2 == 0) && q.iz == nzh - 1)) ? 1.0f : 2.0f;
-    float deconv = 1.0f;
+    const T mult = (q.iz == 0 || ((m.nz % 2 == 0) && q.iz == nzh - 1)) ? (T)1 : (T)2;
+    T deconv = (T)1;
     if (mas_power > 0) {
-      const float w = __fmul_rn(__fmul_rn(sx[q.ix], sy[q.iy]), sz[q.iz]);
-      deconv = powf(w, (float)(-2 * mas_power));
+      const T w = R::mul(R::mul(sx[q.ix], sy[q.iy]), sz[q.iz]);
+      deconv = R::pow_(w, (T)(-2 * mas_power));
     }
-    const float2 a = spec[j];
-    const float pa = __fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y));
-    atomicAdd(&shA[shell], (double)__fmul_rn(__fmul_rn(pa, deconv), mult));
+    const typename R::T2 a = spec[j];
+    const T pa = R::add(R::mul(a.x, a.x), R::mul(a.y, a.y));
+    atomicAdd(&shA[shell], (double)R::mul(R::mul(pa, deconv), mult));
     if (cross) {
-      const float2 b = spec_b[j];
-      const float pb = __fadd_rn(__fmul_rn(b.x, b.x), __fmul_rn(b.y, b.y));
-      const float px = __fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
-      atomicAdd(&shB[shell], (double)__fmul_rn(__fmul_rn(pb, deconv), mult));
-      atomicAdd(&shX[shell], (double)__fmul_rn(__fmul_rn(px, deconv), mult));
+      const typename R::T2 b = spec_b[j];
+      const T pb = R::add(R::mul(b.x, b.x), R::mul(b.y, b.y));
+      const T px = R::add(R::mul(a.x, b.x), R::mul(a.y, b.y));
+      atomicAdd(&shB[shell], (double)R::mul(R::mul(pb, deconv), mult));
+      atomicAdd(&shX[shell], (double)R::mul(R::mul(px, deconv), mult));
     }
   }
   __syncthreads();
@@ -507,13 +578,32 @@ int pk_shells(const float2* spec, Mesh3 m, const float* sinc_tab, int mas_power,
   if (smem > 200 * 1024) return kUnsupported;
   static bool attr = false;
   if (!attr) {
-    PMB_CUDA_CHECK(cudaFuncSetAttribute(pk_shells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    PMB_CUDA_CHECK(cudaFuncSetAttribute(pk_shells_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        200 * 1024));
     attr = true;
   }
   int64_t b = (m.half_cells() + 255) / 256;
   if (b > 148 * 8) b = 148 * 8;
-  pk_shells_kernel<<<(unsigned)(b > 0 ? b : 1), 256, smem, s>>>(spec, m, sinc_tab, mas_power, num_shells, sums,
-                                                                spec_b, sums_b, sums_x);
+  pk_shells_kernel<float><<<(unsigned)(b > 0 ? b : 1), 256, smem, s>>>(spec, m, sinc_tab, mas_power, num_shells, sums,
+                                                                       spec_b, sums_b, sums_x);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int pk_shells64(const double2* spec, Mesh3 m, const double* sinc_tab, int mas_power, int num_shells, double* sums,
+                cudaStream_t s) {
+  const size_t smem = sizeof(double) * num_shells;
+  if (smem > 200 * 1024) return kUnsupported;
+  static bool attr = false;
+  if (!attr) {
+    PMB_CUDA_CHECK(cudaFuncSetAttribute(pk_shells_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        200 * 1024));
+    attr = true;
+  }
+  int64_t b = (m.half_cells() + 255) / 256;
+  if (b > 148 * 8) b = 148 * 8;
+  pk_shells_kernel<double><<<(unsigned)(b > 0 ? b : 1), 256, smem, s>>>(spec, m, sinc_tab, mas_power, num_shells,
+                                                                        sums, nullptr, nullptr, nullptr);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }
@@ -595,15 +685,23 @@ int shell_stats(Mesh3 m, int num_shells, double* counts, double* ksum, cudaStrea
 }
 
 // delta = rho / mean - 1 (power_spectrum.py:371-374), mean from an FP64 sum.
-__global__ void overdensity_kernel(const float* __restrict__ rho, float* __restrict__ delta, int64_t n,
+template <class T>
+__global__ void overdensity_kernel(const T* __restrict__ rho, T* __restrict__ delta, int64_t n,
                                    const double* __restrict__ total) {
-  const float mean = (float)(*total / (double)n);
+  using R = Real<T>;
+  const T mean = (T)(*total / (double)n);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    delta[i] = __fsub_rn(__fdiv_rn(rho[i], mean), 1.0f);
+    delta[i] = R::sub(R::div(rho[i], mean), (T)1);
 }
 
 int overdensity(const float* rho, float* delta, int64_t n, const double* total, cudaStream_t s) {
-  overdensity_kernel<<<grid_for(n, 256), 256, 0, s>>>(rho, delta, n, total);
+  overdensity_kernel<float><<<grid_for(n, 256), 256, 0, s>>>(rho, delta, n, total);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int overdensity64(const double* rho, double* delta, int64_t n, const double* total, cudaStream_t s) {
+  overdensity_kernel<double><<<grid_for(n, 256), 256, 0, s>>>(rho, delta, n, total);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }

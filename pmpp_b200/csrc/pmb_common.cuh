@@ -54,6 +54,46 @@ __device__ __forceinline__ float axis_sign(float f, int b) {
   return d < 0.0f ? 1.0f : (d > 0.0f ? -1.0f : 0.0f);
 }
 
+// Correctly rounded arithmetic and math of the float32 kernels and of their
+// float64 instantiations (the reference's x64 build), so one kernel source
+// serves both precisions with the float path unchanged.
+template <class T>
+struct Real;
+template <>
+struct Real<float> {
+  using T2 = float2;
+  __device__ static __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  __device__ static __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+  __device__ static __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  __device__ static __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+  __device__ static __forceinline__ float sqrt_(float a) { return sqrtf(a); }
+  __device__ static __forceinline__ float log_(float a) { return logf(a); }
+  __device__ static __forceinline__ float cos_(float a) { return cosf(a); }
+  __device__ static __forceinline__ float sin_(float a) { return sinf(a); }
+  __device__ static __forceinline__ float floor_(float a) { return floorf(a); }
+  __device__ static __forceinline__ float fabs_(float a) { return fabsf(a); }
+  __device__ static __forceinline__ float rint_(float a) { return rintf(a); }
+  __device__ static __forceinline__ float pow_(float a, float b) { return powf(a, b); }
+  __device__ static __forceinline__ float2 make2(float a, float b) { return make_float2(a, b); }
+};
+template <>
+struct Real<double> {
+  using T2 = double2;
+  __device__ static __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  __device__ static __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  __device__ static __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  __device__ static __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+  __device__ static __forceinline__ double sqrt_(double a) { return sqrt(a); }
+  __device__ static __forceinline__ double log_(double a) { return log(a); }
+  __device__ static __forceinline__ double cos_(double a) { return cos(a); }
+  __device__ static __forceinline__ double sin_(double a) { return sin(a); }
+  __device__ static __forceinline__ double floor_(double a) { return floor(a); }
+  __device__ static __forceinline__ double fabs_(double a) { return fabs(a); }
+  __device__ static __forceinline__ double rint_(double a) { return rint(a); }
+  __device__ static __forceinline__ double pow_(double a, double b) { return pow(a, b); }
+  __device__ static __forceinline__ double2 make2(double a, double b) { return make_double2(a, b); }
+};
+
 // Sorted particle record: fractions along x, y, z and the raveled lower cell.
 struct __align__(16) Rec {
   float fx, fy, fz;

@@ -11,7 +11,7 @@ struct LinearPowerParams {
   double n_s;
   double pi_c2_over_om;  // pi (c/H0)^2 / Omega_m
   double growth2;        // D(a)^2, or 1 without growth
-  float box_vol;
+  double box_vol;        // rounded to the working precision by the kernel
 };
 
 int white_noise(uint32_t seed, Mesh3 m, float2* out, uint32_t* hashes, cudaStream_t s);
@@ -38,5 +38,20 @@ int pk_shells_adjoint(const float2* spec, Mesh3 m, const float* sinc_tab, int ma
                       const double* wshell, float post, float2* out, cudaStream_t s);
 int overdensity(const float* rho, float* delta, int64_t n, const double* total, cudaStream_t s);
 int shell_stats(Mesh3 m, int num_shells, double* counts, double* ksum, cudaStream_t s);
+
+// float64 instantiations of the same kernels (the reference's x64 build)
+int white_noise64(uint32_t seed, Mesh3 m, double2* out, cudaStream_t s);
+int linear_modes64(const double2* in, double2* out, Mesh3 m, const double* ktab, const double* tk, const double* tt,
+                   int ntab, LinearPowerParams p, cudaStream_t s);
+int lpt_strains64(const double2* modes, double inv_cell_vol, double2* pot1, double2* strains, Mesh3 m,
+                  const double* tab, double inv_n, cudaStream_t s);
+int lpt_source64(const double* s6, double* L, int64_t n, cudaStream_t s);
+int lpt_gradients64(const double2* pot1, const double2* L_hat, double2* grads, Mesh3 m, const double* tab,
+                    double inv_n, cudaStream_t s);
+int lpt_displace64(const int16_t* pmid, double* disp, double* vel, int64_t n, Mesh3 g, double cell, double spacing,
+                   const double* fields, int order, double D1, double V1, double D2, double V2, cudaStream_t s);
+int pk_shells64(const double2* spec, Mesh3 m, const double* sinc_tab, int mas_power, int num_shells, double* sums,
+                cudaStream_t s);
+int overdensity64(const double* rho, double* delta, int64_t n, const double* total, cudaStream_t s);
 
 }  // namespace pmb

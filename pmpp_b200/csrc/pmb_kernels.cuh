@@ -31,6 +31,9 @@ void set_gather_staging(int mode);
 int fft_r2c(Mesh3 m, int batch, float* in, float2* out, void* work, cudaStream_t s);
 int fft_c2r(Mesh3 m, int batch, float2* in, float* out, void* work, cudaStream_t s);
 int64_t fft_work_bytes(Mesh3 m, int batch);
+int64_t fft_work_bytes64(Mesh3 m, int batch);
+int fft_d2z(Mesh3 m, int batch, double* in, double2* out, void* work, cudaStream_t s);
+int fft_z2d(Mesh3 m, int batch, double2* in, double* out, void* work, cudaStream_t s);
 // Gravity spectral multipliers (see spectral.cu for the exact semantics).
 struct GreenParams {
   int green_kernel;     // 0 continuum -1/k^2, 1 discrete Laplacian

@@ -63,10 +63,13 @@ int get_plan(Mesh3 m, int batch, int kind, PlanVal* out) {
   long long cdist = (long long)m.half_cells();
   size_t work = 0;
   cufftResult r;
-  if (kind == 0) {
-    r = cufftMakePlanMany64(h, 3, n, nullptr, 1, rdist, nullptr, 1, cdist, CUFFT_R2C, batch, &work);
+  // kind 0 R2C, 1 C2R (float32); 2 D2Z, 3 Z2D (float64)
+  if (kind == 0 || kind == 2) {
+    r = cufftMakePlanMany64(h, 3, n, nullptr, 1, rdist, nullptr, 1, cdist, kind == 0 ? CUFFT_R2C : CUFFT_D2Z, batch,
+                            &work);
   } else {
-    r = cufftMakePlanMany64(h, 3, n, nullptr, 1, cdist, nullptr, 1, rdist, CUFFT_C2R, batch, &work);
+    r = cufftMakePlanMany64(h, 3, n, nullptr, 1, cdist, nullptr, 1, rdist, kind == 1 ? CUFFT_C2R : CUFFT_Z2D, batch,
+                            &work);
   }
   if (r != CUFFT_SUCCESS) {
     cufftDestroy(h);
@@ -85,6 +88,37 @@ int64_t fft_work_bytes(Mesh3 m, int batch) {
   if (get_plan(m, batch, 0, &a) != kOk) return -1;
   if (get_plan(m, batch, 1, &b) != kOk) return -1;
   return (int64_t)(a.work > b.work ? a.work : b.work);
+}
+
+int64_t fft_work_bytes64(Mesh3 m, int batch) {
+  PlanVal a, b;
+  if (get_plan(m, batch, 2, &a) != kOk) return -1;
+  if (get_plan(m, batch, 3, &b) != kOk) return -1;
+  return (int64_t)(a.work > b.work ? a.work : b.work);
+}
+
+int fft_d2z(Mesh3 m, int batch, double* in, double2* out, void* work, cudaStream_t s) {
+  PlanVal p;
+  int st = get_plan(m, batch, 2, &p);
+  if (st != kOk) return st;
+  if (cufftSetStream(p.h, s) != CUFFT_SUCCESS || cufftSetWorkArea(p.h, work) != CUFFT_SUCCESS ||
+      cufftExecD2Z(p.h, in, (cufftDoubleComplex*)out) != CUFFT_SUCCESS) {
+    set_last_error("cufftExecD2Z failed");
+    return kCufftError;
+  }
+  return kOk;
+}
+
+int fft_z2d(Mesh3 m, int batch, double2* in, double* out, void* work, cudaStream_t s) {
+  PlanVal p;
+  int st = get_plan(m, batch, 3, &p);
+  if (st != kOk) return st;
+  if (cufftSetStream(p.h, s) != CUFFT_SUCCESS || cufftSetWorkArea(p.h, work) != CUFFT_SUCCESS ||
+      cufftExecZ2D(p.h, (cufftDoubleComplex*)in, out) != CUFFT_SUCCESS) {
+    set_last_error("cufftExecZ2D failed");
+    return kCufftError;
+  }
+  return kOk;
 }
 
 int fft_r2c(Mesh3 m, int batch, float* in, float2* out, void* work, cudaStream_t s) {

@@ -30,6 +30,8 @@ class LPTResult:
 
 
 def lpt_full(modes, cosmo, conf):
+    if conf.float_dtype != torch.float32:
+        raise NotImplementedError("lpt_full (with adjoint data) exists for the float32 build; use lpt")
     gx, gy, gz = conf.ptcl_grid_shape
     dev = modes.device
     modes = modes.contiguous()
@@ -50,6 +52,9 @@ def lpt_full(modes, cosmo, conf):
 
 def lpt(modes, cosmo, conf):
     """LPT particles at conf.a_start (acc unset)."""
+    if conf.float_dtype == torch.float64:
+        from . import x64
+        return x64.lpt(modes, cosmo, conf)
     return lpt_full(modes, cosmo, conf).ptcl
 
 

@@ -21,8 +21,13 @@ def _grid(conf):
 
 
 def white_noise_nested(seed, conf, real=False, unit_abs=False, device=None, return_hashes=False):
-    """Hashed Gaussian rFFT modes (modes.py:181-268)."""
+    """Hashed Gaussian rFFT modes (modes.py:181-268); complex128 in the float64 build."""
     device = conf.device if device is None else torch.device(device)
+    if conf.float_dtype == torch.float64:
+        if real or unit_abs or return_hashes:
+            raise NotImplementedError("the float64 build returns the complex modes only")
+        from . import x64
+        return x64.white_noise_nested(seed, conf, device)
     gx, gy, gz = _grid(conf)
     out = torch.empty((gx, gy, gz // 2 + 1), dtype=torch.complex64, device=device)
     hashes = torch.empty((gx, gy, gz // 2 + 1, 2), dtype=torch.int32, device=device) if return_hashes else None
@@ -78,6 +83,11 @@ def _linear_call(modes_in, modes_out, amp_out, cosmo, conf, a, transfer=None, om
 
 def linear_modes(modes, cosmo, conf, a=None, real=False):
     """delta(k) = omega(k) sqrt(V P_lin(|k|, a)) (modes.py:397-454)."""
+    if conf.float_dtype == torch.float64:
+        if a is not None or real or not torch.is_complex(modes):
+            raise NotImplementedError("the float64 build takes complex modes at a = 1")
+        from . import x64
+        return x64.linear_modes(modes, cosmo, conf)
     if not torch.is_complex(modes):
         modes = rfft3(modes) / np.sqrt(conf.ptcl_num)
     modes = modes.contiguous()

@@ -92,6 +92,11 @@ class NBodyRun:
 
     def forward(self, ptcl, a_nbody=None):
         conf, cosmo = self.conf, self.cosmo
+        if conf.float_dtype == torch.float64:
+            if self.correction is not None:
+                raise NotImplementedError("corrections run in the float32 build")
+            from . import x64
+            return x64.nbody(ptcl, cosmo, conf, a_nbody)
         a = conf.a_nbody if a_nbody is None else np.asarray(a_nbody)
         disp = ptcl.disp.clone()
         vel = ptcl.vel.clone() if ptcl.vel is not None else torch.zeros_like(disp)
@@ -147,11 +152,16 @@ class NBodyRun:
         else:
             force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=corr)
 
+    def _require_f32(self):
+        if self.conf.float_dtype != torch.float32:
+            raise NotImplementedError("the hand-written adjoints exist for the float32 build")
+
     def adjoint(self, ptcl, ptcl_cot, force_meshes=None, a_nbody=None, src_hat=None):
         """Reverse sweep from the final state.  Returns (ptcl_in, ptcl_in_cot, Omega_m_cot).
 
         force_meshes must be the force meshes at ptcl's positions (the
         forward pass leaves them in self.final_meshes)."""
+        self._require_f32()
         conf, cosmo, corr = self.conf, self.cosmo, self.correction
         a = conf.a_nbody if a_nbody is None else np.asarray(a_nbody)
         dev = ptcl.disp.device

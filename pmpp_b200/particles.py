@@ -38,7 +38,7 @@ class Particles:
             p = torch.round(torch.linspace(0, sm, sp + 1, dtype=torch.float64, device=device)[:-1]).to(torch.int64)
             d = (torch.arange(sp, device=device, dtype=torch.int64) * sm - p * sp).to(torch.float64) * (conf.cell_size / sp)
             pm.append(p.to(torch.int16))
-            dp.append(d.to(torch.float32))
+            dp.append(d.to(conf.float_dtype))
         pmid = torch.stack(torch.meshgrid(*pm, indexing="ij"), dim=-1).reshape(-1, 3).contiguous()
         disp = torch.stack(torch.meshgrid(*dp, indexing="ij"), dim=-1).reshape(-1, 3).contiguous()
         z = torch.zeros_like(disp)

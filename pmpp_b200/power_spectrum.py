@@ -115,10 +115,16 @@ def _overdensity(density, conf):
 
 
 def density_to_pk(density, conf, mas="CIC"):
+    if conf.float_dtype == torch.float64:
+        from . import x64
+        return x64.density_to_pk(density, conf, _mas(mas))
     return delta_to_pk(_overdensity(density, conf), conf, mas)
 
 
 def particles_to_pk(ptcl, conf, mas="CIC"):
+    if conf.float_dtype == torch.float64:
+        from . import x64
+        return x64.particles_to_pk(ptcl, conf, _mas(mas))
     sp = SortedParticles(ptcl.pmid, ptcl.disp, conf)
     return density_to_pk(sp.scatter()[0], conf, mas)
 
