@@ -44,38 +44,6 @@ def parse():
 
 
 # --------------------------------------------------------------------------
-# distributed plumbing (replicas only: every rank runs its own simulation)
-# --------------------------------------------------------------------------
-def dist_init(n):
-    import torch
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
-    return rank, world, local
-
-
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
-def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-# --------------------------------------------------------------------------
 # clocks sampled during the timed region
 # --------------------------------------------------------------------------
 class ClockSampler:
@@ -200,9 +168,12 @@ def run_reference(args):
 def run_ours(args):
     import torch
 
-    rank, world, local = dist_init(args.gpus)
+    from pmpp_b200 import replicas
+    rank, world, local = replicas.setup("nccl")
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    barrier = lambda w: replicas.barrier(w)
+    max_over_ranks = replicas.max_over_ranks
     import pmpp_b200 as pb
     from pmpp_b200 import _lib
     from pmpp_b200.runtime import StageTimer
@@ -216,7 +187,7 @@ def run_ours(args):
     M = conf.mesh_size
     from pmpp_b200 import modes as pmodes
     from pmpp_b200 import pipeline
-    omega = pmodes.white_noise_nested(1 + rank, conf)
+    omega = pmodes.white_noise_nested(replicas.replica_seed(1, rank), conf)
     model = pipeline.ForwardModel(conf, cos)
     # fixed target spectrum: the first run's P(k) modulated by 10%
     with StageTimer():
@@ -277,9 +248,7 @@ def run_ours(args):
     d2h = int(h_grad.numel() * 8 + 3 * 8 + len(target) * 8)
 
     if rank != 0:
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        replicas.teardown(world)
         return
 
     peak, peak_kind = load_peaks()
@@ -329,9 +298,7 @@ def run_ours(args):
         "learned": learned,
     }
     print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.teardown(world)
 
 
 def main():

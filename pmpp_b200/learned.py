@@ -14,6 +14,10 @@ plain and the learned coarse runs, and the GPU time of a learned 128^3 run
 against a plain 384^3 run.
 
     python -m pmpp_b200.learned --train 64 --test 16 --iters 300 --out learned.json
+
+Under torchrun the training seeds are split across ranks (one GPU each) and
+the MLP gradient is averaged over ranks every step (the one all-reduce of the
+replicated path); rank 0 evaluates and writes the results.
 """
 from __future__ import annotations
 
@@ -139,18 +143,22 @@ def main(argv=None):
     ap.add_argument("--kmax", type=float, default=0.5)
     ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
+    from . import replicas
+    rank, world, _ = replicas.setup()
     coarse, fine = configs(args.nsteps)
     t0 = time.time()
-    samples = [Sample(s, coarse, fine) for s in range(args.train + args.test)]
-    targets = []
-    for smp in samples:
+    mine = [s for s in range(args.train) if s % world == rank]
+    ids = mine + (list(range(args.train, args.train + args.test)) if rank == 0 else [])
+    samples = {s: Sample(s, coarse, fine) for s in ids}
+    targets = {}
+    for s, smp in samples.items():
         _, out = run_forward(smp, fine, smp.cos_f)
-        targets.append((pk_of(out.disp, coarse), density(out.disp, coarse)))
+        targets[s] = (pk_of(out.disp, coarse), density(out.disp, coarse))
     t_data = time.time() - t0
-    model = LearnedGreen("cuda", seed=0)
+    model = LearnedGreen("cuda", seed=0)  # identical initial parameters on every rank
     history = []
     for it in range(args.iters):
-        i = it % args.train
+        i = mine[it % len(mine)]
         smp = samples[i]
         run, out = run_forward(smp, coarse, smp.cos_c, model)
         fin = Particles(coarse, Particles.gen_grid(coarse, device=out.disp.device).pmid, out.disp, out.vel, out.acc)
@@ -158,9 +166,13 @@ def main(argv=None):
         model.zero_grad()
         z = torch.zeros_like(g)
         run.adjoint(fin, Particles(coarse, fin.pmid, g, z, z.clone()))
+        replicas.average_gradient(model.grad, world)
         model.adam_step(lr=args.lr * (0.5 if it > 0.6 * args.iters else 1.0), clip=10.0)
         history.append(float(loss))
     t_train = time.time() - t0 - t_data
+    if rank != 0:
+        replicas.teardown(world)
+        return None
 
     def errs(disp, target):
         k, pk, n = pk_of(disp, coarse)
@@ -170,7 +182,8 @@ def main(argv=None):
         return float(np.max(np.abs(ratio - 1))), float(np.min(r[ka <= args.kmax]))
 
     evals = []
-    for smp, tgt in zip(samples[args.train:], targets[args.train:]):
+    test_ids = range(args.train, args.train + args.test)
+    for smp, tgt in zip((samples[s] for s in test_ids), (targets[s] for s in test_ids)):
         _, plain = run_forward(smp, coarse, smp.cos_c)
         _, learn = run_forward(smp, coarse, smp.cos_c, model)
         ep, rp = errs(plain.disp, tgt)
@@ -186,7 +199,7 @@ def main(argv=None):
     res = {
         "config": {"particles": NP**3, "box": BOX, "coarse_mesh": coarse.mesh_shape[0], "fine_mesh": fine.mesh_shape[0],
                    "kdk_steps": args.nsteps, "train_seeds": args.train, "test_seeds": args.test,
-                   "iters": args.iters, "kmax": args.kmax},
+                   "iters": args.iters, "kmax": args.kmax, "ranks": world},
         "train_loss_first": history[:5], "train_loss_last": history[-5:],
         "test": evals,
         "test_mean_max_pk_err": {"plain": float(np.mean([e["plain_max_pk_err"] for e in evals])),
@@ -201,6 +214,7 @@ def main(argv=None):
         np.save(args.out.replace(".json", "_params.npy"), model.parameters().cpu().numpy().astype(np.float32))
     print(json.dumps({k: res[k] for k in ("test_mean_max_pk_err", "time_ms", "wall_s", "train_loss_first",
                                           "train_loss_last")}))
+    replicas.teardown(world)
     return res
 
 
