@@ -270,9 +270,11 @@ __global__ void __launch_bounds__(256) scatter_pull_kernel(const Rec* __restrict
 }
 
 void scatter_block_shape(Mesh3 m, int C, int* RX, int* RY) {
-  // First of 2x2, 1x2, 1x1 output rows whose accumulator fits in 100 KB
-  // (two or more CTAs per SM; larger blocks measured slower).
-  const int64_t budget = 100 * 1024;
+  // First of 2x2, 1x2, 1x1 output rows whose accumulator fits the budget:
+  // 100 KB for one or two channels, 40 KB for three or four (more resident
+  // blocks beat the extra particle re-reads there; larger blocks measured
+  // slower everywhere).
+  const int64_t budget = (C >= 3 ? 40 : 100) * 1024;
   static const int shapes[3][2] = {{2, 2}, {1, 2}, {1, 1}};
   int rx = 1, ry = 1;
   for (const auto& sh : shapes) {
