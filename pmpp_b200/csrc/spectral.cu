@@ -83,7 +83,10 @@ int get_plan(Mesh3 m, int batch, int kind, PlanVal* out) {
 }
 }  // namespace
 
+static bool split_batches(Mesh3 m);
+
 int64_t fft_work_bytes(Mesh3 m, int batch) {
+  if (batch > 1 && split_batches(m)) batch = 1;
   PlanVal a, b;
   if (get_plan(m, batch, 0, &a) != kOk) return -1;
   if (get_plan(m, batch, 1, &b) != kOk) return -1;
@@ -121,7 +124,19 @@ int fft_z2d(Mesh3 m, int batch, double2* in, double* out, void* work, cudaStream
   return kOk;
 }
 
+// Batched plans of very large meshes measured slower per transform than
+// single transforms (1024^3 on B200: 7.0 ms vs 5.8 ms per R2C, 7.2 ms vs
+// 6.0 ms per C2R), so batches of such meshes run one transform at a time.
+static bool split_batches(Mesh3 m) { return m.cells() > ((int64_t)1 << 27); }
+
 int fft_r2c(Mesh3 m, int batch, float* in, float2* out, void* work, cudaStream_t s) {
+  if (batch > 1 && split_batches(m)) {
+    for (int b = 0; b < batch; ++b) {
+      const int st = fft_r2c(m, 1, in + (int64_t)b * m.cells(), out + (int64_t)b * m.half_cells(), work, s);
+      if (st != kOk) return st;
+    }
+    return kOk;
+  }
   PlanVal p;
   int st = get_plan(m, batch, 0, &p);
   if (st != kOk) return st;
@@ -134,6 +149,13 @@ int fft_r2c(Mesh3 m, int batch, float* in, float2* out, void* work, cudaStream_t
 }
 
 int fft_c2r(Mesh3 m, int batch, float2* in, float* out, void* work, cudaStream_t s) {
+  if (batch > 1 && split_batches(m)) {
+    for (int b = 0; b < batch; ++b) {
+      const int st = fft_c2r(m, 1, in + (int64_t)b * m.half_cells(), out + (int64_t)b * m.cells(), work, s);
+      if (st != kOk) return st;
+    }
+    return kOk;
+  }
   PlanVal p;
   int st = get_plan(m, batch, 1, &p);
   if (st != kOk) return st;
