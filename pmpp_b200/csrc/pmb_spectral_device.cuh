@@ -34,13 +34,10 @@ __device__ __forceinline__ float transfer_of(const GreenParams& g, const SpecTab
   return T;
 }
 
-// Half-spectrum cell j = (ix*ny + iy)*(nz/2+1) + iz of the forward
-// multiplier: three gradient spectra (channel stride `total`) from one
-// source spectrum.
-__device__ __forceinline__ void green_gradient_at(const float2* __restrict__ src, float2* __restrict__ grad, int64_t j,
-                                                  int64_t total, int ix, int iy, int iz, Mesh3 m, const SpecTables& t,
-                                                  const GreenParams& g) {
-  float2 v = src[j];
+// Forward multiplier at half-spectrum cell j = (ix*ny + iy)*(nz/2+1) + iz:
+// the three gradient values from the source value v.
+__device__ __forceinline__ void green_gradient_value(float2 v, int64_t j, int ix, int iy, int iz, Mesh3 m,
+                                                     const SpecTables& t, const GreenParams& g, float2 out[3]) {
   if (t.mx != nullptr) {
     const float mk = __fmul_rn(__fmul_rn(t.mx[ix], t.my[iy]), t.mz[iz]);
     v.x = __fmul_rn(v.x, mk);
@@ -60,23 +57,31 @@ __device__ __forceinline__ void green_gradient_at(const float2* __restrict__ src
   const float c[3] = {t.cx[ix], t.cy[iy], t.cz[iz]};
   const float ps = g.post_scale;
 #pragma unroll
-  for (int d = 0; d < 3; ++d)
-    grad[(int64_t)d * total + j] = make_float2(__fmul_rn(-__fmul_rn(c[d], pi), ps), __fmul_rn(__fmul_rn(c[d], pr), ps));
+  for (int d = 0; d < 3; ++d) out[d] = make_float2(__fmul_rn(-__fmul_rn(c[d], pi), ps), __fmul_rn(__fmul_rn(c[d], pr), ps));
+}
+
+// Half-spectrum cell j of the forward multiplier: three gradient spectra
+// (channel stride `total`) from one source spectrum.
+__device__ __forceinline__ void green_gradient_at(const float2* __restrict__ src, float2* __restrict__ grad, int64_t j,
+                                                  int64_t total, int ix, int iy, int iz, Mesh3 m, const SpecTables& t,
+                                                  const GreenParams& g) {
+  float2 o[3];
+  green_gradient_value(src[j], j, ix, iy, iz, m, t, g, o);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) grad[(int64_t)d * total + j] = o[d];
 }
 
 // Adjoint at half-spectrum cell j: S_cot = K * sum_d conj(i c_d) A_d.  The
 // force map is a real convolution (H_d Hermitian), so its transpose is the
 // correlation with the conjugate multiplier.
-__device__ __forceinline__ void green_gradient_adjoint_at(const float2* __restrict__ gc, float2* __restrict__ out,
-                                                          int64_t j, int64_t total, int ix, int iy, int iz, Mesh3 m,
-                                                          const SpecTables& t, const GreenParams& g) {
+__device__ __forceinline__ float2 green_gradient_adjoint_value(const float2 a[3], int64_t j, int ix, int iy, int iz,
+                                                               Mesh3 m, const SpecTables& t, const GreenParams& g) {
   const float c[3] = {t.cx[ix], t.cy[iy], t.cz[iz]};
   float ar = 0.f, ai = 0.f;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const float2 a = gc[(int64_t)d * total + j];
-    ar = __fadd_rn(ar, __fmul_rn(c[d], a.y));
-    ai = __fsub_rn(ai, __fmul_rn(c[d], a.x));
+    ar = __fadd_rn(ar, __fmul_rn(c[d], a[d].y));
+    ai = __fsub_rn(ai, __fmul_rn(c[d], a[d].x));
   }
   const float k2 = k2_of(t, ix, iy, iz);
   float pr = 0.f, pi = 0.f;
@@ -94,7 +99,14 @@ __device__ __forceinline__ void green_gradient_adjoint_at(const float2* __restri
       pi = __fmul_rn(pi, mk);
     }
   }
-  out[j] = make_float2(__fmul_rn(pr, g.post_scale), __fmul_rn(pi, g.post_scale));
+  return make_float2(__fmul_rn(pr, g.post_scale), __fmul_rn(pi, g.post_scale));
+}
+
+__device__ __forceinline__ void green_gradient_adjoint_at(const float2* __restrict__ gc, float2* __restrict__ out,
+                                                          int64_t j, int64_t total, int ix, int iy, int iz, Mesh3 m,
+                                                          const SpecTables& t, const GreenParams& g) {
+  const float2 a[3] = {gc[j], gc[total + j], gc[2 * total + j]};
+  out[j] = green_gradient_adjoint_value(a, j, ix, iy, iz, m, t, g);
 }
 
 }  // namespace pmb

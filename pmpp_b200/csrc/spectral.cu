@@ -200,6 +200,79 @@ __global__ void green_gradient_adjoint_kernel(const float2* __restrict__ gc, flo
   }
 }
 
+// Four consecutive cells per thread with 32-byte vector loads and stores;
+// the cell coordinates are computed once per group and advanced in place.
+// Needs total % 4 == 0 (and 16-byte aligned spectra, as the workspaces are).
+__device__ __forceinline__ void advance_cell(int& ix, int& iy, int& iz, int nzh, int ny) {
+  if (++iz == nzh) {
+    iz = 0;
+    if (++iy == ny) {
+      iy = 0;
+      ++ix;
+    }
+  }
+}
+
+__global__ void green_gradient_kernel4(const float2* __restrict__ src, float2* __restrict__ grad, Mesh3 m,
+                                       SpecTables t, GreenParams g) {
+  const uint32_t nzh = (uint32_t)(m.nz / 2 + 1), ny = (uint32_t)m.ny;
+  const uint32_t total = (uint32_t)m.half_cells(), groups = total / 4;
+  const float4* s4 = reinterpret_cast<const float4*>(src);
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+    const uint32_t j = 4 * q, r = j / nzh, x = r / ny;
+    int ix = (int)x, iy = (int)(r - x * ny), iz = (int)(j - r * nzh);
+    const float4 a = s4[2 * q], b = s4[2 * q + 1];
+    const float2 v[4] = {make_float2(a.x, a.y), make_float2(a.z, a.w), make_float2(b.x, b.y), make_float2(b.z, b.w)};
+    float2 o[4][3];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      green_gradient_value(v[e], (int64_t)j + e, ix, iy, iz, m, t, g, o[e]);
+      advance_cell(ix, iy, iz, (int)nzh, (int)ny);
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      float4* g4 = reinterpret_cast<float4*>(grad + (int64_t)d * total);
+      g4[2 * q] = make_float4(o[0][d].x, o[0][d].y, o[1][d].x, o[1][d].y);
+      g4[2 * q + 1] = make_float4(o[2][d].x, o[2][d].y, o[3][d].x, o[3][d].y);
+    }
+  }
+}
+
+__global__ void green_gradient_adjoint_kernel4(const float2* __restrict__ gc, float2* __restrict__ out, Mesh3 m,
+                                               SpecTables t, GreenParams g) {
+  const uint32_t nzh = (uint32_t)(m.nz / 2 + 1), ny = (uint32_t)m.ny;
+  const uint32_t total = (uint32_t)m.half_cells(), groups = total / 4;
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+    const uint32_t j = 4 * q, r = j / nzh, x = r / ny;
+    int ix = (int)x, iy = (int)(r - x * ny), iz = (int)(j - r * nzh);
+    float2 a[3][4];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float4* c4 = reinterpret_cast<const float4*>(gc + (int64_t)d * total);
+      const float4 u = c4[2 * q], w = c4[2 * q + 1];
+      a[d][0] = make_float2(u.x, u.y);
+      a[d][1] = make_float2(u.z, u.w);
+      a[d][2] = make_float2(w.x, w.y);
+      a[d][3] = make_float2(w.z, w.w);
+    }
+    float2 o[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const float2 ae[3] = {a[0][e], a[1][e], a[2][e]};
+      o[e] = green_gradient_adjoint_value(ae, (int64_t)j + e, ix, iy, iz, m, t, g);
+      advance_cell(ix, iy, iz, (int)nzh, (int)ny);
+    }
+    float4* o4 = reinterpret_cast<float4*>(out);
+    o4[2 * q] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+    o4[2 * q + 1] = make_float4(o[2].x, o[2].y, o[3].x, o[3].y);
+  }
+}
+
+static bool vec4_ok(Mesh3 m, const void* a, const void* b) {
+  return m.half_cells() % 4 == 0 && m.half_cells() < 2147483648ll && ((uintptr_t)a & 31) == 0 &&
+         ((uintptr_t)b & 31) == 0;
+}
+
 static unsigned grid_for(int64_t total, int th) {
   int64_t b = (total + th - 1) / th;
   int64_t cap = 148 * 32;
@@ -208,7 +281,9 @@ static unsigned grid_for(int64_t total, int th) {
 
 int green_gradient(const float2* src_hat, float2* grad_hat, Mesh3 m, SpecTables t, GreenParams g, cudaStream_t s) {
   const unsigned grid = grid_for(m.half_cells(), 256);
-  if (m.half_cells() < 2147483648ll)
+  if (vec4_ok(m, src_hat, grad_hat))
+    green_gradient_kernel4<<<grid_for(m.half_cells() / 4, 256), 256, 0, s>>>(src_hat, grad_hat, m, t, g);
+  else if (m.half_cells() < 2147483648ll)
     green_gradient_kernel<uint32_t><<<grid, 256, 0, s>>>(src_hat, grad_hat, m, t, g);
   else
     green_gradient_kernel<int64_t><<<grid, 256, 0, s>>>(src_hat, grad_hat, m, t, g);
@@ -219,7 +294,10 @@ int green_gradient(const float2* src_hat, float2* grad_hat, Mesh3 m, SpecTables 
 int green_gradient_adjoint(const float2* grad_cot_hat, float2* src_cot_hat, Mesh3 m, SpecTables t, GreenParams g,
                            cudaStream_t s) {
   const unsigned grid = grid_for(m.half_cells(), 256);
-  if (m.half_cells() < 2147483648ll)
+  if (vec4_ok(m, grad_cot_hat, src_cot_hat))
+    green_gradient_adjoint_kernel4<<<grid_for(m.half_cells() / 4, 256), 256, 0, s>>>(grad_cot_hat, src_cot_hat, m, t,
+                                                                                    g);
+  else if (m.half_cells() < 2147483648ll)
     green_gradient_adjoint_kernel<uint32_t><<<grid, 256, 0, s>>>(grad_cot_hat, src_cot_hat, m, t, g);
   else
     green_gradient_adjoint_kernel<int64_t><<<grid, 256, 0, s>>>(grad_cot_hat, src_cot_hat, m, t, g);
