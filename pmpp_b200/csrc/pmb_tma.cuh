@@ -1,8 +1,8 @@
 // Bulk asynchronous copies (global -> shared, cp.async.bulk) completed through
 // an mbarrier transaction count, with bounded waits.
 //
-// No cluster multicast is used anywhere: every copy reads this GPU's own
-// memory into the issuing CTA's shared memory.  Copies need 16-byte aligned
+// Every copy reads this GPU's own memory into the issuing CTA's shared memory
+// only (no copies into other CTAs of a cluster).  Copies need 16-byte aligned
 // source and destination and a size that is a multiple of 16 bytes.
 #pragma once
 
