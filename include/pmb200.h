@@ -118,6 +118,38 @@ int pmb_green_gradient_adjoint(const void* grad_cot_hat, void* src_cot_hat, int 
                                const float* tables, int has_masks, int green_kernel, const float* transfer,
                                const float* radial, int radial_len, float post_scale, void* stream);
 
+/* ---------------- hand-written PM FFT passes -------------------------------
+ * For meshes whose sides are powers of two (nx, ny in 64..1024, nz in
+ * 128..1024) the fused force and its adjoint run their spectral stages as a
+ * chain of hand-written passes over a y-blocked half-spectrum layout:
+ * channel-major, then rows ((y/32)*nx + x)*32 + y%32 of P = nz/2 + 8 complex
+ * values (columns above nz/2 zero).  pmb_pmfft_channel_elems gives the complex
+ * values per channel (-1 when the mesh is not supported).  Same numpy
+ * conventions as pmb_rfft3 / pmb_irfft3; the inverse drops the imaginary
+ * parts of the kz = 0 and nz/2 bins like irfftn.
+ *
+ * pmb_pmfft_z: real rows -> blocked spectrum (inverse = 0) or back
+ *   (inverse = 1), batch channels.
+ * pmb_pmfft_col: one column pass; mode 0 y forward, 1 y inverse, 2 y inverse
+ *   of channel ch_off into (i c_y Q, i c_z Q) (2 output channels), 3 y forward
+ *   of channels ch_off, ch_off+1 combined as (-i c_y) Y + (-i c_z) Z, 4 x
+ *   forward, 5 x inverse, 6 x forward + Green multiplier + x inverse into
+ *   (i c_x phi, phi) (2 output channels), 7 x forward of channels 0, 1 +
+ *   adjoint multiplier + x inverse.  Modes 0, 1, 4, 5 transform nbatch
+ *   channels starting at ch_off; tables, transfer, radial and post_scale are
+ *   those of pmb_green_gradient (tables may be null for modes 0, 1, 4, 5).
+ * pmb_set_pmfft(0) routes pmb_force / pmb_force_vjp through cuFFT and the
+ * separate multiplier kernels instead (default 1).
+ * pmb_pmfft_timeouts: bounded copy waits in these passes that gave up. */
+int pmb_set_pmfft(int enabled);
+int pmb_pmfft_supported(int nx, int ny, int nz);
+int64_t pmb_pmfft_channel_elems(int nx, int ny, int nz);
+int pmb_pmfft_z(int nx, int ny, int nz, int inverse, int batch, const void* in, void* out, void* stream);
+int pmb_pmfft_col(int nx, int ny, int nz, int mode, int nbatch, int ch_off, const void* in, void* out,
+                  const float* tables, int has_masks, const float* transfer, const float* radial, int radial_len,
+                  float post_scale, void* stream);
+int pmb_pmfft_timeouts(uint32_t* count);
+
 /* ---------------- fused PM force ------------------------------------------
  * One PM force evaluation (nbody/gravity.py:786-814 -> _gravity_from_density
  * :626-633 -> _streamed_acceleration_from_potential :506-543): optional

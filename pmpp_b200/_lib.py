@@ -28,6 +28,13 @@ _SIGS = {
     "pmb_wait_timeouts": (c_int, [c_p]),
     "pmb_set_gather_staging": (c_int, [c_int]),
     "pmb_fft_work_bytes": (c_i64, [c_int, c_int, c_int, c_int]),
+    "pmb_set_pmfft": (c_int, [c_int]),
+    "pmb_pmfft_supported": (c_int, [c_int, c_int, c_int]),
+    "pmb_pmfft_channel_elems": (c_i64, [c_int, c_int, c_int]),
+    "pmb_pmfft_z": (c_int, [c_int, c_int, c_int, c_int, c_int, c_p, c_p, c_p]),
+    "pmb_pmfft_col": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_int, c_p, c_p, c_int, c_f,
+                              c_p]),
+    "pmb_pmfft_timeouts": (c_int, [c_p]),
     "pmb_rfft3": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
     "pmb_irfft3": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
     "pmb_green_gradient": (c_int, [c_p, c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p, c_int, c_f, c_p]),
@@ -139,7 +146,9 @@ _KERNELS = {
     "pmb_overdensity": 1, "pmb_ens_force": 7, "pmb_ens_step": 9, "pmb_ens_set_step": 1,
     "pmb_force64": 5, "pmb_deposit64": 1, "pmb_axpy64": 1, "pmb_sum64": 1, "pmb_white_noise_nested64": 1,
     "pmb_linear_modes64": 1, "pmb_lpt64": 4, "pmb_pk_shells64": 1, "pmb_overdensity64": 1,
+    "pmb_pmfft_z": 1, "pmb_pmfft_col": 1,
 }
+_pmfft = {"enabled": True}
 _launches = [0]
 
 
@@ -147,6 +156,22 @@ def wait_timeouts():
     """Bounded device waits that gave up since the library was loaded."""
     v = ctypes.c_uint32()
     check(lib().pmb_wait_timeouts(ctypes.byref(v)), "pmb_wait_timeouts")
+    return v.value
+
+
+def set_pmfft(enabled):
+    """Route the fused force through the hand-written FFT passes (default) or cuFFT."""
+    check(lib().pmb_set_pmfft(1 if enabled else 0), "pmb_set_pmfft")
+    _pmfft["enabled"] = bool(enabled)
+
+
+def pmfft_active(nx, ny, nz):
+    return _pmfft["enabled"] and bool(lib().pmb_pmfft_supported(int(nx), int(ny), int(nz)))
+
+
+def pmfft_timeouts():
+    v = ctypes.c_uint32()
+    check(lib().pmb_pmfft_timeouts(ctypes.byref(v)), "pmb_pmfft_timeouts")
     return v.value
 
 
@@ -165,3 +190,8 @@ def call(name, *args):
         _launches[0] += 2 if args[6] is None else 3
     else:
         _launches[0] += _KERNELS.get(name, 0)
+        # the hand-written FFT chain adds six passes and drops the multiplier kernel
+        if name == "pmb_force" and pmfft_active(*args[5:8]):
+            _launches[0] += 5
+        elif name == "pmb_force_vjp" and pmfft_active(*args[3:6]):
+            _launches[0] += 5

@@ -200,6 +200,52 @@ int pmb_green_gradient_adjoint(const void* grad_cot_hat, void* src_cot_hat, int 
 // ---------------------------------------------------------------------------
 // Fused force
 // ---------------------------------------------------------------------------
+// Spectral path of the fused force: the hand-written pass chain over the
+// y-blocked layout (pmfft.cu) for power-of-two meshes, cuFFT otherwise.
+static bool g_use_pmfft = true;
+
+static bool use_pmfft(Mesh3 m) { return g_use_pmfft && pmfft_supported(m); }
+
+int pmb_set_pmfft(int enabled) {
+  g_use_pmfft = enabled != 0;
+  return kOk;
+}
+
+int pmb_pmfft_supported(int nx, int ny, int nz) { return pmfft_supported(Mesh3{nx, ny, nz}) ? 1 : 0; }
+
+int64_t pmb_pmfft_channel_elems(int nx, int ny, int nz) {
+  Mesh3 m{nx, ny, nz};
+  return pmfft_supported(m) ? pmfft_channel_elems(m) : -1;
+}
+
+int pmb_pmfft_z(int nx, int ny, int nz, int inverse, int batch, const void* in, void* out, void* stream) {
+  Mesh3 m{nx, ny, nz};
+  PMB_REQUIRE(pmfft_supported(m), "pmb_pmfft_z: mesh not supported (powers of two, 64..1024, nz >= 128)");
+  PMB_REQUIRE(batch >= 1, "pmb_pmfft_z: batch must be positive");
+  if (inverse) return pmfft_z(m, 1, batch, nullptr, (const float2*)in, (float*)out, nullptr, S(stream));
+  return pmfft_z(m, 0, batch, (const float*)in, nullptr, nullptr, (float2*)out, S(stream));
+}
+
+int pmb_pmfft_col(int nx, int ny, int nz, int mode, int nbatch, int ch_off, const void* in, void* out,
+                  const float* tables, int has_masks, const float* transfer, const float* radial, int radial_len,
+                  float post_scale, void* stream) {
+  Mesh3 m{nx, ny, nz};
+  PMB_REQUIRE(pmfft_supported(m), "pmb_pmfft_col: mesh not supported (powers of two, 64..1024, nz >= 128)");
+  PMB_REQUIRE(mode >= 0 && mode <= 7, "pmb_pmfft_col: mode must be 0..7");
+  PMB_REQUIRE(nbatch >= 1 && ch_off >= 0, "pmb_pmfft_col: bad batch");
+  PMB_REQUIRE(tables != nullptr || mode == 0 || mode == 1 || mode == 4 || mode == 5,
+              "pmb_pmfft_col: spectral tables required for the multiplier modes");
+  SpecTables t{};
+  if (tables != nullptr) t = make_tables(tables, m, has_masks);
+  return pmfft_col(m, mode, nbatch, ch_off, (const float2*)in, (float2*)out, t,
+                   make_green(0, transfer, radial, radial_len, post_scale), S(stream));
+}
+
+int pmb_pmfft_timeouts(uint32_t* count) {
+  PMB_REQUIRE(count != nullptr, "pmb_pmfft_timeouts: null output");
+  return pmfft_timeouts(count);
+}
+
 static int64_t force_layout(int64_t n, Mesh3 m, void* ws, int64_t cap, void** sorted, void** bin_scratch,
                             void** scale16, float** src, float2** src_hat, float2** grad_hat, void** fft_work) {
   Carve c(ws, cap);
@@ -207,6 +253,13 @@ static int64_t force_layout(int64_t n, Mesh3 m, void* ws, int64_t cap, void** so
   *bin_scratch = c.take(bin_scratch_bytes(n, m));
   *scale16 = c.take(16);
   *src = (float*)c.take(4 * m.cells());
+  if (use_pmfft(m)) {
+    // five spectral channels for the pass chain
+    *src_hat = (float2*)c.take(5 * 8 * pmfft_channel_elems(m));
+    *grad_hat = nullptr;
+    *fft_work = nullptr;
+    return c.off;
+  }
   *src_hat = (float2*)c.take(8 * m.half_cells());
   *grad_hat = (float2*)c.take(24 * m.half_cells());
   int64_t w = fft_work_bytes(m, 3);
@@ -243,11 +296,16 @@ int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float dr
   cudaStream_t s = S(stream);
   PMB_TRY(pmb_sort_rows(pmid, disp, drift_vel, drift, n, nx, ny, nz, cell, sorted, bins, bin_scratch_bytes(n, m), stream));
   PMB_TRY(pmb_scatter_rows(sorted, n, nx, ny, nz, 1, nullptr, 0, val_const, 1, src_mul, src, scale16, stream));
-  PMB_TRY(fft_r2c(m, 1, src, src_hat, work, s));
   const float inv_m = (float)(1.0 / (double)m.cells());
-  PMB_TRY(green_gradient(src_hat, grad_hat, m, make_tables(tables, m, has_masks),
-                         make_green(green_kernel, transfer, radial, radial_len, inv_m), s));
-  PMB_TRY(fft_c2r(m, 3, grad_hat, force_meshes, work, s));
+  if (use_pmfft(m)) {
+    PMB_TRY(pmfft_force(m, src, force_meshes, src_hat, make_tables(tables, m, has_masks),
+                        make_green(green_kernel, transfer, radial, radial_len, inv_m), s));
+  } else {
+    PMB_TRY(fft_r2c(m, 1, src, src_hat, work, s));
+    PMB_TRY(green_gradient(src_hat, grad_hat, m, make_tables(tables, m, has_masks),
+                           make_green(green_kernel, transfer, radial, radial_len, inv_m), s));
+    PMB_TRY(fft_c2r(m, 3, grad_hat, force_meshes, work, s));
+  }
   SortedView v = sorted_view(sorted, n);
   return gather_sorted(v.rec, v.perm, v.offs, n, m, 3, force_meshes, acc, vel_kick, kick, s);
 }
@@ -261,6 +319,13 @@ static int64_t force_vjp_layout(int64_t n, Mesh3 m, void* ws, int64_t cap, void*
   *scale16 = c.take(16);
   *cot_sorted = (float*)c.take(12 * n);
   *mesh_cot = (float*)c.take(12 * m.cells());
+  if (use_pmfft(m)) {
+    *spec3 = (float2*)c.take(5 * 8 * pmfft_channel_elems(m));
+    *src_hat = nullptr;
+    *src_cot = (float*)c.take(4 * m.cells());
+    *work = nullptr;
+    return c.off;
+  }
   *spec3 = (float2*)c.take(24 * m.half_cells());
   *src_hat = (float2*)c.take(8 * m.half_cells());
   *src_cot = (float*)c.take(4 * m.cells());
@@ -305,11 +370,16 @@ int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int
                              cot_sorted, s));
   PMB_TRY(pmb_scatter_rows(sorted, n, nx, ny, nz, 3, cot_sorted, 1, 0.f, 0, 1.f, mesh_cot, scale16, stream));
   // transposes of the C2R, gradient, Green and R2C stages
-  PMB_TRY(fft_r2c(m, 3, mesh_cot, spec3, work, s));
   const float post = (float)((double)src_mul / (double)m.cells());
-  PMB_TRY(green_gradient_adjoint(spec3, src_hat, m, make_tables(tables, m, has_masks),
-                                 make_green(green_kernel, transfer, radial, radial_len, post), s));
-  PMB_TRY(fft_c2r(m, 1, src_hat, src_cot, work, s));
+  if (use_pmfft(m)) {
+    PMB_TRY(pmfft_force_adjoint(m, mesh_cot, src_cot, spec3, make_tables(tables, m, has_masks),
+                                make_green(green_kernel, transfer, radial, radial_len, post), s));
+  } else {
+    PMB_TRY(fft_r2c(m, 3, mesh_cot, spec3, work, s));
+    PMB_TRY(green_gradient_adjoint(spec3, src_hat, m, make_tables(tables, m, has_masks),
+                                   make_green(green_kernel, transfer, radial, radial_len, post), s));
+    PMB_TRY(fft_c2r(m, 1, src_hat, src_cot, work, s));
+  }
   // scatter adjoint of the density (constant particle value)
   return interp_grad_sorted(v.rec, v.perm, v.offs, n, m, 1, src_cot, nullptr, val_const, cell, 1, disp_cot, nullptr,
                             nullptr, s);

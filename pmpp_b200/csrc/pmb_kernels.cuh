@@ -48,4 +48,19 @@ int green_gradient_adjoint(const float2* grad_cot_hat, float2* src_cot_hat, Mesh
                            cudaStream_t s);
 int scale_real(float* x, int64_t count, float a, float b, cudaStream_t s);
 
+// pmfft.cu: hand-written FFT passes for power-of-two meshes over the
+// y-blocked half-spectrum layout (see pmfft.cu for the layout and modes).
+bool pmfft_supported(Mesh3 m);
+int pmfft_row_len(Mesh3 m);
+int64_t pmfft_channel_elems(Mesh3 m);
+int pmfft_z(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in_c, float* out_r, float2* out_c,
+            cudaStream_t s);
+int pmfft_col(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t, GreenParams g,
+              cudaStream_t s);
+int pmfft_force(Mesh3 m, const float* src, float* force_meshes, float2* work, SpecTables t, GreenParams g,
+                cudaStream_t s);
+int pmfft_force_adjoint(Mesh3 m, const float* mesh_cot, float* src_cot, float2* work, SpecTables t, GreenParams g,
+                        cudaStream_t s);
+int pmfft_timeouts(unsigned int* count);
+
 }  // namespace pmb

@@ -1,0 +1,997 @@
+// Particle-mesh FFT pipeline for power-of-two meshes.
+//
+// The force and its adjoint need, per evaluation, one real-to-complex 3D
+// transform, the Green x gradient multiplier and three complex-to-real
+// transforms (the adjoint the transpose of that).  cuFFT runs each 3D
+// transform as three passes over the whole mesh plus a separate multiplier
+// pass.  Here the passes are hand-written persistent kernels fed by TMA, and
+// the multiplier is fused into the x pass, where all three wavenumbers of a
+// column are known:
+//
+//   forward:  z R2C -> y -> [x, K(k) (i c_d), x^-1] -> y^-1 -> z C2R
+//   adjoint:  z R2C -> y -> [x, K(k) sum_d (-i c_d), x^-1] -> y^-1 -> z C2R
+//
+// Linearity keeps the channel count down: c_y and c_z are constant along x,
+// so the forward x pass writes only W = x^-1(i c_x phi) and Q = x^-1(phi);
+// the inverse y pass makes F_y from i c_y Q and F_z = i c_z y^-1(Q).  The
+// adjoint folds the y and z channels into one in its y pass the same way.
+// Traffic per evaluation: 18 half-spectrum-sized reads/writes (about 28 for
+// separate cuFFT transforms and multiplier).
+//
+// Half-spectrum layout ("y-blocked"): channel-major, then
+//   ((y / BY) * nx + x) * BY + y % BY   rows of P complex values,
+// P = nz/2 + 8 (columns nz/2+1 .. P-1 are zero padding), BY = 32.  Blocking
+// y keeps the x pass's stride at BY * P * 8 bytes (133 KB at 1024^3) instead
+// of a whole (y, kz) plane; with the plain layout the x pass touches a
+// different 2 MB page per row and runs at half the bandwidth.
+//
+// Each column pass (y or x) is a four-step FFT of length L = R1 * R2 over a
+// tile of KT = 8 adjacent columns (64-byte rows): the tile arrives in shared
+// memory by TMA (a ring of S stages, one tile in flight while another is
+// transformed), R1-point DFTs run in registers, twiddles, a transpose through
+// shared memory, R2-point DFTs, and the results are stored from registers.
+// The z passes work on KR = 16 contiguous rows with a bulk copy per tile; the
+// real transform of length nz is a complex transform of length nz/2 plus the
+// usual even/odd split.
+//
+// Semantics follow numpy's rfftn / irfftn (numerics/fft.py): forward
+// unnormalised; the inverse is unnormalised (the multiplier's post scale
+// carries 1/cells) and, like irfftn, drops the imaginary parts of the kz = 0
+// and kz = nz/2 bins after the x and y inverse transforms.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <type_traits>
+#include <vector>
+
+#include "pmb_common.cuh"
+#include "pmb_kernels.cuh"
+#include "pmb_spectral_device.cuh"
+#include "pmb_tma.cuh"
+
+namespace pmb {
+
+namespace {
+
+constexpr int KT = 8;   // columns per column tile
+constexpr int BY = 32;  // y rows per block of the spectral layout
+constexpr int KR = 16;  // rows per z-pass tile
+
+__constant__ float2 c_w32[32];  // exp(-2 pi i k / 32)
+__device__ unsigned int g_fft_timeouts;
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
+// i * c * a
+__device__ __forceinline__ float2 i_times(float c, float2 a) { return make_float2(-c * a.y, c * a.x); }
+
+template <int R>
+struct Log2 {
+  static constexpr int v = 1 + Log2<R / 2>::v;
+};
+template <>
+struct Log2<1> {
+  static constexpr int v = 0;
+};
+
+__host__ __device__ constexpr int bit_reverse(int i, int bits) {
+  int r = 0;
+  for (int b = 0; b < bits; ++b) r |= ((i >> b) & 1) << (bits - 1 - b);
+  return r;
+}
+
+// One radix-2 stage (butterfly span LEN) of an in-register R-point DFT on
+// bit-reversed input; the stages recurse at compile time so every index is
+// a constant and the array stays in registers.
+template <int R, int LEN, bool INV>
+__device__ __forceinline__ void dft_stage(float2 (&v)[R]) {
+  constexpr int H = LEN / 2;
+#pragma unroll
+  for (int i = 0; i < R; i += LEN) {
+#pragma unroll
+    for (int k = 0; k < H; ++k) {
+      float2 b = v[i + k + H];
+      if (k == 0) {
+      } else if (4 * k == LEN) {
+        b = INV ? make_float2(-b.y, b.x) : make_float2(b.y, -b.x);
+      } else {
+        float2 w = c_w32[k * (32 / LEN)];
+        if (INV) w.y = -w.y;
+        b = cmul(b, w);
+      }
+      const float2 a = v[i + k];
+      v[i + k] = cadd(a, b);
+      v[i + k + H] = csub(a, b);
+    }
+  }
+  if constexpr (LEN < R) dft_stage<R, 2 * LEN, INV>(v);
+}
+
+// In-register R-point DFT (R <= 32), natural order in and out; INV uses the
+// conjugate kernel (no scaling).
+template <int R, bool INV>
+__device__ __forceinline__ void reg_dft(float2 (&v)[R]) {
+  constexpr int LB = Log2<R>::v;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int j = bit_reverse(i, LB);
+    if (j > i) {
+      const float2 t = v[i];
+      v[i] = v[j];
+      v[j] = t;
+    }
+  }
+  dft_stage<R, 2, INV>(v);
+}
+
+// Four-step FFT of length A1*A2 over KT columns, first half: the job (n2, c)
+// holds x[A2*n1 + n2], n1 < A1; A1-point DFTs, twiddle W_L^(n2 k1), written
+// transposed to buf[k1][n2][c] (rows padded by 8 values against bank conflicts).
+template <int A1, int A2, bool INV>
+__device__ __forceinline__ void four_step_a(float2 (&v)[A1], float2* buf, int n2, int c, const float2* __restrict__ tw) {
+  constexpr int ROW = A2 * KT + 8;
+  reg_dft<A1, INV>(v);
+#pragma unroll
+  for (int k1 = 0; k1 < A1; ++k1) {
+    float2 r = v[k1];
+    if (k1 != 0) {
+      float2 w = __ldg(&tw[n2 * k1]);
+      if (INV) w.y = -w.y;
+      r = cmul(r, w);
+    }
+    buf[k1 * ROW + n2 * KT + c] = r;
+  }
+}
+
+// Second half: the job (k1, c) reads buf[k1][.][c] and does the A2-point DFT:
+// u[k2] = X[k1 + A1*k2].
+template <int A1, int A2, bool INV>
+__device__ __forceinline__ void four_step_b(float2 (&u)[A2], const float2* buf, int k1, int c) {
+  constexpr int ROW = A2 * KT + 8;
+#pragma unroll
+  for (int n2 = 0; n2 < A2; ++n2) u[n2] = buf[k1 * ROW + n2 * KT + c];
+  reg_dft<A2, INV>(u);
+}
+
+template <int R1, int R2>
+struct ColGeom {
+  static constexpr int L = R1 * R2;
+  static constexpr int T = (R1 > R2 ? R1 : R2) * KT;
+  static constexpr int TILE = L * KT;
+  static constexpr int XA = R1 * (R2 * KT + 8);
+  static constexpr int XB = R2 * (R1 * KT + 8);
+  static constexpr int BUF0 = TILE > XA ? TILE : XA;
+  static constexpr int BUF = BUF0 > XB ? BUF0 : XB;  // float2 per stage
+  static constexpr int BOX = L < 256 ? L : 256;      // rows per TMA box
+};
+
+// Column pass modes.
+enum ColMode : int {
+  kYFwd = 0,     // y forward, 1 -> 1
+  kYInv = 1,     // y inverse, 1 -> 1
+  kYInvYZ = 2,   // y inverse of i c_y Q and i c_z y^-1(Q): 1 -> 2
+  kYFwdYZ = 3,   // (-i c_y) y(A_y) + (-i c_z) y(A_z): 2 -> 1
+  kXFwd = 4,     // x forward, 1 -> 1
+  kXInv = 5,     // x inverse, 1 -> 1
+  kXGreen = 6,   // x, K(k), x^-1 of i c_x phi and phi: 1 -> 2
+  kXGreenAdj = 7 // x of B_x and b, K(k) ((-i c_x) B_x + b), x^-1: 2 -> 1
+};
+
+__host__ __device__ constexpr bool is_y(int mode) { return mode <= kYFwdYZ; }
+__host__ __device__ constexpr int n_in(int mode) { return (mode == kYFwdYZ || mode == kXGreenAdj) ? 2 : 1; }
+__host__ __device__ constexpr int n_out(int mode) { return (mode == kYInvYZ || mode == kXGreen) ? 2 : 1; }
+
+struct ColArgs {
+  float2* out;
+  int64_t ch;      // complex values per channel
+  int64_t sb;      // values per y block (nx * BY * P)
+  int P;           // row length
+  int nx, ny, nz;  // mesh
+  int ncolt;       // column tiles per (outer index)
+  int nouter;      // x (y pass) or y blocks (x pass)
+  int ntiles;      // ncolt * nouter * nbatch
+  int ch_off;      // first input channel
+  const float2* tw;
+  SpecTables t;
+  GreenParams g;
+};
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool kz_valid(int kz, int nz) { return kz <= nz / 2; }
+
+// Green multiplier of the source value at (ix, iy, iz): phi = K(k) S, K =
+// post * mask * T * (-1/k^2), zero at k = 0 (pmb_spectral_device.cuh has the
+// reference citations).
+__device__ __forceinline__ float green_scalar(const ColArgs& a, int ix, int iy, int iz) {
+  const Mesh3 m{a.nx, a.ny, a.nz};
+  const float k2 = k2_of(a.t, ix, iy, iz);
+  if (k2 == 0.f) return 0.f;
+  float K = __fdiv_rn(-a.g.post_scale, k2);
+  if (a.t.mx != nullptr) K = __fmul_rn(K, __fmul_rn(__fmul_rn(a.t.mx[ix], a.t.my[iy]), a.t.mz[iz]));
+  if (a.g.transfer != nullptr || a.g.radial != nullptr) {
+    const int64_t j = ((int64_t)ix * a.ny + iy) * (a.nz / 2 + 1) + iz;
+    K = __fmul_rn(K, transfer_of(a.g, a.t, j, ix, iy, iz, m));
+  }
+  return K;
+}
+
+// Persistent column pass: a ring of S stages, stage slot i holds input q =
+// i % NIN of tile i / NIN of this CTA.
+template <int R1, int R2, int S, int MODE>
+__global__ void __launch_bounds__(ColGeom<R1, R2>::T, 1)
+    col_pass_kernel(const __grid_constant__ CUtensorMap tin, const ColArgs a) {
+  using G = ColGeom<R1, R2>;
+  constexpr int L = G::L;
+  constexpr int NIN = n_in(MODE);
+  constexpr bool YP = is_y(MODE);
+  extern __shared__ __align__(128) float2 smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S * G::BUF);
+  const int t = threadIdx.x;
+  const int c = t % KT;
+  const int tiles_mine = a.ntiles > (int)blockIdx.x ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int slots = tiles_mine * NIN;
+  if (t == 0)
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+  __syncthreads();
+
+  // tile -> (column tile, outer, batch)
+  auto decode = [&](int tile, int& ct, int& outer, int& batch) {
+    ct = tile % a.ncolt;
+    const int r = tile / a.ncolt;
+    outer = r % a.nouter;
+    batch = r / a.nouter;
+  };
+  auto issue = [&](int i) {
+    if (i >= slots) return;
+    const int tile = blockIdx.x + (i / NIN) * gridDim.x;
+    int ct, outer, batch;
+    decode(tile, ct, outer, batch);
+    const int ch = a.ch_off + batch * NIN + i % NIN;
+    const int s = i % S;
+    float2* dst = smem + s * G::BUF;
+    mbar_expect_tx(&bars[s], L * KT * 8);
+    const int nyb = a.ny / BY;
+#pragma unroll 1
+    for (int r = 0; r < L; r += G::BOX) {
+      if (YP)
+        tma_load_4d(dst + r * KT, &tin, ct * KT, r % BY, outer, r / BY + ch * nyb, &bars[s]);
+      else
+        tma_load_3d(dst + r * KT, &tin, ct * KT, r, outer + ch * nyb, &bars[s]);
+    }
+  };
+  if (t == 0)
+    for (int i = 0; i < S; ++i) issue(i);
+
+  // wait for slot i; false (uniformly across the CTA) on a timeout
+  auto acquire = [&](int i) -> bool {
+    const int s = i % S;
+    const bool ok = mbar_wait(&bars[s], (i / S) & 1);
+    if (__syncthreads_or(!ok)) {
+      if (t == 0) atomicAdd(&g_fft_timeouts, 1u);
+      mbar_wait(&bars[s], (i / S) & 1);
+      return false;
+    }
+    return true;
+  };
+  // slot i consumed: hand its stage to the copy engine for slot i + S
+  auto release = [&](int i) {
+    __syncthreads();
+    if (t == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(i + S);
+    }
+  };
+
+  const bool ja = t < R2 * KT;  // first-half jobs (n2 = t / KT)
+  const bool jb = t < R1 * KT;  // second-half jobs (k1 = t / KT)
+  const int q = t / KT;
+
+  // forward or inverse transform of the tile in stage slot i; afterwards the
+  // job (k1 = q, c) holds u[k2] = X[k1 + R1 k2].  Leaves the stage free to
+  // reuse as scratch (not yet released).
+  auto transform = [&](int i, float2 (&u)[R2], auto inv_tag, float ymul_c, bool ymul) {
+    constexpr bool INV = decltype(inv_tag)::value;
+    float2* buf = smem + (i % S) * G::BUF;
+    float2 v[R1];
+    if (ja) {
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) v[n1] = buf[(R2 * n1 + q) * KT + c];
+    }
+    __syncthreads();
+    if (ja) four_step_a<R1, R2, INV>(v, buf, q, c, a.tw);
+    __syncthreads();
+    if (jb) four_step_b<R1, R2, INV>(u, buf, q, c);
+    (void)ymul_c;
+    (void)ymul;
+  };
+
+  // inverse transform of values held as u[k2] at index k1 + R1 k2 (k1 = q),
+  // decomposition (R2, R1); result w[k2'] at index k1' + R2 k2' (k1' = q).
+  auto inverse_held = [&](float2* buf, float2 (&u)[R2], float2 (&w)[R1]) {
+    __syncthreads();
+    if (jb) four_step_a<R2, R1, true>(u, buf, q, c, a.tw);
+    __syncthreads();
+    if (ja) four_step_b<R2, R1, true>(w, buf, q, c);
+  };
+
+  for (int it = 0; it < tiles_mine; ++it) {
+    const int tile = blockIdx.x + it * gridDim.x;
+    int ct, outer, batch;
+    decode(tile, ct, outer, batch);
+    const int i0 = it * NIN;
+    float2 u[R2];
+    if (!acquire(i0)) return;
+    if constexpr (MODE == kYFwd || MODE == kYInv || MODE == kXFwd || MODE == kXInv) {
+      constexpr bool INV = (MODE == kYInv || MODE == kXInv);
+      transform(i0, u, std::integral_constant<bool, INV>{}, 0.f, false);
+      const int64_t ob = (int64_t)batch * a.ch;
+      if (jb) {
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) {
+          const int r = q + R1 * k2;
+          int64_t off;
+          if (YP)
+            off = ob + (int64_t)(r / BY) * a.sb + ((int64_t)outer * BY + r % BY) * a.P + ct * KT + c;
+          else
+            off = ob + (int64_t)outer * a.sb + (int64_t)r * BY * a.P + ct * KT + c;
+          a.out[off] = u[k2];
+        }
+      }
+      release(i0);
+    } else if constexpr (MODE == kYFwdYZ) {
+      // acc = (-i c_y(ky)) y(A_y) + (-i c_z(kz)) y(A_z); rows are ky
+      const int kz = ct * KT + c;
+      const bool kv = kz_valid(kz, a.nz);
+      const float cz = kv ? a.t.cz[kz] : 0.f;
+      float2 acc[R2];
+      transform(i0, u, std::false_type{}, 0.f, false);
+      if (jb) {
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) acc[k2] = i_times(-a.t.cy[q + R1 * k2], u[k2]);
+      }
+      release(i0);
+      if (!acquire(i0 + 1)) return;
+      transform(i0 + 1, u, std::false_type{}, 0.f, false);
+      if (jb) {
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) {
+          const float2 z = i_times(-cz, u[k2]);
+          const float2 r = kv ? cadd(acc[k2], z) : make_float2(0.f, 0.f);
+          const int ky = q + R1 * k2;
+          a.out[(int64_t)(ky / BY) * a.sb + ((int64_t)outer * BY + ky % BY) * a.P + kz] = r;
+        }
+      }
+      release(i0 + 1);
+    } else if constexpr (MODE == kYInvYZ) {
+      // F_y = y^-1(i c_y(ky) Q), F_z = i c_z(kz) y^-1(Q); load rows are ky
+      float2* buf = smem + (i0 % S) * G::BUF;
+      const int kz = ct * KT + c;
+      const bool kv = kz_valid(kz, a.nz);
+      const float cz = kv ? a.t.cz[kz] : 0.f;
+      float2 v[R1], vy[R1];
+      if (ja) {
+#pragma unroll
+        for (int n1 = 0; n1 < R1; ++n1) {
+          v[n1] = buf[(R2 * n1 + q) * KT + c];
+          vy[n1] = i_times(a.t.cy[R2 * n1 + q], v[n1]);
+        }
+      }
+      __syncthreads();
+      if (ja) four_step_a<R1, R2, true>(vy, buf, q, c, a.tw);
+      __syncthreads();
+      auto store = [&](int chan, int k2, float2 val) {
+        const int y = q + R1 * k2;
+        a.out[chan * a.ch + (int64_t)(y / BY) * a.sb + ((int64_t)outer * BY + y % BY) * a.P + kz] = val;
+      };
+      if (jb) {
+        four_step_b<R1, R2, true>(u, buf, q, c);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) store(0, k2, kv ? u[k2] : make_float2(0.f, 0.f));
+      }
+      __syncthreads();
+      if (ja) four_step_a<R1, R2, true>(v, buf, q, c, a.tw);
+      __syncthreads();
+      if (jb) {
+        four_step_b<R1, R2, true>(u, buf, q, c);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) store(1, k2, i_times(cz, u[k2]));
+      }
+      release(i0);
+    } else if constexpr (MODE == kXGreen) {
+      // column j = yi * P + kz of y block `outer`; rows are kx after the transform
+      const int j = ct * KT + c;
+      const int yi = j / a.P, kz = j - yi * a.P;
+      const int iy = outer * BY + yi;
+      const bool kv = kz_valid(kz, a.nz);
+      float2* buf = smem + (i0 % S) * G::BUF;
+      transform(i0, u, std::false_type{}, 0.f, false);
+      float2 w[R2];
+      if (jb) {
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) {
+          const int kx = q + R1 * k2;
+          const float K = kv ? green_scalar(a, kx, iy, kz) : 0.f;
+          u[k2] = make_float2(K * u[k2].x, K * u[k2].y);  // phi
+          w[k2] = i_times(a.t.cx[kx], u[k2]);
+        }
+      }
+      float2 o[R1];
+      auto store = [&](int chan, float2 (&val)[R1]) {
+        if (ja) {
+#pragma unroll
+          for (int k2 = 0; k2 < R1; ++k2) {
+            const int x = q + R2 * k2;
+            a.out[chan * a.ch + (int64_t)outer * a.sb + (int64_t)x * BY * a.P + j] = val[k2];
+          }
+        }
+      };
+      inverse_held(buf, w, o);
+      store(0, o);
+      inverse_held(buf, u, o);
+      store(1, o);
+      release(i0);
+    } else if constexpr (MODE == kXGreenAdj) {
+      const int j = ct * KT + c;
+      const int yi = j / a.P, kz = j - yi * a.P;
+      const int iy = outer * BY + yi;
+      const bool kv = kz_valid(kz, a.nz);
+      float2 acc[R2];
+      transform(i0, u, std::false_type{}, 0.f, false);
+      if (jb) {
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) acc[k2] = i_times(-a.t.cx[q + R1 * k2], u[k2]);
+      }
+      release(i0);
+      if (!acquire(i0 + 1)) return;
+      float2* buf = smem + ((i0 + 1) % S) * G::BUF;
+      transform(i0 + 1, u, std::false_type{}, 0.f, false);
+      if (jb) {
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) {
+          const int kx = q + R1 * k2;
+          const float K = kv ? green_scalar(a, kx, iy, kz) : 0.f;
+          const float2 s = cadd(acc[k2], u[k2]);
+          acc[k2] = make_float2(K * s.x, K * s.y);
+        }
+      }
+      float2 o[R1];
+      inverse_held(buf, acc, o);
+      if (ja) {
+#pragma unroll
+        for (int k2 = 0; k2 < R1; ++k2) {
+          const int x = q + R2 * k2;
+          a.out[(int64_t)outer * a.sb + (int64_t)x * BY * a.P + j] = o[k2];
+        }
+      }
+      release(i0 + 1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z passes (contiguous rows)
+// ---------------------------------------------------------------------------
+template <int R1, int R2>
+struct ZGeom {
+  static constexpr int M = R1 * R2;  // complex length = nz / 2
+  static constexpr int T = 256;
+  static constexpr int ROWZ = R2 + 1;
+  static constexpr int XP = KR * R1 * ROWZ;  // transpose buffer (float2)
+};
+
+struct ZArgs {
+  const float* in_r;   // z R2C input (real rows)
+  const float2* in_c;  // z C2R input (spectral rows)
+  float* out_r;
+  float2* out_c;
+  int64_t ch;      // complex values per spectral channel
+  int64_t cells;   // reals per real channel
+  int64_t sb;      // nx * BY * P
+  int P, nx, ny, nz;
+  int tiles_per_ch, ntiles;
+  const float2* tw_m;  // W_M^k, k < M
+  const float2* tw_n;  // W_nz^k, k < nz
+};
+
+// spectral row offset of mesh row (x, y)
+__device__ __forceinline__ int64_t spec_row(const ZArgs& a, int x, int y) {
+  return (int64_t)(y / BY) * a.sb + ((int64_t)x * BY + y % BY) * a.P;
+}
+
+// Real-to-complex along z: KR rows of nz reals -> KR rows of P complex.
+template <int R1, int R2, int S>
+__global__ void __launch_bounds__(256, 1) z_r2c_kernel(const ZArgs a) {
+  using G = ZGeom<R1, R2>;
+  constexpr int M = G::M;
+  constexpr int STAGE = KR * M;  // float2
+  extern __shared__ __align__(128) float2 smem[];
+  float2* xp = smem + S * STAGE;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(xp + G::XP);
+  const int t = threadIdx.x;
+  const int tiles_mine = a.ntiles > (int)blockIdx.x ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  if (t == 0)
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+  __syncthreads();
+  auto issue = [&](int i) {
+    if (i >= tiles_mine) return;
+    const int tile = blockIdx.x + i * gridDim.x;
+    const int ch = tile / a.tiles_per_ch;
+    const int64_t row0 = (int64_t)(tile % a.tiles_per_ch) * KR;
+    const int s = i % S;
+    mbar_expect_tx(&bars[s], KR * M * 8);
+    bulk_copy_g2s(smem + s * STAGE, a.in_r + ch * a.cells + row0 * a.nz, KR * M * 8, &bars[s]);
+  };
+  if (t == 0)
+    for (int i = 0; i < S; ++i) issue(i);
+  for (int it = 0; it < tiles_mine; ++it) {
+    const int s = it % S;
+    const bool ok = mbar_wait(&bars[s], (it / S) & 1);
+    if (__syncthreads_or(!ok)) {
+      if (t == 0) atomicAdd(&g_fft_timeouts, 1u);
+      mbar_wait(&bars[s], (it / S) & 1);
+      return;
+    }
+    float2* st = smem + s * STAGE;
+    const int tile = blockIdx.x + it * gridDim.x;
+    const int ch = tile / a.tiles_per_ch;
+    const int row0 = (tile % a.tiles_per_ch) * KR;
+    // first half: job (n2, rho)
+    for (int jbq = t; jbq < KR * R2; jbq += G::T) {
+      const int n2 = jbq % R2, rho = jbq / R2;
+      float2 v[R1];
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) v[n1] = st[rho * M + R2 * n1 + n2];
+      reg_dft<R1, false>(v);
+#pragma unroll
+      for (int k1 = 0; k1 < R1; ++k1) {
+        float2 r = v[k1];
+        if (k1 != 0) r = cmul(r, __ldg(&a.tw_m[n2 * k1]));
+        xp[(rho * R1 + k1) * G::ROWZ + n2] = r;
+      }
+    }
+    __syncthreads();
+    // second half: job (k1, rho); Z[k1 + R1 k2] back into the stage, natural order
+    for (int jbq = t; jbq < KR * R1; jbq += G::T) {
+      const int k1 = jbq % R1, rho = jbq / R1;
+      float2 u[R2];
+#pragma unroll
+      for (int n2 = 0; n2 < R2; ++n2) u[n2] = xp[(rho * R1 + k1) * G::ROWZ + n2];
+      reg_dft<R2, false>(u);
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) st[rho * M + k1 + R1 * k2] = u[k2];
+    }
+    __syncthreads();
+    // even/odd split: X[k] = E[k] + W_N^k O[k], k <= M; zero padding after
+    const int x = row0 / a.ny, y0 = row0 % a.ny;
+    float2* orow = a.out_c + ch * a.ch + spec_row(a, x, y0);
+    for (int jq = t; jq < KR * a.P; jq += G::T) {
+      const int rho = jq / a.P, k = jq - rho * a.P;
+      float2 X = make_float2(0.f, 0.f);
+      if (k <= M) {
+        const float2 zk = st[rho * M + (k == M ? 0 : k)];
+        const float2 zm = conjf2(st[rho * M + (M - k) % M]);
+        const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
+        const float2 d = make_float2(0.5f * (zk.x - zm.x), 0.5f * (zk.y - zm.y));
+        const float2 o = make_float2(d.y, -d.x);  // -i d
+        X = cadd(e, cmul(__ldg(&a.tw_n[k]), o));
+      }
+      orow[(int64_t)rho * a.P + k] = X;
+    }
+    __syncthreads();
+    if (t == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(it + S);
+    }
+  }
+}
+
+// Complex-to-real along z: KR rows of P complex -> KR rows of nz reals.
+template <int R1, int R2, int S>
+__global__ void __launch_bounds__(256, 1) z_c2r_kernel(const ZArgs a) {
+  using G = ZGeom<R1, R2>;
+  constexpr int M = G::M;
+  const int P = a.P;
+  const int STAGE = KR * P;  // float2
+  extern __shared__ __align__(128) float2 smem[];
+  float2* xp = smem + S * STAGE;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(xp + G::XP);
+  const int t = threadIdx.x;
+  const int tiles_mine = a.ntiles > (int)blockIdx.x ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  if (t == 0)
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+  __syncthreads();
+  auto issue = [&](int i) {
+    if (i >= tiles_mine) return;
+    const int tile = blockIdx.x + i * gridDim.x;
+    const int ch = tile / a.tiles_per_ch;
+    const int row0 = (tile % a.tiles_per_ch) * KR;
+    const int s = i % S;
+    const int x = row0 / a.ny, y0 = row0 % a.ny;
+    mbar_expect_tx(&bars[s], KR * P * 8);
+    bulk_copy_g2s(smem + s * STAGE, a.in_c + ch * a.ch + spec_row(a, x, y0), KR * P * 8, &bars[s]);
+  };
+  if (t == 0)
+    for (int i = 0; i < S; ++i) issue(i);
+  for (int it = 0; it < tiles_mine; ++it) {
+    const int s = it % S;
+    const bool ok = mbar_wait(&bars[s], (it / S) & 1);
+    if (__syncthreads_or(!ok)) {
+      if (t == 0) atomicAdd(&g_fft_timeouts, 1u);
+      mbar_wait(&bars[s], (it / S) & 1);
+      return;
+    }
+    const float2* st = smem + s * STAGE;
+    const int tile = blockIdx.x + it * gridDim.x;
+    const int ch = tile / a.tiles_per_ch;
+    const int64_t row0 = (int64_t)(tile % a.tiles_per_ch) * KR;
+    // first half with the even/odd merge:
+    // Z[k] = (X[k] + conj X[M-k]) + i conj(W_N^k) (X[k] - conj X[M-k])
+    for (int jbq = t; jbq < KR * R2; jbq += G::T) {
+      const int n2 = jbq % R2, rho = jbq / R2;
+      float2 v[R1];
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) {
+        const int k = R2 * n1 + n2;
+        float2 xk = st[rho * P + k];
+        float2 xm = st[rho * P + M - k];
+        if (k == 0) {
+          xk.y = 0.f;
+          xm.y = 0.f;
+        }
+        xm = conjf2(xm);
+        const float2 e = cadd(xk, xm);
+        const float2 d = cmul(csub(xk, xm), conjf2(__ldg(&a.tw_n[k])));
+        v[n1] = make_float2(e.x - d.y, e.y + d.x);  // e + i d
+      }
+      reg_dft<R1, true>(v);
+#pragma unroll
+      for (int k1 = 0; k1 < R1; ++k1) {
+        float2 r = v[k1];
+        if (k1 != 0) r = cmul(r, conjf2(__ldg(&a.tw_m[n2 * k1])));
+        xp[(rho * R1 + k1) * G::ROWZ + n2] = r;
+      }
+    }
+    __syncthreads();
+    float2* orow = reinterpret_cast<float2*>(a.out_r + ch * a.cells + row0 * a.nz);
+    for (int jbq = t; jbq < KR * R1; jbq += G::T) {
+      const int k1 = jbq % R1, rho = jbq / R1;
+      float2 u[R2];
+#pragma unroll
+      for (int n2 = 0; n2 < R2; ++n2) u[n2] = xp[(rho * R1 + k1) * G::ROWZ + n2];
+      reg_dft<R2, true>(u);
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) orow[(int64_t)rho * M + k1 + R1 * k2] = u[k2];
+    }
+    __syncthreads();
+    if (t == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(it + S);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+bool pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// Per-device twiddle tables W_L^k (k < L) for L = 32 .. 2048 and the
+// constant-memory W_32 table.  Built outside stream capture (the first call
+// per device and length allocates).
+struct TwiddleCache {
+  std::mutex mu;
+  std::map<std::pair<int, int>, float2*> tables;
+  std::map<int, bool> consts;
+};
+TwiddleCache& twiddles() {
+  static TwiddleCache* c = new TwiddleCache();
+  return *c;
+}
+
+std::vector<float2> twiddle_host(int L) {
+  std::vector<float2> h(L);
+  for (int k = 0; k < L; ++k) {
+    const double ang = -2.0 * M_PI * (double)k / (double)L;
+    h[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+  }
+  return h;
+}
+
+int twiddle_table(int L, cudaStream_t s, const float2** out) {
+  int dev = 0;
+  PMB_CUDA_CHECK(cudaGetDevice(&dev));
+  TwiddleCache& c = twiddles();
+  std::lock_guard<std::mutex> lock(c.mu);
+  if (!c.consts[dev]) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PMB_CUDA_CHECK(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+      set_last_error("pmfft: first use of a mesh size inside stream capture; run once before capturing");
+      return kInvalidArgument;
+    }
+    const std::vector<float2> w = twiddle_host(32);
+    PMB_CUDA_CHECK(cudaMemcpyToSymbol(c_w32, w.data(), 32 * sizeof(float2)));
+    c.consts[dev] = true;
+  }
+  auto key = std::make_pair(dev, L);
+  auto it = c.tables.find(key);
+  if (it == c.tables.end()) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PMB_CUDA_CHECK(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+      set_last_error("pmfft: first use of a mesh size inside stream capture; run once before capturing");
+      return kInvalidArgument;
+    }
+    float2* d = nullptr;
+    PMB_CUDA_CHECK(cudaMalloc(&d, L * sizeof(float2)));
+    const std::vector<float2> h = twiddle_host(L);
+    PMB_CUDA_CHECK(cudaMemcpy(d, h.data(), L * sizeof(float2), cudaMemcpyHostToDevice));
+    it = c.tables.emplace(key, d).first;
+  }
+  *out = it->second;
+  return kOk;
+}
+
+int sm_count() {
+  int dev = 0, n = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n;
+}
+
+template <typename K>
+int persistent_grid(K kernel, int threads, int smem, int ntiles) {
+  int per_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const int g = sm_count() * per_sm;
+  return ntiles < g ? (ntiles > 0 ? ntiles : 1) : g;
+}
+
+constexpr int stages_for(int buf_bytes) {
+  const int s = (200 * 1024) / buf_bytes;
+  return s < 2 ? 2 : (s > 6 ? 6 : s);
+}
+
+template <int R1, int R2, int MODE>
+int launch_col(const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
+  using G = ColGeom<R1, R2>;
+  constexpr int S = stages_for(G::BUF * 8);
+  const int smem = S * G::BUF * 8 + S * 8;
+  auto k = col_pass_kernel<R1, R2, S, MODE>;
+  PMB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  const int grid = persistent_grid(k, G::T, smem, a.ntiles);
+  k<<<grid, G::T, smem, s>>>(map, a);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+template <int MODE>
+int launch_col_len(int L, const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
+  switch (L) {
+    case 64: return launch_col<8, 8, MODE>(map, a, s);
+    case 128: return launch_col<16, 8, MODE>(map, a, s);
+    case 256: return launch_col<16, 16, MODE>(map, a, s);
+    case 512: return launch_col<32, 16, MODE>(map, a, s);
+    case 1024: return launch_col<32, 32, MODE>(map, a, s);
+    default: set_last_error("pmfft: unsupported transform length"); return kUnsupported;
+  }
+}
+
+template <int R1, int R2, bool C2R>
+int launch_z(const ZArgs& a, cudaStream_t s) {
+  using G = ZGeom<R1, R2>;
+  constexpr int M = G::M;
+  const int stage = C2R ? KR * a.P * 8 : KR * M * 8;
+  constexpr int S = 2;
+  const int smem = S * stage + G::XP * 8 + S * 8;
+  auto k = C2R ? z_c2r_kernel<R1, R2, S> : z_r2c_kernel<R1, R2, S>;
+  PMB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  const int grid = persistent_grid(k, G::T, smem, a.ntiles);
+  k<<<grid, G::T, smem, s>>>(a);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+template <bool C2R>
+int launch_z_len(int M, const ZArgs& a, cudaStream_t s) {
+  switch (M) {
+    case 64: return launch_z<8, 8, C2R>(a, s);
+    case 128: return launch_z<16, 8, C2R>(a, s);
+    case 256: return launch_z<16, 16, C2R>(a, s);
+    case 512: return launch_z<32, 16, C2R>(a, s);
+    default: set_last_error("pmfft: unsupported z length"); return kUnsupported;
+  }
+}
+
+int encode(CUtensorMap* map, int rank, const void* base, const cuuint64_t* dims, const cuuint64_t* strides_bytes,
+           const cuuint32_t* box) {
+  auto fn = encode_fn();
+  if (fn == nullptr) {
+    set_last_error("pmfft: cuTensorMapEncodeTiled unavailable");
+    return kCudaError;
+  }
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, rank, const_cast<void*>(base), dims, strides_bytes, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_error("pmfft: tensor map encoding failed");
+    return kCudaError;
+  }
+  return kOk;
+}
+
+}  // namespace
+
+bool pmfft_supported(Mesh3 m) {
+  return pow2_in(m.nx, 64, 1024) && pow2_in(m.ny, 64, 1024) && pow2_in(m.nz, 128, 1024);
+}
+
+int pmfft_row_len(Mesh3 m) { return m.nz / 2 + 8; }
+
+int64_t pmfft_channel_elems(Mesh3 m) { return (int64_t)m.nx * m.ny * pmfft_row_len(m); }
+
+int pmfft_z(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in_c, float* out_r, float2* out_c,
+            cudaStream_t s) {
+  if (!pmfft_supported(m) || batch < 1) {
+    set_last_error("pmfft: unsupported mesh");
+    return kUnsupported;
+  }
+  const int M = m.nz / 2;
+  ZArgs a{};
+  a.in_r = in_r;
+  a.in_c = in_c;
+  a.out_r = out_r;
+  a.out_c = out_c;
+  a.P = pmfft_row_len(m);
+  a.ch = pmfft_channel_elems(m);
+  a.cells = m.cells();
+  a.sb = (int64_t)m.nx * BY * a.P;
+  a.nx = m.nx;
+  a.ny = m.ny;
+  a.nz = m.nz;
+  a.tiles_per_ch = (int)(m.rows() / KR);
+  a.ntiles = a.tiles_per_ch * batch;
+  int st = twiddle_table(M, s, &a.tw_m);
+  if (st != kOk) return st;
+  st = twiddle_table(m.nz, s, &a.tw_n);
+  if (st != kOk) return st;
+  return inverse ? launch_z_len<true>(M, a, s) : launch_z_len<false>(M, a, s);
+}
+
+int pmfft_col(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t, GreenParams g,
+              cudaStream_t s) {
+  if (!pmfft_supported(m) || nbatch < 1 || mode < kYFwd || mode > kXGreenAdj) {
+    set_last_error("pmfft: unsupported mesh or mode");
+    return kUnsupported;
+  }
+  const int P = pmfft_row_len(m);
+  const int nyb = m.ny / BY;
+  const int nch = ch_off + nbatch * n_in(mode);
+  ColArgs a{};
+  a.out = out;
+  a.ch = pmfft_channel_elems(m);
+  a.sb = (int64_t)m.nx * BY * P;
+  a.P = P;
+  a.nx = m.nx;
+  a.ny = m.ny;
+  a.nz = m.nz;
+  a.ch_off = ch_off;
+  a.t = t;
+  a.g = g;
+  CUtensorMap map;
+  int L, st;
+  if (is_y(mode)) {
+    L = m.ny;
+    a.ncolt = P / KT;
+    a.nouter = m.nx;
+    const int box_rows = L < 256 ? L : 256;
+    cuuint64_t dims[4] = {(cuuint64_t)P, (cuuint64_t)BY, (cuuint64_t)m.nx, (cuuint64_t)nyb * nch};
+    cuuint64_t strides[3] = {(cuuint64_t)P * 8, (cuuint64_t)BY * P * 8, (cuuint64_t)a.sb * 8};
+    cuuint32_t box[4] = {(cuuint32_t)KT, (cuuint32_t)BY, 1, (cuuint32_t)(box_rows / BY)};
+    st = encode(&map, 4, in, dims, strides, box);
+  } else {
+    L = m.nx;
+    a.ncolt = BY * P / KT;
+    a.nouter = nyb;
+    const int box_rows = L < 256 ? L : 256;
+    cuuint64_t dims[3] = {(cuuint64_t)BY * P, (cuuint64_t)m.nx, (cuuint64_t)nyb * nch};
+    cuuint64_t strides[2] = {(cuuint64_t)BY * P * 8, (cuuint64_t)a.sb * 8};
+    cuuint32_t box[3] = {(cuuint32_t)KT, (cuuint32_t)box_rows, 1};
+    st = encode(&map, 3, in, dims, strides, box);
+  }
+  if (st != kOk) return st;
+  const int64_t ntiles = (int64_t)a.ncolt * a.nouter * nbatch;
+  if (ntiles > 0x7fffffff) {
+    set_last_error("pmfft: too many tiles");
+    return kUnsupported;
+  }
+  a.ntiles = (int)ntiles;
+  st = twiddle_table(L, s, &a.tw);
+  if (st != kOk) return st;
+  switch (mode) {
+    case kYFwd: return launch_col_len<kYFwd>(L, map, a, s);
+    case kYInv: return launch_col_len<kYInv>(L, map, a, s);
+    case kYInvYZ: return launch_col_len<kYInvYZ>(L, map, a, s);
+    case kYFwdYZ: return launch_col_len<kYFwdYZ>(L, map, a, s);
+    case kXFwd: return launch_col_len<kXFwd>(L, map, a, s);
+    case kXInv: return launch_col_len<kXInv>(L, map, a, s);
+    case kXGreen: return launch_col_len<kXGreen>(L, map, a, s);
+    default: return launch_col_len<kXGreenAdj>(L, map, a, s);
+  }
+}
+
+int pmfft_timeouts(unsigned int* count) {
+  PMB_CUDA_CHECK(cudaMemcpyFromSymbol(count, g_fft_timeouts, sizeof(unsigned int)));
+  return kOk;
+}
+
+// Forward force spectral chain: real source (1 channel) -> force meshes (3).
+// work holds 5 channels of pmfft_channel_elems values.
+int pmfft_force(Mesh3 m, const float* src, float* force_meshes, float2* work, SpecTables t, GreenParams g,
+                cudaStream_t s) {
+  const int64_t C = pmfft_channel_elems(m);
+  float2* aq = work;       // A, then W (channel 0) and Q (channel 1)
+  float2* fp = work + 2 * C;  // B (channel 0), then F'_x, F'_y, F'_z
+  GreenParams none = g;
+  int st = pmfft_z(m, 0, 1, src, nullptr, nullptr, aq, s);
+  if (st != kOk) return st;
+  if ((st = pmfft_col(m, kYFwd, 1, 0, aq, fp, t, none, s)) != kOk) return st;
+  if ((st = pmfft_col(m, kXGreen, 1, 0, fp, aq, t, g, s)) != kOk) return st;
+  if ((st = pmfft_col(m, kYInv, 1, 0, aq, fp, t, none, s)) != kOk) return st;
+  if ((st = pmfft_col(m, kYInvYZ, 1, 1, aq, fp + C, t, none, s)) != kOk) return st;
+  return pmfft_z(m, 1, 3, nullptr, fp, force_meshes, nullptr, s);
+}
+
+// Adjoint spectral chain: three mesh cotangents -> source cotangent.
+int pmfft_force_adjoint(Mesh3 m, const float* mesh_cot, float* src_cot, float2* work, SpecTables t, GreenParams g,
+                        cudaStream_t s) {
+  const int64_t C = pmfft_channel_elems(m);
+  float2* a3 = work;          // A_x, A_y, A_z; then S' (0) and S'' (1)
+  float2* bb = work + 3 * C;  // B_x, b
+  int st = pmfft_z(m, 0, 3, mesh_cot, nullptr, nullptr, a3, s);
+  if (st != kOk) return st;
+  if ((st = pmfft_col(m, kYFwd, 1, 0, a3, bb, t, g, s)) != kOk) return st;
+  if ((st = pmfft_col(m, kYFwdYZ, 1, 1, a3, bb + C, t, g, s)) != kOk) return st;
+  if ((st = pmfft_col(m, kXGreenAdj, 1, 0, bb, a3, t, g, s)) != kOk) return st;
+  if ((st = pmfft_col(m, kYInv, 1, 0, a3, a3 + C, t, g, s)) != kOk) return st;
+  return pmfft_z(m, 1, 1, nullptr, a3 + C, src_cot, nullptr, s);
+}
+
+}  // namespace pmb

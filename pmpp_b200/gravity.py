@@ -16,7 +16,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from ._lib import call, lib
+from ._lib import call, lib, pmfft_active
 from .runtime import StageTimer, ptr, require_cuda, stream_handle, workspace
 
 
@@ -28,17 +28,23 @@ def _stage_buffers(n, conf, dev):
     """Workspace views shared by the staged force and force adjoint."""
     L = lib()
     nx, ny, nz = conf.mesh_shape
-    M = conf.mesh_size
-    Mc = nx * ny * (nz // 2 + 1)
     sorted_buf = workspace(L.pmb_sorted_bytes(n, nx, ny, nz), dev, "st_sorted")
     sort_scr = workspace(L.pmb_sort_scratch_bytes(n, nx, ny, nz), dev, "st_sortscr")
     s16 = workspace(16, dev, "st_s16")
-    real3 = workspace(12 * M, dev, "st_real3")
+    real3 = workspace(12 * conf.mesh_size, dev, "st_real3")
+    return sorted_buf, sort_scr, s16, real3
+
+
+def _cufft_buffers(conf, dev):
+    """Half spectra and cuFFT work area of the cuFFT route."""
+    L = lib()
+    nx, ny, nz = conf.mesh_shape
+    Mc = nx * ny * (nz // 2 + 1)
     spec3 = workspace(24 * Mc, dev, "st_spec3")
     spec1 = workspace(8 * Mc, dev, "st_spec1")
     fw = max(L.pmb_fft_work_bytes(nx, ny, nz, 3), L.pmb_fft_work_bytes(nx, ny, nz, 1))
     work = workspace(fw, dev, "st_fftwork")
-    return sorted_buf, sort_scr, s16, real3, spec3, spec1, work
+    return spec3, spec1, work
 
 
 class _NoTimer:
@@ -59,9 +65,7 @@ def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F
     nx, ny, nz = conf.mesh_shape
     dev = disp.device
     s = stream_handle(dev)
-    sorted_buf, sort_scr, s16, real3, spec3, spec1, work = _stage_buffers(n, conf, dev)
-    if src_hat_out is not None:
-        spec1 = src_hat_out
+    sorted_buf, sort_scr, s16, real3 = _stage_buffers(n, conf, dev)
     timer = _NoTimer() if timer is None else timer
     t = timer.start()
     call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
@@ -70,13 +74,36 @@ def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F
     call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 1, None, 0, float(conf.mesh_size / conf.ptcl_num),
          1, 1.5 * _om32(omega_m), real3.data_ptr(), s16.data_ptr(), s)
     t = timer.mark("scatter", t)
-    call("pmb_rfft3", nx, ny, nz, 1, real3.data_ptr(), spec1.data_ptr(), work.data_ptr(), s)
-    t = timer.mark("fft_r2c", t)
-    call("pmb_green_gradient", spec1.data_ptr(), spec3.data_ptr(), nx, ny, nz, tables.data_ptr(),
-         int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, float(1.0 / conf.mesh_size), s)
-    t = timer.mark("green_gradient", t)
-    call("pmb_irfft3", nx, ny, nz, 3, spec3.data_ptr(), F.data_ptr(), work.data_ptr(), s)
-    t = timer.mark("fft_c2r", t)
+    masks = int(conf.has_particle_nyquist_masks)
+    if src_hat_out is None and pmfft_active(nx, ny, nz):
+        # hand-written pass chain (pmfft.cu): z R2C, y, x + Green + x^-1, y^-1, z C2R
+        C8 = 8 * lib().pmb_pmfft_channel_elems(nx, ny, nz)
+        pm = workspace(5 * C8, dev, "st_pm5")
+        aq, fp = pm.data_ptr(), pm.data_ptr() + 2 * C8
+        call("pmb_pmfft_z", nx, ny, nz, 0, 1, real3.data_ptr(), aq, s)
+        t = timer.mark("fft_z_r2c", t)
+        call("pmb_pmfft_col", nx, ny, nz, 0, 1, 0, aq, fp, tables.data_ptr(), masks, None, None, 0, 1.0, s)
+        t = timer.mark("fft_y", t)
+        call("pmb_pmfft_col", nx, ny, nz, 6, 1, 0, fp, aq, tables.data_ptr(), masks, ptr(transfer), ptr(radial), rl,
+             float(1.0 / conf.mesh_size), s)
+        t = timer.mark("fft_x_green", t)
+        call("pmb_pmfft_col", nx, ny, nz, 1, 1, 0, aq, fp, tables.data_ptr(), masks, None, None, 0, 1.0, s)
+        t = timer.mark("fft_y_inv", t)
+        call("pmb_pmfft_col", nx, ny, nz, 2, 1, 1, aq, fp + C8, tables.data_ptr(), masks, None, None, 0, 1.0, s)
+        t = timer.mark("fft_y_inv_yz", t)
+        call("pmb_pmfft_z", nx, ny, nz, 1, 3, fp, F.data_ptr(), s)
+        t = timer.mark("fft_z_c2r3", t)
+    else:
+        spec3, spec1, work = _cufft_buffers(conf, dev)
+        if src_hat_out is not None:
+            spec1 = src_hat_out
+        call("pmb_rfft3", nx, ny, nz, 1, real3.data_ptr(), spec1.data_ptr(), work.data_ptr(), s)
+        t = timer.mark("fft_r2c", t)
+        call("pmb_green_gradient", spec1.data_ptr(), spec3.data_ptr(), nx, ny, nz, tables.data_ptr(), masks, gk,
+             ptr(transfer), ptr(radial), rl, float(1.0 / conf.mesh_size), s)
+        t = timer.mark("green_gradient", t)
+        call("pmb_irfft3", nx, ny, nz, 3, spec3.data_ptr(), F.data_ptr(), work.data_ptr(), s)
+        t = timer.mark("fft_c2r", t)
     call("pmb_gather_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc.data_ptr(), ptr(vel_kick),
          float(kick), s)
     timer.mark("gather", t)
@@ -93,7 +120,7 @@ def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, r
     nx, ny, nz = conf.mesh_shape
     dev = disp.device
     s = stream_handle(dev)
-    sorted_buf, sort_scr, s16, real3, spec3, spec1, work = _stage_buffers(n, conf, dev)
+    sorted_buf, sort_scr, s16, real3 = _stage_buffers(n, conf, dev)
     timer = _NoTimer() if timer is None else timer
     t = timer.start()
     call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), None, 0.0, n, nx, ny, nz, float(conf.cell_size),
@@ -106,17 +133,38 @@ def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, r
     call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, cot_sorted.data_ptr(), 1, 0.0, 0, 1.0,
          real3.data_ptr(), s16.data_ptr(), s)
     t = timer.mark("scatter3", t)
-    call("pmb_rfft3", nx, ny, nz, 3, real3.data_ptr(), spec3.data_ptr(), work.data_ptr(), s)
-    t = timer.mark("fft_r2c", t)
-    if transfer_cot_out is not None:
-        call("pmb_transfer_cot", spec3.data_ptr(), src_hat.data_ptr(), nx, ny, nz, tables.data_ptr(),
-             int(conf.has_particle_nyquist_masks), int(transfer_cot_out.numel()), transfer_cot_out.data_ptr(), s)
     post = float(np.float32(1.5 * _om32(omega_m)) / conf.mesh_size)
-    call("pmb_green_gradient_adjoint", spec3.data_ptr(), spec1.data_ptr(), nx, ny, nz, tables.data_ptr(),
-         int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, post, s)
-    t = timer.mark("green_gradient", t)
-    call("pmb_irfft3", nx, ny, nz, 1, spec1.data_ptr(), real3.data_ptr(), work.data_ptr(), s)
-    t = timer.mark("fft_c2r", t)
+    masks = int(conf.has_particle_nyquist_masks)
+    if transfer_cot_out is None and pmfft_active(nx, ny, nz):
+        # transposed pass chain: z R2C x3, y (x channel; y and z folded), x + adjoint multiplier + x^-1, y^-1, z C2R
+        C8 = 8 * lib().pmb_pmfft_channel_elems(nx, ny, nz)
+        pm = workspace(5 * C8, dev, "st_pm5")
+        a3, bb = pm.data_ptr(), pm.data_ptr() + 3 * C8
+        call("pmb_pmfft_z", nx, ny, nz, 0, 3, real3.data_ptr(), a3, s)
+        t = timer.mark("fft_z_r2c3", t)
+        call("pmb_pmfft_col", nx, ny, nz, 0, 1, 0, a3, bb, tables.data_ptr(), masks, None, None, 0, 1.0, s)
+        t = timer.mark("fft_y", t)
+        call("pmb_pmfft_col", nx, ny, nz, 3, 1, 1, a3, bb + C8, tables.data_ptr(), masks, None, None, 0, 1.0, s)
+        t = timer.mark("fft_y_yz", t)
+        call("pmb_pmfft_col", nx, ny, nz, 7, 1, 0, bb, a3, tables.data_ptr(), masks, ptr(transfer), ptr(radial), rl,
+             post, s)
+        t = timer.mark("fft_x_green_adj", t)
+        call("pmb_pmfft_col", nx, ny, nz, 1, 1, 0, a3, a3 + C8, tables.data_ptr(), masks, None, None, 0, 1.0, s)
+        t = timer.mark("fft_y_inv", t)
+        call("pmb_pmfft_z", nx, ny, nz, 1, 1, a3 + C8, real3.data_ptr(), s)
+        t = timer.mark("fft_z_c2r", t)
+    else:
+        spec3, spec1, work = _cufft_buffers(conf, dev)
+        call("pmb_rfft3", nx, ny, nz, 3, real3.data_ptr(), spec3.data_ptr(), work.data_ptr(), s)
+        t = timer.mark("fft_r2c", t)
+        if transfer_cot_out is not None:
+            call("pmb_transfer_cot", spec3.data_ptr(), src_hat.data_ptr(), nx, ny, nz, tables.data_ptr(), masks,
+                 int(transfer_cot_out.numel()), transfer_cot_out.data_ptr(), s)
+        call("pmb_green_gradient_adjoint", spec3.data_ptr(), spec1.data_ptr(), nx, ny, nz, tables.data_ptr(), masks,
+             gk, ptr(transfer), ptr(radial), rl, post, s)
+        t = timer.mark("green_gradient", t)
+        call("pmb_irfft3", nx, ny, nz, 1, spec1.data_ptr(), real3.data_ptr(), work.data_ptr(), s)
+        t = timer.mark("fft_c2r", t)
     call("pmb_interp_grad_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 1, real3.data_ptr(), None,
          float(conf.mesh_size / conf.ptcl_num), float(conf.cell_size), 1, disp_cot.data_ptr(), None, None, s)
     timer.mark("scatter_adjoint", t)

@@ -144,6 +144,53 @@ def run_set(ptcl, conf, reps, peak):
     return out
 
 
+def pmfft_stages(conf, reps, peak, only=None):
+    """Each pass of the hand-written FFT chain (pmfft.cu) on random inputs."""
+    dev = conf.device
+    L = lib()
+    s = stream_handle(dev)
+    nx, ny, nz = conf.mesh_shape
+    if not L.pmb_pmfft_supported(nx, ny, nz):
+        return {}
+    M = conf.mesh_size
+    Mc = nx * ny * (nz // 2 + 1)
+    C = L.pmb_pmfft_channel_elems(nx, ny, nz)
+    tables = conf.spectral_tables("mesh", dev, 0).data_ptr()
+    masks = int(conf.has_particle_nyquist_masks)
+    g = torch.Generator(device="cpu").manual_seed(5)
+    real3 = torch.randn((3, nx, ny, nz), generator=g).to(dev)
+    real3b = torch.empty_like(real3)
+    pa = torch.zeros(3 * C, dtype=torch.complex64, device=dev)
+    pb_ = torch.zeros(3 * C, dtype=torch.complex64, device=dev)
+    a, b = pa.data_ptr(), pb_.data_ptr()
+    C8 = 8 * C
+    inv_m = float(1.0 / M)
+    col = lambda mode, ch_off, i, o, post=1.0: call("pmb_pmfft_col", nx, ny, nz, mode, 1, ch_off, i, o, tables, masks,
+                                                    None, None, 0, post, s)
+    call("pmb_pmfft_z", nx, ny, nz, 0, 3, real3.data_ptr(), a, s)
+    stages = {
+        "fft_z_r2c": lambda: call("pmb_pmfft_z", nx, ny, nz, 0, 1, real3.data_ptr(), b, s),
+        "fft_z_r2c3": lambda: call("pmb_pmfft_z", nx, ny, nz, 0, 3, real3.data_ptr(), b, s),
+        "fft_y": lambda: col(0, 0, a, b),
+        "fft_y_yz": lambda: col(3, 1, a, b),
+        "fft_x_green": lambda: col(6, 0, a, b, inv_m),
+        "fft_x_green_adj": lambda: col(7, 0, a, b, inv_m),
+        "fft_y_inv": lambda: col(1, 0, a, b),
+        "fft_y_inv_yz": lambda: col(2, 0, a, b),
+        "fft_z_c2r": lambda: call("pmb_pmfft_z", nx, ny, nz, 1, 1, a, real3b.data_ptr(), s),
+        "fft_z_c2r3": lambda: call("pmb_pmfft_z", nx, ny, nz, 1, 3, a, real3b.data_ptr(), s),
+    }
+    out = {}
+    for name, fn in stages.items():
+        if only and name not in only:
+            continue
+        ms = _time(fn, reps)
+        alg = algorithmic_bytes(name, 0, M, Mc=Mc, R=nx * ny)
+        gbs = alg / (ms * 1e-3) / 1e9
+        out[name] = {"ms": round(ms, 4), "algorithmic_bytes": alg, "GB/s": round(gbs, 1), "frac_hbm": round(gbs / peak, 4)}
+    return out
+
+
 def load_peak():
     path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
     try:
@@ -159,7 +206,19 @@ def main(argv=None):
     ap.add_argument("--mesh", type=int, default=2)
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--sets", default="U,K")
+    ap.add_argument("--pmfft-shape", type=int, nargs=3, default=None,
+                    help="time only the FFT pass chain on this mesh shape")
+    ap.add_argument("--stages", default=None, help="comma-separated pass names (with --pmfft-shape)")
     args = ap.parse_args(argv)
+    if args.pmfft_shape is not None:
+        nx, ny, nz = args.pmfft_shape
+        conf = Configuration(4.0, (nx // 2, ny // 2, nz // 2), 2, a_start=0.1, device="cuda")
+        peak, kind = load_peak()
+        only = args.stages.split(",") if args.stages else None
+        res = {"config": {"mesh_shape": [nx, ny, nz], "reps": args.reps}, "peak_gbs": peak, "peak_kind": kind,
+               "pmfft": pmfft_stages(conf, args.reps, peak, only)}
+        print(json.dumps(res))
+        return res
     if args.ptcl % 64:
         raise ValueError("--ptcl must be a multiple of 64 (set K tiles the 64^3 run)")
     conf = Configuration(4.0, (args.ptcl, ) * 3, args.mesh, a_start=0.1, device="cuda")
@@ -171,6 +230,8 @@ def main(argv=None):
         res[name] = run_set(ptcl, conf, args.reps, peak)
         del ptcl
         torch.cuda.empty_cache()
+    res["pmfft"] = pmfft_stages(conf, args.reps, peak)
+    torch.cuda.empty_cache()
     print(json.dumps(res))
     return res
 

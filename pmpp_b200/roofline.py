@@ -5,7 +5,8 @@ rows, T distinct mesh cells touched by the particles' CIC corners (at most
 min(M, 8N); the upper bound is used when T is not measured).  Every input is
 counted once and every output once, at the sizes of the reference's data
 layout (pmid int16 x 3 + disp float32 x 3 = 18 B per particle); re-reads,
-halo redundancy and cuFFT's extra passes are not counted, so a stage's
+halo redundancy, the pass chain's zero padding and cuFFT's extra passes are not
+counted, so a stage's
 achieved GB/s is directly comparable with the HBM copy bandwidth.
 """
 from __future__ import annotations
@@ -27,6 +28,17 @@ def algorithmic_bytes(op, N, M, Mc=None, R=None, T=None):
         "fft_r2c_x3": 3 * (4 * M + 8 * Mc),
         "fft_c2r": 8 * Mc + 4 * M,
         "fft_c2r_x3": 3 * (8 * Mc + 4 * M),
+        # hand-written pass chain (pmfft.cu), complex channels counted at Mc
+        "fft_z_r2c": 4 * M + 8 * Mc,
+        "fft_z_r2c3": 3 * (4 * M + 8 * Mc),
+        "fft_y": 16 * Mc,
+        "fft_y_yz": 24 * Mc,
+        "fft_y_inv": 16 * Mc,
+        "fft_y_inv_yz": 24 * Mc,
+        "fft_x_green": 24 * Mc,
+        "fft_x_green_adj": 24 * Mc,
+        "fft_z_c2r": 8 * Mc + 4 * M,
+        "fft_z_c2r3": 3 * (8 * Mc + 4 * M),
         "green_gradient": 8 * Mc + 24 * Mc,
         "green_gradient_adjoint": 24 * Mc + 8 * Mc,
         "kdk": 6 * N + 24 * N + 24 * N + 12 * N,
