@@ -140,7 +140,9 @@ int pmb_green_gradient_adjoint(const void* grad_cot_hat, void* src_cot_hat, int 
  *   those of pmb_green_gradient (tables may be null for modes 0, 1, 4, 5).
  * pmb_set_pmfft(0) routes pmb_force / pmb_force_vjp through cuFFT and the
  * separate multiplier kernels instead (default 1).
- * pmb_pmfft_timeouts: bounded copy waits in these passes that gave up. */
+ * pmb_pmfft_timeouts: bounded copy waits in these passes that gave up.
+ * pmb_pmfft_set_col_ctas(1 or 2): resident CTAs per SM of the column passes
+ *   (a tuning knob; results are identical). */
 int pmb_set_pmfft(int enabled);
 int pmb_pmfft_supported(int nx, int ny, int nz);
 int64_t pmb_pmfft_channel_elems(int nx, int ny, int nz);
@@ -149,6 +151,7 @@ int pmb_pmfft_col(int nx, int ny, int nz, int mode, int nbatch, int ch_off, cons
                   const float* tables, int has_masks, const float* transfer, const float* radial, int radial_len,
                   float post_scale, void* stream);
 int pmb_pmfft_timeouts(uint32_t* count);
+int pmb_pmfft_set_col_ctas(int ctas);
 
 /* ---------------- fused PM force ------------------------------------------
  * One PM force evaluation (nbody/gravity.py:786-814 -> _gravity_from_density

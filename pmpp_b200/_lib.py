@@ -35,6 +35,7 @@ _SIGS = {
     "pmb_pmfft_col": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_int, c_p, c_p, c_int, c_f,
                               c_p]),
     "pmb_pmfft_timeouts": (c_int, [c_p]),
+    "pmb_pmfft_set_col_ctas": (c_int, [c_int]),
     "pmb_rfft3": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
     "pmb_irfft3": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
     "pmb_green_gradient": (c_int, [c_p, c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p, c_int, c_f, c_p]),

@@ -241,6 +241,8 @@ int pmb_pmfft_col(int nx, int ny, int nz, int mode, int nbatch, int ch_off, cons
                    make_green(0, transfer, radial, radial_len, post_scale), S(stream));
 }
 
+int pmb_pmfft_set_col_ctas(int ctas) { return pmfft_set_col_ctas(ctas); }
+
 int pmb_pmfft_timeouts(uint32_t* count) {
   PMB_REQUIRE(count != nullptr, "pmb_pmfft_timeouts: null output");
   return pmfft_timeouts(count);

@@ -62,5 +62,6 @@ int pmfft_force(Mesh3 m, const float* src, float* force_meshes, float2* work, Sp
 int pmfft_force_adjoint(Mesh3 m, const float* mesh_cot, float* src_cot, float2* work, SpecTables t, GreenParams g,
                         cudaStream_t s);
 int pmfft_timeouts(unsigned int* count);
+int pmfft_set_col_ctas(int ctas);
 
 }  // namespace pmb

@@ -135,14 +135,14 @@ __device__ __forceinline__ void reg_dft(float2 (&v)[R]) {
 // holds x[A2*n1 + n2], n1 < A1; A1-point DFTs, twiddle W_L^(n2 k1), written
 // transposed to buf[k1][n2][c] (rows padded by 8 values against bank conflicts).
 template <int A1, int A2, bool INV>
-__device__ __forceinline__ void four_step_a(float2 (&v)[A1], float2* buf, int n2, int c, const float2* __restrict__ tw) {
+__device__ __forceinline__ void four_step_a(float2 (&v)[A1], float2* buf, int n2, int c, const float2* tw) {
   constexpr int ROW = A2 * KT + 8;
   reg_dft<A1, INV>(v);
 #pragma unroll
   for (int k1 = 0; k1 < A1; ++k1) {
     float2 r = v[k1];
     if (k1 != 0) {
-      float2 w = __ldg(&tw[n2 * k1]);
+      float2 w = tw[n2 * k1];
       if (INV) w.y = -w.y;
       r = cmul(r, w);
     }
@@ -188,6 +188,11 @@ __host__ __device__ constexpr bool is_y(int mode) { return mode <= kYFwdYZ; }
 __host__ __device__ constexpr int n_in(int mode) { return (mode == kYFwdYZ || mode == kXGreenAdj) ? 2 : 1; }
 __host__ __device__ constexpr int n_out(int mode) { return (mode == kYInvYZ || mode == kXGreen) ? 2 : 1; }
 
+// floats of per-axis tables a column pass keeps in shared memory
+__host__ __device__ constexpr int col_table_floats(int mode, int L) {
+  return (mode == kXGreen || mode == kXGreenAdj) ? 3 * L : ((mode == kYInvYZ || mode == kYFwdYZ) ? L : 0);
+}
+
 struct ColArgs {
   float2* out;
   int64_t ch;      // complex values per channel
@@ -224,37 +229,51 @@ __device__ __forceinline__ bool kz_valid(int kz, int nz) { return kz <= nz / 2; 
 
 // Green multiplier of the source value at (ix, iy, iz): phi = K(k) S, K =
 // post * mask * T * (-1/k^2), zero at k = 0 (pmb_spectral_device.cuh has the
-// reference citations).
-__device__ __forceinline__ float green_scalar(const ColArgs& a, int ix, int iy, int iz) {
-  const Mesh3 m{a.nx, a.ny, a.nz};
-  const float k2 = k2_of(a.t, ix, iy, iz);
+// reference citations).  kx2 / mx are the x-axis tables in shared memory;
+// kyz2 = ky^2 + kz^2 and myz = my * mz are the column's constants.
+__device__ __forceinline__ float green_scalar(const ColArgs& a, const float* kx2, const float* mx, float kyz2,
+                                              float myz, int ix, int iy, int iz) {
+  const float k2 = kx2[ix] + kyz2;
   if (k2 == 0.f) return 0.f;
-  float K = __fdiv_rn(-a.g.post_scale, k2);
-  if (a.t.mx != nullptr) K = __fmul_rn(K, __fmul_rn(__fmul_rn(a.t.mx[ix], a.t.my[iy]), a.t.mz[iz]));
+  float K = (-a.g.post_scale * myz * mx[ix]) * __frcp_rn(k2);
   if (a.g.transfer != nullptr || a.g.radial != nullptr) {
+    const Mesh3 m{a.nx, a.ny, a.nz};
     const int64_t j = ((int64_t)ix * a.ny + iy) * (a.nz / 2 + 1) + iz;
-    K = __fmul_rn(K, transfer_of(a.g, a.t, j, ix, iy, iz, m));
+    K *= transfer_of(a.g, a.t, j, ix, iy, iz, m);
   }
   return K;
 }
 
 // Persistent column pass: a ring of S stages, stage slot i holds input q =
 // i % NIN of tile i / NIN of this CTA.
-template <int R1, int R2, int S, int MODE>
-__global__ void __launch_bounds__(ColGeom<R1, R2>::T, 1)
+template <int R1, int R2, int S, int MODE, int CTAS>
+__global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
     col_pass_kernel(const __grid_constant__ CUtensorMap tin, const ColArgs a) {
   using G = ColGeom<R1, R2>;
   constexpr int L = G::L;
   constexpr int NIN = n_in(MODE);
   constexpr bool YP = is_y(MODE);
   extern __shared__ __align__(128) float2 smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S * G::BUF);
+  // [S stages][twiddles W_L^k][axis tables][barriers]
+  float2* stw = smem + S * G::BUF;
+  float* tab = reinterpret_cast<float*>(stw + L);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tab + col_table_floats(MODE, L));
   const int t = threadIdx.x;
   const int c = t % KT;
   const int tiles_mine = a.ntiles > (int)blockIdx.x ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const int slots = tiles_mine * NIN;
   if (t == 0)
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+  for (int i = t; i < L; i += G::T) {
+    stw[i] = a.tw[i];
+    if constexpr (MODE == kYInvYZ || MODE == kYFwdYZ) tab[i] = a.t.cy[i];
+    if constexpr (MODE == kXGreen || MODE == kXGreenAdj) {
+      const float kx = a.t.kx[i];
+      tab[i] = kx * kx;                                  // kx^2
+      tab[L + i] = a.t.cx[i];                            // c_x
+      tab[2 * L + i] = a.t.mx != nullptr ? a.t.mx[i] : 1.f;  // particle-Nyquist mask
+    }
+  }
   __syncthreads();
 
   // tile -> (column tile, outer, batch)
@@ -321,7 +340,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, 1)
       for (int n1 = 0; n1 < R1; ++n1) v[n1] = buf[(R2 * n1 + q) * KT + c];
     }
     __syncthreads();
-    if (ja) four_step_a<R1, R2, INV>(v, buf, q, c, a.tw);
+    if (ja) four_step_a<R1, R2, INV>(v, buf, q, c, stw);
     __syncthreads();
     if (jb) four_step_b<R1, R2, INV>(u, buf, q, c);
     (void)ymul_c;
@@ -332,7 +351,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, 1)
   // decomposition (R2, R1); result w[k2'] at index k1' + R2 k2' (k1' = q).
   auto inverse_held = [&](float2* buf, float2 (&u)[R2], float2 (&w)[R1]) {
     __syncthreads();
-    if (jb) four_step_a<R2, R1, true>(u, buf, q, c, a.tw);
+    if (jb) four_step_a<R2, R1, true>(u, buf, q, c, stw);
     __syncthreads();
     if (ja) four_step_b<R2, R1, true>(w, buf, q, c);
   };
@@ -370,7 +389,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, 1)
       transform(i0, u, std::false_type{}, 0.f, false);
       if (jb) {
 #pragma unroll
-        for (int k2 = 0; k2 < R2; ++k2) acc[k2] = i_times(-a.t.cy[q + R1 * k2], u[k2]);
+        for (int k2 = 0; k2 < R2; ++k2) acc[k2] = i_times(-tab[q + R1 * k2], u[k2]);
       }
       release(i0);
       if (!acquire(i0 + 1)) return;
@@ -396,11 +415,11 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, 1)
 #pragma unroll
         for (int n1 = 0; n1 < R1; ++n1) {
           v[n1] = buf[(R2 * n1 + q) * KT + c];
-          vy[n1] = i_times(a.t.cy[R2 * n1 + q], v[n1]);
+          vy[n1] = i_times(tab[R2 * n1 + q], v[n1]);
         }
       }
       __syncthreads();
-      if (ja) four_step_a<R1, R2, true>(vy, buf, q, c, a.tw);
+      if (ja) four_step_a<R1, R2, true>(vy, buf, q, c, stw);
       __syncthreads();
       auto store = [&](int chan, int k2, float2 val) {
         const int y = q + R1 * k2;
@@ -412,7 +431,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, 1)
         for (int k2 = 0; k2 < R2; ++k2) store(0, k2, kv ? u[k2] : make_float2(0.f, 0.f));
       }
       __syncthreads();
-      if (ja) four_step_a<R1, R2, true>(v, buf, q, c, a.tw);
+      if (ja) four_step_a<R1, R2, true>(v, buf, q, c, stw);
       __syncthreads();
       if (jb) {
         four_step_b<R1, R2, true>(u, buf, q, c);
@@ -426,6 +445,11 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, 1)
       const int yi = j / a.P, kz = j - yi * a.P;
       const int iy = outer * BY + yi;
       const bool kv = kz_valid(kz, a.nz);
+      float kyz2 = 0.f, myz = 1.f;
+      if (kv) {
+        kyz2 = a.t.ky[iy] * a.t.ky[iy] + a.t.kz[kz] * a.t.kz[kz];
+        if (a.t.mx != nullptr) myz = a.t.my[iy] * a.t.mz[kz];
+      }
       float2* buf = smem + (i0 % S) * G::BUF;
       transform(i0, u, std::false_type{}, 0.f, false);
       float2 w[R2];
@@ -433,9 +457,9 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, 1)
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) {
           const int kx = q + R1 * k2;
-          const float K = kv ? green_scalar(a, kx, iy, kz) : 0.f;
+          const float K = kv ? green_scalar(a, tab, tab + 2 * L, kyz2, myz, kx, iy, kz) : 0.f;
           u[k2] = make_float2(K * u[k2].x, K * u[k2].y);  // phi
-          w[k2] = i_times(a.t.cx[kx], u[k2]);
+          w[k2] = i_times(tab[L + kx], u[k2]);
         }
       }
       float2 o[R1];
@@ -458,11 +482,16 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, 1)
       const int yi = j / a.P, kz = j - yi * a.P;
       const int iy = outer * BY + yi;
       const bool kv = kz_valid(kz, a.nz);
+      float kyz2 = 0.f, myz = 1.f;
+      if (kv) {
+        kyz2 = a.t.ky[iy] * a.t.ky[iy] + a.t.kz[kz] * a.t.kz[kz];
+        if (a.t.mx != nullptr) myz = a.t.my[iy] * a.t.mz[kz];
+      }
       float2 acc[R2];
       transform(i0, u, std::false_type{}, 0.f, false);
       if (jb) {
 #pragma unroll
-        for (int k2 = 0; k2 < R2; ++k2) acc[k2] = i_times(-a.t.cx[q + R1 * k2], u[k2]);
+        for (int k2 = 0; k2 < R2; ++k2) acc[k2] = i_times(-tab[L + q + R1 * k2], u[k2]);
       }
       release(i0);
       if (!acquire(i0 + 1)) return;
@@ -472,7 +501,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, 1)
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) {
           const int kx = q + R1 * k2;
-          const float K = kv ? green_scalar(a, kx, iy, kz) : 0.f;
+          const float K = kv ? green_scalar(a, tab, tab + 2 * L, kyz2, myz, kx, iy, kz) : 0.f;
           const float2 s = cadd(acc[k2], u[k2]);
           acc[k2] = make_float2(K * s.x, K * s.y);
         }
@@ -497,9 +526,11 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, 1)
 template <int R1, int R2>
 struct ZGeom {
   static constexpr int M = R1 * R2;  // complex length = nz / 2
+  static constexpr int P = M + 8;    // spectral row length
   static constexpr int T = 256;
   static constexpr int ROWZ = R2 + 1;
   static constexpr int XP = KR * R1 * ROWZ;  // transpose buffer (float2)
+  static constexpr int TW = M + M + 8;       // W_M^k (k < M), W_N^k (k <= M), padded
 };
 
 struct ZArgs {
@@ -510,30 +541,40 @@ struct ZArgs {
   int64_t ch;      // complex values per spectral channel
   int64_t cells;   // reals per real channel
   int64_t sb;      // nx * BY * P
-  int P, nx, ny, nz;
+  int nx, ny, nz;
   int tiles_per_ch, ntiles;
   const float2* tw_m;  // W_M^k, k < M
   const float2* tw_n;  // W_nz^k, k < nz
 };
 
 // spectral row offset of mesh row (x, y)
+template <int P>
 __device__ __forceinline__ int64_t spec_row(const ZArgs& a, int x, int y) {
-  return (int64_t)(y / BY) * a.sb + ((int64_t)x * BY + y % BY) * a.P;
+  return (int64_t)(y / BY) * a.sb + ((int64_t)x * BY + y % BY) * P;
+}
+
+// twiddles of the z passes into shared memory: W_M^k then W_N^k (k <= M)
+template <int M>
+__device__ __forceinline__ void load_z_twiddles(const ZArgs& a, float2* tw) {
+  for (int i = threadIdx.x; i < M; i += blockDim.x) tw[i] = a.tw_m[i];
+  for (int i = threadIdx.x; i <= M; i += blockDim.x) tw[M + i] = a.tw_n[i];
 }
 
 // Real-to-complex along z: KR rows of nz reals -> KR rows of P complex.
 template <int R1, int R2, int S>
 __global__ void __launch_bounds__(256, 1) z_r2c_kernel(const ZArgs a) {
   using G = ZGeom<R1, R2>;
-  constexpr int M = G::M;
+  constexpr int M = G::M, P = G::P;
   constexpr int STAGE = KR * M;  // float2
   extern __shared__ __align__(128) float2 smem[];
   float2* xp = smem + S * STAGE;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(xp + G::XP);
+  float2* tw = xp + G::XP;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tw + G::TW);
   const int t = threadIdx.x;
   const int tiles_mine = a.ntiles > (int)blockIdx.x ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   if (t == 0)
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+  load_z_twiddles<M>(a, tw);
   __syncthreads();
   auto issue = [&](int i) {
     if (i >= tiles_mine) return;
@@ -559,6 +600,7 @@ __global__ void __launch_bounds__(256, 1) z_r2c_kernel(const ZArgs a) {
     const int ch = tile / a.tiles_per_ch;
     const int row0 = (tile % a.tiles_per_ch) * KR;
     // first half: job (n2, rho)
+#pragma unroll 1
     for (int jbq = t; jbq < KR * R2; jbq += G::T) {
       const int n2 = jbq % R2, rho = jbq / R2;
       float2 v[R1];
@@ -568,43 +610,51 @@ __global__ void __launch_bounds__(256, 1) z_r2c_kernel(const ZArgs a) {
 #pragma unroll
       for (int k1 = 0; k1 < R1; ++k1) {
         float2 r = v[k1];
-        if (k1 != 0) r = cmul(r, __ldg(&a.tw_m[n2 * k1]));
+        if (k1 != 0) r = cmul(r, tw[n2 * k1]);
         xp[(rho * R1 + k1) * G::ROWZ + n2] = r;
       }
     }
     __syncthreads();
-    // second half: job (k1, rho); Z[k1 + R1 k2] back into the stage, natural order
+    if (t == 0) {  // the stage is consumed: start the copy of tile it + S
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(it + S);
+    }
+    // second half: job (k1, rho) holds Z[k1 + R1 k2]; the even/odd split
+    // X[k] = E[k] + W_N^k O[k] needs Z[M - k], held by the lane of job
+    // ((R1 - k1) mod R1, rho) of the same warp (jobs run k1 fastest).
+    const int x = row0 / a.ny, y0 = row0 % a.ny;
+    float2* orow = a.out_c + ch * a.ch + spec_row<P>(a, x, y0);
+    const int lane = t & 31;
+    const int src = (lane & ~(R1 - 1)) | ((R1 - (lane & (R1 - 1))) & (R1 - 1));
+#pragma unroll 1
     for (int jbq = t; jbq < KR * R1; jbq += G::T) {
       const int k1 = jbq % R1, rho = jbq / R1;
       float2 u[R2];
 #pragma unroll
       for (int n2 = 0; n2 < R2; ++n2) u[n2] = xp[(rho * R1 + k1) * G::ROWZ + n2];
       reg_dft<R2, false>(u);
+      float2* orr = orow + (int64_t)rho * P;
 #pragma unroll
-      for (int k2 = 0; k2 < R2; ++k2) st[rho * M + k1 + R1 * k2] = u[k2];
-    }
-    __syncthreads();
-    // even/odd split: X[k] = E[k] + W_N^k O[k], k <= M; zero padding after
-    const int x = row0 / a.ny, y0 = row0 % a.ny;
-    float2* orow = a.out_c + ch * a.ch + spec_row(a, x, y0);
-    for (int jq = t; jq < KR * a.P; jq += G::T) {
-      const int rho = jq / a.P, k = jq - rho * a.P;
-      float2 X = make_float2(0.f, 0.f);
-      if (k <= M) {
-        const float2 zk = st[rho * M + (k == M ? 0 : k)];
-        const float2 zm = conjf2(st[rho * M + (M - k) % M]);
+      for (int k2 = 0; k2 < R2; ++k2) {
+        // partner value: Z[M - k] = Z[(R1 - k1) + R1 (R2 - 1 - k2)] for k1 > 0;
+        // for k1 = 0 it is this lane's own Z[R1 ((R2 - k2) mod R2)]
+        const float2 send = u[R2 - 1 - k2];
+        float2 zm;
+        zm.x = __shfl_sync(0xffffffffu, send.x, src);
+        zm.y = __shfl_sync(0xffffffffu, send.y, src);
+        if (k1 == 0) zm = u[(R2 - k2) % R2];
+        zm = conjf2(zm);
+        const float2 zk = u[k2];
         const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
         const float2 d = make_float2(0.5f * (zk.x - zm.x), 0.5f * (zk.y - zm.y));
         const float2 o = make_float2(d.y, -d.x);  // -i d
-        X = cadd(e, cmul(__ldg(&a.tw_n[k]), o));
+        const int k = k1 + R1 * k2;
+        orr[k] = cadd(e, cmul(tw[M + k], o));
       }
-      orow[(int64_t)rho * a.P + k] = X;
+      // X[M] = Re Z[0] - Im Z[0]; zero padding after it
+      if (k1 < 8) orr[M + k1] = k1 == 0 ? make_float2(u[0].x - u[0].y, 0.f) : make_float2(0.f, 0.f);
     }
-    __syncthreads();
-    if (t == 0) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(it + S);
-    }
+    __syncthreads();  // transpose buffer free
   }
 }
 
@@ -612,16 +662,17 @@ __global__ void __launch_bounds__(256, 1) z_r2c_kernel(const ZArgs a) {
 template <int R1, int R2, int S>
 __global__ void __launch_bounds__(256, 1) z_c2r_kernel(const ZArgs a) {
   using G = ZGeom<R1, R2>;
-  constexpr int M = G::M;
-  const int P = a.P;
-  const int STAGE = KR * P;  // float2
+  constexpr int M = G::M, P = G::P;
+  constexpr int STAGE = KR * P;  // float2
   extern __shared__ __align__(128) float2 smem[];
   float2* xp = smem + S * STAGE;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(xp + G::XP);
+  float2* tw = xp + G::XP;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tw + G::TW);
   const int t = threadIdx.x;
   const int tiles_mine = a.ntiles > (int)blockIdx.x ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   if (t == 0)
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+  load_z_twiddles<M>(a, tw);
   __syncthreads();
   auto issue = [&](int i) {
     if (i >= tiles_mine) return;
@@ -631,7 +682,7 @@ __global__ void __launch_bounds__(256, 1) z_c2r_kernel(const ZArgs a) {
     const int s = i % S;
     const int x = row0 / a.ny, y0 = row0 % a.ny;
     mbar_expect_tx(&bars[s], KR * P * 8);
-    bulk_copy_g2s(smem + s * STAGE, a.in_c + ch * a.ch + spec_row(a, x, y0), KR * P * 8, &bars[s]);
+    bulk_copy_g2s(smem + s * STAGE, a.in_c + ch * a.ch + spec_row<P>(a, x, y0), KR * P * 8, &bars[s]);
   };
   if (t == 0)
     for (int i = 0; i < S; ++i) issue(i);
@@ -649,6 +700,7 @@ __global__ void __launch_bounds__(256, 1) z_c2r_kernel(const ZArgs a) {
     const int64_t row0 = (int64_t)(tile % a.tiles_per_ch) * KR;
     // first half with the even/odd merge:
     // Z[k] = (X[k] + conj X[M-k]) + i conj(W_N^k) (X[k] - conj X[M-k])
+#pragma unroll 1
     for (int jbq = t; jbq < KR * R2; jbq += G::T) {
       const int n2 = jbq % R2, rho = jbq / R2;
       float2 v[R1];
@@ -663,19 +715,24 @@ __global__ void __launch_bounds__(256, 1) z_c2r_kernel(const ZArgs a) {
         }
         xm = conjf2(xm);
         const float2 e = cadd(xk, xm);
-        const float2 d = cmul(csub(xk, xm), conjf2(__ldg(&a.tw_n[k])));
+        const float2 d = cmul(csub(xk, xm), conjf2(tw[M + k]));
         v[n1] = make_float2(e.x - d.y, e.y + d.x);  // e + i d
       }
       reg_dft<R1, true>(v);
 #pragma unroll
       for (int k1 = 0; k1 < R1; ++k1) {
         float2 r = v[k1];
-        if (k1 != 0) r = cmul(r, conjf2(__ldg(&a.tw_m[n2 * k1])));
+        if (k1 != 0) r = cmul(r, conjf2(tw[n2 * k1]));
         xp[(rho * R1 + k1) * G::ROWZ + n2] = r;
       }
     }
     __syncthreads();
+    if (t == 0) {  // the stage is consumed: start the copy of tile it + S
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(it + S);
+    }
     float2* orow = reinterpret_cast<float2*>(a.out_r + ch * a.cells + row0 * a.nz);
+#pragma unroll 1
     for (int jbq = t; jbq < KR * R1; jbq += G::T) {
       const int k1 = jbq % R1, rho = jbq / R1;
       float2 u[R2];
@@ -685,11 +742,7 @@ __global__ void __launch_bounds__(256, 1) z_c2r_kernel(const ZArgs a) {
 #pragma unroll
       for (int k2 = 0; k2 < R2; ++k2) orow[(int64_t)rho * M + k1 + R1 * k2] = u[k2];
     }
-    __syncthreads();
-    if (t == 0) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(it + S);
-    }
+    __syncthreads();  // transpose buffer free
   }
 }
 
@@ -783,22 +836,32 @@ int persistent_grid(K kernel, int threads, int smem, int ntiles) {
   return ntiles < g ? (ntiles > 0 ? ntiles : 1) : g;
 }
 
-constexpr int stages_for(int buf_bytes) {
-  const int s = (200 * 1024) / buf_bytes;
-  return s < 2 ? 2 : (s > 6 ? 6 : s);
+constexpr int stages_for(int buf_bytes, int extra, int ctas) {
+  const int s = ((224 * 1024) / ctas - extra - 1024) / buf_bytes;
+  return s < 1 ? 1 : (s > 6 ? 6 : s);
 }
 
-template <int R1, int R2, int MODE>
-int launch_col(const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
+// Resident CTAs per SM of the column passes (1: 255 registers and up to 3
+// stages per CTA; 2: 128 registers and one or two stages each).
+int g_col_ctas = 1;
+
+template <int R1, int R2, int MODE, int CTAS>
+int launch_col_ctas(const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
   using G = ColGeom<R1, R2>;
-  constexpr int S = stages_for(G::BUF * 8);
-  const int smem = S * G::BUF * 8 + S * 8;
-  auto k = col_pass_kernel<R1, R2, S, MODE>;
+  constexpr int EXTRA = G::L * 8 + col_table_floats(MODE, G::L) * 4;
+  constexpr int S = stages_for(G::BUF * 8, EXTRA, CTAS);
+  const int smem = S * G::BUF * 8 + EXTRA + S * 8;
+  auto k = col_pass_kernel<R1, R2, S, MODE, CTAS>;
   PMB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   const int grid = persistent_grid(k, G::T, smem, a.ntiles);
   k<<<grid, G::T, smem, s>>>(map, a);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
+}
+
+template <int R1, int R2, int MODE>
+int launch_col(const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
+  return g_col_ctas == 2 ? launch_col_ctas<R1, R2, MODE, 2>(map, a, s) : launch_col_ctas<R1, R2, MODE, 1>(map, a, s);
 }
 
 template <int MODE>
@@ -816,10 +879,9 @@ int launch_col_len(int L, const CUtensorMap& map, const ColArgs& a, cudaStream_t
 template <int R1, int R2, bool C2R>
 int launch_z(const ZArgs& a, cudaStream_t s) {
   using G = ZGeom<R1, R2>;
-  constexpr int M = G::M;
-  const int stage = C2R ? KR * a.P * 8 : KR * M * 8;
+  constexpr int stage = C2R ? KR * G::P * 8 : KR * G::M * 8;
   constexpr int S = 2;
-  const int smem = S * stage + G::XP * 8 + S * 8;
+  constexpr int smem = S * stage + G::XP * 8 + G::TW * 8 + S * 8;
   auto k = C2R ? z_c2r_kernel<R1, R2, S> : z_r2c_kernel<R1, R2, S>;
   PMB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   const int grid = persistent_grid(k, G::T, smem, a.ntiles);
@@ -879,10 +941,9 @@ int pmfft_z(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in
   a.in_c = in_c;
   a.out_r = out_r;
   a.out_c = out_c;
-  a.P = pmfft_row_len(m);
   a.ch = pmfft_channel_elems(m);
   a.cells = m.cells();
-  a.sb = (int64_t)m.nx * BY * a.P;
+  a.sb = (int64_t)m.nx * BY * pmfft_row_len(m);
   a.nx = m.nx;
   a.ny = m.ny;
   a.nz = m.nz;
@@ -955,6 +1016,15 @@ int pmfft_col(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float
     case kXGreen: return launch_col_len<kXGreen>(L, map, a, s);
     default: return launch_col_len<kXGreenAdj>(L, map, a, s);
   }
+}
+
+int pmfft_set_col_ctas(int ctas) {
+  if (ctas != 1 && ctas != 2) {
+    set_last_error("pmfft: column-pass CTAs per SM must be 1 or 2");
+    return kInvalidArgument;
+  }
+  g_col_ctas = ctas;
+  return kOk;
 }
 
 int pmfft_timeouts(unsigned int* count) {

@@ -209,7 +209,10 @@ def main(argv=None):
     ap.add_argument("--pmfft-shape", type=int, nargs=3, default=None,
                     help="time only the FFT pass chain on this mesh shape")
     ap.add_argument("--stages", default=None, help="comma-separated pass names (with --pmfft-shape)")
+    ap.add_argument("--col-ctas", type=int, default=None, help="resident CTAs per SM of the column passes")
     args = ap.parse_args(argv)
+    if args.col_ctas is not None:
+        call("pmb_pmfft_set_col_ctas", args.col_ctas)
     if args.pmfft_shape is not None:
         nx, ny, nz = args.pmfft_shape
         conf = Configuration(4.0, (nx // 2, ny // 2, nz // 2), 2, a_start=0.1, device="cuda")
