@@ -141,8 +141,9 @@ int pmb_green_gradient_adjoint(const void* grad_cot_hat, void* src_cot_hat, int 
  * pmb_set_pmfft(0) routes pmb_force / pmb_force_vjp through cuFFT and the
  * separate multiplier kernels instead (default 1).
  * pmb_pmfft_timeouts: bounded copy waits in these passes that gave up.
- * pmb_pmfft_set_col_ctas(1 or 2): resident CTAs per SM of the column passes
- *   (a tuning knob; results are identical). */
+ * pmb_pmfft_set_col_ctas(0, 1 or 2): resident CTAs per SM of the column
+ *   passes, 0 = the measured per-mode default (a tuning knob; results are
+ *   identical). */
 int pmb_set_pmfft(int enabled);
 int pmb_pmfft_supported(int nx, int ny, int nz);
 int64_t pmb_pmfft_channel_elems(int nx, int ny, int nz);
@@ -158,7 +159,9 @@ int pmb_pmfft_set_col_ctas(int ctas);
  * :626-633 -> _streamed_acceleration_from_potential :506-543): optional
  * drift, cell sort, deterministic scatter to the Poisson source, R2C, Green x
  * gradient, batched C2R into force_meshes (3,nx,ny,nz), 3-channel gather into
- * acc (n,3), optional fused half-kick vel_kick += acc * kick. */
+ * acc (n,3), optional fused half-kick vel_kick += acc * kick.  On return
+ * the first pmb_sorted_bytes(n, nx, ny, nz) bytes of the workspace hold the
+ * sorted records of the (post-drift) positions. */
 int64_t pmb_force_workspace_bytes(int64_t n, int nx, int ny, int nz);
 int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float drift, int64_t n, int nx, int ny, int nz,
               float cell, float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
@@ -172,6 +175,14 @@ int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int
                   float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
                   const float* transfer, const float* radial, int radial_len, const float* force_meshes,
                   const float* acc_cot, float* disp_cot, void* workspace, int64_t workspace_bytes, void* stream);
+/* pmb_force_vjp without its cell sort: sorted holds the records of exactly
+ * these positions (pmb_sort_rows output, or the head of a pmb_force
+ * workspace after a force evaluation at the same positions). */
+int pmb_force_vjp_presorted(const void* sorted, int64_t n, int nx, int ny, int nz, float cell, float val_const,
+                            float src_mul, const float* tables, int has_masks, int green_kernel,
+                            const float* transfer, const float* radial, int radial_len, const float* force_meshes,
+                            const float* acc_cot, float* disp_cot, void* workspace, int64_t workspace_bytes,
+                            void* stream);
 
 /* ---------------- time integration ---------------------------------------
  * y += x * f in float (drift integrator.py:225, kick :536). */

@@ -47,6 +47,8 @@ _SIGS = {
     "pmb_force_vjp_workspace_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
     "pmb_force_vjp": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_f, c_f, c_f, c_p, c_int, c_int, c_p, c_p, c_int,
                               c_p, c_p, c_p, c_p, c_i64, c_p]),
+    "pmb_force_vjp_presorted": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_f, c_f, c_f, c_p, c_int, c_int, c_p, c_p,
+                                        c_int, c_p, c_p, c_p, c_p, c_i64, c_p]),
     "pmb_axpy": (c_int, [c_p, c_p, c_i64, c_f, c_p]),
     "pmb_kick_adj": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_p, c_p]),
     "pmb_drift_adj": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_p, c_p]),
@@ -142,7 +144,7 @@ def check(status, what):
 _KERNELS = {
     "pmb_sort_rows": 5, "pmb_gather_rows": 1, "pmb_interp_grad_rows": 1, "pmb_green_gradient": 1,
     "pmb_green_gradient_adjoint": 1, "pmb_axpy": 1, "pmb_kick_adj": 1, "pmb_drift_adj": 1, "pmb_dot": 1,
-    "pmb_force": 9, "pmb_force_vjp": 11, "pmb_sum": 1, "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,
+    "pmb_force": 9, "pmb_force_vjp": 11, "pmb_force_vjp_presorted": 6, "pmb_sum": 1, "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,
     "pmb_lpt": 4, "pmb_lpt_vjp": 6, "pmb_pk_shells": 1, "pmb_shell_stats": 1, "pmb_pk_shells_adjoint": 1,
     "pmb_overdensity": 1, "pmb_ens_force": 7, "pmb_ens_step": 9, "pmb_ens_set_step": 1,
     "pmb_force64": 5, "pmb_deposit64": 1, "pmb_axpy64": 1, "pmb_sum64": 1, "pmb_white_noise_nested64": 1,
@@ -195,4 +197,6 @@ def call(name, *args):
         if name == "pmb_force" and pmfft_active(*args[5:8]):
             _launches[0] += 5
         elif name == "pmb_force_vjp" and pmfft_active(*args[3:6]):
+            _launches[0] += 5
+        elif name == "pmb_force_vjp_presorted" and pmfft_active(*args[2:5]):
             _launches[0] += 5

@@ -345,10 +345,13 @@ int64_t pmb_force_vjp_workspace_bytes(int64_t n, int nx, int ny, int nz) {
   return force_vjp_layout(n, Mesh3{nx, ny, nz}, nullptr, 0, &a, &b, &c, &cs, &mc, &s3, &sh, &sc, &w);
 }
 
-int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int ny, int nz, float cell,
-                  float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
-                  const float* transfer, const float* radial, int radial_len, const float* force_meshes,
-                  const float* acc_cot, float* disp_cot, void* workspace, int64_t workspace_bytes, void* stream) {
+// presorted (may be null): records of exactly these positions left by an
+// earlier pmb_force / pmb_sort_rows; the sort is skipped.
+static int force_vjp_impl(const int16_t* pmid, const float* disp, int64_t n, int nx, int ny, int nz, float cell,
+                          float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
+                          const float* transfer, const float* radial, int radial_len, const float* force_meshes,
+                          const float* acc_cot, float* disp_cot, const void* presorted, void* workspace,
+                          int64_t workspace_bytes, void* stream) {
   Mesh3 m{nx, ny, nz};
   PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_force_vjp: unsupported mesh shape");
   PMB_REQUIRE(n >= 0 && n < 4294967295ll, "pmb_force_vjp: particle count out of range");
@@ -364,8 +367,11 @@ int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int
     return kScratchTooSmall;
   }
   cudaStream_t s = S(stream);
-  PMB_TRY(pmb_sort_rows(pmid, (float*)disp, nullptr, 0.f, n, nx, ny, nz, cell, sorted, bins, bin_scratch_bytes(n, m),
-                        stream));
+  if (presorted != nullptr)
+    sorted = const_cast<void*>(presorted);
+  else
+    PMB_TRY(pmb_sort_rows(pmid, (float*)disp, nullptr, 0.f, n, nx, ny, nz, cell, sorted, bins,
+                          bin_scratch_bytes(n, m), stream));
   SortedView v = sorted_view(sorted, n);
   // gather adjoint: position term and the 3-channel scatter of acc_cot
   PMB_TRY(interp_grad_sorted(v.rec, v.perm, v.offs, n, m, 3, force_meshes, acc_cot, 0.f, cell, 1, disp_cot, nullptr,
@@ -385,6 +391,26 @@ int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int
   // scatter adjoint of the density (constant particle value)
   return interp_grad_sorted(v.rec, v.perm, v.offs, n, m, 1, src_cot, nullptr, val_const, cell, 1, disp_cot, nullptr,
                             nullptr, s);
+}
+
+int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int ny, int nz, float cell,
+                  float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
+                  const float* transfer, const float* radial, int radial_len, const float* force_meshes,
+                  const float* acc_cot, float* disp_cot, void* workspace, int64_t workspace_bytes, void* stream) {
+  return force_vjp_impl(pmid, disp, n, nx, ny, nz, cell, val_const, src_mul, tables, has_masks, green_kernel,
+                        transfer, radial, radial_len, force_meshes, acc_cot, disp_cot, nullptr, workspace,
+                        workspace_bytes, stream);
+}
+
+int pmb_force_vjp_presorted(const void* sorted, int64_t n, int nx, int ny, int nz, float cell, float val_const,
+                            float src_mul, const float* tables, int has_masks, int green_kernel,
+                            const float* transfer, const float* radial, int radial_len, const float* force_meshes,
+                            const float* acc_cot, float* disp_cot, void* workspace, int64_t workspace_bytes,
+                            void* stream) {
+  PMB_REQUIRE(sorted != nullptr, "pmb_force_vjp_presorted: null sorted records");
+  return force_vjp_impl(nullptr, nullptr, n, nx, ny, nz, cell, val_const, src_mul, tables, has_masks, green_kernel,
+                        transfer, radial, radial_len, force_meshes, acc_cot, disp_cot, sorted, workspace,
+                        workspace_bytes, stream);
 }
 
 // ---------------------------------------------------------------------------

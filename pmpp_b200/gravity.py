@@ -110,7 +110,7 @@ def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F
 
 
 def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc_cot, disp_cot, timer,
-                      src_hat=None, transfer_cot_out=None):
+                      src_hat=None, transfer_cot_out=None, presorted=False):
     """pmb_force_vjp as separate stage calls with a CUDA event after each stage.
 
     With src_hat (the source spectrum at the same positions) and
@@ -123,9 +123,10 @@ def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, r
     sorted_buf, sort_scr, s16, real3 = _stage_buffers(n, conf, dev)
     timer = _NoTimer() if timer is None else timer
     t = timer.start()
-    call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), None, 0.0, n, nx, ny, nz, float(conf.cell_size),
-         sorted_buf.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
-    t = timer.mark("sort", t)
+    if not presorted:
+        call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), None, 0.0, n, nx, ny, nz, float(conf.cell_size),
+             sorted_buf.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
+        t = timer.mark("sort", t)
     cot_sorted = workspace(12 * n, dev, "st_cot_sorted")
     call("pmb_interp_grad_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc_cot.data_ptr(), 0.0,
          float(conf.cell_size), 1, disp_cot.data_ptr(), None, cot_sorted.data_ptr(), s)
@@ -212,8 +213,12 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
 
 
 def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *, a=None, cosmo=None,
-              correction=None, src_hat=None, transfer_cot_out=None):
-    """disp_cot (+)= (d acc / d disp)^T acc_cot, with force_meshes computed at disp."""
+              correction=None, src_hat=None, transfer_cot_out=None, presorted=False):
+    """disp_cot (+)= (d acc / d disp)^T acc_cot, with force_meshes computed at disp.
+
+    presorted: the last force() call on this device was at exactly these
+    positions and took the same route (fused or staged); its cell-sorted
+    records are reused instead of sorting again."""
     require_cuda(pmid, disp, force_meshes, acc_cot, disp_cot)
     n = pmid.shape[0]
     nx, ny, nz = conf.mesh_shape
@@ -224,10 +229,18 @@ def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *
     tables = conf.spectral_tables("mesh", dev, gk)
     if StageTimer.active is not None or transfer_cot_out is not None:
         _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc_cot,
-                          disp_cot, StageTimer.active, src_hat, transfer_cot_out)
+                          disp_cot, StageTimer.active, src_hat, transfer_cot_out, presorted)
         return disp_cot
     wb = lib().pmb_force_vjp_workspace_bytes(n, nx, ny, nz)
     ws = workspace(wb, dev, "force_vjp")
+    if presorted:
+        # head of the fused force's workspace: its sorted records
+        head = workspace(lib().pmb_force_workspace_bytes(n, nx, ny, nz), dev, "force")
+        call("pmb_force_vjp_presorted", head.data_ptr(), n, nx, ny, nz, float(conf.cell_size),
+             float(conf.mesh_size / conf.ptcl_num), 1.5 * _om32(omega_m), tables.data_ptr(),
+             int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, force_meshes.data_ptr(),
+             acc_cot.data_ptr(), disp_cot.data_ptr(), ws.data_ptr(), ws.numel(), stream_handle(dev))
+        return disp_cot
     call("pmb_force_vjp", pmid.data_ptr(), disp.data_ptr(), n, nx, ny, nz, float(conf.cell_size),
          float(conf.mesh_size / conf.ptcl_num), 1.5 * _om32(omega_m), tables.data_ptr(),
          int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, force_meshes.data_ptr(),

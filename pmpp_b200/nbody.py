@@ -140,17 +140,20 @@ class NBodyRun:
         nx, ny, nz = self.conf.mesh_shape
         return torch.empty((nx, ny, nz // 2 + 1), dtype=torch.complex64, device=device)
 
-    def _force_adjoint(self, pmid, disp, F, S, ac, dc, a):
-        """Force adjoint; with a trainable correction also its parameter gradient."""
+    def _force_adjoint(self, pmid, disp, F, S, ac, dc, a, presorted=False):
+        """Force adjoint; with a trainable correction also its parameter gradient.
+
+        presorted: the previous force() call was at exactly these positions."""
         conf, cosmo, corr = self.conf, self.cosmo, self.correction
         if self._trainable():
             from .corrections import radial_table_len
             tc = torch.zeros(radial_table_len(conf), dtype=torch.float64, device=disp.device)
             force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=corr, src_hat=S,
-                      transfer_cot_out=tc)
+                      transfer_cot_out=tc, presorted=presorted)
             corr.accumulate(a, cosmo, conf, tc)
         else:
-            force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=corr)
+            force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=corr,
+                      presorted=presorted)
 
     def _require_f32(self):
         if self.conf.float_dtype != torch.float32:
@@ -180,6 +183,9 @@ class NBodyRun:
         force_slots = []
         slot = 0
         om32 = _om32(cosmo.Omega_m)
+        # after the first force adjoint every one follows the force recompute at
+        # the same positions (the kick adjoint between them moves no particle)
+        recomputed = False
         for a_prev, a_next in zip(a[:-1][::-1], a[1:][::-1]):
             for st in reversed(_schedule(a_prev, a_next, conf)):
                 if st[0] == "kick":
@@ -194,7 +200,7 @@ class NBodyRun:
                 call("pmb_dot", ac.data_ptr(), acc.data_ptr(), ac.numel(), dots[slot:].data_ptr(), s)
                 force_slots.append(slot)
                 slot += 1
-                self._force_adjoint(pmid, disp, F, S, ac, dc, float(a_dn))
+                self._force_adjoint(pmid, disp, F, S, ac, dc, float(a_dn), presorted=recomputed)
                 ac.zero_()
                 D, dD = cosmo.drift_factor(a_vel, a_dp, a_dn, with_grad=True)
                 call("pmb_drift_adj", disp.data_ptr(), vel.data_ptr(), dc.data_ptr(), vc.data_ptr(), disp.numel(),
@@ -204,12 +210,13 @@ class NBodyRun:
                 # recompute the incoming acceleration; keep its meshes for the next force adjoint
                 force(pmid, disp, conf, cosmo.Omega_m, a=float(a_acc_in), cosmo=cosmo, correction=corr,
                       force_meshes=F2, acc=acc, src_hat_out=S2)
+                recomputed = True
                 F, F2 = F2, F
                 S, S2 = S2, S
         # the initial force evaluation (solver.py:437-441)
         call("pmb_dot", ac.data_ptr(), acc.data_ptr(), ac.numel(), dots[slot:].data_ptr(), s)
         force_slots.append(slot)
-        self._force_adjoint(pmid, disp, F, S, ac, dc, float(a[0]))
+        self._force_adjoint(pmid, disp, F, S, ac, dc, float(a[0]), presorted=recomputed)
         ac.zero_()
         d = dots.cpu().numpy()
         om_cot = sum(g * d[k] for g, k in grads) + sum(d[k] for k in force_slots) / om32

@@ -97,3 +97,22 @@ def test_nbody_adjoint_matches_oracle():
     np.testing.assert_allclose(om, rom, rtol=1e-3)
     # the reverse sweep reconstructs the initial state up to float32 round-off
     assert rel_err(p0.disp.cpu().numpy(), disp) < 1e-4
+
+
+@pytest.mark.parametrize("staged", [False, True])
+@pytest.mark.parametrize("shape,mesh", [((16, 16, 16), 2), ((32, 32, 32), 4)])
+def test_force_vjp_presorted_matches_sorting_route(staged, shape, mesh):
+    """The reverse sweep reuses the force recompute's cell-sorted records."""
+    import contextlib
+
+    from pmpp_b200.gravity import force, force_vjp
+    from pmpp_b200.runtime import StageTimer
+    pb, co, conf = _confs(shape=shape, mesh=mesh)
+    pmid, disp = random_particles(co, seed=14, spread=2.0)
+    pm, d = torch.from_numpy(pmid).cuda(), torch.from_numpy(disp).cuda()
+    ac = torch.from_numpy(np.random.default_rng(3).normal(size=disp.shape).astype(np.float32)).cuda()
+    with (StageTimer() if staged else contextlib.nullcontext()):
+        _, F = force(pm, d, conf, 0.3)
+        got = force_vjp(pm, d, conf, 0.3, F, ac, presorted=True)
+        ref = force_vjp(pm, d, conf, 0.3, F, ac)
+    assert torch.equal(got, ref)
