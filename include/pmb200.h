@@ -190,6 +190,14 @@ int pmb_axpy(float* y, const float* x, int64_t n, float f, void* stream);
 /* Kick adjoint (integrator.py:566-580); dot (double, device) += sum vel_cot*acc. */
 int pmb_kick_adj(float* vel, const float* acc, const float* vel_cot, float* acc_cot, int64_t n, float kick,
                  double* dot, void* stream);
+/* One or two consecutive kick adjoints with the same acc (kick_a first),
+ * bit-identical to as many pmb_kick_adj calls: dot_a (and dot_b) += sum
+ * vel_cot*acc; dot_force (may be null) += sum acc_cot*acc of the updated
+ * cotangent (the Omega_m term of the force adjoint that follows);
+ * zero_cot = 1 treats acc_cot as zero on entry. */
+int pmb_kick_adj2(float* vel, const float* acc, const float* vel_cot, float* acc_cot, int64_t n, float kick_a,
+                  float kick_b, int two, int zero_cot, double* dot_a, double* dot_b, double* dot_force,
+                  void* stream);
 /* Drift adjoint (integrator.py:459-474); dot += sum disp_cot*vel. */
 int pmb_drift_adj(float* disp, const float* vel, const float* disp_cot, float* vel_cot, int64_t n, float drift,
                   double* dot, void* stream);

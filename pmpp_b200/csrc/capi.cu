@@ -424,6 +424,14 @@ int pmb_kick_adj(float* vel, const float* acc, const float* vel_cot, float* acc_
   return kick_adj(vel, acc, vel_cot, acc_cot, n, kick, dot, S(stream));
 }
 
+int pmb_kick_adj2(float* vel, const float* acc, const float* vel_cot, float* acc_cot, int64_t n, float kick_a,
+                  float kick_b, int two, int zero_cot, double* dot_a, double* dot_b, double* dot_force,
+                  void* stream) {
+  PMB_REQUIRE(dot_a != nullptr && (two == 0 || dot_b != nullptr), "pmb_kick_adj2: dot accumulators required");
+  return kick_adj2(vel, acc, vel_cot, acc_cot, n, kick_a, kick_b, two != 0, zero_cot != 0, dot_a, dot_b, dot_force,
+                   S(stream));
+}
+
 int pmb_drift_adj(float* disp, const float* vel, const float* disp_cot, float* vel_cot, int64_t n, float drift,
                   double* dot, void* stream) {
   PMB_REQUIRE(dot != nullptr, "pmb_drift_adj: dot accumulator required");

@@ -55,6 +55,34 @@ __global__ void kick_adj_kernel(float* __restrict__ vel, const float* __restrict
 
 // Drift adjoint (integrator.py:459-474): disp -= vel*D; vel_cot += disp_cot*D;
 // dot += sum(disp_cot * vel).
+// One or two consecutive kick adjoints with the same acceleration (the closing
+// half-kick of one step and the opening one of the next), in the order the
+// separate kernels would apply them, plus the force-slot dot sum(acc_cot * acc)
+// of the force adjoint that follows.  zero_cot: acc_cot is taken as zero
+// (the force adjoint before consumed it).
+__global__ void kick_adj2_kernel(float* __restrict__ vel, const float* __restrict__ acc,
+                                 const float* __restrict__ vel_cot, float* __restrict__ acc_cot, int64_t n, float ka,
+                                 float kb, int two, int zero_cot, double* __restrict__ dot_a,
+                                 double* __restrict__ dot_b, double* __restrict__ dot_f) {
+  double s = 0.0, sf = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float a = acc[i], vc = vel_cot[i];
+    float v = __fsub_rn(vel[i], __fmul_rn(a, ka));
+    float c = __fadd_rn(zero_cot ? 0.f : acc_cot[i], __fmul_rn(vc, ka));
+    if (two) {
+      v = __fsub_rn(v, __fmul_rn(a, kb));
+      c = __fadd_rn(c, __fmul_rn(vc, kb));
+    }
+    vel[i] = v;
+    acc_cot[i] = c;
+    s += (double)vc * (double)a;
+    sf += (double)c * (double)a;
+  }
+  block_add(s, dot_a);
+  if (two) block_add(s, dot_b);
+  if (dot_f != nullptr) block_add(sf, dot_f);
+}
+
 __global__ void drift_adj_kernel(float* __restrict__ disp, const float* __restrict__ vel,
                                  const float* __restrict__ disp_cot, float* __restrict__ vel_cot, int64_t n, float d,
                                  double* __restrict__ dot) {
@@ -93,6 +121,15 @@ int axpy(float* y, const float* x, int64_t n, float f, cudaStream_t s) {
 int kick_adj(float* vel, const float* acc, const float* vel_cot, float* acc_cot, int64_t n, float k, double* dot,
              cudaStream_t s) {
   if (n > 0) kick_adj_kernel<<<grid_n(n, 256), 256, 0, s>>>(vel, acc, vel_cot, acc_cot, n, k, dot);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int kick_adj2(float* vel, const float* acc, const float* vel_cot, float* acc_cot, int64_t n, float ka, float kb,
+              int two, int zero_cot, double* dot_a, double* dot_b, double* dot_f, cudaStream_t s) {
+  if (n > 0)
+    kick_adj2_kernel<<<grid_n(n, 256), 256, 0, s>>>(vel, acc, vel_cot, acc_cot, n, ka, kb, two, zero_cot, dot_a, dot_b,
+                                                    dot_f);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }

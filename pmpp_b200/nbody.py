@@ -178,46 +178,80 @@ class NBodyRun:
         F2 = torch.empty_like(F)
         S = (self.final_src_hat if src_hat is None else src_hat) if self._trainable() else None
         S2 = self._src_hat_buffer(dev)
-        dots = torch.zeros(4 * len(a) + 8, dtype=torch.float64, device=dev)
+        # reversed stage list of the whole run, then the initial force evaluation
+        ops = []
+        for a_prev, a_next in zip(a[:-1][::-1], a[1:][::-1]):
+            ops.extend(reversed(_schedule(a_prev, a_next, conf)))
+        ops.append(("init", ))
+        dots = torch.zeros(2 * len(ops) + 2, dtype=torch.float64, device=dev)
         grads = []  # (d factor / d Omega_m, dot slot) pairs, reduced on the host at the end
         force_slots = []
         slot = 0
         om32 = _om32(cosmo.Omega_m)
+        n3 = vel.numel()
         # after the first force adjoint every one follows the force recompute at
-        # the same positions (the kick adjoint between them moves no particle)
+        # the same positions (the kick adjoints between them move no particle)
         recomputed = False
-        for a_prev, a_next in zip(a[:-1][::-1], a[1:][::-1]):
-            for st in reversed(_schedule(a_prev, a_next, conf)):
-                if st[0] == "kick":
-                    K, dK = cosmo.kick_factor(st[1], st[2], st[3], with_grad=True)
-                    call("pmb_kick_adj", vel.data_ptr(), acc.data_ptr(), vc.data_ptr(), ac.data_ptr(), vel.numel(),
-                         _f32(K), dots[slot:].data_ptr(), s)
-                    grads.append((dK, slot))
-                    slot += 1
-                    continue
-                _, a_vel, a_dp, a_dn, a_acc_in = st
-                # force adjoint at the post-drift positions
+        zero_pending = False  # acc_cot consumed by a force adjoint, not yet cleared
+        force_dot_done = False
+        i = 0
+        while i < len(ops):
+            st = ops[i]
+            if st[0] == "kick":
+                # consecutive kick adjoints share acc: one kernel for up to two,
+                # which also forms the force-slot dot of a following force adjoint
+                ks = [st] + ([ops[i + 1]] if i + 1 < len(ops) and ops[i + 1][0] == "kick" else [])
+                j = i + len(ks)
+                force_next = j < len(ops) and ops[j][0] in ("drift", "init")
+                Ks = [cosmo.kick_factor(k[1], k[2], k[3], with_grad=True) for k in ks]
+                two = len(ks) == 2
+                sa = slot
+                sb = slot + 1 if two else None
+                sf = slot + len(ks) if force_next else None
+                slot += len(ks) + (1 if force_next else 0)
+                call("pmb_kick_adj2", vel.data_ptr(), acc.data_ptr(), vc.data_ptr(), ac.data_ptr(), n3,
+                     _f32(Ks[0][0]), _f32(Ks[1][0]) if two else 0.0, int(two), int(zero_pending),
+                     dots[sa:].data_ptr(), dots[sb:].data_ptr() if two else None,
+                     dots[sf:].data_ptr() if force_next else None, s)
+                grads.append((Ks[0][1], sa))
+                if two:
+                    grads.append((Ks[1][1], sb))
+                if force_next:
+                    force_slots.append(sf)
+                    force_dot_done = True
+                zero_pending = False
+                i = j
+                continue
+            # force adjoint at the post-drift positions (or the initial evaluation)
+            if zero_pending:
+                ac.zero_()
+                zero_pending = False
+            if not force_dot_done:
                 call("pmb_dot", ac.data_ptr(), acc.data_ptr(), ac.numel(), dots[slot:].data_ptr(), s)
                 force_slots.append(slot)
                 slot += 1
-                self._force_adjoint(pmid, disp, F, S, ac, dc, float(a_dn), presorted=recomputed)
+            force_dot_done = False
+            a_force = float(a[0]) if st[0] == "init" else float(st[3])
+            self._force_adjoint(pmid, disp, F, S, ac, dc, a_force, presorted=recomputed)
+            i += 1
+            if st[0] == "init":
                 ac.zero_()
-                D, dD = cosmo.drift_factor(a_vel, a_dp, a_dn, with_grad=True)
-                call("pmb_drift_adj", disp.data_ptr(), vel.data_ptr(), dc.data_ptr(), vc.data_ptr(), disp.numel(),
-                     _f32(D), dots[slot:].data_ptr(), s)
-                grads.append((dD, slot))
-                slot += 1
-                # recompute the incoming acceleration; keep its meshes for the next force adjoint
-                force(pmid, disp, conf, cosmo.Omega_m, a=float(a_acc_in), cosmo=cosmo, correction=corr,
-                      force_meshes=F2, acc=acc, src_hat_out=S2)
-                recomputed = True
-                F, F2 = F2, F
-                S, S2 = S2, S
-        # the initial force evaluation (solver.py:437-441)
-        call("pmb_dot", ac.data_ptr(), acc.data_ptr(), ac.numel(), dots[slot:].data_ptr(), s)
-        force_slots.append(slot)
-        self._force_adjoint(pmid, disp, F, S, ac, dc, float(a[0]), presorted=recomputed)
-        ac.zero_()
+                continue
+            zero_pending = True
+            _, a_vel, a_dp, a_dn, a_acc_in = st
+            D, dD = cosmo.drift_factor(a_vel, a_dp, a_dn, with_grad=True)
+            call("pmb_drift_adj", disp.data_ptr(), vel.data_ptr(), dc.data_ptr(), vc.data_ptr(), disp.numel(),
+                 _f32(D), dots[slot:].data_ptr(), s)
+            grads.append((dD, slot))
+            slot += 1
+            # recompute the incoming acceleration; keep its meshes for the next force adjoint
+            force(pmid, disp, conf, cosmo.Omega_m, a=float(a_acc_in), cosmo=cosmo, correction=corr,
+                  force_meshes=F2, acc=acc, src_hat_out=S2)
+            recomputed = True
+            F, F2 = F2, F
+            S, S2 = S2, S
+        if zero_pending:
+            ac.zero_()
         d = dots.cpu().numpy()
         om_cot = sum(g * d[k] for g, k in grads) + sum(d[k] for k in force_slots) / om32
         return (ptcl.replace(disp=disp, vel=vel, acc=acc), Particles(conf, pmid, dc, vc, ac), float(om_cot))

@@ -116,3 +116,29 @@ def test_force_vjp_presorted_matches_sorting_route(staged, shape, mesh):
         got = force_vjp(pm, d, conf, 0.3, F, ac, presorted=True)
         ref = force_vjp(pm, d, conf, 0.3, F, ac)
     assert torch.equal(got, ref)
+
+
+@pytest.mark.parametrize("two,zero", [(0, 0), (1, 0), (1, 1), (0, 1)])
+def test_kick_adj2_matches_separate_kernels(two, zero):
+    """The merged kick adjoint applies the same float operations as separate ones."""
+    from pmpp_b200._lib import call
+    from pmpp_b200.runtime import stream_handle
+    g = torch.Generator().manual_seed(8)
+    n = 3 * 100003
+    vel, acc, vc, ac = (torch.randn(n, generator=g).cuda() for _ in range(4))
+    s = stream_handle(vel.device)
+    ka, kb = 0.37, -1.21
+    v1, c1 = vel.clone(), ac.clone()
+    if zero:
+        c1.zero_()
+    d1 = torch.zeros(3, dtype=torch.float64, device="cuda")
+    call("pmb_kick_adj", v1.data_ptr(), acc.data_ptr(), vc.data_ptr(), c1.data_ptr(), n, ka, d1[0:].data_ptr(), s)
+    if two:
+        call("pmb_kick_adj", v1.data_ptr(), acc.data_ptr(), vc.data_ptr(), c1.data_ptr(), n, kb, d1[1:].data_ptr(), s)
+    call("pmb_dot", c1.data_ptr(), acc.data_ptr(), n, d1[2:].data_ptr(), s)
+    v2, c2 = vel.clone(), ac.clone()
+    d2 = torch.zeros(3, dtype=torch.float64, device="cuda")
+    call("pmb_kick_adj2", v2.data_ptr(), acc.data_ptr(), vc.data_ptr(), c2.data_ptr(), n, ka, kb, two, zero,
+         d2[0:].data_ptr(), d2[1:].data_ptr(), d2[2:].data_ptr(), s)
+    assert torch.equal(v1, v2) and torch.equal(c1, c2)
+    torch.testing.assert_close(d1, d2, rtol=1e-12, atol=1e-9)
