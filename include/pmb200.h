@@ -135,7 +135,7 @@ int pmb_green_gradient_adjoint(const void* grad_cot_hat, void* src_cot_hat, int 
  *   of channels ch_off, ch_off+1 combined as (-i c_y) Y + (-i c_z) Z, 4 x
  *   forward, 5 x inverse, 6 x forward + Green multiplier + x inverse into
  *   (i c_x phi, phi) (2 output channels), 7 x forward of channels 0, 1 +
- *   adjoint multiplier + x inverse.  Modes 0, 1, 4, 5 transform nbatch
+ *   adjoint multiplier + x inverse, 8 the same without the x inverse.  Modes 0, 1, 4, 5 transform nbatch
  *   channels starting at ch_off; tables, transfer, radial and post_scale are
  *   those of pmb_green_gradient (tables may be null for modes 0, 1, 4, 5).
  * pmb_set_pmfft(0) routes pmb_force / pmb_force_vjp through cuFFT and the

@@ -194,7 +194,7 @@ def call(name, *args):
         _launches[0] += 2 if args[6] is None else 3
     else:
         _launches[0] += _KERNELS.get(name, 0)
-        # the hand-written FFT chain adds six passes and drops the multiplier kernel
+        # the hand-written FFT chain replaces the multiplier kernel by six passes
         if name == "pmb_force" and pmfft_active(*args[5:8]):
             _launches[0] += 5
         elif name == "pmb_force_vjp" and pmfft_active(*args[3:6]):

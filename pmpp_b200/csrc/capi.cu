@@ -231,7 +231,7 @@ int pmb_pmfft_col(int nx, int ny, int nz, int mode, int nbatch, int ch_off, cons
                   float post_scale, void* stream) {
   Mesh3 m{nx, ny, nz};
   PMB_REQUIRE(pmfft_supported(m), "pmb_pmfft_col: mesh not supported (powers of two, 64..1024, nz >= 128)");
-  PMB_REQUIRE(mode >= 0 && mode <= 7, "pmb_pmfft_col: mode must be 0..7");
+  PMB_REQUIRE(mode >= 0 && mode <= 8, "pmb_pmfft_col: mode must be 0..8");
   PMB_REQUIRE(nbatch >= 1 && ch_off >= 0, "pmb_pmfft_col: bad batch");
   PMB_REQUIRE(tables != nullptr || mode == 0 || mode == 1 || mode == 4 || mode == 5,
               "pmb_pmfft_col: spectral tables required for the multiplier modes");

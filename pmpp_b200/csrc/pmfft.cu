@@ -181,16 +181,20 @@ enum ColMode : int {
   kXFwd = 4,     // x forward, 1 -> 1
   kXInv = 5,     // x inverse, 1 -> 1
   kXGreen = 6,   // x, K(k), x^-1 of i c_x phi and phi: 1 -> 2
-  kXGreenAdj = 7 // x of B_x and b, K(k) ((-i c_x) B_x + b), x^-1: 2 -> 1
+  kXGreenAdj = 7, // x of B_x and b, K(k) ((-i c_x) B_x + b), x^-1: 2 -> 1
+  kXFwdAdjK = 8   // x of B_x and b, K(k) ((-i c_x) B_x + b) (no inverse): 2 -> 1
 };
 
 __host__ __device__ constexpr bool is_y(int mode) { return mode <= kYFwdYZ; }
-__host__ __device__ constexpr int n_in(int mode) { return (mode == kYFwdYZ || mode == kXGreenAdj) ? 2 : 1; }
+__host__ __device__ constexpr int n_in(int mode) {
+  return (mode == kYFwdYZ || mode == kXGreenAdj || mode == kXFwdAdjK) ? 2 : 1;
+}
 __host__ __device__ constexpr int n_out(int mode) { return (mode == kYInvYZ || mode == kXGreen) ? 2 : 1; }
 
 // floats of per-axis tables a column pass keeps in shared memory
 __host__ __device__ constexpr int col_table_floats(int mode, int L) {
-  return (mode == kXGreen || mode == kXGreenAdj) ? 3 * L : ((mode == kYInvYZ || mode == kYFwdYZ) ? L : 0);
+  return (mode == kXGreen || mode == kXGreenAdj || mode == kXFwdAdjK) ? 3 * L
+                                                                     : ((mode == kYInvYZ || mode == kYFwdYZ) ? L : 0);
 }
 
 struct ColArgs {
@@ -229,14 +233,17 @@ __device__ __forceinline__ bool kz_valid(int kz, int nz) { return kz <= nz / 2; 
 
 // Green multiplier of the source value at (ix, iy, iz): phi = K(k) S, K =
 // post * mask * T * (-1/k^2), zero at k = 0 (pmb_spectral_device.cuh has the
-// reference citations).  kx2 / mx are the x-axis tables in shared memory;
-// kyz2 = ky^2 + kz^2 and myz = my * mz are the column's constants.
+// reference citations).  kx2 / mx are the x-axis tables in shared memory; the
+// column's constants are kyz2 = ky^2 + kz^2 and c0 = -post * my * mz (0 on
+// the zero-padding columns); HAS_T: a transfer or radial table is present.
+// The quotient uses the fast division (2 ulp), well inside the float32 bar
+// of the force parity tests.
+template <bool HAS_T>
 __device__ __forceinline__ float green_scalar(const ColArgs& a, const float* kx2, const float* mx, float kyz2,
-                                              float myz, int ix, int iy, int iz) {
+                                              float c0, int ix, int iy, int iz) {
   const float k2 = kx2[ix] + kyz2;
-  if (k2 == 0.f) return 0.f;
-  float K = (-a.g.post_scale * myz * mx[ix]) * __frcp_rn(k2);
-  if (a.g.transfer != nullptr || a.g.radial != nullptr) {
+  float K = k2 == 0.f ? 0.f : __fdividef(c0 * mx[ix], k2);
+  if constexpr (HAS_T) {
     const Mesh3 m{a.nx, a.ny, a.nz};
     const int64_t j = ((int64_t)ix * a.ny + iy) * (a.nz / 2 + 1) + iz;
     K *= transfer_of(a.g, a.t, j, ix, iy, iz, m);
@@ -267,7 +274,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
   for (int i = t; i < L; i += G::T) {
     stw[i] = a.tw[i];
     if constexpr (MODE == kYInvYZ || MODE == kYFwdYZ) tab[i] = a.t.cy[i];
-    if constexpr (MODE == kXGreen || MODE == kXGreenAdj) {
+    if constexpr (MODE == kXGreen || MODE == kXGreenAdj || MODE == kXFwdAdjK) {
       const float kx = a.t.kx[i];
       tab[i] = kx * kx;                                  // kx^2
       tab[L + i] = a.t.cx[i];                            // c_x
@@ -381,86 +388,163 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
       }
       release(i0);
     } else if constexpr (MODE == kYFwdYZ) {
-      // acc = (-i c_y(ky)) y(A_y) + (-i c_z(kz)) y(A_z); rows are ky
-      const int kz = ct * KT + c;
-      const bool kv = kz_valid(kz, a.nz);
-      const float cz = kv ? a.t.cz[kz] : 0.f;
-      float2 acc[R2];
-      transform(i0, u, std::false_type{}, 0.f, false);
-      if (jb) {
+      if constexpr (R1 == R2) {
+        // one forward four-step call site run once per input (code stays small)
+        const int kz = ct * KT + c;
+        const bool kv = kz_valid(kz, a.nz);
+        const float cz = kv ? a.t.cz[kz] : 0.f;
+        float2 acc[R2];
+#pragma unroll 1
+        for (int ph = 0; ph < 2; ++ph) {
+          if (ph == 1) {
+            release(i0);
+            if (!acquire(i0 + 1)) return;
+          }
+          float2* buf = smem + ((i0 + ph) % S) * G::BUF;
+          float2 v[R1];
 #pragma unroll
-        for (int k2 = 0; k2 < R2; ++k2) acc[k2] = i_times(-tab[q + R1 * k2], u[k2]);
-      }
-      release(i0);
-      if (!acquire(i0 + 1)) return;
-      transform(i0 + 1, u, std::false_type{}, 0.f, false);
-      if (jb) {
+          for (int n1 = 0; n1 < R1; ++n1) v[n1] = buf[(R2 * n1 + q) * KT + c];
+          __syncthreads();
+          four_step_a<R1, R2, false>(v, buf, q, c, stw);
+          __syncthreads();
+          four_step_b<R1, R2, false>(u, buf, q, c);
+          if (ph == 0) {
 #pragma unroll
-        for (int k2 = 0; k2 < R2; ++k2) {
-          const float2 z = i_times(-cz, u[k2]);
-          const float2 r = kv ? cadd(acc[k2], z) : make_float2(0.f, 0.f);
-          const int ky = q + R1 * k2;
-          a.out[(int64_t)(ky / BY) * a.sb + ((int64_t)outer * BY + ky % BY) * a.P + kz] = r;
+            for (int k2 = 0; k2 < R2; ++k2) acc[k2] = i_times(-tab[q + R1 * k2], u[k2]);
+          } else {
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) {
+              const float2 r = kv ? cadd(acc[k2], i_times(-cz, u[k2])) : make_float2(0.f, 0.f);
+              const int ky = q + R1 * k2;
+              a.out[(int64_t)(ky / BY) * a.sb + ((int64_t)outer * BY + ky % BY) * a.P + kz] = r;
+            }
+          }
         }
+        release(i0 + 1);
+      } else {
+        // acc = (-i c_y(ky)) y(A_y) + (-i c_z(kz)) y(A_z); rows are ky
+        const int kz = ct * KT + c;
+        const bool kv = kz_valid(kz, a.nz);
+        const float cz = kv ? a.t.cz[kz] : 0.f;
+        float2 acc[R2];
+        transform(i0, u, std::false_type{}, 0.f, false);
+        if (jb) {
+  #pragma unroll
+          for (int k2 = 0; k2 < R2; ++k2) acc[k2] = i_times(-tab[q + R1 * k2], u[k2]);
+        }
+        release(i0);
+        if (!acquire(i0 + 1)) return;
+        transform(i0 + 1, u, std::false_type{}, 0.f, false);
+        if (jb) {
+  #pragma unroll
+          for (int k2 = 0; k2 < R2; ++k2) {
+            const float2 z = i_times(-cz, u[k2]);
+            const float2 r = kv ? cadd(acc[k2], z) : make_float2(0.f, 0.f);
+            const int ky = q + R1 * k2;
+            a.out[(int64_t)(ky / BY) * a.sb + ((int64_t)outer * BY + ky % BY) * a.P + kz] = r;
+          }
+        }
+        release(i0 + 1);
       }
-      release(i0 + 1);
     } else if constexpr (MODE == kYInvYZ) {
-      // F_y = y^-1(i c_y(ky) Q), F_z = i c_z(kz) y^-1(Q); load rows are ky
-      float2* buf = smem + (i0 % S) * G::BUF;
-      const int kz = ct * KT + c;
-      const bool kv = kz_valid(kz, a.nz);
-      const float cz = kv ? a.t.cz[kz] : 0.f;
-      float2 v[R1], vy[R1];
-      if (ja) {
+      if constexpr (R1 == R2) {
+        // inverses as conj(FFT(conj(.))): one forward four-step call site
+        float2* buf = smem + (i0 % S) * G::BUF;
+        const int kz = ct * KT + c;
+        const bool kv = kz_valid(kz, a.nz);
+        const float cz = kv ? a.t.cz[kz] : 0.f;
+        float2 keep[R1];
+#pragma unroll 1
+        for (int ph = 0; ph < 2; ++ph) {
+          float2 v[R1];
 #pragma unroll
-        for (int n1 = 0; n1 < R1; ++n1) {
-          v[n1] = buf[(R2 * n1 + q) * KT + c];
-          vy[n1] = i_times(tab[R2 * n1 + q], v[n1]);
+          for (int n1 = 0; n1 < R1; ++n1) {
+            if (ph == 0) {
+              keep[n1] = buf[(R2 * n1 + q) * KT + c];
+              v[n1] = conjf2(i_times(tab[R2 * n1 + q], keep[n1]));
+            } else {
+              v[n1] = conjf2(keep[n1]);
+            }
+          }
+          __syncthreads();
+          four_step_a<R1, R2, false>(v, buf, q, c, stw);
+          __syncthreads();
+          four_step_b<R1, R2, false>(u, buf, q, c);
+#pragma unroll
+          for (int k2 = 0; k2 < R2; ++k2) {
+            const int y = q + R1 * k2;
+            const float2 r = conjf2(u[k2]);
+            const float2 val = ph == 0 ? (kv ? r : make_float2(0.f, 0.f)) : i_times(cz, r);
+            a.out[ph * a.ch + (int64_t)(y / BY) * a.sb + ((int64_t)outer * BY + y % BY) * a.P + kz] = val;
+          }
         }
+        release(i0);
+      } else {
+        // F_y = y^-1(i c_y(ky) Q), F_z = i c_z(kz) y^-1(Q); load rows are ky
+        float2* buf = smem + (i0 % S) * G::BUF;
+        const int kz = ct * KT + c;
+        const bool kv = kz_valid(kz, a.nz);
+        const float cz = kv ? a.t.cz[kz] : 0.f;
+        float2 v[R1], vy[R1];
+        if (ja) {
+  #pragma unroll
+          for (int n1 = 0; n1 < R1; ++n1) {
+            v[n1] = buf[(R2 * n1 + q) * KT + c];
+            vy[n1] = i_times(tab[R2 * n1 + q], v[n1]);
+          }
+        }
+        __syncthreads();
+        if (ja) four_step_a<R1, R2, true>(vy, buf, q, c, stw);
+        __syncthreads();
+        auto store = [&](int chan, int k2, float2 val) {
+          const int y = q + R1 * k2;
+          a.out[chan * a.ch + (int64_t)(y / BY) * a.sb + ((int64_t)outer * BY + y % BY) * a.P + kz] = val;
+        };
+        if (jb) {
+          four_step_b<R1, R2, true>(u, buf, q, c);
+  #pragma unroll
+          for (int k2 = 0; k2 < R2; ++k2) store(0, k2, kv ? u[k2] : make_float2(0.f, 0.f));
+        }
+        __syncthreads();
+        if (ja) four_step_a<R1, R2, true>(v, buf, q, c, stw);
+        __syncthreads();
+        if (jb) {
+          four_step_b<R1, R2, true>(u, buf, q, c);
+  #pragma unroll
+          for (int k2 = 0; k2 < R2; ++k2) store(1, k2, i_times(cz, u[k2]));
+        }
+        release(i0);
       }
-      __syncthreads();
-      if (ja) four_step_a<R1, R2, true>(vy, buf, q, c, stw);
-      __syncthreads();
-      auto store = [&](int chan, int k2, float2 val) {
-        const int y = q + R1 * k2;
-        a.out[chan * a.ch + (int64_t)(y / BY) * a.sb + ((int64_t)outer * BY + y % BY) * a.P + kz] = val;
-      };
-      if (jb) {
-        four_step_b<R1, R2, true>(u, buf, q, c);
-#pragma unroll
-        for (int k2 = 0; k2 < R2; ++k2) store(0, k2, kv ? u[k2] : make_float2(0.f, 0.f));
-      }
-      __syncthreads();
-      if (ja) four_step_a<R1, R2, true>(v, buf, q, c, stw);
-      __syncthreads();
-      if (jb) {
-        four_step_b<R1, R2, true>(u, buf, q, c);
-#pragma unroll
-        for (int k2 = 0; k2 < R2; ++k2) store(1, k2, i_times(cz, u[k2]));
-      }
-      release(i0);
     } else if constexpr (MODE == kXGreen) {
       // column j = yi * P + kz of y block `outer`; rows are kx after the transform
       const int j = ct * KT + c;
       const int yi = j / a.P, kz = j - yi * a.P;
       const int iy = outer * BY + yi;
       const bool kv = kz_valid(kz, a.nz);
-      float kyz2 = 0.f, myz = 1.f;
+      float kyz2 = 0.f, c0 = 0.f;
       if (kv) {
         kyz2 = a.t.ky[iy] * a.t.ky[iy] + a.t.kz[kz] * a.t.kz[kz];
-        if (a.t.mx != nullptr) myz = a.t.my[iy] * a.t.mz[kz];
+        c0 = -a.g.post_scale * (a.t.mx != nullptr ? a.t.my[iy] * a.t.mz[kz] : 1.f);
       }
+      // the transfer tables cover kz <= nz/2 only: never read on padding columns
+      const bool has_t = kv && (a.g.transfer != nullptr || a.g.radial != nullptr);
       float2* buf = smem + (i0 % S) * G::BUF;
       transform(i0, u, std::false_type{}, 0.f, false);
       float2 w[R2];
-      if (jb) {
+      auto multiply = [&](auto ht) {
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) {
           const int kx = q + R1 * k2;
-          const float K = kv ? green_scalar(a, tab, tab + 2 * L, kyz2, myz, kx, iy, kz) : 0.f;
+          const float K = green_scalar<decltype(ht)::value>(a, tab, tab + 2 * L, kyz2, c0, kx, iy, kz);
           u[k2] = make_float2(K * u[k2].x, K * u[k2].y);  // phi
           w[k2] = i_times(tab[L + kx], u[k2]);
         }
+      };
+      if (jb) {
+        if (has_t)
+          multiply(std::true_type{});
+        else
+          multiply(std::false_type{});
       }
       float2 o[R1];
       auto store = [&](int chan, float2 (&val)[R1]) {
@@ -482,11 +566,13 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
       const int yi = j / a.P, kz = j - yi * a.P;
       const int iy = outer * BY + yi;
       const bool kv = kz_valid(kz, a.nz);
-      float kyz2 = 0.f, myz = 1.f;
+      float kyz2 = 0.f, c0 = 0.f;
       if (kv) {
         kyz2 = a.t.ky[iy] * a.t.ky[iy] + a.t.kz[kz] * a.t.kz[kz];
-        if (a.t.mx != nullptr) myz = a.t.my[iy] * a.t.mz[kz];
+        c0 = -a.g.post_scale * (a.t.mx != nullptr ? a.t.my[iy] * a.t.mz[kz] : 1.f);
       }
+      // the transfer tables cover kz <= nz/2 only: never read on padding columns
+      const bool has_t = kv && (a.g.transfer != nullptr || a.g.radial != nullptr);
       float2 acc[R2];
       transform(i0, u, std::false_type{}, 0.f, false);
       if (jb) {
@@ -497,14 +583,20 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
       if (!acquire(i0 + 1)) return;
       float2* buf = smem + ((i0 + 1) % S) * G::BUF;
       transform(i0 + 1, u, std::false_type{}, 0.f, false);
-      if (jb) {
+      auto multiply = [&](auto ht) {
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) {
           const int kx = q + R1 * k2;
-          const float K = kv ? green_scalar(a, tab, tab + 2 * L, kyz2, myz, kx, iy, kz) : 0.f;
+          const float K = green_scalar<decltype(ht)::value>(a, tab, tab + 2 * L, kyz2, c0, kx, iy, kz);
           const float2 s = cadd(acc[k2], u[k2]);
           acc[k2] = make_float2(K * s.x, K * s.y);
         }
+      };
+      if (jb) {
+        if (has_t)
+          multiply(std::true_type{});
+        else
+          multiply(std::false_type{});
       }
       float2 o[R1];
       inverse_held(buf, acc, o);
@@ -513,6 +605,63 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
         for (int k2 = 0; k2 < R1; ++k2) {
           const int x = q + R2 * k2;
           a.out[(int64_t)outer * a.sb + (int64_t)x * BY * a.P + j] = o[k2];
+        }
+      }
+      release(i0 + 1);
+    } else if constexpr (MODE == kXFwdAdjK) {
+      // s = K(k) ((-i c_x) x(B_x) + x(b)); rows are kx
+      const int j = ct * KT + c;
+      const int yi = j / a.P, kz = j - yi * a.P;
+      const int iy = outer * BY + yi;
+      const bool kv = kz_valid(kz, a.nz);
+      float kyz2 = 0.f, c0 = 0.f;
+      if (kv) {
+        kyz2 = a.t.ky[iy] * a.t.ky[iy] + a.t.kz[kz] * a.t.kz[kz];
+        c0 = -a.g.post_scale * (a.t.mx != nullptr ? a.t.my[iy] * a.t.mz[kz] : 1.f);
+      }
+      // the transfer tables cover kz <= nz/2 only: never read on padding columns
+      const bool has_t = kv && (a.g.transfer != nullptr || a.g.radial != nullptr);
+      float2 acc[R2];
+#pragma unroll 1
+      for (int ph = 0; ph < 2; ++ph) {
+        if (ph == 1) {
+          release(i0);
+          if (!acquire(i0 + 1)) return;
+        }
+        if constexpr (R1 == R2) {
+          // square transform: every thread runs both halves, no job guards
+          float2* buf = smem + ((i0 + ph) % S) * G::BUF;
+          float2 v[R1];
+#pragma unroll
+          for (int n1 = 0; n1 < R1; ++n1) v[n1] = buf[(R2 * n1 + q) * KT + c];
+          __syncthreads();
+          four_step_a<R1, R2, false>(v, buf, q, c, stw);
+          __syncthreads();
+          four_step_b<R1, R2, false>(u, buf, q, c);
+        } else {
+          transform(i0 + ph, u, std::false_type{}, 0.f, false);
+        }
+        if (jb) {
+          if (ph == 0) {
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) acc[k2] = i_times(-tab[L + q + R1 * k2], u[k2]);
+          } else {
+            float2* orow = a.out + (int64_t)outer * a.sb + j;
+            const int64_t rs = (int64_t)BY * a.P;
+            auto multiply = [&](auto ht) {
+#pragma unroll
+              for (int k2 = 0; k2 < R2; ++k2) {
+                const int kx = q + R1 * k2;
+                const float K = green_scalar<decltype(ht)::value>(a, tab, tab + 2 * L, kyz2, c0, kx, iy, kz);
+                const float2 sum = cadd(acc[k2], u[k2]);
+                orow[kx * rs] = make_float2(K * sum.x, K * sum.y);
+              }
+            };
+            if (has_t)
+              multiply(std::true_type{});
+            else
+              multiply(std::false_type{});
+          }
         }
       }
       release(i0 + 1);
@@ -859,13 +1008,12 @@ int launch_col_ctas(const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
   return kOk;
 }
 
-// The fused modes that combine two transforms per tile with little state
-// run faster with two resident CTAs per SM (measured at 1024^3 on B200:
-// x + multiplier 6.0 -> 5.3 ms, adjoint 6.0 -> 5.6 ms, y combine 3.3 -> 3.0 ms),
-// the others with one CTA and three stages.
+// The fused x passes run faster with two resident CTAs per SM (measured at
+// 1024^3 on B200: x + multiplier 6.0 -> 5.3 ms, adjoint 6.0 -> 5.6 ms), the
+// others with one CTA and three stages.
 template <int R1, int R2, int MODE>
 int launch_col(const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
-  constexpr bool two = (MODE == kXGreen || MODE == kXGreenAdj || MODE == kYFwdYZ) && R1 == 32 && R2 == 32;
+  constexpr bool two = (MODE == kXGreen || MODE == kXGreenAdj) && R1 == 32 && R2 == 32;
   const int ctas = g_col_ctas != 0 ? g_col_ctas : (two ? 2 : 1);
   return ctas == 2 ? launch_col_ctas<R1, R2, MODE, 2>(map, a, s) : launch_col_ctas<R1, R2, MODE, 1>(map, a, s);
 }
@@ -964,7 +1112,7 @@ int pmfft_z(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in
 
 int pmfft_col(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t, GreenParams g,
               cudaStream_t s) {
-  if (!pmfft_supported(m) || nbatch < 1 || mode < kYFwd || mode > kXGreenAdj) {
+  if (!pmfft_supported(m) || nbatch < 1 || mode < kYFwd || mode > kXFwdAdjK) {
     set_last_error("pmfft: unsupported mesh or mode");
     return kUnsupported;
   }
@@ -1020,7 +1168,8 @@ int pmfft_col(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float
     case kXFwd: return launch_col_len<kXFwd>(L, map, a, s);
     case kXInv: return launch_col_len<kXInv>(L, map, a, s);
     case kXGreen: return launch_col_len<kXGreen>(L, map, a, s);
-    default: return launch_col_len<kXGreenAdj>(L, map, a, s);
+    case kXGreenAdj: return launch_col_len<kXGreenAdj>(L, map, a, s);
+    default: return launch_col_len<kXFwdAdjK>(L, map, a, s);
   }
 }
 
@@ -1065,6 +1214,8 @@ int pmfft_force_adjoint(Mesh3 m, const float* mesh_cot, float* src_cot, float2* 
   if (st != kOk) return st;
   if ((st = pmfft_col(m, kYFwd, 1, 0, a3, bb, t, g, s)) != kOk) return st;
   if ((st = pmfft_col(m, kYFwdYZ, 1, 1, a3, bb + C, t, g, s)) != kOk) return st;
+  // fused x pass (4.45 ms at 1024^3) rather than the multiplier pass plus a
+  // plain inverse x pass (3.45 + 1.49 ms)
   if ((st = pmfft_col(m, kXGreenAdj, 1, 0, bb, a3, t, g, s)) != kOk) return st;
   if ((st = pmfft_col(m, kYInv, 1, 0, a3, a3 + C, t, g, s)) != kOk) return st;
   return pmfft_z(m, 1, 1, nullptr, a3 + C, src_cot, nullptr, s);

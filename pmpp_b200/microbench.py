@@ -175,6 +175,8 @@ def pmfft_stages(conf, reps, peak, only=None):
         "fft_y_yz": lambda: col(3, 1, a, b),
         "fft_x_green": lambda: col(6, 0, a, b, inv_m),
         "fft_x_green_adj": lambda: col(7, 0, a, b, inv_m),
+        "fft_x_adj": lambda: col(8, 0, a, b, inv_m),
+        "fft_x_inv": lambda: col(5, 0, a, b),
         "fft_y_inv": lambda: col(1, 0, a, b),
         "fft_y_inv_yz": lambda: col(2, 0, a, b),
         "fft_z_c2r": lambda: call("pmb_pmfft_z", nx, ny, nz, 1, 1, a, real3b.data_ptr(), s),

@@ -37,6 +37,8 @@ def algorithmic_bytes(op, N, M, Mc=None, R=None, T=None):
         "fft_y_inv_yz": 24 * Mc,
         "fft_x_green": 24 * Mc,
         "fft_x_green_adj": 24 * Mc,
+        "fft_x_adj": 24 * Mc,
+        "fft_x_inv": 16 * Mc,
         "fft_z_c2r": 8 * Mc + 4 * M,
         "fft_z_c2r3": 3 * (8 * Mc + 4 * M),
         "green_gradient": 8 * Mc + 24 * Mc,
