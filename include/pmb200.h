@@ -198,6 +198,11 @@ int pmb_kick_adj(float* vel, const float* acc, const float* vel_cot, float* acc_
 int pmb_kick_adj2(float* vel, const float* acc, const float* vel_cot, float* acc_cot, int64_t n, float kick_a,
                   float kick_b, int two, int zero_cot, double* dot_a, double* dot_b, double* dot_force,
                   void* stream);
+/* Cotangent half of pmb_drift_adj (vel_cot += disp_cot * drift, dot += sum
+ * disp_cot * vel); the position half is a drift by -drift, fused into the
+ * next pmb_force's sort (bit-identical to pmb_drift_adj's position update). */
+int pmb_drift_cot_adj(const float* vel, const float* disp_cot, float* vel_cot, int64_t n, float drift, double* dot,
+                      void* stream);
 /* Drift adjoint (integrator.py:459-474); dot += sum disp_cot*vel. */
 int pmb_drift_adj(float* disp, const float* vel, const float* disp_cot, float* vel_cot, int64_t n, float drift,
                   double* dot, void* stream);

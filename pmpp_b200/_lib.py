@@ -52,6 +52,7 @@ _SIGS = {
     "pmb_axpy": (c_int, [c_p, c_p, c_i64, c_f, c_p]),
     "pmb_kick_adj": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_p, c_p]),
     "pmb_kick_adj2": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_f, c_int, c_int, c_p, c_p, c_p, c_p]),
+    "pmb_drift_cot_adj": (c_int, [c_p, c_p, c_p, c_i64, c_f, c_p, c_p]),
     "pmb_drift_adj": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_p, c_p]),
     "pmb_dot": (c_int, [c_p, c_p, c_i64, c_p, c_p]),
     "pmb_sum": (c_int, [c_p, c_i64, c_p, c_p]),
@@ -144,7 +145,7 @@ def check(status, what):
 # Hand-written kernels launched per entry point (cuFFT's own kernels excluded).
 _KERNELS = {
     "pmb_sort_rows": 5, "pmb_gather_rows": 1, "pmb_interp_grad_rows": 1, "pmb_green_gradient": 1,
-    "pmb_green_gradient_adjoint": 1, "pmb_axpy": 1, "pmb_kick_adj": 1, "pmb_kick_adj2": 1, "pmb_drift_adj": 1, "pmb_dot": 1,
+    "pmb_green_gradient_adjoint": 1, "pmb_axpy": 1, "pmb_kick_adj": 1, "pmb_kick_adj2": 1, "pmb_drift_cot_adj": 1, "pmb_drift_adj": 1, "pmb_dot": 1,
     "pmb_force": 9, "pmb_force_vjp": 11, "pmb_force_vjp_presorted": 6, "pmb_sum": 1, "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,
     "pmb_lpt": 4, "pmb_lpt_vjp": 6, "pmb_pk_shells": 1, "pmb_shell_stats": 1, "pmb_pk_shells_adjoint": 1,
     "pmb_overdensity": 1, "pmb_ens_force": 7, "pmb_ens_step": 9, "pmb_ens_set_step": 1,

@@ -432,6 +432,12 @@ int pmb_kick_adj2(float* vel, const float* acc, const float* vel_cot, float* acc
                    S(stream));
 }
 
+int pmb_drift_cot_adj(const float* vel, const float* disp_cot, float* vel_cot, int64_t n, float drift, double* dot,
+                      void* stream) {
+  PMB_REQUIRE(dot != nullptr, "pmb_drift_cot_adj: dot accumulator required");
+  return drift_cot_adj(vel, disp_cot, vel_cot, n, drift, dot, S(stream));
+}
+
 int pmb_drift_adj(float* disp, const float* vel, const float* disp_cot, float* vel_cot, int64_t n, float drift,
                   double* dot, void* stream) {
   PMB_REQUIRE(dot != nullptr, "pmb_drift_adj: dot accumulator required");

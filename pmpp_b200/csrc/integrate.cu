@@ -83,6 +83,20 @@ __global__ void kick_adj2_kernel(float* __restrict__ vel, const float* __restric
   if (dot_f != nullptr) block_add(sf, dot_f);
 }
 
+// Cotangent half of the drift adjoint: vel_cot += disp_cot * d, dot += sum
+// disp_cot * vel.  The position half (disp -= vel * d) runs fused into the
+// next force evaluation's sort as a drift by -d (the same float operations).
+__global__ void drift_cot_adj_kernel(const float* __restrict__ vel, const float* __restrict__ disp_cot,
+                                     float* __restrict__ vel_cot, int64_t n, float d, double* __restrict__ dot) {
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float dc = disp_cot[i];
+    vel_cot[i] = __fadd_rn(vel_cot[i], __fmul_rn(dc, d));
+    s += (double)dc * (double)vel[i];
+  }
+  block_add(s, dot);
+}
+
 __global__ void drift_adj_kernel(float* __restrict__ disp, const float* __restrict__ vel,
                                  const float* __restrict__ disp_cot, float* __restrict__ vel_cot, int64_t n, float d,
                                  double* __restrict__ dot) {
@@ -130,6 +144,13 @@ int kick_adj2(float* vel, const float* acc, const float* vel_cot, float* acc_cot
   if (n > 0)
     kick_adj2_kernel<<<grid_n(n, 256), 256, 0, s>>>(vel, acc, vel_cot, acc_cot, n, ka, kb, two, zero_cot, dot_a, dot_b,
                                                     dot_f);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int drift_cot_adj(const float* vel, const float* disp_cot, float* vel_cot, int64_t n, float d, double* dot,
+                  cudaStream_t s) {
+  if (n > 0) drift_cot_adj_kernel<<<grid_n(n, 256), 256, 0, s>>>(vel, disp_cot, vel_cot, n, d, dot);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }

@@ -24,14 +24,24 @@ def _om32(omega_m):
     return float(np.float32(omega_m))
 
 
-def _stage_buffers(n, conf, dev):
-    """Workspace views shared by the staged force and force adjoint."""
+def _lane_suffix(lane):
+    """Lane "0" is the default workspace (a forward run's last force doubles as it)."""
+    return "" if lane in ("", "0") else lane
+
+
+def _stage_buffers(n, conf, dev, sorted_lane="", work_lane=""):
+    """Workspace views of the staged force and force adjoint.
+
+    sorted_lane names the sorted-record buffer (the reverse sweep alternates
+    two so a force adjoint can read one while the next force writes the
+    other); work_lane the scratch, meshes and spectra ("v" gives a force
+    adjoint its own set, for running beside a force evaluation)."""
     L = lib()
     nx, ny, nz = conf.mesh_shape
-    sorted_buf = workspace(L.pmb_sorted_bytes(n, nx, ny, nz), dev, "st_sorted")
-    sort_scr = workspace(L.pmb_sort_scratch_bytes(n, nx, ny, nz), dev, "st_sortscr")
-    s16 = workspace(16, dev, "st_s16")
-    real3 = workspace(12 * conf.mesh_size, dev, "st_real3")
+    sorted_buf = workspace(L.pmb_sorted_bytes(n, nx, ny, nz), dev, "st_sorted" + _lane_suffix(sorted_lane))
+    sort_scr = workspace(L.pmb_sort_scratch_bytes(n, nx, ny, nz), dev, "st_sortscr" + work_lane)
+    s16 = workspace(16, dev, "st_s16" + work_lane)
+    real3 = workspace(12 * conf.mesh_size, dev, "st_real3" + work_lane)
     return sorted_buf, sort_scr, s16, real3
 
 
@@ -56,7 +66,7 @@ class _NoTimer:
 
 
 def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc, drift_vel, drift, vel_kick,
-                  kick, timer, src_hat_out=None):
+                  kick, timer, src_hat_out=None, lane=""):
     """pmb_force as separate stage calls with a CUDA event after each stage.
 
     With src_hat_out (complex64, half spectrum) the rFFT of the Poisson source
@@ -65,7 +75,7 @@ def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F
     nx, ny, nz = conf.mesh_shape
     dev = disp.device
     s = stream_handle(dev)
-    sorted_buf, sort_scr, s16, real3 = _stage_buffers(n, conf, dev)
+    sorted_buf, sort_scr, s16, real3 = _stage_buffers(n, conf, dev, sorted_lane=lane)
     timer = _NoTimer() if timer is None else timer
     t = timer.start()
     call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
@@ -110,7 +120,7 @@ def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F
 
 
 def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc_cot, disp_cot, timer,
-                      src_hat=None, transfer_cot_out=None, presorted=False):
+                      src_hat=None, transfer_cot_out=None, presorted=False, sorted_lane="", work_lane=""):
     """pmb_force_vjp as separate stage calls with a CUDA event after each stage.
 
     With src_hat (the source spectrum at the same positions) and
@@ -120,14 +130,15 @@ def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, r
     nx, ny, nz = conf.mesh_shape
     dev = disp.device
     s = stream_handle(dev)
-    sorted_buf, sort_scr, s16, real3 = _stage_buffers(n, conf, dev)
+    sorted_buf, sort_scr, s16, real3 = _stage_buffers(n, conf, dev, sorted_lane if presorted else work_lane,
+                                                      work_lane)
     timer = _NoTimer() if timer is None else timer
     t = timer.start()
     if not presorted:
         call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), None, 0.0, n, nx, ny, nz, float(conf.cell_size),
              sorted_buf.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
         t = timer.mark("sort", t)
-    cot_sorted = workspace(12 * n, dev, "st_cot_sorted")
+    cot_sorted = workspace(12 * n, dev, "st_cot_sorted" + work_lane)
     call("pmb_interp_grad_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc_cot.data_ptr(), 0.0,
          float(conf.cell_size), 1, disp_cot.data_ptr(), None, cot_sorted.data_ptr(), s)
     t = timer.mark("gather_adjoint", t)
@@ -139,7 +150,7 @@ def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, r
     if transfer_cot_out is None and pmfft_active(nx, ny, nz):
         # transposed pass chain: z R2C x3, y (x channel; y and z folded), x + adjoint multiplier + x^-1, y^-1, z C2R
         C8 = 8 * lib().pmb_pmfft_channel_elems(nx, ny, nz)
-        pm = workspace(5 * C8, dev, "st_pm5")
+        pm = workspace(5 * C8, dev, "st_pm5" + work_lane)
         a3, bb = pm.data_ptr(), pm.data_ptr() + 3 * C8
         call("pmb_pmfft_z", nx, ny, nz, 0, 3, real3.data_ptr(), a3, s)
         t = timer.mark("fft_z_r2c3", t)
@@ -181,12 +192,13 @@ def _correction_args(correction, a, cosmo, conf):
 
 
 def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, force_meshes=None, acc=None,
-          drift_vel=None, drift=0.0, vel_kick=None, kick=0.0, src_hat_out=None):
+          drift_vel=None, drift=0.0, vel_kick=None, kick=0.0, src_hat_out=None, lane=""):
     """One PM force evaluation on device tensors.
 
     Returns (acc (N,3), force_meshes (3,Mx,My,Mz)).  With drift_vel the
     particles are drifted first (disp updated in place); with vel_kick the
-    half-kick vel_kick += acc * kick is fused into the gather."""
+    half-kick vel_kick += acc * kick is fused into the gather.  lane selects
+    the workspace that keeps the sorted records (see force_vjp)."""
     require_cuda(pmid, disp, drift_vel, vel_kick)
     n = pmid.shape[0]
     nx, ny, nz = conf.mesh_shape
@@ -199,12 +211,12 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
     tables = conf.spectral_tables("mesh", dev, gk)
     if StageTimer.active is not None or src_hat_out is not None:
         _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc, drift_vel,
-                      drift, vel_kick, kick, StageTimer.active, src_hat_out)
+                      drift, vel_kick, kick, StageTimer.active, src_hat_out, lane)
         return acc, force_meshes
     wb = lib().pmb_force_workspace_bytes(n, nx, ny, nz)
     if wb < 0:
         raise RuntimeError("pmb_force_workspace_bytes failed: " + lib().pmb_last_error().decode())
-    ws = workspace(wb, dev, "force")
+    ws = workspace(wb, dev, "force" + _lane_suffix(lane))
     call("pmb_force", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
          float(conf.cell_size), float(conf.mesh_size / conf.ptcl_num), 1.5 * _om32(omega_m), tables.data_ptr(),
          int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, force_meshes.data_ptr(),
@@ -213,12 +225,15 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
 
 
 def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *, a=None, cosmo=None,
-              correction=None, src_hat=None, transfer_cot_out=None, presorted=False):
+              correction=None, src_hat=None, transfer_cot_out=None, presorted=False, sorted_lane="",
+              concurrent=False):
     """disp_cot (+)= (d acc / d disp)^T acc_cot, with force_meshes computed at disp.
 
-    presorted: the last force() call on this device was at exactly these
-    positions and took the same route (fused or staged); its cell-sorted
-    records are reused instead of sorting again."""
+    presorted: the last force() call with lane=sorted_lane was at exactly
+    these positions and took the same route (fused or staged); its
+    cell-sorted records are reused instead of sorting again (disp is then not
+    read).  concurrent: use workspaces of its own so that a force() may run on
+    another stream at the same time."""
     require_cuda(pmid, disp, force_meshes, acc_cot, disp_cot)
     n = pmid.shape[0]
     nx, ny, nz = conf.mesh_shape
@@ -229,13 +244,14 @@ def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *
     tables = conf.spectral_tables("mesh", dev, gk)
     if StageTimer.active is not None or transfer_cot_out is not None:
         _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc_cot,
-                          disp_cot, StageTimer.active, src_hat, transfer_cot_out, presorted)
+                          disp_cot, StageTimer.active, src_hat, transfer_cot_out, presorted, sorted_lane,
+                          "v" if concurrent else "")
         return disp_cot
     wb = lib().pmb_force_vjp_workspace_bytes(n, nx, ny, nz)
     ws = workspace(wb, dev, "force_vjp")
     if presorted:
         # head of the fused force's workspace: its sorted records
-        head = workspace(lib().pmb_force_workspace_bytes(n, nx, ny, nz), dev, "force")
+        head = workspace(lib().pmb_force_workspace_bytes(n, nx, ny, nz), dev, "force" + _lane_suffix(sorted_lane))
         call("pmb_force_vjp_presorted", head.data_ptr(), n, nx, ny, nz, float(conf.cell_size),
              float(conf.mesh_size / conf.ptcl_num), 1.5 * _om32(omega_m), tables.data_ptr(),
              int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, force_meshes.data_ptr(),

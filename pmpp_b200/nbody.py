@@ -19,7 +19,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from ._lib import call
+from ._lib import call, pmfft_active
 from .gravity import force, force_vjp, _om32
 from .particles import Particles
 from .runtime import stream_handle
@@ -85,10 +85,16 @@ def integrate(a_prev, a_next, ptcl, cosmo, conf, correction=None):
 class NBodyRun:
     """Fused forward integration that keeps the final force meshes for the adjoint."""
 
-    def __init__(self, conf, cosmo, correction=None):
+    def __init__(self, conf, cosmo, correction=None, overlap=False):
         self.conf = conf
         self.cosmo = cosmo
         self.correction = correction
+        # reverse sweep: run each force recompute on a side stream beside the
+        # force adjoint it does not depend on (results are unchanged).  Off by
+        # default: at 512^3 / 1024^3 the step went 3.54 -> 4.03 s, the
+        # persistent FFT passes (static tile order, one CTA per SM) stalling
+        # behind the other stream's CTAs.
+        self.overlap = overlap
 
     def forward(self, ptcl, a_nbody=None):
         conf, cosmo = self.conf, self.cosmo
@@ -140,20 +146,20 @@ class NBodyRun:
         nx, ny, nz = self.conf.mesh_shape
         return torch.empty((nx, ny, nz // 2 + 1), dtype=torch.complex64, device=device)
 
-    def _force_adjoint(self, pmid, disp, F, S, ac, dc, a, presorted=False):
+    def _force_adjoint(self, pmid, disp, F, S, ac, dc, a, presorted=False, lane="", concurrent=False):
         """Force adjoint; with a trainable correction also its parameter gradient.
 
-        presorted: the previous force() call was at exactly these positions."""
+        presorted: the force() call with this lane was at exactly these positions."""
         conf, cosmo, corr = self.conf, self.cosmo, self.correction
         if self._trainable():
             from .corrections import radial_table_len
             tc = torch.zeros(radial_table_len(conf), dtype=torch.float64, device=disp.device)
             force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=corr, src_hat=S,
-                      transfer_cot_out=tc, presorted=presorted)
+                      transfer_cot_out=tc, presorted=presorted, sorted_lane=lane, concurrent=concurrent)
             corr.accumulate(a, cosmo, conf, tc)
         else:
             force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=corr,
-                      presorted=presorted)
+                      presorted=presorted, sorted_lane=lane, concurrent=concurrent)
 
     def _require_f32(self):
         if self.conf.float_dtype != torch.float32:
@@ -194,9 +200,23 @@ class NBodyRun:
         recomputed = False
         zero_pending = False  # acc_cot consumed by a force adjoint, not yet cleared
         force_dot_done = False
+        # The recompute at the previous positions needs only vel (after the kick
+        # adjoints) and disp; the force adjoint at the current positions reads
+        # its sorted records, meshes and cotangents.  With overlap the recompute
+        # runs on a side stream beside it, the drift's position half fused into
+        # its sort, alternating two sorted-record lanes.
+        overlap = (self.overlap and dev.type == "cuda" and not self._trainable()
+                   and pmfft_active(*conf.mesh_shape))
+        main = torch.cuda.current_stream(dev) if dev.type == "cuda" else None
+        side = torch.cuda.Stream(device=dev) if overlap else None
+        ev_force = None  # side-stream force that main must see before touching vel / acc
+        lane = 0  # lane holding the sorted records of the current positions
         i = 0
         while i < len(ops):
             st = ops[i]
+            if ev_force is not None:
+                main.wait_event(ev_force)
+                ev_force = None
             if st[0] == "kick":
                 # consecutive kick adjoints share acc: one kernel for up to two,
                 # which also forms the force-slot dot of a following force adjoint
@@ -232,7 +252,13 @@ class NBodyRun:
                 slot += 1
             force_dot_done = False
             a_force = float(a[0]) if st[0] == "init" else float(st[3])
-            self._force_adjoint(pmid, disp, F, S, ac, dc, a_force, presorted=recomputed)
+            ev_ready = None
+            if overlap and recomputed:
+                ev_ready = main.record_event()  # vel and acc final for this step
+            self._force_adjoint(pmid, disp, F, S, ac, dc, a_force, presorted=recomputed, lane=str(lane),
+                                concurrent=overlap)
+            if overlap and ev_ready is None:
+                ev_ready = main.record_event()  # the first adjoint sorted disp itself
             i += 1
             if st[0] == "init":
                 ac.zero_()
@@ -240,16 +266,31 @@ class NBodyRun:
             zero_pending = True
             _, a_vel, a_dp, a_dn, a_acc_in = st
             D, dD = cosmo.drift_factor(a_vel, a_dp, a_dn, with_grad=True)
-            call("pmb_drift_adj", disp.data_ptr(), vel.data_ptr(), dc.data_ptr(), vc.data_ptr(), disp.numel(),
-                 _f32(D), dots[slot:].data_ptr(), s)
+            D32 = _f32(D)
+            # recompute the incoming acceleration at disp - D vel (the drift's
+            # position half, fused into the sort); keep its meshes for the next
+            # force adjoint
+            if overlap:
+                side.wait_event(ev_ready)
+                with torch.cuda.stream(side):
+                    force(pmid, disp, conf, cosmo.Omega_m, a=float(a_acc_in), cosmo=cosmo, correction=corr,
+                          force_meshes=F2, acc=acc, src_hat_out=S2, drift_vel=vel, drift=-D32,
+                          lane=str(1 - lane))
+                ev_force = side.record_event()
+            # the drift's cotangent half: vel_cot += D disp_cot (after the force adjoint)
+            call("pmb_drift_cot_adj", vel.data_ptr(), dc.data_ptr(), vc.data_ptr(), disp.numel(), D32,
+                 dots[slot:].data_ptr(), s)
             grads.append((dD, slot))
             slot += 1
-            # recompute the incoming acceleration; keep its meshes for the next force adjoint
-            force(pmid, disp, conf, cosmo.Omega_m, a=float(a_acc_in), cosmo=cosmo, correction=corr,
-                  force_meshes=F2, acc=acc, src_hat_out=S2)
+            if not overlap:
+                force(pmid, disp, conf, cosmo.Omega_m, a=float(a_acc_in), cosmo=cosmo, correction=corr,
+                      force_meshes=F2, acc=acc, src_hat_out=S2, drift_vel=vel, drift=-D32, lane=str(1 - lane))
+            lane = 1 - lane
             recomputed = True
             F, F2 = F2, F
             S, S2 = S2, S
+        if ev_force is not None:
+            main.wait_event(ev_force)
         if zero_pending:
             ac.zero_()
         d = dots.cpu().numpy()
