@@ -142,8 +142,7 @@ int pmb_green_gradient_adjoint(const void* grad_cot_hat, void* src_cot_hat, int 
  * separate multiplier kernels instead (default 1).
  * pmb_pmfft_timeouts: bounded copy waits in these passes that gave up.
  * pmb_pmfft_set_col_ctas(0, 1 or 2): resident CTAs per SM of the column
- *   passes, 0 = the measured per-mode default (a tuning knob; results are
- *   identical). */
+ *   passes, 0 = the default (one); a tuning knob, results are identical. */
 int pmb_set_pmfft(int enabled);
 int pmb_pmfft_supported(int nx, int ny, int nz);
 int64_t pmb_pmfft_channel_elems(int nx, int ny, int nz);

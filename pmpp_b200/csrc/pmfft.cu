@@ -991,7 +991,7 @@ constexpr int stages_for(int buf_bytes, int extra, int ctas) {
 }
 
 // Resident CTAs per SM of the column passes (1: 255 registers and up to 3
-// stages per CTA; 2: 128 registers and one or two stages each; 0: per mode).
+// stages per CTA; 2: 128 registers and one or two stages each; 0: default).
 int g_col_ctas = 0;
 
 template <int R1, int R2, int MODE, int CTAS>
@@ -1008,14 +1008,13 @@ int launch_col_ctas(const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
   return kOk;
 }
 
-// The fused x passes run faster with two resident CTAs per SM (measured at
-// 1024^3 on B200: x + multiplier 6.0 -> 5.3 ms, adjoint 6.0 -> 5.6 ms), the
-// others with one CTA and three stages.
+// One resident CTA per SM (255 registers, three stages) for every pass.  Two
+// CTAs of 128 registers spill in the fused x passes; with the multiplier's
+// tables in shared memory one CTA is faster (1024^3 on B200: x + multiplier
+// 4.07 against 4.53 ms, adjoint 4.02 against 4.45 ms).
 template <int R1, int R2, int MODE>
 int launch_col(const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
-  constexpr bool two = (MODE == kXGreen || MODE == kXGreenAdj) && R1 == 32 && R2 == 32;
-  const int ctas = g_col_ctas != 0 ? g_col_ctas : (two ? 2 : 1);
-  return ctas == 2 ? launch_col_ctas<R1, R2, MODE, 2>(map, a, s) : launch_col_ctas<R1, R2, MODE, 1>(map, a, s);
+  return g_col_ctas == 2 ? launch_col_ctas<R1, R2, MODE, 2>(map, a, s) : launch_col_ctas<R1, R2, MODE, 1>(map, a, s);
 }
 
 template <int MODE>
