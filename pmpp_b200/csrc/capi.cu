@@ -127,7 +127,7 @@ int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int 
   } else {
     float a = fabsf(val_const);
     PMB_REQUIRE(a < INFINITY, "pmb_scatter_rows: non-finite value");
-    PMB_TRY(set_double(scale, a > 0.f ? fixed_point_pow2(n) / (double)a : 1.0, S(stream)));
+    PMB_TRY(set_double(scale, fixed_point_scale(fixed_point_pow2(n), a), S(stream)));
   }
   return scatter_sorted(v.rec, v.perm, v.offs, m, C, val, val_sorted, val_const, scale, mode, src_mul, out,
                         S(stream));

@@ -204,9 +204,10 @@ int bin_particles(const int16_t* pmid, float* disp, const float* vel, float drif
 // ---------------------------------------------------------------------------
 // Fixed-point scale for the deterministic scatter
 // ---------------------------------------------------------------------------
-// Contributions val*w are converted to int64 units of 1/scale with
-// scale = 2^e / max|val|, e = 62 - ceil(log2(n + 1)), so that the sum of up to
-// n contributions of magnitude <= max|val| cannot overflow.
+// Contributions val*w are converted to int64 units of 1/scale with the power
+// of two scale = 2^e / 2^ceil(log2 max|val|), e = 62 - ceil(log2(n + 1)) (at
+// most 52), so that the sum of up to n contributions of magnitude <= max|val|
+// cannot overflow and val*w*scale is exact in float.
 __global__ void absmax_kernel(const float* __restrict__ v, int64_t count, unsigned int* __restrict__ out) {
   float mx = 0.f;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
@@ -224,7 +225,7 @@ __global__ void scale_from_absmax_kernel(const unsigned int* __restrict__ bits, 
     *scale = __longlong_as_double(0x7ff8000000000000ll);
     return;
   }
-  *scale = mx > 0.f ? pow2e / (double)mx : 1.0;
+  *scale = fixed_point_scale(pow2e, mx);
 }
 
 double fixed_point_pow2(int64_t n) {

@@ -473,7 +473,7 @@ int pmb_ens_create(int nsims, const int64_t* counts, const int32_t* mesh_shapes,
     q.src_mul = src_muls[s];
     q.post = (float)(1.0 / (double)q.m.cells());
     const float a = fabsf(vals[s]);
-    q.scale = a > 0.f ? fixed_point_pow2(q.n) / (double)a : 1.0;
+    q.scale = fixed_point_scale(fixed_point_pow2(q.n), a);
     q.rx = 2;
     q.ry = 2;
     if (q.rx > q.m.nx) q.rx = q.m.nx;

@@ -108,7 +108,7 @@ extern "C" int pmb_scatter_density_noalloc(const int16_t* pmid, const float* dis
     set_last_error("pmb_scatter_density_noalloc: non-finite value");
     return kInvalidArgument;
   }
-  st = set_double(scale, a > 0.f ? fixed_point_pow2(n) / (double)a : 1.0, s);
+  st = set_double(scale, fixed_point_scale(fixed_point_pow2(n), a), s);
   if (st != kOk) return st;
   return scatter_sorted(rec, perm, offs, m, 1, nullptr, 0, val, scale, 0, 1.f, out, s);
 }

@@ -98,8 +98,12 @@ __device__ __forceinline__ void scatter_tile(const Rec* __restrict__ rec, const 
   const uint32_t ntot = sm.seg_pre[nsrc];
   const bool split = ntot < 65536u;
   unsigned long long* acc64 = reinterpret_cast<unsigned long long*>(acc);
+  // the scale is a power of two: contrib * scale is exact in float when the
+  // scale itself is a float (always, unless max|val| < 2^-74)
+  const bool fscale = scale < 0x1p126;
+  const float scalef = fscale ? (float)scale : 0.f;
+  int k = 0;  // source segment of idx; idx only grows, so the search resumes
   for (uint32_t idx = threadIdx.x; idx < ntot; idx += blockDim.x) {
-    int k = 0;
     while (idx >= sm.seg_pre[k + 1]) ++k;
     const int sx = k / (RY + 1) - 1, sy = k % (RY + 1) - 1;
     const uint32_t i = sm.seg_beg[k] + (idx - sm.seg_pre[k]);
@@ -132,7 +136,8 @@ __device__ __forceinline__ void scatter_tile(const Rec* __restrict__ rec, const 
 #pragma unroll
           for (int c = 0; c < C; ++c) {
             const float contrib = __fmul_rn(v[c], w);
-            const long long q = __double2ll_rn((double)contrib * scale);
+            const long long q = fscale ? __float2ll_rn(__fmul_rn(contrib, scalef))
+                                       : __double2ll_rn((double)contrib * scale);
             const int a = ((lx * RY + ly) * C + c) * nz + z;
             if (split) {
               atomicAdd(&acc[a], (unsigned int)(q >> 32));

@@ -10,6 +10,7 @@
 // the row of their lower CIC corner, so bin order equals raveled-cell order.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -136,6 +137,17 @@ inline SpecTables spec_tables_from(const float* t, Mesh3 m, int has_masks) {
     s.mx = s.my = s.mz = nullptr;
   }
   return s;
+}
+
+// Scale of the fixed-point deposit: pow2e / 2^ceil(log2 amax), the largest
+// power of two with scale * amax <= pow2e, so val * w * scale is exact in
+// float and rounding it to an integer is the only rounding (1.0 for a zero or
+// negative amax).
+__host__ __device__ inline double fixed_point_scale(double pow2e, float amax) {
+  if (!(amax > 0.f)) return 1.0;
+  int x = 0;
+  const double m = frexp((double)amax, &x);  // amax = m 2^x, m in [0.5, 1)
+  return ldexp(pow2e, m == 0.5 ? 1 - x : -x);
 }
 
 // Floats in one spectral table of mesh m.

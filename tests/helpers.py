@@ -25,8 +25,8 @@ def fixed_point_scatter(pmid, disp, conf_o, val):
 
     float32 corner weights as the reference enmesh forms them, contributions
     c = float32(val * w), q = round_half_even(float64(c) * scale) summed exactly
-    in int64 per cell, result float32(float64(sum) / scale), with
-    scale = 2^e / max|val| and e = min(62 - ceil(log2(n + 1)), 52)."""
+    in int64 per cell, result float32(float64(sum) / scale), with the power of
+    two scale = 2^e / 2^ceil(log2 max|val|) and e = min(62 - ceil(log2(n + 1)), 52)."""
     mesh_shape = conf_o.mesh_shape
     cell, d, fl = opm.enmesh(pmid, disp, conf_o)
     w, _ = opm.corner_weights(d, fl, np.float32)
@@ -37,7 +37,8 @@ def fixed_point_scatter(pmid, disp, conf_o, val):
         lg += 1
     e = min(62 - lg, 52)
     val = np.asarray(val, np.float32)
-    scale = np.ldexp(1.0, e) / float(np.abs(val).max())
+    m, x = np.frexp(float(np.abs(val).max()))
+    scale = np.ldexp(1.0, e - (int(x) - 1 if m == 0.5 else int(x)))
     M = int(np.prod(mesh_shape))
     chans = [val] if val.ndim <= 1 else [val[:, c] for c in range(val.shape[1])]
     outs = []
