@@ -188,21 +188,32 @@ struct Corners {
 // corner c moves +1 along axis a when bit a of c is set.
 __device__ __forceinline__ void corners_of(const Rec& r, Mesh3 m, Corners& k) {
   const uint32_t key = r.key;
-  const int cz = (int)(key % (uint32_t)m.nz);
-  const uint32_t rowk = key / (uint32_t)m.nz;
-  const int cy = (int)(rowk % (uint32_t)m.ny);
-  const int cx = (int)(rowk / (uint32_t)m.ny);
-  const int x1 = cx + 1 == m.nx ? 0 : cx + 1;
-  const int y1 = cy + 1 == m.ny ? 0 : cy + 1;
-  const int z1 = cz + 1 == m.nz ? 0 : cz + 1;
+  int cx, cy, cz;
+  if (((m.nz & (m.nz - 1)) | (m.ny & (m.ny - 1))) == 0) {
+    // power-of-two rows and planes: shifts instead of divisions
+    const int lz = __ffs(m.nz) - 1, ly = __ffs(m.ny) - 1;
+    cz = (int)(key & (uint32_t)(m.nz - 1));
+    cy = (int)((key >> lz) & (uint32_t)(m.ny - 1));
+    cx = (int)(key >> (lz + ly));
+  } else {
+    cz = (int)(key % (uint32_t)m.nz);
+    const uint32_t rowk = key / (uint32_t)m.nz;
+    cy = (int)(rowk % (uint32_t)m.ny);
+    cx = (int)(rowk / (uint32_t)m.ny);
+  }
+  // lower corner and the (periodic) steps to the upper one along each axis
+  const int64_t plane = (int64_t)m.ny * m.nz;
+  const int64_t base = (int64_t)key;  // raveled lower cell, (cx * ny + cy) * nz + cz
+  const int64_t dx = cx + 1 == m.nx ? -(int64_t)cx * plane : plane;
+  const int64_t dy = cy + 1 == m.ny ? -(int64_t)cy * m.nz : (int64_t)m.nz;
+  const int64_t dz = cz + 1 == m.nz ? -(int64_t)cz : 1;
   const float wx[2] = {axis_weight(r.fx, 0), axis_weight(r.fx, 1)};
   const float wy[2] = {axis_weight(r.fy, 0), axis_weight(r.fy, 1)};
   const float wz[2] = {axis_weight(r.fz, 0), axis_weight(r.fz, 1)};
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
     const int bx = c & 1, by = (c >> 1) & 1, bz = (c >> 2) & 1;
-    const int x = bx ? x1 : cx, y = by ? y1 : cy, z = bz ? z1 : cz;
-    k.idx[c] = ((int64_t)x * m.ny + y) * m.nz + z;
+    k.idx[c] = base + (bx ? dx : 0) + (by ? dy : 0) + (bz ? dz : 0);
     k.w[c] = __fmul_rn(__fmul_rn(wx[bx], wy[by]), wz[bz]);
   }
 }
