@@ -103,12 +103,13 @@ __device__ __forceinline__ void scatter_tile(const Rec* __restrict__ rec, const 
   const bool fscale = scale < 0x1p126;
   const float scalef = fscale ? (float)scale : 0.f;
   int k = 0;  // source segment of idx; idx only grows, so the search resumes
+  const bool zpow2 = (nz & (nz - 1)) == 0;
   for (uint32_t idx = threadIdx.x; idx < ntot; idx += blockDim.x) {
     while (idx >= sm.seg_pre[k + 1]) ++k;
     const int sx = k / (RY + 1) - 1, sy = k % (RY + 1) - 1;
     const uint32_t i = sm.seg_beg[k] + (idx - sm.seg_pre[k]);
     const Rec r = rec[i];
-    const int cz = (int)(r.key % (uint32_t)nz);
+    const int cz = zpow2 ? (int)(r.key & (uint32_t)(nz - 1)) : (int)(r.key % (uint32_t)nz);
     float v[C];
     if (val != nullptr) {
       const int64_t src = val_sorted ? (int64_t)i : (int64_t)perm[i];
