@@ -206,6 +206,14 @@ static bool g_use_pmfft = true;
 
 static bool use_pmfft(Mesh3 m) { return g_use_pmfft && pmfft_supported(m); }
 
+}  // extern "C"
+
+namespace pmb {
+bool pmfft_enabled() { return g_use_pmfft; }
+}  // namespace pmb
+
+extern "C" {
+
 int pmb_set_pmfft(int enabled) {
   g_use_pmfft = enabled != 0;
   return kOk;

@@ -52,6 +52,7 @@ struct EnsSim {
   float2* grad_hat;  // three gradient spectra
   float* force;      // three force meshes
   SpecTables t;
+  int pm;            // 1: the spectral stages run the hand-written pass chain
 };
 
 struct EnsDev {
@@ -194,6 +195,7 @@ __global__ void ens_green_kernel(EnsDev d) {
        jg += (int64_t)gridDim.x * blockDim.x) {
     const int s = find_sim(ss, d.nsims, jg);
     const EnsSim& sim = d.sims[s];
+    if (sim.pm) continue;  // multiplier fused into the member's FFT pass chain
     GreenParams g;
     g.green_kernel = 0;
     g.cell = 0.f;
@@ -254,6 +256,11 @@ struct Ensemble {
   uint32_t* tile_sums = nullptr;
   void* fft_work = nullptr;
   int64_t fft_bytes = 0;
+  // the hand-written FFT pass chain (power-of-two member meshes): one work
+  // area of five blocked spectral channels, reused member after member
+  void* pm_work = nullptr;
+  int64_t pm_bytes = 0;
+  bool any_cufft = false;
   float* rho = nullptr;
   float2* rho_hat = nullptr;
   float2* grad_hat = nullptr;
@@ -302,7 +309,7 @@ size_t scatter_smem_of(const Ensemble* e) {
 // Workspace: descriptors, prefix tables, factor table, step and work
 // counters, sorted records, row offsets, sort scratch, cuFFT work area.
 struct EnsLayout {
-  int64_t sims, pst, tst, sst, fac, step, work, rec, perm, offs, counts, row_of, rank_of, tsums, fft, total;
+  int64_t sims, pst, tst, sst, fac, step, work, rec, perm, offs, counts, row_of, rank_of, tsums, fft, pm, total;
 };
 
 EnsLayout layout(const Ensemble* e) {
@@ -329,6 +336,7 @@ EnsLayout layout(const Ensemble* e) {
   L.rank_of = take(4 * e->ntot);
   L.tsums = take(4 * scan_tmp_elems(e->rows + 1));
   L.fft = take(e->fft_bytes);
+  L.pm = take(e->pm_bytes);
   L.total = off;
   return L;
 }
@@ -395,15 +403,34 @@ int run_stage(Ensemble* e, int stage, int drift, int kick, cudaStream_t s) {
       break;
     }
     case kStR2C:
-      for (const EnsClass& c : e->classes)
-        ENS_TRY(fft_r2c(c.m, c.count, e->sims[c.first].rho, e->sims[c.first].rho_hat, e->fft_work, s));
+      // members on the pass chain run their whole spectral chain here (the
+      // same kernels as a single run's pmb_force); the others R2C by class
+      for (const EnsClass& c : e->classes) {
+        if (e->sims[c.first].pm) {
+          for (int i = c.first; i < c.first + c.count; ++i) {
+            const EnsSim& q = e->sims[i];
+            GreenParams g;
+            g.green_kernel = 0;
+            g.cell = 0.f;
+            g.transfer = nullptr;
+            g.radial = nullptr;
+            g.radial_len = 0;
+            g.post_scale = q.post;
+            ENS_TRY(pmfft_force(q.m, q.rho, q.force, (float2*)e->pm_work, q.t, g, s));
+          }
+        } else {
+          ENS_TRY(fft_r2c(c.m, c.count, e->sims[c.first].rho, e->sims[c.first].rho_hat, e->fft_work, s));
+        }
+      }
       break;
     case kStGreen:
-      if (e->nspec > 0) ens_green_kernel<<<grid_of(e, kStGreen, e->nspec), e->threads[kStGreen], 0, s>>>(d);
+      if (e->nspec > 0 && e->any_cufft)
+        ens_green_kernel<<<grid_of(e, kStGreen, e->nspec), e->threads[kStGreen], 0, s>>>(d);
       break;
     case kStC2R:
       for (const EnsClass& c : e->classes)
-        ENS_TRY(fft_c2r(c.m, 3 * c.count, e->sims[c.first].grad_hat, e->sims[c.first].force, e->fft_work, s));
+        if (!e->sims[c.first].pm)
+          ENS_TRY(fft_c2r(c.m, 3 * c.count, e->sims[c.first].grad_hat, e->sims[c.first].force, e->fft_work, s));
       break;
     case kStGather:
       if (e->ntot > 0) ens_gather_kernel<<<grid_of(e, kStGather, e->ntot), e->threads[kStGather], 0, s>>>(d, kick);
@@ -494,6 +521,13 @@ int pmb_ens_create(int nsims, const int64_t* counts, const int32_t* mesh_shapes,
   recount_tiles(e);
   int64_t fb = 0;
   for (const EnsClass& c : e->classes) {
+    if (pmfft_enabled() && pmfft_supported(c.m)) {
+      for (int i = c.first; i < c.first + c.count; ++i) e->sims[i].pm = 1;
+      const int64_t pb = 5 * 8 * pmfft_channel_elems(c.m);
+      e->pm_bytes = e->pm_bytes > pb ? e->pm_bytes : pb;
+      continue;
+    }
+    e->any_cufft = true;
     const int64_t w1 = fft_work_bytes(c.m, c.count), w3 = fft_work_bytes(c.m, 3 * c.count);
     if (w1 < 0 || w3 < 0) {
       delete e;
@@ -557,6 +591,7 @@ int pmb_ens_bind(void* handle, const int16_t* pmid, float* disp, float* vel, flo
   e->d_sims = (EnsSim*)(w + L.sims);
   e->tile_sums = (uint32_t*)(w + L.tsums);
   e->fft_work = w + L.fft;
+  e->pm_work = w + L.pm;
   EnsDev& d = e->dev;
   d.sims = e->d_sims;
   d.p_start = (const int64_t*)(w + L.pst);

@@ -63,5 +63,7 @@ int pmfft_force_adjoint(Mesh3 m, const float* mesh_cot, float* src_cot, float2* 
                         cudaStream_t s);
 int pmfft_timeouts(unsigned int* count);
 int pmfft_set_col_ctas(int ctas);
+// process-wide switch of pmb_set_pmfft (capi.cu)
+bool pmfft_enabled();
 
 }  // namespace pmb

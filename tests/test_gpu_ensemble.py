@@ -3,7 +3,8 @@
 With one member per mesh shape every batched FFT is a batch-1 plan, so an
 ensemble run must equal NBodyRun.forward of every member bit for bit; with
 several members per shape the batched cuFFT plans may round differently, so
-members agree within float32 round-off carried over a few steps.
+members agree within float32 round-off carried over a few steps.  Members on
+power-of-two meshes (the hand-written FFT pass chain) are bitwise in every case.
 """
 import numpy as np
 import pytest
@@ -80,3 +81,23 @@ def test_ensemble_initial_conditions_bitwise(graph):
     ref = pb.NBodyRun(confs[0], coss[0]).forward(
         pl.lpt(pm.linear_modes(pm.white_noise_nested(seeds[0], confs[0]), coss[0], confs[0]), coss[0], confs[0]))
     assert torch.equal(outs[0].disp, ref.disp)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_fft_chain_members_are_bitwise_single_runs(graph):
+    """Members on power-of-two meshes run the hand-written FFT pass chain one
+    after another (the same kernels as a single run), so even several members
+    of one mesh shape equal their single runs bit for bit."""
+    import pmpp_b200 as pb
+    from pmpp_b200 import _lib
+    from pmpp_b200.ensemble import Ensemble
+    confs, coss, ics = _members([(32, 4, 128.0, 0.3), (64, 2, 256.0, 0.28), (32, 4, 160.0, 0.31),
+                                 (16, 2, 64.0, 0.3)], nsteps=3)
+    assert _lib.pmfft_active(*confs[0].mesh_shape) and not _lib.pmfft_active(*confs[3].mesh_shape)
+    ens = Ensemble(confs, coss)
+    outs = ens.forward(ics, graph=graph)
+    for conf, cos, ic, out in zip(confs, coss, ics, outs):
+        ref = pb.NBodyRun(conf, cos).forward(ic)
+        for name in ("disp", "vel", "acc"):
+            assert torch.equal(getattr(out, name), getattr(ref, name)), name
+    assert _lib.pmfft_timeouts() == 0
