@@ -75,6 +75,10 @@ int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int 
  * vel != NULL also vel += out * kick (nbody/integrator.py:536). */
 int pmb_gather_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh, float* out,
                     float* vel, float kick, void* stream);
+/* pmb_gather_rows with a second half-kick vel += out * kick2 after the first
+ * (the next step's opening kick, same acceleration; kick2 = 0: none). */
+int pmb_gather_rows2(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh, float* out,
+                     float* vel, float kick, float kick2, void* stream);
 /* Position term of the CIC adjoints (cic/gather.py:495-502,
  * cic/scatter.py:366-373): disp_cot[p] (+)= sum_b (sum_c u[p,c] mesh_c[i_b])
  * grad w_b / cell; optional wsum[p,c] = sum_b mesh_c[i_b] w_b and
@@ -166,6 +170,12 @@ int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float dr
               float cell, float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
               const float* transfer, const float* radial, int radial_len, float* force_meshes, float* acc,
               float* vel_kick, float kick, void* workspace, int64_t workspace_bytes, void* stream);
+/* pmb_force with a second fused half-kick vel_kick += acc * kick2 after the
+ * first (the next KDK step's opening kick; kick2 = 0: none). */
+int pmb_force2(const int16_t* pmid, float* disp, const float* drift_vel, float drift, int64_t n, int nx, int ny, int nz,
+               float cell, float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
+               const float* transfer, const float* radial, int radial_len, float* force_meshes, float* acc,
+               float* vel_kick, float kick, float kick2, void* workspace, int64_t workspace_bytes, void* stream);
 /* Transpose of pmb_force w.r.t. disp given force_meshes at the same disp
  * (the force VJP of nbody/integrator.py:620-686): disp_cot (n,3) +=
  * gather-adjoint position term + scatter-adjoint term of the density. */

@@ -23,6 +23,7 @@ _SIGS = {
     "pmb_sort_by_cell_scratch_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
     "pmb_scatter_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_int, c_f, c_int, c_f, c_p, c_p, c_p]),
     "pmb_gather_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_f, c_p]),
+    "pmb_gather_rows2": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_f, c_f, c_p]),
     "pmb_interp_grad_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_p, c_f, c_f, c_int, c_p, c_p,
                                      c_p, c_p]),
     "pmb_wait_timeouts": (c_int, [c_p]),
@@ -44,6 +45,8 @@ _SIGS = {
     "pmb_force_workspace_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
     "pmb_force": (c_int, [c_p, c_p, c_p, c_f, c_i64, c_int, c_int, c_int, c_f, c_f, c_f, c_p, c_int, c_int, c_p, c_p,
                           c_int, c_p, c_p, c_p, c_f, c_p, c_i64, c_p]),
+    "pmb_force2": (c_int, [c_p, c_p, c_p, c_f, c_i64, c_int, c_int, c_int, c_f, c_f, c_f, c_p, c_int, c_int, c_p, c_p,
+                          c_int, c_p, c_p, c_p, c_f, c_f, c_p, c_i64, c_p]),
     "pmb_force_vjp_workspace_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
     "pmb_force_vjp": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_f, c_f, c_f, c_p, c_int, c_int, c_p, c_p, c_int,
                               c_p, c_p, c_p, c_p, c_i64, c_p]),
@@ -144,9 +147,10 @@ def check(status, what):
 
 # Hand-written kernels launched per entry point (cuFFT's own kernels excluded).
 _KERNELS = {
-    "pmb_sort_rows": 5, "pmb_gather_rows": 1, "pmb_interp_grad_rows": 1, "pmb_green_gradient": 1,
+    "pmb_sort_rows": 5, "pmb_gather_rows": 1, "pmb_gather_rows2": 1, "pmb_interp_grad_rows": 1, "pmb_green_gradient": 1,
     "pmb_green_gradient_adjoint": 1, "pmb_axpy": 1, "pmb_kick_adj": 1, "pmb_kick_adj2": 1, "pmb_drift_cot_adj": 1, "pmb_drift_adj": 1, "pmb_dot": 1,
-    "pmb_force": 9, "pmb_force_vjp": 11, "pmb_force_vjp_presorted": 6, "pmb_sum": 1, "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,
+    "pmb_force": 9, "pmb_force2": 9, "pmb_force_vjp": 11, "pmb_force_vjp_presorted": 6, "pmb_sum": 1,
+    "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,
     "pmb_lpt": 4, "pmb_lpt_vjp": 6, "pmb_pk_shells": 1, "pmb_shell_stats": 1, "pmb_pk_shells_adjoint": 1,
     "pmb_overdensity": 1, "pmb_ens_force": 7, "pmb_ens_step": 9, "pmb_ens_set_step": 1,
     "pmb_force64": 5, "pmb_deposit64": 1, "pmb_axpy64": 1, "pmb_sum64": 1, "pmb_white_noise_nested64": 1,
@@ -196,7 +200,7 @@ def call(name, *args):
     else:
         _launches[0] += _KERNELS.get(name, 0)
         # the hand-written FFT chain replaces the multiplier kernel by six passes
-        if name == "pmb_force" and pmfft_active(*args[5:8]):
+        if name in ("pmb_force", "pmb_force2") and pmfft_active(*args[5:8]):
             _launches[0] += 5
         elif name == "pmb_force_vjp" and pmfft_active(*args[3:6]):
             _launches[0] += 5

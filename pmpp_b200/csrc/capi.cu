@@ -133,13 +133,18 @@ int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int 
                         S(stream));
 }
 
-int pmb_gather_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh, float* out,
-                    float* vel, float kick, void* stream) {
+int pmb_gather_rows2(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh, float* out,
+                     float* vel, float kick, float kick2, void* stream) {
   Mesh3 m{nx, ny, nz};
   PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_gather_rows: unsupported mesh shape");
   PMB_REQUIRE(C >= 1 && C <= 4, "pmb_gather_rows: 1..4 channels supported");
   SortedView v = sorted_view((void*)sorted, n);
-  return gather_sorted(v.rec, v.perm, v.offs, n, m, C, mesh, out, vel, kick, S(stream));
+  return gather_sorted(v.rec, v.perm, v.offs, n, m, C, mesh, out, vel, kick, kick2, S(stream));
+}
+
+int pmb_gather_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh, float* out,
+                    float* vel, float kick, void* stream) {
+  return pmb_gather_rows2(sorted, n, nx, ny, nz, C, mesh, out, vel, kick, 0.f, stream);
 }
 
 int pmb_interp_grad_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh,
@@ -286,10 +291,10 @@ int64_t pmb_force_workspace_bytes(int64_t n, int nx, int ny, int nz) {
   return force_layout(n, Mesh3{nx, ny, nz}, nullptr, 0, &a, &b, &c, &s, &sh, &gh, &f);
 }
 
-int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float drift, int64_t n, int nx, int ny, int nz,
-              float cell, float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
-              const float* transfer, const float* radial, int radial_len, float* force_meshes, float* acc,
-              float* vel_kick, float kick, void* workspace, int64_t workspace_bytes, void* stream) {
+int pmb_force2(const int16_t* pmid, float* disp, const float* drift_vel, float drift, int64_t n, int nx, int ny, int nz,
+               float cell, float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
+               const float* transfer, const float* radial, int radial_len, float* force_meshes, float* acc,
+               float* vel_kick, float kick, float kick2, void* workspace, int64_t workspace_bytes, void* stream) {
   Mesh3 m{nx, ny, nz};
   PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_force: unsupported mesh shape");
   PMB_REQUIRE(n >= 0 && n < 4294967295ll, "pmb_force: particle count out of range");
@@ -317,7 +322,16 @@ int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float dr
     PMB_TRY(fft_c2r(m, 3, grad_hat, force_meshes, work, s));
   }
   SortedView v = sorted_view(sorted, n);
-  return gather_sorted(v.rec, v.perm, v.offs, n, m, 3, force_meshes, acc, vel_kick, kick, s);
+  return gather_sorted(v.rec, v.perm, v.offs, n, m, 3, force_meshes, acc, vel_kick, kick, kick2, s);
+}
+
+int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float drift, int64_t n, int nx, int ny, int nz,
+              float cell, float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
+              const float* transfer, const float* radial, int radial_len, float* force_meshes, float* acc,
+              float* vel_kick, float kick, void* workspace, int64_t workspace_bytes, void* stream) {
+  return pmb_force2(pmid, disp, drift_vel, drift, n, nx, ny, nz, cell, val_const, src_mul, tables, has_masks,
+                    green_kernel, transfer, radial, radial_len, force_meshes, acc, vel_kick, kick, 0.f, workspace,
+                    workspace_bytes, stream);
 }
 
 static int64_t force_vjp_layout(int64_t n, Mesh3 m, void* ws, int64_t cap, void** sorted, void** bins, void** scale16,

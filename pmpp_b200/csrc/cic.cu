@@ -325,15 +325,16 @@ int scatter_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, M
 // Gather and adjoint position terms
 // ---------------------------------------------------------------------------
 // out[src, c] = sum_b mesh_c[i_b] w_b (gather.py:452-472, pallas.py:305-318).
-// With kick != 0 the second half-kick vel += out * kick is applied in place
-// (integrator.py:536), saving a pass over the particles.
+// With vel the half-kick vel += out * kick is applied in place (integrator.py:536),
+// and with kick2 != 0 the next step's opening half-kick after it, saving passes
+// over the particles.
 template <int C>
 __global__ void gather_kernel(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm, int64_t n, Mesh3 m,
                               const float* __restrict__ mesh, float* __restrict__ out, float* __restrict__ vel,
-                              float kick) {
+                              float kick, float kick2) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  gather_one<C>(rec[i], perm[i], m, mesh, out, vel, kick);
+  gather_one<C>(rec[i], perm[i], m, mesh, out, vel, kick, kick2);
 }
 
 // ---------------------------------------------------------------------------
@@ -442,7 +443,7 @@ __global__ void __launch_bounds__(256) gather_staged_kernel(const Rec* __restric
                                                             const uint32_t* __restrict__ offs, Mesh3 m, int RX, int RY,
                                                             uint32_t min_stage, const float* __restrict__ mesh,
                                                             float* __restrict__ out, float* __restrict__ vel,
-                                                            float kick) {
+                                                            float kick, float kick2) {
   extern __shared__ __align__(16) float stage[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t seg_b[kStageMaxRX], seg_n[kStageMaxRX];
@@ -455,7 +456,7 @@ __global__ void __launch_bounds__(256) gather_staged_kernel(const Rec* __restric
     for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
       int k;
       const uint32_t i = tile_particle(j, seg_b, seg_n, &k);
-      gather_one<C>(rec[i], perm[i], m, mesh, out, vel, kick);
+      gather_one<C>(rec[i], perm[i], m, mesh, out, vel, kick, kick2);
     }
     return;
   }
@@ -483,7 +484,7 @@ __global__ void __launch_bounds__(256) gather_staged_kernel(const Rec* __restric
         a = __fadd_rn(a, __fmul_rn(v, __fmul_rn(__fmul_rn(wx[bx], wy[by]), wz[bz])));
       }
       out[(int64_t)src * C + c] = a;
-      if (vel != nullptr) vel[(int64_t)src * C + c] = __fadd_rn(vel[(int64_t)src * C + c], __fmul_rn(a, kick));
+      if (vel != nullptr) vel[(int64_t)src * C + c] = kicked(vel[(int64_t)src * C + c], a, kick, kick2);
     }
   }
 }
@@ -495,7 +496,8 @@ __global__ void __launch_bounds__(256) gather_staged_kernel(const Rec* __restric
 template <int C>
 __global__ void __launch_bounds__(256) gather_kernel_x2(const Rec* __restrict__ rec, const uint32_t* __restrict__ perm,
                                                         int64_t n, Mesh3 m, const float* __restrict__ mesh,
-                                                        float* __restrict__ out, float* __restrict__ vel, float kick) {
+                                                        float* __restrict__ out, float* __restrict__ vel, float kick,
+                                                        float kick2) {
   const int64_t i0 = (int64_t)blockIdx.x * (2 * blockDim.x) + threadIdx.x;
   const int64_t i1 = i0 + blockDim.x;
   if (i0 >= n) return;
@@ -523,16 +525,16 @@ __global__ void __launch_bounds__(256) gather_kernel_x2(const Rec* __restrict__ 
       a1 = __fadd_rn(a1, __fmul_rn(v1[b], k1.w[b]));
     }
     out[(int64_t)s0 * C + c] = a0;
-    if (vel != nullptr) vel[(int64_t)s0 * C + c] = __fadd_rn(vel[(int64_t)s0 * C + c], __fmul_rn(a0, kick));
+    if (vel != nullptr) vel[(int64_t)s0 * C + c] = kicked(vel[(int64_t)s0 * C + c], a0, kick, kick2);
     if (two) {
       out[(int64_t)s1 * C + c] = a1;
-      if (vel != nullptr) vel[(int64_t)s1 * C + c] = __fadd_rn(vel[(int64_t)s1 * C + c], __fmul_rn(a1, kick));
+      if (vel != nullptr) vel[(int64_t)s1 * C + c] = kicked(vel[(int64_t)s1 * C + c], a1, kick, kick2);
     }
   }
 }
 
 int gather_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, int64_t n, Mesh3 m, int C,
-                  const float* mesh, float* out, float* vel, float kick, cudaStream_t s) {
+                  const float* mesh, float* out, float* vel, float kick, float kick2, cudaStream_t s) {
   if (n == 0) return kOk;
   int RX, RY;
   if (offs != nullptr && stage_shape(m, C, mesh, &RX, &RY)) {
@@ -548,7 +550,7 @@ int gather_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, in
       attr_##CC = true;                                                                                        \
     }                                                                                                          \
     gather_staged_kernel<CC><<<grid, 256, (size_t)smem, s>>>(rec, perm, offs, m, RX, RY, min_stage, mesh, out, vel, \
-                                                              kick);                                            \
+                                                              kick, kick2);                                     \
   } while (0)
     switch (C) {
       case 1: PMB_LAUNCH_GS(1); break;
@@ -564,15 +566,16 @@ int gather_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, in
   const int th = 256;
   const unsigned g = (unsigned)((n + th - 1) / th);
   if (C == 3) {
-    gather_kernel_x2<3><<<(unsigned)((n + 2 * th - 1) / (2 * th)), th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick);
+    gather_kernel_x2<3><<<(unsigned)((n + 2 * th - 1) / (2 * th)), th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick,
+                                                                              kick2);
     PMB_CUDA_CHECK(cudaGetLastError());
     return kOk;
   }
   switch (C) {
-    case 1: gather_kernel<1><<<g, th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick); break;
-    case 2: gather_kernel<2><<<g, th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick); break;
-    case 3: gather_kernel<3><<<g, th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick); break;
-    case 4: gather_kernel<4><<<g, th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick); break;
+    case 1: gather_kernel<1><<<g, th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick, kick2); break;
+    case 2: gather_kernel<2><<<g, th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick, kick2); break;
+    case 3: gather_kernel<3><<<g, th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick, kick2); break;
+    case 4: gather_kernel<4><<<g, th, 0, s>>>(rec, perm, n, m, mesh, out, vel, kick, kick2); break;
     default: return kUnsupported;
   }
   PMB_CUDA_CHECK(cudaGetLastError());

@@ -221,9 +221,18 @@ __device__ __forceinline__ void corners_of(const Rec& r, Mesh3 m, Corners& k) {
 
 // out[src, c] = sum_b mesh_c[i_b] w_b for one sorted record; with vel the
 // half-kick vel += out * kick is applied in place (integrator.py:536).
+// vel + a k1 (+ a k2): one or two half-kicks with the same acceleration, in
+// order, each with two roundings as the separate update would (k2 == 0: none).
+__device__ __forceinline__ float kicked(float v, float a, float k1, float k2) {
+  v = __fadd_rn(v, __fmul_rn(a, k1));
+  if (k2 != 0.f) v = __fadd_rn(v, __fmul_rn(a, k2));
+  return v;
+}
+
 template <int C>
 __device__ __forceinline__ void gather_one(const Rec& r, uint32_t src, Mesh3 m, const float* __restrict__ mesh,
-                                           float* __restrict__ out, float* __restrict__ vel, float kick) {
+                                           float* __restrict__ out, float* __restrict__ vel, float kick,
+                                           float kick2 = 0.f) {
   Corners k;
   corners_of(r, m, k);
   const int64_t cells = m.cells();
@@ -234,7 +243,7 @@ __device__ __forceinline__ void gather_one(const Rec& r, uint32_t src, Mesh3 m, 
 #pragma unroll
     for (int b = 0; b < 8; ++b) a = __fadd_rn(a, __fmul_rn(__ldg(mc + k.idx[b]), k.w[b]));
     out[(int64_t)src * C + c] = a;
-    if (vel != nullptr) vel[(int64_t)src * C + c] = __fadd_rn(vel[(int64_t)src * C + c], __fmul_rn(a, kick));
+    if (vel != nullptr) vel[(int64_t)src * C + c] = kicked(vel[(int64_t)src * C + c], a, kick, kick2);
   }
 }
 

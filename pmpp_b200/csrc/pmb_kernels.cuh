@@ -20,7 +20,7 @@ int scatter_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, M
                    cudaStream_t s);
 // offs (row offsets, may be null) enables the staged kernels.
 int gather_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, int64_t n, Mesh3 m, int C,
-                  const float* mesh, float* out, float* vel, float kick, cudaStream_t s);
+                  const float* mesh, float* out, float* vel, float kick, float kick2, cudaStream_t s);
 int interp_grad_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, int64_t n, Mesh3 m, int C,
                        const float* mesh, const float* u, float u_const, float cell, int accumulate, float* disp_cot,
                        float* wsum, float* u_sorted, cudaStream_t s);

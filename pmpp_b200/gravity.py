@@ -66,7 +66,7 @@ class _NoTimer:
 
 
 def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc, drift_vel, drift, vel_kick,
-                  kick, timer, src_hat_out=None, lane=""):
+                  kick, timer, src_hat_out=None, lane="", kick2=0.0):
     """pmb_force as separate stage calls with a CUDA event after each stage.
 
     With src_hat_out (complex64, half spectrum) the rFFT of the Poisson source
@@ -114,8 +114,8 @@ def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F
         t = timer.mark("green_gradient", t)
         call("pmb_irfft3", nx, ny, nz, 3, spec3.data_ptr(), F.data_ptr(), work.data_ptr(), s)
         t = timer.mark("fft_c2r", t)
-    call("pmb_gather_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc.data_ptr(), ptr(vel_kick),
-         float(kick), s)
+    call("pmb_gather_rows2", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc.data_ptr(), ptr(vel_kick),
+         float(kick), float(kick2), s)
     timer.mark("gather", t)
 
 
@@ -192,13 +192,14 @@ def _correction_args(correction, a, cosmo, conf):
 
 
 def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, force_meshes=None, acc=None,
-          drift_vel=None, drift=0.0, vel_kick=None, kick=0.0, src_hat_out=None, lane=""):
+          drift_vel=None, drift=0.0, vel_kick=None, kick=0.0, kick2=0.0, src_hat_out=None, lane=""):
     """One PM force evaluation on device tensors.
 
     Returns (acc (N,3), force_meshes (3,Mx,My,Mz)).  With drift_vel the
     particles are drifted first (disp updated in place); with vel_kick the
-    half-kick vel_kick += acc * kick is fused into the gather.  lane selects
-    the workspace that keeps the sorted records (see force_vjp)."""
+    half-kick vel_kick += acc * kick is fused into the gather, followed by
+    vel_kick += acc * kick2 when kick2 != 0 (the next step's opening kick).
+    lane selects the workspace that keeps the sorted records (see force_vjp)."""
     require_cuda(pmid, disp, drift_vel, vel_kick)
     n = pmid.shape[0]
     nx, ny, nz = conf.mesh_shape
@@ -211,16 +212,16 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
     tables = conf.spectral_tables("mesh", dev, gk)
     if StageTimer.active is not None or src_hat_out is not None:
         _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc, drift_vel,
-                      drift, vel_kick, kick, StageTimer.active, src_hat_out, lane)
+                      drift, vel_kick, kick, StageTimer.active, src_hat_out, lane, kick2)
         return acc, force_meshes
     wb = lib().pmb_force_workspace_bytes(n, nx, ny, nz)
     if wb < 0:
         raise RuntimeError("pmb_force_workspace_bytes failed: " + lib().pmb_last_error().decode())
     ws = workspace(wb, dev, "force" + _lane_suffix(lane))
-    call("pmb_force", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
+    call("pmb_force2", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
          float(conf.cell_size), float(conf.mesh_size / conf.ptcl_num), 1.5 * _om32(omega_m), tables.data_ptr(),
          int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, force_meshes.data_ptr(),
-         acc.data_ptr(), ptr(vel_kick), float(kick), ws.data_ptr(), ws.numel(), stream_handle(dev))
+         acc.data_ptr(), ptr(vel_kick), float(kick), float(kick2), ws.data_ptr(), ws.numel(), stream_handle(dev))
     return acc, force_meshes
 
 

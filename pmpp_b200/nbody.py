@@ -110,28 +110,36 @@ class NBodyRun:
         F = torch.empty((3, ) + conf.mesh_shape, dtype=torch.float32, device=disp.device)
         s = stream_handle(disp.device)
         S = self._src_hat_buffer(disp.device)
-        force(ptcl.pmid, disp, conf, cosmo.Omega_m, a=float(a[0]), cosmo=cosmo, correction=self.correction,
-              force_meshes=F, acc=acc, src_hat_out=S)
+        # stage list of the whole run; every force evaluation takes the kicks
+        # that directly follow it (a step's closing kick and the next step's
+        # opening kick share its acceleration) into its gather
+        ops = [("init", )]
         for a_prev, a_next in zip(a[:-1], a[1:]):
-            stages = _schedule(a_prev, a_next, conf)
-            i = 0
-            while i < len(stages):
-                st = stages[i]
-                if st[0] == "kick":
-                    call("pmb_axpy", vel.data_ptr(), acc.data_ptr(), vel.numel(),
-                         _f32(cosmo.kick_factor(st[1], st[2], st[3])), s)
-                    i += 1
-                    continue
-                D = _f32(cosmo.drift_factor(st[1], st[2], st[3]))
-                # fuse a directly following kick into the gather
-                kick_f, vk = 0.0, None
-                if i + 1 < len(stages) and stages[i + 1][0] == "kick":
-                    kst = stages[i + 1]
-                    kick_f, vk = _f32(cosmo.kick_factor(kst[1], kst[2], kst[3])), vel
-                    i += 1
-                force(ptcl.pmid, disp, conf, cosmo.Omega_m, a=float(st[3]), cosmo=cosmo, correction=self.correction,
-                      force_meshes=F, acc=acc, drift_vel=vel, drift=D, vel_kick=vk, kick=kick_f, src_hat_out=S)
+            ops.extend(_schedule(a_prev, a_next, conf))
+        i = 0
+        while i < len(ops):
+            st = ops[i]
+            if st[0] == "kick":  # a kick with no force evaluation before it
+                call("pmb_axpy", vel.data_ptr(), acc.data_ptr(), vel.numel(),
+                     _f32(cosmo.kick_factor(st[1], st[2], st[3])), s)
                 i += 1
+                continue
+            ks = []
+            while i + 1 + len(ks) < len(ops) and ops[i + 1 + len(ks)][0] == "kick" and len(ks) < 2:
+                k = ops[i + 1 + len(ks)]
+                ks.append(_f32(cosmo.kick_factor(k[1], k[2], k[3])))
+            kick_f = ks[0] if ks else 0.0
+            kick2 = ks[1] if len(ks) == 2 else 0.0
+            vk = vel if ks else None
+            if st[0] == "init":
+                force(ptcl.pmid, disp, conf, cosmo.Omega_m, a=float(a[0]), cosmo=cosmo, correction=self.correction,
+                      force_meshes=F, acc=acc, vel_kick=vk, kick=kick_f, kick2=kick2, src_hat_out=S)
+            else:
+                D = _f32(cosmo.drift_factor(st[1], st[2], st[3]))
+                force(ptcl.pmid, disp, conf, cosmo.Omega_m, a=float(st[3]), cosmo=cosmo, correction=self.correction,
+                      force_meshes=F, acc=acc, drift_vel=vel, drift=D, vel_kick=vk, kick=kick_f, kick2=kick2,
+                      src_hat_out=S)
+            i += 1 + len(ks)
         self.final_meshes = F
         self.final_src_hat = S
         return ptcl.replace(disp=disp, vel=vel, acc=acc)
