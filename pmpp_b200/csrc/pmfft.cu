@@ -189,7 +189,6 @@ __host__ __device__ constexpr bool is_y(int mode) { return mode <= kYFwdYZ; }
 __host__ __device__ constexpr int n_in(int mode) {
   return (mode == kYFwdYZ || mode == kXGreenAdj || mode == kXFwdAdjK) ? 2 : 1;
 }
-__host__ __device__ constexpr int n_out(int mode) { return (mode == kYInvYZ || mode == kXGreen) ? 2 : 1; }
 
 // floats of per-axis tables a column pass keeps in shared memory
 __host__ __device__ constexpr int col_table_floats(int mode, int L) {
@@ -338,7 +337,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
   // forward or inverse transform of the tile in stage slot i; afterwards the
   // job (k1 = q, c) holds u[k2] = X[k1 + R1 k2].  Leaves the stage free to
   // reuse as scratch (not yet released).
-  auto transform = [&](int i, float2 (&u)[R2], auto inv_tag, float ymul_c, bool ymul) {
+  auto transform = [&](int i, float2 (&u)[R2], auto inv_tag) {
     constexpr bool INV = decltype(inv_tag)::value;
     float2* buf = smem + (i % S) * G::BUF;
     float2 v[R1];
@@ -350,8 +349,6 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
     if (ja) four_step_a<R1, R2, INV>(v, buf, q, c, stw);
     __syncthreads();
     if (jb) four_step_b<R1, R2, INV>(u, buf, q, c);
-    (void)ymul_c;
-    (void)ymul;
   };
 
   // inverse transform of values held as u[k2] at index k1 + R1 k2 (k1 = q),
@@ -372,7 +369,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
     if (!acquire(i0)) return;
     if constexpr (MODE == kYFwd || MODE == kYInv || MODE == kXFwd || MODE == kXInv) {
       constexpr bool INV = (MODE == kYInv || MODE == kXInv);
-      transform(i0, u, std::integral_constant<bool, INV>{}, 0.f, false);
+      transform(i0, u, std::integral_constant<bool, INV>{});
       const int64_t ob = (int64_t)batch * a.ch;
       if (jb) {
 #pragma unroll
@@ -427,14 +424,14 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
         const bool kv = kz_valid(kz, a.nz);
         const float cz = kv ? a.t.cz[kz] : 0.f;
         float2 acc[R2];
-        transform(i0, u, std::false_type{}, 0.f, false);
+        transform(i0, u, std::false_type{});
         if (jb) {
   #pragma unroll
           for (int k2 = 0; k2 < R2; ++k2) acc[k2] = i_times(-tab[q + R1 * k2], u[k2]);
         }
         release(i0);
         if (!acquire(i0 + 1)) return;
-        transform(i0 + 1, u, std::false_type{}, 0.f, false);
+        transform(i0 + 1, u, std::false_type{});
         if (jb) {
   #pragma unroll
           for (int k2 = 0; k2 < R2; ++k2) {
@@ -529,7 +526,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
       // the transfer tables cover kz <= nz/2 only: never read on padding columns
       const bool has_t = kv && (a.g.transfer != nullptr || a.g.radial != nullptr);
       float2* buf = smem + (i0 % S) * G::BUF;
-      transform(i0, u, std::false_type{}, 0.f, false);
+      transform(i0, u, std::false_type{});
       float2 w[R2];
       auto multiply = [&](auto ht) {
 #pragma unroll
@@ -574,7 +571,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
       // the transfer tables cover kz <= nz/2 only: never read on padding columns
       const bool has_t = kv && (a.g.transfer != nullptr || a.g.radial != nullptr);
       float2 acc[R2];
-      transform(i0, u, std::false_type{}, 0.f, false);
+      transform(i0, u, std::false_type{});
       if (jb) {
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) acc[k2] = i_times(-tab[L + q + R1 * k2], u[k2]);
@@ -582,7 +579,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
       release(i0);
       if (!acquire(i0 + 1)) return;
       float2* buf = smem + ((i0 + 1) % S) * G::BUF;
-      transform(i0 + 1, u, std::false_type{}, 0.f, false);
+      transform(i0 + 1, u, std::false_type{});
       auto multiply = [&](auto ht) {
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) {
@@ -639,7 +636,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
           __syncthreads();
           four_step_b<R1, R2, false>(u, buf, q, c);
         } else {
-          transform(i0 + ph, u, std::false_type{}, 0.f, false);
+          transform(i0 + ph, u, std::false_type{});
         }
         if (jb) {
           if (ph == 0) {
