@@ -45,7 +45,6 @@
 #include <map>
 #include <mutex>
 #include <type_traits>
-#include <vector>
 
 #include "pmb_common.cuh"
 #include "pmb_kernels.cuh"
@@ -60,8 +59,36 @@ constexpr int KT = 8;   // columns per column tile
 constexpr int BY = 32;  // y rows per block of the spectral layout
 constexpr int KR = 16;  // rows per z-pass tile
 
-__constant__ float2 c_w32[32];  // exp(-2 pi i k / 32)
 __device__ unsigned int g_fft_timeouts;
+
+// exp(-2 pi i k / 32) for k < 16, the float nearest to cos / sin of k pi / 16
+// (k = 4 and 8 are never read: those butterflies are handled exactly).
+__device__ __forceinline__ float2 w32(int k) {
+  constexpr float re[16] = {1.0f,         0.98078525f,  0.9238795f,   0.8314696f,   0.70710677f,  0.55557024f,
+                            0.38268343f,  0.19509032f,  0.0f,         -0.19509032f, -0.38268343f, -0.55557024f,
+                            -0.70710677f, -0.8314696f,  -0.9238795f,  -0.98078525f};
+  constexpr float im[16] = {-0.0f,        -0.19509032f, -0.38268343f, -0.55557024f, -0.70710677f, -0.8314696f,
+                            -0.9238795f,  -0.98078525f, -1.0f,        -0.98078525f, -0.9238795f,  -0.8314696f,
+                            -0.70710677f, -0.55557024f, -0.38268343f, -0.19509032f};
+  return make_float2(re[k], im[k]);
+}
+
+// Twiddle tables W_L^k (k < L) of every L = 32 .. 2048, table L at offset
+// L - 32, in a static device array filled once per device by
+// twiddle_init_kernel on the caller's stream (no allocation, no host sync).
+constexpr int kTwTotal = 2048 * 2 - 32;
+__device__ float2 g_twiddles[kTwTotal];
+
+__global__ void twiddle_init_kernel() {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kTwTotal; i += gridDim.x * blockDim.x) {
+    int L = 32;
+    while (i >= 2 * L - 32) L *= 2;  // table L covers [L - 32, 2 L - 32)
+    const int k = i - (L - 32);
+    double sn, cs;
+    sincospi(-2.0 * (double)k / (double)L, &sn, &cs);
+    g_twiddles[i] = make_float2((float)cs, (float)sn);
+  }
+}
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -102,7 +129,7 @@ __device__ __forceinline__ void dft_stage(float2 (&v)[R]) {
       } else if (4 * k == LEN) {
         b = INV ? make_float2(-b.y, b.x) : make_float2(b.y, -b.x);
       } else {
-        float2 w = c_w32[k * (32 / LEN)];
+        float2 w = w32(k * (32 / LEN));
         if (INV) w.y = -w.y;
         b = cmul(b, w);
       }
@@ -910,60 +937,42 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// Per-device twiddle tables W_L^k (k < L) for L = 32 .. 2048 and the
-// constant-memory W_32 table.  Built outside stream capture (the first call
-// per device and length allocates).
-struct TwiddleCache {
+// Pointer to the twiddle table of length L on the current device; the first
+// call per device enqueues the table fill on stream s (which must not be
+// capturing: run one call outside a graph capture first).
+struct TwiddleState {
   std::mutex mu;
-  std::map<std::pair<int, int>, float2*> tables;
-  std::map<int, bool> consts;
+  std::map<int, float2*> base;  // device -> g_twiddles
 };
-TwiddleCache& twiddles() {
-  static TwiddleCache* c = new TwiddleCache();
-  return *c;
-}
-
-std::vector<float2> twiddle_host(int L) {
-  std::vector<float2> h(L);
-  for (int k = 0; k < L; ++k) {
-    const double ang = -2.0 * M_PI * (double)k / (double)L;
-    h[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
-  }
-  return h;
+TwiddleState& twiddles() {
+  static TwiddleState* t = new TwiddleState();
+  return *t;
 }
 
 int twiddle_table(int L, cudaStream_t s, const float2** out) {
+  if (L < 32 || L > 2048 || (L & (L - 1)) != 0) {
+    set_last_error("pmfft: unsupported twiddle table length");
+    return kUnsupported;
+  }
   int dev = 0;
   PMB_CUDA_CHECK(cudaGetDevice(&dev));
-  TwiddleCache& c = twiddles();
-  std::lock_guard<std::mutex> lock(c.mu);
-  if (!c.consts[dev]) {
+  TwiddleState& t = twiddles();
+  std::lock_guard<std::mutex> lock(t.mu);
+  auto it = t.base.find(dev);
+  if (it == t.base.end()) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     PMB_CUDA_CHECK(cudaStreamIsCapturing(s, &cs));
     if (cs != cudaStreamCaptureStatusNone) {
-      set_last_error("pmfft: first use of a mesh size inside stream capture; run once before capturing");
+      set_last_error("pmfft: first use on this device inside stream capture; run once before capturing");
       return kInvalidArgument;
     }
-    const std::vector<float2> w = twiddle_host(32);
-    PMB_CUDA_CHECK(cudaMemcpyToSymbol(c_w32, w.data(), 32 * sizeof(float2)));
-    c.consts[dev] = true;
+    void* p = nullptr;
+    PMB_CUDA_CHECK(cudaGetSymbolAddress(&p, g_twiddles));
+    twiddle_init_kernel<<<(kTwTotal + 255) / 256, 256, 0, s>>>();
+    PMB_CUDA_CHECK(cudaGetLastError());
+    it = t.base.emplace(dev, (float2*)p).first;
   }
-  auto key = std::make_pair(dev, L);
-  auto it = c.tables.find(key);
-  if (it == c.tables.end()) {
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    PMB_CUDA_CHECK(cudaStreamIsCapturing(s, &cs));
-    if (cs != cudaStreamCaptureStatusNone) {
-      set_last_error("pmfft: first use of a mesh size inside stream capture; run once before capturing");
-      return kInvalidArgument;
-    }
-    float2* d = nullptr;
-    PMB_CUDA_CHECK(cudaMalloc(&d, L * sizeof(float2)));
-    const std::vector<float2> h = twiddle_host(L);
-    PMB_CUDA_CHECK(cudaMemcpy(d, h.data(), L * sizeof(float2), cudaMemcpyHostToDevice));
-    it = c.tables.emplace(key, d).first;
-  }
-  *out = it->second;
+  *out = it->second + (L - 32);
   return kOk;
 }
 
