@@ -73,22 +73,58 @@ __device__ __forceinline__ float2 w32(int k) {
   return make_float2(re[k], im[k]);
 }
 
-// Twiddle tables W_L^k (k < L) of every L = 32 .. 2048, table L at offset
-// L - 32, in a static device array filled once per device by
-// twiddle_init_kernel on the caller's stream (no allocation, no host sync).
+// Twiddle tables W_L^k = exp(-2 pi i k / L) (k < L) of every L = 32 .. 2048,
+// table L at offset L - 32, evaluated at compile time into a constant device
+// array (no fill at run time, so no first-use ordering between streams).
+// Each entry: the quadrant j = floor(4k / L) and the remainder are exact
+// integers, the remainder is folded to an angle b in [0, pi/4], and sin b /
+// cos b come from their Taylor series in double (13 terms; the first omitted
+// term is below 1e-28), then rounded once to float.  Exact zeros carry the
+// signs of sinpi / cospi of -2k/L: sine -0, cosine +0.
 constexpr int kTwTotal = 2048 * 2 - 32;
-__device__ float2 g_twiddles[kTwTotal];
 
-__global__ void twiddle_init_kernel() {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kTwTotal; i += gridDim.x * blockDim.x) {
-    int L = 32;
-    while (i >= 2 * L - 32) L *= 2;  // table L covers [L - 32, 2 L - 32)
-    const int k = i - (L - 32);
-    double sn, cs;
-    sincospi(-2.0 * (double)k / (double)L, &sn, &cs);
-    g_twiddles[i] = make_float2((float)cs, (float)sn);
+struct TwiddleTable {
+  float2 v[kTwTotal];
+};
+
+struct SinCos {
+  double s, c;
+};
+
+constexpr SinCos sincos_taylor(double b) {
+  const double b2 = b * b;
+  double ts = b, s = b, tc = 1.0, c = 1.0;
+  for (int k = 1; k <= 12; ++k) {
+    ts *= -b2 / ((2.0 * k) * (2.0 * k + 1.0));
+    tc *= -b2 / ((2.0 * k - 1.0) * (2.0 * k));
+    s += ts;
+    c += tc;
   }
+  return SinCos{s, c};
 }
+
+constexpr float2 twiddle_entry(int k, int L) {
+  constexpr double kPi = 3.14159265358979323846264338327950288;
+  const int j = (4 * k) / L;
+  int r = 4 * k - j * L;  // angle 2 pi k / L = (pi / 2) (j + r / L)
+  const bool swap = 2 * r > L;
+  if (swap) r = L - r;
+  const SinCos t = sincos_taylor(0.5 * kPi * (double)r / (double)L);
+  const double sb = swap ? t.c : t.s, cb = swap ? t.s : t.c;
+  const double s = j == 0 ? sb : j == 1 ? cb : j == 2 ? -sb : -cb;
+  const double c = j == 0 ? cb : j == 1 ? -sb : j == 2 ? -cb : sb;
+  return float2{c == 0.0 ? 0.0f : (float)c, s == 0.0 ? -0.0f : (float)-s};
+}
+
+constexpr TwiddleTable make_twiddles() {
+  TwiddleTable t{};
+  int i = 0;
+  for (int L = 32; L <= 2048; L *= 2)
+    for (int k = 0; k < L; ++k) t.v[i++] = twiddle_entry(k, L);
+  return t;
+}
+
+__device__ const TwiddleTable g_twiddles = make_twiddles();
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -937,19 +973,17 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// Pointer to the twiddle table of length L on the current device; the first
-// call per device enqueues the table fill on stream s (which must not be
-// capturing: run one call outside a graph capture first).
+// Pointer to the twiddle table of length L on the current device.
 struct TwiddleState {
   std::mutex mu;
-  std::map<int, float2*> base;  // device -> g_twiddles
+  std::map<int, const float2*> base;  // device -> g_twiddles
 };
 TwiddleState& twiddles() {
   static TwiddleState* t = new TwiddleState();
   return *t;
 }
 
-int twiddle_table(int L, cudaStream_t s, const float2** out) {
+int twiddle_table(int L, const float2** out) {
   if (L < 32 || L > 2048 || (L & (L - 1)) != 0) {
     set_last_error("pmfft: unsupported twiddle table length");
     return kUnsupported;
@@ -960,17 +994,9 @@ int twiddle_table(int L, cudaStream_t s, const float2** out) {
   std::lock_guard<std::mutex> lock(t.mu);
   auto it = t.base.find(dev);
   if (it == t.base.end()) {
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    PMB_CUDA_CHECK(cudaStreamIsCapturing(s, &cs));
-    if (cs != cudaStreamCaptureStatusNone) {
-      set_last_error("pmfft: first use on this device inside stream capture; run once before capturing");
-      return kInvalidArgument;
-    }
     void* p = nullptr;
     PMB_CUDA_CHECK(cudaGetSymbolAddress(&p, g_twiddles));
-    twiddle_init_kernel<<<(kTwTotal + 255) / 256, 256, 0, s>>>();
-    PMB_CUDA_CHECK(cudaGetLastError());
-    it = t.base.emplace(dev, (float2*)p).first;
+    it = t.base.emplace(dev, reinterpret_cast<const float2*>(p)).first;
   }
   *out = it->second + (L - 32);
   return kOk;
@@ -1108,9 +1134,9 @@ int pmfft_z(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in
   a.nz = m.nz;
   a.tiles_per_ch = (int)(m.rows() / KR);
   a.ntiles = a.tiles_per_ch * batch;
-  int st = twiddle_table(M, s, &a.tw_m);
+  int st = twiddle_table(M, &a.tw_m);
   if (st != kOk) return st;
-  st = twiddle_table(m.nz, s, &a.tw_n);
+  st = twiddle_table(m.nz, &a.tw_n);
   if (st != kOk) return st;
   return inverse ? launch_z_len<true>(M, a, s) : launch_z_len<false>(M, a, s);
 }
@@ -1163,7 +1189,7 @@ int pmfft_col(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float
     return kUnsupported;
   }
   a.ntiles = (int)ntiles;
-  st = twiddle_table(L, s, &a.tw);
+  st = twiddle_table(L, &a.tw);
   if (st != kOk) return st;
   switch (mode) {
     case kYFwd: return launch_col_len<kYFwd>(L, map, a, s);
