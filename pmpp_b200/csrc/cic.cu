@@ -300,12 +300,7 @@ int scatter_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, M
   const unsigned grid = (unsigned)((int64_t)nbx * nby);
 #define PMB_LAUNCH_SCATTER(CC)                                                                                   \
   do {                                                                                                           \
-    static bool attr_##CC = false;                                                                               \
-    if (!attr_##CC) {                                                                                            \
-      PMB_CUDA_CHECK(cudaFuncSetAttribute(scatter_pull_kernel<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                          200 * 1024));                                                         \
-      attr_##CC = true;                                                                                          \
-    }                                                                                                            \
+    PMB_CUDA_CHECK(smem_optin((const void*)scatter_pull_kernel<CC>, 200 * 1024));                              \
     scatter_pull_kernel<CC><<<grid, 256, (size_t)smem, s>>>(rec, perm, offs, m, RX, RY, val, val_sorted,         \
                                                              val_const, scale_dev, mode, src_mul, out);         \
   } while (0)
@@ -543,12 +538,7 @@ int gather_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, in
     const unsigned grid = (unsigned)((int64_t)((m.nx + RX - 1) / RX) * ((m.ny + RY - 1) / RY));
 #define PMB_LAUNCH_GS(CC)                                                                                      \
   do {                                                                                                         \
-    static bool attr_##CC = false;                                                                             \
-    if (!attr_##CC) {                                                                                          \
-      PMB_CUDA_CHECK(cudaFuncSetAttribute(gather_staged_kernel<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                          (int)kStageBudget));                                                \
-      attr_##CC = true;                                                                                        \
-    }                                                                                                          \
+    PMB_CUDA_CHECK(smem_optin((const void*)gather_staged_kernel<CC>, (int)kStageBudget));                     \
     gather_staged_kernel<CC><<<grid, 256, (size_t)smem, s>>>(rec, perm, offs, m, RX, RY, min_stage, mesh, out, vel, \
                                                               kick, kick2);                                     \
   } while (0)
@@ -764,12 +754,7 @@ int interp_grad_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* off
     const unsigned grid = (unsigned)((int64_t)((m.nx + RX - 1) / RX) * ((m.ny + RY - 1) / RY));
 #define PMB_LAUNCH_IS(CC)                                                                                       \
   do {                                                                                                          \
-    static bool attr_##CC = false;                                                                              \
-    if (!attr_##CC) {                                                                                           \
-      PMB_CUDA_CHECK(cudaFuncSetAttribute(interp_grad_staged_kernel<CC>,                                        \
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBudget));     \
-      attr_##CC = true;                                                                                         \
-    }                                                                                                           \
+    PMB_CUDA_CHECK(smem_optin((const void*)interp_grad_staged_kernel<CC>, (int)kStageBudget));                 \
     interp_grad_staged_kernel<CC><<<grid, 256, (size_t)smem, s>>>(rec, perm, offs, m, RX, RY, min_stage, mesh, u, \
                                                                    u_const, cell, accumulate, disp_cot, wsum,   \
                                                                    u_sorted);                                   \

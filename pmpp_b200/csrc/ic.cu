@@ -576,12 +576,7 @@ int pk_shells(const float2* spec, Mesh3 m, const float* sinc_tab, int mas_power,
   const int nsh = spec_b != nullptr ? 3 * num_shells : num_shells;
   const size_t smem = sizeof(double) * nsh;
   if (smem > 200 * 1024) return kUnsupported;
-  static bool attr = false;
-  if (!attr) {
-    PMB_CUDA_CHECK(cudaFuncSetAttribute(pk_shells_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        200 * 1024));
-    attr = true;
-  }
+  PMB_CUDA_CHECK(smem_optin((const void*)pk_shells_kernel<float>, 200 * 1024));
   int64_t b = (m.half_cells() + 255) / 256;
   if (b > 148 * 8) b = 148 * 8;
   pk_shells_kernel<float><<<(unsigned)(b > 0 ? b : 1), 256, smem, s>>>(spec, m, sinc_tab, mas_power, num_shells, sums,
@@ -594,12 +589,7 @@ int pk_shells64(const double2* spec, Mesh3 m, const double* sinc_tab, int mas_po
                 cudaStream_t s) {
   const size_t smem = sizeof(double) * num_shells;
   if (smem > 200 * 1024) return kUnsupported;
-  static bool attr = false;
-  if (!attr) {
-    PMB_CUDA_CHECK(cudaFuncSetAttribute(pk_shells_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        200 * 1024));
-    attr = true;
-  }
+  PMB_CUDA_CHECK(smem_optin((const void*)pk_shells_kernel<double>, 200 * 1024));
   int64_t b = (m.half_cells() + 255) / 256;
   if (b > 148 * 8) b = 148 * 8;
   pk_shells_kernel<double><<<(unsigned)(b > 0 ? b : 1), 256, smem, s>>>(spec, m, sinc_tab, mas_power, num_shells,
@@ -672,11 +662,7 @@ __global__ void shell_stats_kernel(Mesh3 m, int num_shells, double* __restrict__
 int shell_stats(Mesh3 m, int num_shells, double* counts, double* ksum, cudaStream_t s) {
   const size_t smem = sizeof(double) * 2 * num_shells;
   if (smem > 200 * 1024) return kUnsupported;
-  static bool attr = false;
-  if (!attr) {
-    PMB_CUDA_CHECK(cudaFuncSetAttribute(shell_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr = true;
-  }
+  PMB_CUDA_CHECK(smem_optin((const void*)shell_stats_kernel, 200 * 1024));
   int64_t b = (m.half_cells() + 255) / 256;
   if (b > 148 * 8) b = 148 * 8;
   shell_stats_kernel<<<(unsigned)(b > 0 ? b : 1), 256, smem, s>>>(m, num_shells, counts, ksum);

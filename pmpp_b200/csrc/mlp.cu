@@ -338,12 +338,7 @@ int mlp_table(const void* w, const float* b, MlpCond c, int len, float* table, c
 int mlp_backward(const void* w, const float* b, MlpCond c, int len, const double* tcot, float* grad, cudaStream_t s) {
   int blocks = (len + kTile - 1) / kTile;
   if (blocks > 148 * 2) blocks = 148 * 2;
-  static bool attr = false;
-  if (!attr) {
-    PMB_CUDA_CHECK(cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)sizeof(BackSmem)));
-    attr = true;
-  }
+  PMB_CUDA_CHECK(smem_optin((const void*)mlp_backward_kernel, (int)sizeof(BackSmem)));
   mlp_backward_kernel<<<blocks > 0 ? blocks : 1, 128, sizeof(BackSmem), s>>>((const __nv_bfloat16*)w, b, c, len, tcot,
                                                                             grad);
   PMB_CUDA_CHECK(cudaGetLastError());
@@ -353,11 +348,7 @@ int mlp_backward(const void* w, const float* b, MlpCond c, int len, const double
 int transfer_cot(const float2* R3, const float2* S_hat, Mesh3 m, SpecTables t, int len, double* out, cudaStream_t s) {
   const size_t smem = sizeof(double) * (size_t)len;
   if (smem > 200 * 1024) return kUnsupported;
-  static bool attr = false;
-  if (!attr) {
-    PMB_CUDA_CHECK(cudaFuncSetAttribute(transfer_cot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr = true;
-  }
+  PMB_CUDA_CHECK(smem_optin((const void*)transfer_cot_kernel, 200 * 1024));
   int64_t blocks = (m.half_cells() + 255) / 256;
   if (blocks > 148 * 4) blocks = 148 * 4;
   transfer_cot_kernel<<<(unsigned)(blocks > 0 ? blocks : 1), 256, smem, s>>>(R3, S_hat, m, t, 1.0 / (double)m.cells(),

@@ -13,6 +13,9 @@
 #include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <map>
+#include <mutex>
+#include <utility>
 
 namespace pmb {
 
@@ -169,4 +172,21 @@ inline int64_t spec_table_len(Mesh3 m, int has_masks) {
 
 namespace pmb {
 void set_last_error(const char* msg);
+
+// Raises kernel fn's dynamic shared-memory limit to at least `bytes` on the
+// current device.  The attribute belongs to the device's context, so it is
+// tracked per (device, kernel): a process may drive several GPUs.  Thread-safe.
+inline cudaError_t smem_optin(const void* fn, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  int& have = done[std::make_pair(dev, fn)];
+  if (have >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) have = bytes;
+  return e;
+}
 }

@@ -1033,7 +1033,7 @@ int launch_col_ctas(const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
   constexpr int S = stages_for(G::BUF * 8, EXTRA, CTAS);
   const int smem = S * G::BUF * 8 + EXTRA + S * 8;
   auto k = col_pass_kernel<R1, R2, S, MODE, CTAS>;
-  PMB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  PMB_CUDA_CHECK(smem_optin((const void*)k, smem));
   const int grid = persistent_grid(k, G::T, smem, a.ntiles);
   k<<<grid, G::T, smem, s>>>(map, a);
   PMB_CUDA_CHECK(cudaGetLastError());
@@ -1068,7 +1068,7 @@ int launch_z(const ZArgs& a, cudaStream_t s) {
   constexpr int S = 2;
   constexpr int smem = S * stage + G::XP * 8 + G::TW * 8 + S * 8;
   auto k = C2R ? z_c2r_kernel<R1, R2, S> : z_r2c_kernel<R1, R2, S>;
-  PMB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  PMB_CUDA_CHECK(smem_optin((const void*)k, smem));
   const int grid = persistent_grid(k, G::T, smem, a.ntiles);
   k<<<grid, G::T, smem, s>>>(a);
   PMB_CUDA_CHECK(cudaGetLastError());
