@@ -503,6 +503,17 @@ __global__ void __launch_bounds__(256) gather_kernel_x2(const Rec* __restrict__ 
   corners_of(r0, m, k0);
   corners_of(r1, m, k1);
   const uint32_t s0 = perm[i0], s1 = two ? perm[i1] : s0;
+  // velocities of the folded kicks, loaded ahead of the corner loads so their
+  // latency (particle-order addresses) overlaps them instead of following
+  // each channel's sum
+  float u0[C], u1[C];
+  if (vel != nullptr) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      u0[c] = vel[(int64_t)s0 * C + c];
+      u1[c] = vel[(int64_t)s1 * C + c];
+    }
+  }
   const int64_t cells = m.cells();
 #pragma unroll
   for (int c = 0; c < C; ++c) {
@@ -520,10 +531,10 @@ __global__ void __launch_bounds__(256) gather_kernel_x2(const Rec* __restrict__ 
       a1 = __fadd_rn(a1, __fmul_rn(v1[b], k1.w[b]));
     }
     out[(int64_t)s0 * C + c] = a0;
-    if (vel != nullptr) vel[(int64_t)s0 * C + c] = kicked(vel[(int64_t)s0 * C + c], a0, kick, kick2);
+    if (vel != nullptr) vel[(int64_t)s0 * C + c] = kicked(u0[c], a0, kick, kick2);
     if (two) {
       out[(int64_t)s1 * C + c] = a1;
-      if (vel != nullptr) vel[(int64_t)s1 * C + c] = kicked(vel[(int64_t)s1 * C + c], a1, kick, kick2);
+      if (vel != nullptr) vel[(int64_t)s1 * C + c] = kicked(u1[c], a1, kick, kick2);
     }
   }
 }

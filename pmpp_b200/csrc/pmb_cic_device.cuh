@@ -235,6 +235,12 @@ __device__ __forceinline__ void gather_one(const Rec& r, uint32_t src, Mesh3 m, 
                                            float kick2 = 0.f) {
   Corners k;
   corners_of(r, m, k);
+  // velocities loaded ahead of the corner loads (latency overlapped)
+  float u[C];
+  if (vel != nullptr) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) u[c] = vel[(int64_t)src * C + c];
+  }
   const int64_t cells = m.cells();
 #pragma unroll
   for (int c = 0; c < C; ++c) {
@@ -243,7 +249,7 @@ __device__ __forceinline__ void gather_one(const Rec& r, uint32_t src, Mesh3 m, 
 #pragma unroll
     for (int b = 0; b < 8; ++b) a = __fadd_rn(a, __fmul_rn(__ldg(mc + k.idx[b]), k.w[b]));
     out[(int64_t)src * C + c] = a;
-    if (vel != nullptr) vel[(int64_t)src * C + c] = kicked(vel[(int64_t)src * C + c], a, kick, kick2);
+    if (vel != nullptr) vel[(int64_t)src * C + c] = kicked(u[c], a, kick, kick2);
   }
 }
 

@@ -64,6 +64,9 @@ class _NoTimer:
     def mark(self, name, start):
         return None
 
+    def tag(self, name):
+        return None
+
 
 def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc, drift_vel, drift, vel_kick,
                   kick, timer, src_hat_out=None, lane="", kick2=0.0):
@@ -117,6 +120,8 @@ def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F
     call("pmb_gather_rows2", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc.data_ptr(), ptr(vel_kick),
          float(kick), float(kick2), s)
     timer.mark("gather", t)
+    if vel_kick is not None:
+        timer.tag("gather_kick")  # this gather also read and wrote the velocities
 
 
 def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc_cot, disp_cot, timer,

@@ -68,6 +68,10 @@ class StageTimer:
         e.record()
         return e
 
+    def tag(self, name):
+        """Count a variant of the last stage (no event): e.g. gathers that also kick."""
+        self.counts[name] = self.counts.get(name, 0) + 1
+
     def totals(self):
         torch.cuda.synchronize()
         out = {}
