@@ -96,8 +96,8 @@ class ClockSampler:
 # --set full capture of the same kernels at 256^3 particles / 512^3 mesh (mesh cells = 8 particles);
 # traffic scales with particles at a fixed cells-per-particle ratio.
 MEASURED_TRAFFIC_PER_PARTICLE = {
-    "gather": (1.949 + 0.198) * 1e9 / 256**3,
-    "gather_kick": (2.149674 + 0.391597) * 1e9 / 256**3,
+    "gather": (1.949012 + 0.193225) * 1e9 / 256**3,       # gather_kernel_x2<3>, no velocities
+    "gather_kick": (2.150708 + 0.389332) * 1e9 / 256**3,  # gather_kernel_x2<3> with the folded kicks
     "scatter3": (0.472 + 1.556) * 1e9 / 256**3,
     "scatter": (0.270 + 0.484) * 1e9 / 256**3,
     "scatter_adjoint": (1.075 + 0.189) * 1e9 / 256**3,
