@@ -598,12 +598,14 @@ int wait_timeouts(unsigned int* count) {
 // u[src, c] (the weights in sorted order, so a following scatter of u reads
 // them coalesced instead of through the permutation).
 // Per-particle body shared by the direct and staged kernels; fetch(c, b)
-// returns channel c of corner b (bit a of b: +1 along axis a).
+// returns channel c of corner b (bit a of b: +1 along axis a).  With
+// accumulate, dprev (if given) holds disp_cot[src] loaded by the caller ahead
+// of the corner loads.
 template <int C, class Fetch>
 __device__ __forceinline__ void interp_grad_one(const Rec& r, uint32_t src, int64_t i, const Fetch& fetch,
                                                 const float* __restrict__ u, float u_const, float cell, int accumulate,
                                                 float* __restrict__ disp_cot, float* __restrict__ wsum,
-                                                float* __restrict__ u_sorted) {
+                                                float* __restrict__ u_sorted, const float* dprev = nullptr) {
   const float f[3] = {r.fx, r.fy, r.fz};
   float wa[3][2], sg[3][2];
 #pragma unroll
@@ -648,9 +650,9 @@ __device__ __forceinline__ void interp_grad_one(const Rec& r, uint32_t src, int6
   g2 = __fdiv_rn(g2, cell);
   float* dc = disp_cot + 3 * (int64_t)src;
   if (accumulate) {
-    dc[0] = __fadd_rn(dc[0], g0);
-    dc[1] = __fadd_rn(dc[1], g1);
-    dc[2] = __fadd_rn(dc[2], g2);
+    dc[0] = __fadd_rn(dprev ? dprev[0] : dc[0], g0);
+    dc[1] = __fadd_rn(dprev ? dprev[1] : dc[1], g1);
+    dc[2] = __fadd_rn(dprev ? dprev[2] : dc[2], g2);
   } else {
     dc[0] = g0;
     dc[1] = g1;
@@ -694,6 +696,17 @@ __global__ void __launch_bounds__(256) interp_grad_kernel_x2(const Rec* __restri
   Corners k0, k1;
   corners_of(r0, m, k0);
   corners_of(r1, m, k1);
+  const uint32_t s0 = perm[i0], s1 = two ? perm[i1] : s0;
+  // accumulated position cotangents, loaded ahead of the corner loads: read
+  // after each particle's sums, their particle-order latency ran in series
+  float d0[3] = {0.f, 0.f, 0.f}, d1[3] = {0.f, 0.f, 0.f};
+  if (accumulate) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      d0[a] = disp_cot[3 * (int64_t)s0 + a];
+      d1[a] = disp_cot[3 * (int64_t)s1 + a];
+    }
+  }
   const int64_t cells = m.cells();
   float v0[C][8], v1[C][8];
 #pragma unroll
@@ -704,10 +717,10 @@ __global__ void __launch_bounds__(256) interp_grad_kernel_x2(const Rec* __restri
       v1[c][b] = __ldg(mesh + (int64_t)c * cells + k1.idx[b]);
     }
   auto f0 = [&](int c, int b) { return v0[c][b]; };
-  interp_grad_one<C>(r0, perm[i0], i0, f0, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted);
+  interp_grad_one<C>(r0, s0, i0, f0, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted, d0);
   if (two) {
     auto f1 = [&](int c, int b) { return v1[c][b]; };
-    interp_grad_one<C>(r1, perm[i1], i1, f1, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted);
+    interp_grad_one<C>(r1, s1, i1, f1, u, u_const, cell, accumulate, disp_cot, wsum, u_sorted, d1);
   }
 }
 
