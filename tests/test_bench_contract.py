@@ -1,0 +1,50 @@
+"""CPU checks of bench.py's output contract: the reference arm's JSON line (a
+tiny oracle sample), the workload config both arms share, and the byte models
+the roofline divides by."""
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import types
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _bench():
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_reference_arm_line():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0", "--cpu-ptcl", "16"], capture_output=True, text=True, timeout=600,
+                         cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in d, key
+    assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    b = _bench()
+    args = types.SimpleNamespace(ptcl=512, mesh=2, nsteps=32, gpus=1)
+    assert d["config"] == b.arm_config(args, 1)
+    assert d["metric"] == b.METRIC and d["unit"] == b.UNIT
+
+
+def test_roofline_byte_models():
+    from pmpp_b200.roofline import algorithmic_bytes
+    N, M = 256**3, 512**3
+    assert algorithmic_bytes("gather_kick", N, M) - algorithmic_bytes("gather", N, M) == 24 * N
+    b = _bench()
+    # measured traffic per launch stays within a few percent of the algorithmic bytes
+    for name in ("gather", "gather_kick"):
+        ratio = b.MEASURED_TRAFFIC_PER_PARTICLE[name] * N / algorithmic_bytes(name, N, M)
+        assert 0.95 < ratio < 1.05, (name, ratio)
+    assert b.STAGE_VARIANTS["gather"] == "gather_kick"
