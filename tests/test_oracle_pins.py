@@ -12,6 +12,8 @@ closed-form / invariant assertions of the reference test suite, restated:
   * tests/test_deep_boltzmann_contracts.py:20-31 transfer normalisation
   * tests/test_finite_diff.py:87-124            adjoints vs 4th-order central
                                                 differences in float64
+  * tests/test_gravity_particle_nyquist_filter.py:11-40  refined force meshes do
+                                                not alias the particle lattice
 """
 import numpy as np
 
@@ -173,3 +175,28 @@ def test_oracle_nbody_adjoint_vs_finite_differences():
         return float((o[0] * dcot).sum() + (o[1] * vcot).sum())
 
     np.testing.assert_allclose((dc * u).sum(), _fd4(L, disp, u, 1e-4), rtol=1e-6)
+
+
+def _x_force_modes(mesh, res=16, box=1000.0, amp=0.5):
+    """|rFFT| of the x-mean of the x force for lattice positions displaced by
+    amp sin(2 pi x / box) along x (ordered particles: pmid the lattice cell,
+    disp the nearest-image offset), normalised by res / 2."""
+    conf = opm.Conf(box / res, (res, res, res), mesh_shape=mesh, a_start=1 / 128, a_nbody_maxstep=1 / 20)
+    pmid, _ = opm.gen_grid(conf)
+    axis = np.arange(res, dtype=np.float32) * np.float32(box / res)
+    x, y, z = np.meshgrid(axis, axis, axis, indexing="ij")
+    pos = np.stack([x, y, z], axis=-1).reshape(-1, 3)
+    pos[:, 0] = (pos[:, 0] + np.float32(amp) * np.sin(np.float32(2 * np.pi / box) * pos[:, 0])) % np.float32(box)
+    disp = pos.astype(np.float64) - pmid.astype(np.float64) * conf.cell_size
+    disp = ((disp + box / 2) % box - box / 2).astype(np.float32)
+    acc = opm.gravity(pmid, disp, conf, 0.3)
+    mean_x = acc[:, 0].reshape(res, res, res).mean(axis=(1, 2))
+    return np.abs(np.fft.rfft(mean_x)) / (res / 2)
+
+
+def test_refined_force_mesh_does_not_alias_particle_lattice():
+    base = _x_force_modes(1)[1]
+    for mesh in (2, 4):
+        modes = _x_force_modes(mesh)
+        assert np.isclose(modes[1], base, rtol=0.03)
+        assert modes[2] < 0.10 * base
