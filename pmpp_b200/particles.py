@@ -44,6 +44,42 @@ class Particles:
         z = torch.zeros_like(disp)
         return cls(conf, pmid, disp, z.clone() if vel else None, z.clone() if acc else None)
 
+    @classmethod
+    def from_pos(cls, conf, pos, vel=None, acc=None, wrap=True):
+        """Anchor every particle at its nearest mesh cell (particles.py:441-479,
+        single device): pmid = rint(pos / cell), disp = pos - pmid * cell in the
+        positions' dtype, then cast; with wrap, pmid modulo the mesh.  Anchors
+        of different particles may coincide."""
+        pos = torch.as_tensor(pos)
+        pmid = torch.round(pos / conf.cell_size)  # half to even, like rint
+        disp = pos - pmid * conf.cell_size
+        pmid = pmid.to(torch.int16)
+        if wrap:
+            pmid = torch.remainder(pmid, torch.tensor(conf.mesh_shape, dtype=torch.int16, device=pmid.device))
+        return cls(conf, pmid.contiguous(), disp.to(conf.float_dtype).contiguous(), vel, acc)
+
+    @classmethod
+    def from_ordered_pos(cls, conf, pos, vel=None, acc=None, wrap=True):
+        """Positions given in particle-grid order (LPT outputs, snapshots) keep
+        the lattice anchors of gen_grid, which are unique where rounding the
+        positions would collide (particles.py:497-545).  disp is the nearest
+        periodic image of pos - anchor, computed in the working float dtype.
+        ``wrap`` is accepted for signature parity; the nearest-image offset
+        already wraps."""
+        del wrap
+        pos = torch.as_tensor(pos)
+        grid = cls.gen_grid(conf, device=pos.device)
+        if pos.shape[0] != grid.pmid.shape[0]:
+            raise ValueError("from_ordered_pos requires a full particle-grid ordered position array: "
+                             f"expected {grid.pmid.shape[0]} particles, got {pos.shape[0]}.")
+        dt = conf.float_dtype
+        p = pos.to(dt)
+        anchor = grid.pmid.to(dt) * torch.tensor(conf.cell_size, dtype=dt, device=p.device)
+        box = torch.tensor(conf.box_size, dtype=dt, device=p.device)
+        half = torch.tensor(0.5, dtype=dt, device=p.device) * box
+        disp = torch.remainder(p - anchor + half, box) - half
+        return cls(conf, grid.pmid, disp.contiguous(), vel, acc)
+
     def pos(self, dtype=torch.float64, wrap=True):
         """particles.py:773-798."""
         pos = self.pmid.to(dtype) * self.conf.cell_size + self.disp.to(dtype)

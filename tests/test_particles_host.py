@@ -1,0 +1,94 @@
+"""Host-side particle constructors (no GPU): from_pos / from_ordered_pos
+against the reference's ordered-initialisation test (restated from
+tests/test_particles_ordered_init.py:9-29) and against numpy restatements of
+particles.py:441-479 and :497-545 in float32; gen_grid against the oracle."""
+import numpy as np
+import torch
+
+import pmpp_b200 as pb
+
+
+def _raveled(pmid, conf):
+    m = torch.tensor(conf.mesh_shape, dtype=torch.int64)
+    p = torch.remainder(pmid.to(torch.int64), m)
+    return ((p[:, 0] * m[1] + p[:, 1]) * m[2] + p[:, 2]).numpy()
+
+
+def _lattice(conf):
+    axes = [np.arange(n, dtype=np.float32) * np.float32(conf.ptcl_spacing) for n in conf.ptcl_grid_shape]
+    return np.stack(np.meshgrid(*axes, indexing="ij"), axis=-1).reshape(-1, 3)
+
+
+def test_from_ordered_pos_keeps_unique_anchors_under_collisions():
+    conf = pb.Configuration(1.0, (4, 4, 4), 1, device="cpu")
+    pos = _lattice(conf)
+    # particles 0 and 16 share y, z; moving both to x = 0.6 makes them round to the same cell
+    pos[0, 0] = np.float32(0.6)
+    pos[16, 0] = np.float32(0.6)
+    colliding = pb.Particles.from_pos(conf, torch.from_numpy(pos))
+    assert np.unique(_raveled(colliding.pmid, conf)).size < conf.ptcl_num
+    ordered = pb.Particles.from_ordered_pos(conf, torch.from_numpy(pos))
+    assert np.unique(_raveled(ordered.pmid, conf)).size == conf.ptcl_num
+    np.testing.assert_allclose(ordered.pos(dtype=torch.float32).numpy(), pos, atol=1e-6, rtol=1e-6)
+
+
+def _scattered_positions(conf, seed):
+    rng = np.random.default_rng(seed)
+    base = _lattice(conf).astype(np.float64)
+    box = np.asarray(conf.box_size, dtype=np.float64)
+    return ((base + rng.normal(0, 2.0 * conf.cell_size, size=base.shape)) % box).astype(np.float32)
+
+
+def test_from_ordered_pos_matches_nearest_image_restatement():
+    for shape, mesh in (((8, 8, 8), 2), ((4, 8, 16), 1), ((6, 4, 8), 2)):
+        conf = pb.Configuration(1.5, shape, mesh, device="cpu")
+        pos = _scattered_positions(conf, seed=sum(shape))
+        got = pb.Particles.from_ordered_pos(conf, torch.from_numpy(pos))
+        grid = pb.Particles.gen_grid(conf)
+        assert torch.equal(got.pmid, grid.pmid)
+        anchor = grid.pmid.numpy().astype(np.float32) * np.float32(conf.cell_size)
+        box = np.asarray(conf.box_size, dtype=np.float32)
+        ref = (pos - anchor + np.float32(0.5) * box) % box - np.float32(0.5) * box
+        np.testing.assert_array_equal(got.disp.numpy(), ref)
+        # positions come back to within float32 rounding of the box
+        back = got.pos(dtype=torch.float64).numpy()
+        d = (back - pos.astype(np.float64) + box / 2) % box - box / 2
+        assert np.abs(d).max() < 1e-4
+
+
+def test_from_pos_matches_rint_restatement():
+    conf = pb.Configuration(1.5, (8, 8, 8), 2, device="cpu")
+    pos = _scattered_positions(conf, seed=4)
+    got = pb.Particles.from_pos(conf, torch.from_numpy(pos))
+    c = np.float32(conf.cell_size)
+    pm = np.rint(pos / c)
+    disp = pos - pm * c
+    pm = np.mod(pm.astype(np.int16), np.asarray(conf.mesh_shape, dtype=np.int16))
+    np.testing.assert_array_equal(got.pmid.numpy(), pm)
+    np.testing.assert_array_equal(got.disp.numpy(), disp.astype(np.float32))
+
+
+def test_from_ordered_pos_rejects_partial_arrays():
+    conf = pb.Configuration(1.0, (4, 4, 4), 1, device="cpu")
+    pos = torch.from_numpy(_lattice(conf)[:10])
+    try:
+        pb.Particles.from_ordered_pos(conf, pos)
+    except ValueError as e:
+        assert "expected 64 particles, got 10" in str(e)
+    else:
+        raise AssertionError("partial array accepted")
+
+
+def test_gen_grid_matches_oracle_bitwise():
+    """Lattice anchors and displacements of gen_grid (particles.py:615-727),
+    including mesh / particle ratios that are not integers, where the anchors
+    come from rounding."""
+    from oracle import pm as opm
+    for shape, mesh in (((4, 4, 4), 1), ((8, 8, 8), 2), ((6, 4, 10), (9, 6, 15)), ((16, 16, 16), 1.5),
+                        ((12, 12, 12), (20, 20, 20))):
+        co = opm.Conf(2.0, shape, mesh_shape=mesh)
+        conf = pb.Configuration(2.0, shape, mesh, device="cpu")
+        pmid, disp = opm.gen_grid(co)
+        g = pb.Particles.gen_grid(conf)
+        np.testing.assert_array_equal(g.pmid.numpy(), pmid)
+        np.testing.assert_array_equal(g.disp.numpy(), disp.astype(np.float32))
