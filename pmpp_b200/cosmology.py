@@ -179,5 +179,50 @@ def tophat_variance(R, cosmo, conf=None):
     return h / 3 * (f[0] + f[-1] + 4 * f[1:-1:2].sum() + 2 * f[2:-1:2].sum())
 
 
+def transfer(k, cosmo, conf=None):
+    """Matter transfer function at k [1/L], interpolated in the table that
+    boltzmann fills (boltzmann.py:140-174)."""
+    conf = cosmo.conf if conf is None else conf
+    if cosmo.transfer is None:
+        raise ValueError("Transfer table is empty. Call boltzmann first.")
+    k = np.asarray(k)
+    dtype = np.promote_types(k.dtype, np.float64)
+    return np.interp(k, conf.transfer_k, cosmo.transfer).astype(dtype)
+
+
+def varlin(R, a, cosmo, conf=None):
+    """Linear matter variance sigma^2(R) at scales R [L], times D(a)^2 unless a
+    is None (boltzmann.py:314-355).  Each R is evaluated by the Simpson
+    quadrature of tophat_variance rather than interpolated in a table."""
+    conf = cosmo.conf if conf is None else conf
+    if cosmo.transfer is None or cosmo.growth is None:
+        raise ValueError("Linear matter overdensity variance needs the boltzmann tables. Call boltzmann first.")
+    R = np.asarray(R, dtype=np.float64)
+    s2 = np.vectorize(lambda r: tophat_variance(float(r), cosmo, conf), otypes=[np.float64])(R)
+    if a is not None:
+        s2 = s2 * np.asarray(growth(a, cosmo, conf), dtype=np.float64)**2
+    return s2
+
+
+def cosmology_param_names(cosmo):
+    """Differentiable parameter names of this instance (models.py:267-288):
+    the five base parameters and each optional one that is set."""
+    names = ["A_s_1e9", "n_s", "Omega_m", "Omega_b", "h"]
+    names += [n for n in ("Omega_k_", "w_0_", "w_a_") if getattr(cosmo, n) is not None]
+    return tuple(names)
+
+
+def cosmology_param_values(cosmo, names=None):
+    """Parameter values in the order of names (default cosmology_param_names)
+    (models.py:291-309)."""
+    names = cosmology_param_names(cosmo) if names is None else names
+    return tuple(getattr(cosmo, n) for n in names)
+
+
+def replace_cosmology_params(cosmo, names, values):
+    """A cosmology with the named parameters replaced (models.py:312-329)."""
+    return cosmo.replace(**dict(zip(names, values)))
+
+
 def _touch():
     lib()

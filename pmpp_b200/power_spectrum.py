@@ -151,6 +151,17 @@ def particles_to_cross_correlation(ptcl_a, ptcl_b, conf, mas="CIC", eps=1e-30):
     return density_to_cross_correlation(ra, rb, conf, mas, eps)
 
 
+def cross_correlation(delta_a, delta_b, conf, mas="CIC", eps=1e-30):
+    """delta_to_cross_correlation on overdensity fields (power_spectrum.py:471-490)."""
+    return delta_to_cross_correlation(delta_a, delta_b, conf, mas=mas, eps=eps)
+
+
+# the earlier public names of the P(k) functions (power_spectrum.py:493-496)
+delta_to_quijote_pk = delta_to_pk
+density_to_quijote_pk = density_to_pk
+particles_to_quijote_pk = particles_to_pk
+
+
 def log_binned(k, pk, nmodes, nbins=32, kmin=None, kmax=None):
     """Mode-count-weighted rebinning of integer shells into log-spaced bins."""
     kmin = k[0] if kmin is None else kmin

@@ -56,3 +56,40 @@ def test_linear_power_matches_oracle():
     oc = opm.boltzmann(ocos.Cosmo(), co)
     k = np.geomspace(1e-3, 5, 50)
     np.testing.assert_allclose(pb.linear_power(k, None, c), ocos.linear_power(k, None, oc, co.transfer_k), rtol=1e-12)
+
+
+def test_transfer_and_varlin_helpers():
+    """transfer / varlin (boltzmann.py:140-174, 314-355): table interpolation,
+    sigma8 consistency and growth scaling; both refuse an empty table."""
+    import pytest
+    from pmpp_b200 import cosmology as C
+    pb, co, conf = _pair()
+    c = pb.boltzmann(pb.SimpleLCDM(conf))
+    tk = conf.transfer_k
+    np.testing.assert_array_equal(C.transfer(tk[10:20], c), c.transfer[10:20])
+    mid = np.sqrt(tk[10] * tk[11])
+    assert min(c.transfer[10], c.transfer[11]) <= C.transfer(mid, c) <= max(c.transfer[10], c.transfer[11])
+    np.testing.assert_allclose(np.sqrt(C.varlin(8.0, 1.0, c)), c.sigma8, rtol=1e-12)
+    s2 = C.varlin(np.array([4.0, 8.0, 16.0]), None, c)
+    assert s2.shape == (3, ) and np.all(np.diff(s2) < 0)
+    np.testing.assert_allclose(C.varlin(8.0, 0.5, c), s2[1] * float(pb.growth(0.5, c))**2, rtol=1e-12)
+    bare = pb.SimpleLCDM(conf)
+    with pytest.raises(ValueError):
+        C.transfer(tk[:3], bare)
+    with pytest.raises(ValueError):
+        C.varlin(8.0, 1.0, bare)
+
+
+def test_cosmology_param_helpers():
+    """models.py:267-329: names include set optional parameters, values follow
+    the names, replace returns a new instance."""
+    from pmpp_b200 import cosmology as C
+    pb, co, conf = _pair()
+    c = pb.SimpleLCDM(conf)
+    assert C.cosmology_param_names(c) == ("A_s_1e9", "n_s", "Omega_m", "Omega_b", "h")
+    w = c.replace(w_0_=-0.9, Omega_k_=0.01)
+    assert C.cosmology_param_names(w) == ("A_s_1e9", "n_s", "Omega_m", "Omega_b", "h", "Omega_k_", "w_0_")
+    assert C.cosmology_param_values(w) == (2.0, 0.96, 0.3, 0.05, 0.7, 0.01, -0.9)
+    assert C.cosmology_param_values(w, ("h", "Omega_m")) == (0.7, 0.3)
+    r = C.replace_cosmology_params(c, ("Omega_m", "h"), (0.31, 0.68))
+    assert (r.Omega_m, r.h, c.Omega_m, c.h) == (0.31, 0.68, 0.3, 0.7)
