@@ -26,8 +26,23 @@ def _fftfreq(shape, spacing, dtype=np.float32):
 class Configuration:
     """PM configuration; see core/configuration.py:22-243 for field meanings."""
 
+    # SI constants and the code units [L] = Mpc/h, [T] = 1/H_0, [M] = 1e10 Msun/h
+    # (configuration.py:198-209; the values must agree for the time factors)
+    M_sun_SI = 1.98847e30
+    Mpc_SI = 3.0856775815e22
+    H_0_SI = 1e5 / Mpc_SI
+    c_SI = 299792458
+    G_SI = 6.67430e-11
+    M = 1e10 * M_sun_SI
+    L = Mpc_SI
+    T = 1 / H_0_SI
+    # the reference's multi-GPU attributes at their single-device values
+    use_mGPU = False
+    mesh_halo_width = 0
+    ptcl_halo_width = 0
+
     def __init__(self, ptcl_spacing, ptcl_grid_shape, mesh_shape=1, *, a_start=1 / 64, a_stop=1.0,
-                 a_lpt_maxstep=1 / 128, a_nbody_maxstep=1 / 64, a_custom=None,
+                 a_lpt_maxstep=1 / 128, a_nbody_maxstep=1 / 64, a_custom=None, growth_a_custom=None,
                  symp_splits=((0, 0.5), (1, 0.5)), lpt_order=2, growth_rtol=None, growth_atol=None,
                  growth_inistep=(1, None), transfer_fit=True, transfer_fit_nowiggle=False, transfer_lgk_min=-4,
                  transfer_lgk_max=3, transfer_lgk_maxstep=1 / 128, T_cmb=2.7255, k_pivot_Mpc=0.05,
@@ -37,7 +52,9 @@ class Configuration:
         if isinstance(mesh_shape, (int, float)):
             mesh_shape = tuple(round(s * mesh_shape) for s in self.ptcl_grid_shape)
         self.mesh_shape = tuple(int(s) for s in mesh_shape)
-        if len(self.ptcl_grid_shape) != 3 or len(self.mesh_shape) != 3:
+        if len(self.ptcl_grid_shape) != len(self.mesh_shape):
+            raise ValueError('particle and mesh grid dimensions differ')
+        if len(self.ptcl_grid_shape) != 3:
             raise ValueError("only three spatial dimensions are supported")
         if any(sm < sp for sp, sm in zip(self.ptcl_grid_shape, self.mesh_shape)):
             raise ValueError('mesh grid cannot be smaller than particle grid')
@@ -55,6 +72,8 @@ class Configuration:
         self.a_lpt_maxstep = a_lpt_maxstep
         self.a_nbody_maxstep = a_nbody_maxstep
         self.a_custom = None if a_custom is None else tuple(float(a) for a in np.asarray(a_custom).tolist())
+        self.growth_a_custom = (None if growth_a_custom is None else
+                                tuple(float(a) for a in np.asarray(growth_a_custom).tolist()))
         if any(len(s) != 2 for s in symp_splits):
             raise ValueError(f'symp_splits={symp_splits} not supported')
         if tuple(sum(s) for s in zip(*symp_splits)) != (1, 1):
@@ -119,8 +138,50 @@ class Configuration:
         return float(np.prod(self.box_size))
 
     @property
+    def disp_size(self):
+        """Inverse mesh-cell size (displacements in cell units)."""
+        return 1 / self.cell_size
+
+    @property
+    def local_mesh_shape(self):
+        return self.mesh_shape
+
+    @property
+    def local_mesh_with_halo_shape(self):
+        return self.mesh_shape
+
+    @property
+    def local_mesh_size(self):
+        return self.mesh_size
+
+    # ---- units (configuration.py:483-506) ----
+    @property
+    def V(self):
+        return self.L / self.T
+
+    @property
+    def H_0(self):
+        return self.H_0_SI * self.T
+
+    @property
+    def c(self):
+        return self.c_SI / self.V
+
+    @property
+    def G(self):
+        return self.G_SI * self.M / (self.L * self.V**2)
+
+    @property
+    def rho_crit(self):
+        return 3 * self.H_0**2 / (8 * np.pi * self.G)
+
+    @property
     def transfer_k_num(self):
         return 1 + math.ceil((self.transfer_lgk_max - self.transfer_lgk_min) / self.transfer_lgk_maxstep) + 1
+
+    @property
+    def transfer_lgk_step(self):
+        return (self.transfer_lgk_max - self.transfer_lgk_min) / (self.transfer_k_num - 2)
 
     @property
     def transfer_k(self):
@@ -140,6 +201,10 @@ class Configuration:
         return math.ceil((self.a_stop - self.a_start) / self.a_nbody_maxstep)
 
     @property
+    def a_nbody_step(self):
+        return (self.a_stop - self.a_start) / self.a_nbody_num
+
+    @property
     def a_lpt(self):
         return np.linspace(0, self.a_start, num=self.a_lpt_num + 1)
 
@@ -151,6 +216,10 @@ class Configuration:
 
     @property
     def growth_a(self):
+        """Growth-table scale factors: growth_a_custom, else a_lpt then a_nbody[1:]
+        (configuration.py:559-563)."""
+        if self.growth_a_custom is not None:
+            return np.array(self.growth_a_custom, dtype=np.float64)
         return np.concatenate((self.a_lpt, self.a_nbody[1:]))
 
     @property
