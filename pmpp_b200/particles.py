@@ -1,6 +1,7 @@
 """Particle state (nbody/particles.py:33-127) as device tensors.
 
-pmid int16 (N,3) anchor mesh cells, disp/vel/acc float32 (N,3).
+pmid int16 (N,3) anchor mesh cells, disp/vel/acc float32 (N,3); attr an
+optional dict of per-particle attributes in the float dtype.
 """
 from __future__ import annotations
 
@@ -17,16 +18,69 @@ class Particles:
     disp: torch.Tensor
     vel: Optional[torch.Tensor] = None
     acc: Optional[torch.Tensor] = None
+    attr: Optional[dict] = None
+
+    def __post_init__(self):
+        if self.attr is not None:  # custom per-particle features in the float dtype (particles.py:115-118)
+            self.attr = {k: torch.as_tensor(v).to(self.conf.float_dtype) for k, v in self.attr.items()}
 
     def __len__(self):
         return self.pmid.shape[0]
+
+    def __getitem__(self, key):
+        """The particles selected by key (an index, slice or mask) in every field."""
+        g = lambda t: None if t is None else t[key]
+        attr = None if self.attr is None else {k: v[key] for k, v in self.attr.items()}
+        return Particles(self.conf, self.pmid[key], self.disp[key], g(self.vel), g(self.acc), attr)
 
     def replace(self, **kw):
         return replace(self, **kw)
 
     def clone(self):
         c = lambda t: None if t is None else t.clone()
-        return Particles(self.conf, self.pmid, c(self.disp), c(self.vel), c(self.acc))
+        attr = None if self.attr is None else {k: v.clone() for k, v in self.attr.items()}
+        return Particles(self.conf, self.pmid, c(self.disp), c(self.vel), c(self.acc), attr)
+
+    def raveled_id(self, dtype=torch.int64, wrap=False):
+        """Raveled mesh index of each anchor, ((x My) + y) Mz + z (particles.py:729-772).
+        int64 by default (the reference's uint64 is not a full torch dtype)."""
+        if dtype.is_floating_point or dtype.is_complex or dtype == torch.bool:
+            raise TypeError("raveled particle IDs require an integer dtype")
+        if self.conf.mesh_size - 1 > torch.iinfo(dtype).max:
+            raise OverflowError(f"mesh size {self.conf.mesh_size} does not fit {dtype}")
+        pmid = self.pmid
+        if wrap:
+            pmid = torch.remainder(pmid, torch.tensor(self.conf.mesh_shape, dtype=pmid.dtype, device=pmid.device))
+        _, my, mz = self.conf.mesh_shape
+        p = pmid.to(dtype)
+        return (p[:, 0] * (my * mz) + p[:, 1] * mz + p[:, 2]).to(dtype)
+
+    @staticmethod
+    def pmid_to_pos(pmid, disp, conf):
+        """pmid * cell + disp, wrapped into the box (particles.py:800-816)."""
+        pos = pmid.to(disp.dtype) * conf.cell_size + disp
+        return torch.remainder(pos, torch.tensor(conf.box_size, dtype=pos.dtype, device=pos.device))
+
+    @staticmethod
+    def pos_to_pmid(pos, conf):
+        """Nearest-cell anchors (wrapped) and displacements of positions (particles.py:818-840)."""
+        p = Particles.from_pos(conf, pos, wrap=True)
+        return p.pmid, p.disp
+
+    @classmethod
+    def from_pmid(cls, conf, pmid, disp, vel=None, acc=None):
+        """Particles from anchors and displacements as given (particles.py:546-571)."""
+        return cls(conf, torch.as_tensor(pmid), torch.as_tensor(disp), vel, acc)
+
+    @classmethod
+    def from_ptcl(cls, ptcl, conf=None, wrap=True):
+        """A copy of ptcl's state in conf's dtypes, anchors wrapped into the mesh
+        unless wrap is False (particles.py:573-613)."""
+        conf = ptcl.conf if conf is None else conf
+        pmid = ptcl.pmid.to(torch.int16)
+        if wrap:
+            pmid = torch.remainder(pmid, torch.tensor(conf.mesh_shape, dtype=torch.int16, device=pmid.device))
+        return cls(conf, pmid, ptcl.disp.to(conf.float_dtype), ptcl.vel, ptcl.acc)
 
     @classmethod
     def gen_grid(cls, conf, vel=False, acc=False, device=None):
@@ -57,6 +111,11 @@ class Particles:
         if wrap:
             pmid = torch.remainder(pmid, torch.tensor(conf.mesh_shape, dtype=torch.int16, device=pmid.device))
         return cls(conf, pmid.contiguous(), disp.to(conf.float_dtype).contiguous(), vel, acc)
+
+    @classmethod
+    def from_pos_sharded(cls, conf, pos, vel=None, acc=None, wrap=True):
+        """from_pos (one device; particles.py:481-494)."""
+        return cls.from_pos(conf, pos, vel=vel, acc=acc, wrap=wrap)
 
     @classmethod
     def from_ordered_pos(cls, conf, pos, vel=None, acc=None, wrap=True):

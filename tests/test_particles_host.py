@@ -92,3 +92,71 @@ def test_gen_grid_matches_oracle_bitwise():
         g = pb.Particles.gen_grid(conf)
         np.testing.assert_array_equal(g.pmid.numpy(), pmid)
         np.testing.assert_array_equal(g.disp.numpy(), disp.astype(np.float32))
+
+
+def _small_conf(shape=(3, 2, 2), mesh=2):
+    return pb.Configuration(0.75, shape, mesh, device="cpu")
+
+
+def test_coordinate_conversions_keep_subcell_offsets_and_periodicity():
+    """Restated from the reference's tests/test_deep_particles.py:39-60."""
+    conf = _small_conf()
+    box = np.asarray(conf.box_size, dtype=np.float32)
+    pos = torch.tensor([[-0.03, 0.11, 0.73], [0.38, 0.77, 1.51], [2.26, -0.01, 0.05]], dtype=torch.float32)
+    unwrapped = pb.Particles.from_pos(conf, pos, wrap=False)
+    wrapped = pb.Particles.from_pos_sharded(conf, pos, wrap=True)
+    expected = np.mod(pos.numpy(), box)
+    np.testing.assert_allclose(unwrapped.pos(dtype=torch.float32, wrap=False).numpy(), pos.numpy(), atol=2e-7)
+    np.testing.assert_allclose(wrapped.pos(dtype=torch.float32).numpy(), expected, atol=2e-7)
+    assert bool((unwrapped.pmid != wrapped.pmid).any()) and bool((wrapped.pmid >= 0).all())
+    pmid, disp = pb.Particles.pos_to_pmid(pos, conf)
+    np.testing.assert_allclose(pb.Particles.pmid_to_pos(pmid, disp, conf).numpy(), expected, atol=2e-7)
+    assert torch.equal(pmid, wrapped.pmid)
+    np.testing.assert_allclose(disp.numpy(), wrapped.disp.numpy(), atol=1e-7)
+    jac = torch.autograd.functional.jacobian(
+        lambda x: pb.Particles.from_pos(conf, x, wrap=False).pos(dtype=torch.float32, wrap=False), pos)
+    np.testing.assert_allclose(jac.reshape(pos.numel(), pos.numel()).numpy(), np.eye(pos.numel()), atol=2e-6)
+
+
+def test_ids_indexing_attributes_and_ordered_initialisation():
+    """Restated from the reference's tests/test_deep_particles.py:63-92."""
+    conf = _small_conf(shape=(2, 2, 2), mesh=2)
+    grid = pb.Particles.gen_grid(conf, vel=True, acc=True)
+    assert len(grid) == conf.ptcl_num
+    assert grid.pmid.dtype == torch.int16 and grid.disp.dtype == conf.float_dtype
+    assert float(grid.vel.abs().max()) == 0 and float(grid.acc.abs().max()) == 0
+    expected = np.ravel_multi_index(tuple(grid.pmid.numpy().astype(np.int64).T), conf.mesh_shape)
+    np.testing.assert_array_equal(grid.raveled_id().numpy(), expected)
+    first = grid[0]
+    assert tuple(first.pmid.shape) == (3, ) and torch.equal(first.pmid, grid.pmid[0])
+    attr = {"mass": np.arange(conf.ptcl_num, dtype=np.float64), "tag": np.ones((conf.ptcl_num, 2))}
+    attributed = pb.Particles(conf, grid.pmid, grid.disp, attr=attr)
+    assert attributed.attr["mass"].dtype == conf.float_dtype and attributed.attr["tag"].dtype == conf.float_dtype
+    np.testing.assert_array_equal(attributed[:2].attr["mass"].numpy(), [0, 1])
+    shifted = grid.pos(dtype=torch.float32).clone()
+    shifted[:, 0] += np.float32(0.37)
+    ordered = pb.Particles.from_ordered_pos(conf, shifted, vel=torch.ones_like(shifted),
+                                            acc=2 * torch.ones_like(shifted))
+    assert torch.equal(ordered.pmid, grid.pmid)
+    np.testing.assert_allclose(ordered.pos(dtype=torch.float32).numpy(), shifted.numpy(), atol=2e-7)
+    import pytest
+    with pytest.raises(ValueError, match="full particle-grid ordered"):
+        pb.Particles.from_ordered_pos(conf, shifted[:-1])
+
+
+def test_raveled_ids_and_copies_wrap_only_when_requested():
+    """Restated from the reference's tests/test_deep_particles.py:95-109."""
+    conf = _small_conf(shape=(2, 2, 2), mesh=1)
+    pmid = torch.tensor([[-1, 0, 0], [0, 1, 1], [2, 0, 0]], dtype=torch.int16)
+    disp = torch.zeros((3, 3), dtype=torch.float32)
+    original = pb.Particles.from_pmid(conf, pmid, disp, vel=torch.ones_like(disp), acc=2 * torch.ones_like(disp))
+    np.testing.assert_array_equal(original.raveled_id(dtype=torch.int32, wrap=True).numpy(), [4, 3, 0])
+    np.testing.assert_array_equal(original.raveled_id(dtype=torch.int32, wrap=False).numpy(), [-4, 3, 8])
+    copied = pb.Particles.from_ptcl(original)
+    unwrapped = pb.Particles.from_ptcl(original, conf=conf, wrap=False)
+    np.testing.assert_array_equal(copied.pmid.numpy(), [[1, 0, 0], [0, 1, 1], [0, 0, 0]])
+    assert torch.equal(unwrapped.pmid, pmid)
+    assert float(copied.vel.min()) == 1 and float(copied.acc.min()) == 2
+    import pytest
+    with pytest.raises(TypeError):
+        original.raveled_id(dtype=torch.float32)
