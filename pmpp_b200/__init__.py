@@ -11,14 +11,14 @@ include/pmb200.h); this package is the host-side mirror of PM++'s Python API:
 """
 from .configuration import Configuration
 from .cosmology import Cosmology, SimpleLCDM, boltzmann, growth, linear_power
-from .particles import Particles
+from .particles import Particles, pmid_to_idx
 from . import cic
 from .cic import scatter, gather, scatter_vjp, gather_vjp
 from .gravity import gravity, gravity_vjp
 from .nbody import nbody, nbody_adj, integrate, kick, drift, NBodyRun
 
 __all__ = [
-    "Configuration", "Cosmology", "SimpleLCDM", "boltzmann", "growth", "linear_power", "Particles", "cic", "scatter",
+    "Configuration", "Cosmology", "SimpleLCDM", "boltzmann", "growth", "linear_power", "Particles", "pmid_to_idx", "cic", "scatter",
     "gather", "scatter_vjp", "gather_vjp", "gravity", "gravity_vjp", "nbody", "nbody_adj", "integrate", "kick",
     "drift", "NBodyRun"
 ]

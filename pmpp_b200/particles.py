@@ -145,3 +145,14 @@ class Particles:
         if wrap:
             pos = torch.remainder(pos, torch.tensor(self.conf.box_size, dtype=dtype, device=pos.device))
         return pos
+
+
+def pmid_to_idx(pmid, conf, unused_index=None, dtype=torch.int32):
+    """Flat cell key ((x mod Mx) My + (y mod My)) Mz + (z mod Mz) of each anchor;
+    entries flagged in unused_index get -1 (core/utils.py:292-326)."""
+    m = [torch.tensor(s, dtype=dtype, device=pmid.device) for s in conf.mesh_shape]
+    ix, iy, iz = (torch.remainder(pmid[:, d].to(dtype), m[d]) for d in range(3))
+    idx = (ix * m[1] + iy) * m[2] + iz
+    if unused_index is not None:
+        idx = torch.where(torch.as_tensor(unused_index, device=idx.device), torch.full_like(idx, -1), idx)
+    return idx

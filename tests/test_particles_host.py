@@ -9,9 +9,7 @@ import pmpp_b200 as pb
 
 
 def _raveled(pmid, conf):
-    m = torch.tensor(conf.mesh_shape, dtype=torch.int64)
-    p = torch.remainder(pmid.to(torch.int64), m)
-    return ((p[:, 0] * m[1] + p[:, 1]) * m[2] + p[:, 2]).numpy()
+    return pb.pmid_to_idx(pmid, conf).numpy()
 
 
 def _lattice(conf):
@@ -160,3 +158,14 @@ def test_raveled_ids_and_copies_wrap_only_when_requested():
     import pytest
     with pytest.raises(TypeError):
         original.raveled_id(dtype=torch.float32)
+
+
+def test_pmid_to_idx_wraps_and_masks():
+    """core/utils.py:292-326: int32 keys, anchors wrapped, unused slots -1."""
+    conf = _small_conf(shape=(2, 2, 2), mesh=1)
+    pmid = torch.tensor([[-1, 0, 0], [0, 1, 1], [2, 0, 0], [1, 1, 1]], dtype=torch.int16)
+    idx = pb.pmid_to_idx(pmid, conf)
+    assert idx.dtype == torch.int32
+    np.testing.assert_array_equal(idx.numpy(), [4, 3, 0, 7])
+    masked = pb.pmid_to_idx(pmid, conf, unused_index=torch.tensor([False, True, False, False]))
+    np.testing.assert_array_equal(masked.numpy(), [4, -1, 0, 7])
