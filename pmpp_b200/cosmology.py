@@ -119,10 +119,15 @@ def transfer_fit(k, cosmo, conf=None):
     return out
 
 
-def boltzmann(cosmo, conf=None):
-    """Transfer and growth tables (boltzmann.py:358-398)."""
+def boltzmann(cosmo, conf=None, transfer=True, growth=True, varlin=True):
+    """Transfer and growth tables (boltzmann.py:358-398); a component switched
+    off stays unset.  The variance needs no table here (varlin integrates on
+    demand), so ``varlin`` only mirrors the reference's signature."""
     conf = cosmo.conf if conf is None else conf
-    T = transfer_fit(conf.transfer_k, cosmo, conf)
+    del varlin
+    T = transfer_fit(conf.transfer_k, cosmo, conf) if transfer else None
+    if not growth:
+        return cosmo.replace(conf=conf, transfer=T, growth=None, growth_dOm=None)
     ga = np.ascontiguousarray(conf.growth_a, dtype=np.float64)
     tab = np.zeros(6 * len(ga))
     dtab = np.zeros(6 * len(ga))
@@ -135,6 +140,8 @@ def boltzmann(cosmo, conf=None):
 def growth(a, cosmo, conf=None, order=1, deriv=0):
     """D_m and ln-a derivatives by table interpolation (growth.py:75-111)."""
     conf = cosmo.conf if conf is None else conf
+    if cosmo.growth is None:
+        raise ValueError("Growth table is empty. Call boltzmann first.")
     a = np.asarray(a, dtype=np.float64)
     xp = conf.growth_a
     fp = cosmo.growth[order - 1][deriv]
@@ -154,6 +161,10 @@ def E2(a, cosmo):
 def linear_power(k, a, cosmo, conf=None):
     """P_lin(k) [L^3] (boltzmann.py:428-484), optionally times D(a)^2."""
     conf = cosmo.conf if conf is None else conf
+    if getattr(conf, "dim", 3) != 3:
+        raise ValueError(f"dim={conf.dim} not supported")
+    if cosmo.transfer is None:
+        raise ValueError("Transfer table is empty. Call boltzmann first.")
     k = np.ascontiguousarray(k, dtype=np.float64)
     out = np.empty_like(k)
     tk = np.ascontiguousarray(conf.transfer_k, dtype=np.float64)
@@ -195,8 +206,8 @@ def varlin(R, a, cosmo, conf=None):
     is None (boltzmann.py:314-355).  Each R is evaluated by the Simpson
     quadrature of tophat_variance rather than interpolated in a table."""
     conf = cosmo.conf if conf is None else conf
-    if cosmo.transfer is None or cosmo.growth is None:
-        raise ValueError("Linear matter overdensity variance needs the boltzmann tables. Call boltzmann first.")
+    if cosmo.transfer is None or (a is not None and cosmo.growth is None):
+        raise ValueError("Linear matter overdensity variance table is empty. Call boltzmann first.")
     R = np.asarray(R, dtype=np.float64)
     s2 = np.vectorize(lambda r: tophat_variance(float(r), cosmo, conf), otypes=[np.float64])(R)
     if a is not None:

@@ -93,3 +93,42 @@ def test_cosmology_param_helpers():
     assert C.cosmology_param_values(w, ("h", "Omega_m")) == (0.7, 0.3)
     r = C.replace_cosmology_params(c, ("Omega_m", "h"), (0.31, 0.68))
     assert (r.Omega_m, r.h, c.Omega_m, c.h) == (0.31, 0.68, 0.3, 0.7)
+
+
+def test_boltzmann_contracts():
+    """Restated from the reference's tests/test_deep_boltzmann_contracts.py:19-53:
+    both Eisenstein-Hu fits are exactly 1 at k = 0, the no-wiggle fit is finite,
+    non-increasing and within 2e-3 of the baryonic one on large scales (and
+    matches the oracle); missing tables fail explicitly; switched-off
+    components stay unset; variance scales with D(a)^2."""
+    import pytest
+    from pmpp_b200 import cosmology as C
+    import pmpp_b200 as pb
+    conf = pb.Configuration(10.0, (8, 8, 8), 1, a_start=1 / 64, a_nbody_maxstep=1 / 64, device="cpu")
+    smooth_conf = pb.Configuration(10.0, (8, 8, 8), 1, a_start=1 / 64, a_nbody_maxstep=1 / 64,
+                                   transfer_fit_nowiggle=True, device="cpu")
+    cosmo = pb.SimpleLCDM(conf)
+    k = np.concatenate(([0.0], np.geomspace(1e-4, 0.5, 64)))
+    baryonic = C.transfer_fit(k, cosmo, conf)
+    smooth = C.transfer_fit(k, cosmo, smooth_conf)
+    assert np.all(np.isfinite(smooth)) and smooth[0] == 1 and baryonic[0] == 1
+    np.testing.assert_allclose(smooth[1], baryonic[1], rtol=2e-3, atol=2e-6)
+    assert np.all(np.diff(smooth) <= 1e-12)
+    np.testing.assert_allclose(smooth, ocos.transfer_fit(k, ocos.Cosmo(), nowiggle=True), rtol=1e-13, atol=1e-15)
+    empty = pb.SimpleLCDM(conf)
+    with pytest.raises(ValueError, match="Transfer table is empty"):
+        C.transfer(np.asarray([0.1]), empty, conf)
+    with pytest.raises(ValueError, match="Growth table is empty"):
+        C.growth(0.5, empty, conf)
+    with pytest.raises(ValueError, match="variance table is empty"):
+        C.varlin(1.0, None, empty, conf)
+    disabled = C.boltzmann(empty, conf, transfer=False, growth=False, varlin=False)
+    assert disabled.transfer is None and disabled.growth is None
+    complete = C.boltzmann(empty, conf)
+    radius = np.asarray([5.0, 10.0, 20.0])
+    np.testing.assert_allclose(C.varlin(radius, 0.4, complete, conf),
+                               C.varlin(radius, None, complete, conf) * C.growth(0.4, complete, conf)**2,
+                               rtol=2e-14, atol=0)
+    with pytest.raises(ValueError, match="dim=2 not supported"):
+        import types
+        C.linear_power(np.asarray([0.1]), None, complete, types.SimpleNamespace(dim=2))
