@@ -169,3 +169,16 @@ def test_pmid_to_idx_wraps_and_masks():
     np.testing.assert_array_equal(idx.numpy(), [4, 3, 0, 7])
     masked = pb.pmid_to_idx(pmid, conf, unused_index=torch.tensor([False, True, False, False]))
     np.testing.assert_array_equal(masked.numpy(), [4, -1, 0, 7])
+
+
+def test_large_meshes_keep_exact_sizes_and_ids_fail_closed():
+    """Restated from the reference's tests/test_lpt_large_index.py:46-60:
+    2048^3 sizes stay exact integers; raveled ids refuse a dtype that cannot
+    hold every mesh index."""
+    import pytest
+    conf = pb.Configuration(1.0, (2048, 2048, 2048), 1, device="cpu")
+    assert conf.ptcl_num == 8_589_934_592 and conf.mesh_size == 8_589_934_592
+    p = pb.Particles(conf, torch.tensor([[2047, 2047, 2047]], dtype=torch.int16), torch.zeros((1, 3)))
+    with pytest.raises(OverflowError):
+        p.raveled_id(dtype=torch.int32)
+    assert int(p.raveled_id()[0]) == 8_589_934_591
