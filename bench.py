@@ -10,7 +10,10 @@ particles x 32 macro steps per second.  Inputs are larger than L2.
 
 ``--impl reference`` times the CPU oracle (NumPy restatement of PM++, the
 reference's own JAX stack is not installable here) on the host cores, on a
-bounded sample of the same workload.
+bounded sample of the same workload: one forward + adjoint KDK step of a
+periodic sub-volume at the workload's resolution per bench step.  With
+``--gpus N > 1`` outside torchrun the command re-launches itself as N local
+ranks.
 """
 from __future__ import annotations
 
@@ -39,7 +42,7 @@ def parse():
     p.add_argument("--nsteps", type=int, default=32)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-learned", action="store_true")
-    p.add_argument("--cpu-ptcl", type=int, default=128)
+    p.add_argument("--cpu-ptcl", type=int, default=64)
     return p.parse_args()
 
 
@@ -123,12 +126,18 @@ def load_peaks():
 # --------------------------------------------------------------------------
 # CPU baseline: the oracle on a bounded sample
 # --------------------------------------------------------------------------
-def cpu_sample_rate(ptcl=128, mesh=2, nsteps=1, seed=0):
-    """One forward + adjoint macro step of the oracle at ptcl^3 / (mesh*ptcl)^3."""
+def cpu_sample_rate(ptcl=64, mesh=2, nsteps=1, seed=0, full_ptcl=512):
+    """One forward + adjoint KDK step of the oracle on a periodic sub-volume of the
+    workload: ptcl^3 particles on a (mesh*ptcl)^3 mesh at the workload's particle
+    spacing and cell size (1024 Mpc/h over 512 particles), the first of its 32 log
+    steps, FFTs and CIC loops threaded over the host cores.  Particle-steps/s
+    of PM depends on the size only through the FFTs' log factor, so the rate
+    stands for the full run; the line says so.  Returns (rate, seconds, sample)."""
     sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
     from oracle import cosmology as ocos
     from oracle import pm as opm
-    opm.set_fft_workers(os.cpu_count() or 1)
+    cores = os.cpu_count() or 1
+    opm.set_fft_workers(cores)
     box = 1024.0 * ptcl / 512
     a = np.geomspace(0.1, 1.0, 33)[:nsteps + 1]
     co = opm.Conf(box / ptcl, (ptcl, ) * 3, mesh_shape=mesh, a_start=0.1, a_custom=a)
@@ -143,7 +152,13 @@ def cpu_sample_rate(ptcl=128, mesh=2, nsteps=1, seed=0):
     opm.nbody_adj(pmid, d, v, acc, cot, cot, np.zeros_like(cot), co, oc, om_grads=False)
     dt = time.perf_counter() - t0
     n = ptcl**3
-    return n * nsteps / dt, dt, f"oracle fwd+adj, {ptcl}^3 particles / {mesh * ptcl}^3 mesh, {nsteps} step(s), {dt:.1f}s"
+    rate = n * nsteps / dt
+    full = full_ptcl**3 * 32 / rate
+    sample = (f"oracle (NumPy restatement, {cores} threads) forward + adjoint of {nsteps} KDK step(s) on a "
+              f"{ptcl}^3-particle / {mesh * ptcl}^3-mesh periodic sub-volume ({box:.0f} Mpc/h) at the workload's "
+              f"resolution ({1024.0 / 512:.0f} Mpc/h spacing), {dt:.2f} s; rate extrapolated to the "
+              f"{full_ptcl}^3 / {mesh * full_ptcl}^3 run: {full:.0f} s per 32-step forward + adjoint run")
+    return rate, dt, sample
 
 
 def arm_config(args, world):
@@ -157,21 +172,24 @@ def arm_config(args, world):
 
 
 def run_reference(args):
+    """The reference arm: rank 0 times the oracle on host cores (the other ranks
+    of a torchrun launch exit without work)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     rates = []
     for i in range(args.warmup + args.steps):
-        r, dt, sample = cpu_sample_rate(args.cpu_ptcl, args.mesh, 1, seed=i)
+        r, dt, sample = cpu_sample_rate(args.cpu_ptcl, args.mesh, 1, seed=i, full_ptcl=args.ptcl)
         if i >= args.warmup:
             rates.append(r)
     v = float(np.mean(rates))
     cores = os.cpu_count() or 1
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     line = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * (args.cpu_ptcl**3) / v, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": arm_config(args, args.gpus),
+        "config": arm_config(args, world),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -299,7 +317,7 @@ def run_ours(args):
         learned = pl.evaluate(wpath)
     cpu = None
     if not args.no_cpu_baseline:
-        r, dt, sample = cpu_sample_rate(args.cpu_ptcl, args.mesh, 1)
+        r, dt, sample = cpu_sample_rate(args.cpu_ptcl, args.mesh, 1, full_ptcl=args.ptcl)
         cpu = {"value": r, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port", "sample": sample}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -323,8 +341,26 @@ def run_ours(args):
     replicas.teardown(world)
 
 
+def self_launch(args):
+    """With --gpus N > 1 outside torchrun, re-run this command as N local ranks
+    (one process per GPU, rendezvous on 127.0.0.1) and return their exit code;
+    None when this process is already a rank (or N == 1)."""
+    if args.gpus <= 1 or "WORLD_SIZE" in os.environ:
+        return None
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
+    rc = self_launch(args)
+    if rc is not None:
+        sys.exit(rc)
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -46,7 +46,31 @@ _fft = _FFT()
 
 
 def set_fft_workers(n):
+    """Threads for the FFTs and the particle loops of the CIC functions (the
+    timed CPU baseline); 1 (the default, used by the tests) is plain serial
+    NumPy."""
     _fft.workers = int(n)
+
+
+def _chunks(n):
+    """Particle ranges of the threaded CIC (None: run serially)."""
+    w = _fft.workers
+    if w <= 1 or n < 65536:
+        return None
+    b = np.linspace(0, n, w + 1).astype(np.int64)
+    return [(int(b[i]), int(b[i + 1])) for i in range(w) if b[i + 1] > b[i]]
+
+
+def _pmap(fn, ranges):
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(len(ranges)) as ex:
+        return list(ex.map(lambda r: fn(*r), ranges))
+
+
+def _rows(x, lo, hi):
+    """Particle slice of a per-particle array (scalars pass through)."""
+    x = np.asarray(x) if x is not None else None
+    return x if x is None or x.ndim == 0 else x[lo:hi]
 
 
 class Conf:
@@ -280,6 +304,18 @@ def scatter(pmid, disp, conf, val=None, mesh_shape=None):
     from float-dtype weights (the reference accumulates with unordered
     float atomics; the difference is below the dtype's rounding)."""
     mesh_shape = conf.mesh_shape if mesh_shape is None else mesh_shape
+    ranges = _chunks(pmid.shape[0])
+    if ranges is not None:
+        # threaded: partial meshes of particle chunks, summed in chunk order
+        if val is None:
+            val = default_val(conf)
+        parts = _pmap(lambda lo, hi: _scatter1(pmid[lo:hi], disp[lo:hi], conf, _rows(val, lo, hi), mesh_shape),
+                      ranges)
+        return sum(parts[1:], parts[0])
+    return _scatter1(pmid, disp, conf, val, mesh_shape)
+
+
+def _scatter1(pmid, disp, conf, val, mesh_shape):
     cell, d, fl = enmesh(pmid, disp, conf, mesh_shape)
     w, _ = corner_weights(d, fl, conf.float_dtype)
     idx = corner_index(cell, mesh_shape)
@@ -300,6 +336,13 @@ def scatter(pmid, disp, conf, val=None, mesh_shape=None):
 
 def gather(pmid, disp, conf, mesh):
     """CIC interpolation, cic/gather.py:452-472.  mesh: (M...) or (C, M...)."""
+    ranges = _chunks(pmid.shape[0])
+    if ranges is not None:
+        return np.concatenate(_pmap(lambda lo, hi: _gather1(pmid[lo:hi], disp[lo:hi], conf, mesh), ranges))
+    return _gather1(pmid, disp, conf, mesh)
+
+
+def _gather1(pmid, disp, conf, mesh):
     mesh_shape = mesh.shape[-3:]
     cell, d, fl = enmesh(pmid, disp, conf, mesh_shape)
     w, _ = corner_weights(d, fl, conf.float_dtype)
@@ -314,6 +357,17 @@ def gather(pmid, disp, conf, mesh):
 def scatter_vjp(pmid, disp, conf, mesh_cot, val=None):
     """cic/scatter.py:341-437: disp_cot = sum_b mesh_cot[i_b] val grad_b / cell,
     val_cot = sum_b mesh_cot[i_b] w_b (summed over particles for scalar val)."""
+    ranges = _chunks(pmid.shape[0])
+    if ranges is not None:
+        parts = _pmap(lambda lo, hi: _scatter_vjp1(pmid[lo:hi], disp[lo:hi], conf, mesh_cot, _rows(val, lo, hi)),
+                      ranges)
+        dc = np.concatenate([p[0] for p in parts])
+        vcs = [p[1] for p in parts]
+        return dc, (sum(vcs[1:], vcs[0]) if np.ndim(vcs[0]) == 0 else np.concatenate(vcs))
+    return _scatter_vjp1(pmid, disp, conf, mesh_cot, val)
+
+
+def _scatter_vjp1(pmid, disp, conf, mesh_cot, val):
     mesh_shape = mesh_cot.shape[-3:]
     cell, d, fl = enmesh(pmid, disp, conf, mesh_shape)
     w, g = corner_weights(d, fl, conf.float_dtype)
@@ -340,6 +394,15 @@ def scatter_vjp(pmid, disp, conf, mesh_cot, val=None):
 def gather_vjp(pmid, disp, conf, mesh, val_cot):
     """cic/gather.py:475-548: disp_cot = sum_b (sum_c val_cot mesh_c[i_b]) grad_b / cell,
     mesh_cot_c = scatter of val_cot_c w_b."""
+    ranges = _chunks(pmid.shape[0])
+    if ranges is not None:
+        parts = _pmap(lambda lo, hi: _gather_vjp1(pmid[lo:hi], disp[lo:hi], conf, mesh, val_cot[lo:hi]), ranges)
+        mcs = [p[1] for p in parts]
+        return np.concatenate([p[0] for p in parts]), sum(mcs[1:], mcs[0])
+    return _gather_vjp1(pmid, disp, conf, mesh, val_cot)
+
+
+def _gather_vjp1(pmid, disp, conf, mesh, val_cot):
     mesh_shape = mesh.shape[-3:]
     cell, d, fl = enmesh(pmid, disp, conf, mesh_shape)
     w, g = corner_weights(d, fl, conf.float_dtype)

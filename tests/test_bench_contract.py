@@ -48,3 +48,19 @@ def test_roofline_byte_models():
         ratio = b.MEASURED_TRAFFIC_PER_PARTICLE[name] * N / algorithmic_bytes(name, N, M)
         assert 0.95 < ratio < 1.05, (name, ratio)
     assert b.STAGE_VARIANTS["gather"] == "gather_kick"
+
+
+def test_gpus_flag_self_launches_ranks():
+    """`bench.py --gpus 2` outside torchrun re-runs itself as two local ranks
+    (torch.distributed.run, rendezvous on 127.0.0.1); exactly one line, from rank
+    0, reports the job's two ranks.  The reference arm runs here (no GPU)."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                          "--steps", "1", "--warmup", "0", "--cpu-ptcl", "16"], capture_output=True, text=True,
+                         timeout=600, cwd=ROOT, env=env)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, out.stdout
+    d = json.loads(lines[0])
+    assert d["n_gpus"] == 2 and d["config"]["parallelism"] == "replicas x2"
+    assert "sub-volume" in d["cpu_baseline"]["sample"]
