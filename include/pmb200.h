@@ -7,8 +7,14 @@
  * as the reference's XLA FFI handlers, cuda/route_kernels.cu:1-7).  All
  * pointers are device pointers unless stated otherwise.  Return value: 0 on
  * success, a negative pmb status otherwise (-1 invalid argument, -2 CUDA
- * error, -3 cuFFT error, -4 unsupported shape, -5 scratch too small); the
+ * error, -3 cuFFT error, -4 unsupported shape, -5 scratch too small, -6 the
+ * device flagged bad input or a timed-out wait, see pmb_device_status); the
  * message of the last failure on the calling thread is pmb_last_error().
+ * Exceptions to "never allocates, never synchronises": the first call of a
+ * cuFFT-route entry point for a new mesh shape creates its plan (cuFFT may
+ * allocate and synchronise then; later calls reuse it, with the caller's work
+ * area bound), and the status queries pmb_sorted_status / pmb_device_status /
+ * pmb_*_timeouts are synchronous by design.
  *
  * Layouts (C order): pmid int16 (n,3); disp/vel/acc float (n,3); meshes float
  * (C,nx,ny,nz) planar channels; spectra float2 (C,nx,ny,nz/2+1).
@@ -35,28 +41,47 @@ const char* pmb_last_error(void);
  * ordering that cuda/route_kernels.cu:131-145, 615-724 maintain, using the
  * binning of cic/enmesh.py:139-147.  Particles are counting-sorted by the
  * mesh row (x, y) of their lower CIC corner; `sorted` receives 16-byte
- * records (fx, fy, fz, raveled cell key), the permutation (uint32) and the
- * row offsets (uint32, nx*ny+1).  With vel != NULL the drift
- * disp += vel * drift (nbody/integrator.py:223-225) is applied first and
- * written back to disp. */
+ * records (fx, fy, fz, raveled cell key), the permutation (uint32), the
+ * row offsets (uint32, nx*ny+1) and a status word.  With vel != NULL the
+ * drift disp += vel * drift (nbody/integrator.py:223-225) is applied first and
+ * written back to disp.  A displacement that is NaN or infinite (after the
+ * drift) is binned at its anchor cell and raises flag 2 in the status word
+ * (the reference's fail-closed checks, core/utils.py:206-231); every later
+ * scatter, gather or adjoint given a flagged buffer writes nothing. */
 int64_t pmb_sorted_bytes(int64_t n, int nx, int ny, int nz);
 int64_t pmb_sort_scratch_bytes(int64_t n, int nx, int ny, int nz);
 int pmb_sort_rows(const int16_t* pmid, float* disp, const float* vel, float drift, int64_t n, int nx, int ny, int nz,
                   float cell, void* sorted, void* scratch, int64_t scratch_bytes, void* stream);
+/* pmb_sort_rows for the reference's scatter / gather options (cic/scatter.py:
+ * 235-312, cic/gather.py:414-472; cic/pallas.py:133-141, 225-238): the mesh
+ * origin sits at (ox, oy, oz) in the particles' frame -- split on the host
+ * into whole cells q = floor(o / cell) and the remainder o - q * cell (rounded
+ * once to float), the binning is (disp - remainder) / cell from the anchor
+ * pmid - q -- and particles with valid[p] == 0 (uint8, device; NULL = all
+ * valid) are left out of every row: they deposit nothing, gather 0, leave vel
+ * unkicked and take zero adjoint terms (or keep disp_cot when accumulating).
+ * Their records follow the last row, from offs[nx*ny] to n, with the key
+ * 0xFFFFFFFF.  A zero offset and no mask give pmb_sort_rows' records. */
+int pmb_sort_rows_ex(const int16_t* pmid, float* disp, const float* vel, float drift, int64_t n, int nx, int ny,
+                     int nz, float cell, float ox, float oy, float oz, const uint8_t* valid, void* sorted,
+                     void* scratch, int64_t scratch_bytes, void* stream);
 /* Density scatter that allocates nothing and takes no workspace.  No
  * counterpart in the reference: it exists for callers that may not allocate
  * device memory (framework plugins whose host program owns every allocation
  * and hands them no scratch).  Same result as pmb_sort_rows +
  * pmb_scatter_rows (mode 0, constant val).  Its scratch is a fixed 32 MiB
  * device array inside the library (held on every GPU that loads it until
- * exit); problems needing more (28 B per particle + ~8 B per mesh row) are
- * rejected.  Calls share that array, so calls that overlap on the GPU race;
- * the first call on a device resolves the array's address and should come
- * before any stream capture. */
+ * exit); problems needing more (28 B per particle + 12 B per mesh row) are
+ * rejected before any work is queued.  Calls share that array, so calls that
+ * overlap on the GPU race; the first call on a device resolves the array's
+ * address and should come before any stream capture. */
 int pmb_scatter_density_noalloc(const int16_t* pmid, const float* disp, int64_t n, int nx, int ny, int nz, float cell,
                                 float val, float* out, void* stream);
 /* Stable per-cell order of the reference key ((x*My+y)*Mz+z), ties keep
  * source order: keys_out[n] (uint32) and perm_out[n] (uint32). */
+/* Status word of a sorted buffer (DeviceFlag bits: 2 non-finite displacement,
+ * 4 non-finite deposit value).  Synchronises `stream`. */
+int pmb_sorted_status(const void* sorted, int64_t n, int nx, int ny, int nz, uint32_t* flags, void* stream);
 int pmb_sort_by_cell(const int16_t* pmid, const float* disp, int64_t n, int nx, int ny, int nz, float cell,
                      uint32_t* keys_out, uint32_t* perm_out, void* scratch, int64_t scratch_bytes, void* stream);
 int64_t pmb_sort_by_cell_scratch_bytes(int64_t n, int nx, int ny, int nz);
@@ -68,7 +93,9 @@ int64_t pmb_sort_by_cell_scratch_bytes(int64_t n, int nx, int ny, int nz);
  * (as pmb_interp_grad_rows writes it to u_sorted).  mode 0 writes the sum;
  * mode 1 writes (sum - 1) * src_mul (the Poisson source of
  * nbody/gravity.py:628-630).  The sum is exact in 64-bit fixed point, so the
- * result does not depend on particle order.  scratch: 16 bytes. */
+ * result does not depend on particle order.  A NaN or infinite val leaves out
+ * untouched and raises flag 4 (pmb_sorted_status, pmb_device_status).
+ * scratch: 16 bytes. */
 int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* val, int val_sorted,
                      float val_const, int mode, float src_mul, float* out, void* scratch16, void* stream);
 /* Gather (cic/gather.py:452-472, cic/pallas.py:305-318): out[p,c]; with
@@ -87,6 +114,32 @@ int pmb_interp_grad_rows(const void* sorted, int64_t n, int nx, int ny, int nz, 
                          const float* u, float u_const, float cell, int accumulate, float* disp_cot, float* wsum,
                          float* u_sorted, void* stream);
 
+/* CIC onto a mesh whose cell size cell2 differs from the particles' cell
+ * (the explicit cell_size argument of cic/scatter.py:235, cic/gather.py:414;
+ * semantics of cic/pallas.py:192-222 and cic/enmesh.py:108-127): per axis,
+ * p = mod((pmid * cell + disp) - o, g * cell) on the particles' periodic
+ * (gx, gy, gz) mesh; corner b sits at i_b = floor(mod(p + b * cell2, g *
+ * cell) / cell2) of the (nx, ny, nz) target mesh with the folded offset
+ * p - i_b * cell2 giving weight 1 - |.| / cell2; corners outside the target
+ * mesh are dropped.  valid (uint8, device, NULL = all valid) masks particles
+ * as in pmb_sort_rows_ex.  No cell sort: the deposit sums exact 64-bit fixed
+ * point with global integer atomics (deterministic) in the scratch of
+ * pmb_cic_general_scratch_bytes and writes out = the deposit (not added to
+ * out); the gather writes out[p, c]; interp_grad writes disp_cot[p] = sum_b
+ * (sum_c u[p,c] mesh_c[i_b]) grad w_b / cell2 and wsum[p, c] (may be NULL). */
+int64_t pmb_cic_general_scratch_bytes(int nx, int ny, int nz, int C);
+int pmb_cic_general_scatter(const int16_t* pmid, const float* disp, const uint8_t* valid, int64_t n, int gx, int gy,
+                            int gz, float cell, float ox, float oy, float oz, float cell2, int nx, int ny, int nz,
+                            int C, const float* val, float val_const, float* out, void* scratch,
+                            int64_t scratch_bytes, void* stream);
+int pmb_cic_general_gather(const int16_t* pmid, const float* disp, const uint8_t* valid, int64_t n, int gx, int gy,
+                           int gz, float cell, float ox, float oy, float oz, float cell2, int nx, int ny, int nz,
+                           int C, const float* mesh, float* out, void* stream);
+int pmb_cic_general_interp_grad(const int16_t* pmid, const float* disp, const uint8_t* valid, int64_t n, int gx,
+                                int gy, int gz, float cell, float ox, float oy, float oz, float cell2, int nx, int ny,
+                                int nz, int C, const float* mesh, const float* u, float u_const, float* disp_cot,
+                                float* wsum, void* stream);
+
 /* Mesh-row staging of pmb_gather_rows / pmb_interp_grad_rows (process-wide):
  * 0 (default) direct corner loads; 1 stage the rows a tile of particle rows
  * touches into shared memory with bulk asynchronous copies when the tile
@@ -95,9 +148,21 @@ int pmb_interp_grad_rows(const void* sorted, int64_t n, int nx, int ny, int nz, 
  * particles and slower for clustered ones. */
 int pmb_set_gather_staging(int mode);
 /* Count of bounded device waits (bulk-copy completions in the staged
- * gathers) that gave up since the library was loaded; 0 in a healthy run.
- * Synchronous: reads a device counter. */
+ * gathers) that gave up since the library was loaded or the last
+ * pmb_device_status; 0 in a healthy run.  Synchronous: reads a device
+ * counter. */
 int pmb_wait_timeouts(uint32_t* count);
+/* Poll limit of the first bounded wait of every staged gather and FFT pass
+ * (process-wide; a negative value restores the default 2^22 polls, 0 gives up
+ * at once).  After a timeout a CTA still waits (2^22 polls) for the copies it
+ * has in flight, raises the timeout counter and returns without writing the
+ * tile: that launch's results are invalid. */
+int pmb_set_wait_limit(int64_t polls);
+/* Device-wide flags since the last call, cleared on return: 1 a bounded wait
+ * gave up (either timeout counter), 2 a non-finite displacement reached a cell
+ * sort, 4 a non-finite value reached a deposit.  Returns 0 when none is set,
+ * else -6 with the conditions in pmb_last_error().  Synchronises the device. */
+int pmb_device_status(uint32_t* flags);
 
 /* ---------------- spectral ------------------------------------------------
  * 3-D R2C / C2R (numpy convention: forward unnormalised, the inverse is NOT

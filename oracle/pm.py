@@ -101,6 +101,21 @@ class Conf:
         self.kvec_spacing = fftfreq(self.ptcl_grid_shape, self.ptcl_spacing, self.float_dtype)
         self.neg_ik = tuple(self._neg_k(k) for k in self.kvec)
 
+    def fastpm_neg_k(self, k):
+        """Real factor c with neg_ik = i*c for FastPM's 4-point derivative,
+        (8 sin(k dx) - sin(2 k dx)) / (6 dx) (gravity.py:385-387), in the float dtype."""
+        f = self.float_dtype.type
+        phase = (k * f(self.cell_size)).astype(self.float_dtype)
+        d = ((f(8.0) * np.sin(phase)).astype(self.float_dtype) - np.sin(f(2.0) * phase)).astype(self.float_dtype)
+        return (-(d / f(6.0 * self.cell_size))).astype(self.float_dtype)
+
+    def derivative_factors(self, gradient="spectral"):
+        if gradient == "spectral":
+            return self.neg_ik
+        if gradient == "fastpm_4point":
+            return tuple(self.fastpm_neg_k(k) for k in self.kvec)
+        raise ValueError(f"Unsupported force-gradient kernel {gradient!r}.")
+
     def _neg_k(self, k):
         """Real factor c with neg_ik = i*c (configuration.py:370-376)."""
         f = self.float_dtype.type
@@ -235,17 +250,29 @@ def positions(pmid, disp, conf):
 # --------------------------------------------------------------------------
 # CIC binning, cic/enmesh.py:34-165 (a2=None branch) and pallas.py:225-256
 # --------------------------------------------------------------------------
-def enmesh(pmid, disp, conf, mesh_shape=None):
+def offset_shift(offset, cell, dtype):
+    """Mesh origin offset as whole cells q = floor(o / cell) and the remainder
+    o - q * cell rounded once to the float dtype (the common-grid offset path,
+    cic/pallas.py:225-238, cic/enmesh.py:128-147).  The offset itself is first
+    rounded to the float dtype, as the reference casts it (pallas.py:108-111)."""
+    o = np.broadcast_to(np.asarray(offset, dtype=dtype).astype(np.float64), (3, ))
+    q = np.floor(o / float(cell))
+    return q.astype(np.int64), (o - q * float(cell)).astype(dtype)
+
+
+def enmesh(pmid, disp, conf, mesh_shape=None, offset=0):
     """Return lower-corner cells (N,3) int64, normalised fractions (N,3).
 
     The float arithmetic follows enmesh.py:139-143 in ``conf.float_dtype``:
-    d = disp / cell, i = floor(d), f = d - i, with the neighbour deltas
-    d - (i + b) formed later in :func:`corner_weights`."""
+    d = (disp - r) / cell, i = floor(d), f = d - i, with the neighbour deltas
+    d - (i + b) formed later in :func:`corner_weights`; the offset's whole
+    cells q shift the anchor (r = q = 0 without an offset)."""
     mesh_shape = conf.mesh_shape if mesh_shape is None else mesh_shape
     ft = conf.float_dtype.type
-    d = disp.astype(conf.float_dtype) / ft(conf.cell_size)
+    q, r = offset_shift(offset, conf.cell_size, conf.float_dtype)
+    d = (disp.astype(conf.float_dtype) - r) / ft(conf.cell_size)
     fl = np.floor(d)
-    cell = (pmid.astype(np.int64) + fl.astype(np.int64)) % np.array(mesh_shape)
+    cell = (pmid.astype(np.int64) - q + fl.astype(np.int64)) % np.array(mesh_shape)
     return cell, d, fl
 
 
@@ -278,6 +305,77 @@ def corner_index(cell, mesh_shape):
     return idx
 
 
+def _fmod_floor(x, y):
+    r = np.fmod(x, y)
+    return np.where((r != 0) & ((r < 0) != (y < 0)), r + y, r).astype(x.dtype)
+
+
+def explicit_corners(pmid, disp, conf, offset, cell2, mesh_shape):
+    """CIC onto a mesh of cell size cell2 (the explicit cell_size branch,
+    cic/pallas.py:192-222, cic/enmesh.py:108-127), in the float dtype: per
+    axis p = mod((pmid a1 + disp) - o, L a1); for bit b, i_b = floor(mod(p +
+    b a2, L a1) / a2), delta = p - i_b a2 folded into the half period; weight
+    1 - |delta / a2|.  Returns idx (N,8) with -1 for corners outside the
+    target mesh, w (N,8) and the weight gradients g (N,8,3) (before / a2)."""
+    dt = conf.float_dtype
+    ft = dt.type
+    a1, a2 = ft(conf.cell_size), ft(cell2)
+    o = np.broadcast_to(np.asarray(offset, dtype=dt), (3, ))
+    n = pmid.shape[0]
+    ia, wa, sa = np.empty((n, 3, 2), np.int64), np.empty((n, 3, 2), dt), np.empty((n, 3, 2), dt)
+    for ax in range(3):
+        period = (ft(conf.mesh_shape[ax]) * a1).astype(dt)
+        p = ((pmid[:, ax].astype(dt) * a1).astype(dt) + disp[:, ax].astype(dt)).astype(dt)
+        p = _fmod_floor((p - o[ax]).astype(dt), period)
+        for b in range(2):
+            npos = _fmod_floor((p + ft(b) * a2).astype(dt), period)
+            i = np.floor((npos / a2).astype(dt)).astype(np.int64)
+            delta = (p - (i.astype(dt) * a2).astype(dt)).astype(dt)
+            half = (ft(0.5) * period).astype(dt)
+            delta = np.where(delta > half, delta - period, delta).astype(dt)
+            delta = np.where(delta < -half, delta + period, delta).astype(dt)
+            q = (delta / a2).astype(dt)
+            wa[:, ax, b] = (ft(1) - np.abs(q)).astype(dt)
+            sa[:, ax, b] = np.where(q < 0, ft(1), np.where(q > 0, ft(-1), ft(0)))
+            ia[:, ax, b] = np.where((i >= 0) & (i < mesh_shape[ax]), i, -1)
+    idx = np.empty((n, 8), np.int64)
+    w = np.empty((n, 8), dt)
+    g = np.empty((n, 8, 3), dt)
+    for c in range(8):
+        b = NEIGHBORS[c]
+        ix, iy, iz = ia[:, 0, b[0]], ia[:, 1, b[1]], ia[:, 2, b[2]]
+        wx, wy, wz = wa[:, 0, b[0]], wa[:, 1, b[1]], wa[:, 2, b[2]]
+        sx, sy, sz = sa[:, 0, b[0]], sa[:, 1, b[1]], sa[:, 2, b[2]]
+        ok = (ix >= 0) & (iy >= 0) & (iz >= 0)
+        idx[:, c] = np.where(ok, (ix * mesh_shape[1] + iy) * mesh_shape[2] + iz, -1)
+        w[:, c] = (wx * wy) * wz
+        g[:, c, 0] = (sx * wy) * wz
+        g[:, c, 1] = (sy * wz) * wx
+        g[:, c, 2] = (sz * wx) * wy
+    return idx, w, g
+
+
+def corners(pmid, disp, conf, mesh_shape, offset=0, cell_size=None, valid=None):
+    """Raveled corner indices (N,8; -1 = dropped), weights, weight gradients and
+    the cell size the gradients divide by, for either grid path; particles with
+    valid == False drop every corner (cic/pallas.py:133-141)."""
+    if cell_size is None:
+        cell, d, fl = enmesh(pmid, disp, conf, mesh_shape, offset)
+        w, g = corner_weights(d, fl, conf.float_dtype)
+        idx, a = corner_index(cell, mesh_shape), conf.cell_size
+    else:
+        idx, w, g = explicit_corners(pmid, disp, conf, offset, cell_size, mesh_shape)
+        a = cell_size
+    if valid is not None:
+        idx = np.where(np.asarray(valid, dtype=bool)[:, None], idx, -1)
+    return idx, w, g, a
+
+
+def _take(chan, idx):
+    """chan[idx] with dropped corners (-1) reading 0."""
+    return np.where(idx >= 0, chan[np.maximum(idx, 0)], 0.0)
+
+
 def cell_key(pmid, disp, conf):
     """Raveled lower-corner cell key ((x*My)+y)*Mz+z (core/utils.py:292-326)."""
     cell, _, _ = enmesh(pmid, disp, conf)
@@ -297,81 +395,81 @@ def default_val(conf):
     return conf.float_dtype.type(conf.mesh_size / conf.ptcl_num)
 
 
-def scatter(pmid, disp, conf, val=None, mesh_shape=None):
+def scatter(pmid, disp, conf, val=None, mesh_shape=None, offset=0, cell_size=None, valid=None):
     """CIC deposit, cic/scatter.py:315-338.  val: scalar, (N,) or (N,C).
 
     Returns a float64 mesh (M...) or (C, M...) accumulated exactly in float64
     from float-dtype weights (the reference accumulates with unordered
     float atomics; the difference is below the dtype's rounding)."""
     mesh_shape = conf.mesh_shape if mesh_shape is None else mesh_shape
+    kw = dict(offset=offset, cell_size=cell_size)
     ranges = _chunks(pmid.shape[0])
     if ranges is not None:
         # threaded: partial meshes of particle chunks, summed in chunk order
         if val is None:
             val = default_val(conf)
-        parts = _pmap(lambda lo, hi: _scatter1(pmid[lo:hi], disp[lo:hi], conf, _rows(val, lo, hi), mesh_shape),
-                      ranges)
+        parts = _pmap(lambda lo, hi: _scatter1(pmid[lo:hi], disp[lo:hi], conf, _rows(val, lo, hi), mesh_shape,
+                                               valid=_rows(valid, lo, hi), **kw), ranges)
         return sum(parts[1:], parts[0])
-    return _scatter1(pmid, disp, conf, val, mesh_shape)
+    return _scatter1(pmid, disp, conf, val, mesh_shape, valid=valid, **kw)
 
 
-def _scatter1(pmid, disp, conf, val, mesh_shape):
-    cell, d, fl = enmesh(pmid, disp, conf, mesh_shape)
-    w, _ = corner_weights(d, fl, conf.float_dtype)
-    idx = corner_index(cell, mesh_shape)
+def _scatter1(pmid, disp, conf, val, mesh_shape, offset=0, cell_size=None, valid=None):
+    idx, w, _, _ = corners(pmid, disp, conf, mesh_shape, offset, cell_size, valid)
+    keep = idx >= 0
     M = math.prod(mesh_shape)
     if val is None:
         val = default_val(conf)
     val = np.asarray(val, dtype=conf.float_dtype)
     if val.ndim <= 1:
         vw = (val[:, None] if val.ndim == 1 else val) * w
-        out = np.bincount(idx.ravel(), weights=vw.astype(np.float64).ravel(), minlength=M)
+        vw = np.broadcast_to(vw, idx.shape)
+        out = np.bincount(idx[keep], weights=vw[keep].astype(np.float64), minlength=M)
         return out.reshape(mesh_shape)
     outs = []
     for c in range(val.shape[1]):
         vw = val[:, c, None] * w
-        outs.append(np.bincount(idx.ravel(), weights=vw.astype(np.float64).ravel(), minlength=M).reshape(mesh_shape))
+        outs.append(np.bincount(idx[keep], weights=vw[keep].astype(np.float64), minlength=M).reshape(mesh_shape))
     return np.stack(outs)
 
 
-def gather(pmid, disp, conf, mesh):
+def gather(pmid, disp, conf, mesh, offset=0, cell_size=None, valid=None):
     """CIC interpolation, cic/gather.py:452-472.  mesh: (M...) or (C, M...)."""
+    kw = dict(offset=offset, cell_size=cell_size)
     ranges = _chunks(pmid.shape[0])
     if ranges is not None:
-        return np.concatenate(_pmap(lambda lo, hi: _gather1(pmid[lo:hi], disp[lo:hi], conf, mesh), ranges))
-    return _gather1(pmid, disp, conf, mesh)
+        return np.concatenate(_pmap(lambda lo, hi: _gather1(pmid[lo:hi], disp[lo:hi], conf, mesh,
+                                                            valid=_rows(valid, lo, hi), **kw), ranges))
+    return _gather1(pmid, disp, conf, mesh, valid=valid, **kw)
 
 
-def _gather1(pmid, disp, conf, mesh):
+def _gather1(pmid, disp, conf, mesh, offset=0, cell_size=None, valid=None):
     mesh_shape = mesh.shape[-3:]
-    cell, d, fl = enmesh(pmid, disp, conf, mesh_shape)
-    w, _ = corner_weights(d, fl, conf.float_dtype)
-    idx = corner_index(cell, mesh_shape)
+    idx, w, _, _ = corners(pmid, disp, conf, mesh_shape, offset, cell_size, valid)
     chans = mesh.reshape(-1, math.prod(mesh_shape)) if mesh.ndim == 4 else mesh.reshape(1, -1)
     out = np.empty((pmid.shape[0], chans.shape[0]), dtype=np.float64)
     for c in range(chans.shape[0]):
-        out[:, c] = (chans[c][idx] * w).sum(axis=1)
+        out[:, c] = (_take(chans[c], idx) * w).sum(axis=1)
     return out if mesh.ndim == 4 else out[:, 0]
 
 
-def scatter_vjp(pmid, disp, conf, mesh_cot, val=None):
+def scatter_vjp(pmid, disp, conf, mesh_cot, val=None, offset=0, cell_size=None, valid=None):
     """cic/scatter.py:341-437: disp_cot = sum_b mesh_cot[i_b] val grad_b / cell,
     val_cot = sum_b mesh_cot[i_b] w_b (summed over particles for scalar val)."""
+    kw = dict(offset=offset, cell_size=cell_size)
     ranges = _chunks(pmid.shape[0])
     if ranges is not None:
-        parts = _pmap(lambda lo, hi: _scatter_vjp1(pmid[lo:hi], disp[lo:hi], conf, mesh_cot, _rows(val, lo, hi)),
-                      ranges)
+        parts = _pmap(lambda lo, hi: _scatter_vjp1(pmid[lo:hi], disp[lo:hi], conf, mesh_cot, _rows(val, lo, hi),
+                                                   valid=_rows(valid, lo, hi), **kw), ranges)
         dc = np.concatenate([p[0] for p in parts])
         vcs = [p[1] for p in parts]
         return dc, (sum(vcs[1:], vcs[0]) if np.ndim(vcs[0]) == 0 else np.concatenate(vcs))
-    return _scatter_vjp1(pmid, disp, conf, mesh_cot, val)
+    return _scatter_vjp1(pmid, disp, conf, mesh_cot, val, valid=valid, **kw)
 
 
-def _scatter_vjp1(pmid, disp, conf, mesh_cot, val):
+def _scatter_vjp1(pmid, disp, conf, mesh_cot, val, offset=0, cell_size=None, valid=None):
     mesh_shape = mesh_cot.shape[-3:]
-    cell, d, fl = enmesh(pmid, disp, conf, mesh_shape)
-    w, g = corner_weights(d, fl, conf.float_dtype)
-    idx = corner_index(cell, mesh_shape)
+    idx, w, g, a = corners(pmid, disp, conf, mesh_shape, offset, cell_size, valid)
     if val is None:
         val = default_val(conf)
     val = np.asarray(val, dtype=np.float64)
@@ -380,10 +478,10 @@ def _scatter_vjp1(pmid, disp, conf, mesh_cot, val):
     inner = np.zeros(idx.shape, dtype=np.float64)
     val_cot = np.zeros((pmid.shape[0], chans.shape[0]))
     for c in range(chans.shape[0]):
-        mc = chans[c][idx]
+        mc = _take(chans[c], idx)
         inner += mc * vals[:, min(c, vals.shape[1] - 1)][:, None]
         val_cot[:, c] = (mc * w).sum(axis=1)
-    disp_cot = (inner[..., None] * g).sum(axis=1) / conf.cell_size
+    disp_cot = (inner[..., None] * g).sum(axis=1) / a
     if val.ndim == 0:
         val_cot = val_cot.sum()
     elif val.ndim == 1:
@@ -391,31 +489,33 @@ def _scatter_vjp1(pmid, disp, conf, mesh_cot, val):
     return disp_cot, val_cot
 
 
-def gather_vjp(pmid, disp, conf, mesh, val_cot):
+def gather_vjp(pmid, disp, conf, mesh, val_cot, offset=0, cell_size=None, valid=None):
     """cic/gather.py:475-548: disp_cot = sum_b (sum_c val_cot mesh_c[i_b]) grad_b / cell,
     mesh_cot_c = scatter of val_cot_c w_b."""
+    kw = dict(offset=offset, cell_size=cell_size)
     ranges = _chunks(pmid.shape[0])
     if ranges is not None:
-        parts = _pmap(lambda lo, hi: _gather_vjp1(pmid[lo:hi], disp[lo:hi], conf, mesh, val_cot[lo:hi]), ranges)
+        parts = _pmap(lambda lo, hi: _gather_vjp1(pmid[lo:hi], disp[lo:hi], conf, mesh, val_cot[lo:hi],
+                                                  valid=_rows(valid, lo, hi), **kw), ranges)
         mcs = [p[1] for p in parts]
         return np.concatenate([p[0] for p in parts]), sum(mcs[1:], mcs[0])
-    return _gather_vjp1(pmid, disp, conf, mesh, val_cot)
+    return _gather_vjp1(pmid, disp, conf, mesh, val_cot, valid=valid, **kw)
 
 
-def _gather_vjp1(pmid, disp, conf, mesh, val_cot):
+def _gather_vjp1(pmid, disp, conf, mesh, val_cot, offset=0, cell_size=None, valid=None):
     mesh_shape = mesh.shape[-3:]
-    cell, d, fl = enmesh(pmid, disp, conf, mesh_shape)
-    w, g = corner_weights(d, fl, conf.float_dtype)
-    idx = corner_index(cell, mesh_shape)
+    idx, w, g, a = corners(pmid, disp, conf, mesh_shape, offset, cell_size, valid)
+    keep = idx >= 0
     chans = mesh.reshape(-1, math.prod(mesh_shape)) if mesh.ndim == 4 else mesh.reshape(1, -1)
     vc = val_cot.reshape(pmid.shape[0], -1).astype(np.float64)
     inner = np.zeros(idx.shape, dtype=np.float64)
     M = math.prod(mesh_shape)
     mesh_cot = []
     for c in range(chans.shape[0]):
-        inner += vc[:, c, None] * chans[c][idx]
-        mesh_cot.append(np.bincount(idx.ravel(), weights=(vc[:, c, None] * w).ravel(), minlength=M).reshape(mesh_shape))
-    disp_cot = (inner[..., None] * g).sum(axis=1) / conf.cell_size
+        inner += vc[:, c, None] * _take(chans[c], idx)
+        wc = vc[:, c, None] * w
+        mesh_cot.append(np.bincount(idx[keep], weights=wc[keep], minlength=M).reshape(mesh_shape))
+    disp_cot = (inner[..., None] * g).sum(axis=1) / a
     mesh_cot = np.stack(mesh_cot) if mesh.ndim == 4 else mesh_cot[0]
     return disp_cot, mesh_cot
 
@@ -483,30 +583,32 @@ def potential_kernel(conf, green_kernel="continuum", transfer=None):
     return G
 
 
-def force_meshes(rho, conf, Omega_m, kernel=None):
-    """Density (M) -> 3 real force meshes, gravity.py:626-633 + 506-543."""
+def force_meshes(rho, conf, Omega_m, kernel=None, gradient="spectral"):
+    """Density (M) -> 3 real force meshes, gravity.py:626-633 + 506-543;
+    gradient "fastpm_4point" takes FastPM's derivative (gravity.py:355-391)."""
     kernel = potential_kernel(conf) if kernel is None else kernel
+    cs = conf.derivative_factors(gradient)
     om = float(np.float32(Omega_m)) if conf.float_dtype == np.float32 else float(Omega_m)
     S = (rho - 1.0) * (1.5 * om)
     Sh = _fft.rfftn(S)
     pot = Sh * kernel
     out = []
     for d in range(3):
-        c = conf.neg_ik[d].astype(np.float64)
+        c = cs[d].astype(np.float64)
         shape = [1, 1, 1]
         shape[d] = -1
         out.append(_fft.irfftn(1j * c.reshape(shape) * pot, s=conf.mesh_shape))
     return np.stack(out)
 
 
-def gravity(pmid, disp, conf, Omega_m, kernel=None):
+def gravity(pmid, disp, conf, Omega_m, kernel=None, gradient="spectral"):
     """gravity(), gravity.py:786-814, uncorrected (or fixed real transfer)."""
     rho = scatter(pmid, disp, conf)
-    F = force_meshes(rho, conf, Omega_m, kernel)
+    F = force_meshes(rho, conf, Omega_m, kernel, gradient)
     return gather(pmid, disp, conf, F)
 
 
-def gravity_vjp(pmid, disp, conf, Omega_m, acc_cot, kernel=None, val=None):
+def gravity_vjp(pmid, disp, conf, Omega_m, acc_cot, kernel=None, val=None, gradient="spectral"):
     """Transpose of gravity w.r.t. disp and Omega_m.
 
     The map S -> A_d is the real convolution irfft(H_d rfft(S)) with
@@ -515,11 +617,12 @@ def gravity_vjp(pmid, disp, conf, Omega_m, acc_cot, kernel=None, val=None):
     kernel = potential_kernel(conf) if kernel is None else kernel
     om = float(np.float32(Omega_m)) if conf.float_dtype == np.float32 else float(Omega_m)
     rho = scatter(pmid, disp, conf, val)
-    F = force_meshes(rho, conf, Omega_m, kernel)
+    F = force_meshes(rho, conf, Omega_m, kernel, gradient)
     dc_gather, A_cot = gather_vjp(pmid, disp, conf, F, acc_cot)
+    cs = conf.derivative_factors(gradient)
     spec = 0
     for d in range(3):
-        c = conf.neg_ik[d].astype(np.float64)
+        c = cs[d].astype(np.float64)
         shape = [1, 1, 1]
         shape[d] = -1
         spec = spec + (-1j) * c.reshape(shape) * _fft.rfftn(A_cot[d])

@@ -15,12 +15,13 @@ from .particles import Particles, pmid_to_idx
 from . import cic
 from .cic import scatter, gather, scatter_vjp, gather_vjp
 from .gravity import gravity, gravity_vjp
-from .nbody import nbody, nbody_adj, integrate, kick, drift, NBodyRun
+from .nbody import (nbody, nbody_adj, integrate, kick, drift, NBodyRun, kick_adj, drift_adj_from_output,
+                    force_adj, integrate_adj)
 
 __all__ = [
     "Configuration", "Cosmology", "SimpleLCDM", "boltzmann", "growth", "linear_power", "Particles", "pmid_to_idx", "cic", "scatter",
     "gather", "scatter_vjp", "gather_vjp", "gravity", "gravity_vjp", "nbody", "nbody_adj", "integrate", "kick",
-    "drift", "NBodyRun"
+    "drift", "NBodyRun", "kick_adj", "drift_adj_from_output", "force_adj", "integrate_adj"
 ]
 from . import modes, lpt, power_spectrum, pipeline  # noqa: E402
 from .modes import white_noise_nested, linear_modes  # noqa: E402

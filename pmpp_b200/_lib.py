@@ -19,7 +19,16 @@ _SIGS = {
     "pmb_sorted_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
     "pmb_sort_scratch_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
     "pmb_sort_rows": (c_int, [c_p, c_p, c_p, c_f, c_i64, c_int, c_int, c_int, c_f, c_p, c_p, c_i64, c_p]),
+    "pmb_sort_rows_ex": (c_int, [c_p, c_p, c_p, c_f, c_i64, c_int, c_int, c_int, c_f, c_f, c_f, c_f, c_p, c_p, c_p,
+                                 c_i64, c_p]),
     "pmb_sort_by_cell": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_f, c_p, c_p, c_p, c_i64, c_p]),
+    "pmb_cic_general_scratch_bytes": (c_i64, [c_int, c_int, c_int, c_int]),
+    "pmb_cic_general_scatter": (c_int, [c_p, c_p, c_p, c_i64, c_int, c_int, c_int, c_f, c_f, c_f, c_f, c_f, c_int,
+                                        c_int, c_int, c_int, c_p, c_f, c_p, c_p, c_i64, c_p]),
+    "pmb_cic_general_gather": (c_int, [c_p, c_p, c_p, c_i64, c_int, c_int, c_int, c_f, c_f, c_f, c_f, c_f, c_int,
+                                       c_int, c_int, c_int, c_p, c_p, c_p]),
+    "pmb_cic_general_interp_grad": (c_int, [c_p, c_p, c_p, c_i64, c_int, c_int, c_int, c_f, c_f, c_f, c_f, c_f,
+                                            c_int, c_int, c_int, c_int, c_p, c_p, c_f, c_p, c_p, c_p]),
     "pmb_sort_by_cell_scratch_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
     "pmb_scatter_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_int, c_f, c_int, c_f, c_p, c_p, c_p]),
     "pmb_gather_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_f, c_p]),
@@ -27,6 +36,9 @@ _SIGS = {
     "pmb_interp_grad_rows": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_int, c_p, c_p, c_f, c_f, c_int, c_p, c_p,
                                      c_p, c_p]),
     "pmb_wait_timeouts": (c_int, [c_p]),
+    "pmb_set_wait_limit": (c_int, [c_i64]),
+    "pmb_sorted_status": (c_int, [c_p, c_i64, c_int, c_int, c_int, c_p, c_p]),
+    "pmb_device_status": (c_int, [c_p]),
     "pmb_set_gather_staging": (c_int, [c_int]),
     "pmb_fft_work_bytes": (c_i64, [c_int, c_int, c_int, c_int]),
     "pmb_set_pmfft": (c_int, [c_int]),
@@ -147,7 +159,8 @@ def check(status, what):
 
 # Hand-written kernels launched per entry point (cuFFT's own kernels excluded).
 _KERNELS = {
-    "pmb_sort_rows": 5, "pmb_gather_rows": 1, "pmb_gather_rows2": 1, "pmb_interp_grad_rows": 1, "pmb_green_gradient": 1,
+    "pmb_sort_rows": 5, "pmb_sort_rows_ex": 5, "pmb_cic_general_scatter": 3, "pmb_cic_general_gather": 1,
+    "pmb_cic_general_interp_grad": 1, "pmb_gather_rows": 1, "pmb_gather_rows2": 1, "pmb_interp_grad_rows": 1, "pmb_green_gradient": 1,
     "pmb_green_gradient_adjoint": 1, "pmb_axpy": 1, "pmb_kick_adj": 1, "pmb_kick_adj2": 1, "pmb_drift_cot_adj": 1, "pmb_drift_adj": 1, "pmb_dot": 1,
     "pmb_force": 9, "pmb_force2": 9, "pmb_force_vjp": 11, "pmb_force_vjp_presorted": 6, "pmb_sum": 1,
     "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,
@@ -166,6 +179,21 @@ def wait_timeouts():
     v = ctypes.c_uint32()
     check(lib().pmb_wait_timeouts(ctypes.byref(v)), "pmb_wait_timeouts")
     return v.value
+
+
+def device_status():
+    """Device-wide flags (1 timed-out wait, 2 non-finite displacement, 4
+    non-finite deposit value) since the last call, then cleared; raises
+    PMBError naming the conditions when any is set.  Synchronises the device."""
+    v = ctypes.c_uint32()
+    check(lib().pmb_device_status(ctypes.byref(v)), "pmb_device_status")
+    return v.value
+
+
+def set_wait_limit(polls):
+    """Poll limit of the first bounded wait of the staged / TMA-fed kernels
+    (None or a negative value: the default)."""
+    check(lib().pmb_set_wait_limit(-1 if polls is None else int(polls)), "pmb_set_wait_limit")
 
 
 def set_pmfft(enabled):

@@ -8,9 +8,12 @@ adjoints ``scatter_vjp`` / ``gather_vjp`` restate ``_scatter_bwd`` /
 ``Gather`` are torch.autograd Functions wrapping the same kernels.
 
 Every call sorts the particles by lower-corner mesh row on the device
-(pmb_sort_rows) and runs the deterministic pull scatter / sorted gather.
-Only offset=0 with the configuration's cell size (the PM force path) is
-supported.
+(pmb_sort_rows, or pmb_sort_rows_ex with a mesh offset or unused slots) and
+runs the deterministic pull scatter / sorted gather.  ``offset`` moves the
+mesh origin as in the reference (cic/enmesh.py:128-147); slots flagged in
+``ptcl.unused_index`` take no part (cic/scatter.py:258-272,
+cic/gather.py:356-357); an explicit ``cell_size`` resamples onto a mesh of
+another cell size through the per-particle pmb_cic_general_* kernels.
 """
 from __future__ import annotations
 
@@ -20,11 +23,24 @@ from ._lib import call, lib
 from .runtime import ptr, require_cuda, stream_handle, workspace
 
 
-class SortedParticles:
-    """Device buffer of particles sorted by lower-corner mesh row."""
+def offset3(offset):
+    """Mesh offset as three floats (a scalar applies to every axis)."""
+    o = torch.as_tensor(offset, dtype=torch.float64).reshape(-1).tolist()
+    if len(o) == 1:
+        o = o * 3
+    if len(o) != 3:
+        raise ValueError(f"offset must be a scalar or have 3 entries, got {len(o)}")
+    return [float(x) for x in o]
 
-    def __init__(self, pmid, disp, conf, mesh_shape=None, drift_vel=None, drift=0.0):
-        require_cuda(pmid, disp, drift_vel)
+
+class SortedParticles:
+    """Device buffer of particles sorted by lower-corner mesh row.
+
+    offset: mesh origin in the particles' frame; valid: uint8 (N,) mask of the
+    used slots (None: all)."""
+
+    def __init__(self, pmid, disp, conf, mesh_shape=None, drift_vel=None, drift=0.0, offset=0.0, valid=None):
+        require_cuda(pmid, disp, drift_vel, valid)
         self.conf = conf
         self.shape = tuple(mesh_shape or conf.mesh_shape)
         self.n = pmid.shape[0]
@@ -34,8 +50,14 @@ class SortedParticles:
         self.buf = torch.empty(L.pmb_sorted_bytes(self.n, nx, ny, nz), dtype=torch.uint8, device=dev)
         sb = L.pmb_sort_scratch_bytes(self.n, nx, ny, nz)
         scratch = workspace(sb, dev, "sort")
-        call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), self.n, nx, ny, nz,
-             float(conf.cell_size), self.buf.data_ptr(), scratch.data_ptr(), scratch.numel(), stream_handle(dev))
+        o = offset3(offset)
+        if valid is None and o == [0.0, 0.0, 0.0]:
+            call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), self.n, nx, ny, nz,
+                 float(conf.cell_size), self.buf.data_ptr(), scratch.data_ptr(), scratch.numel(), stream_handle(dev))
+        else:
+            call("pmb_sort_rows_ex", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), self.n, nx, ny,
+                 nz, float(conf.cell_size), o[0], o[1], o[2], ptr(valid), self.buf.data_ptr(), scratch.data_ptr(),
+                 scratch.numel(), stream_handle(dev))
 
     def scatter(self, val=None, val_const=None, channels=1, mode=0, src_mul=1.0, out=None, val_sorted=False):
         """Deposit; val (n, channels) is in particle order, or in sorted order
@@ -98,43 +120,108 @@ def _val_array(val, n, device):
     return v.reshape(n, -1).contiguous(), None, v.reshape(n, -1).shape[1]
 
 
+def _masked_val(v, valid):
+    """Zero the values of unused slots (cic/scatter.py:268-272)."""
+    if v is None or valid is None:
+        return v
+    keep = valid.to(torch.bool)
+    return torch.where(keep.reshape((-1, ) + (1, ) * (v.dim() - 1)), v, torch.zeros_like(v)).contiguous()
+
+
+class _General:
+    """Argument pack of the pmb_cic_general_* entry points (explicit cell size)."""
+
+    def __init__(self, ptcl, conf, mesh_shape, offset, cell_size):
+        require_cuda(ptcl.pmid, ptcl.disp)
+        self.valid = ptcl.valid_mask()
+        self.n = len(ptcl)
+        self.head = (ptcl.pmid.data_ptr(), ptcl.disp.data_ptr(), ptr(self.valid), self.n, *conf.mesh_shape,
+                     float(conf.cell_size), *offset3(offset), float(cell_size), *mesh_shape)
+        self.shape = tuple(mesh_shape)
+        self.dev = ptcl.disp.device
+
+
+def _general_scatter(g, val, vc, C):
+    nx, ny, nz = g.shape
+    out = torch.empty((C, nx, ny, nz), dtype=torch.float32, device=g.dev)
+    sb = lib().pmb_cic_general_scratch_bytes(nx, ny, nz, C)
+    scratch = workspace(sb, g.dev, "cic_general")
+    call("pmb_cic_general_scatter", *g.head, C, ptr(val), float(vc or 0.0), out.data_ptr(), scratch.data_ptr(),
+         scratch.numel(), stream_handle(g.dev))
+    return out
+
+
+def _general_interp_grad(g, mp, u, u_const, wsum=False):
+    C = mp.shape[0]
+    disp_cot = torch.empty((g.n, 3), dtype=torch.float32, device=g.dev)
+    ws = torch.empty((g.n, C), dtype=torch.float32, device=g.dev) if wsum else None
+    call("pmb_cic_general_interp_grad", *g.head, C, mp.data_ptr(), ptr(u), float(u_const), disp_cot.data_ptr(),
+         ptr(ws), stream_handle(g.dev))
+    return disp_cot, ws
+
+
 def scatter(ptcl, conf, mesh=None, val=None, offset=0, cell_size=None):
-    """CIC deposit (cic/scatter.py:235-275); val defaults to mesh_size/ptcl_num."""
+    """CIC deposit (cic/scatter.py:235-275); val defaults to mesh_size/ptcl_num.
+
+    Unused slots (ptcl.unused_index) deposit nothing; offset moves the mesh
+    origin; cell_size resamples onto a mesh of that cell size (the shape of
+    ``mesh`` when given, else the configuration's mesh shape)."""
     if conf.float_dtype == torch.float64:
         if mesh is not None or offset not in (0, 0.0) or cell_size is not None or (val is not None and
                                                                                      not isinstance(val, float)):
             raise NotImplementedError("the float64 build deposits a constant value on the configuration mesh")
         from . import x64
         return x64.scatter(ptcl, conf, val)
-    if (offset not in (0, 0.0)) or cell_size is not None:
-        raise NotImplementedError("only offset=0 and the configuration cell size are supported")
-    sp = SortedParticles(ptcl.pmid, ptcl.disp, conf)
+    valid = ptcl.valid_mask()
     v, vc, C = _val_array(val, len(ptcl), ptcl.disp.device)
-    out = sp.scatter(val=v, val_const=vc, channels=C)
+    v = _masked_val(v, valid)
+    if v is None and vc is None:
+        vc = float(conf.mesh_size / conf.ptcl_num)
+    if cell_size is not None:
+        shape = tuple(mesh.shape[:3]) if mesh is not None else tuple(conf.mesh_shape)
+        out = _general_scatter(_General(ptcl, conf, shape, offset, cell_size), v, vc, C)
+    else:
+        sp = SortedParticles(ptcl.pmid, ptcl.disp, conf, offset=offset, valid=valid)
+        out = sp.scatter(val=v, val_const=vc, channels=C)
     out = out[0] if (v is None or v.dim() == 1) else out.permute(1, 2, 3, 0)
     if mesh is not None:
         out = out + mesh
     return out
 
 
-def gather(ptcl, conf, mesh):
-    """CIC interpolation (cic/gather.py:323-360)."""
-    sp = SortedParticles(ptcl.pmid, ptcl.disp, conf, mesh_shape=tuple(mesh.shape[:3]))
+def gather(ptcl, conf, mesh, offset=0, cell_size=None):
+    """CIC interpolation (cic/gather.py:323-360); unused slots gather 0.
+    offset / cell_size as the private _gather (cic/gather.py:447-472)."""
     mp, had = _planar(mesh, conf)
-    out = sp.gather(mp)
+    shape = tuple(mesh.shape[:3])
+    if cell_size is not None:
+        g = _General(ptcl, conf, shape, offset, cell_size)
+        out = torch.empty((g.n, mp.shape[0]), dtype=torch.float32, device=g.dev)
+        call("pmb_cic_general_gather", *g.head, mp.shape[0], mp.data_ptr(), out.data_ptr(), stream_handle(g.dev))
+    else:
+        sp = SortedParticles(ptcl.pmid, ptcl.disp, conf, mesh_shape=shape, offset=offset, valid=ptcl.valid_mask())
+        out = sp.gather(mp)
     return out if had else out[:, 0]
 
 
-def scatter_vjp(ptcl, conf, mesh_cot, val=None):
+def scatter_vjp(ptcl, conf, mesh_cot, val=None, offset=0, cell_size=None):
     """Adjoint of scatter (scatter.py:386-437): returns (disp_cot, val_cot).
 
-    val_cot is summed over particles when val is a scalar (or None)."""
-    sp = SortedParticles(ptcl.pmid, ptcl.disp, conf, mesh_shape=tuple(mesh_cot.shape[:3]))
+    val_cot is summed over particles when val is a scalar (or None); unused
+    slots get zero cotangents."""
+    valid = ptcl.valid_mask()
+    shape = tuple(mesh_cot.shape[:3])
     mp, had = _planar(mesh_cot, conf)
     v, vc, C = _val_array(val, len(ptcl), ptcl.disp.device)
+    v = _masked_val(v, valid)
     if v is None and vc is None:
         vc = float(conf.mesh_size / conf.ptcl_num)
-    disp_cot, wsum = sp.interp_grad(mp, u=v, u_const=0.0 if vc is None else vc, wsum=True)
+    if cell_size is not None:
+        disp_cot, wsum = _general_interp_grad(_General(ptcl, conf, shape, offset, cell_size), mp, v,
+                                              0.0 if vc is None else vc, wsum=True)
+    else:
+        sp = SortedParticles(ptcl.pmid, ptcl.disp, conf, mesh_shape=shape, offset=offset, valid=valid)
+        disp_cot, wsum = sp.interp_grad(mp, u=v, u_const=0.0 if vc is None else vc, wsum=True)
     if v is None:
         val_cot = wsum.sum(dtype=torch.float64).to(torch.float32)
     else:
@@ -148,13 +235,21 @@ def scatter_vjp(ptcl, conf, mesh_cot, val=None):
     return disp_cot, val_cot
 
 
-def gather_vjp(ptcl, conf, mesh, val_cot):
-    """Adjoint of gather (gather.py:517-548): returns (disp_cot, mesh_cot)."""
-    sp = SortedParticles(ptcl.pmid, ptcl.disp, conf, mesh_shape=tuple(mesh.shape[:3]))
+def gather_vjp(ptcl, conf, mesh, val_cot, offset=0, cell_size=None):
+    """Adjoint of gather (gather.py:517-548): returns (disp_cot, mesh_cot);
+    unused slots contribute nothing."""
+    valid = ptcl.valid_mask()
+    shape = tuple(mesh.shape[:3])
     mp, had = _planar(mesh, conf)
-    vc = val_cot.to(torch.float32).reshape(len(ptcl), -1).contiguous()
-    disp_cot, _ = sp.interp_grad(mp, u=vc)
-    mesh_cot = sp.scatter(val=vc, channels=vc.shape[1])
+    vc = _masked_val(val_cot.to(torch.float32).reshape(len(ptcl), -1).contiguous(), valid)
+    if cell_size is not None:
+        g = _General(ptcl, conf, shape, offset, cell_size)
+        disp_cot, _ = _general_interp_grad(g, mp, vc, 0.0)
+        mesh_cot = _general_scatter(g, vc, None, vc.shape[1])
+    else:
+        sp = SortedParticles(ptcl.pmid, ptcl.disp, conf, mesh_shape=shape, offset=offset, valid=valid)
+        disp_cot, _ = sp.interp_grad(mp, u=vc)
+        mesh_cot = sp.scatter(val=vc, channels=vc.shape[1])
     return disp_cot, _channels_last(mesh_cot, had)
 
 

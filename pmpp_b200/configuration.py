@@ -233,22 +233,32 @@ class Configuration:
         limit = kn + kn * f(8 * np.finfo(self.np_dtype).eps)
         return tuple((np.abs(k) <= limit).astype(self.np_dtype) for k in self.kvec)
 
-    def spectral_tables(self, which="mesh", device=None, green_kernel=0):
+    @staticmethod
+    def _fastpm_neg_k(k, spacing):
+        """Derivative factor c (neg_ik = i c) of FastPM's 4-point gradient,
+        (8 sin(k dx) - sin(2 k dx)) / (6 dx) (gravity.py:355-391), in k's dtype."""
+        f = k.dtype.type
+        phase = (k * f(spacing)).astype(k.dtype)
+        d = ((f(8.0) * np.sin(phase)).astype(k.dtype) - np.sin(f(2.0) * phase)).astype(k.dtype)
+        return (-(d / f(6.0 * spacing))).astype(k.dtype)
+
+    def spectral_tables(self, which="mesh", device=None, green_kernel=0, gradient_kernel=0):
         """Device table [kx ky kz cx cy cz (mx my mz)] for pmb_green_gradient.
 
         which="mesh" uses the force mesh (kvec, cell_size); "particle" the
         particle grid (kvec_spacing, ptcl_spacing).  green_kernel=1 replaces
         k by the discrete-Laplacian wavenumber 2 sin(k dx/2)/dx
-        (gravity.py:122-171)."""
+        (gravity.py:122-171); gradient_kernel=1 takes FastPM's 4-point
+        derivative for c instead of the spectral -k (gravity.py:355-391)."""
         device = self.device if device is None else torch.device(device)
-        key = (which, str(device), green_kernel)
+        key = (which, str(device), green_kernel, gradient_kernel)
         if key not in self._tables:
             if which == "mesh":
                 ks, spacing, masks = self.kvec, self.cell_size, (self.particle_nyquist_masks()
                                                                  if self.has_particle_nyquist_masks else ())
             else:
                 ks, spacing, masks = self.kvec_spacing, self.ptcl_spacing, ()
-            cs = [self._neg_k(k, spacing) for k in ks]
+            cs = [(self._fastpm_neg_k(k, spacing) if gradient_kernel == 1 else self._neg_k(k, spacing)) for k in ks]
             if green_kernel == 1:
                 f = self.np_dtype.type
                 c = f(spacing)

@@ -28,10 +28,21 @@ from .runtime import stream_handle
 
 
 class PMWindowCompensation:
+    """corrections/window.py:23-265 (PMWindowCompensationCorrection): transfer
+    gain W(k)^(-order*windows*alpha) capped and tapered, the Green's function
+    ("continuum" or "discrete_laplacian") and the force derivative
+    ("spectral" or FastPM's "fastpm_4point")."""
+
     green_kernel = 1  # discrete Laplacian (window.py:100-108 default)
 
     def __init__(self, alpha=0.48, max_gain=4.0, assignment_order=2, windows=2, taper_start=0.75, taper_stop=1.0,
-                 green_kernel="discrete_laplacian"):
+                 green_kernel="discrete_laplacian", gradient_kernel="spectral", interlacing=False):
+        if green_kernel not in ("continuum", "discrete_laplacian"):
+            raise ValueError(f"Unsupported PM Green's function {green_kernel!r}.")
+        if gradient_kernel not in ("spectral", "fastpm_4point"):
+            raise ValueError(f"Unsupported force-gradient kernel {gradient_kernel!r}.")
+        if interlacing:
+            raise NotImplementedError("interlaced assignment is not built (the force takes one scatter)")
         self.alpha = alpha
         self.max_gain = max_gain
         self.assignment_order = assignment_order
@@ -39,9 +50,12 @@ class PMWindowCompensation:
         self.taper_start = taper_start
         self.taper_stop = taper_stop
         self.green_kernel = 1 if green_kernel == "discrete_laplacian" else 0
+        self.gradient_kernel = gradient_kernel
         self._cache = {}
 
     def transfer_tables(self, a, cosmo, conf):
+        if self.alpha == 0:
+            return None, None  # gain W^0 = 1 everywhere: no transfer
         dev = conf.device
         key = (conf.mesh_shape, conf.cell_size, conf.ptcl_spacing, str(dev))
         if key not in self._cache:
@@ -64,6 +78,22 @@ class PMWindowCompensation:
                 gain = 1.0 + (gain - 1.0) * (1.0 - t * t * (3.0 - 2.0 * t))
             self._cache[key] = gain.to(torch.float32).contiguous()
         return self._cache[key], None
+
+
+def init_potential_correction(model, **kwargs):
+    """The analytic models of init_potential_correction (corrections/core.py:40-151):
+    "pm_window" / "cic_compensation" / "cic_window_compensation" (the window
+    compensation), "fastpm_1_4" (continuum Green's function) and "fastpm_3_4"
+    (discrete Laplacian), both with FastPM's 4-point gradient and no window
+    gain."""
+    if model in ("pm_window", "cic_compensation", "cic_window_compensation"):
+        return PMWindowCompensation(**kwargs)
+    if model in ("fastpm_1_4", "fastpm_3_4"):
+        kw = dict(kwargs)
+        kw.update(alpha=0.0, green_kernel="continuum" if model == "fastpm_1_4" else "discrete_laplacian",
+                  gradient_kernel="fastpm_4point")
+        return PMWindowCompensation(**kw)
+    raise ValueError(f"Unsupported correction model {model!r}.")
 
 
 def radial_table_len(conf):

@@ -1,15 +1,18 @@
 // extern "C" entry points of libpmb200.so (declared in include/pmb200.h).
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
 
 #include "../../include/pmb200.h"
+#include "pmb_cic_device.cuh"
 #include "pmb_common.cuh"
 #include "pmb_ic.cuh"
 #include "pmb_integrate.cuh"
 #include "pmb_kernels.cuh"
 #include "pmb_mlp.cuh"
 #include "pmb_sort.cuh"
+#include "pmb_tma.cuh"
 
 namespace pmb {
 namespace {
@@ -44,13 +47,16 @@ bool valid_mesh(int nx, int ny, int nz) {
     if (_st != kOk) return _st;  \
   } while (0)
 
+// Sorted buffer: records, permutation, row offsets and a status word (the
+// DeviceFlag bits the sort raised).
 struct SortedView {
   Rec* rec;
   uint32_t* perm;
   uint32_t* offs;
+  uint32_t* status;
 };
 
-SortedView sorted_view(void* sorted, int64_t n) {
+SortedView sorted_view(void* sorted, int64_t n, Mesh3 m) {
   char* p = (char*)sorted;
   SortedView v;
   v.rec = (Rec*)p;
@@ -58,10 +64,14 @@ SortedView sorted_view(void* sorted, int64_t n) {
   v.perm = (uint32_t*)p;
   p += align_up(4 * n, 256);
   v.offs = (uint32_t*)p;
+  p += align_up(4 * (m.rows() + 1), 256);
+  v.status = (uint32_t*)p;
   return v;
 }
 
-int64_t sorted_bytes(int64_t n, Mesh3 m) { return align_up(16 * n, 256) + align_up(4 * n, 256) + align_up(4 * (m.rows() + 1), 256); }
+int64_t sorted_bytes(int64_t n, Mesh3 m) {
+  return align_up(16 * n, 256) + align_up(4 * n, 256) + align_up(4 * (m.rows() + 1), 256) + 256;
+}
 
 SpecTables make_tables(const float* t, Mesh3 m, int has_masks) { return spec_tables_from(t, m, has_masks); }
 
@@ -94,7 +104,7 @@ struct Carve {
 
 extern "C" {
 
-int pmb_abi_version(void) { return 2; }
+int pmb_abi_version(void) { return 3; }
 
 const char* pmb_last_error(void) { return g_last_error.c_str(); }
 
@@ -109,17 +119,50 @@ int pmb_sort_rows(const int16_t* pmid, float* disp, const float* vel, float drif
   PMB_REQUIRE(n >= 0 && n < 4294967295ll, "pmb_sort_rows: particle count out of range");
   PMB_REQUIRE(cell > 0.f, "pmb_sort_rows: cell size must be positive");
   PMB_REQUIRE(scratch_bytes >= bin_scratch_bytes(n, m), "pmb_sort_rows: scratch too small");
-  SortedView v = sorted_view(sorted, n);
-  return bin_particles(pmid, disp, vel, drift, n, m, cell, v.rec, v.perm, v.offs, scratch, S(stream));
+  SortedView v = sorted_view(sorted, n, m);
+  return bin_particles(pmid, disp, vel, drift, n, m, cell, v.rec, v.perm, v.offs, scratch, S(stream), nullptr,
+                       nullptr, v.status);
+}
+
+int pmb_sort_rows_ex(const int16_t* pmid, float* disp, const float* vel, float drift, int64_t n, int nx, int ny,
+                     int nz, float cell, float ox, float oy, float oz, const uint8_t* valid, void* sorted,
+                     void* scratch, int64_t scratch_bytes, void* stream) {
+  Mesh3 m{nx, ny, nz};
+  PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_sort_rows_ex: unsupported mesh shape");
+  PMB_REQUIRE(n >= 0 && n < 4294967295ll, "pmb_sort_rows_ex: particle count out of range");
+  PMB_REQUIRE(cell > 0.f, "pmb_sort_rows_ex: cell size must be positive");
+  PMB_REQUIRE(std::isfinite(ox) && std::isfinite(oy) && std::isfinite(oz), "pmb_sort_rows_ex: non-finite offset");
+  PMB_REQUIRE(scratch_bytes >= bin_scratch_bytes(n, m), "pmb_sort_rows_ex: scratch too small");
+  // whole cells and remainder of the offset, the remainder rounded once to float
+  BinShift sh;
+  const float o[3] = {ox, oy, oz};
+  int q[3];
+  float r[3];
+  for (int a = 0; a < 3; ++a) {
+    const double qd = std::floor((double)o[a] / (double)cell);
+    PMB_REQUIRE(std::fabs(qd) < 1e9, "pmb_sort_rows_ex: offset too large");
+    q[a] = (int)qd;
+    r[a] = (float)((double)o[a] - qd * (double)cell);
+  }
+  sh.qx = q[0];
+  sh.qy = q[1];
+  sh.qz = q[2];
+  sh.rx = r[0];
+  sh.ry = r[1];
+  sh.rz = r[2];
+  SortedView v = sorted_view(sorted, n, m);
+  return bin_particles(pmid, disp, vel, drift, n, m, cell, v.rec, v.perm, v.offs, scratch, S(stream), &sh, valid,
+                       v.status);
 }
 
 int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* val, int val_sorted,
                      float val_const, int mode, float src_mul, float* out, void* scratch16, void* stream) {
   Mesh3 m{nx, ny, nz};
   PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_scatter_rows: unsupported mesh shape");
+  PMB_REQUIRE(n >= 0 && n < 4294967295ll, "pmb_scatter_rows: particle count out of range");
   PMB_REQUIRE(C >= 1 && C <= 4, "pmb_scatter_rows: 1..4 channels supported");
   PMB_REQUIRE(mode == 0 || mode == 1, "pmb_scatter_rows: mode must be 0 or 1");
-  SortedView v = sorted_view((void*)sorted, n);
+  SortedView v = sorted_view((void*)sorted, n, m);
   double* scale = (double*)scratch16;
   unsigned int* tmp = (unsigned int*)((char*)scratch16 + 8);
   if (val != nullptr) {
@@ -130,16 +173,17 @@ int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int 
     PMB_TRY(set_double(scale, fixed_point_scale(fixed_point_pow2(n), a), S(stream)));
   }
   return scatter_sorted(v.rec, v.perm, v.offs, m, C, val, val_sorted, val_const, scale, mode, src_mul, out,
-                        S(stream));
+                        S(stream), n, v.status);
 }
 
 int pmb_gather_rows2(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh, float* out,
                      float* vel, float kick, float kick2, void* stream) {
   Mesh3 m{nx, ny, nz};
   PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_gather_rows: unsupported mesh shape");
+  PMB_REQUIRE(n >= 0 && n < 4294967295ll, "pmb_gather_rows: particle count out of range");
   PMB_REQUIRE(C >= 1 && C <= 4, "pmb_gather_rows: 1..4 channels supported");
-  SortedView v = sorted_view((void*)sorted, n);
-  return gather_sorted(v.rec, v.perm, v.offs, n, m, C, mesh, out, vel, kick, kick2, S(stream));
+  SortedView v = sorted_view((void*)sorted, n, m);
+  return gather_sorted(v.rec, v.perm, v.offs, n, m, C, mesh, out, vel, kick, kick2, S(stream), v.status);
 }
 
 int pmb_gather_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh, float* out,
@@ -152,16 +196,107 @@ int pmb_interp_grad_rows(const void* sorted, int64_t n, int nx, int ny, int nz, 
                          float* u_sorted, void* stream) {
   Mesh3 m{nx, ny, nz};
   PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_interp_grad_rows: unsupported mesh shape");
+  PMB_REQUIRE(n >= 0 && n < 4294967295ll, "pmb_interp_grad_rows: particle count out of range");
   PMB_REQUIRE(C >= 1 && C <= 4, "pmb_interp_grad_rows: 1..4 channels supported");
-  SortedView v = sorted_view((void*)sorted, n);
+  SortedView v = sorted_view((void*)sorted, n, m);
   return interp_grad_sorted(v.rec, v.perm, v.offs, n, m, C, mesh, u, u_const, cell, accumulate, disp_cot, wsum,
-                            u_sorted, S(stream));
+                            u_sorted, S(stream), v.status);
+}
+
+// ---------------------------------------------------------------------------
+// CIC onto a mesh of another cell size
+// ---------------------------------------------------------------------------
+static int general_grid(int gx, int gy, int gz, float cell, float ox, float oy, float oz, float cell2, int nx, int ny,
+                        int nz, GeneralGrid* G) {
+  PMB_REQUIRE(gx > 0 && gy > 0 && gz > 0 && cell > 0.f && cell2 > 0.f, "pmb_cic_general: bad particle grid");
+  PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_cic_general: unsupported mesh shape");
+  PMB_REQUIRE(std::isfinite(ox) && std::isfinite(oy) && std::isfinite(oz), "pmb_cic_general: non-finite offset");
+  G->gx = gx;
+  G->gy = gy;
+  G->gz = gz;
+  G->a1 = cell;
+  G->a2 = cell2;
+  G->ox = ox;
+  G->oy = oy;
+  G->oz = oz;
+  G->t = Mesh3{nx, ny, nz};
+  return kOk;
+}
+
+int64_t pmb_cic_general_scratch_bytes(int nx, int ny, int nz, int C) {
+  return general_scatter_scratch_bytes(Mesh3{nx, ny, nz}, C);
+}
+
+int pmb_cic_general_scatter(const int16_t* pmid, const float* disp, const uint8_t* valid, int64_t n, int gx, int gy,
+                            int gz, float cell, float ox, float oy, float oz, float cell2, int nx, int ny, int nz,
+                            int C, const float* val, float val_const, float* out, void* scratch,
+                            int64_t scratch_bytes, void* stream) {
+  GeneralGrid G;
+  PMB_TRY(general_grid(gx, gy, gz, cell, ox, oy, oz, cell2, nx, ny, nz, &G));
+  PMB_REQUIRE(n >= 0 && C >= 1 && C <= 4, "pmb_cic_general_scatter: bad particle count or channels");
+  PMB_REQUIRE(val != nullptr || std::isfinite(val_const), "pmb_cic_general_scatter: non-finite value");
+  if (scratch_bytes < general_scatter_scratch_bytes(G.t, C)) {
+    set_last_error("pmb_cic_general_scatter: scratch too small");
+    return kScratchTooSmall;
+  }
+  return general_scatter(pmid, disp, valid, n, G, C, val, val_const, out, scratch, S(stream));
+}
+
+int pmb_cic_general_gather(const int16_t* pmid, const float* disp, const uint8_t* valid, int64_t n, int gx, int gy,
+                           int gz, float cell, float ox, float oy, float oz, float cell2, int nx, int ny, int nz,
+                           int C, const float* mesh, float* out, void* stream) {
+  GeneralGrid G;
+  PMB_TRY(general_grid(gx, gy, gz, cell, ox, oy, oz, cell2, nx, ny, nz, &G));
+  PMB_REQUIRE(n >= 0 && C >= 1 && C <= 4, "pmb_cic_general_gather: bad particle count or channels");
+  return general_gather(pmid, disp, valid, n, G, C, mesh, out, S(stream));
+}
+
+int pmb_cic_general_interp_grad(const int16_t* pmid, const float* disp, const uint8_t* valid, int64_t n, int gx,
+                                int gy, int gz, float cell, float ox, float oy, float oz, float cell2, int nx, int ny,
+                                int nz, int C, const float* mesh, const float* u, float u_const, float* disp_cot,
+                                float* wsum, void* stream) {
+  GeneralGrid G;
+  PMB_TRY(general_grid(gx, gy, gz, cell, ox, oy, oz, cell2, nx, ny, nz, &G));
+  PMB_REQUIRE(n >= 0 && C >= 1 && C <= 4, "pmb_cic_general_interp_grad: bad particle count or channels");
+  return general_interp_grad(pmid, disp, valid, n, G, C, mesh, u, u_const, disp_cot, wsum, S(stream));
 }
 
 int pmb_set_gather_staging(int mode) {
   PMB_REQUIRE(mode >= 0 && mode <= 2, "pmb_set_gather_staging: mode must be 0, 1 or 2");
   set_gather_staging(mode);
   return kOk;
+}
+
+int pmb_set_wait_limit(int64_t polls) {
+  set_wait_polls(polls < 0 ? kWaitPolls : (polls > 0xFFFFFFFFll ? 0xFFFFFFFFu : (uint32_t)polls));
+  return kOk;
+}
+
+int pmb_sorted_status(const void* sorted, int64_t n, int nx, int ny, int nz, uint32_t* flags, void* stream) {
+  PMB_REQUIRE(flags != nullptr && sorted != nullptr, "pmb_sorted_status: null argument");
+  PMB_REQUIRE(valid_mesh(nx, ny, nz) && n >= 0, "pmb_sorted_status: bad shape");
+  SortedView v = sorted_view(const_cast<void*>(sorted), n, Mesh3{nx, ny, nz});
+  PMB_CUDA_CHECK(cudaMemcpyAsync(flags, v.status, 4, cudaMemcpyDeviceToHost, S(stream)));
+  PMB_CUDA_CHECK(cudaStreamSynchronize(S(stream)));
+  return kOk;
+}
+
+int pmb_device_status(uint32_t* flags) {
+  PMB_REQUIRE(flags != nullptr, "pmb_device_status: null output");
+  PMB_CUDA_CHECK(cudaDeviceSynchronize());
+  unsigned int f = 0, fft = 0;
+  PMB_TRY(device_flags_take(&f));
+  PMB_TRY(pmfft_timeouts(&fft));
+  PMB_TRY(pmfft_timeouts_clear());
+  if (fft) f |= kFlagWaitTimeout;
+  *flags = f;
+  if (f == 0) return kOk;
+  std::string msg = "pmb_device_status:";
+  if (f & kFlagWaitTimeout) msg += " a bounded wait on bulk/TMA copies gave up (results of that launch are invalid);";
+  if (f & kFlagNonFiniteDisp) msg += " a non-finite displacement reached the cell sort (its outputs were not written);";
+  if (f & kFlagNonFiniteValue) msg += " a non-finite value reached a deposit (its output was not written);";
+  set_last_error(msg.c_str());
+  return kDeviceFlagged;
 }
 
 int pmb_wait_timeouts(uint32_t* count) {
@@ -321,8 +456,8 @@ int pmb_force2(const int16_t* pmid, float* disp, const float* drift_vel, float d
                            make_green(green_kernel, transfer, radial, radial_len, inv_m), s));
     PMB_TRY(fft_c2r(m, 3, grad_hat, force_meshes, work, s));
   }
-  SortedView v = sorted_view(sorted, n);
-  return gather_sorted(v.rec, v.perm, v.offs, n, m, 3, force_meshes, acc, vel_kick, kick, kick2, s);
+  SortedView v = sorted_view(sorted, n, m);
+  return gather_sorted(v.rec, v.perm, v.offs, n, m, 3, force_meshes, acc, vel_kick, kick, kick2, s, v.status);
 }
 
 int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float drift, int64_t n, int nx, int ny, int nz,
@@ -394,10 +529,10 @@ static int force_vjp_impl(const int16_t* pmid, const float* disp, int64_t n, int
   else
     PMB_TRY(pmb_sort_rows(pmid, (float*)disp, nullptr, 0.f, n, nx, ny, nz, cell, sorted, bins,
                           bin_scratch_bytes(n, m), stream));
-  SortedView v = sorted_view(sorted, n);
+  SortedView v = sorted_view(sorted, n, m);
   // gather adjoint: position term and the 3-channel scatter of acc_cot
   PMB_TRY(interp_grad_sorted(v.rec, v.perm, v.offs, n, m, 3, force_meshes, acc_cot, 0.f, cell, 1, disp_cot, nullptr,
-                             cot_sorted, s));
+                             cot_sorted, s, v.status));
   PMB_TRY(pmb_scatter_rows(sorted, n, nx, ny, nz, 3, cot_sorted, 1, 0.f, 0, 1.f, mesh_cot, scale16, stream));
   // transposes of the C2R, gradient, Green and R2C stages
   const float post = (float)((double)src_mul / (double)m.cells());
@@ -412,7 +547,7 @@ static int force_vjp_impl(const int16_t* pmid, const float* disp, int64_t n, int
   }
   // scatter adjoint of the density (constant particle value)
   return interp_grad_sorted(v.rec, v.perm, v.offs, n, m, 1, src_cot, nullptr, val_const, cell, 1, disp_cot, nullptr,
-                            nullptr, s);
+                            nullptr, s, v.status);
 }
 
 int pmb_force_vjp(const int16_t* pmid, const float* disp, int64_t n, int nx, int ny, int nz, float cell,

@@ -14,8 +14,10 @@
 // Costs and limits:
 //  * the array is kNoAllocScratchBytes (32 MiB) of device memory that every
 //    GPU which loads this library holds until the process exits;
-//  * a call needs 28 bytes per particle plus about 8 bytes per mesh row; larger
-//    problems are rejected with an error (use the workspace entry points);
+//  * a call needs 28 bytes per particle plus 12 bytes per mesh row (and a few
+//    hundred bytes of alignment); larger problems, like invalid arguments, are
+//    rejected with an error before any work is queued (use the workspace entry
+//    points instead);
 //  * every call on a device shares the same array and leaves its contents
 //    behind, so calls whose execution overlaps on the GPU (different streams,
 //    or host threads) race and corrupt each other: serialise them;
@@ -79,14 +81,18 @@ extern "C" int pmb_scatter_density_noalloc(const int16_t* pmid, const float* dis
     set_last_error("pmb_scatter_density_noalloc: invalid argument");
     return kInvalidArgument;
   }
+  if (!(fabsf(val) < INFINITY)) {
+    set_last_error("pmb_scatter_density_noalloc: non-finite value");
+    return kInvalidArgument;
+  }
   Mesh3 m{nx, ny, nz};
   const int64_t rec_bytes = align_up(16 * n, 256), perm_bytes = align_up(4 * n, 256);
   const int64_t offs_bytes = align_up(4 * (m.rows() + 1), 256);
   const int64_t bins_bytes = bin_scratch_bytes(n, m);
-  const int64_t need = rec_bytes + perm_bytes + offs_bytes + bins_bytes + 256;
+  const int64_t need = rec_bytes + perm_bytes + offs_bytes + bins_bytes + 256 + 256;
   if (need > kNoAllocScratchBytes) {
     set_last_error("pmb_scatter_density_noalloc: problem needs more than the fixed 32 MiB scratch "
-                   "(28 B per particle + ~8 B per mesh row); use pmb_sort_rows + pmb_scatter_rows");
+                   "(28 B per particle + 12 B per mesh row); use pmb_sort_rows + pmb_scatter_rows");
     return kInvalidArgument;
   }
   void* base = nullptr;
@@ -98,17 +104,14 @@ extern "C" int pmb_scatter_density_noalloc(const int16_t* pmid, const float* dis
   uint32_t* offs = (uint32_t*)(p + rec_bytes + perm_bytes);
   void* bins = p + rec_bytes + perm_bytes + offs_bytes;
   double* scale = (double*)(p + rec_bytes + perm_bytes + offs_bytes + bins_bytes);
+  uint32_t* status = (uint32_t*)(p + rec_bytes + perm_bytes + offs_bytes + bins_bytes + 256);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   // bin_particles zeroes the row counts itself; the scale word is rewritten
   // below, so nothing left over from an earlier call is read.
-  st = bin_particles(pmid, const_cast<float*>(disp), nullptr, 0.f, n, m, cell, rec, perm, offs, bins, s);
+  st = bin_particles(pmid, const_cast<float*>(disp), nullptr, 0.f, n, m, cell, rec, perm, offs, bins, s, nullptr,
+                     nullptr, status);
   if (st != kOk) return st;
-  const float a = fabsf(val);
-  if (!(a < INFINITY)) {
-    set_last_error("pmb_scatter_density_noalloc: non-finite value");
-    return kInvalidArgument;
-  }
-  st = set_double(scale, fixed_point_scale(fixed_point_pow2(n), a), s);
+  st = set_double(scale, fixed_point_scale(fixed_point_pow2(n), fabsf(val)), s);
   if (st != kOk) return st;
-  return scatter_sorted(rec, perm, offs, m, 1, nullptr, 0, val, scale, 0, 1.f, out, s);
+  return scatter_sorted(rec, perm, offs, m, 1, nullptr, 0, val, scale, 0, 1.f, out, s, n, status);
 }

@@ -16,10 +16,15 @@ struct Binned {
 
 // Lower CIC corner and fractions of one particle: d = disp / cell in IEEE
 // float, corner = pmid + floor(d) (periodic), fraction = d - floor(d).
+// A non-finite displacement is binned as zero (the anchor cell) so that every
+// index stays in the mesh; the sort flags it (kFlagNonFiniteDisp).
+__device__ __forceinline__ float finite_or_zero(float x) { return isfinite(x) ? x : 0.f; }
+
 __device__ __forceinline__ Binned bin_particle(const int16_t* __restrict__ pmid, const float d0, const float d1,
                                                const float d2, int64_t i, Mesh3 m, float cell) {
   Binned b;
-  float q0 = __fdiv_rn(d0, cell), q1 = __fdiv_rn(d1, cell), q2 = __fdiv_rn(d2, cell);
+  float q0 = finite_or_zero(__fdiv_rn(d0, cell)), q1 = finite_or_zero(__fdiv_rn(d1, cell)),
+        q2 = finite_or_zero(__fdiv_rn(d2, cell));
   float l0 = floorf(q0), l1 = floorf(q1), l2 = floorf(q2);
   b.fx = __fsub_rn(q0, l0);
   b.fy = __fsub_rn(q1, l1);
@@ -28,6 +33,48 @@ __device__ __forceinline__ Binned bin_particle(const int16_t* __restrict__ pmid,
   b.cy = pmod((int)pmid[3 * i + 1] + (int)l1, m.ny);
   b.cz = pmod((int)pmid[3 * i + 2] + (int)l2, m.nz);
   return b;
+}
+
+// Origin of the mesh in the particles' frame, split as whole cells q and a
+// remainder r in [0, cell): the reference's common-grid offset path
+// (cic/pallas.py:225-238, cic/enmesh.py:128-147) bins (disp - r) / cell from
+// the anchor pmid - q.  A zero shift reproduces bin_particle bit for bit
+// (d - 0 == d for every float).
+struct BinShift {
+  int qx, qy, qz;
+  float rx, ry, rz;
+};
+
+__device__ __forceinline__ Binned bin_particle(const int16_t* __restrict__ pmid, float d0, float d1, float d2,
+                                               int64_t i, Mesh3 m, float cell, const BinShift& sh) {
+  Binned b;
+  const float q0 = finite_or_zero(__fdiv_rn(__fsub_rn(d0, sh.rx), cell)),
+              q1 = finite_or_zero(__fdiv_rn(__fsub_rn(d1, sh.ry), cell)),
+              q2 = finite_or_zero(__fdiv_rn(__fsub_rn(d2, sh.rz), cell));
+  const float l0 = floorf(q0), l1 = floorf(q1), l2 = floorf(q2);
+  b.fx = __fsub_rn(q0, l0);
+  b.fy = __fsub_rn(q1, l1);
+  b.fz = __fsub_rn(q2, l2);
+  b.cx = pmod((int)pmid[3 * i + 0] - sh.qx + (int)l0, m.nx);
+  b.cy = pmod((int)pmid[3 * i + 1] - sh.qy + (int)l1, m.ny);
+  b.cz = pmod((int)pmid[3 * i + 2] - sh.qz + (int)l2, m.nz);
+  return b;
+}
+
+// Key of the records of particles left out by a validity mask (cic/pallas.py:
+// 133-141): they follow the last mesh row, deposit nothing, gather zero and
+// take no adjoint.  No cell has this key (meshes hold fewer than 2^32 - 1
+// cells).
+constexpr uint32_t kMaskedKey = 0xFFFFFFFFu;
+
+// A record that is safe to interpolate from (cell 0) in place of a masked one.
+__device__ __forceinline__ Rec unmasked_or_origin(const Rec& r, bool* masked) {
+  *masked = r.key == kMaskedKey;
+  if (!*masked) return r;
+  Rec z;
+  z.fx = z.fy = z.fz = 0.f;
+  z.key = 0u;
+  return z;
 }
 
 constexpr int kMaxSrcRows = 25;  // (RX+1)*(RY+1) with RX, RY <= 4
@@ -233,6 +280,12 @@ template <int C>
 __device__ __forceinline__ void gather_one(const Rec& r, uint32_t src, Mesh3 m, const float* __restrict__ mesh,
                                            float* __restrict__ out, float* __restrict__ vel, float kick,
                                            float kick2 = 0.f) {
+  if (r.key == kMaskedKey) {
+    // masked particle: zero value, velocity untouched (a zero kick)
+#pragma unroll
+    for (int c = 0; c < C; ++c) out[(int64_t)src * C + c] = 0.f;
+    return;
+  }
   Corners k;
   corners_of(r, m, k);
   // velocities loaded ahead of the corner loads (latency overlapped)

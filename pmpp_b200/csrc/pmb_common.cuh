@@ -27,6 +27,15 @@ enum Status : int {
   kCufftError = -3,
   kUnsupported = -4,
   kScratchTooSmall = -5,
+  kDeviceFlagged = -6,
+};
+
+// Conditions the kernels report through the status word of a sorted buffer
+// and the device-wide flags (pmb_sorted_status, pmb_device_status).
+enum DeviceFlag : unsigned int {
+  kFlagWaitTimeout = 1u,     // a bounded wait on bulk / TMA copies gave up
+  kFlagNonFiniteDisp = 2u,   // a displacement reaching the cell sort was NaN or infinite
+  kFlagNonFiniteValue = 4u,  // a deposited value was NaN or infinite
 };
 
 struct Mesh3 {

@@ -11,21 +11,51 @@ namespace pmb {
 int64_t scan_tmp_elems(int64_t len);
 int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t len, uint32_t* tile_sums, cudaStream_t s);
 int64_t bin_scratch_bytes(int64_t n, Mesh3 m);
+// Cell sort; shift (may be null: none) offsets the mesh origin, valid (may
+// be null: all valid) leaves masked particles out of every row.
+struct BinShift;
+// status (may be null): the sorted buffer's status word, reset here and
+// raised (DeviceFlag bits) by the sort; consumers given a raised word write
+// nothing.
 int bin_particles(const int16_t* pmid, float* disp, const float* vel, float drift, int64_t n, Mesh3 m, float cell,
-                  Rec* rec, uint32_t* perm, uint32_t* offs, void* scratch, cudaStream_t s);
+                  Rec* rec, uint32_t* perm, uint32_t* offs, void* scratch, cudaStream_t s,
+                  const BinShift* shift = nullptr, const uint8_t* valid = nullptr, uint32_t* status = nullptr);
 double fixed_point_pow2(int64_t n);
 int compute_scale(const float* val, int64_t count, int64_t n, double* scale_dev, unsigned int* tmp, cudaStream_t s);
+// n: particles the sort placed (bounds the fixed-point sums)
 int scatter_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, Mesh3 m, int C, const float* val,
                    int val_sorted, float val_const, const double* scale_dev, int mode, float src_mul, float* out,
-                   cudaStream_t s);
+                   cudaStream_t s, int64_t n, uint32_t* status);
+
+// cic_general.cu: CIC onto a mesh of another cell size (no sort)
+struct GeneralGrid {
+  int gx, gy, gz;        // the particles' periodic mesh (cells of size a1)
+  float a1, a2;          // particle-grid and target-mesh cell sizes
+  float ox, oy, oz;      // target-mesh origin in the particles' frame
+  Mesh3 t;               // target mesh shape
+};
+int64_t general_scatter_scratch_bytes(Mesh3 t, int C);
+int general_scatter(const int16_t* pmid, const float* disp, const uint8_t* valid, int64_t n, GeneralGrid G, int C,
+                    const float* val, float val_const, float* out, void* scratch, cudaStream_t s);
+int general_gather(const int16_t* pmid, const float* disp, const uint8_t* valid, int64_t n, GeneralGrid G, int C,
+                   const float* mesh, float* out, cudaStream_t s);
+int general_interp_grad(const int16_t* pmid, const float* disp, const uint8_t* valid, int64_t n, GeneralGrid G,
+                        int C, const float* mesh, const float* u, float u_const, float* disp_cot, float* wsum,
+                        cudaStream_t s);
 // offs (row offsets, may be null) enables the staged kernels.
 int gather_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, int64_t n, Mesh3 m, int C,
-                  const float* mesh, float* out, float* vel, float kick, float kick2, cudaStream_t s);
+                  const float* mesh, float* out, float* vel, float kick, float kick2, cudaStream_t s,
+                  const uint32_t* status);
 int interp_grad_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, int64_t n, Mesh3 m, int C,
                        const float* mesh, const float* u, float u_const, float cell, int accumulate, float* disp_cot,
-                       float* wsum, float* u_sorted, cudaStream_t s);
+                       float* wsum, float* u_sorted, cudaStream_t s, const uint32_t* status);
 int wait_timeouts(unsigned int* count);
+// device-wide DeviceFlag bits (the staged gathers' timeouts included), cleared
+int device_flags_take(unsigned int* flags);
 void set_gather_staging(int mode);
+// poll limit of the first bounded wait of the staged / TMA-fed kernels
+void set_wait_polls(uint32_t polls);
+uint32_t wait_polls();
 
 // spectral.cu
 int fft_r2c(Mesh3 m, int batch, float* in, float2* out, void* work, cudaStream_t s);
@@ -62,6 +92,7 @@ int pmfft_force(Mesh3 m, const float* src, float* force_meshes, float2* work, Sp
 int pmfft_force_adjoint(Mesh3 m, const float* mesh_cot, float* src_cot, float2* work, SpecTables t, GreenParams g,
                         cudaStream_t s);
 int pmfft_timeouts(unsigned int* count);
+int pmfft_timeouts_clear();
 int pmfft_set_col_ctas(int ctas);
 // process-wide switch of pmb_set_pmfft (capi.cu)
 bool pmfft_enabled();

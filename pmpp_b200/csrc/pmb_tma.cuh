@@ -28,11 +28,15 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
       : "memory");
 }
 
-// Waits for the given phase parity of the barrier; gives up after a bounded
-// number of polls (each poll may suspend the thread for a short,
-// hardware-defined time) and returns false.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); ++it) {
+// Default poll limit of a bounded wait (pmb_set_wait_limit changes the limit
+// of the first wait; the drain after a timeout always uses this one).
+constexpr uint32_t kWaitPolls = 1u << 22;
+
+// Waits for the given phase parity of the barrier; gives up after `polls`
+// polls (each poll may suspend the thread for a short, hardware-defined time;
+// 0 polls gives up at once) and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t polls = kWaitPolls) {
+  for (uint32_t it = 0; it < polls; ++it) {
     uint32_t done;
     asm volatile(
         "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
@@ -44,12 +48,23 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-// Wait used by every thread of a CTA after issuing bulk copies: on a timeout
-// the counter (a device variable of the calling file, reported by
-// pmb_wait_timeouts) is raised and the copies still in flight get one more
-// bounded wait before the caller returns without touching the staged data.
-__device__ __forceinline__ bool mbar_wait_or_flag(uint64_t* bar, uint32_t parity, unsigned int* timeouts) {
-  if (mbar_wait(bar, parity)) return true;
+// After a timed-out wait on ring slot `first` of an S-stage ring whose slots
+// [first, end) were issued: waits (kWaitPolls each) for every copy still in
+// flight, so that none lands in shared memory after the CTA has moved on.  If
+// one of these waits gives up as well, the launch's results are undefined;
+// the timeout is reported either way.
+__device__ __forceinline__ void mbar_drain(uint64_t* bars, int S, int first, int end) {
+  for (int j = first; j < end && j < first + S; ++j) mbar_wait(&bars[j % S], (uint32_t)((j / S) & 1));
+}
+
+// Wait used by every thread of a CTA after issuing bulk copies on one
+// barrier: on a timeout the counter (a device variable of the calling file,
+// reported by pmb_wait_timeouts and pmb_device_status) is raised and the
+// copies still in flight get the drain wait before the caller returns without
+// touching the staged data.
+__device__ __forceinline__ bool mbar_wait_or_flag(uint64_t* bar, uint32_t parity, unsigned int* timeouts,
+                                                  uint32_t polls = kWaitPolls) {
+  if (__syncthreads_or(!mbar_wait(bar, parity, polls)) == 0) return true;
   if (threadIdx.x == 0) atomicAdd(timeouts, 1u);
   mbar_wait(bar, parity);
   return false;

@@ -269,6 +269,7 @@ struct ColArgs {
   int nouter;      // x (y pass) or y blocks (x pass)
   int ntiles;      // ncolt * nouter * nbatch
   int ch_off;      // first input channel
+  uint32_t polls;  // poll limit of the first wait on a stage (pmb_set_wait_limit)
   const float2* tw;
   SpecTables t;
   GreenParams g;
@@ -373,13 +374,14 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
   if (t == 0)
     for (int i = 0; i < S; ++i) issue(i);
 
-  // wait for slot i; false (uniformly across the CTA) on a timeout
+  // wait for slot i; false (uniformly across the CTA) on a timeout, after
+  // draining every slot still in flight (i .. i + S - 1 were issued)
   auto acquire = [&](int i) -> bool {
     const int s = i % S;
-    const bool ok = mbar_wait(&bars[s], (i / S) & 1);
+    const bool ok = mbar_wait(&bars[s], (i / S) & 1, a.polls);
     if (__syncthreads_or(!ok)) {
       if (t == 0) atomicAdd(&g_fft_timeouts, 1u);
-      mbar_wait(&bars[s], (i / S) & 1);
+      mbar_drain(bars, S, i, slots);
       return false;
     }
     return true;
@@ -752,6 +754,7 @@ struct ZArgs {
   int64_t sb;      // nx * BY * P
   int nx, ny, nz;
   int tiles_per_ch, ntiles;
+  uint32_t polls;      // poll limit of the first wait on a stage (pmb_set_wait_limit)
   const float2* tw_m;  // W_M^k, k < M
   const float2* tw_n;  // W_nz^k, k < nz
 };
@@ -798,10 +801,10 @@ __global__ void __launch_bounds__(256, 1) z_r2c_kernel(const ZArgs a) {
     for (int i = 0; i < S; ++i) issue(i);
   for (int it = 0; it < tiles_mine; ++it) {
     const int s = it % S;
-    const bool ok = mbar_wait(&bars[s], (it / S) & 1);
+    const bool ok = mbar_wait(&bars[s], (it / S) & 1, a.polls);
     if (__syncthreads_or(!ok)) {
       if (t == 0) atomicAdd(&g_fft_timeouts, 1u);
-      mbar_wait(&bars[s], (it / S) & 1);
+      mbar_drain(bars, S, it, tiles_mine);
       return;
     }
     float2* st = smem + s * STAGE;
@@ -897,10 +900,10 @@ __global__ void __launch_bounds__(256, 1) z_c2r_kernel(const ZArgs a) {
     for (int i = 0; i < S; ++i) issue(i);
   for (int it = 0; it < tiles_mine; ++it) {
     const int s = it % S;
-    const bool ok = mbar_wait(&bars[s], (it / S) & 1);
+    const bool ok = mbar_wait(&bars[s], (it / S) & 1, a.polls);
     if (__syncthreads_or(!ok)) {
       if (t == 0) atomicAdd(&g_fft_timeouts, 1u);
-      mbar_wait(&bars[s], (it / S) & 1);
+      mbar_drain(bars, S, it, tiles_mine);
       return;
     }
     const float2* st = smem + s * STAGE;
@@ -1134,6 +1137,7 @@ int pmfft_z(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in
   a.nz = m.nz;
   a.tiles_per_ch = (int)(m.rows() / KR);
   a.ntiles = a.tiles_per_ch * batch;
+  a.polls = wait_polls();
   int st = twiddle_table(M, &a.tw_m);
   if (st != kOk) return st;
   st = twiddle_table(m.nz, &a.tw_n);
@@ -1159,6 +1163,7 @@ int pmfft_col(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float
   a.ny = m.ny;
   a.nz = m.nz;
   a.ch_off = ch_off;
+  a.polls = wait_polls();
   a.t = t;
   a.g = g;
   CUtensorMap map;
@@ -1215,6 +1220,12 @@ int pmfft_set_col_ctas(int ctas) {
 
 int pmfft_timeouts(unsigned int* count) {
   PMB_CUDA_CHECK(cudaMemcpyFromSymbol(count, g_fft_timeouts, sizeof(unsigned int)));
+  return kOk;
+}
+
+int pmfft_timeouts_clear() {
+  const unsigned int zero = 0;
+  PMB_CUDA_CHECK(cudaMemcpyToSymbol(g_fft_timeouts, &zero, sizeof(unsigned int)));
   return kOk;
 }
 

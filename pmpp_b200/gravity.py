@@ -196,6 +196,16 @@ def _correction_args(correction, a, cosmo, conf):
     return gk, transfer, radial, rl
 
 
+def _tables(conf, dev, gk, correction):
+    """Spectral tables for the correction's Green's function and force
+    derivative (corrections/core.py:396-422: force_green_kernel,
+    force_gradient_kernel)."""
+    grad = getattr(correction, "gradient_kernel", "spectral") if correction is not None else "spectral"
+    if grad not in ("spectral", "fastpm_4point"):
+        raise ValueError(f"Unsupported force-gradient kernel {grad!r}.")
+    return conf.spectral_tables("mesh", dev, gk, 1 if grad == "fastpm_4point" else 0)
+
+
 def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, force_meshes=None, acc=None,
           drift_vel=None, drift=0.0, vel_kick=None, kick=0.0, kick2=0.0, src_hat_out=None, lane=""):
     """One PM force evaluation on device tensors.
@@ -214,7 +224,7 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
     if acc is None:
         acc = torch.empty((n, 3), dtype=torch.float32, device=dev)
     gk, transfer, radial, rl = _correction_args(correction, a, cosmo, conf)
-    tables = conf.spectral_tables("mesh", dev, gk)
+    tables = _tables(conf, dev, gk, correction)
     if StageTimer.active is not None or src_hat_out is not None:
         _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc, drift_vel,
                       drift, vel_kick, kick, StageTimer.active, src_hat_out, lane, kick2)
@@ -247,7 +257,7 @@ def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *
     if disp_cot is None:
         disp_cot = torch.zeros((n, 3), dtype=torch.float32, device=dev)
     gk, transfer, radial, rl = _correction_args(correction, a, cosmo, conf)
-    tables = conf.spectral_tables("mesh", dev, gk)
+    tables = _tables(conf, dev, gk, correction)
     if StageTimer.active is not None or transfer_cot_out is not None:
         _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc_cot,
                           disp_cot, StageTimer.active, src_hat, transfer_cot_out, presorted, sorted_lane,

@@ -99,11 +99,14 @@ def evaluate(params_path, test_seeds=range(64, 80), nsteps=20, kmax=0.5):
     """Held-out evaluation with stored parameters (float32 .npy of weights then biases).
 
     Returns plain / learned max |P/P_fine - 1| (k <= kmax) averaged over the
-    seeds and the CUDA-graph times of a learned 128^3 and a plain 384^3 run."""
+    seeds, the smallest cross-correlation coefficient r(k) (k <= kmax) of the
+    final density of each coarse run with the plain 384^3 run's (both
+    deposited on the 128^3 grid; power_spectrum.py:308-345), and the
+    CUDA-graph times of a learned 128^3 and a plain 384^3 run."""
     coarse, fine = configs(nsteps)
     model = LearnedGreen("cuda", seed=0)
     model.load_parameters(torch.from_numpy(np.load(params_path)))
-    ep, el = [], []
+    ep, el, rp, rl = [], [], [], []
     for s in test_seeds:
         smp = Sample(s, coarse, fine)
         _, out_f = run_forward(smp, fine, smp.cos_f)
@@ -113,11 +116,16 @@ def evaluate(params_path, test_seeds=range(64, 80), nsteps=20, kmax=0.5):
         _, learn = run_forward(smp, coarse, smp.cos_c, model)
         ep.append(float(np.max(np.abs(pk_of(plain.disp, coarse)[1][sel] / tgt[1][sel] - 1))))
         el.append(float(np.max(np.abs(pk_of(learn.disp, coarse)[1][sel] / tgt[1][sel] - 1))))
+        rho_f = density(out_f.disp, coarse)
+        for out, acc in ((plain, rp), (learn, rl)):
+            k, r = _ps.density_to_cross_correlation(density(out.disp, coarse), rho_f, coarse)[:2]
+            acc.append(float(np.min(r[k <= kmax])))
     g_learn, g_fine = graphed_runs(smp, coarse, fine, model)
     tl = gpu_time(g_learn, reps=10)
     tf = gpu_time(g_fine, reps=5)
     return {"seeds": len(ep), "max_pk_err_plain_128": float(np.mean(ep)), "max_pk_err_learned_128": float(np.mean(el)),
-            "worst_pk_err_learned_128": float(np.max(el)), "kmax": kmax, "time_ms_learned_128": tl,
+            "worst_pk_err_learned_128": float(np.max(el)), "min_r_plain_128": float(np.min(rp)),
+            "min_r_learned_128": float(np.min(rl)), "kmax": kmax, "time_ms_learned_128": tl,
             "time_ms_plain_384": tf, "speedup": tf / tl}
 
 

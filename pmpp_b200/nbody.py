@@ -82,6 +82,77 @@ def integrate(a_prev, a_next, ptcl, cosmo, conf, correction=None):
     return ptcl
 
 
+# ---------------------------------------------------------------------------
+# Per-operation adjoints (nbody/integrator.py:429-509, 541-582, 620-686,
+# 781-837).  The cosmology cotangent is the Omega_m cotangent, a float: the
+# time factors depend on the cosmology through the growth tables of Omega_m,
+# and the force is linear in Omega_m.  NBodyRun.adjoint runs the same
+# operations fused; these are the step-by-step forms.
+# ---------------------------------------------------------------------------
+def _zeros_like(t, ref):
+    return torch.zeros_like(ref) if t is None else t.clone().float().contiguous()
+
+
+def kick_adj(a_acc, a_prev, a_next, ptcl, ptcl_cot, cosmo, cosmo_cot, conf):
+    """Reverse a kick from the post-kick state (integrator.py:541-582):
+    vel_in = vel - acc K, acc_cot += vel_cot K, cosmo_cot += dK/dOmega_m
+    sum(vel_cot acc).  Returns (ptcl_in, ptcl_cot_in, cosmo_cot)."""
+    K, dK = cosmo.kick_factor(a_acc, a_prev, a_next, with_grad=True)
+    vel = ptcl.vel.clone()
+    vc = _zeros_like(ptcl_cot.vel, vel)
+    ac = _zeros_like(ptcl_cot.acc, vel)
+    dot = torch.zeros(1, dtype=torch.float64, device=vel.device)
+    call("pmb_kick_adj", vel.data_ptr(), ptcl.acc.data_ptr(), vc.data_ptr(), ac.data_ptr(), vel.numel(), _f32(K),
+         dot.data_ptr(), stream_handle(vel.device))
+    return ptcl.replace(vel=vel), ptcl_cot.replace(vel=vc, acc=ac), float(cosmo_cot) + dK * float(dot.item())
+
+
+def drift_adj_from_output(a_vel, a_prev, a_next, ptcl, ptcl_cot, cosmo, cosmo_cot, conf):
+    """Reverse a drift from the post-drift state (integrator.py:429-509):
+    disp_in = disp - vel D, vel_cot += disp_cot D, cosmo_cot += dD/dOmega_m
+    sum(disp_cot vel).  Returns (ptcl_in, ptcl_cot_in, cosmo_cot)."""
+    D, dD = cosmo.drift_factor(a_vel, a_prev, a_next, with_grad=True)
+    disp = ptcl.disp.clone()
+    dc = _zeros_like(ptcl_cot.disp, disp)
+    vc = _zeros_like(ptcl_cot.vel, disp)
+    dot = torch.zeros(1, dtype=torch.float64, device=disp.device)
+    call("pmb_drift_adj", disp.data_ptr(), ptcl.vel.data_ptr(), dc.data_ptr(), vc.data_ptr(), disp.numel(), _f32(D),
+         dot.data_ptr(), stream_handle(disp.device))
+    return ptcl.replace(disp=disp), ptcl_cot.replace(disp=dc, vel=vc), float(cosmo_cot) + dD * float(dot.item())
+
+
+def force_adj(a, ptcl, ptcl_cot, cosmo, conf, correction=None):
+    """Pull the acceleration cotangent through one force evaluation
+    (integrator.py:620-686): disp_cot += (d acc / d disp)^T acc_cot, acc_cot
+    -> 0, and the Omega_m cotangent sum(acc_cot acc) / Omega_m (the force is
+    linear in Omega_m).  Returns (ptcl with acc recomputed, ptcl_cot_in,
+    Omega_m cotangent, None: the correction's own cotangent is trained through
+    pmpp_b200.learned)."""
+    acc, F = force(ptcl.pmid, ptcl.disp.clone(), conf, cosmo.Omega_m, a=a, cosmo=cosmo, correction=correction)
+    ac = _zeros_like(ptcl_cot.acc, acc)
+    dc = _zeros_like(ptcl_cot.disp, acc)
+    force_vjp(ptcl.pmid, ptcl.disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=correction)
+    om = float((ac.double() * acc.double()).sum()) / _om32(cosmo.Omega_m)
+    return ptcl.replace(acc=acc), ptcl_cot.replace(disp=dc, acc=torch.zeros_like(ac)), om, None
+
+
+def integrate_adj(a_prev, a_next, ptcl, ptcl_cot, cosmo, cosmo_cot, conf, correction=None, correction_cot=None):
+    """Reverse one macro step (integrator.py:781-837) with the stage adjoints
+    above, restoring the incoming acceleration after each force stage.
+    Returns (ptcl_in, ptcl_cot_in, cosmo_cot, correction_cot)."""
+    for st in reversed(_schedule(a_prev, a_next, conf)):
+        if st[0] == "kick":
+            ptcl, ptcl_cot, cosmo_cot = kick_adj(st[1], st[2], st[3], ptcl, ptcl_cot, cosmo, cosmo_cot, conf)
+            continue
+        _, a_vel, a_disp, a_disp_next, a_acc_in = st
+        ptcl, ptcl_cot, om, _ = force_adj(a_disp_next, ptcl, ptcl_cot, cosmo, conf, correction)
+        cosmo_cot = float(cosmo_cot) + om
+        ptcl, ptcl_cot, cosmo_cot = drift_adj_from_output(a_vel, a_disp, a_disp_next, ptcl, ptcl_cot, cosmo,
+                                                          cosmo_cot, conf)
+        ptcl = force_state(a_acc_in, ptcl, cosmo, conf, correction)
+    return ptcl, ptcl_cot, cosmo_cot, correction_cot
+
+
 class NBodyRun:
     """Fused forward integration that keeps the final force meshes for the adjoint."""
 

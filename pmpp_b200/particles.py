@@ -19,6 +19,9 @@ class Particles:
     vel: Optional[torch.Tensor] = None
     acc: Optional[torch.Tensor] = None
     attr: Optional[dict] = None
+    # bool (N,): True marks an unused (padding) slot, left out of every CIC
+    # operation (particles.py:33-127 unused_index; cic/scatter.py:258)
+    unused_index: Optional[torch.Tensor] = None
 
     def __post_init__(self):
         if self.attr is not None:  # custom per-particle features in the float dtype (particles.py:115-118)
@@ -31,7 +34,8 @@ class Particles:
         """The particles selected by key (an index, slice or mask) in every field."""
         g = lambda t: None if t is None else t[key]
         attr = None if self.attr is None else {k: v[key] for k, v in self.attr.items()}
-        return Particles(self.conf, self.pmid[key], self.disp[key], g(self.vel), g(self.acc), attr)
+        return Particles(self.conf, self.pmid[key], self.disp[key], g(self.vel), g(self.acc), attr,
+                         g(self.unused_index))
 
     def replace(self, **kw):
         return replace(self, **kw)
@@ -39,7 +43,15 @@ class Particles:
     def clone(self):
         c = lambda t: None if t is None else t.clone()
         attr = None if self.attr is None else {k: v.clone() for k, v in self.attr.items()}
-        return Particles(self.conf, self.pmid, c(self.disp), c(self.vel), c(self.acc), attr)
+        return Particles(self.conf, self.pmid, c(self.disp), c(self.vel), c(self.acc), attr, c(self.unused_index))
+
+    def valid_mask(self):
+        """uint8 (N,) device mask of the used slots (1) for the C ABI, or None
+        when every slot is used."""
+        if self.unused_index is None:
+            return None
+        u = torch.as_tensor(self.unused_index, device=self.disp.device)
+        return (~u.to(torch.bool)).to(torch.uint8).contiguous()
 
     def raveled_id(self, dtype=torch.int64, wrap=False):
         """Raveled mesh index of each anchor, ((x My) + y) Mz + z (particles.py:729-772).

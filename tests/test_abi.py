@@ -22,7 +22,7 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in declared_symbols() if not hasattr(L, s)]
     assert not missing, missing
     assert set(declared_symbols()) <= set(_lib.exported_symbols()) | {"pmb_last_error"}
-    assert L.pmb_abi_version() == 2
+    assert L.pmb_abi_version() == 3
 
 
 def test_workspace_queries_without_device():
@@ -71,3 +71,30 @@ def test_ensemble_create_rejects_bad_layouts_without_device_work():
     assert st == -1
     st, _ = create([(8, 8, 0)])
     assert st == -1
+
+
+def test_count_and_shape_limits_rejected_on_the_host():
+    """Particle counts past the uint32 permutation (n >= 2^32 - 1) and meshes of
+    2^32 cells or more (uint32 cell keys) are rejected before any device work,
+    with the output pointers never touched (they are null here)."""
+    from pmpp_b200 import _lib
+    L = _lib.lib()
+    big_n = 2**32
+    calls = [
+        ("pmb_sort_rows", (None, None, None, 0.0, big_n, 16, 16, 16, 1.0, None, None, 1 << 40, None)),
+        ("pmb_sort_rows_ex", (None, None, None, 0.0, big_n, 16, 16, 16, 1.0, 0.0, 0.0, 0.0, None, None, None, 1 << 40,
+                              None)),
+        ("pmb_scatter_rows", (None, big_n, 16, 16, 16, 1, None, 0, 1.0, 0, 1.0, None, None, None)),
+        ("pmb_gather_rows", (None, big_n, 16, 16, 16, 3, None, None, None, 0.0, None)),
+        ("pmb_interp_grad_rows", (None, big_n, 16, 16, 16, 1, None, None, 1.0, 1.0, 0, None, None, None, None)),
+        # 2048 x 2048 x 1024 = 2^32 cells
+        ("pmb_sort_rows", (None, None, None, 0.0, 10, 2048, 2048, 1024, 1.0, None, None, 1 << 40, None)),
+        ("pmb_scatter_rows", (None, 10, 2048, 2048, 1024, 1, None, 0, 1.0, 0, 1.0, None, None, None)),
+        ("pmb_force", (None, None, None, 0.0, 10, 2048, 2048, 1024, 1.0, 1.0, 1.0, None, 0, 0, None, None, 0, None,
+                       None, None, 0.0, None, 1 << 40, None)),
+        ("pmb_scatter_density_noalloc", (None, None, big_n, 16, 16, 16, 1.0, 1.0, None, None)),
+    ]
+    for name, args in calls:
+        st = getattr(L, name)(*args)
+        assert st == -1, (name, st, L.pmb_last_error())
+    assert L.pmb_set_wait_limit(-1) == 0

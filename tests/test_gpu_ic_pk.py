@@ -3,7 +3,7 @@
 Bars: white-noise hashes bit-exact and the Gaussian modes within float32
 round-off of the oracle; shared low-k modes bitwise equal across resolutions
 (reference tests/test_nested_white_noise.py:53-68); linear modes, LPT states
-and P(k) within 2e-5; shell mode counts exact; adjoints within 2e-3 of
+and P(k) within 1e-5; shell mode counts exact; adjoints within 2e-3 of
 float64 central differences of the oracle.
 """
 import numpy as np
@@ -64,7 +64,7 @@ def test_linear_modes_matches_oracle():
     w = pm.white_noise_nested(3, conf)
     lm = pm.linear_modes(w, cos, conf).cpu().numpy()
     ref = opm.linear_modes(w.cpu().numpy(), oc, co)
-    assert np.abs(lm - ref).max() < 2e-5 * np.abs(ref).max()
+    assert np.abs(lm - ref).max() < 1e-5 * np.abs(ref).max()
 
 
 @pytest.mark.parametrize("order", [1, 2])
@@ -77,8 +77,8 @@ def test_lpt_matches_oracle(order):
     ptcl = pl.lpt(lm, cos, conf)
     pmid, disp, vel = opm.lpt(lm.cpu().numpy(), oc, co)
     assert np.array_equal(ptcl.pmid.cpu().numpy(), pmid)
-    assert rel_err(ptcl.disp.cpu().numpy(), disp) < 2e-5
-    assert rel_err(ptcl.vel.cpu().numpy(), vel) < 2e-5
+    assert rel_err(ptcl.disp.cpu().numpy(), disp) < 1e-5
+    assert rel_err(ptcl.vel.cpu().numpy(), vel) < 1e-5
 
 
 def test_lpt_adjoint_vs_finite_differences():
@@ -124,7 +124,7 @@ def test_shell_statistics_and_pk_match_oracle():
     kk, pk, nm = ps.density_to_pk(torch.from_numpy(rho).cuda(), conf)
     rk2, rpk, rnm = opm.density_to_pk(rho.astype(np.float64), co)
     assert np.array_equal(nm, rnm)
-    assert rel_err(pk, rpk) < 2e-5
+    assert rel_err(pk, rpk) < 1e-5
 
 
 def test_pk_loss_gradient_vs_finite_differences():

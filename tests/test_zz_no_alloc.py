@@ -5,9 +5,11 @@ scratch) cannot call cudaMalloc and cannot supply the workspace the regular
 entry points take; this entry point keeps its scratch in a fixed device array
 inside the library.  The test calls it through the C ABI twice in a row (the
 second call sees the first call's leftovers in the shared array) and compares
-each result with the workspace path pmb_sort_rows + pmb_scatter_rows, within
-the tolerance the other scatter tests use.  It lives in its own file so that a
-run stopping at the first failure has already run every other test.
+each result with the workspace path pmb_sort_rows + pmb_scatter_rows bit for
+bit (both sum the same exact fixed-point contributions), including a problem
+just under the fixed scratch size; one just over it is rejected before any
+work is queued.  It lives in its own file so that a run stopping at the first
+failure has already run every other test.
 """
 import numpy as np
 import pytest
@@ -52,9 +54,8 @@ def _noalloc_scatter(pmid, disp, dims, cell, val):
     return out
 
 
-def _rel(a, b):
-    a, b = a.double().cpu(), b.double().cpu()
-    return float((a - b).abs().max() / b.abs().max())
+def _bits(t):
+    return t.cpu().numpy().view(np.uint32)
 
 
 def test_noalloc_scatter_matches_workspace_path_on_consecutive_calls():
@@ -66,8 +67,27 @@ def test_noalloc_scatter_matches_workspace_path_on_consecutive_calls():
             ref = _reference_scatter(pmid, disp, dims, 1.0, val)
             got = _noalloc_scatter(pmid, disp, dims, 1.0, val)
             torch.cuda.synchronize()
-            assert _rel(got, ref) < 2e-6
+            assert np.array_equal(_bits(got), _bits(ref))
             np.testing.assert_allclose(float(got.double().sum()), val * pmid.shape[0], rtol=1e-5)
+
+
+# A 128^3 mesh needs 28 B per particle plus 12 B per mesh row and 768 B for
+# alignment, the scale and the status word: 28 n + 198144 bytes for n a
+# multiple of 64, so 1191296 particles fill the 32 MiB (33554432 B) scratch
+# exactly and 1191360 do not fit.
+N_FITS, N_OVER = 1191296, 1191360
+
+
+def test_noalloc_scatter_just_under_the_limit():
+    rng = np.random.default_rng(4)
+    pmid = torch.from_numpy(rng.integers(0, 128, size=(N_FITS, 3)).astype(np.int16)).cuda()
+    disp = torch.from_numpy(rng.uniform(-2.0, 2.0, size=(N_FITS, 3)).astype(np.float32)).cuda()
+    dims = (128, 128, 128)
+    for _ in range(2):
+        ref = _reference_scatter(pmid, disp, dims, 1.0, 0.5)
+        got = _noalloc_scatter(pmid, disp, dims, 1.0, 0.5)
+        torch.cuda.synchronize()
+        assert np.array_equal(_bits(got), _bits(ref))
 
 
 def test_noalloc_scatter_rejects_oversized_problems():
@@ -79,3 +99,12 @@ def test_noalloc_scatter_rejects_oversized_problems():
                                                     1.0, disp.data_ptr(), stream_handle())
     assert status == -1
     assert b"32 MiB" in _lib.lib().pmb_last_error()
+    # just over the limit on a 128^3 mesh: rejected, the output left untouched
+    pmid = torch.zeros((N_OVER, 3), dtype=torch.int16, device="cuda")
+    disp = torch.zeros((N_OVER, 3), dtype=torch.float32, device="cuda")
+    out = torch.full((128, 128, 128), 7.0, device="cuda")
+    status = _lib.lib().pmb_scatter_density_noalloc(pmid.data_ptr(), disp.data_ptr(), N_OVER, 128, 128, 128, 1.0,
+                                                    1.0, out.data_ptr(), stream_handle())
+    assert status == -1
+    torch.cuda.synchronize()
+    assert bool((out == 7.0).all())
