@@ -52,9 +52,13 @@ def set_fft_workers(n):
     _fft.workers = int(n)
 
 
-def _chunks(n):
-    """Particle ranges of the threaded CIC (None: run serially)."""
-    w = _fft.workers
+def _chunks(n, partial_bytes=0):
+    """Particle ranges of the threaded CIC (None: run serially).  At most 16
+    chunks, and few enough that the partial meshes of a deposit (partial_bytes
+    each, all in flight at once) stay within 8 GB."""
+    w = min(_fft.workers, 16)
+    if partial_bytes > 0:
+        w = min(w, max(1, int(8e9 // partial_bytes)))
     if w <= 1 or n < 65536:
         return None
     b = np.linspace(0, n, w + 1).astype(np.int64)
@@ -65,6 +69,17 @@ def _pmap(fn, ranges):
     from concurrent.futures import ThreadPoolExecutor
     with ThreadPoolExecutor(len(ranges)) as ex:
         return list(ex.map(lambda r: fn(*r), ranges))
+
+
+def _psum(fn, ranges):
+    """Sum of fn over the chunks, in chunk order, keeping one running total."""
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(len(ranges)) as ex:
+        it = ex.map(lambda r: fn(*r), ranges)
+        total = next(it)
+        for part in it:
+            total = total + part
+        return total
 
 
 def _rows(x, lo, hi):
@@ -403,14 +418,14 @@ def scatter(pmid, disp, conf, val=None, mesh_shape=None, offset=0, cell_size=Non
     float atomics; the difference is below the dtype's rounding)."""
     mesh_shape = conf.mesh_shape if mesh_shape is None else mesh_shape
     kw = dict(offset=offset, cell_size=cell_size)
-    ranges = _chunks(pmid.shape[0])
+    nch = 1 if val is None or np.ndim(val) <= 1 else np.shape(val)[1]
+    ranges = _chunks(pmid.shape[0], 8 * math.prod(mesh_shape) * nch)
     if ranges is not None:
         # threaded: partial meshes of particle chunks, summed in chunk order
         if val is None:
             val = default_val(conf)
-        parts = _pmap(lambda lo, hi: _scatter1(pmid[lo:hi], disp[lo:hi], conf, _rows(val, lo, hi), mesh_shape,
-                                               valid=_rows(valid, lo, hi), **kw), ranges)
-        return sum(parts[1:], parts[0])
+        return _psum(lambda lo, hi: _scatter1(pmid[lo:hi], disp[lo:hi], conf, _rows(val, lo, hi), mesh_shape,
+                                              valid=_rows(valid, lo, hi), **kw), ranges)
     return _scatter1(pmid, disp, conf, val, mesh_shape, valid=valid, **kw)
 
 
@@ -493,12 +508,17 @@ def gather_vjp(pmid, disp, conf, mesh, val_cot, offset=0, cell_size=None, valid=
     """cic/gather.py:475-548: disp_cot = sum_b (sum_c val_cot mesh_c[i_b]) grad_b / cell,
     mesh_cot_c = scatter of val_cot_c w_b."""
     kw = dict(offset=offset, cell_size=cell_size)
-    ranges = _chunks(pmid.shape[0])
+    ranges = _chunks(pmid.shape[0], 8 * mesh.size)
     if ranges is not None:
-        parts = _pmap(lambda lo, hi: _gather_vjp1(pmid[lo:hi], disp[lo:hi], conf, mesh, val_cot[lo:hi],
-                                                  valid=_rows(valid, lo, hi), **kw), ranges)
-        mcs = [p[1] for p in parts]
-        return np.concatenate([p[0] for p in parts]), sum(mcs[1:], mcs[0])
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(len(ranges)) as ex:
+            it = ex.map(lambda r: _gather_vjp1(pmid[r[0]:r[1]], disp[r[0]:r[1]], conf, mesh, val_cot[r[0]:r[1]],
+                                               valid=_rows(valid, r[0], r[1]), **kw), ranges)
+            dcs, mesh_cot = [], None
+            for dc, mc in it:  # chunk order; one running mesh total
+                dcs.append(dc)
+                mesh_cot = mc if mesh_cot is None else mesh_cot + mc
+        return np.concatenate(dcs), mesh_cot
     return _gather_vjp1(pmid, disp, conf, mesh, val_cot, valid=valid, **kw)
 
 

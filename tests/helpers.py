@@ -48,9 +48,13 @@ def fixed_point_scatter(pmid, disp, conf_o, val, offset=0, valid=None, cell_size
         contrib = np.broadcast_to((v[:, None] if v.ndim == 1 else v) * w, idx.shape)
         q = np.rint(contrib.astype(np.float64) * scale)[keep]
         # integer sums in float64 are exact (any order) while every partial sum
-        # stays below 2^53, which the sum of |q| per cell bounds
+        # stays below 2^53, which the sum of |q| per cell bounds; else int64
         bound = np.bincount(idx[keep], weights=np.abs(q), minlength=M)
-        assert bound.max() < 2.0**53
-        acc = np.bincount(idx[keep], weights=q, minlength=M)
+        if bound.max() < 2.0**53:
+            acc = np.bincount(idx[keep], weights=q, minlength=M)
+        else:
+            acc = np.zeros(M, np.int64)
+            np.add.at(acc, idx[keep], q.astype(np.int64))
+            acc = acc.astype(np.float64)
         outs.append((acc * (1.0 / scale)).astype(np.float32).reshape(mesh_shape))
     return outs[0] if val.ndim <= 1 else np.stack(outs)

@@ -176,12 +176,12 @@ def test_force_with_analytic_corrections_matches_oracle(model, pmfft):
     """The window compensation (corrections/window.py:229-265), the discrete
     Laplacian (gravity.py:122-171) and FastPM's 4-point gradient
     (gravity.py:355-391) in the force and its adjoint, through the FFT pass
-    chain (64^3 mesh) and the cuFFT route, within 1e-5 of the oracle."""
+    chain (128^3 mesh) and the cuFFT route, within 1e-5 of the oracle."""
     import pmpp_b200 as pb
     from pmpp_b200 import _lib
     from pmpp_b200.corrections import init_potential_correction
-    co = opm.Conf(4.0, (32, 32, 32), mesh_shape=2, a_start=0.1)
-    conf = pb.Configuration(4.0, (32, 32, 32), 2, a_start=0.1, device="cuda")
+    co = opm.Conf(4.0, (64, 64, 64), mesh_shape=2, a_start=0.1)
+    conf = pb.Configuration(4.0, (64, 64, 64), 2, a_start=0.1, device="cuda")
     pmid, disp = random_particles(co, 5, 1.0)
     corr = init_potential_correction(model)
     gk = "discrete_laplacian" if corr.green_kernel == 1 else "continuum"

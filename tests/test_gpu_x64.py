@@ -84,8 +84,8 @@ def test_x64_config0_matches_oracle(seed):
 def test_float32_drift_from_float64_config0():
     """The float32 path against the float64 build on config 0 (same seed, 2LPT +
     10 KDK steps): the multi-step drift of float32 round-off, reported on its
-    own beside the float64 gate above.  Measured: final positions ~1e-3 cells,
-    P(k) ~1e-4; bars: 5e-2 cells, 1e-3 in P(k)."""
+    own beside the float64 gate above.  Measured: final positions 9e-6 cells,
+    P(k) 2.2e-6; bars: 1e-4 cells, 1e-5 in P(k)."""
     import pmpp_b200 as pb
     from pmpp_b200 import lpt as pl, modes as pm, power_spectrum as ps
     res = {}
@@ -102,5 +102,5 @@ def test_float32_drift_from_float64_config0():
     drift_pos = float(np.abs(dx).max() / conf.cell_size)
     drift_pk = float(np.max(np.abs(p32 / p64 - 1)))
     print(f"float32 vs float64, config 0: max position drift {drift_pos:.3e} cells, max |P32/P64 - 1| {drift_pk:.3e}")
-    assert drift_pos < 5e-2
-    assert drift_pk < 1e-3
+    assert drift_pos < 1e-4
+    assert drift_pk < 1e-5
