@@ -241,6 +241,19 @@ int pmb_force2(const int16_t* pmid, float* disp, const float* drift_vel, float d
                float cell, float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
                const float* transfer, const float* radial, int radial_len, float* force_meshes, float* acc,
                float* vel_kick, float kick, float kick2, void* workspace, int64_t workspace_bytes, void* stream);
+/* Low-memory forward force: the streamed gravity of nbody/gravity.py:643-658
+ * (forward only, no correction tape): sort (optional drift), deposit of the
+ * Poisson source, R2C, then one force component at a time -- its Green x
+ * gradient spectrum, C2R into one real mesh, a 1-channel gather -- and acc
+ * (n,3) assembled from the three.  Holds one real mesh and two half spectra
+ * (about 12 bytes per cell) instead of the fused force's three real meshes
+ * and its spectral channels (about 36); cuFFT route, same arithmetic per
+ * component as pmb_force's cuFFT route. */
+int64_t pmb_force_streamed_workspace_bytes(int64_t n, int nx, int ny, int nz);
+int pmb_force_streamed(const int16_t* pmid, float* disp, const float* drift_vel, float drift, int64_t n, int nx,
+                       int ny, int nz, float cell, float val_const, float src_mul, const float* tables, int has_masks,
+                       int green_kernel, const float* transfer, const float* radial, int radial_len, float* acc,
+                       void* workspace, int64_t workspace_bytes, void* stream);
 /* Transpose of pmb_force w.r.t. disp given force_meshes at the same disp
  * (the force VJP of nbody/integrator.py:620-686): disp_cot (n,3) +=
  * gather-adjoint position term + scatter-adjoint term of the density. */

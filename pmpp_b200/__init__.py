@@ -14,14 +14,15 @@ from .cosmology import Cosmology, SimpleLCDM, boltzmann, growth, linear_power
 from .particles import Particles, pmid_to_idx
 from . import cic
 from .cic import scatter, gather, scatter_vjp, gather_vjp
-from .gravity import gravity, gravity_vjp
+from .gravity import gravity, gravity_vjp, gravity_streamed
 from .nbody import (nbody, nbody_adj, integrate, kick, drift, NBodyRun, kick_adj, drift_adj_from_output,
-                    force_adj, integrate_adj)
+                    force_adj, integrate_adj, nbody_low_memory)
 
 __all__ = [
     "Configuration", "Cosmology", "SimpleLCDM", "boltzmann", "growth", "linear_power", "Particles", "pmid_to_idx", "cic", "scatter",
     "gather", "scatter_vjp", "gather_vjp", "gravity", "gravity_vjp", "nbody", "nbody_adj", "integrate", "kick",
-    "drift", "NBodyRun", "kick_adj", "drift_adj_from_output", "force_adj", "integrate_adj"
+    "drift", "NBodyRun", "kick_adj", "drift_adj_from_output", "force_adj", "integrate_adj", "gravity_streamed",
+    "nbody_low_memory"
 ]
 from . import modes, lpt, power_spectrum, pipeline  # noqa: E402
 from .modes import white_noise_nested, linear_modes  # noqa: E402

@@ -469,6 +469,68 @@ int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float dr
                     workspace_bytes, stream);
 }
 
+// ---------------------------------------------------------------------------
+// Low-memory forward force
+// ---------------------------------------------------------------------------
+static int64_t force_streamed_layout(int64_t n, Mesh3 m, void* ws, int64_t cap, void** sorted, void** bins,
+                                     void** scale16, float** real, float2** src_hat, float2** comp_hat,
+                                     float** planar, void** work) {
+  Carve c(ws, cap);
+  *sorted = c.take(sorted_bytes(n, m));
+  *bins = c.take(bin_scratch_bytes(n, m));
+  *scale16 = c.take(16);
+  *real = (float*)c.take(4 * m.cells());
+  *src_hat = (float2*)c.take(8 * m.half_cells());
+  *comp_hat = (float2*)c.take(8 * m.half_cells());
+  *planar = (float*)c.take(12 * n);
+  const int64_t w = fft_work_bytes(m, 1);
+  if (w < 0) return -1;
+  *work = c.take(w);
+  return c.off;
+}
+
+int64_t pmb_force_streamed_workspace_bytes(int64_t n, int nx, int ny, int nz) {
+  void *a, *b, *c, *w;
+  float *r, *p;
+  float2 *sh, *ch;
+  return force_streamed_layout(n, Mesh3{nx, ny, nz}, nullptr, 0, &a, &b, &c, &r, &sh, &ch, &p, &w);
+}
+
+int pmb_force_streamed(const int16_t* pmid, float* disp, const float* drift_vel, float drift, int64_t n, int nx,
+                       int ny, int nz, float cell, float val_const, float src_mul, const float* tables, int has_masks,
+                       int green_kernel, const float* transfer, const float* radial, int radial_len, float* acc,
+                       void* workspace, int64_t workspace_bytes, void* stream) {
+  Mesh3 m{nx, ny, nz};
+  PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_force_streamed: unsupported mesh shape");
+  PMB_REQUIRE(n >= 0 && n < 4294967295ll, "pmb_force_streamed: particle count out of range");
+  PMB_REQUIRE(cell > 0.f, "pmb_force_streamed: cell size must be positive");
+  void *sorted, *bins, *scale16, *work;
+  float *real, *planar;
+  float2 *src_hat, *comp_hat;
+  const int64_t need = force_streamed_layout(n, m, workspace, workspace_bytes, &sorted, &bins, &scale16, &real,
+                                             &src_hat, &comp_hat, &planar, &work);
+  PMB_REQUIRE(need >= 0, "pmb_force_streamed: cuFFT plan creation failed");
+  if (need > workspace_bytes) {
+    set_last_error("pmb_force_streamed: workspace too small");
+    return kScratchTooSmall;
+  }
+  cudaStream_t s = S(stream);
+  PMB_TRY(pmb_sort_rows(pmid, disp, drift_vel, drift, n, nx, ny, nz, cell, sorted, bins, bin_scratch_bytes(n, m),
+                        stream));
+  PMB_TRY(pmb_scatter_rows(sorted, n, nx, ny, nz, 1, nullptr, 0, val_const, 1, src_mul, real, scale16, stream));
+  PMB_TRY(fft_r2c(m, 1, real, src_hat, work, s));
+  SortedView v = sorted_view(sorted, n, m);
+  const SpecTables t = make_tables(tables, m, has_masks);
+  const GreenParams g = make_green(green_kernel, transfer, radial, radial_len, (float)(1.0 / (double)m.cells()));
+  for (int d = 0; d < 3; ++d) {
+    PMB_TRY(green_gradient_component(src_hat, comp_hat, m, t, g, d, s));
+    PMB_TRY(fft_c2r(m, 1, comp_hat, real, work, s));
+    PMB_TRY(gather_sorted(v.rec, v.perm, v.offs, n, m, 1, real, planar + (int64_t)d * n, nullptr, 0.f, 0.f, s,
+                          v.status));
+  }
+  return interleave3(planar, acc, n, s);
+}
+
 static int64_t force_vjp_layout(int64_t n, Mesh3 m, void* ws, int64_t cap, void** sorted, void** bins, void** scale16,
                                 float** cot_sorted, float** mesh_cot, float2** spec3, float2** src_hat, float** src_cot,
                                 void** work) {

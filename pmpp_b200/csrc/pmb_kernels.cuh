@@ -77,6 +77,11 @@ int green_gradient(const float2* src_hat, float2* grad_hat, Mesh3 m, SpecTables 
 int green_gradient_adjoint(const float2* grad_cot_hat, float2* src_cot_hat, Mesh3 m, SpecTables t, GreenParams g,
                            cudaStream_t s);
 int scale_real(float* x, int64_t count, float a, float b, cudaStream_t s);
+// component d of the forward multiplier (streamed force)
+int green_gradient_component(const float2* src_hat, float2* out, Mesh3 m, SpecTables t, GreenParams g, int d,
+                             cudaStream_t s);
+// acc (n,3) from three planar (3,n) channels
+int interleave3(const float* planar, float* acc, int64_t n, cudaStream_t s);
 
 // pmfft.cu: hand-written FFT passes for power-of-two meshes over the
 // y-blocked half-spectrum layout (see pmfft.cu for the layout and modes).

@@ -268,6 +268,29 @@ __global__ void green_gradient_adjoint_kernel4(const float2* __restrict__ gc, fl
   }
 }
 
+// One gradient component d of the forward multiplier (the streamed force
+// builds the components one at a time into a single spectrum).
+__global__ void green_gradient_component_kernel(const float2* __restrict__ src, float2* __restrict__ out, Mesh3 m,
+                                                SpecTables t, GreenParams g, int d) {
+  const int64_t nzh = m.nz / 2 + 1, ny = m.ny;
+  const int64_t total = m.half_cells();
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = j / nzh, ix = r / ny;
+    float2 o[3];
+    green_gradient_value(src[j], j, (int)ix, (int)(r - ix * ny), (int)(j - r * nzh), m, t, g, o);
+    out[j] = o[d];
+  }
+}
+
+// acc[3 i + d] = planar[d * n + i]
+__global__ void interleave3_kernel(const float* __restrict__ planar, float* __restrict__ acc, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    acc[3 * i] = planar[i];
+    acc[3 * i + 1] = planar[n + i];
+    acc[3 * i + 2] = planar[2 * n + i];
+  }
+}
+
 static bool vec4_ok(Mesh3 m, const void* a, const void* b) {
   return m.half_cells() % 4 == 0 && m.half_cells() < 2147483648ll && ((uintptr_t)a & 31) == 0 &&
          ((uintptr_t)b & 31) == 0;
@@ -287,6 +310,19 @@ int green_gradient(const float2* src_hat, float2* grad_hat, Mesh3 m, SpecTables 
     green_gradient_kernel<uint32_t><<<grid, 256, 0, s>>>(src_hat, grad_hat, m, t, g);
   else
     green_gradient_kernel<int64_t><<<grid, 256, 0, s>>>(src_hat, grad_hat, m, t, g);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int green_gradient_component(const float2* src_hat, float2* out, Mesh3 m, SpecTables t, GreenParams g, int d,
+                             cudaStream_t s) {
+  green_gradient_component_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(src_hat, out, m, t, g, d);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int interleave3(const float* planar, float* acc, int64_t n, cudaStream_t s) {
+  if (n > 0) interleave3_kernel<<<grid_for(n, 256), 256, 0, s>>>(planar, acc, n);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }

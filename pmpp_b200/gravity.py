@@ -280,6 +280,35 @@ def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *
     return disp_cot
 
 
+def force_streamed(pmid, disp, conf, omega_m, *, acc=None, drift_vel=None, drift=0.0):
+    """The low-memory forward force (pmb_force_streamed): one force component
+    at a time through one real mesh; forward only."""
+    require_cuda(pmid, disp, drift_vel)
+    n = pmid.shape[0]
+    nx, ny, nz = conf.mesh_shape
+    dev = disp.device
+    if acc is None:
+        acc = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    wb = lib().pmb_force_streamed_workspace_bytes(n, nx, ny, nz)
+    if wb < 0:
+        raise RuntimeError("pmb_force_streamed_workspace_bytes failed: " + lib().pmb_last_error().decode())
+    ws = workspace(wb, dev, "force_streamed")
+    tables = conf.spectral_tables("mesh", dev, 0)
+    call("pmb_force_streamed", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
+         float(conf.cell_size), float(conf.mesh_size / conf.ptcl_num), 1.5 * _om32(omega_m), tables.data_ptr(),
+         int(conf.has_particle_nyquist_masks), 0, None, None, 0, acc.data_ptr(), ws.data_ptr(), ws.numel(),
+         stream_handle(dev))
+    return acc
+
+
+def gravity_streamed(a, ptcl, cosmo, conf, correction=None):
+    """Uncorrected PM accelerations with sequential component FFTs
+    (nbody/gravity.py:643-658): the memory-lean forward path."""
+    if correction is not None:
+        raise ValueError("streamed gravity currently requires correction=None.")
+    return force_streamed(ptcl.pmid, ptcl.disp, conf, cosmo.Omega_m)
+
+
 def gravity(a, ptcl, cosmo, conf, correction=None):
     """Gravitational accelerations [H_0^2 L] (gravity.py:786-814)."""
     acc, _ = force(ptcl.pmid, ptcl.disp, conf, cosmo.Omega_m, a=a, cosmo=cosmo, correction=correction)

@@ -377,6 +377,41 @@ class NBodyRun:
         return (ptcl.replace(disp=disp, vel=vel, acc=acc), Particles(conf, pmid, dc, vc, ac), float(om_cot))
 
 
+def nbody_low_memory(ptcl, cosmo, conf, reverse=False, correction=None):
+    """Forward-only KDK run with the streamed force (nbody/solver.py:559-602,
+    nbody_low_memory): each force holds one real mesh instead of three, the
+    drift is fused into the force's cell sort and nothing is kept for an
+    adjoint.  Rejects reverse integration and force corrections, as the
+    reference does."""
+    if reverse:
+        raise ValueError("nbody_low_memory does not support reverse integration.")
+    if correction is not None:
+        raise ValueError("nbody_low_memory does not support force corrections.")
+    if conf.float_dtype != torch.float32:
+        raise ValueError("nbody_low_memory runs the float32 path")
+    from .gravity import force_streamed
+    a = conf.a_nbody
+    dev = ptcl.disp.device
+    s = stream_handle(dev)
+    disp = ptcl.disp.clone()
+    vel = ptcl.vel.clone() if ptcl.vel is not None else torch.zeros_like(disp)
+    acc = force_streamed(ptcl.pmid, disp, conf, cosmo.Omega_m)
+    for a_prev, a_next in zip(a[:-1], a[1:]):
+        stages = _schedule(a_prev, a_next, conf)
+        i = 0
+        while i < len(stages):
+            st = stages[i]
+            if st[0] == "kick":
+                call("pmb_axpy", vel.data_ptr(), acc.data_ptr(), vel.numel(),
+                     _f32(cosmo.kick_factor(st[1], st[2], st[3])), s)
+            else:
+                # drift fused into the streamed force's sort
+                D = _f32(cosmo.drift_factor(st[1], st[2], st[3]))
+                force_streamed(ptcl.pmid, disp, conf, cosmo.Omega_m, acc=acc, drift_vel=vel, drift=D)
+            i += 1
+    return ptcl.replace(disp=disp, vel=vel, acc=acc)
+
+
 def nbody(ptcl, cosmo, conf, reverse=False, correction=None):
     """Advance particles through conf.a_nbody (nbody/solver.py:605-642)."""
     a = conf.a_nbody[::-1] if reverse else conf.a_nbody

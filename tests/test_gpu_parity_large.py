@@ -116,7 +116,8 @@ def test_c1_cic_sort_force_and_adjoints(which):
 
 def test_c2_force_adjoint_kicks_keys_and_slab():
     import pmpp_b200 as pb
-    from pmpp_b200 import _lib, gravity, lpt, modes, x64
+    from pmpp_b200 import _lib, lpt, modes, x64
+    from pmpp_b200.gravity import force, force_vjp
     from pmpp_b200.cic import SortedParticles
     n1 = 512
     conf = pb.Configuration(2.0, (n1, ) * 3, 2, a_start=0.1, device="cuda")
@@ -128,7 +129,7 @@ def test_c2_force_adjoint_kicks_keys_and_slab():
     om = cos.Omega_m
     assert _lib.pmfft_active(*conf.mesh_shape)
     # force: pass chain (float32) against the float64 path
-    acc, F = gravity.force(pmid, disp.clone(), conf, om)
+    acc, F = force(pmid, disp.clone(), conf, om)
     acc = acc.cpu().numpy()
     del F
     from pmpp_b200 import runtime
@@ -148,10 +149,10 @@ def test_c2_force_adjoint_kicks_keys_and_slab():
     for route in (True, False):
         _lib.set_pmfft(route)
         try:
-            a_, F = gravity.force(pmid, disp.clone(), conf, om)
-            res[route] = gravity.force_vjp(pmid, disp, conf, om, F, cot).cpu().numpy()
+            a_, F = force(pmid, disp.clone(), conf, om)
+            res[route] = force_vjp(pmid, disp, conf, om, F, cot).cpu().numpy()
             if route:
-                d2 = gravity.force_vjp(pmid, disp, conf, om, F, cot, presorted=True).cpu().numpy()
+                d2 = force_vjp(pmid, disp, conf, om, F, cot, presorted=True).cpu().numpy()
                 assert np.array_equal(d2.view(np.uint32), res[route].view(np.uint32))
             del a_, F
             runtime.release_workspaces()
@@ -164,7 +165,7 @@ def test_c2_force_adjoint_kicks_keys_and_slab():
     vel0 = torch.randn((n, 3), generator=torch.Generator().manual_seed(4)).cuda()
     vel = vel0.clone()
     k1, k2 = 0.37, 0.29
-    acc_k, F = gravity.force(pmid, disp.clone(), conf, om, vel_kick=vel, kick=k1, kick2=k2)
+    acc_k, F = force(pmid, disp.clone(), conf, om, vel_kick=vel, kick=k1, kick2=k2)
     del F
     ref = (vel0 + acc_k * np.float32(k1)) + acc_k * np.float32(k2)
     assert torch.equal(vel, ref)
