@@ -187,6 +187,19 @@ int pmb_green_gradient_adjoint(const void* grad_cot_hat, void* src_cot_hat, int 
                                const float* tables, int has_masks, int green_kernel, const float* transfer,
                                const float* radial, int radial_len, float post_scale, void* stream);
 
+/* Interlaced CIC assignment (replaces the phase-and-average step of
+ * nbody/gravity.py:440-463, _interlacing_phase / _gravity_potential_interlaced).
+ * spec0 / spec1: half spectra (nx, ny, nz/2+1) complex64 of the regular deposit
+ * and of the deposit shifted by half a cell on every axis (pmb_sort_rows_ex
+ * offset cell/2 on x, y and z, then pmb_scatter_rows).
+ * P = exp(-i (kx + ky + kz) cell / 2), k as fftfreq on x and y and rfftfreq on z.
+ *   mode 0: spec0 = (spec0 + P spec1) / 2 (the interlaced source spectrum);
+ *   mode 1: spec1 = conj(P) spec0 / 2, spec0 = spec0 / 2 (its transpose: a source
+ *           cotangent spectrum split into the two deposits' cotangents).
+ * The transpose is exact when the mesh Nyquist planes carry no signal (meshes
+ * finer than the particle grid, whose particle-Nyquist masks zero them). */
+int pmb_interlace_spectra(void* spec0, void* spec1, int nx, int ny, int nz, int mode, void* stream);
+
 /* ---------------- hand-written PM FFT passes -------------------------------
  * For meshes whose sides are powers of two (nx, ny in 64..1024, nz in
  * 128..1024) the fused force and its adjoint run their spectral stages as a

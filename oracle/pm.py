@@ -592,6 +592,25 @@ def window_gain(conf, alpha=0.48, max_gain=4.0, assignment_order=2, windows=2, t
     return gain
 
 
+def pgd_transfer(conf, a, alpha0=0.1, A=0.0, B=0.0, kl=0.1, ks=1.0):
+    """1 - alpha(a) exp(-kl^2/k^2 - k^4/ks^4), 0 band at k = 0 (corrections/pgd.py:154-237)."""
+    kx, ky, kz = [k.astype(np.float64) for k in conf.kvec]
+    k2 = kx[:, None, None]**2 + ky[None, :, None]**2 + kz[None, None, :]**2
+    safe = np.where(k2 > 0, k2, 1.0)
+    band = np.where(k2 > 0, np.exp(-kl**2 / safe - safe**2 / ks**4), 0.0)
+    return 1.0 - alpha0 * 10.0**(A * a**2 - B * a) * band
+
+
+def softening_transfer(conf, strength=0.0, start=0.7, stop=1.0, mode="smoothstep"):
+    """max(1 - strength taper(max_i |k_i| / k_Ny), 0) (corrections/softening.py:49-80)."""
+    kn = np.pi / conf.ptcl_spacing
+    ka = [np.abs(k.astype(np.float64)) / kn for k in conf.kvec]
+    q = np.maximum(np.maximum(ka[0][:, None, None], ka[1][None, :, None]), ka[2][None, None, :])
+    t = np.clip((q - start) / max(stop - start, 1e-6), 0.0, 1.0)
+    taper = t * t * (3.0 - 2.0 * t) if mode == "smoothstep" else t
+    return np.maximum(1.0 - strength * taper, 0.0)
+
+
 def potential_kernel(conf, green_kernel="continuum", transfer=None):
     """Real multiplier from density-hat to potential-hat: G * nyquist * transfer."""
     G = green(conf, green_kernel)
@@ -603,14 +622,31 @@ def potential_kernel(conf, green_kernel="continuum", transfer=None):
     return G
 
 
-def force_meshes(rho, conf, Omega_m, kernel=None, gradient="spectral"):
+def interlacing_phase(conf):
+    """exp(-i (kx + ky + kz) cell / 2) on the half spectrum (gravity.py:440-443)."""
+    kx, ky, kz = [k.astype(np.float64) for k in conf.kvec]
+    ksum = kx[:, None, None] + ky[None, :, None] + kz[None, None, :]
+    return np.exp(-1j * ksum * (conf.cell_size / 2))
+
+
+def interlaced_density(pmid, disp, conf, val=None):
+    """The regular deposit and the one shifted by half a cell on every axis
+    (gravity.py:446-463: scatter(..., offset=cell/2))."""
+    return scatter(pmid, disp, conf, val), scatter(pmid, disp, conf, val, offset=conf.cell_size / 2)
+
+
+def force_meshes(rho, conf, Omega_m, kernel=None, gradient="spectral", rho_shifted=None):
     """Density (M) -> 3 real force meshes, gravity.py:626-633 + 506-543;
-    gradient "fastpm_4point" takes FastPM's derivative (gravity.py:355-391)."""
+    gradient "fastpm_4point" takes FastPM's derivative (gravity.py:355-391).
+    With rho_shifted (the half-cell-shifted deposit) the source spectrum is the
+    interlaced average 0.5 (rfft(S) + rfft(S_shifted) P) (gravity.py:446-463)."""
     kernel = potential_kernel(conf) if kernel is None else kernel
     cs = conf.derivative_factors(gradient)
     om = float(np.float32(Omega_m)) if conf.float_dtype == np.float32 else float(Omega_m)
     S = (rho - 1.0) * (1.5 * om)
     Sh = _fft.rfftn(S)
+    if rho_shifted is not None:
+        Sh = 0.5 * (Sh + _fft.rfftn((rho_shifted - 1.0) * (1.5 * om)) * interlacing_phase(conf))
     pot = Sh * kernel
     out = []
     for d in range(3):
@@ -621,23 +657,35 @@ def force_meshes(rho, conf, Omega_m, kernel=None, gradient="spectral"):
     return np.stack(out)
 
 
-def gravity(pmid, disp, conf, Omega_m, kernel=None, gradient="spectral"):
-    """gravity(), gravity.py:786-814, uncorrected (or fixed real transfer)."""
-    rho = scatter(pmid, disp, conf)
-    F = force_meshes(rho, conf, Omega_m, kernel, gradient)
+def gravity(pmid, disp, conf, Omega_m, kernel=None, gradient="spectral", interlacing=False):
+    """gravity(), gravity.py:786-814, uncorrected (or fixed real transfer);
+    interlacing averages the regular and half-cell-shifted deposits
+    (gravity.py:809-811, 446-463)."""
+    if interlacing:
+        rho, rho1 = interlaced_density(pmid, disp, conf)
+    else:
+        rho, rho1 = scatter(pmid, disp, conf), None
+    F = force_meshes(rho, conf, Omega_m, kernel, gradient, rho1)
     return gather(pmid, disp, conf, F)
 
 
-def gravity_vjp(pmid, disp, conf, Omega_m, acc_cot, kernel=None, val=None, gradient="spectral"):
+def gravity_vjp(pmid, disp, conf, Omega_m, acc_cot, kernel=None, val=None, gradient="spectral", interlacing=False):
     """Transpose of gravity w.r.t. disp and Omega_m.
 
     The map S -> A_d is the real convolution irfft(H_d rfft(S)) with
     H_d = i c_d K(k) Hermitian, so its transpose is irfft(conj(H_d) rfft(.)).
+    With interlacing the shifted source enters through H_d P / 2 and the
+    regular one through H_d / 2 (Hermitian wherever K is non-zero once the
+    mesh Nyquist planes are masked), so their transposes are
+    irfft(conj(P) conj(H_d) rfft(.)) / 2 and irfft(conj(H_d) rfft(.)) / 2.
     Returns (disp_cot, Omega_m_cot)."""
     kernel = potential_kernel(conf) if kernel is None else kernel
     om = float(np.float32(Omega_m)) if conf.float_dtype == np.float32 else float(Omega_m)
-    rho = scatter(pmid, disp, conf, val)
-    F = force_meshes(rho, conf, Omega_m, kernel, gradient)
+    if interlacing:
+        rho, rho1 = interlaced_density(pmid, disp, conf, val)
+    else:
+        rho, rho1 = scatter(pmid, disp, conf, val), None
+    F = force_meshes(rho, conf, Omega_m, kernel, gradient, rho1)
     dc_gather, A_cot = gather_vjp(pmid, disp, conf, F, acc_cot)
     cs = conf.derivative_factors(gradient)
     spec = 0
@@ -646,11 +694,18 @@ def gravity_vjp(pmid, disp, conf, Omega_m, acc_cot, kernel=None, val=None, gradi
         shape = [1, 1, 1]
         shape[d] = -1
         spec = spec + (-1j) * c.reshape(shape) * _fft.rfftn(A_cot[d])
-    S_cot = _fft.irfftn(spec * kernel, s=conf.mesh_shape)
-    rho_cot = S_cot * (1.5 * om)
-    dc_scatter, _ = scatter_vjp(pmid, disp, conf, rho_cot, val)
-    om_cot = 1.5 * float(((rho - 1.0) * S_cot).sum())
-    return dc_gather + dc_scatter, om_cot
+    spec = spec * kernel
+    if rho1 is None:
+        S_cot = _fft.irfftn(spec, s=conf.mesh_shape)
+        dc_scatter, _ = scatter_vjp(pmid, disp, conf, S_cot * (1.5 * om), val)
+        om_cot = 1.5 * float(((rho - 1.0) * S_cot).sum())
+        return dc_gather + dc_scatter, om_cot
+    S_cot = 0.5 * _fft.irfftn(spec, s=conf.mesh_shape)
+    S1_cot = 0.5 * _fft.irfftn(spec * np.conj(interlacing_phase(conf)), s=conf.mesh_shape)
+    dc0, _ = scatter_vjp(pmid, disp, conf, S_cot * (1.5 * om), val)
+    dc1, _ = scatter_vjp(pmid, disp, conf, S1_cot * (1.5 * om), val, offset=conf.cell_size / 2)
+    om_cot = 1.5 * float(((rho - 1.0) * S_cot).sum() + ((rho1 - 1.0) * S1_cot).sum())
+    return dc_gather + dc0 + dc1, om_cot
 
 
 # --------------------------------------------------------------------------
@@ -699,20 +754,20 @@ def stage_schedule(a_prev, a_next, conf):
     return stages
 
 
-def nbody(pmid, disp, vel, conf, cosmo, kernel=None, acc=None):
+def nbody(pmid, disp, vel, conf, cosmo, kernel=None, acc=None, interlacing=False):
     """nbody/solver.py:253-273 forward (init force + scan of integrate)."""
     ft = conf.float_dtype
     a = conf.a_nbody
     K = kernel if callable(kernel) else (lambda _a: kernel)
     disp = disp.astype(ft).copy()
     vel = vel.astype(ft).copy()
-    acc = gravity(pmid, disp, conf, cosmo.Omega_m, K(a[0])).astype(ft)
+    acc = gravity(pmid, disp, conf, cosmo.Omega_m, K(a[0]), interlacing=interlacing).astype(ft)
     for a_prev, a_next in zip(a[:-1], a[1:]):
         for st in stage_schedule(a_prev, a_next, conf):
             if st[0] == "drift":
                 f = ft.type(drift_factor(st[1], st[2], st[3], cosmo, conf))
                 disp = (disp + vel * f).astype(ft)
-                acc = gravity(pmid, disp, conf, cosmo.Omega_m, K(st[3])).astype(ft)
+                acc = gravity(pmid, disp, conf, cosmo.Omega_m, K(st[3]), interlacing=interlacing).astype(ft)
             else:
                 f = ft.type(kick_factor(st[1], st[2], st[3], cosmo, conf))
                 vel = (vel + acc * f).astype(ft)
@@ -732,12 +787,16 @@ def _factor_dOm(fn, args, cosmo, conf, h=1e-4):
     return (vals[0] - vals[1]) / (2 * h)
 
 
-def nbody_adj(pmid, disp, vel, acc, disp_cot, vel_cot, acc_cot, conf, cosmo, kernel=None, om_grads=True):
+def nbody_adj(pmid, disp, vel, acc, disp_cot, vel_cot, acc_cot, conf, cosmo, kernel=None, om_grads=True,
+              interlacing=False, om_terms=None):
     """Reverse sweep, nbody/solver.py:385-444 + integrator.py:541-582, 429-509,
     620-686, 781-837.  States are rebuilt algebraically (disp -= vel*D,
     vel -= acc*K) and the force at the earlier time is recomputed.
 
-    Returns (disp, vel, disp_cot, vel_cot, Omega_m_cot) at the initial time."""
+    Returns (disp, vel, disp_cot, vel_cot, Omega_m_cot) at the initial time;
+    om_terms (a list) receives every term of the Omega_m cotangent's sum (the
+    sum can cancel to far below its terms)."""
+    om_terms = [] if om_terms is None else om_terms
     ft = conf.float_dtype
     a = conf.a_nbody
     disp, vel, acc = disp.astype(ft).copy(), vel.astype(ft).copy(), acc.astype(ft).copy()
@@ -753,23 +812,27 @@ def nbody_adj(pmid, disp, vel, acc, disp_cot, vel_cot, acc_cot, conf, cosmo, ker
                 vel = (vel - acc * f).astype(ft)
                 ac = ac + vc * float(f)
                 if om_grads:
-                    om_cot += _factor_dOm(kick_factor, st[1:], cosmo, conf) * float((vc * acc).sum())
+                    om_terms.append(_factor_dOm(kick_factor, st[1:], cosmo, conf) * float((vc * acc).sum()))
+                    om_cot += om_terms[-1]
                 continue
             _, a_vel, a_dp, a_dn, a_acc_in = st
-            g, oc = gravity_vjp(pmid, disp, conf, cosmo.Omega_m, ac, kernel)
+            g, oc = gravity_vjp(pmid, disp, conf, cosmo.Omega_m, ac, kernel, interlacing=interlacing)
             dc = dc + g
             om_cot += oc
+            om_terms.append(oc)
             ac = np.zeros_like(ac)
             f64 = drift_factor(a_vel, a_dp, a_dn, cosmo, conf)
             f = ft.type(f64)
             disp = (disp - vel * f).astype(ft)
             vc = vc + dc * float(f)
             if om_grads:
-                om_cot += _factor_dOm(drift_factor, (a_vel, a_dp, a_dn), cosmo, conf) * float((dc * vel).sum())
-            acc = gravity(pmid, disp, conf, cosmo.Omega_m, kernel).astype(ft)
-    g, oc = gravity_vjp(pmid, disp, conf, cosmo.Omega_m, ac, kernel)
+                om_terms.append(_factor_dOm(drift_factor, (a_vel, a_dp, a_dn), cosmo, conf) * float((dc * vel).sum()))
+                om_cot += om_terms[-1]
+            acc = gravity(pmid, disp, conf, cosmo.Omega_m, kernel, interlacing=interlacing).astype(ft)
+    g, oc = gravity_vjp(pmid, disp, conf, cosmo.Omega_m, ac, kernel, interlacing=interlacing)
     dc = dc + g
     om_cot += oc
+    om_terms.append(oc)
     return disp, vel, dc, vc, om_cot
 
 

@@ -31,7 +31,8 @@ class PMWindowCompensation:
     """corrections/window.py:23-265 (PMWindowCompensationCorrection): transfer
     gain W(k)^(-order*windows*alpha) capped and tapered, the Green's function
     ("continuum" or "discrete_laplacian") and the force derivative
-    ("spectral" or FastPM's "fastpm_4point")."""
+    ("spectral" or FastPM's "fastpm_4point"); interlacing selects the
+    interlaced force (two deposits, gravity.py:446-463)."""
 
     green_kernel = 1  # discrete Laplacian (window.py:100-108 default)
 
@@ -41,8 +42,6 @@ class PMWindowCompensation:
             raise ValueError(f"Unsupported PM Green's function {green_kernel!r}.")
         if gradient_kernel not in ("spectral", "fastpm_4point"):
             raise ValueError(f"Unsupported force-gradient kernel {gradient_kernel!r}.")
-        if interlacing:
-            raise NotImplementedError("interlaced assignment is not built (the force takes one scatter)")
         self.alpha = alpha
         self.max_gain = max_gain
         self.assignment_order = assignment_order
@@ -51,6 +50,7 @@ class PMWindowCompensation:
         self.taper_stop = taper_stop
         self.green_kernel = 1 if green_kernel == "discrete_laplacian" else 0
         self.gradient_kernel = gradient_kernel
+        self.interlacing = bool(interlacing)
         self._cache = {}
 
     def transfer_tables(self, a, cosmo, conf):
@@ -80,19 +80,144 @@ class PMWindowCompensation:
         return self._cache[key], None
 
 
+class PGDPotentialCorrection:
+    """FastPM-style PGD residual potential as a multiplicative transfer
+    (corrections/pgd.py:14-35, 154-237): T(k, a) = 1 - alpha(a) band(k) with
+    alpha(a) = alpha0 10^(A a^2 - B a) and band = exp(-kl^2/k^2 - k^4/ks^4)
+    (0 at k = 0), evaluated in float32 per scale factor."""
+
+    green_kernel = 0
+    gradient_kernel = "spectral"
+
+    def __init__(self, alpha0=0.1, A=0.0, B=0.0, kl=0.1, ks=1.0):
+        self.alpha0, self.A, self.B, self.kl, self.ks = alpha0, A, B, kl, ks
+        self._cache = {}
+
+    def alpha(self, a):
+        f = np.float32
+        return f(self.alpha0) * (f(10.0)**(f(self.A) * f(a)**2 - f(self.B) * f(a)))
+
+    def transfer_tables(self, a, cosmo, conf):
+        a = 1.0 if a is None else float(a)
+        key = (a, conf.mesh_shape, conf.cell_size, str(conf.device))
+        if key not in self._cache:
+            if len(self._cache) > 64:
+                self._cache.clear()
+            dev = conf.device
+            kx, ky, kz = [torch.from_numpy(k.astype(np.float32)).to(dev) for k in conf.kvec]
+            k2 = (kx[:, None, None]**2 + ky[None, :, None]**2) + kz[None, None, :]**2
+            safe = torch.where(k2 > 0, k2, torch.ones_like(k2))
+            band = torch.exp(-np.float32(self.kl)**2 / safe - safe**2 / np.float32(self.ks)**4)
+            band = torch.where(k2 > 0, band, torch.zeros_like(band))
+            self._cache[key] = (1.0 - float(self.alpha(a)) * band).to(torch.float32).contiguous()
+        return self._cache[key], None
+
+
+class HighKSofteningCorrection:
+    """High-k spectral softening (corrections/softening.py:12-80): T = max(1 -
+    strength taper(q), 0) with q = max_i |k_i| / k_Ny(particles) and taper the
+    smoothstep (or linear) ramp from start to stop."""
+
+    green_kernel = 0
+    gradient_kernel = "spectral"
+
+    def __init__(self, strength=0.0, start=0.7, stop=1.0, mode="smoothstep"):
+        if mode not in ("smoothstep", "linear"):
+            raise ValueError(f"Unsupported high-k softening mode {mode!r}.")
+        self.strength, self.start, self.stop, self.mode = strength, start, stop, mode
+        self._cache = {}
+
+    def transfer_tables(self, a, cosmo, conf):
+        key = (conf.mesh_shape, conf.cell_size, conf.ptcl_spacing, str(conf.device))
+        if key not in self._cache:
+            dev = conf.device
+            kx, ky, kz = [torch.from_numpy(k.astype(np.float32)).to(dev).abs() for k in conf.kvec]
+            kn = np.float32(np.pi / conf.ptcl_spacing)
+            q = torch.maximum(torch.maximum(kx[:, None, None] / kn, ky[None, :, None] / kn), kz[None, None, :] / kn)
+            t = torch.clamp((q - np.float32(self.start)) / max(np.float32(self.stop - self.start), np.float32(1e-6)),
+                            0.0, 1.0)
+            taper = t * t * (3.0 - 2.0 * t) if self.mode == "smoothstep" else t
+            self._cache[key] = torch.clamp(1.0 - np.float32(self.strength) * taper, min=0.0).to(torch.float32)
+        return self._cache[key], None
+
+
+class CombinedPotentialCorrection:
+    """Several corrections at once (corrections/core.py:286-334, combined.py):
+    the product of their transfers, the first non-continuum Green's function and
+    the one non-spectral force derivative they ask for."""
+
+    def __init__(self, window=None, pgd=None, softening=None, radial=None):
+        self.parts = [c for c in (window, pgd, softening, radial) if c is not None]
+        self.green_kernel = next((c.green_kernel for c in self.parts if getattr(c, "green_kernel", 0) != 0), 0)
+        grads = {getattr(c, "gradient_kernel", "spectral") for c in self.parts} - {"spectral"}
+        if len(grads) > 1:
+            raise ValueError(f"Combined correction requests incompatible force-gradient kernels: {sorted(grads)!r}.")
+        self.gradient_kernel = next(iter(grads), "spectral")
+
+    def transfer_tables(self, a, cosmo, conf):
+        T, R = None, None
+        for c in self.parts:
+            t, r = c.transfer_tables(a, cosmo, conf)
+            if t is not None:
+                T = t if T is None else T * t
+            if r is not None:
+                if R is not None:
+                    raise ValueError("at most one radial table per combined correction")
+                R = r
+        return (None if T is None else T.contiguous()), R
+
+
+def _window_from(kw):
+    """init_pm_window_compensation_correction's keywords and aliases (corrections/window.py:159-177)."""
+    return PMWindowCompensation(
+        alpha=kw.get("alpha", kw.get("window_alpha", 0.48)), max_gain=kw.get("max_gain", kw.get("window_max_gain", 4.0)),
+        assignment_order=kw.get("assignment_order", 2), windows=kw.get("windows", 2),
+        taper_start=kw.get("taper_start", kw.get("window_taper_start", 0.75)),
+        taper_stop=kw.get("taper_stop", kw.get("window_taper_stop", 1.0)), interlacing=kw.get("interlacing", False),
+        green_kernel=kw.get("green_kernel", "discrete_laplacian"),
+        gradient_kernel=kw.get("gradient_kernel", kw.get("window_gradient_kernel", "spectral")))
+
+
+def _pgd_from(kw):
+    """init_pgd_potential_correction's keywords and aliases (corrections/pgd.py:88-104)."""
+    return PGDPotentialCorrection(alpha0=kw.get("alpha0", kw.get("pgd_alpha0", 0.1)), A=kw.get("A", kw.get("pgd_A", 0.0)),
+                                  B=kw.get("B", kw.get("pgd_B", 0.0)), kl=kw.get("kl", kw.get("pgd_kl", 0.1)),
+                                  ks=kw.get("ks", kw.get("pgd_ks", 1.0)))
+
+
+def _softening_from(kw):
+    """init_high_k_softening_correction's keywords and aliases (corrections/softening.py:32-46)."""
+    return HighKSofteningCorrection(strength=kw.get("strength", kw.get("softening_strength", 0.0)),
+                                    start=kw.get("start", kw.get("softening_start", 0.7)),
+                                    stop=kw.get("stop", kw.get("softening_stop", 1.0)),
+                                    mode=kw.get("mode", kw.get("softening_mode", "smoothstep")))
+
+
 def init_potential_correction(model, **kwargs):
     """The analytic models of init_potential_correction (corrections/core.py:40-151):
     "pm_window" / "cic_compensation" / "cic_window_compensation" (the window
     compensation), "fastpm_1_4" (continuum Green's function) and "fastpm_3_4"
     (discrete Laplacian), both with FastPM's 4-point gradient and no window
-    gain."""
+    gain, "pgd" / "fastpm_pgd", "high_k_softening" / "softening" /
+    "fastpm_softening", and the window combined with either ("windowed_pgd",
+    "pm_window+pgd", "pgd_window", "windowed_softening", "pm_window+softening").
+    The trainable and neural variants other than LearnedGreen are not built."""
+    kw = dict(kwargs)
+    kw.pop("dtype", None)
     if model in ("pm_window", "cic_compensation", "cic_window_compensation"):
-        return PMWindowCompensation(**kwargs)
+        return _window_from(kw)
     if model in ("fastpm_1_4", "fastpm_3_4"):
-        kw = dict(kwargs)
-        kw.update(alpha=0.0, green_kernel="continuum" if model == "fastpm_1_4" else "discrete_laplacian",
-                  gradient_kernel="fastpm_4point")
-        return PMWindowCompensation(**kw)
+        kw.update(window_alpha=0.0, alpha=0.0, gradient_kernel="fastpm_4point",
+                  green_kernel="continuum" if model == "fastpm_1_4" else "discrete_laplacian")
+        return _window_from(kw)
+    if model in ("pgd", "fastpm_pgd"):
+        return _pgd_from(kw)
+    if model in ("high_k_softening", "softening", "fastpm_softening"):
+        return _softening_from(kw)
+    if model in ("windowed_pgd", "pm_window+pgd", "pgd_window"):
+        return CombinedPotentialCorrection(window=_window_from(kw), pgd=_pgd_from(kw))
+    if model in ("windowed_softening", "pm_window+softening"):
+        return CombinedPotentialCorrection(window=_window_from(kw), softening=_softening_from(kw))
     raise ValueError(f"Unsupported correction model {model!r}.")
 
 

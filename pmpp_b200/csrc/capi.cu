@@ -337,6 +337,14 @@ int pmb_green_gradient_adjoint(const void* grad_cot_hat, void* src_cot_hat, int 
                                 make_green(green_kernel, transfer, radial, radial_len, post_scale), S(stream));
 }
 
+int pmb_interlace_spectra(void* spec0, void* spec1, int nx, int ny, int nz, int mode, void* stream) {
+  Mesh3 m{nx, ny, nz};
+  PMB_REQUIRE(nx > 0 && ny > 0 && nz > 0, "pmb_interlace_spectra: bad shape");
+  PMB_REQUIRE(mode == 0 || mode == 1, "pmb_interlace_spectra: mode must be 0 (combine) or 1 (transpose)");
+  PMB_REQUIRE(spec0 != nullptr && spec1 != nullptr && spec0 != spec1, "pmb_interlace_spectra: two distinct spectra");
+  return interlace((float2*)spec0, (float2*)spec1, m, mode, S(stream));
+}
+
 // ---------------------------------------------------------------------------
 // Fused force
 // ---------------------------------------------------------------------------

@@ -341,6 +341,43 @@ int green_gradient_adjoint(const float2* grad_cot_hat, float2* src_cot_hat, Mesh
   return kOk;
 }
 
+// Interlaced assignment (nbody/gravity.py:440-463).  The deposit shifted by
+// half a cell on every axis has the spectrum of the regular one times
+// exp(+i (kx + ky + kz) h / 2); P = exp(-i (kx + ky + kz) h / 2) moves it
+// back.  With k_d h / 2 = pi s_d / n_d over the signed frequency s_d (x and y
+// as fftfreq, the Nyquist index negative; z >= 0 as rfftfreq) the phase is
+// exp(-i pi t), t = sx / nx + sy / ny + sz / nz, taken with sincospif.
+//   mode 0 (forward):   s0 = (s0 + P s1) / 2
+//   mode 1 (transpose): s1 = conj(P) s0 / 2, then s0 = s0 / 2
+__global__ void interlace_kernel(float2* __restrict__ s0, float2* __restrict__ s1, Mesh3 m, int mode) {
+  const int64_t nzh = m.nz / 2 + 1, ny = m.ny;
+  const int64_t total = m.half_cells();
+  const float inx = 1.0f / (float)m.nx, iny = 1.0f / (float)m.ny, inz = 1.0f / (float)m.nz;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = j / nzh, ix = r / ny;
+    const int iy = (int)(r - ix * ny), iz = (int)(j - r * nzh);
+    const int sx = (2 * ix >= m.nx) ? (int)ix - m.nx : (int)ix;
+    const int sy = (2 * iy >= m.ny) ? iy - m.ny : iy;
+    const float t = (float)sx * inx + (float)sy * iny + (float)iz * inz;
+    float sn, cs;
+    sincospif(t, &sn, &cs);  // P = cs - i sn
+    const float2 a = s0[j];
+    if (mode == 0) {
+      const float2 b = s1[j];
+      s0[j] = make_float2(0.5f * (a.x + (cs * b.x + sn * b.y)), 0.5f * (a.y + (cs * b.y - sn * b.x)));
+    } else {
+      s1[j] = make_float2(0.5f * (cs * a.x - sn * a.y), 0.5f * (cs * a.y + sn * a.x));
+      s0[j] = make_float2(0.5f * a.x, 0.5f * a.y);
+    }
+  }
+}
+
+int interlace(float2* s0, float2* s1, Mesh3 m, int mode, cudaStream_t s) {
+  interlace_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(s0, s1, m, mode);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
 // x = x * a + b, elementwise in float.
 __global__ void scale_real_kernel(float* __restrict__ x, int64_t n, float a, float b) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)

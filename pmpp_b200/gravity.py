@@ -7,9 +7,11 @@ straight into the Poisson source, R2C, fused Green x gradient, one batched
 C2R for the three force meshes, and a three-channel gather.
 
 ``correction`` accepts None or an object with ``green_kernel`` (0 continuum,
-1 discrete Laplacian) and ``transfer_tables(a, cosmo, conf)`` returning
+1 discrete Laplacian), ``gradient_kernel`` ("spectral" or "fastpm_4point"),
+optionally ``interlacing`` and ``transfer_tables(a, cosmo, conf)`` returning
 (transfer half-spectrum tensor or None, radial |n|^2 table or None); see
-pmpp_b200/corrections.py.
+pmpp_b200/corrections.py.  An interlaced correction takes its own staged
+route (two deposits, cuFFT, pmb_interlace_spectra).
 """
 from __future__ import annotations
 
@@ -55,6 +57,129 @@ def _cufft_buffers(conf, dev):
     fw = max(L.pmb_fft_work_bytes(nx, ny, nz, 3), L.pmb_fft_work_bytes(nx, ny, nz, 1))
     work = workspace(fw, dev, "st_fftwork")
     return spec3, spec1, work
+
+
+def uses_interlacing(correction):
+    """force_uses_interlacing (corrections/core.py:381-393): a correction, or
+    any part of a combined one, asking for interlaced assignment."""
+    if correction is None:
+        return False
+    parts = getattr(correction, "parts", None)
+    if parts is not None:
+        return any(uses_interlacing(c) for c in parts)
+    return bool(getattr(correction, "interlacing", False))
+
+
+def _interlace_buffers(n, conf, dev, sorted_lane="", work_lane=""):
+    """Sorted records at the half-cell-shifted origin, two half spectra, three
+    half spectra and the cuFFT work area of the interlaced route."""
+    L = lib()
+    nx, ny, nz = conf.mesh_shape
+    Mc = nx * ny * (nz // 2 + 1)
+    sorted_sh = workspace(L.pmb_sorted_bytes(n, nx, ny, nz), dev, "st_sorted_sh" + _lane_suffix(sorted_lane))
+    spec2 = workspace(16 * Mc, dev, "il_spec2" + work_lane)
+    spec3 = workspace(24 * Mc, dev, "il_spec3" + work_lane)
+    fw = max(L.pmb_fft_work_bytes(nx, ny, nz, b) for b in (1, 2, 3))
+    work = workspace(fw, dev, "il_fftwork" + work_lane)
+    return sorted_sh, spec2, spec3, work
+
+
+def _sort_both(pmid, disp, conf, drift_vel, drift, sorted_buf, sorted_sh, sort_scr, s):
+    """Cell-sorted records at the mesh origin and at (cell/2, cell/2, cell/2)
+    (gravity.py:455-457: scatter(..., offset=cell/2)); the drift, when given,
+    is applied by the first sort."""
+    n = pmid.shape[0]
+    nx, ny, nz = conf.mesh_shape
+    h = float(conf.cell_size) / 2
+    call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
+         float(conf.cell_size), sorted_buf.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
+    call("pmb_sort_rows_ex", pmid.data_ptr(), disp.data_ptr(), None, 0.0, n, nx, ny, nz, float(conf.cell_size), h, h,
+         h, None, sorted_sh.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
+
+
+def _force_interlaced(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc, drift_vel, drift, vel_kick,
+                      kick, kick2, timer, src_hat_out=None, lane=""):
+    """Interlaced force (gravity.py:446-463, 809-811): the regular and the
+    half-cell-shifted deposits, one batched R2C of both, the phase-shifted
+    average (pmb_interlace_spectra), then Green x gradient, three C2R and the
+    three-channel gather at the regular origin."""
+    n = pmid.shape[0]
+    nx, ny, nz = conf.mesh_shape
+    dev = disp.device
+    s = stream_handle(dev)
+    M = conf.mesh_size
+    Mc = nx * ny * (nz // 2 + 1)
+    sorted_buf, sort_scr, s16, real3 = _stage_buffers(n, conf, dev, sorted_lane=lane)
+    sorted_sh, spec2, spec3, work = _interlace_buffers(n, conf, dev, sorted_lane=lane)
+    timer = _NoTimer() if timer is None else timer
+    t = timer.start()
+    _sort_both(pmid, disp, conf, drift_vel, drift, sorted_buf, sorted_sh, sort_scr, s)
+    t = timer.mark("sort", t)
+    vc = float(conf.mesh_size / conf.ptcl_num)
+    for k, sb in enumerate((sorted_buf, sorted_sh)):
+        call("pmb_scatter_rows", sb.data_ptr(), n, nx, ny, nz, 1, None, 0, vc, 1, 1.5 * _om32(omega_m),
+             real3.data_ptr() + 4 * M * k, s16.data_ptr(), s)
+    t = timer.mark("scatter", t)
+    call("pmb_rfft3", nx, ny, nz, 2, real3.data_ptr(), spec2.data_ptr(), work.data_ptr(), s)
+    t = timer.mark("fft_r2c", t)
+    call("pmb_interlace_spectra", spec2.data_ptr(), spec2.data_ptr() + 8 * Mc, nx, ny, nz, 0, s)
+    if src_hat_out is not None:
+        src_hat_out.view(torch.uint8).view(-1)[:8 * Mc].copy_(spec2[:8 * Mc])
+    call("pmb_green_gradient", spec2.data_ptr(), spec3.data_ptr(), nx, ny, nz, tables.data_ptr(),
+         int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, float(1.0 / M), s)
+    t = timer.mark("green_gradient", t)
+    call("pmb_irfft3", nx, ny, nz, 3, spec3.data_ptr(), F.data_ptr(), work.data_ptr(), s)
+    t = timer.mark("fft_c2r", t)
+    call("pmb_gather_rows2", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc.data_ptr(), ptr(vel_kick),
+         float(kick), float(kick2), s)
+    timer.mark("gather", t)
+
+
+def _force_vjp_interlaced(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc_cot, disp_cot, timer,
+                          src_hat=None, transfer_cot_out=None, presorted=False, sorted_lane="", work_lane=""):
+    """Transpose of the interlaced force: the gather adjoint, the acceleration
+    cotangents deposited, R2C, the adjoint multiplier, the transposed phase
+    split (pmb_interlace_spectra mode 1) into the two deposits' cotangent
+    spectra, one batched C2R and the deposit adjoints at both origins."""
+    n = pmid.shape[0]
+    nx, ny, nz = conf.mesh_shape
+    dev = disp.device
+    s = stream_handle(dev)
+    M = conf.mesh_size
+    Mc = nx * ny * (nz // 2 + 1)
+    slane = sorted_lane if presorted else work_lane
+    sorted_buf, sort_scr, s16, real3 = _stage_buffers(n, conf, dev, slane, work_lane)
+    sorted_sh, spec2, spec3, work = _interlace_buffers(n, conf, dev, slane, work_lane)
+    timer = _NoTimer() if timer is None else timer
+    t = timer.start()
+    if not presorted:
+        _sort_both(pmid, disp, conf, None, 0.0, sorted_buf, sorted_sh, sort_scr, s)
+        t = timer.mark("sort", t)
+    cot_sorted = workspace(12 * n, dev, "st_cot_sorted" + work_lane)
+    call("pmb_interp_grad_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc_cot.data_ptr(), 0.0,
+         float(conf.cell_size), 1, disp_cot.data_ptr(), None, cot_sorted.data_ptr(), s)
+    t = timer.mark("gather_adjoint", t)
+    call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, cot_sorted.data_ptr(), 1, 0.0, 0, 1.0,
+         real3.data_ptr(), s16.data_ptr(), s)
+    t = timer.mark("scatter3", t)
+    masks = int(conf.has_particle_nyquist_masks)
+    call("pmb_rfft3", nx, ny, nz, 3, real3.data_ptr(), spec3.data_ptr(), work.data_ptr(), s)
+    t = timer.mark("fft_r2c", t)
+    if transfer_cot_out is not None:
+        call("pmb_transfer_cot", spec3.data_ptr(), src_hat.data_ptr(), nx, ny, nz, tables.data_ptr(), masks,
+             int(transfer_cot_out.numel()), transfer_cot_out.data_ptr(), s)
+    post = float(np.float32(1.5 * _om32(omega_m)) / M)
+    call("pmb_green_gradient_adjoint", spec3.data_ptr(), spec2.data_ptr(), nx, ny, nz, tables.data_ptr(), masks, gk,
+         ptr(transfer), ptr(radial), rl, post, s)
+    call("pmb_interlace_spectra", spec2.data_ptr(), spec2.data_ptr() + 8 * Mc, nx, ny, nz, 1, s)
+    t = timer.mark("green_gradient", t)
+    call("pmb_irfft3", nx, ny, nz, 2, spec2.data_ptr(), real3.data_ptr(), work.data_ptr(), s)
+    t = timer.mark("fft_c2r", t)
+    vc = float(conf.mesh_size / conf.ptcl_num)
+    for k, sb in enumerate((sorted_buf, sorted_sh)):
+        call("pmb_interp_grad_rows", sb.data_ptr(), n, nx, ny, nz, 1, real3.data_ptr() + 4 * M * k, None, vc,
+             float(conf.cell_size), 1, disp_cot.data_ptr(), None, None, s)
+    timer.mark("scatter_adjoint", t)
 
 
 class _NoTimer:
@@ -225,6 +350,10 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
         acc = torch.empty((n, 3), dtype=torch.float32, device=dev)
     gk, transfer, radial, rl = _correction_args(correction, a, cosmo, conf)
     tables = _tables(conf, dev, gk, correction)
+    if uses_interlacing(correction):
+        _force_interlaced(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc, drift_vel,
+                          drift, vel_kick, kick, kick2, StageTimer.active, src_hat_out, lane)
+        return acc, force_meshes
     if StageTimer.active is not None or src_hat_out is not None:
         _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc, drift_vel,
                       drift, vel_kick, kick, StageTimer.active, src_hat_out, lane, kick2)
@@ -258,6 +387,11 @@ def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *
         disp_cot = torch.zeros((n, 3), dtype=torch.float32, device=dev)
     gk, transfer, radial, rl = _correction_args(correction, a, cosmo, conf)
     tables = _tables(conf, dev, gk, correction)
+    if uses_interlacing(correction):
+        _force_vjp_interlaced(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc_cot,
+                              disp_cot, StageTimer.active, src_hat, transfer_cot_out, presorted, sorted_lane,
+                              "v" if concurrent else "")
+        return disp_cot
     if StageTimer.active is not None or transfer_cot_out is not None:
         _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc_cot,
                           disp_cot, StageTimer.active, src_hat, transfer_cot_out, presorted, sorted_lane,

@@ -16,6 +16,7 @@ closed-form / invariant assertions of the reference test suite, restated:
                                                 not alias the particle lattice
 """
 import numpy as np
+import pytest
 
 from oracle import cosmology as ocos
 from oracle import pm as opm
@@ -153,6 +154,31 @@ def test_oracle_adjoints_vs_finite_differences():
     dc, om = opm.gravity_vjp(pmid, disp, conf, 0.3, ac)
     fd = _fd4(lambda d: (opm.gravity(pmid, d, conf, 0.3) * ac).sum(), disp, v)
     np.testing.assert_allclose((dc * v).sum(), fd, rtol=1e-7, atol=1e-9)
+
+
+@pytest.mark.parametrize("mesh", [2, 3])
+def test_oracle_interlaced_gravity_adjoint_vs_finite_differences(mesh):
+    """The interlaced force (gravity.py:446-463) and its transpose, with the
+    window and PGD transfers on, against 4th-order differences in float64;
+    the interlaced force of a uniform lattice is zero too."""
+    conf = opm.Conf(4.0, (6, 6, 6), mesh_shape=mesh, float_dtype=np.float64)
+    rng = np.random.default_rng(1)
+    pmid, disp = opm.gen_grid(conf)
+    kern = opm.potential_kernel(conf, "discrete_laplacian", opm.window_gain(conf) * opm.pgd_transfer(conf, 0.5))
+    assert np.abs(opm.gravity(pmid, disp, conf, 0.3, kern, interlacing=True)).max() < 1e-12
+    disp = disp + rng.normal(0, 2.0, size=disp.shape)
+    v = rng.normal(size=disp.shape)
+    v /= np.linalg.norm(v)
+    ac = rng.normal(size=disp.shape)
+    dc, om = opm.gravity_vjp(pmid, disp, conf, 0.3, ac, kern, interlacing=True)
+    fd = _fd4(lambda d: (opm.gravity(pmid, d, conf, 0.3, kern, interlacing=True) * ac).sum(), disp, v)
+    np.testing.assert_allclose((dc * v).sum(), fd, rtol=1e-7, atol=1e-9)
+    fdo = _fd4(lambda o: (opm.gravity(pmid, disp, conf, 0.3 + o[0], kern, interlacing=True) * ac).sum(),
+               np.zeros(1), np.ones(1))
+    np.testing.assert_allclose(om, fdo, rtol=1e-7)
+    # interlacing changes the force (it is not the regular one)
+    reg = opm.gravity(pmid, disp, conf, 0.3, kern)
+    assert np.abs(opm.gravity(pmid, disp, conf, 0.3, kern, interlacing=True) - reg).max() > 1e-3 * np.abs(reg).max()
 
 
 def test_oracle_nbody_adjoint_vs_finite_differences():
