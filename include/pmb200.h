@@ -200,6 +200,16 @@ int pmb_green_gradient_adjoint(const void* grad_cot_hat, void* src_cot_hat, int 
  * finer than the particle grid, whose particle-Nyquist masks zero them). */
 int pmb_interlace_spectra(void* spec0, void* spec1, int nx, int ny, int nz, int mode, void* stream);
 
+/* Windowed periodic projection of a C-order (nx, ny, nz) float mesh along one
+ * axis (replaces the sum of nbody/observers.py:50-54 density_projection_observer
+ * and the wraparound_slice sums of observers.py:113-124, core/utils.py:420-463).
+ * out (the other two axes, C order) = sum over t < count of the planes
+ * (start + t) mod n_axis, count = min(stop - start, max_width) (max_width < 0:
+ * no cap; 0 when stop <= start).  Full projection: start 0, stop n_axis.
+ * FP64 sums in a fixed order: deterministic. */
+int pmb_project_density(const float* mesh, int nx, int ny, int nz, int axis, int start, int stop, int max_width,
+                        float* out, void* stream);
+
 /* ---------------- hand-written PM FFT passes -------------------------------
  * For meshes whose sides are powers of two (nx, ny in 64..1024, nz in
  * 128..1024) the fused force and its adjoint run their spectral stages as a

@@ -16,13 +16,19 @@ from . import cic
 from .cic import scatter, gather, scatter_vjp, gather_vjp
 from .gravity import gravity, gravity_vjp, gravity_streamed
 from .nbody import (nbody, nbody_adj, integrate, kick, drift, NBodyRun, kick_adj, drift_adj_from_output,
-                    force_adj, integrate_adj, nbody_low_memory)
+                    force_adj, integrate_adj, nbody_low_memory, nbody_scheduled, nbody_static_halo_scheduled,
+                    nbody_init, nbody_step, nbody_collect, nbody_observe)
+from . import observers, checkpoint
+from .observers import density_projection_observer, nbody_kappa
+from .checkpoint import save_state, load_state
 
 __all__ = [
     "Configuration", "Cosmology", "SimpleLCDM", "boltzmann", "growth", "linear_power", "Particles", "pmid_to_idx", "cic", "scatter",
     "gather", "scatter_vjp", "gather_vjp", "gravity", "gravity_vjp", "nbody", "nbody_adj", "integrate", "kick",
     "drift", "NBodyRun", "kick_adj", "drift_adj_from_output", "force_adj", "integrate_adj", "gravity_streamed",
-    "nbody_low_memory"
+    "nbody_low_memory", "nbody_scheduled", "nbody_static_halo_scheduled", "nbody_init", "nbody_step",
+    "nbody_collect", "nbody_observe", "observers", "checkpoint", "density_projection_observer", "nbody_kappa",
+    "save_state", "load_state"
 ]
 from . import modes, lpt, power_spectrum, pipeline  # noqa: E402
 from .modes import white_noise_nested, linear_modes  # noqa: E402

@@ -53,6 +53,7 @@ _SIGS = {
     "pmb_irfft3": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
     "pmb_green_gradient": (c_int, [c_p, c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p, c_int, c_f, c_p]),
     "pmb_interlace_spectra": (c_int, [c_p, c_p, c_int, c_int, c_int, c_int, c_p]),
+    "pmb_project_density": (c_int, [c_p, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_p, c_p]),
     "pmb_green_gradient_adjoint": (c_int, [c_p, c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p, c_int, c_f,
                                            c_p]),
     "pmb_force_workspace_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
@@ -165,7 +166,8 @@ def check(status, what):
 _KERNELS = {
     "pmb_sort_rows": 5, "pmb_sort_rows_ex": 5, "pmb_cic_general_scatter": 3, "pmb_cic_general_gather": 1,
     "pmb_cic_general_interp_grad": 1, "pmb_gather_rows": 1, "pmb_gather_rows2": 1, "pmb_interp_grad_rows": 1,
-    "pmb_green_gradient": 1, "pmb_interlace_spectra": 1, "pmb_green_gradient_adjoint": 1, "pmb_axpy": 1,
+    "pmb_green_gradient": 1, "pmb_interlace_spectra": 1, "pmb_project_density": 1,
+    "pmb_green_gradient_adjoint": 1, "pmb_axpy": 1,
     "pmb_kick_adj": 1, "pmb_kick_adj2": 1, "pmb_drift_cot_adj": 1, "pmb_drift_adj": 1, "pmb_dot": 1,
     "pmb_force": 9, "pmb_force2": 9, "pmb_force_streamed": 14, "pmb_force_vjp": 11, "pmb_force_vjp_presorted": 6, "pmb_sum": 1,
     "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,

@@ -46,7 +46,8 @@ class Configuration:
                  symp_splits=((0, 0.5), (1, 0.5)), lpt_order=2, growth_rtol=None, growth_atol=None,
                  growth_inistep=(1, None), transfer_fit=True, transfer_fit_nowiggle=False, transfer_lgk_min=-4,
                  transfer_lgk_max=3, transfer_lgk_maxstep=1 / 128, T_cmb=2.7255, k_pivot_Mpc=0.05,
-                 float_dtype="float32", device=None):
+                 float_dtype="float32", device=None, to_save_z=None, to_save_a=None, slice_to_save=None,
+                 max_slice_width=None):
         self.ptcl_spacing = float(ptcl_spacing)
         self.ptcl_grid_shape = tuple(int(s) for s in ptcl_grid_shape)
         if isinstance(mesh_shape, (int, float)):
@@ -95,6 +96,13 @@ class Configuration:
         self.T_cmb = T_cmb
         self.k_pivot_Mpc = k_pivot_Mpc
         self.device = torch.device(device if device is not None else ("cuda" if torch.cuda.is_available() else "cpu"))
+        # saved-map controls of the forward observers (configuration.py:235-238, 311-318)
+        self.to_save_z = None if to_save_z is None else list(to_save_z)
+        if to_save_a is None and to_save_z is not None:
+            to_save_a = [1 / (1 + z) for z in to_save_z]
+        self.to_save_a = None if to_save_a is None else list(to_save_a)
+        self.slice_to_save = None if slice_to_save is None else [int(i) for i in slice_to_save]
+        self.max_slice_width = None if max_slice_width is None else int(max_slice_width)
         # cached spectral operators (configuration.py:301-307, 365-376)
         self.kvec = _fftfreq(self.mesh_shape, self.cell_size, self.np_dtype)
         self.kvec_spacing = _fftfreq(self.ptcl_grid_shape, self.ptcl_spacing, self.np_dtype)
@@ -112,6 +120,10 @@ class Configuration:
     @property
     def dim(self):
         return 3
+
+    @property
+    def nMesh(self):
+        return self.mesh_shape[0]
 
     @property
     def ptcl_num(self):

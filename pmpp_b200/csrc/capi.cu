@@ -345,6 +345,14 @@ int pmb_interlace_spectra(void* spec0, void* spec1, int nx, int ny, int nz, int 
   return interlace((float2*)spec0, (float2*)spec1, m, mode, S(stream));
 }
 
+int pmb_project_density(const float* mesh, int nx, int ny, int nz, int axis, int start, int stop, int max_width,
+                        float* out, void* stream) {
+  PMB_REQUIRE(nx > 0 && ny > 0 && nz > 0, "pmb_project_density: bad shape");
+  PMB_REQUIRE(axis >= 0 && axis <= 2, "pmb_project_density: axis must be 0, 1 or 2");
+  PMB_REQUIRE(mesh != nullptr && out != nullptr, "pmb_project_density: null buffer");
+  return project_window(mesh, Mesh3{nx, ny, nz}, axis, start, stop, max_width, out, S(stream));
+}
+
 // ---------------------------------------------------------------------------
 // Fused force
 // ---------------------------------------------------------------------------

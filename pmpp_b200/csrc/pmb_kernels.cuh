@@ -82,6 +82,10 @@ int green_gradient_component(const float2* src_hat, float2* out, Mesh3 m, SpecTa
                              cudaStream_t s);
 // interlaced-assignment phase: mode 0 s0 = (s0 + P s1) / 2, mode 1 its transpose
 int interlace(float2* s0, float2* s1, Mesh3 m, int mode, cudaStream_t s);
+
+// observe.cu: windowed periodic projection of a mesh along one axis
+int project_window(const float* mesh, Mesh3 m, int axis, int start, int stop, int max_width, float* out,
+                   cudaStream_t s);
 // acc (n,3) from three planar (3,n) channels
 int interleave3(const float* planar, float* acc, int64_t n, cudaStream_t s);
 

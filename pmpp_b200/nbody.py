@@ -418,6 +418,70 @@ def nbody(ptcl, cosmo, conf, reverse=False, correction=None):
     return NBodyRun(conf, cosmo, correction).forward(ptcl, a)
 
 
+def nbody_scheduled(ptcl, cosmo, confs, reverse=False, correction=None):
+    """Run through several configuration segments in turn, each with its own
+    schedule, passing the particles on (nbody_static_halo_scheduled,
+    nbody/solver.py:645-679); reverse runs the segments, and each schedule,
+    backwards."""
+    for c in (confs[::-1] if reverse else confs):
+        ptcl = nbody(ptcl, cosmo, c, reverse=reverse, correction=correction)
+    return ptcl
+
+
+nbody_static_halo_scheduled = nbody_scheduled
+
+
+def nbody_init(a, ptcl, cosmo, conf, correction=None):
+    """The starting acceleration (nbody/solver.py:21-43)."""
+    return force_state(a, ptcl, cosmo, conf, correction)
+
+
+def nbody_step(a_prev, a_next, ptcl, cosmo, conf, correction=None):
+    """One macro step (nbody/solver.py:46-65)."""
+    return integrate(a_prev, a_next, ptcl, cosmo, conf, correction)
+
+
+def nbody_collect(ptcl, cosmo, conf, collector, collector_state, reverse=False, return_final=False,
+                  correction=None):
+    """Forward run updating caller state after every macro step
+    (nbody/solver.py:116-167): state = collector(state, a_prev, a_next, ptcl,
+    cosmo, conf).  Forward only; returns the state, or (final particles,
+    state) with return_final."""
+    a = conf.a_nbody[::-1] if reverse else conf.a_nbody
+    ptcl = nbody_init(float(a[0]), ptcl, cosmo, conf, correction)
+    state = collector_state
+    for a_prev, a_next in zip(a[:-1], a[1:]):
+        ptcl = nbody_step(float(a_prev), float(a_next), ptcl, cosmo, conf, correction)
+        state = collector(state, float(a_prev), float(a_next), ptcl, cosmo, conf)
+    return (ptcl, state) if return_final else state
+
+
+def _stack_tree(obs):
+    """Stack a list of observation trees (tensors, numbers, dicts, tuples) along a new leading axis."""
+    first = obs[0]
+    if isinstance(first, dict):
+        return {k: _stack_tree([o[k] for o in obs]) for k in first}
+    if isinstance(first, (tuple, list)):
+        return type(first)(_stack_tree([o[i] for o in obs]) for i in range(len(first)))
+    if torch.is_tensor(first):
+        return torch.stack(obs)
+    return torch.as_tensor(np.asarray(obs))
+
+
+def nbody_observe(ptcl, cosmo, conf, observer, reverse=False, include_start=False, return_final=False,
+                  correction=None):
+    """Forward run stacking observer(a, ptcl, cosmo, conf) after every macro
+    step, and at the start with include_start (nbody/solver.py:170-227)."""
+    a = conf.a_nbody[::-1] if reverse else conf.a_nbody
+    ptcl = nbody_init(float(a[0]), ptcl, cosmo, conf, correction)
+    obs = [observer(float(a[0]), ptcl, cosmo, conf)] if include_start else []
+    for a_prev, a_next in zip(a[:-1], a[1:]):
+        ptcl = nbody_step(float(a_prev), float(a_next), ptcl, cosmo, conf, correction)
+        obs.append(observer(float(a_next), ptcl, cosmo, conf))
+    stacked = _stack_tree(obs) if obs else None
+    return (ptcl, stacked) if return_final else stacked
+
+
 def nbody_adj(ptcl, ptcl_cot, cosmo, conf, reverse=False, correction=None):
     """Reverse sweep from the final state (nbody/solver.py:385-444).
 
