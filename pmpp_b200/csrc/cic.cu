@@ -397,6 +397,76 @@ __device__ __forceinline__ void deposit_k(int k, const Rec& r, const float* v, i
   }
 }
 
+// Epilogue of the split scatters: (float)(sum / scale) as scatter_tile
+// computes it, for the block's RX x RY rows of C channels.  With |h|, |l| <
+// 2^22 both convert exactly through the magic constant and one fma forms
+// h 2^s + l with a single rounding; |sum| < 2^53, so this equals the
+// double-precision route (which the other cells take).
+template <int C, int RX, int RY>
+__device__ __forceinline__ void split_epilogue(const unsigned int* acc, int cells, bool split, int s, double scale,
+                                               float two_s, Mesh3 m, int x0, int y0, int mode, float src_mul,
+                                               float* __restrict__ out) {
+  const double inv = 1.0 / scale;
+  const float invf = (float)inv;
+  const bool fconv = split && invf >= 0x1p-126f;
+  const int64_t mcells = m.cells();
+  const int nz = m.nz, nz4 = nz >> 2;
+  const unsigned long long* acc64 = reinterpret_cast<const unsigned long long*>(acc);
+#pragma unroll
+  for (int lx = 0; lx < RX; ++lx) {
+    if (x0 + lx >= m.nx) break;
+#pragma unroll
+    for (int ly = 0; ly < RY; ++ly) {
+      if (y0 + ly >= m.ny) break;
+      const int64_t row_off = ((int64_t)(x0 + lx) * m.ny + (y0 + ly)) * nz;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int a0 = ((lx * RY + ly) * C + c) * nz;
+        float* o = out + (int64_t)c * mcells + row_off;
+        for (int z4 = threadIdx.x; z4 < nz4; z4 += blockDim.x) {
+          float res[4];
+          if (split) {
+            const int4 lo = *reinterpret_cast<const int4*>(&acc[a0 + 4 * z4]);
+            const int4 hi = *reinterpret_cast<const int4*>(&acc[cells + a0 + 4 * z4]);
+            const int los[4] = {lo.x, lo.y, lo.z, lo.w};
+            const int his[4] = {hi.x, hi.y, hi.z, hi.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int h = his[q], l = los[q];
+              if (fconv && h > -(1 << 22) && h < (1 << 22) && l > -(1 << 22) && l < (1 << 22)) {
+                const float hf = __fsub_rn(__int_as_float(kMagicBits + h), kMagic);
+                const float lf = __fsub_rn(__int_as_float(kMagicBits + l), kMagic);
+                res[q] = __fmul_rn(__fmaf_rn(hf, two_s, lf), invf);
+              } else {
+                res[q] = (float)((double)((long long)h * (1ll << s) + (long long)l) * inv);
+              }
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) res[q] = (float)((double)(long long)acc64[a0 + 4 * z4 + q] * inv);
+          }
+          if (mode == 1) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) res[q] = __fmul_rn(__fsub_rn(res[q], 1.0f), src_mul);
+          }
+          *reinterpret_cast<float4*>(o + 4 * z4) = make_float4(res[0], res[1], res[2], res[3]);
+        }
+      }
+    }
+  }
+}
+
+// Split parameters of a block holding ntot particles (contributions per cell
+// at most ntot * dup): the plane shift s and whether the 32-bit planes apply.
+__device__ __forceinline__ void split_shift(uint32_t ntot, int dup, int E, double scale, int& s, bool& split) {
+  const uint64_t kmax = (uint64_t)ntot * (uint64_t)dup;
+  const int L = kmax ? 64 - __clzll((long long)kmax) : 0;  // kmax < 2^L
+  s = E - 21;
+  if (L + E - 31 > s) s = L + E - 31;
+  if (s < 1) s = 1;
+  split = s <= 22 && s <= 32 - L && scale < 0x1p126;
+}
+
 template <int C, int RX, int RY>
 __global__ void __launch_bounds__(256) scatter_split_kernel(const Rec* __restrict__ rec,
                                                             const uint32_t* __restrict__ perm,
@@ -454,13 +524,10 @@ __global__ void __launch_bounds__(256) scatter_split_kernel(const Rec* __restric
   __syncthreads();
   const uint32_t ntot = s_ntot;
   const uint32_t nitems = item_pre[NSRC];
-  const uint64_t kmax = (uint64_t)ntot * (uint64_t)dup;  // contributions per cell at most
-  const int L = kmax ? 64 - __clzll((long long)kmax) : 0;  // kmax < 2^L
-  int s = E - 21;
-  if (L + E - 31 > s) s = L + E - 31;
-  if (s < 1) s = 1;
   const double scale = *scale_dev;
-  const bool split = s <= 22 && s <= 32 - L && scale < 0x1p126;
+  int s;
+  bool split;
+  split_shift(ntot, dup, E, scale, s, split);
   SplitAcc A;
   A.acc = acc;
   A.cells = cells;
@@ -493,58 +560,107 @@ __global__ void __launch_bounds__(256) scatter_split_kernel(const Rec* __restric
     }
   }
   __syncthreads();
-  // Epilogue: (float)(sum / scale) as scatter_tile computes it.  With |h|, |l|
-  // < 2^22 both convert exactly through the magic constant and one fma forms
-  // h 2^s + l with a single rounding; |sum| < 2^53, so this equals the
-  // double-precision route (which the other cells take).
-  const double inv = 1.0 / scale;
-  const float invf = (float)inv;
-  const bool fconv = split && invf >= 0x1p-126f;
-  const float two_s = A.two_s;
-  const int64_t mcells = m.cells();
-  const int nz4 = nz >> 2;
+  split_epilogue<C, RX, RY>(acc, cells, split, s, scale, A.two_s, m, x0, y0, mode, src_mul, out);
+}
+
+// One output row per block (1 x 1 tile) with the particle visits of its four
+// source rows flattened over the block's threads: consecutive threads take
+// consecutive records whatever their source row, so every lane is busy (the
+// per-row 32-particle chunks of scatter_split_kernel leave the last chunk of
+// each row part-empty).  A particle of source row (x0 - 1 + sx, y0 - 1 + sy)
+// reaches the row through its corner (1 - sx, 1 - sy).  Same split planes
+// and epilogue, so the output is bit-identical.  Used for three channels,
+// where it measured 14-15% faster at 512^3 / 1024^3.
+template <int C>
+__global__ void __launch_bounds__(256) scatter_flat_kernel(const Rec* __restrict__ rec,
+                                                           const uint32_t* __restrict__ perm,
+                                                           const uint32_t* __restrict__ offs, Mesh3 m,
+                                                           const float* __restrict__ val, int val_sorted,
+                                                           float val_const, const double* __restrict__ scale_dev,
+                                                           int E, int dup, int mode, float src_mul,
+                                                           float* __restrict__ out, uint32_t* __restrict__ status) {
+  if (flagged(status)) return;
+  if (!(*scale_dev == *scale_dev)) {  // NaN scale: a non-finite value
+    if (threadIdx.x == 0) raise_flag(status, kFlagNonFiniteValue);
+    return;
+  }
+  extern __shared__ __align__(16) unsigned int acc[];  // 8 * C * nz bytes
+  __shared__ uint32_t s_beg[4], s_pre[5];
+  const int x0 = (int)(blockIdx.x / m.ny), y0 = (int)(blockIdx.x % m.ny);
+  const int nz = m.nz;
+  const int cells = C * nz;
+  {
+    uint4* a4 = reinterpret_cast<uint4*>(acc);
+    const int n4 = (2 * cells) >> 2;
+    for (int t = threadIdx.x; t < n4; t += blockDim.x) a4[t] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  if (threadIdx.x < 32) {
+    const int k = threadIdx.x;
+    uint32_t b = 0, c = 0;
+    if (k < 4) {
+      const int px = pmod(x0 - 1 + (k >> 1), m.nx), py = pmod(y0 - 1 + (k & 1), m.ny);
+      const int64_t row = (int64_t)px * m.ny + py;
+      b = offs[row];
+      c = offs[row + 1] - b;
+    }
+    uint32_t tot = c;
 #pragma unroll
-  for (int lx = 0; lx < RX; ++lx) {
-    if (x0 + lx >= m.nx) break;
+    for (int o = 1; o < 4; o <<= 1) {
+      const uint32_t z = __shfl_up_sync(0xFFFFFFFFu, tot, o);
+      if (k >= o) tot += z;
+    }
+    if (k < 4) {
+      s_beg[k] = b;
+      s_pre[k + 1] = tot;
+    }
+    if (k == 0) s_pre[0] = 0;
+  }
+  __syncthreads();
+  const uint32_t p1 = s_pre[1], p2 = s_pre[2], p3 = s_pre[3], ntot = s_pre[4];
+  // record index = visit index + (segment begin - segment prefix), mod 2^32
+  const uint32_t d0 = s_beg[0], d1 = s_beg[1] - p1, d2 = s_beg[2] - p2, d3 = s_beg[3] - p3;
+  const double scale = *scale_dev;
+  int s;
+  bool split;
+  split_shift(ntot, dup, E, scale, s, split);
+  SplitAcc A;
+  A.acc = acc;
+  A.cells = cells;
+  A.y_scale = split ? __fmul_rn((float)scale, __int_as_float((127 - s) << 23)) : 0.f;
+  A.two_s = __int_as_float((127 + s) << 23);
+  unsigned long long* acc64 = reinterpret_cast<unsigned long long*>(acc);
+  const bool zpow2 = (nz & (nz - 1)) == 0;
+  for (uint32_t vi = threadIdx.x; vi < ntot; vi += blockDim.x) {
+    const int k = (vi >= p1) + (vi >= p2) + (vi >= p3);
+    const uint32_t i = vi + (k == 0 ? d0 : k == 1 ? d1 : k == 2 ? d2 : d3);
+    const Rec r = rec[i];
+    const int cz = zpow2 ? (int)(r.key & (uint32_t)(nz - 1)) : (int)(r.key % (uint32_t)nz);
+    const int cz1 = cz + 1 == nz ? 0 : cz + 1;
+    float v[C];
+    if (val != nullptr) {
+      const int64_t src = val_sorted ? (int64_t)i : (int64_t)perm[i];
 #pragma unroll
-    for (int ly = 0; ly < RY; ++ly) {
-      if (y0 + ly >= m.ny) break;
-      const int64_t row_off = ((int64_t)(x0 + lx) * m.ny + (y0 + ly)) * nz;
+      for (int c = 0; c < C; ++c) v[c] = val[src * C + c];
+    } else {
 #pragma unroll
-      for (int c = 0; c < C; ++c) {
-        const int a0 = ((lx * RY + ly) * C + c) * nz;
-        float* o = out + (int64_t)c * mcells + row_off;
-        for (int z4 = threadIdx.x; z4 < nz4; z4 += blockDim.x) {
-          float res[4];
-          if (split) {
-            const int4 lo = *reinterpret_cast<const int4*>(&acc[a0 + 4 * z4]);
-            const int4 hi = *reinterpret_cast<const int4*>(&acc[cells + a0 + 4 * z4]);
-            const int los[4] = {lo.x, lo.y, lo.z, lo.w};
-            const int his[4] = {hi.x, hi.y, hi.z, hi.w};
+      for (int c = 0; c < C; ++c) v[c] = val_const;
+    }
+    const float wxy = __fmul_rn(axis_weight(r.fx, 1 - (k >> 1)), axis_weight(r.fy, 1 - (k & 1)));
+    const float w0 = __fmul_rn(wxy, axis_weight(r.fz, 0)), w1 = __fmul_rn(wxy, axis_weight(r.fz, 1));
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const int h = his[q], l = los[q];
-              if (fconv && h > -(1 << 22) && h < (1 << 22) && l > -(1 << 22) && l < (1 << 22)) {
-                const float hf = __fsub_rn(__int_as_float(kMagicBits + h), kMagic);
-                const float lf = __fsub_rn(__int_as_float(kMagicBits + l), kMagic);
-                res[q] = __fmul_rn(__fmaf_rn(hf, two_s, lf), invf);
-              } else {
-                res[q] = (float)((double)((long long)h * (1ll << s) + (long long)l) * inv);
-              }
-            }
-          } else {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) res[q] = (float)((double)(long long)acc64[a0 + 4 * z4 + q] * inv);
-          }
-          if (mode == 1) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) res[q] = __fmul_rn(__fsub_rn(res[q], 1.0f), src_mul);
-          }
-          *reinterpret_cast<float4*>(o + 4 * z4) = make_float4(res[0], res[1], res[2], res[3]);
-        }
+    for (int c = 0; c < C; ++c) {
+      const float c0 = __fmul_rn(v[c], w0), c1 = __fmul_rn(v[c], w1);
+      if (split) {
+        A.add(c * nz + cz, c0);
+        A.add(c * nz + cz1, c1);
+      } else {
+        atomicAdd(&acc64[c * nz + cz], (unsigned long long)__double2ll_rn((double)c0 * scale));
+        atomicAdd(&acc64[c * nz + cz1], (unsigned long long)__double2ll_rn((double)c1 * scale));
       }
     }
   }
+  __syncthreads();
+  split_epilogue<C, 1, 1>(acc, cells, split, s, scale, A.two_s, m, x0, y0, mode, src_mul, out);
 }
 
 // Block shape of the split scatter for C channels, or false when the mesh
@@ -603,7 +719,11 @@ int scatter_sorted(const Rec* rec, const uint32_t* perm, const uint32_t* offs, M
     switch (C) {
       case 1: PMB_LAUNCH_SPLIT(1, 2, 2); break;
       case 2: PMB_LAUNCH_SPLIT(2, 1, 2); break;
-      case 3: PMB_LAUNCH_SPLIT(3, 1, 1); break;
+      case 3:
+        PMB_CUDA_CHECK(smem_optin((const void*)scatter_flat_kernel<3>, 200 * 1024));
+        scatter_flat_kernel<3><<<grid, 256, (size_t)smem, s>>>(rec, perm, offs, m, val, val_sorted, val_const,
+                                                               scale_dev, E, dup, mode, src_mul, out, status);
+        break;
       default: PMB_LAUNCH_SPLIT(4, 1, 1); break;
     }
 #undef PMB_LAUNCH_SPLIT
