@@ -438,6 +438,21 @@ int pmb_deposit64(const int16_t* pmid, const double* disp, int64_t n, int nx, in
                   double* rho, void* stream);
 int pmb_axpy64(double* y, const double* x, int64_t n, double f, void* stream);
 int pmb_sum64(const double* a, int64_t n, double* out, void* stream);
+/* Force adjoint of pmb_force64 at the same positions (replaces the float64
+ * jax.vjp of gravity, nbody/gravity.py:786-814, as the float32
+ * pmb_force_vjp does): disp_cot += (d acc / d disp)^T acc_cot -- the gather
+ * adjoint's position term, the deposit of acc_cot, D2Z, the transposed
+ * Green x gradient (post src_mul / cells), Z2D and the deposit adjoint's
+ * position term with the deposited value val (cic/gather.py:475-548,
+ * cic/scatter.py:341-437).  force_meshes are pmb_force64's at these
+ * positions. */
+int64_t pmb_force_vjp64_workspace_bytes(int nx, int ny, int nz);
+int pmb_force_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz, double cell,
+                    double val, double src_mul, const double* tables, int has_masks, const double* force_meshes,
+                    const double* acc_cot, double* disp_cot, void* workspace, int64_t workspace_bytes, void* stream);
+/* *out += sum a[i] b[i] in float64 (the Omega_m cotangent dots of the float64
+ * reverse sweep, nbody/integrator.py:173-199). */
+int pmb_dot64(const double* a, const double* b, int64_t n, double* out, void* stream);
 int64_t pmb_fft64_work_bytes(int nx, int ny, int nz, int batch);
 int pmb_rfft3_64(int nx, int ny, int nz, int batch, double* in, void* out, void* work, void* stream);
 int pmb_irfft3_64(int nx, int ny, int nz, int batch, void* in, double* out, void* work, void* stream);

@@ -41,6 +41,9 @@ class SortedParticles:
 
     def __init__(self, pmid, disp, conf, mesh_shape=None, drift_vel=None, drift=0.0, offset=0.0, valid=None):
         require_cuda(pmid, disp, drift_vel, valid)
+        if disp.dtype != torch.float32:
+            raise TypeError("the cell-sorted CIC kernels take float32 displacements (the float64 build has its own "
+                            "deposit and force)")
         self.conf = conf
         self.shape = tuple(mesh_shape or conf.mesh_shape)
         self.n = pmid.shape[0]

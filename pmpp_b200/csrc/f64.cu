@@ -138,6 +138,123 @@ __global__ void gather64_kernel(const int16_t* __restrict__ pmid, const double* 
   }
 }
 
+// sign(-(f - b)) as in enmesh.py:155 (0 exactly at f == b).
+__device__ __forceinline__ double sign64(double f, int b) {
+  const double d = b ? RD::sub(f, 1.0) : f;
+  return d < 0.0 ? 1.0 : (d > 0.0 ? -1.0 : 0.0);
+}
+
+// Position term of the CIC adjoints in float64 (gather.py:495-502 with u the
+// value cotangent, scatter.py:366-370 with u the deposited value):
+//   disp_cot += sum_b (sum_c u_c mesh_c[i_b]) grad w_b / cell,
+//   grad_i w_b = sign(-(f_i - b_i)) w_{i+1} w_{i+2} (enmesh.py:155-160).
+// u: (N, C) per particle, or u_const when null.
+template <int C>
+__global__ void interp_grad64_kernel(const int16_t* __restrict__ pmid, const double* __restrict__ disp, int64_t n,
+                                     Mesh3 m, double cell, const double* __restrict__ mesh,
+                                     const double* __restrict__ u, double u_const, double* __restrict__ disp_cot) {
+  const int64_t cells = m.cells();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const Cell64 b = bin64(pmid, disp, i, m, cell);
+    double uu[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) uu[c] = u ? u[i * C + c] : u_const;
+    double w[3][2], sg[3][2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      w[a][0] = w64(b.f[a], 0);
+      w[a][1] = w64(b.f[a], 1);
+      sg[a][0] = sign64(b.f[a], 0);
+      sg[a][1] = sign64(b.f[a], 1);
+    }
+    double g[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int bx = k & 1, by = (k >> 1) & 1, bz = (k >> 2) & 1;
+      const int x = bx ? (b.c[0] + 1 == m.nx ? 0 : b.c[0] + 1) : b.c[0];
+      const int y = by ? (b.c[1] + 1 == m.ny ? 0 : b.c[1] + 1) : b.c[1];
+      const int z = bz ? (b.c[2] + 1 == m.nz ? 0 : b.c[2] + 1) : b.c[2];
+      const int64_t idx = ((int64_t)x * m.ny + y) * m.nz + z;
+      double inner = 0.0;
+#pragma unroll
+      for (int c = 0; c < C; ++c) inner = RD::add(inner, RD::mul(uu[c], mesh[(int64_t)c * cells + idx]));
+      g[0] = RD::add(g[0], RD::mul(inner, RD::mul(RD::mul(sg[0][bx], w[1][by]), w[2][bz])));
+      g[1] = RD::add(g[1], RD::mul(inner, RD::mul(RD::mul(sg[1][by], w[2][bz]), w[0][bx])));
+      g[2] = RD::add(g[2], RD::mul(inner, RD::mul(RD::mul(sg[2][bz], w[0][bx]), w[1][by])));
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) disp_cot[3 * i + a] = RD::add(disp_cot[3 * i + a], RD::div(g[a], cell));
+  }
+}
+
+// CIC deposit of per-particle C-vectors (the acceleration cotangents) into C
+// planar float64 meshes (cic/scatter.py:275-281), double atomics.
+template <int C>
+__global__ void deposit64v_kernel(const int16_t* __restrict__ pmid, const double* __restrict__ disp, int64_t n, Mesh3 m,
+                                  double cell, const double* __restrict__ val, double* __restrict__ out) {
+  const int64_t cells = m.cells();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const Cell64 b = bin64(pmid, disp, i, m, cell);
+    double v[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) v[c] = val[i * C + c];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int bx = k & 1, by = (k >> 1) & 1, bz = (k >> 2) & 1;
+      const int x = bx ? (b.c[0] + 1 == m.nx ? 0 : b.c[0] + 1) : b.c[0];
+      const int y = by ? (b.c[1] + 1 == m.ny ? 0 : b.c[1] + 1) : b.c[1];
+      const int z = bz ? (b.c[2] + 1 == m.nz ? 0 : b.c[2] + 1) : b.c[2];
+      const double w = RD::mul(RD::mul(w64(b.f[0], bx), w64(b.f[1], by)), w64(b.f[2], bz));
+      const int64_t idx = ((int64_t)x * m.ny + y) * m.nz + z;
+#pragma unroll
+      for (int c = 0; c < C; ++c) atomicAdd(&out[(int64_t)c * cells + idx], RD::mul(v[c], w));
+    }
+  }
+}
+
+// Transpose of green64_kernel (gravity.py:226-260, 290-321):
+// src_cot = post * mask * (-1/k^2) * sum_d conj(i c_d) A_d, zero at k = 0.
+__global__ void green64_adjoint_kernel(const double2* __restrict__ gc, double2* __restrict__ out, Mesh3 m, Tables64 t,
+                                       double post) {
+  const int nzh = m.nz / 2 + 1;
+  const int64_t total = m.half_cells();
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
+    const int iz = (int)(j % nzh);
+    const int64_t r = j / nzh;
+    const int iy = (int)(r % m.ny), ix = (int)(r / m.ny);
+    const double c[3] = {t.cx[ix], t.cy[iy], t.cz[iz]};
+    double sr = 0.0, si = 0.0;  // sum_d (-i c_d) A_d
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double2 a = gc[(int64_t)d * total + j];
+      sr = RD::add(sr, RD::mul(c[d], a.y));
+      si = RD::sub(si, RD::mul(c[d], a.x));
+    }
+    const double k2 = RD::add(RD::add(RD::mul(t.kx[ix], t.kx[ix]), RD::mul(t.ky[iy], t.ky[iy])),
+                              RD::mul(t.kz[iz], t.kz[iz]));
+    double pr = 0.0, pi = 0.0;
+    if (k2 != 0.0) {
+      pr = RD::div(-sr, k2);
+      pi = RD::div(-si, k2);
+    }
+    if (t.mx != nullptr) {
+      const double mk = RD::mul(RD::mul(t.mx[ix], t.my[iy]), t.mz[iz]);
+      pr = RD::mul(pr, mk);
+      pi = RD::mul(pi, mk);
+    }
+    out[j] = make_double2(RD::mul(pr, post), RD::mul(pi, post));
+  }
+}
+
+__global__ void dot64_kernel(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
+                             double* __restrict__ out) {
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s = fma(a[i], b[i], s);
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
 __global__ void axpy64_kernel(double* __restrict__ y, const double* __restrict__ x, int64_t n, double f) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     y[i] = RD::add(y[i], RD::mul(x[i], f));
@@ -167,6 +284,17 @@ int64_t force64_layout(Mesh3 m, void* ws, double** rho, double2** rho_hat, doubl
   *rho = (double*)c.take(8 * m.cells());
   *rho_hat = (double2*)c.take(16 * m.half_cells());
   *grad_hat = (double2*)c.take(48 * m.half_cells());
+  const int64_t w3 = fft_work_bytes64(m, 3), w1 = fft_work_bytes64(m, 1);
+  if (w3 < 0 || w1 < 0) return -1;
+  *work = c.take(w3 > w1 ? w3 : w1);
+  return c.off;
+}
+
+int64_t force_vjp64_layout(Mesh3 m, void* ws, double** mesh3, double2** spec3, double2** spec1, void** work) {
+  Carve64 c(ws);
+  *mesh3 = (double*)c.take(24 * m.cells());
+  *spec3 = (double2*)c.take(48 * m.half_cells());
+  *spec1 = (double2*)c.take(16 * m.half_cells());
   const int64_t w3 = fft_work_bytes64(m, 3), w1 = fft_work_bytes64(m, 1);
   if (w3 < 0 || w1 < 0) return -1;
   *work = c.take(w3 > w1 ? w3 : w1);
@@ -266,6 +394,55 @@ int pmb_force64(const int16_t* pmid, double* disp, const double* drift_vel, doub
   PMB_CUDA_CHECK(cudaGetLastError());
   F64_TRY(fft_z2d(m, 3, grad_hat, force_meshes, work, s));
   if (n > 0) gather64_kernel<<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, n, m, cell, force_meshes, acc, vel_kick, kick);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int64_t pmb_force_vjp64_workspace_bytes(int nx, int ny, int nz) {
+  double* m3;
+  double2 *s3, *s1;
+  void* w;
+  return force_vjp64_layout(Mesh3{nx, ny, nz}, nullptr, &m3, &s3, &s1, &w);
+}
+
+int pmb_force_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz, double cell,
+                    double val, double src_mul, const double* tables, int has_masks, const double* force_meshes,
+                    const double* acc_cot, double* disp_cot, void* workspace, int64_t workspace_bytes, void* stream) {
+  Mesh3 m{nx, ny, nz};
+  F64_REQUIRE(valid64(nx, ny, nz), "pmb_force_vjp64: unsupported mesh shape");
+  F64_REQUIRE(n >= 0 && n < 4294967296ll && cell > 0.0, "pmb_force_vjp64: bad particle count or cell size");
+  F64_REQUIRE(n == 0 || (pmid && disp && force_meshes && acc_cot && disp_cot), "pmb_force_vjp64: null buffer");
+  double* mesh3;
+  double2 *spec3, *spec1;
+  void* work;
+  const int64_t need = force_vjp64_layout(m, workspace, &mesh3, &spec3, &spec1, &work);
+  F64_REQUIRE(need >= 0, "pmb_force_vjp64: cuFFT plan creation failed");
+  if (need > workspace_bytes) {
+    set_last_error("pmb_force_vjp64: workspace too small");
+    return kScratchTooSmall;
+  }
+  cudaStream_t s = S(stream);
+  if (n > 0)  // gather adjoint, position term (gather.py:495-502)
+    interp_grad64_kernel<3><<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, n, m, cell, force_meshes, acc_cot, 0.0,
+                                                             disp_cot);
+  PMB_CUDA_CHECK(cudaMemsetAsync(mesh3, 0, 24 * m.cells(), s));
+  if (n > 0)  // gather adjoint, mesh term: deposit of the cotangents
+    deposit64v_kernel<3><<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, n, m, cell, acc_cot, mesh3);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  F64_TRY(fft_d2z(m, 3, mesh3, spec3, work, s));
+  green64_adjoint_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(spec3, spec1, m, tables64(tables, m, has_masks),
+                                                                       src_mul / (double)m.cells());
+  PMB_CUDA_CHECK(cudaGetLastError());
+  F64_TRY(fft_z2d(m, 1, spec1, mesh3, work, s));
+  if (n > 0)  // scatter adjoint, position term (scatter.py:366-370)
+    interp_grad64_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, n, m, cell, mesh3, nullptr, val, disp_cot);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int pmb_dot64(const double* a, const double* b, int64_t n, double* out, void* stream) {
+  F64_REQUIRE(out != nullptr && n >= 0, "pmb_dot64: bad arguments");
+  if (n > 0) dot64_kernel<<<grid_for(n, 256), 256, 0, S(stream)>>>(a, b, n, out);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }

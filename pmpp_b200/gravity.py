@@ -339,8 +339,16 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
     particles are drifted first (disp updated in place); with vel_kick the
     half-kick vel_kick += acc * kick is fused into the gather, followed by
     vel_kick += acc * kick2 when kick2 != 0 (the next step's opening kick).
-    lane selects the workspace that keeps the sorted records (see force_vjp)."""
+    lane selects the workspace that keeps the sorted records (see force_vjp).
+    float64 displacements take the float64 build (x64.force; no correction,
+    one folded kick)."""
     require_cuda(pmid, disp, drift_vel, vel_kick)
+    if disp.dtype == torch.float64:
+        if correction is not None or kick2 != 0.0 or src_hat_out is not None:
+            raise NotImplementedError("the float64 force takes no correction, one folded kick and no spectrum")
+        from . import x64
+        return x64.force(pmid, disp, conf, omega_m, acc=acc, force_meshes=force_meshes, drift_vel=drift_vel,
+                         drift=drift, vel_kick=vel_kick, kick=kick)
     n = pmid.shape[0]
     nx, ny, nz = conf.mesh_shape
     dev = disp.device
@@ -378,8 +386,14 @@ def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *
     these positions and took the same route (fused or staged); its
     cell-sorted records are reused instead of sorting again (disp is then not
     read).  concurrent: use workspaces of its own so that a force() may run on
-    another stream at the same time."""
+    another stream at the same time.  float64 displacements take
+    x64.force_vjp."""
     require_cuda(pmid, disp, force_meshes, acc_cot, disp_cot)
+    if disp.dtype == torch.float64:
+        if correction is not None or transfer_cot_out is not None:
+            raise NotImplementedError("the float64 force adjoint takes no correction")
+        from . import x64
+        return x64.force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot)
     n = pmid.shape[0]
     nx, ny, nz = conf.mesh_shape
     dev = disp.device
@@ -454,5 +468,6 @@ def gravity_vjp(a, ptcl, cosmo, conf, acc_cot, correction=None):
     acc, F = force(ptcl.pmid, ptcl.disp.clone(), conf, cosmo.Omega_m, a=a, cosmo=cosmo, correction=correction)
     dc = force_vjp(ptcl.pmid, ptcl.disp, conf, cosmo.Omega_m, F, acc_cot.contiguous(), a=a, cosmo=cosmo,
                    correction=correction)
-    om_cot = float((acc_cot.double() * acc.double()).sum()) / _om32(cosmo.Omega_m)
+    om = float(cosmo.Omega_m) if acc.dtype == torch.float64 else _om32(cosmo.Omega_m)
+    om_cot = float((acc_cot.double() * acc.double()).sum()) / om
     return dc, om_cot

@@ -51,16 +51,24 @@ def _f32(x):
 
 def kick(a_acc, a_prev, a_next, ptcl, cosmo, conf):
     """vel += acc * K (integrator.py:512-538), in place on a copy of vel."""
-    K = _f32(cosmo.kick_factor(a_acc, a_prev, a_next))
     vel = ptcl.vel.clone()
+    if vel.dtype == torch.float64:
+        from . import x64
+        x64.axpy(vel, ptcl.acc, cosmo.kick_factor(a_acc, a_prev, a_next))
+        return ptcl.replace(vel=vel)
+    K = _f32(cosmo.kick_factor(a_acc, a_prev, a_next))
     call("pmb_axpy", vel.data_ptr(), ptcl.acc.data_ptr(), vel.numel(), K, stream_handle(vel.device))
     return ptcl.replace(vel=vel)
 
 
 def drift(a_vel, a_prev, a_next, ptcl, cosmo, conf):
     """disp += vel * D (integrator.py:202-237)."""
-    D = _f32(cosmo.drift_factor(a_vel, a_prev, a_next))
     disp = ptcl.disp.clone()
+    if disp.dtype == torch.float64:
+        from . import x64
+        x64.axpy(disp, ptcl.vel, cosmo.drift_factor(a_vel, a_prev, a_next))
+        return ptcl.replace(disp=disp)
+    D = _f32(cosmo.drift_factor(a_vel, a_prev, a_next))
     call("pmb_axpy", disp.data_ptr(), ptcl.vel.data_ptr(), disp.numel(), D, stream_handle(disp.device))
     return ptcl.replace(disp=disp)
 
@@ -90,7 +98,7 @@ def integrate(a_prev, a_next, ptcl, cosmo, conf, correction=None):
 # operations fused; these are the step-by-step forms.
 # ---------------------------------------------------------------------------
 def _zeros_like(t, ref):
-    return torch.zeros_like(ref) if t is None else t.clone().float().contiguous()
+    return torch.zeros_like(ref) if t is None else t.clone().to(ref.dtype).contiguous()
 
 
 def kick_adj(a_acc, a_prev, a_next, ptcl, ptcl_cot, cosmo, cosmo_cot, conf):
@@ -102,6 +110,12 @@ def kick_adj(a_acc, a_prev, a_next, ptcl, ptcl_cot, cosmo, cosmo_cot, conf):
     vc = _zeros_like(ptcl_cot.vel, vel)
     ac = _zeros_like(ptcl_cot.acc, vel)
     dot = torch.zeros(1, dtype=torch.float64, device=vel.device)
+    if vel.dtype == torch.float64:
+        from . import x64
+        x64.dot(vc, ptcl.acc, dot, 0)
+        x64.axpy(vel, ptcl.acc, -K)
+        x64.axpy(ac, vc, K)
+        return ptcl.replace(vel=vel), ptcl_cot.replace(vel=vc, acc=ac), float(cosmo_cot) + dK * float(dot.item())
     call("pmb_kick_adj", vel.data_ptr(), ptcl.acc.data_ptr(), vc.data_ptr(), ac.data_ptr(), vel.numel(), _f32(K),
          dot.data_ptr(), stream_handle(vel.device))
     return ptcl.replace(vel=vel), ptcl_cot.replace(vel=vc, acc=ac), float(cosmo_cot) + dK * float(dot.item())
@@ -116,6 +130,12 @@ def drift_adj_from_output(a_vel, a_prev, a_next, ptcl, ptcl_cot, cosmo, cosmo_co
     dc = _zeros_like(ptcl_cot.disp, disp)
     vc = _zeros_like(ptcl_cot.vel, disp)
     dot = torch.zeros(1, dtype=torch.float64, device=disp.device)
+    if disp.dtype == torch.float64:
+        from . import x64
+        x64.axpy(disp, ptcl.vel, -D)
+        x64.axpy(vc, dc, D)
+        x64.dot(dc, ptcl.vel, dot, 0)
+        return ptcl.replace(disp=disp), ptcl_cot.replace(disp=dc, vel=vc), float(cosmo_cot) + dD * float(dot.item())
     call("pmb_drift_adj", disp.data_ptr(), ptcl.vel.data_ptr(), dc.data_ptr(), vc.data_ptr(), disp.numel(), _f32(D),
          dot.data_ptr(), stream_handle(disp.device))
     return ptcl.replace(disp=disp), ptcl_cot.replace(disp=dc, vel=vc), float(cosmo_cot) + dD * float(dot.item())
@@ -132,7 +152,8 @@ def force_adj(a, ptcl, ptcl_cot, cosmo, conf, correction=None):
     ac = _zeros_like(ptcl_cot.acc, acc)
     dc = _zeros_like(ptcl_cot.disp, acc)
     force_vjp(ptcl.pmid, ptcl.disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=correction)
-    om = float((ac.double() * acc.double()).sum()) / _om32(cosmo.Omega_m)
+    om_div = float(cosmo.Omega_m) if acc.dtype == torch.float64 else _om32(cosmo.Omega_m)
+    om = float((ac.double() * acc.double()).sum()) / om_div
     return ptcl.replace(acc=acc), ptcl_cot.replace(disp=dc, acc=torch.zeros_like(ac)), om, None
 
 
@@ -249,9 +270,13 @@ class NBodyRun:
 
         force_meshes must be the force meshes at ptcl's positions (the
         forward pass leaves them in self.final_meshes)."""
-        self._require_f32()
         conf, cosmo, corr = self.conf, self.cosmo, self.correction
         a = conf.a_nbody if a_nbody is None else np.asarray(a_nbody)
+        if conf.float_dtype == torch.float64:
+            if corr is not None:
+                raise NotImplementedError("corrections run in the float32 build")
+            from . import x64
+            return x64.nbody_adj(ptcl, ptcl_cot, cosmo, conf, a, force_meshes)
         dev = ptcl.disp.device
         s = stream_handle(dev)
         pmid = ptcl.pmid
@@ -488,6 +513,8 @@ def nbody_adj(ptcl, ptcl_cot, cosmo, conf, reverse=False, correction=None):
     Returns (ptcl_in, ptcl_in_cot, Omega_m_cot)."""
     a = conf.a_nbody[::-1] if reverse else conf.a_nbody
     run = NBodyRun(conf, cosmo, correction)
+    if conf.float_dtype == torch.float64:
+        return run.adjoint(ptcl, ptcl_cot, a_nbody=a)
     _, F = force(ptcl.pmid, ptcl.disp.clone(), conf, cosmo.Omega_m, a=float(a[-1]), cosmo=cosmo,
                  correction=correction)
     return run.adjoint(ptcl, ptcl_cot, force_meshes=F, a_nbody=a)

@@ -80,6 +80,94 @@ def force(pmid, disp, conf, omega_m, acc=None, force_meshes=None, drift_vel=None
     return acc, force_meshes
 
 
+def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None):
+    """disp_cot (+)= (d acc / d disp)^T acc_cot in float64 (pmb_force_vjp64),
+    force_meshes being force()'s at these positions."""
+    nx, ny, nz = conf.mesh_shape
+    dev = disp.device
+    n = pmid.shape[0]
+    if disp_cot is None:
+        disp_cot = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    acc_cot = acc_cot.to(torch.float64).contiguous()
+    ws = workspace(lib().pmb_force_vjp64_workspace_bytes(nx, ny, nz), dev, "force_vjp64")
+    call("pmb_force_vjp64", pmid.data_ptr(), disp.data_ptr(), n, nx, ny, nz, float(conf.cell_size),
+         float(conf.mesh_size / conf.ptcl_num), 1.5 * float(omega_m), conf.spectral_tables("mesh", dev).data_ptr(),
+         int(conf.has_particle_nyquist_masks), force_meshes.data_ptr(), acc_cot.data_ptr(), disp_cot.data_ptr(),
+         ws.data_ptr(), ws.numel(), stream_handle(dev))
+    return disp_cot
+
+
+def dot(a, b, out, slot):
+    """out[slot] += sum a * b (float64, on the device)."""
+    call("pmb_dot64", a.data_ptr(), b.data_ptr(), a.numel(), out[slot:].data_ptr(), stream_handle(a.device))
+
+
+def axpy(y, x, f):
+    """y += x * f in place (two roundings, as the reference's update)."""
+    call("pmb_axpy64", y.data_ptr(), x.data_ptr(), y.numel(), float(f), stream_handle(y.device))
+
+
+def nbody_adj(ptcl, ptcl_cot, cosmo, conf, a_nbody=None, force_meshes=None):
+    """Reverse sweep in float64 (nbody/solver.py:385-444; integrator.py:429-509,
+    541-582, 620-686, 781-837), stage by stage: a kick adjoint restores vel
+    and moves vel_cot into acc_cot; a drift stage takes the force adjoint at
+    the current positions, restores disp, moves disp_cot into vel_cot and
+    recomputes the acceleration there.  The Omega_m cotangent sums the time
+    factors' derivatives times their dots and, per force, sum(acc_cot acc) /
+    Omega_m (the force is linear in Omega_m).  force_meshes: force()'s meshes
+    at ptcl's positions (recomputed when None).  Returns (ptcl_in,
+    ptcl_cot_in, Omega_m_cot)."""
+    from .nbody import _schedule
+    a = conf.a_nbody if a_nbody is None else np.asarray(a_nbody)
+    f64 = lambda t: t.to(torch.float64).clone().contiguous()
+    pmid = ptcl.pmid
+    disp, vel = f64(ptcl.disp), f64(ptcl.vel)
+    dev = disp.device
+    z = torch.zeros_like(disp)
+    dc = f64(ptcl_cot.disp) if ptcl_cot.disp is not None else z.clone()
+    vc = f64(ptcl_cot.vel) if ptcl_cot.vel is not None else z.clone()
+    ac = f64(ptcl_cot.acc) if ptcl_cot.acc is not None else z.clone()
+    if force_meshes is None or ptcl.acc is None:
+        acc, F = force(pmid, disp, conf, cosmo.Omega_m)
+    else:
+        acc, F = f64(ptcl.acc), force_meshes
+    stages = []
+    for a_prev, a_next in zip(a[:-1][::-1], a[1:][::-1]):
+        stages.extend(reversed(_schedule(a_prev, a_next, conf)))
+    dots = torch.zeros(3 * len(stages) + 1, dtype=torch.float64, device=dev)
+    grads, force_slots, slot = [], [], 0
+    for st in stages:
+        if st[0] == "kick":
+            K, dK = cosmo.kick_factor(st[1], st[2], st[3], with_grad=True)
+            dot(vc, acc, dots, slot)
+            grads.append((dK, slot))
+            slot += 1
+            axpy(vel, acc, -K)
+            axpy(ac, vc, K)
+            continue
+        _, a_vel, a_dp, a_dn, a_acc_in = st
+        dot(ac, acc, dots, slot)
+        force_slots.append(slot)
+        slot += 1
+        force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc)
+        ac.zero_()
+        D, dD = cosmo.drift_factor(a_vel, a_dp, a_dn, with_grad=True)
+        axpy(disp, vel, -D)
+        axpy(vc, dc, D)
+        dot(dc, vel, dots, slot)
+        grads.append((dD, slot))
+        slot += 1
+        acc, F = force(pmid, disp, conf, cosmo.Omega_m, acc=acc, force_meshes=F)
+    dot(ac, acc, dots, slot)
+    force_slots.append(slot)
+    force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc)
+    ac.zero_()
+    d = dots.cpu().numpy()
+    om = sum(g * d[k] for g, k in grads) + sum(d[k] for k in force_slots) / float(cosmo.Omega_m)
+    from .particles import Particles
+    return (ptcl.replace(disp=disp, vel=vel, acc=acc), Particles(conf, pmid, dc, vc, ac), float(om))
+
+
 def nbody(ptcl, cosmo, conf, a_nbody=None):
     """Kick-drift-kick run (solver.py:253-273) in float64: initial force, then
     per step kick, drift + force, closing kick (fused into the gather)."""

@@ -1,0 +1,117 @@
+"""float64 adjoints (the reference's x64 gradients, tests/test_grad_nbody.py:
+118-179 and tests/test_finite_diff.py:87-124) against the float64 oracle.
+
+Bars: one force adjoint within 1e-12 of the oracle's transpose (relative to
+the field maximum) and its Omega_m cotangent within 1e-12; a 3-step run of a
+strongly perturbed random state (velocities of 0.5, crossing orbits) and its
+reverse sweep: final positions and the position / velocity cotangents within
+1e-10 (measured 3.5e-11 / 5.1e-11 / 4.3e-11: the orbits amplify float64
+rounding, the reconstructed initial state agrees to 1.4e-15), the Omega_m
+cotangent within 1e-5 (measured 5.4e-6: the oracle takes the time factors'
+Omega_m derivatives by central differences of step 1e-4, the build by
+complex step); stepping the per-operation adjoints reproduces the sweep
+within 1e-13; a fourth-order finite difference of the float64 run (step
+1e-4) matches the sweep's directional derivative within 1e-6, as the
+reference's protocol."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import cosmology as ocos
+from oracle import pm as opm
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _confs(n=16, mesh=2, a=None, spacing=4.0):
+    import pmpp_b200 as pb
+    co = opm.Conf(spacing, (n, n, n), mesh_shape=mesh, a_start=0.1, a_custom=a, float_dtype=np.float64)
+    conf = pb.Configuration(spacing, (n, n, n), mesh, a_start=0.1, a_custom=a, float_dtype="float64",
+                            device="cuda")
+    return pb, co, conf
+
+
+def _state(co, conf, pb, seed, spread=2.0, vel_sd=0.5):
+    rng = np.random.default_rng(seed)
+    pmid, disp = opm.gen_grid(co)
+    disp = disp + rng.normal(0, spread, size=disp.shape)
+    vel = rng.normal(0, vel_sd, size=disp.shape)
+    ptcl = pb.Particles(conf, torch.from_numpy(pmid).cuda(), torch.from_numpy(disp).cuda(),
+                        torch.from_numpy(vel).cuda())
+    return pmid, disp, vel, ptcl
+
+
+@pytest.mark.parametrize("mesh", [1, 2])
+def test_force_adjoint_float64(mesh):
+    pb, co, conf = _confs(16, mesh)
+    pmid, disp, _, ptcl = _state(co, conf, pb, 1)
+    cos = pb.boltzmann(pb.SimpleLCDM(conf))
+    ac = np.random.default_rng(2).normal(size=disp.shape)
+    dc, om = pb.gravity_vjp(1.0, ptcl, cos, conf, torch.from_numpy(ac).cuda())
+    assert dc.dtype == torch.float64
+    rdc, rom = opm.gravity_vjp(pmid, disp, co, cos.Omega_m, ac)
+    assert _rel(dc.cpu().numpy(), rdc) < 1e-12
+    np.testing.assert_allclose(om, rom, rtol=1e-12)
+
+
+def test_reverse_sweep_float64_matches_oracle():
+    a = np.linspace(0.1, 1.0, 4)
+    pb, co, conf = _confs(16, 2, a)
+    cos = pb.boltzmann(pb.SimpleLCDM(conf))
+    oc = opm.boltzmann(ocos.Cosmo(), co)
+    pmid, disp, vel, ptcl = _state(co, conf, pb, 3, 1.0)
+    run = pb.NBodyRun(conf, cos)
+    out = run.forward(ptcl)
+    rd, rv, ra = opm.nbody(pmid, disp, vel, co, oc)
+    assert _rel(out.disp.cpu().numpy(), rd) < 1e-10
+    rng = np.random.default_rng(4)
+    dcot, vcot = rng.normal(size=disp.shape), rng.normal(size=disp.shape)
+    cot = pb.Particles(conf, ptcl.pmid, torch.from_numpy(dcot).cuda(), torch.from_numpy(vcot).cuda(),
+                       torch.zeros_like(out.disp))
+    p0, c0, om = run.adjoint(out, cot)
+    _, _, rdc, rvc, rom = opm.nbody_adj(pmid, rd, rv, ra, dcot, vcot, np.zeros_like(dcot), co, oc)
+    assert _rel(c0.disp.cpu().numpy(), rdc) < 1e-10
+    assert _rel(c0.vel.cpu().numpy(), rvc) < 1e-10
+    np.testing.assert_allclose(om, rom, rtol=1e-5)
+    # the reverse sweep rebuilds the initial state to float64 round-off
+    assert _rel(p0.disp.cpu().numpy(), disp) < 1e-12
+    # the per-operation adjoints stepped by hand give the same cotangents
+    p, c, omi = out, cot, 0.0
+    for a_prev, a_next in list(zip(a[:-1], a[1:]))[::-1]:
+        p, c, omi, _ = pb.integrate_adj(a_prev, a_next, p, c, cos, omi, conf)
+    p, c, om_f, _ = pb.force_adj(float(a[0]), p, c, cos, conf)
+    omi += om_f
+    assert _rel(c.disp.cpu().numpy(), c0.disp.cpu().numpy()) < 1e-13
+    assert _rel(c.vel.cpu().numpy(), c0.vel.cpu().numpy()) < 1e-13
+    np.testing.assert_allclose(omi, om, rtol=1e-12)
+
+
+def test_reverse_sweep_float64_finite_differences():
+    a = np.linspace(0.1, 1.0, 4)
+    pb, co, conf = _confs(6, 2, a, spacing=8.0)
+    cos = pb.boltzmann(pb.SimpleLCDM(conf))
+    pmid, disp, vel, ptcl = _state(co, conf, pb, 1, 1.0, 0.3)
+    rng = np.random.default_rng(7)
+    dcot, vcot = rng.normal(size=disp.shape), rng.normal(size=disp.shape)
+    u = rng.normal(size=disp.shape)
+    u /= np.linalg.norm(u)
+    run = pb.NBodyRun(conf, cos)
+
+    def L(d):
+        p = pb.Particles(conf, ptcl.pmid, torch.from_numpy(d).cuda(), ptcl.vel)
+        o = run.forward(p)
+        return float((o.disp.cpu().numpy() * dcot).sum() + (o.vel.cpu().numpy() * vcot).sum())
+
+    eps = 1e-4
+    fd = (-L(disp + 2 * eps * u) + 8 * L(disp + eps * u) - 8 * L(disp - eps * u) + L(disp - 2 * eps * u)) / (12 * eps)
+    out = run.forward(ptcl)
+    cot = pb.Particles(conf, ptcl.pmid, torch.from_numpy(dcot).cuda(), torch.from_numpy(vcot).cuda(),
+                       torch.zeros_like(out.disp))
+    _, c0, _ = run.adjoint(out, cot)
+    np.testing.assert_allclose(float((c0.disp.cpu().numpy() * u).sum()), fd, rtol=1e-6)
