@@ -464,6 +464,27 @@ int64_t pmb_lpt64_workspace_bytes(int gx, int gy, int gz);
 int pmb_lpt64(const void* modes, int gx, int gy, int gz, double spacing, double cell_vol, const double* tables,
               int order, double D1, double V1, double D2, double V2, const int16_t* pmid, double* disp, double* vel,
               int64_t n, double cell, double* fields, void* workspace, int64_t workspace_bytes, void* stream);
+/* pmb_lpt64 with index_out (nullable): each particle's Lagrangian grid cell,
+ * which the float64 LPT adjoint needs, as pmb_lpt's index_out. */
+int pmb_lpt64_ex(const void* modes, int gx, int gy, int gz, double spacing, double cell_vol, const double* tables,
+                 int order, double D1, double V1, double D2, double V2, const int16_t* pmid, double* disp,
+                 double* vel, int64_t n, double cell, double* fields, int64_t* index_out, void* workspace,
+                 int64_t workspace_bytes, void* stream);
+/* float64 pmb_lpt_vjp (replaces the x64 jax.vjp of lpt, initial_conditions/
+ * lpt.py:337-449, as pmb_lpt_vjp does in float32): same arguments in double
+ * precision (modes / modes_cot complex128, fields, cotangents and amp
+ * float64), the same packed dL/dRe + i dL/dIm convention and growth-factor
+ * dots. */
+int64_t pmb_lpt_vjp64_workspace_bytes(int gx, int gy, int gz);
+int pmb_lpt_vjp64(const void* modes, int gx, int gy, int gz, double cell_vol, const double* tables, int order,
+                  double D1, double V1, double D2, double V2, const int64_t* index, const double* fields,
+                  const double* disp_cot, const double* vel_cot, int64_t n, const double* amp, void* modes_cot,
+                  double* dots, void* workspace, int64_t workspace_bytes, void* stream);
+/* Position term of the float64 deposit's adjoint for a constant deposited
+ * value (cic/scatter.py:366-370): disp_cot += val * sum_b mesh_cot[i_b]
+ * grad w_b / cell, particles binned directly (no sort), as pmb_deposit64. */
+int pmb_scatter_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz, double cell,
+                      double val, const double* mesh_cot, double* disp_cot, void* stream);
 int pmb_pk_shells64(const void* spec, int nx, int ny, int nz, const double* sinc_tab, int mas_power, int num_shells,
                     double* sums, void* stream);
 int pmb_overdensity64(const double* rho, double* delta, int64_t n, const double* total, void* stream);

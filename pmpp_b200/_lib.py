@@ -109,6 +109,12 @@ _SIGS = {
     "pmb_force_vjp64": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p,
                                 c_i64, c_p]),
     "pmb_dot64": (c_int, [c_p, c_p, c_i64, c_p, c_p]),
+    "pmb_lpt64_ex": (c_int, [c_p, c_int, c_int, c_int, c_d, c_d, c_p, c_int, c_d, c_d, c_d, c_d, c_p, c_p, c_p, c_i64,
+                             c_d, c_p, c_p, c_p, c_i64, c_p]),
+    "pmb_lpt_vjp64_workspace_bytes": (c_i64, [c_int, c_int, c_int]),
+    "pmb_lpt_vjp64": (c_int, [c_p, c_int, c_int, c_int, c_d, c_p, c_int, c_d, c_d, c_d, c_d, c_p, c_p, c_p, c_p, c_i64,
+                              c_p, c_p, c_p, c_p, c_i64, c_p]),
+    "pmb_scatter_vjp64": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_d, c_d, c_p, c_p, c_p]),
     "pmb_fft64_work_bytes": (c_i64, [c_int, c_int, c_int, c_int]),
     "pmb_rfft3_64": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
     "pmb_irfft3_64": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
@@ -177,7 +183,8 @@ _KERNELS = {
     "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,
     "pmb_lpt": 4, "pmb_lpt_vjp": 6, "pmb_pk_shells": 1, "pmb_shell_stats": 1, "pmb_pk_shells_adjoint": 1,
     "pmb_overdensity": 1, "pmb_ens_force": 7, "pmb_ens_step": 9, "pmb_ens_set_step": 1,
-    "pmb_force64": 5, "pmb_deposit64": 1, "pmb_axpy64": 1, "pmb_sum64": 1, "pmb_force_vjp64": 4, "pmb_dot64": 1, "pmb_white_noise_nested64": 1,
+    "pmb_force64": 5, "pmb_deposit64": 1, "pmb_axpy64": 1, "pmb_sum64": 1, "pmb_force_vjp64": 4, "pmb_dot64": 1, "pmb_lpt64_ex": 4, "pmb_lpt_vjp64": 6,
+    "pmb_scatter_vjp64": 1, "pmb_white_noise_nested64": 1,
     "pmb_linear_modes64": 1, "pmb_lpt64": 4, "pmb_pk_shells64": 1, "pmb_overdensity64": 1,
     "pmb_pmfft_z": 1, "pmb_pmfft_col": 1,
 }

@@ -211,7 +211,14 @@ def scatter_vjp(ptcl, conf, mesh_cot, val=None, offset=0, cell_size=None):
     """Adjoint of scatter (scatter.py:386-437): returns (disp_cot, val_cot).
 
     val_cot is summed over particles when val is a scalar (or None); unused
-    slots get zero cotangents."""
+    slots get zero cotangents.  The float64 build takes constant values on the
+    configuration mesh."""
+    if conf.float_dtype == torch.float64:
+        if offset not in (0, 0.0) or cell_size is not None or not (val is None or isinstance(val, float)) or \
+                tuple(mesh_cot.shape) != tuple(conf.mesh_shape) or ptcl.valid_mask() is not None:
+            raise NotImplementedError("the float64 deposit adjoint takes a constant value on the configuration mesh")
+        from . import x64
+        return x64.scatter_vjp(ptcl, conf, mesh_cot, val)
     valid = ptcl.valid_mask()
     shape = tuple(mesh_cot.shape[:3])
     mp, had = _planar(mesh_cot, conf)

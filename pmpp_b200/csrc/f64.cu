@@ -316,6 +316,23 @@ int64_t lpt64_layout(Mesh3 g, void* ws, double2** pot1, double2** spec6, double*
   return c.off;
 }
 
+int64_t lpt_vjp64_layout(Mesh3 g, void* ws, double** cot6, double2** F6, double2** Lhat, double** L, double2** pot1,
+                         double2** spec6, double** real6, void** work) {
+  Carve64 c(ws);
+  const int64_t ng = g.cells(), mc = g.half_cells();
+  *cot6 = (double*)c.take(48 * ng);
+  *F6 = (double2*)c.take(96 * mc);
+  *Lhat = (double2*)c.take(16 * mc);
+  *L = (double*)c.take(8 * ng);
+  *pot1 = (double2*)c.take(16 * mc);
+  *spec6 = (double2*)c.take(96 * mc);
+  *real6 = (double*)c.take(48 * ng);
+  const int64_t w6 = fft_work_bytes64(g, 6), w1 = fft_work_bytes64(g, 1);
+  if (w6 < 0 || w1 < 0) return -1;
+  *work = c.take(w6 > w1 ? w6 : w1);
+  return c.off;
+}
+
 Tables64 tables64(const double* t, Mesh3 m, int has_masks) {
   const int nzh = m.nz / 2 + 1;
   Tables64 s;
@@ -517,6 +534,14 @@ int64_t pmb_lpt64_workspace_bytes(int gx, int gy, int gz) {
 int pmb_lpt64(const void* modes, int gx, int gy, int gz, double spacing, double cell_vol, const double* tables,
               int order, double D1, double V1, double D2, double V2, const int16_t* pmid, double* disp, double* vel,
               int64_t n, double cell, double* fields, void* workspace, int64_t workspace_bytes, void* stream) {
+  return pmb_lpt64_ex(modes, gx, gy, gz, spacing, cell_vol, tables, order, D1, V1, D2, V2, pmid, disp, vel, n, cell,
+                      fields, nullptr, workspace, workspace_bytes, stream);
+}
+
+int pmb_lpt64_ex(const void* modes, int gx, int gy, int gz, double spacing, double cell_vol, const double* tables,
+                 int order, double D1, double V1, double D2, double V2, const int16_t* pmid, double* disp,
+                 double* vel, int64_t n, double cell, double* fields, int64_t* index_out, void* workspace,
+                 int64_t workspace_bytes, void* stream) {
   Mesh3 g{gx, gy, gz};
   F64_REQUIRE(valid64(gx, gy, gz), "pmb_lpt64: bad grid");
   F64_REQUIRE(order >= 0 && order <= 2, "pmb_lpt64: order must be 0, 1 or 2");
@@ -541,7 +566,63 @@ int pmb_lpt64(const void* modes, int gx, int gy, int gz, double spacing, double 
   }
   F64_TRY(lpt_gradients64(pot1, Lh, spec6, g, tables, inv_n, s));
   F64_TRY(fft_z2d(g, 6, spec6, fields, work, s));
-  return lpt_displace64(pmid, disp, vel, n, g, cell, spacing, fields, order, D1, V1, D2, V2, s);
+  return lpt_displace64(pmid, disp, vel, n, g, cell, spacing, fields, order, D1, V1, D2, V2, index_out, s);
+}
+
+int64_t pmb_lpt_vjp64_workspace_bytes(int gx, int gy, int gz) {
+  double *a, *l, *r;
+  double2 *f, *lh, *p, *sp;
+  void* w;
+  return lpt_vjp64_layout(Mesh3{gx, gy, gz}, nullptr, &a, &f, &lh, &l, &p, &sp, &r, &w);
+}
+
+int pmb_lpt_vjp64(const void* modes, int gx, int gy, int gz, double cell_vol, const double* tables, int order,
+                  double D1, double V1, double D2, double V2, const int64_t* index, const double* fields,
+                  const double* disp_cot, const double* vel_cot, int64_t n, const double* amp, void* modes_cot,
+                  double* dots, void* workspace, int64_t workspace_bytes, void* stream) {
+  Mesh3 g{gx, gy, gz};
+  F64_REQUIRE(valid64(gx, gy, gz), "pmb_lpt_vjp64: bad grid");
+  F64_REQUIRE(order >= 1 && order <= 2, "pmb_lpt_vjp64: order must be 1 or 2");
+  F64_REQUIRE(dots != nullptr && index != nullptr, "pmb_lpt_vjp64: dots and index required");
+  double *cot6, *L, *real6;
+  double2 *F6, *Lhat, *pot1, *spec6;
+  void* work;
+  const int64_t need = lpt_vjp64_layout(g, workspace, &cot6, &F6, &Lhat, &L, &pot1, &spec6, &real6, &work);
+  F64_REQUIRE(need >= 0, "pmb_lpt_vjp64: cuFFT plan creation failed");
+  if (need > workspace_bytes) {
+    set_last_error("pmb_lpt_vjp64: workspace too small");
+    return kScratchTooSmall;
+  }
+  cudaStream_t s = S(stream);
+  const int64_t ng = g.cells();
+  const double inv_n = 1.0 / (double)ng;
+  PMB_CUDA_CHECK(cudaMemsetAsync(cot6, 0, 48 * ng, s));
+  F64_TRY(lpt_field_cot64(index, disp_cot, vel_cot, n, ng, fields, order, D1, V1, D2, V2, cot6, dots, s));
+  F64_TRY(fft_d2z(g, 6, cot6, F6, work, s));
+  const double2* FS = nullptr;
+  if (order >= 2) {
+    F64_TRY(lpt_grad2_adjoint64(F6 + 3 * g.half_cells(), Lhat, g, tables, inv_n, s));
+    F64_TRY(fft_z2d(g, 1, Lhat, L, work, s));
+    F64_TRY(lpt_strains64((const double2*)modes, 1.0 / cell_vol, pot1, spec6, g, tables, inv_n, s));
+    F64_TRY(fft_z2d(g, 6, spec6, real6, work, s));
+    F64_TRY(lpt_source_adjoint64(real6, L, cot6, ng, s));
+    F64_TRY(fft_d2z(g, 6, cot6, spec6, work, s));
+    FS = spec6;
+  }
+  return lpt_modes_adjoint64(F6, FS, amp, (double2*)modes_cot, g, tables, 1.0 / (cell_vol * (double)ng), s);
+}
+
+int pmb_scatter_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz, double cell,
+                      double val, const double* mesh_cot, double* disp_cot, void* stream) {
+  Mesh3 m{nx, ny, nz};
+  F64_REQUIRE(valid64(nx, ny, nz), "pmb_scatter_vjp64: unsupported mesh shape");
+  F64_REQUIRE(n >= 0 && n < 4294967296ll && cell > 0.0, "pmb_scatter_vjp64: bad particle count or cell size");
+  F64_REQUIRE(n == 0 || (pmid && disp && mesh_cot && disp_cot), "pmb_scatter_vjp64: null buffer");
+  if (n > 0)
+    interp_grad64_kernel<1><<<grid_for(n, 256), 256, 0, S(stream)>>>(pmid, disp, n, m, cell, mesh_cot, nullptr, val,
+                                                                     disp_cot);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
 }
 
 int pmb_pk_shells64(const void* spec, int nx, int ny, int nz, const double* sinc_tab, int mas_power, int num_shells,

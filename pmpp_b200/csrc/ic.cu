@@ -368,9 +368,10 @@ int lpt_gradients64(const double2* pot1, const double2* L_hat, double2* grads, M
 }
 
 int lpt_displace64(const int16_t* pmid, double* disp, double* vel, int64_t n, Mesh3 g, double cell, double spacing,
-                   const double* fields, int order, double D1, double V1, double D2, double V2, cudaStream_t s) {
+                   const double* fields, int order, double D1, double V1, double D2, double V2, int64_t* index_out,
+                   cudaStream_t s) {
   lpt_displace_kernel<double><<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, vel, n, g, cell, spacing, fields, order,
-                                                                D1, V1, D2, V2, nullptr);
+                                                                D1, V1, D2, V2, index_out);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }
@@ -381,20 +382,22 @@ int lpt_displace64(const int16_t* pmid, double* disp, double* vel, int64_t n, Me
 // Field cotangents from particle cotangents (transpose of the sampling):
 // cot[m][d][idx_p] += D_m disp_cot[p,d] + V_m vel_cot[p,d], plus the FP64 dots
 // sum_p g_m[d](idx_p) * disp_cot / vel_cot for the growth-factor cotangents.
-__global__ void lpt_field_cot_kernel(const int64_t* __restrict__ index, const float* __restrict__ disp_cot,
-                                     const float* __restrict__ vel_cot, int64_t n, int64_t ng,
-                                     const float* __restrict__ fields, int order, float D1, float V1, float D2,
-                                     float V2, float* __restrict__ cot, double* __restrict__ dots) {
+template <class T>
+__global__ void lpt_field_cot_kernel(const int64_t* __restrict__ index, const T* __restrict__ disp_cot,
+                                     const T* __restrict__ vel_cot, int64_t n, int64_t ng,
+                                     const T* __restrict__ fields, int order, T D1, T V1, T D2, T V2,
+                                     T* __restrict__ cot, double* __restrict__ dots) {
+  using R = Real<T>;
   double acc[4] = {0, 0, 0, 0};
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
     const int64_t idx = index[p];
-    const float Ds[2] = {D1, D2}, Vs[2] = {V1, V2};
+    const T Ds[2] = {D1, D2}, Vs[2] = {V1, V2};
     for (int mo = 0; mo < order; ++mo) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const float dc = disp_cot[3 * p + d], vc = vel_cot[3 * p + d];
-        atomicAdd(&cot[(int64_t)(3 * mo + d) * ng + idx], __fadd_rn(__fmul_rn(Ds[mo], dc), __fmul_rn(Vs[mo], vc)));
-        const float gv = fields[(int64_t)(3 * mo + d) * ng + idx];
+        const T dc = disp_cot[3 * p + d], vc = vel_cot[3 * p + d];
+        atomicAdd(&cot[(int64_t)(3 * mo + d) * ng + idx], R::add(R::mul(Ds[mo], dc), R::mul(Vs[mo], vc)));
+        const T gv = fields[(int64_t)(3 * mo + d) * ng + idx];
         acc[2 * mo] += (double)gv * dc;
         acc[2 * mo + 1] += (double)gv * vc;
       }
@@ -409,107 +412,143 @@ __global__ void lpt_field_cot_kernel(const int64_t* __restrict__ index, const fl
 
 // L_hat_cot = G * sum_d (-i c_d) F2_d  (times post), the transpose of the
 // second-order gradient stage; F2 = rFFT of the order-2 field cotangents.
-__global__ void lpt_grad2_adjoint_kernel(const float2* __restrict__ F2, float2* __restrict__ out, Mesh3 m,
-                                         const float* __restrict__ tab, float post) {
-  const LptTables<float> t = lpt_tables(tab, m);
+template <class T>
+__global__ void lpt_grad2_adjoint_kernel(const typename Real<T>::T2* __restrict__ F2,
+                                         typename Real<T>::T2* __restrict__ out, Mesh3 m, const T* __restrict__ tab,
+                                         T post) {
+  using R = Real<T>;
+  const LptTables<T> t = lpt_tables(tab, m);
   const int64_t total = m.half_cells();
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
     const Idx3 q = unravel_half(j, m);
-    const float c[3] = {t.cx[q.ix], t.cy[q.iy], t.cz[q.iz]};
-    float ar = 0.f, ai = 0.f;
+    const T c[3] = {t.cx[q.ix], t.cy[q.iy], t.cz[q.iz]};
+    T ar = 0, ai = 0;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const float2 a = F2[(int64_t)d * total + j];
-      ar = __fadd_rn(ar, __fmul_rn(c[d], a.y));
-      ai = __fsub_rn(ai, __fmul_rn(c[d], a.x));
+      const typename Real<T>::T2 a = F2[(int64_t)d * total + j];
+      ar = R::add(ar, R::mul(c[d], a.y));
+      ai = R::sub(ai, R::mul(c[d], a.x));
     }
-    const float2 p = pot_from<float>(make_float2(ar, ai), k2_at(t, q));
-    out[j] = make_float2(__fmul_rn(p.x, post), __fmul_rn(p.y, post));
+    const typename Real<T>::T2 p = pot_from<T>(R::make2(ar, ai), k2_at(t, q));
+    out[j] = R::make2(R::mul(p.x, post), R::mul(p.y, post));
   }
 }
 
 // Cotangents of the six strains given the source cotangent L_cot:
 // d_i: L_cot * sum_{j != i} d_j;  s_ij: -2 L_cot s_ij.
-__global__ void lpt_source_adjoint_kernel(const float* __restrict__ s6, const float* __restrict__ Lc,
-                                          float* __restrict__ c6, int64_t n) {
+template <class T>
+__global__ void lpt_source_adjoint_kernel(const T* __restrict__ s6, const T* __restrict__ Lc, T* __restrict__ c6,
+                                          int64_t n) {
+  using R = Real<T>;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const float d0 = s6[i], d1 = s6[n + i], d2 = s6[2 * n + i];
-    const float l = Lc[i];
-    c6[i] = __fmul_rn(l, __fadd_rn(d1, d2));
-    c6[n + i] = __fmul_rn(l, __fadd_rn(d0, d2));
-    c6[2 * n + i] = __fmul_rn(l, __fadd_rn(d0, d1));
+    const T d0 = s6[i], d1 = s6[n + i], d2 = s6[2 * n + i];
+    const T l = Lc[i];
+    c6[i] = R::mul(l, R::add(d1, d2));
+    c6[n + i] = R::mul(l, R::add(d0, d2));
+    c6[2 * n + i] = R::mul(l, R::add(d0, d1));
 #pragma unroll
-    for (int s = 3; s < 6; ++s) c6[(int64_t)s * n + i] = __fmul_rn(__fmul_rn(-2.0f, l), s6[(int64_t)s * n + i]);
+    for (int s = 3; s < 6; ++s) c6[(int64_t)s * n + i] = R::mul(R::mul((T)-2, l), s6[(int64_t)s * n + i]);
   }
 }
 
 // modes_cot = G/V_cell * mult/N * [sum_d (-i c_d) F1_d + sum_s (-k_i k_j)_s FS_s]
 // (the packed d/dRe + i d/dIm convention), optionally times the linear-mode
 // amplitude; FS = rFFT of the strain cotangents.
-__global__ void lpt_modes_adjoint_kernel(const float2* __restrict__ F1, const float2* __restrict__ FS,
-                                         const float* __restrict__ amp, float2* __restrict__ out, Mesh3 m,
-                                         const float* __restrict__ tab, float scale) {
-  const LptTables<float> t = lpt_tables(tab, m);
+template <class T>
+__global__ void lpt_modes_adjoint_kernel(const typename Real<T>::T2* __restrict__ F1,
+                                         const typename Real<T>::T2* __restrict__ FS, const T* __restrict__ amp,
+                                         typename Real<T>::T2* __restrict__ out, Mesh3 m, const T* __restrict__ tab,
+                                         T scale) {
+  using R = Real<T>;
+  const LptTables<T> t = lpt_tables(tab, m);
   const int64_t total = m.half_cells();
   const int nzh = m.nz / 2 + 1;
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
     const Idx3 q = unravel_half(j, m);
-    const float c[3] = {t.cx[q.ix], t.cy[q.iy], t.cz[q.iz]};
-    const float k[3] = {t.kx[q.ix], t.ky[q.iy], t.kz[q.iz]};
-    const float kz0[3] = {-c[0], -c[1], -c[2]};
-    float ar = 0.f, ai = 0.f;
+    const T c[3] = {t.cx[q.ix], t.cy[q.iy], t.cz[q.iz]};
+    const T k[3] = {t.kx[q.ix], t.ky[q.iy], t.kz[q.iz]};
+    const T kz0[3] = {-c[0], -c[1], -c[2]};
+    T ar = 0, ai = 0;
     if (F1 != nullptr) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const float2 a = F1[(int64_t)d * total + j];
-        ar = __fadd_rn(ar, __fmul_rn(c[d], a.y));
-        ai = __fsub_rn(ai, __fmul_rn(c[d], a.x));
+        const typename Real<T>::T2 a = F1[(int64_t)d * total + j];
+        ar = R::add(ar, R::mul(c[d], a.y));
+        ai = R::sub(ai, R::mul(c[d], a.x));
       }
     }
     if (FS != nullptr) {
       const int pi[6] = {0, 1, 2, 0, 0, 1}, pj[6] = {0, 1, 2, 1, 2, 2};
 #pragma unroll
       for (int s = 0; s < 6; ++s) {
-        const float ki = s < 3 ? k[pi[s]] : kz0[pi[s]];
-        const float kj = s < 3 ? k[pj[s]] : kz0[pj[s]];
-        const float f = __fmul_rn(-ki, kj);
-        const float2 a = FS[(int64_t)s * total + j];
-        ar = __fadd_rn(ar, __fmul_rn(f, a.x));
-        ai = __fadd_rn(ai, __fmul_rn(f, a.y));
+        const T ki = s < 3 ? k[pi[s]] : kz0[pi[s]];
+        const T kj = s < 3 ? k[pj[s]] : kz0[pj[s]];
+        const T f = R::mul(-ki, kj);
+        const typename Real<T>::T2 a = FS[(int64_t)s * total + j];
+        ar = R::add(ar, R::mul(f, a.x));
+        ai = R::add(ai, R::mul(f, a.y));
       }
     }
-    const float mult = (q.iz == 0 || ((m.nz % 2 == 0) && q.iz == nzh - 1)) ? 1.0f : 2.0f;
-    float2 p = pot_from<float>(make_float2(ar, ai), k2_at(t, q));
-    float f = __fmul_rn(scale, mult);
-    if (amp != nullptr) f = __fmul_rn(f, amp[j]);
-    out[j] = make_float2(__fmul_rn(p.x, f), __fmul_rn(p.y, f));
+    const T mult = (q.iz == 0 || ((m.nz % 2 == 0) && q.iz == nzh - 1)) ? (T)1 : (T)2;
+    typename Real<T>::T2 p = pot_from<T>(R::make2(ar, ai), k2_at(t, q));
+    T f = R::mul(scale, mult);
+    if (amp != nullptr) f = R::mul(f, amp[j]);
+    out[j] = R::make2(R::mul(p.x, f), R::mul(p.y, f));
   }
 }
 
 int lpt_field_cot(const int64_t* index, const float* disp_cot, const float* vel_cot, int64_t n, int64_t ng,
                   const float* fields, int order, float D1, float V1, float D2, float V2, float* cot, double* dots,
                   cudaStream_t s) {
-  lpt_field_cot_kernel<<<grid_for(n, 256), 256, 0, s>>>(index, disp_cot, vel_cot, n, ng, fields, order, D1, V1, D2,
+  lpt_field_cot_kernel<float><<<grid_for(n, 256), 256, 0, s>>>(index, disp_cot, vel_cot, n, ng, fields, order, D1, V1, D2,
                                                          V2, cot, dots);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }
 
 int lpt_grad2_adjoint(const float2* F2, float2* out, Mesh3 m, const float* tab, float post, cudaStream_t s) {
-  lpt_grad2_adjoint_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(F2, out, m, tab, post);
+  lpt_grad2_adjoint_kernel<float><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(F2, out, m, tab, post);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }
 
 int lpt_source_adjoint(const float* s6, const float* Lc, float* c6, int64_t n, cudaStream_t s) {
-  lpt_source_adjoint_kernel<<<grid_for(n, 256), 256, 0, s>>>(s6, Lc, c6, n);
+  lpt_source_adjoint_kernel<float><<<grid_for(n, 256), 256, 0, s>>>(s6, Lc, c6, n);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }
 
 int lpt_modes_adjoint(const float2* F1, const float2* FS, const float* amp, float2* out, Mesh3 m, const float* tab,
                       float scale, cudaStream_t s) {
-  lpt_modes_adjoint_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(F1, FS, amp, out, m, tab, scale);
+  lpt_modes_adjoint_kernel<float><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(F1, FS, amp, out, m, tab, scale);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int lpt_field_cot64(const int64_t* index, const double* disp_cot, const double* vel_cot, int64_t n, int64_t ng,
+                    const double* fields, int order, double D1, double V1, double D2, double V2, double* cot,
+                    double* dots, cudaStream_t s) {
+  lpt_field_cot_kernel<double><<<grid_for(n, 256), 256, 0, s>>>(index, disp_cot, vel_cot, n, ng, fields, order, D1, V1,
+                                                                 D2, V2, cot, dots);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int lpt_grad2_adjoint64(const double2* F2, double2* out, Mesh3 m, const double* tab, double post, cudaStream_t s) {
+  lpt_grad2_adjoint_kernel<double><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(F2, out, m, tab, post);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int lpt_source_adjoint64(const double* s6, const double* Lc, double* c6, int64_t n, cudaStream_t s) {
+  lpt_source_adjoint_kernel<double><<<grid_for(n, 256), 256, 0, s>>>(s6, Lc, c6, n);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int lpt_modes_adjoint64(const double2* F1, const double2* FS, const double* amp, double2* out, Mesh3 m,
+                        const double* tab, double scale, cudaStream_t s) {
+  lpt_modes_adjoint_kernel<double><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(F1, FS, amp, out, m, tab, scale);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }

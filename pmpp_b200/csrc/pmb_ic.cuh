@@ -49,7 +49,15 @@ int lpt_source64(const double* s6, double* L, int64_t n, cudaStream_t s);
 int lpt_gradients64(const double2* pot1, const double2* L_hat, double2* grads, Mesh3 m, const double* tab,
                     double inv_n, cudaStream_t s);
 int lpt_displace64(const int16_t* pmid, double* disp, double* vel, int64_t n, Mesh3 g, double cell, double spacing,
-                   const double* fields, int order, double D1, double V1, double D2, double V2, cudaStream_t s);
+                   const double* fields, int order, double D1, double V1, double D2, double V2, int64_t* index_out,
+                   cudaStream_t s);
+int lpt_field_cot64(const int64_t* index, const double* disp_cot, const double* vel_cot, int64_t n, int64_t ng,
+                    const double* fields, int order, double D1, double V1, double D2, double V2, double* cot,
+                    double* dots, cudaStream_t s);
+int lpt_grad2_adjoint64(const double2* F2, double2* out, Mesh3 m, const double* tab, double post, cudaStream_t s);
+int lpt_source_adjoint64(const double* s6, const double* Lc, double* c6, int64_t n, cudaStream_t s);
+int lpt_modes_adjoint64(const double2* F1, const double2* FS, const double* amp, double2* out, Mesh3 m,
+                        const double* tab, double scale, cudaStream_t s);
 int pk_shells64(const double2* spec, Mesh3 m, const double* sinc_tab, int mas_power, int num_shells, double* sums,
                 cudaStream_t s);
 int overdensity64(const double* rho, double* delta, int64_t n, const double* total, cudaStream_t s);

@@ -30,8 +30,9 @@ class LPTResult:
 
 
 def lpt_full(modes, cosmo, conf):
-    if conf.float_dtype != torch.float32:
-        raise NotImplementedError("lpt_full (with adjoint data) exists for the float32 build; use lpt")
+    if conf.float_dtype == torch.float64:
+        from . import x64
+        return x64.lpt_full(modes, cosmo, conf)
     gx, gy, gz = conf.ptcl_grid_shape
     dev = modes.device
     modes = modes.contiguous()
@@ -65,6 +66,9 @@ def lpt_vjp(res, disp_cot, vel_cot, cosmo, conf, amp=None):
     coefficient (the complex conjugate of JAX's gradient of a real loss).  With
     amp the cotangent is chained through the linear-mode amplitude (the result
     is then w.r.t. the white-noise modes)."""
+    if res.modes.dtype == torch.complex128:
+        from . import x64
+        return x64.lpt_vjp(res, disp_cot, vel_cot, cosmo, conf, amp)
     gx, gy, gz = conf.ptcl_grid_shape
     dev = res.modes.device
     order = int(conf.lpt_order)

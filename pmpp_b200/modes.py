@@ -99,8 +99,13 @@ def linear_modes(modes, cosmo, conf, a=None, real=False):
 
 
 def linear_amplitude(cosmo, conf, a=None, device=None):
-    """sqrt(V P_lin(|k|)) per rFFT cell (float32)."""
+    """sqrt(V P_lin(|k|)) per rFFT cell (float32; float64 in the float64 build, at a = 1)."""
     device = conf.device if device is None else torch.device(device)
+    if conf.float_dtype == torch.float64:
+        if a is not None:
+            raise NotImplementedError("the float64 build takes the linear amplitude at a = 1")
+        from . import x64
+        return x64.linear_amplitude(cosmo, conf, device)
     gx, gy, gz = _grid(conf)
     amp = torch.empty((gx, gy, gz // 2 + 1), dtype=torch.float32, device=device)
     _linear_call(None, None, amp, cosmo, conf, a)

@@ -5,8 +5,10 @@ With ``Configuration(..., float_dtype="float64")`` the public functions
 ``NBodyRun.forward``, ``scatter`` and ``particles_to_pk`` route here: the same
 operations as the float32 kernels, evaluated in double precision on the
 device (cuFFT D2Z / Z2D, double-precision CIC deposit and gather), for parity
-with the reference's float64 results.  The hand-written adjoints exist for
-the float32 build only.
+with the reference's float64 results.  The adjoints of the N-body run, the
+force, the LPT displacements and the deposit exist here too (``nbody_adj``,
+``force_vjp``, ``lpt_vjp``, ``scatter_vjp``); the P(k) loss adjoint and the
+cosmology cotangents of the linear modes are float32 only.
 """
 from __future__ import annotations
 
@@ -43,6 +45,81 @@ def linear_modes(modes, cosmo, conf):
          tt.data_ptr(), int(tk.numel()), float(cosmo.A_s), float(cosmo.n_s), float(cosmo.Omega_m),
          float(cosmo.k_pivot), 1.0, float(conf.box_vol), stream_handle(dev))
     return out
+
+
+def linear_amplitude(cosmo, conf, device=None):
+    """sqrt(V P_lin(|k|)) per rFFT cell at a = 1, float64: the linear-mode
+    kernel applied to unit modes."""
+    device = conf.device if device is None else torch.device(device)
+    gx, gy, gz = conf.ptcl_grid_shape
+    ones = torch.ones((gx, gy, gz // 2 + 1), dtype=torch.complex128, device=device)
+    return linear_modes(ones, cosmo, conf).real.contiguous()
+
+
+def lpt_full(modes, cosmo, conf):
+    """lpt() that also keeps what the adjoint needs (LPTResult: sampled
+    gradient fields, each particle's Lagrangian grid cell, growth factors)."""
+    from .lpt import LPTResult
+    gx, gy, gz = conf.ptcl_grid_shape
+    dev = modes.device
+    modes = modes.to(torch.complex128).contiguous()
+    ptcl = Particles.gen_grid(conf, vel=True, device=dev)
+    fac, dfac = cosmo.lpt_factors(conf.a_start)
+    fields = torch.empty((6, gx, gy, gz), dtype=torch.float64, device=dev)
+    index = torch.empty(len(ptcl), dtype=torch.int64, device=dev)
+    ws = workspace(lib().pmb_lpt64_workspace_bytes(gx, gy, gz), dev, "lpt64")
+    call("pmb_lpt64_ex", modes.data_ptr(), gx, gy, gz, float(conf.ptcl_spacing), float(conf.ptcl_cell_vol),
+         conf.spectral_tables("particle", dev).data_ptr(), int(conf.lpt_order), float(fac[0, 0]), float(fac[0, 2]),
+         float(fac[1, 0]), float(fac[1, 2]), ptcl.pmid.data_ptr(), ptcl.disp.data_ptr(), ptcl.vel.data_ptr(),
+         len(ptcl), float(conf.cell_size), fields.data_ptr(), index.data_ptr(), ws.data_ptr(), ws.numel(),
+         stream_handle(dev))
+    return LPTResult(ptcl, modes, fields, index, fac, dfac)
+
+
+def lpt_vjp(res, disp_cot, vel_cot, cosmo, conf, amp=None):
+    """float64 adjoint of lpt (pmb_lpt_vjp64): (modes_cot in the packed
+    dL/dRe + i dL/dIm convention, Omega_m cotangent of the growth factors);
+    with amp (float64) the cotangent is w.r.t. the white-noise modes."""
+    gx, gy, gz = conf.ptcl_grid_shape
+    dev = res.modes.device
+    order = int(conf.lpt_order)
+    fac = res.factors
+    mc = torch.empty_like(res.modes)
+    if order == 0:
+        mc.zero_()
+        return mc, 0.0
+    dots = torch.zeros(4, dtype=torch.float64, device=dev)
+    ws = workspace(lib().pmb_lpt_vjp64_workspace_bytes(gx, gy, gz), dev, "lpt_vjp64")
+    dcot = disp_cot.to(torch.float64).contiguous()
+    vcot = vel_cot.to(torch.float64).contiguous()
+    amp = None if amp is None else amp.to(torch.float64).contiguous()
+    call("pmb_lpt_vjp64", res.modes.data_ptr(), gx, gy, gz, float(conf.ptcl_cell_vol),
+         conf.spectral_tables("particle", dev).data_ptr(), order, float(fac[0, 0]), float(fac[0, 2]), float(fac[1, 0]),
+         float(fac[1, 2]), res.index.data_ptr(), res.fields.data_ptr(), dcot.data_ptr(), vcot.data_ptr(),
+         res.index.numel(), None if amp is None else amp.data_ptr(), mc.data_ptr(), dots.data_ptr(), ws.data_ptr(),
+         ws.numel(), stream_handle(dev))
+    d = dots.cpu().numpy()
+    dfac = res.dfactors
+    om = sum(dfac[m, 0] * d[2 * m] + dfac[m, 2] * d[2 * m + 1] for m in range(order))
+    return mc, float(om)
+
+
+def scatter_vjp(ptcl, conf, mesh_cot, val=None):
+    """float64 adjoint of the constant-value deposit: (disp_cot, val_cot), val_cot
+    = sum(mesh_cot * deposit of unit values) (cic/scatter.py:386-437)."""
+    nx, ny, nz = conf.mesh_shape
+    dev = ptcl.disp.device
+    v = float(conf.mesh_size / conf.ptcl_num) if val is None else float(val)
+    mc = mesh_cot.to(torch.float64).contiguous()
+    disp = ptcl.disp.to(torch.float64).contiguous()
+    dc = torch.zeros_like(disp)
+    s = stream_handle(dev)
+    call("pmb_scatter_vjp64", ptcl.pmid.data_ptr(), disp.data_ptr(), len(ptcl), nx, ny, nz, float(conf.cell_size), v,
+         mc.data_ptr(), dc.data_ptr(), s)
+    unit = scatter(ptcl, conf, 1.0)
+    tot = torch.zeros(1, dtype=torch.float64, device=dev)
+    call("pmb_dot64", mc.data_ptr(), unit.data_ptr(), mc.numel(), tot.data_ptr(), s)
+    return dc, float(tot.item())
 
 
 def lpt(modes, cosmo, conf):

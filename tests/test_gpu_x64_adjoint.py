@@ -12,7 +12,11 @@ Omega_m derivatives by central differences of step 1e-4, the build by
 complex step); stepping the per-operation adjoints reproduces the sweep
 within 1e-13; a fourth-order finite difference of the float64 run (step
 1e-4) matches the sweep's directional derivative within 1e-6, as the
-reference's protocol."""
+reference's protocol.  The float64 LPT adjoint (tests/test_grad_lpt.py:
+82-134) against fourth-order differences of the 2LPT displacements, which
+are quadratic in the modes, so the difference is exact up to rounding (1e-9);
+the gradient of a density loss through linear modes, 2LPT, a 2-step run and
+the deposit w.r.t. the white-noise modes against differences (1e-6)."""
 import numpy as np
 import pytest
 import torch
@@ -115,3 +119,69 @@ def test_reverse_sweep_float64_finite_differences():
                        torch.zeros_like(out.disp))
     _, c0, _ = run.adjoint(out, cot)
     np.testing.assert_allclose(float((c0.disp.cpu().numpy() * u).sum()), fd, rtol=1e-6)
+
+
+def _mode_fd(f, x, u, eps):
+    return (-f(x + 2 * eps * u) + 8 * f(x + eps * u) - 8 * f(x - eps * u) + f(x - 2 * eps * u)) / (12 * eps)
+
+
+def _cdot(g, u):
+    """Directional derivative from the packed dL/dRe + i dL/dIm gradient."""
+    return float((g.real * u.real).sum() + (g.imag * u.imag).sum())
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_lpt_adjoint_float64_finite_differences(order):
+    import pmpp_b200 as pb
+    from pmpp_b200 import lpt as plpt
+    conf = pb.Configuration(4.0, (16, 16, 16), 2, a_start=0.1, float_dtype="float64", lpt_order=order,
+                            device="cuda")
+    cos = pb.boltzmann(pb.SimpleLCDM(conf))
+    lin = pb.linear_modes(pb.white_noise_nested(1, conf), cos, conf)
+    rng = np.random.default_rng(3)
+    n = conf.ptcl_num
+    dcot = torch.from_numpy(rng.normal(size=(n, 3))).cuda()
+    vcot = torch.from_numpy(rng.normal(size=(n, 3))).cuda()
+    res = plpt.lpt_full(lin, cos, conf)
+    g, _ = plpt.lpt_vjp(res, dcot, vcot, cos, conf)
+    assert g.dtype == torch.complex128
+    u = torch.from_numpy(rng.normal(size=lin.shape) + 1j * rng.normal(size=lin.shape)).cuda()
+    u = u * (lin.abs().max() / u.abs().max())
+
+    def L(m):
+        p = plpt.lpt(m, cos, conf)
+        return float((p.disp * dcot).sum() + (p.vel * vcot).sum())
+
+    fd = _mode_fd(L, lin, u, 1e-3)
+    np.testing.assert_allclose(_cdot(g, u), fd, rtol=1e-9)
+
+
+def test_density_loss_gradient_float64_finite_differences():
+    import pmpp_b200 as pb
+    from pmpp_b200 import lpt as plpt
+    from pmpp_b200 import modes as pmodes
+    a = np.linspace(0.1, 0.5, 3)
+    conf = pb.Configuration(8.0, (8, 8, 8), 2, a_start=0.1, a_custom=a, float_dtype="float64", device="cuda")
+    cos = pb.boltzmann(pb.SimpleLCDM(conf))
+    omega = pb.white_noise_nested(2, conf)
+    amp = pmodes.linear_amplitude(cos, conf)
+    rng = np.random.default_rng(5)
+    target = torch.from_numpy(rng.normal(1.0, 0.3, size=conf.mesh_shape)).cuda()
+    run = pb.NBodyRun(conf, cos)
+
+    def forward(w):
+        res = plpt.lpt_full(pb.linear_modes(w, cos, conf), cos, conf)
+        out = run.forward(res.ptcl)
+        return res, out, pb.scatter(out, conf)
+
+    def L(w):
+        return float(((forward(w)[2] - target)**2).sum())
+
+    res, out, rho = forward(omega)
+    dc, _ = pb.cic.scatter_vjp(out, conf, 2 * (rho - target))
+    z = torch.zeros_like(dc)
+    _, c0, _ = run.adjoint(out, pb.Particles(conf, out.pmid, dc, z, z.clone()))
+    g, _ = plpt.lpt_vjp(res, c0.disp, c0.vel, cos, conf, amp=amp)
+    u = torch.from_numpy(rng.normal(size=omega.shape) + 1j * rng.normal(size=omega.shape)).cuda()
+    fd = _mode_fd(L, omega, u, 1e-4)
+    np.testing.assert_allclose(_cdot(g, u), fd, rtol=1e-6)
