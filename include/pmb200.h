@@ -200,6 +200,48 @@ int pmb_green_gradient_adjoint(const void* grad_cot_hat, void* src_cot_hat, int 
  * finer than the particle grid, whose particle-Nyquist masks zero them). */
 int pmb_interlace_spectra(void* spec0, void* spec1, int nx, int ny, int nz, int mode, void* stream);
 
+/* ---------------- mesh-CNN residual potential ------------------------------
+ * Kernels of the mesh-CNN potential correction (replace the haiku network of
+ * corrections/mesh_cnn.py:66-110 and its use in corrections/core.py:321-331;
+ * the host composes the network).  Tensors are channel-planar float32
+ * (C, nx, ny, nz).
+ * pmb_cnn_conv3d: periodic 3x3x3 convolution (haiku Conv3D after wrap padding
+ *   by one, 'VALID'): out_z[co] = bias[co] (+ res[co]) + sum_tap sum_ci
+ *   in[ci](p + off) W[tap][ci][co], W as (3, 3, 3, ci, co); act 1 also writes
+ *   out_h = gelu(out_z) (jax.nn.gelu, tanh form); act 2 multiplies by
+ *   gelu'(zref) (a backward step).  transposed: the input gradient of a layer
+ *   with weights (3, 3, 3, co, ci), read at p - off.  Channel pairs: (2, C),
+ *   (C, C), (C, 1), C in {4, 8, 16} (forward orientation).
+ * pmb_cnn_conv3d_wgrad: dW[tap][ci][co] += sum_p in[ci](p + off) dout[co](p),
+ *   db[co] += sum_p dout[co](p) (FP64 accumulators, db nullable).
+ * pmb_cnn_stem_input: x0 = [S * inv_s, phi * inv_p].
+ * pmb_cnn_residual: R = g phi + c tanh(o); pmb_cnn_residual_adjoint: its
+ *   transpose, dots[0] += sum Rc phi, dots[1] += sum Rc tanh(o).
+ * pmb_cnn_norm_adjoint: dS = dx0[0] inv_s - S cS, dphi += dx0[1] inv_p - phi cP.
+ * pmb_green_potential: P = K(k) S_hat * post (the potential spectrum, same
+ *   tables and options as pmb_green_gradient); pmb_gradient_spectra:
+ *   grad_d = (i c_d) (P + res_scale Q) * post (Q nullable);
+ *   pmb_gradient_adjoint_plain: out = sum_d conj(i c_d) A_d * post. */
+int pmb_cnn_conv3d(const float* in, int ci, const float* W, const float* bias, const float* res, const float* zref,
+                   int act, float* out_z, float* out_h, int co, int nx, int ny, int nz, int transposed,
+                   void* stream);
+int pmb_cnn_conv3d_wgrad(const float* in, int ci, const float* dout, int co, int nx, int ny, int nz, double* dW,
+                         double* db, void* stream);
+int pmb_cnn_stem_input(const float* S, const float* phi, int64_t n, float inv_s, float inv_p, float* x0,
+                       void* stream);
+int pmb_cnn_residual(const float* phi, const float* o, int64_t n, float g, float c, float* R, void* stream);
+int pmb_cnn_residual_adjoint(const float* Rc, const float* phi, const float* o, int64_t n, float g, float c,
+                             float* dphi, float* dout, double* dots, void* stream);
+int pmb_cnn_norm_adjoint(const float* dx0, const float* S, const float* phi, int64_t n, float inv_s, float cS,
+                         float inv_p, float cP, float* dS, float* dphi, void* stream);
+int pmb_green_potential(const void* src_hat, void* pot_hat, int nx, int ny, int nz, const float* tables, int has_masks,
+                        int green_kernel, const float* transfer, const float* radial, int radial_len, float post_scale,
+                        void* stream);
+int pmb_gradient_spectra(const void* pot_hat, const void* res_hat, float res_scale, void* grad_hat, int nx, int ny,
+                         int nz, const float* tables, float post_scale, void* stream);
+int pmb_gradient_adjoint_plain(const void* grad_cot_hat, void* out_hat, int nx, int ny, int nz, const float* tables,
+                               float post_scale, void* stream);
+
 /* Windowed periodic projection of a C-order (nx, ny, nz) float mesh along one
  * axis (replaces the sum of nbody/observers.py:50-54 density_projection_observer
  * and the wraparound_slice sums of observers.py:113-124, core/utils.py:420-463).

@@ -611,6 +611,70 @@ def softening_transfer(conf, strength=0.0, start=0.7, stop=1.0, mode="smoothstep
     return np.maximum(1.0 - strength * taper, 0.0)
 
 
+def _gelu(x):
+    """jax.nn.gelu (approximate=True)."""
+    return 0.5 * x * (1.0 + np.tanh(np.sqrt(2.0 / np.pi) * (x + 0.044715 * x**3)))
+
+
+def periodic_conv3d(x, w, b):
+    """haiku Conv3D after periodic padding by one cell ('VALID'),
+    corrections/mesh_cnn.py:54-64: x (Cin, nx, ny, nz), w (3, 3, 3, Cin, Cout)."""
+    out = np.zeros((w.shape[4], ) + x.shape[1:])
+    for kd in range(3):
+        for kh in range(3):
+            for kw in range(3):
+                xs = np.roll(x, shift=(-(kd - 1), -(kh - 1), -(kw - 1)), axis=(1, 2, 3))
+                out += np.einsum("cxyz,co->oxyz", xs, w[kd, kh, kw])
+    return out + np.asarray(b)[:, None, None, None]
+
+
+def mesh_cnn_residual(params, S, phi, a, omega_m, sigma8, depth=4, max_residual=0.1):
+    """MeshResidualPotentialCorrection.__call__ (corrections/mesh_cnn.py:80-109)
+    in float64: params maps haiku names to arrays."""
+    P = {k: np.asarray(v, np.float64) for k, v in params.items()}
+    sS = np.sqrt(np.mean(S**2) + 1e-6)
+    sP = np.sqrt(np.mean(phi**2) + 1e-6)
+    feat = np.array([a, omega_m, sigma8], np.float64)
+    const = [np.full(S.shape, v) for v in feat]
+    x = np.stack([S / sS, phi / sP] + const)
+    h = _gelu(periodic_conv3d(x, P["stem/w"], P["stem/b"]))
+    for i in range(max(depth - 1, 0)):
+        r = h
+        t = _gelu(periodic_conv3d(h, P[f"block_{i}_conv1/w"], P[f"block_{i}_conv1/b"]))
+        h = _gelu(periodic_conv3d(t, P[f"block_{i}_conv2/w"], P[f"block_{i}_conv2/b"]) + r)
+    o = periodic_conv3d(h, P["out/w"], P["out/b"])[0]
+    conv_res = max_residual * np.tanh(o) * sP
+    g = max_residual * np.tanh(feat @ P["direct_gain/w"][:, 0] + P["direct_gain/b"][0])
+    return g * phi + conv_res
+
+
+def force_meshes_cnn(rho, conf, Omega_m, params, a, sigma8, kernel=None, depth=4, max_residual=0.1):
+    """force_meshes with the mesh-CNN residual added to the potential spectrum
+    (corrections/core.py:321-331): pot += rfft(R(S, irfft(pot)))."""
+    kernel = potential_kernel(conf) if kernel is None else kernel
+    cs = conf.derivative_factors("spectral")
+    om = float(np.float32(Omega_m)) if conf.float_dtype == np.float32 else float(Omega_m)
+    S = (rho - 1.0) * (1.5 * om)
+    pot = _fft.rfftn(S) * kernel
+    phi = _fft.irfftn(pot, s=conf.mesh_shape)
+    pot = pot + _fft.rfftn(mesh_cnn_residual(params, S, phi, a, om, sigma8, depth, max_residual))
+    out = []
+    for d in range(3):
+        c = cs[d].astype(np.float64)
+        shape = [1, 1, 1]
+        shape[d] = -1
+        out.append(_fft.irfftn(1j * c.reshape(shape) * pot, s=conf.mesh_shape))
+    return np.stack(out)
+
+
+def gravity_cnn(pmid, disp, conf, Omega_m, params, a, sigma8, kernel=None, depth=4, max_residual=0.1):
+    """gravity() with a mesh-CNN correction (gravity.py:786-814 via
+    _gravity_potential_from_density, :626-633)."""
+    rho = scatter(pmid, disp, conf)
+    F = force_meshes_cnn(rho, conf, Omega_m, params, a, sigma8, kernel, depth, max_residual)
+    return gather(pmid, disp, conf, F)
+
+
 def potential_kernel(conf, green_kernel="continuum", transfer=None):
     """Real multiplier from density-hat to potential-hat: G * nyquist * transfer."""
     G = green(conf, green_kernel)

@@ -54,6 +54,15 @@ _SIGS = {
     "pmb_green_gradient": (c_int, [c_p, c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p, c_int, c_f, c_p]),
     "pmb_interlace_spectra": (c_int, [c_p, c_p, c_int, c_int, c_int, c_int, c_p]),
     "pmb_project_density": (c_int, [c_p, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_p, c_p]),
+    "pmb_cnn_conv3d": (c_int, [c_p, c_int, c_p, c_p, c_p, c_p, c_int, c_p, c_p, c_int, c_int, c_int, c_int, c_int, c_p]),
+    "pmb_cnn_conv3d_wgrad": (c_int, [c_p, c_int, c_p, c_int, c_int, c_int, c_int, c_p, c_p, c_p]),
+    "pmb_cnn_stem_input": (c_int, [c_p, c_p, c_i64, c_f, c_f, c_p, c_p]),
+    "pmb_cnn_residual": (c_int, [c_p, c_p, c_i64, c_f, c_f, c_p, c_p]),
+    "pmb_cnn_residual_adjoint": (c_int, [c_p, c_p, c_p, c_i64, c_f, c_f, c_p, c_p, c_p, c_p]),
+    "pmb_cnn_norm_adjoint": (c_int, [c_p, c_p, c_p, c_i64, c_f, c_f, c_f, c_f, c_p, c_p, c_p]),
+    "pmb_green_potential": (c_int, [c_p, c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p, c_int, c_f, c_p]),
+    "pmb_gradient_spectra": (c_int, [c_p, c_p, c_f, c_p, c_int, c_int, c_int, c_p, c_f, c_p]),
+    "pmb_gradient_adjoint_plain": (c_int, [c_p, c_p, c_int, c_int, c_int, c_p, c_f, c_p]),
     "pmb_green_gradient_adjoint": (c_int, [c_p, c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p, c_int, c_f,
                                            c_p]),
     "pmb_force_workspace_bytes": (c_i64, [c_i64, c_int, c_int, c_int]),
@@ -176,7 +185,9 @@ def check(status, what):
 _KERNELS = {
     "pmb_sort_rows": 5, "pmb_sort_rows_ex": 5, "pmb_cic_general_scatter": 3, "pmb_cic_general_gather": 1,
     "pmb_cic_general_interp_grad": 1, "pmb_gather_rows": 1, "pmb_gather_rows2": 1, "pmb_interp_grad_rows": 1,
-    "pmb_green_gradient": 1, "pmb_interlace_spectra": 1, "pmb_project_density": 1,
+    "pmb_green_gradient": 1, "pmb_interlace_spectra": 1, "pmb_project_density": 1, "pmb_cnn_conv3d": 1,
+    "pmb_cnn_conv3d_wgrad": 1, "pmb_cnn_stem_input": 1, "pmb_cnn_residual": 1, "pmb_cnn_residual_adjoint": 1,
+    "pmb_cnn_norm_adjoint": 1, "pmb_green_potential": 1, "pmb_gradient_spectra": 1, "pmb_gradient_adjoint_plain": 1,
     "pmb_green_gradient_adjoint": 1, "pmb_axpy": 1,
     "pmb_kick_adj": 1, "pmb_kick_adj2": 1, "pmb_drift_cot_adj": 1, "pmb_drift_adj": 1, "pmb_dot": 1,
     "pmb_force": 9, "pmb_force2": 9, "pmb_force_streamed": 14, "pmb_force_vjp": 11, "pmb_force_vjp_presorted": 6, "pmb_sum": 1,

@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpmb200.so")
-SOURCES = ["cic.cu", "spectral.cu", "integrate.cu", "sort.cu", "ic.cu", "capi.cu", "cosmo.cpp", "noalloc.cu", "cic_general.cu", "mlp.cu", "ensemble.cu", "f64.cu", "pmfft.cu", "observe.cu"]
+SOURCES = ["cic.cu", "spectral.cu", "integrate.cu", "sort.cu", "ic.cu", "capi.cu", "cosmo.cpp", "noalloc.cu", "cic_general.cu", "mlp.cu", "ensemble.cu", "f64.cu", "pmfft.cu", "observe.cu", "meshcnn.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

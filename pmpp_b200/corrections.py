@@ -146,8 +146,9 @@ class CombinedPotentialCorrection:
     the product of their transfers, the first non-continuum Green's function and
     the one non-spectral force derivative they ask for."""
 
-    def __init__(self, window=None, pgd=None, softening=None, radial=None):
-        self.parts = [c for c in (window, pgd, softening, radial) if c is not None]
+    def __init__(self, window=None, pgd=None, softening=None, radial=None, mesh_cnn=None):
+        self.parts = [c for c in (window, pgd, softening, radial, mesh_cnn) if c is not None]
+        self.mesh_cnn_part = mesh_cnn
         self.green_kernel = next((c.green_kernel for c in self.parts if getattr(c, "green_kernel", 0) != 0), 0)
         grads = {getattr(c, "gradient_kernel", "spectral") for c in self.parts} - {"spectral"}
         if len(grads) > 1:
@@ -193,6 +194,19 @@ def _softening_from(kw):
                                     mode=kw.get("mode", kw.get("softening_mode", "smoothstep")))
 
 
+def _mesh_cnn_from(kw):
+    """init_mesh_cnn_potential_correction's keywords (corrections/mesh_cnn.py:158-205,
+    the mesh_* aliases of corrections/core.py:28-37)."""
+    from .meshcnn import MeshCNNCorrection
+    return MeshCNNCorrection(channels=kw.get("channels", kw.get("mesh_channels", 8)),
+                             depth=kw.get("depth", kw.get("mesh_depth", 4)),
+                             max_residual=kw.get("max_residual", kw.get("mesh_max_residual", 0.1)),
+                             output_init_scale=kw.get("output_init_scale", kw.get("mesh_output_init_scale", 1e-2)),
+                             seed=kw.get("seed", 0), device=kw.get("device", "cuda"),
+                             sigma8_value=kw.get("sigma8_value", 0.8),
+                             allow_missing_sigma8=kw.get("allow_missing_sigma8", False))
+
+
 def init_potential_correction(model, **kwargs):
     """The analytic models of init_potential_correction (corrections/core.py:40-151):
     "pm_window" / "cic_compensation" / "cic_window_compensation" (the window
@@ -200,8 +214,10 @@ def init_potential_correction(model, **kwargs):
     (discrete Laplacian), both with FastPM's 4-point gradient and no window
     gain, "pgd" / "fastpm_pgd", "high_k_softening" / "softening" /
     "fastpm_softening", and the window combined with either ("windowed_pgd",
-    "pm_window+pgd", "pgd_window", "windowed_softening", "pm_window+softening").
-    The trainable and neural variants other than LearnedGreen are not built."""
+    "pm_window+pgd", "pgd_window", "windowed_softening", "pm_window+softening"), the
+    mesh CNN ("mesh_cnn", "cnn") and the window with it ("windowed_mesh_cnn",
+    "pm_window+mesh_cnn").  The trainable window / PGD variants and the radial
+    spline (LearnedGreen stands in for it) are not built."""
     kw = dict(kwargs)
     kw.pop("dtype", None)
     if model in ("pm_window", "cic_compensation", "cic_window_compensation"):
@@ -218,6 +234,10 @@ def init_potential_correction(model, **kwargs):
         return CombinedPotentialCorrection(window=_window_from(kw), pgd=_pgd_from(kw))
     if model in ("windowed_softening", "pm_window+softening"):
         return CombinedPotentialCorrection(window=_window_from(kw), softening=_softening_from(kw))
+    if model in ("mesh_cnn", "cnn"):
+        return _mesh_cnn_from(kw)
+    if model in ("windowed_mesh_cnn", "pm_window+mesh_cnn"):
+        return CombinedPotentialCorrection(window=_window_from(kw), mesh_cnn=_mesh_cnn_from(kw))
     raise ValueError(f"Unsupported correction model {model!r}.")
 
 

@@ -345,6 +345,32 @@ int pmb_interlace_spectra(void* spec0, void* spec1, int nx, int ny, int nz, int 
   return interlace((float2*)spec0, (float2*)spec1, m, mode, S(stream));
 }
 
+int pmb_green_potential(const void* src_hat, void* pot_hat, int nx, int ny, int nz, const float* tables, int has_masks,
+                        int green_kernel, const float* transfer, const float* radial, int radial_len, float post_scale,
+                        void* stream) {
+  Mesh3 m{nx, ny, nz};
+  PMB_REQUIRE(nx > 0 && ny > 0 && nz > 0, "pmb_green_potential: bad shape");
+  PMB_REQUIRE(green_kernel == 0 || green_kernel == 1, "pmb_green_potential: unknown Green's function");
+  return green_potential((const float2*)src_hat, (float2*)pot_hat, m, make_tables(tables, m, has_masks),
+                         make_green(green_kernel, transfer, radial, radial_len, post_scale), S(stream));
+}
+
+int pmb_gradient_spectra(const void* pot_hat, const void* res_hat, float res_scale, void* grad_hat, int nx, int ny,
+                         int nz, const float* tables, float post_scale, void* stream) {
+  Mesh3 m{nx, ny, nz};
+  PMB_REQUIRE(nx > 0 && ny > 0 && nz > 0 && pot_hat && grad_hat, "pmb_gradient_spectra: bad arguments");
+  return gradient_spectra((const float2*)pot_hat, (const float2*)res_hat, res_scale, (float2*)grad_hat, m,
+                          make_tables(tables, m, 0), post_scale, S(stream));
+}
+
+int pmb_gradient_adjoint_plain(const void* grad_cot_hat, void* out_hat, int nx, int ny, int nz, const float* tables,
+                               float post_scale, void* stream) {
+  Mesh3 m{nx, ny, nz};
+  PMB_REQUIRE(nx > 0 && ny > 0 && nz > 0 && grad_cot_hat && out_hat, "pmb_gradient_adjoint_plain: bad arguments");
+  return gradient_adjoint_plain((const float2*)grad_cot_hat, (float2*)out_hat, m, make_tables(tables, m, 0),
+                                post_scale, S(stream));
+}
+
 int pmb_project_density(const float* mesh, int nx, int ny, int nz, int axis, int start, int stop, int max_width,
                         float* out, void* stream) {
   PMB_REQUIRE(nx > 0 && ny > 0 && nz > 0, "pmb_project_density: bad shape");

@@ -82,6 +82,11 @@ int green_gradient_component(const float2* src_hat, float2* out, Mesh3 m, SpecTa
                              cudaStream_t s);
 // interlaced-assignment phase: mode 0 s0 = (s0 + P s1) / 2, mode 1 its transpose
 int interlace(float2* s0, float2* s1, Mesh3 m, int mode, cudaStream_t s);
+// residual-potential force stages (mesh-CNN correction)
+int green_potential(const float2* src, float2* out, Mesh3 m, SpecTables t, GreenParams g, cudaStream_t s);
+int gradient_spectra(const float2* P, const float2* Q, float q_scale, float2* grad, Mesh3 m, SpecTables t, float post,
+                     cudaStream_t s);
+int gradient_adjoint_plain(const float2* A, float2* out, Mesh3 m, SpecTables t, float post, cudaStream_t s);
 
 // observe.cu: windowed periodic projection of a mesh along one axis
 int project_window(const float* mesh, Mesh3 m, int axis, int start, int stop, int max_width, float* out,

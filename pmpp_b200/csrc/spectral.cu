@@ -378,6 +378,99 @@ int interlace(float2* s0, float2* s1, Mesh3 m, int mode, cudaStream_t s) {
   return kOk;
 }
 
+// Stages of a force with a real-space residual potential (the mesh-CNN
+// correction, corrections/core.py:321-331): the potential spectrum alone,
+// the gradients of a potential plus a residual spectrum, and the transpose
+// of the gradient without the Green's function.
+//   P = K(k) S_hat * post                      (pmb_green_potential)
+//   grad_d = (i c_d) (P + q_scale Q) * post    (pmb_gradient_spectra)
+//   out = sum_d conj(i c_d) A_d * post         (pmb_gradient_adjoint_plain)
+__global__ void green_potential_kernel(const float2* __restrict__ src, float2* __restrict__ out, Mesh3 m,
+                                       SpecTables t, GreenParams g) {
+  const int64_t nzh = m.nz / 2 + 1, ny = m.ny;
+  const int64_t total = m.half_cells();
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = j / nzh, ix = r / ny;
+    const int iy = (int)(r - ix * ny), iz = (int)(j - r * nzh);
+    float2 v = src[j];
+    if (t.mx != nullptr) {
+      const float mk = __fmul_rn(__fmul_rn(t.mx[ix], t.my[iy]), t.mz[iz]);
+      v.x = __fmul_rn(v.x, mk);
+      v.y = __fmul_rn(v.y, mk);
+    }
+    const float k2 = k2_of(t, (int)ix, iy, iz);
+    float pr = 0.f, pi = 0.f;
+    if (k2 != 0.f) {
+      pr = __fdiv_rn(-v.x, k2);
+      pi = __fdiv_rn(-v.y, k2);
+      if (g.transfer != nullptr || g.radial != nullptr) {
+        const float T = transfer_of(g, t, j, (int)ix, iy, iz, m);
+        pr = __fmul_rn(pr, T);
+        pi = __fmul_rn(pi, T);
+      }
+    }
+    out[j] = make_float2(__fmul_rn(pr, g.post_scale), __fmul_rn(pi, g.post_scale));
+  }
+}
+
+__global__ void gradient_spectra_kernel(const float2* __restrict__ P, const float2* __restrict__ Q, float q_scale,
+                                        float2* __restrict__ grad, Mesh3 m, SpecTables t, float post) {
+  const int64_t nzh = m.nz / 2 + 1, ny = m.ny;
+  const int64_t total = m.half_cells();
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = j / nzh, ix = r / ny;
+    const int iy = (int)(r - ix * ny), iz = (int)(j - r * nzh);
+    float2 v = P[j];
+    if (Q != nullptr) {
+      const float2 q = Q[j];
+      v.x = __fadd_rn(v.x, __fmul_rn(q_scale, q.x));
+      v.y = __fadd_rn(v.y, __fmul_rn(q_scale, q.y));
+    }
+    const float c[3] = {t.cx[ix], t.cy[iy], t.cz[iz]};
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      grad[(int64_t)d * total + j] = make_float2(__fmul_rn(-__fmul_rn(c[d], v.y), post), __fmul_rn(__fmul_rn(c[d], v.x), post));
+  }
+}
+
+__global__ void gradient_adjoint_plain_kernel(const float2* __restrict__ A, float2* __restrict__ out, Mesh3 m,
+                                              SpecTables t, float post) {
+  const int64_t nzh = m.nz / 2 + 1, ny = m.ny;
+  const int64_t total = m.half_cells();
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = j / nzh, ix = r / ny;
+    const int iy = (int)(r - ix * ny), iz = (int)(j - r * nzh);
+    const float c[3] = {t.cx[ix], t.cy[iy], t.cz[iz]};
+    float sr = 0.f, si = 0.f;  // sum_d (-i c_d) A_d
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float2 a = A[(int64_t)d * total + j];
+      sr = __fadd_rn(sr, __fmul_rn(c[d], a.y));
+      si = __fsub_rn(si, __fmul_rn(c[d], a.x));
+    }
+    out[j] = make_float2(__fmul_rn(sr, post), __fmul_rn(si, post));
+  }
+}
+
+int green_potential(const float2* src, float2* out, Mesh3 m, SpecTables t, GreenParams g, cudaStream_t s) {
+  green_potential_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(src, out, m, t, g);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int gradient_spectra(const float2* P, const float2* Q, float q_scale, float2* grad, Mesh3 m, SpecTables t, float post,
+                     cudaStream_t s) {
+  gradient_spectra_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(P, Q, q_scale, grad, m, t, post);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int gradient_adjoint_plain(const float2* A, float2* out, Mesh3 m, SpecTables t, float post, cudaStream_t s) {
+  gradient_adjoint_plain_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(A, out, m, t, post);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
 // x = x * a + b, elementwise in float.
 __global__ void scale_real_kernel(float* __restrict__ x, int64_t n, float a, float b) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)

@@ -59,6 +59,148 @@ def _cufft_buffers(conf, dev):
     return spec3, spec1, work
 
 
+def mesh_cnn_of(correction):
+    """The mesh-CNN part of a correction (itself, or a combined correction's), or None."""
+    if correction is None:
+        return None
+    if getattr(correction, "mesh_cnn", False):
+        return correction
+    for c in getattr(correction, "parts", None) or ():
+        if getattr(c, "mesh_cnn", False):
+            return c
+    return None
+
+
+def _cnn_buffers(conf, dev, lane=""):
+    """Two extra half spectra and real meshes of the residual-potential route."""
+    L = lib()
+    nx, ny, nz = conf.mesh_shape
+    Mc = nx * ny * (nz // 2 + 1)
+    specA = workspace(8 * Mc, dev, "cnn_specA" + lane)
+    specB = workspace(8 * Mc, dev, "cnn_specB" + lane)
+    real2 = workspace(8 * conf.mesh_size, dev, "cnn_real2" + lane)
+    return specA, specB, real2
+
+
+def _cnn_potential_and_residual(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, sorted_buf, s16, real3,
+                                spec1, specA, work, cnn, a, cosmo, keep, s):
+    """S (real3[0]), its spectrum (spec1), phi = irfft(K S_hat) (real3[1]) and
+    the residual R of the mesh CNN (corrections/core.py:321-331)."""
+    n = pmid.shape[0]
+    nx, ny, nz = conf.mesh_shape
+    M = conf.mesh_size
+    masks = int(conf.has_particle_nyquist_masks)
+    call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 1, None, 0, float(conf.mesh_size / conf.ptcl_num),
+         1, 1.5 * _om32(omega_m), real3.data_ptr(), s16.data_ptr(), s)
+    call("pmb_rfft3", nx, ny, nz, 1, real3.data_ptr(), spec1.data_ptr(), work.data_ptr(), s)
+    call("pmb_green_potential", spec1.data_ptr(), specA.data_ptr(), nx, ny, nz, tables.data_ptr(), masks, gk,
+         ptr(transfer), ptr(radial), rl, float(1.0 / M), s)
+    call("pmb_irfft3", nx, ny, nz, 1, specA.data_ptr(), real3.data_ptr() + 4 * M, work.data_ptr(), s)
+    f32 = real3.view(torch.float32)
+    S, phi = f32[:M].view(nx, ny, nz), f32[M:2 * M].view(nx, ny, nz)
+    return S, phi, cnn.residual(S, phi, a, cosmo, keep=keep)
+
+
+def _force_cnn(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc, drift_vel, drift, vel_kick, kick,
+               kick2, timer, cnn, a, cosmo, lane=""):
+    """Force with the mesh-CNN residual potential on the cuFFT route:
+    sort, deposit S, R2C, P = K S_hat, phi = C2R(P), R = CNN(S, phi), R2C,
+    gradients of P + rfft(R) / cells, three C2R, gather."""
+    n = pmid.shape[0]
+    nx, ny, nz = conf.mesh_shape
+    dev = disp.device
+    s = stream_handle(dev)
+    M = conf.mesh_size
+    sorted_buf, sort_scr, s16, real3 = _stage_buffers(n, conf, dev, sorted_lane=lane)
+    spec3, spec1, work = _cufft_buffers(conf, dev)
+    specA, specB, _ = _cnn_buffers(conf, dev)
+    timer = _NoTimer() if timer is None else timer
+    t = timer.start()
+    call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
+         float(conf.cell_size), sorted_buf.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
+    t = timer.mark("sort", t)
+    _, _, R = _cnn_potential_and_residual(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, sorted_buf, s16,
+                                          real3, spec1, specA, work, cnn, a, cosmo, False, s)
+    t = timer.mark("mesh_cnn", t)
+    call("pmb_rfft3", nx, ny, nz, 1, R.data_ptr(), specB.data_ptr(), work.data_ptr(), s)
+    masks = int(conf.has_particle_nyquist_masks)
+    call("pmb_green_potential", spec1.data_ptr(), specA.data_ptr(), nx, ny, nz, tables.data_ptr(), masks, gk,
+         ptr(transfer), ptr(radial), rl, float(1.0 / M), s)
+    call("pmb_gradient_spectra", specA.data_ptr(), specB.data_ptr(), float(1.0 / M), spec3.data_ptr(), nx, ny, nz,
+         tables.data_ptr(), 1.0, s)
+    call("pmb_irfft3", nx, ny, nz, 3, spec3.data_ptr(), F.data_ptr(), work.data_ptr(), s)
+    t = timer.mark("fft_green_c2r", t)
+    call("pmb_gather_rows2", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc.data_ptr(), ptr(vel_kick),
+         float(kick), float(kick2), s)
+    timer.mark("gather", t)
+
+
+def _force_vjp_cnn(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc_cot, disp_cot, timer, cnn, a,
+                   cosmo, presorted=False, sorted_lane="", work_lane="", om_out=None):
+    """Transpose of _force_cnn.  With H_d = i c_d K and the residual path
+    R -> irfft(i c_d rfft(R)) both real convolutions, the source cotangent is
+    irfft(conj(H_d) rfft(F_cot)) + dS_R + irfft(K rfft(dphi)), where R_cot =
+    irfft(conj(i c_d) rfft(F_cot)) and (dS_R, dphi) come from the network's
+    backward; the network's parameter gradients go to cnn.grad.  om_out (a
+    list) receives the Omega_m cotangent: sum(S_cot S) / Omega_m plus the
+    conditioning feature's."""
+    n = pmid.shape[0]
+    nx, ny, nz = conf.mesh_shape
+    dev = disp.device
+    s = stream_handle(dev)
+    M = conf.mesh_size
+    masks = int(conf.has_particle_nyquist_masks)
+    slane = sorted_lane if presorted else work_lane
+    sorted_buf, sort_scr, s16, real3 = _stage_buffers(n, conf, dev, slane, work_lane)
+    spec3, spec1, work = _cufft_buffers(conf, dev)
+    specA, specB, real2 = _cnn_buffers(conf, dev, work_lane)
+    timer = _NoTimer() if timer is None else timer
+    t = timer.start()
+    if not presorted:
+        call("pmb_sort_rows", pmid.data_ptr(), disp.data_ptr(), None, 0.0, n, nx, ny, nz, float(conf.cell_size),
+             sorted_buf.data_ptr(), sort_scr.data_ptr(), sort_scr.numel(), s)
+        t = timer.mark("sort", t)
+    cot_sorted = workspace(12 * n, dev, "st_cot_sorted" + work_lane)
+    call("pmb_interp_grad_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc_cot.data_ptr(), 0.0,
+         float(conf.cell_size), 1, disp_cot.data_ptr(), None, cot_sorted.data_ptr(), s)
+    call("pmb_scatter_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 3, cot_sorted.data_ptr(), 1, 0.0, 0, 1.0,
+         real3.data_ptr(), s16.data_ptr(), s)
+    call("pmb_rfft3", nx, ny, nz, 3, real3.data_ptr(), spec3.data_ptr(), work.data_ptr(), s)
+    # direct path (S_cot1) and residual path (R_cot), both with 1 / cells
+    f2 = real2.view(torch.float32)
+    Sc, Rc = f2[:M].view(nx, ny, nz), f2[M:2 * M].view(nx, ny, nz)
+    call("pmb_green_gradient_adjoint", spec3.data_ptr(), spec1.data_ptr(), nx, ny, nz, tables.data_ptr(), masks, gk,
+         ptr(transfer), ptr(radial), rl, float(1.0 / M), s)
+    call("pmb_irfft3", nx, ny, nz, 1, spec1.data_ptr(), Sc.data_ptr(), work.data_ptr(), s)
+    call("pmb_gradient_adjoint_plain", spec3.data_ptr(), specB.data_ptr(), nx, ny, nz, tables.data_ptr(),
+         float(1.0 / M), s)
+    call("pmb_irfft3", nx, ny, nz, 1, specB.data_ptr(), Rc.data_ptr(), work.data_ptr(), s)
+    t = timer.mark("adjoint_spectral", t)
+    # the network at these positions, then its backward
+    S, phi, _ = _cnn_potential_and_residual(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, sorted_buf,
+                                            s16, real3, spec1, specA, work, cnn, a, cosmo, True, s)
+    dS, dphi, dparams, dfeat = cnn.residual_adjoint(Rc)
+    if cnn.accumulate_grads:
+        cnn.grad += dparams
+    t = timer.mark("mesh_cnn_adjoint", t)
+    # phi = irfft(K rfft(S)) is a real convolution with K even: its transpose is itself
+    call("pmb_rfft3", nx, ny, nz, 1, dphi.data_ptr(), specB.data_ptr(), work.data_ptr(), s)
+    call("pmb_green_potential", specB.data_ptr(), specA.data_ptr(), nx, ny, nz, tables.data_ptr(), masks, gk,
+         ptr(transfer), ptr(radial), rl, float(1.0 / M), s)
+    call("pmb_irfft3", nx, ny, nz, 1, specA.data_ptr(), dphi.data_ptr(), work.data_ptr(), s)
+    call("pmb_axpy", Sc.data_ptr(), dS.data_ptr(), M, 1.0, s)
+    call("pmb_axpy", Sc.data_ptr(), dphi.data_ptr(), M, 1.0, s)
+    om32 = _om32(omega_m)
+    if om_out is not None:
+        d = torch.zeros(1, dtype=torch.float64, device=dev)
+        call("pmb_dot", Sc.data_ptr(), S.data_ptr(), M, d.data_ptr(), s)
+        om_out.append(float(d.item()) / om32 + float(dfeat[1]))
+    call("pmb_interp_grad_rows", sorted_buf.data_ptr(), n, nx, ny, nz, 1, Sc.data_ptr(), None,
+         float(conf.mesh_size / conf.ptcl_num) * 1.5 * om32, float(conf.cell_size), 1, disp_cot.data_ptr(), None,
+         None, s)
+    timer.mark("scatter_adjoint", t)
+
+
 def uses_interlacing(correction):
     """force_uses_interlacing (corrections/core.py:381-393): a correction, or
     any part of a combined one, asking for interlaced assignment."""
@@ -358,6 +500,13 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
         acc = torch.empty((n, 3), dtype=torch.float32, device=dev)
     gk, transfer, radial, rl = _correction_args(correction, a, cosmo, conf)
     tables = _tables(conf, dev, gk, correction)
+    cnn = mesh_cnn_of(correction)
+    if cnn is not None:
+        if uses_interlacing(correction) or src_hat_out is not None:
+            raise NotImplementedError("the mesh-CNN correction takes no interlacing and no learned radial transfer")
+        _force_cnn(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc, drift_vel, drift,
+                   vel_kick, kick, kick2, StageTimer.active, cnn, a, cosmo, lane)
+        return acc, force_meshes
     if uses_interlacing(correction):
         _force_interlaced(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc, drift_vel,
                           drift, vel_kick, kick, kick2, StageTimer.active, src_hat_out, lane)
@@ -379,7 +528,7 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
 
 def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *, a=None, cosmo=None,
               correction=None, src_hat=None, transfer_cot_out=None, presorted=False, sorted_lane="",
-              concurrent=False):
+              concurrent=False, om_out=None):
     """disp_cot (+)= (d acc / d disp)^T acc_cot, with force_meshes computed at disp.
 
     presorted: the last force() call with lane=sorted_lane was at exactly
@@ -387,7 +536,8 @@ def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *
     cell-sorted records are reused instead of sorting again (disp is then not
     read).  concurrent: use workspaces of its own so that a force() may run on
     another stream at the same time.  float64 displacements take
-    x64.force_vjp."""
+    x64.force_vjp.  om_out (a list) receives the force's Omega_m cotangent
+    where it is not sum(acc_cot acc) / Omega_m (the mesh-CNN correction)."""
     require_cuda(pmid, disp, force_meshes, acc_cot, disp_cot)
     if disp.dtype == torch.float64:
         if correction is not None or transfer_cot_out is not None:
@@ -401,6 +551,13 @@ def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *
         disp_cot = torch.zeros((n, 3), dtype=torch.float32, device=dev)
     gk, transfer, radial, rl = _correction_args(correction, a, cosmo, conf)
     tables = _tables(conf, dev, gk, correction)
+    cnn = mesh_cnn_of(correction)
+    if cnn is not None:
+        if uses_interlacing(correction) or transfer_cot_out is not None:
+            raise NotImplementedError("the mesh-CNN correction takes no interlacing and no learned radial transfer")
+        _force_vjp_cnn(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc_cot, disp_cot,
+                       StageTimer.active, cnn, a, cosmo, presorted, sorted_lane, "v" if concurrent else "", om_out)
+        return disp_cot
     if uses_interlacing(correction):
         _force_vjp_interlaced(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc_cot,
                               disp_cot, StageTimer.active, src_hat, transfer_cot_out, presorted, sorted_lane,
@@ -466,8 +623,11 @@ def gravity(a, ptcl, cosmo, conf, correction=None):
 def gravity_vjp(a, ptcl, cosmo, conf, acc_cot, correction=None):
     """Returns (disp_cot, Omega_m_cot) of gravity w.r.t. acc_cot."""
     acc, F = force(ptcl.pmid, ptcl.disp.clone(), conf, cosmo.Omega_m, a=a, cosmo=cosmo, correction=correction)
+    om_out = []
     dc = force_vjp(ptcl.pmid, ptcl.disp, conf, cosmo.Omega_m, F, acc_cot.contiguous(), a=a, cosmo=cosmo,
-                   correction=correction)
+                   correction=correction, om_out=om_out)
+    if om_out:
+        return dc, om_out[0]
     om = float(cosmo.Omega_m) if acc.dtype == torch.float64 else _om32(cosmo.Omega_m)
     om_cot = float((acc_cot.double() * acc.double()).sum()) / om
     return dc, om_cot

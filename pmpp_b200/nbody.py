@@ -151,9 +151,11 @@ def force_adj(a, ptcl, ptcl_cot, cosmo, conf, correction=None):
     acc, F = force(ptcl.pmid, ptcl.disp.clone(), conf, cosmo.Omega_m, a=a, cosmo=cosmo, correction=correction)
     ac = _zeros_like(ptcl_cot.acc, acc)
     dc = _zeros_like(ptcl_cot.disp, acc)
-    force_vjp(ptcl.pmid, ptcl.disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=correction)
+    om_out = []
+    force_vjp(ptcl.pmid, ptcl.disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=correction,
+              om_out=om_out)
     om_div = float(cosmo.Omega_m) if acc.dtype == torch.float64 else _om32(cosmo.Omega_m)
-    om = float((ac.double() * acc.double()).sum()) / om_div
+    om = om_out[0] if om_out else float((ac.double() * acc.double()).sum()) / om_div
     return ptcl.replace(acc=acc), ptcl_cot.replace(disp=dc, acc=torch.zeros_like(ac)), om, None
 
 
@@ -259,7 +261,7 @@ class NBodyRun:
             corr.accumulate(a, cosmo, conf, tc)
         else:
             force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=a, cosmo=cosmo, correction=corr,
-                      presorted=presorted, sorted_lane=lane, concurrent=concurrent)
+                      presorted=presorted, sorted_lane=lane, concurrent=concurrent, om_out=self._om_exact)
 
     def _require_f32(self):
         if self.conf.float_dtype != torch.float32:
@@ -294,6 +296,9 @@ class NBodyRun:
             ops.extend(reversed(_schedule(a_prev, a_next, conf)))
         ops.append(("init", ))
         dots = torch.zeros(2 * len(ops) + 2, dtype=torch.float64, device=dev)
+        # forces whose Omega_m cotangent is not sum(acc_cot acc) / Omega_m
+        # (the mesh-CNN correction) report it here instead
+        self._om_exact = []
         grads = []  # (d factor / d Omega_m, dot slot) pairs, reduced on the host at the end
         force_slots = []
         slot = 0
@@ -398,7 +403,10 @@ class NBodyRun:
         if zero_pending:
             ac.zero_()
         d = dots.cpu().numpy()
-        om_cot = sum(g * d[k] for g, k in grads) + sum(d[k] for k in force_slots) / om32
+        if self._om_exact:
+            om_cot = sum(g * d[k] for g, k in grads) + sum(self._om_exact)
+        else:
+            om_cot = sum(g * d[k] for g, k in grads) + sum(d[k] for k in force_slots) / om32
         return (ptcl.replace(disp=disp, vel=vel, acc=acc), Particles(conf, pmid, dc, vc, ac), float(om_cot))
 
 

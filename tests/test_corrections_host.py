@@ -90,3 +90,66 @@ def test_windowed_softening_and_gradient_selection():
     w4 = PMWindowCompensation(gradient_kernel="fastpm_4point")
     with pytest.raises(ValueError, match="incompatible force-gradient kernels"):
         CombinedPotentialCorrection(window=w4, pgd=Other())
+
+
+def test_pgd_and_softening_reference_cases():
+    """tests/test_potential_correction.py:224-275 restated: the PGD transfer is
+    1 at k = 0 and 1 - alpha0 band elsewhere; softening of strength 0.2 keeps
+    the transfer in [0.8, 1] and 1 below the taper."""
+    import pmpp_b200 as pb
+    conf = pb.Configuration(1.0, (8, 8, 8), 1, device="cpu")
+    co = opm.Conf(1.0, (8, 8, 8), mesh_shape=1)
+    from pmpp_b200.corrections import init_potential_correction
+    p = init_potential_correction("pgd", pgd_alpha0=0.25, pgd_A=0.0, pgd_B=0.0, pgd_kl=0.5, pgd_ks=2.0)
+    T, _ = p.transfer_tables(1.0, None, conf)
+    assert float(T[0, 0, 0]) == 1.0
+    k2 = sum(np.meshgrid(*[k.astype(np.float64)**2 for k in co.kvec], indexing="ij"))
+    band = np.where(k2 > 0, np.exp(-0.25 / np.where(k2 > 0, k2, 1) - np.where(k2 > 0, k2, 1)**2 / 16.0), 0.0)
+    np.testing.assert_allclose(T.numpy(), 1 - 0.25 * band, atol=1e-6)
+    s = init_potential_correction("high_k_softening", softening_strength=0.2, softening_start=0.5,
+                                  softening_stop=1.0)
+    Ts, _ = s.transfer_tables(1.0, None, conf)
+    assert float(Ts[0, 0, 0]) == 1.0 and float(Ts.min()) < 1.0 and float(Ts.min()) >= 0.8 - 1e-6
+
+
+def test_mesh_cnn_parameters_follow_haiku_layout_and_init():
+    """Parameter names and shapes of MeshResidualPotentialCorrection
+    (corrections/mesh_cnn.py:80-109): stem over 5 input channels, depth-1
+    residual blocks, a zero-initialised output layer and a gain of stddev
+    output_init_scale; the window+mesh-CNN model combines both."""
+    from pmpp_b200.corrections import CombinedPotentialCorrection, init_potential_correction
+    c = init_potential_correction("mesh_cnn", mesh_channels=8, mesh_depth=4, output_init_scale=0.05, device="cpu")
+    shapes = dict(c.layout)
+    assert shapes["stem/w"] == (3, 3, 3, 5, 8) and shapes["out/w"] == (3, 3, 3, 8, 1)
+    assert [n for n in shapes if n.startswith("block_")] == [f"block_{i}_conv{j}/{p}" for i in range(3)
+                                                              for j in (1, 2) for p in ("w", "b")]
+    assert float(c.view("out/w").abs().max()) == 0.0 and float(c.view("stem/b").abs().max()) == 0.0
+    w = c.view("stem/w")
+    assert abs(float(w.std()) - (1 / 135)**0.5) < 0.03 and float(w.abs().max()) <= 2 * (1 / 135)**0.5 / 0.8796 + 1e-6
+    assert float(c.view("direct_gain/w").abs().max()) < 0.5
+    cw = init_potential_correction("pm_window+mesh_cnn", channels=4, depth=2, device="cpu")
+    assert isinstance(cw, CombinedPotentialCorrection) and cw.green_kernel == 1 and cw.mesh_cnn_part is not None
+    with pytest.raises(ValueError, match="4, 8 or 16"):
+        init_potential_correction("cnn", channels=6, device="cpu")
+
+
+def test_oracle_mesh_cnn_reference_properties():
+    """The restatement: zero output layer and zero gain give no residual, a
+    zero output layer alone a uniform rescaling of the potential, and zero
+    parameters leave the force unchanged."""
+    from pmpp_b200.meshcnn import param_layout
+    rng = np.random.default_rng(0)
+    P = {n: rng.normal(size=s) * 0.2 for n, s in param_layout(4, 2)}
+    P["out/w"][:] = 0
+    P["out/b"][:] = 0
+    S, phi = rng.normal(size=(6, 6, 6)), rng.normal(size=(6, 6, 6))
+    R = opm.mesh_cnn_residual(P, S, phi, 1.0, 0.3, 0.8, depth=2, max_residual=0.2)
+    np.testing.assert_allclose(R / phi, (R / phi).flat[0], rtol=1e-12)
+    P["direct_gain/w"][:] = 0
+    P["direct_gain/b"][:] = 0
+    assert np.all(opm.mesh_cnn_residual(P, S, phi, 1.0, 0.3, 0.8, depth=2, max_residual=0.2) == 0)
+    co = opm.Conf(4.0, (4, 4, 4), mesh_shape=2)
+    pmid, disp = opm.gen_grid(co)
+    disp = disp + rng.normal(0, 1.0, disp.shape)
+    np.testing.assert_allclose(opm.gravity_cnn(pmid, disp, co, 0.3, P, 1.0, 0.8, depth=2),
+                               opm.gravity(pmid, disp, co, 0.3), rtol=1e-12, atol=1e-14)
