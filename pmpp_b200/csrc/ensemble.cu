@@ -233,6 +233,11 @@ __global__ void ens_advance_kernel(int* step) { *step += 1; }
 struct EnsClass {
   Mesh3 m;
   int first, count;
+  // pass-chain classes: the members' tables at a uniform stride (set at bind)
+  const float* tab_base = nullptr;
+  int64_t tab_stride = 0;
+  int has_masks = 0;
+  bool batched = false;
 };
 
 struct Ensemble {
@@ -406,7 +411,18 @@ int run_stage(Ensemble* e, int stage, int drift, int kick, cudaStream_t s) {
       // members on the pass chain run their whole spectral chain here (the
       // same kernels as a single run's pmb_force); the others R2C by class
       for (const EnsClass& c : e->classes) {
-        if (e->sims[c.first].pm) {
+        if (e->sims[c.first].pm && c.batched) {
+          // the whole class in one launch per pass, each member with its tables
+          GreenParams g;
+          g.green_kernel = 0;
+          g.cell = 0.f;
+          g.transfer = nullptr;
+          g.radial = nullptr;
+          g.radial_len = 0;
+          g.post_scale = e->sims[c.first].post;
+          ENS_TRY(pmfft_force_batched(c.m, c.count, e->sims[c.first].rho, e->sims[c.first].force,
+                                      (float2*)e->pm_work, c.tab_base, c.tab_stride, c.has_masks, g, s));
+        } else if (e->sims[c.first].pm) {
           for (int i = c.first; i < c.first + c.count; ++i) {
             const EnsSim& q = e->sims[i];
             GreenParams g;
@@ -523,7 +539,7 @@ int pmb_ens_create(int nsims, const int64_t* counts, const int32_t* mesh_shapes,
   for (const EnsClass& c : e->classes) {
     if (pmfft_enabled() && pmfft_supported(c.m)) {
       for (int i = c.first; i < c.first + c.count; ++i) e->sims[i].pm = 1;
-      const int64_t pb = 5 * 8 * pmfft_channel_elems(c.m);
+      const int64_t pb = 5 * 8 * pmfft_channel_elems(c.m) * c.count;
       e->pm_bytes = e->pm_bytes > pb ? e->pm_bytes : pb;
       continue;
     }
@@ -587,6 +603,18 @@ int pmb_ens_bind(void* handle, const int16_t* pmid, float* disp, float* vel, flo
     q.grad_hat = (float2*)grad_hat + 3 * e->spec_start[i];
     q.force = force + 3 * e->mesh_start[i];
     q.t = spec_tables_from(tables + table_offsets[i], q.m, e->has_masks[i]);
+  }
+  for (EnsClass& c : e->classes) {
+    // one batched pass chain per class when the members' tables sit at a
+    // uniform stride with the same masks (the layout the host builds)
+    c.tab_base = tables + table_offsets[c.first];
+    c.has_masks = e->has_masks[c.first];
+    c.tab_stride = c.count > 1 ? table_offsets[c.first + 1] - table_offsets[c.first] : 0;
+    bool ok = true;
+    for (int i = c.first; i < c.first + c.count; ++i)
+      ok = ok && e->has_masks[i] == c.has_masks &&
+           table_offsets[i] == table_offsets[c.first] + (int64_t)(i - c.first) * c.tab_stride;
+    c.batched = ok;
   }
   e->d_sims = (EnsSim*)(w + L.sims);
   e->tile_sums = (uint32_t*)(w + L.tsums);

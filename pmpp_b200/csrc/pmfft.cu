@@ -273,7 +273,30 @@ struct ColArgs {
   const float2* tw;
   SpecTables t;
   GreenParams g;
+  // batches of equal-shape meshes with their own tables (ensembles): batch b
+  // reads the table array at tab_base + b * tab_stride (null: t for all)
+  const float* tab_base;
+  int64_t tab_stride;
+  int has_masks;
+  // output channel of (batch, channel c): oofs + batch * ostride + c * cstride
+  int oofs, ostride, cstride;
 };
+
+// SpecTables of a table array [kx ky kz cx cy cz (mx my mz)] on the device
+__device__ __forceinline__ SpecTables tables_at(const float* tb, int nx, int ny, int nz, int has_masks) {
+  const int nzh = nz / 2 + 1;
+  SpecTables r;
+  r.kx = tb;
+  r.ky = r.kx + nx;
+  r.kz = r.ky + ny;
+  r.cx = r.kz + nzh;
+  r.cy = r.cx + nx;
+  r.cz = r.cy + ny;
+  r.mx = has_masks ? r.cz + nzh : nullptr;
+  r.my = has_masks ? r.mx + nx : nullptr;
+  r.mz = has_masks ? r.my + ny : nullptr;
+  return r;
+}
 
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
   asm volatile(
@@ -334,17 +357,30 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
   const int slots = tiles_mine * NIN;
   if (t == 0)
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
-  for (int i = t; i < L; i += G::T) {
-    stw[i] = a.tw[i];
-    if constexpr (MODE == kYInvYZ || MODE == kYFwdYZ) tab[i] = a.t.cy[i];
-    if constexpr (MODE == kXGreen || MODE == kXGreenAdj || MODE == kXFwdAdjK) {
-      const float kx = a.t.kx[i];
-      tab[i] = kx * kx;                                  // kx^2
-      tab[L + i] = a.t.cx[i];                            // c_x
-      tab[2 * L + i] = a.t.mx != nullptr ? a.t.mx[i] : 1.f;  // particle-Nyquist mask
+  // tables of the current batch (the configuration's for unbatched passes)
+  SpecTables T = a.t;
+  int tab_batch = 0;
+  auto load_tables = [&]() {
+    for (int i = t; i < L; i += G::T) {
+      if constexpr (MODE == kYInvYZ || MODE == kYFwdYZ) tab[i] = T.cy[i];
+      if constexpr (MODE == kXGreen || MODE == kXGreenAdj || MODE == kXFwdAdjK) {
+        const float kx = T.kx[i];
+        tab[i] = kx * kx;                                  // kx^2
+        tab[L + i] = T.cx[i];                              // c_x
+        tab[2 * L + i] = T.mx != nullptr ? T.mx[i] : 1.f;  // particle-Nyquist mask
+      }
     }
+  };
+  if (a.tab_base != nullptr && tiles_mine > 0) {
+    tab_batch = (int)(blockIdx.x / (a.ncolt * a.nouter));
+    T = tables_at(a.tab_base + (int64_t)tab_batch * a.tab_stride, a.nx, a.ny, a.nz, a.has_masks);
   }
+  for (int i = t; i < L; i += G::T) stw[i] = a.tw[i];
+  load_tables();
   __syncthreads();
+  auto out_ch = [&](int batch, int chan) -> int64_t {
+    return (int64_t)(a.oofs + batch * a.ostride + chan * a.cstride) * a.ch;
+  };
 
   // tile -> (column tile, outer, batch)
   auto decode = [&](int tile, int& ct, int& outer, int& batch) {
@@ -429,13 +465,22 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
     const int tile = blockIdx.x + it * gridDim.x;
     int ct, outer, batch;
     decode(tile, ct, outer, batch);
+    if (a.tab_base != nullptr && batch != tab_batch) {
+      // a new batch: its own tables (the previous tile released its stage
+      // with a barrier, so no thread still reads them)
+      __syncthreads();
+      tab_batch = batch;
+      T = tables_at(a.tab_base + (int64_t)batch * a.tab_stride, a.nx, a.ny, a.nz, a.has_masks);
+      load_tables();
+      __syncthreads();
+    }
     const int i0 = it * NIN;
     float2 u[R2];
     if (!acquire(i0)) return;
     if constexpr (MODE == kYFwd || MODE == kYInv || MODE == kXFwd || MODE == kXInv) {
       constexpr bool INV = (MODE == kYInv || MODE == kXInv);
       transform(i0, u, std::integral_constant<bool, INV>{});
-      const int64_t ob = (int64_t)batch * a.ch;
+      const int64_t ob = out_ch(batch, 0);
       if (jb) {
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) {
@@ -454,7 +499,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
         // one forward four-step call site run once per input (code stays small)
         const int kz = ct * KT + c;
         const bool kv = kz_valid(kz, a.nz);
-        const float cz = kv ? a.t.cz[kz] : 0.f;
+        const float cz = kv ? T.cz[kz] : 0.f;
         float2 acc[R2];
 #pragma unroll 1
         for (int ph = 0; ph < 2; ++ph) {
@@ -487,7 +532,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
         // acc = (-i c_y(ky)) y(A_y) + (-i c_z(kz)) y(A_z); rows are ky
         const int kz = ct * KT + c;
         const bool kv = kz_valid(kz, a.nz);
-        const float cz = kv ? a.t.cz[kz] : 0.f;
+        const float cz = kv ? T.cz[kz] : 0.f;
         float2 acc[R2];
         transform(i0, u, std::false_type{});
         if (jb) {
@@ -514,7 +559,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
         float2* buf = smem + (i0 % S) * G::BUF;
         const int kz = ct * KT + c;
         const bool kv = kz_valid(kz, a.nz);
-        const float cz = kv ? a.t.cz[kz] : 0.f;
+        const float cz = kv ? T.cz[kz] : 0.f;
         float2 keep[R1];
 #pragma unroll 1
         for (int ph = 0; ph < 2; ++ph) {
@@ -537,7 +582,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
             const int y = q + R1 * k2;
             const float2 r = conjf2(u[k2]);
             const float2 val = ph == 0 ? (kv ? r : make_float2(0.f, 0.f)) : i_times(cz, r);
-            a.out[ph * a.ch + (int64_t)(y / BY) * a.sb + ((int64_t)outer * BY + y % BY) * a.P + kz] = val;
+            a.out[out_ch(batch, ph) + (int64_t)(y / BY) * a.sb + ((int64_t)outer * BY + y % BY) * a.P + kz] = val;
           }
         }
         release(i0);
@@ -546,7 +591,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
         float2* buf = smem + (i0 % S) * G::BUF;
         const int kz = ct * KT + c;
         const bool kv = kz_valid(kz, a.nz);
-        const float cz = kv ? a.t.cz[kz] : 0.f;
+        const float cz = kv ? T.cz[kz] : 0.f;
         float2 v[R1], vy[R1];
         if (ja) {
   #pragma unroll
@@ -560,7 +605,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
         __syncthreads();
         auto store = [&](int chan, int k2, float2 val) {
           const int y = q + R1 * k2;
-          a.out[chan * a.ch + (int64_t)(y / BY) * a.sb + ((int64_t)outer * BY + y % BY) * a.P + kz] = val;
+          a.out[out_ch(batch, chan) + (int64_t)(y / BY) * a.sb + ((int64_t)outer * BY + y % BY) * a.P + kz] = val;
         };
         if (jb) {
           four_step_b<R1, R2, true>(u, buf, q, c);
@@ -585,8 +630,8 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
       const bool kv = kz_valid(kz, a.nz);
       float kyz2 = 0.f, c0 = 0.f;
       if (kv) {
-        kyz2 = a.t.ky[iy] * a.t.ky[iy] + a.t.kz[kz] * a.t.kz[kz];
-        c0 = -a.g.post_scale * (a.t.mx != nullptr ? a.t.my[iy] * a.t.mz[kz] : 1.f);
+        kyz2 = T.ky[iy] * T.ky[iy] + T.kz[kz] * T.kz[kz];
+        c0 = -a.g.post_scale * (T.mx != nullptr ? T.my[iy] * T.mz[kz] : 1.f);
       }
       // the transfer tables cover kz <= nz/2 only: never read on padding columns
       const bool has_t = kv && (a.g.transfer != nullptr || a.g.radial != nullptr);
@@ -614,7 +659,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
 #pragma unroll
           for (int k2 = 0; k2 < R1; ++k2) {
             const int x = q + R2 * k2;
-            a.out[chan * a.ch + (int64_t)outer * a.sb + (int64_t)x * BY * a.P + j] = val[k2];
+            a.out[out_ch(batch, chan) + (int64_t)outer * a.sb + (int64_t)x * BY * a.P + j] = val[k2];
           }
         }
       };
@@ -630,8 +675,8 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
       const bool kv = kz_valid(kz, a.nz);
       float kyz2 = 0.f, c0 = 0.f;
       if (kv) {
-        kyz2 = a.t.ky[iy] * a.t.ky[iy] + a.t.kz[kz] * a.t.kz[kz];
-        c0 = -a.g.post_scale * (a.t.mx != nullptr ? a.t.my[iy] * a.t.mz[kz] : 1.f);
+        kyz2 = T.ky[iy] * T.ky[iy] + T.kz[kz] * T.kz[kz];
+        c0 = -a.g.post_scale * (T.mx != nullptr ? T.my[iy] * T.mz[kz] : 1.f);
       }
       // the transfer tables cover kz <= nz/2 only: never read on padding columns
       const bool has_t = kv && (a.g.transfer != nullptr || a.g.radial != nullptr);
@@ -678,8 +723,8 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
       const bool kv = kz_valid(kz, a.nz);
       float kyz2 = 0.f, c0 = 0.f;
       if (kv) {
-        kyz2 = a.t.ky[iy] * a.t.ky[iy] + a.t.kz[kz] * a.t.kz[kz];
-        c0 = -a.g.post_scale * (a.t.mx != nullptr ? a.t.my[iy] * a.t.mz[kz] : 1.f);
+        kyz2 = T.ky[iy] * T.ky[iy] + T.kz[kz] * T.kz[kz];
+        c0 = -a.g.post_scale * (T.mx != nullptr ? T.my[iy] * T.mz[kz] : 1.f);
       }
       // the transfer tables cover kz <= nz/2 only: never read on padding columns
       const bool has_t = kv && (a.g.transfer != nullptr || a.g.radial != nullptr);
@@ -1147,6 +1192,12 @@ int pmfft_z(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in
 
 int pmfft_col(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t, GreenParams g,
               cudaStream_t s) {
+  return pmfft_col_batched(m, mode, nbatch, ch_off, in, out, t, g, nullptr, 0, 0, 0, 1, 1, s);
+}
+
+int pmfft_col_batched(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t,
+                      GreenParams g, const float* tab_base, int64_t tab_stride, int has_masks, int oofs, int ostride,
+                      int cstride, cudaStream_t s) {
   if (!pmfft_supported(m) || nbatch < 1 || mode < kYFwd || mode > kXFwdAdjK) {
     set_last_error("pmfft: unsupported mesh or mode");
     return kUnsupported;
@@ -1166,6 +1217,12 @@ int pmfft_col(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float
   a.polls = wait_polls();
   a.t = t;
   a.g = g;
+  a.tab_base = tab_base;
+  a.tab_stride = tab_stride;
+  a.has_masks = has_masks;
+  a.oofs = oofs;
+  a.ostride = ostride;
+  a.cstride = cstride;
   CUtensorMap map;
   int L, st;
   if (is_y(mode)) {
@@ -1244,6 +1301,31 @@ int pmfft_force(Mesh3 m, const float* src, float* force_meshes, float2* work, Sp
   if ((st = pmfft_col(m, kYInv, 1, 0, aq, fp, t, none, s)) != kOk) return st;
   if ((st = pmfft_col(m, kYInvYZ, 1, 1, aq, fp + C, t, none, s)) != kOk) return st;
   return pmfft_z(m, 1, 3, nullptr, fp, force_meshes, nullptr, s);
+}
+
+// The forward chain for `count` equal-shape meshes in one launch per pass
+// (ensembles): sources src[b], force meshes force_meshes[3 b + d], member b's
+// tables at tab_base + b * tab_stride.  work holds 5 * count channels: the z
+// pass and x pass outputs (W of every member, then Q), then the three force
+// spectra of each member in order.
+int pmfft_force_batched(Mesh3 m, int count, const float* src, float* force_meshes, float2* work,
+                        const float* tab_base, int64_t tab_stride, int has_masks, GreenParams g, cudaStream_t s) {
+  const int64_t C = pmfft_channel_elems(m);
+  float2* aq = work;                  // A (count), then W (count) and Q (count)
+  float2* fp = work + 2 * count * C;  // B (count), then F'_x, F'_y, F'_z per member
+  GreenParams none = g;
+  const SpecTables t0 = spec_tables_from(tab_base, m, has_masks);
+  int st = pmfft_z(m, 0, count, src, nullptr, nullptr, aq, s);
+  if (st != kOk) return st;
+  if ((st = pmfft_col_batched(m, kYFwd, count, 0, aq, fp, t0, none, nullptr, 0, 0, 0, 1, 1, s)) != kOk) return st;
+  if ((st = pmfft_col_batched(m, kXGreen, count, 0, fp, aq, t0, g, tab_base, tab_stride, has_masks, 0, 1, count, s)) !=
+      kOk)
+    return st;
+  if ((st = pmfft_col_batched(m, kYInv, count, 0, aq, fp, t0, none, nullptr, 0, 0, 0, 3, 1, s)) != kOk) return st;
+  if ((st = pmfft_col_batched(m, kYInvYZ, count, count, aq, fp, t0, none, tab_base, tab_stride, has_masks, 1, 3, 1,
+                              s)) != kOk)
+    return st;
+  return pmfft_z(m, 1, 3 * count, nullptr, fp, force_meshes, nullptr, s);
 }
 
 // Adjoint spectral chain: three mesh cotangents -> source cotangent.
