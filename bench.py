@@ -113,6 +113,16 @@ MEASURED_TRAFFIC_PER_PARTICLE = {
 STAGE_VARIANTS = {"gather": "gather_kick"}
 
 
+def live_fractions(conf):
+    """(fy, fz): live fractions of ky and kz (nz/2+1 values) of the pass chain
+    pruned to the particle-Nyquist box, or None when the chain is not pruned."""
+    from pmpp_b200._lib import pmfft_active
+    if not conf.has_particle_nyquist_masks or not pmfft_active(*conf.mesh_shape):
+        return None
+    my, mz = conf.particle_nyquist_masks()[1:]
+    return float((my != 0).sum()) / len(my), float((mz != 0).sum()) / len(mz)
+
+
 def load_peaks():
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
     try:
@@ -292,7 +302,8 @@ def run_ours(args):
     per_launch_ms = ours[dom] / counts[dom]
     from pmpp_b200.roofline import algorithmic_bytes
     nx, ny, nz = conf.mesh_shape
-    alg = algorithmic_bytes(dom, N, M, Mc=nx * ny * (nz // 2 + 1), R=nx * ny)
+    live = live_fractions(conf)
+    alg = algorithmic_bytes(dom, N, M, Mc=nx * ny * (nz // 2 + 1), R=nx * ny, live=live)
     traffic_pp = MEASURED_TRAFFIC_PER_PARTICLE.get(dom)
     mix = None
     var = STAGE_VARIANTS.get(dom)
@@ -307,6 +318,16 @@ def run_ours(args):
     counts["other (kick/drift adjoints, LPT, P(k), host)"] = args.steps
     breakdown = {k: {"ms_total": round(v, 3), "launches": counts[k], "share": round(v / (ms * args.steps), 4)}
                  for k, v in sorted(stages.items(), key=lambda kv: -kv[1])}
+    for k, b in breakdown.items():
+        try:  # each stage's fraction of the HBM peak in its algorithmic bytes
+            ab = algorithmic_bytes(k, N, M, Mc=nx * ny * (nz // 2 + 1), R=nx * ny, live=live)
+        except KeyError:
+            continue
+        if k in STAGE_VARIANTS and counts.get(STAGE_VARIANTS[k], 0):
+            nv = counts[STAGE_VARIANTS[k]]
+            ab = (nv * algorithmic_bytes(STAGE_VARIANTS[k], N, M, Mc=nx * ny * (nz // 2 + 1), R=nx * ny)
+                  + (counts[k] - nv) * ab) / counts[k]
+        b["frac"] = round(ab / (b["ms_total"] / b["launches"] * 1e-3) / 1e9 / peak, 3)
     learned = None
     wpath = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pmpp_b200", "data", "learned_green_c3.npy")
     if world == 1 and not args.no_learned and os.path.exists(wpath):

@@ -274,6 +274,18 @@ int pmb_project_density(const float* mesh, int nx, int ny, int nz, int axis, int
  *   those of pmb_green_gradient (tables may be null for modes 0, 1, 4, 5).
  * pmb_set_pmfft(0) routes pmb_force / pmb_force_vjp through cuFFT and the
  * separate multiplier kernels instead (default 1).
+ * pmb_pmfft_z2 / pmb_pmfft_col2: the same passes as one stage of a pruned
+ *   force chain (prune = 1 with particle-Nyquist masks in tables): on a mesh
+ *   finer than the particle grid the masks zero every mode outside
+ *   |ky| <= ny_p/2, kz <= nz_p/2 (and the same in kx), so the forward y
+ *   passes (modes 0, 3) run only the live kz columns and store only the live
+ *   ky rows, the x passes (6, 7) run only live (ky, kz) columns, the inverse
+ *   y passes (1, 2) run only live kz columns and read only live ky rows, and
+ *   the z C2R takes the dead kz columns as zeros (the z R2C is unchanged).
+ *   Every pass of a chain must then be run pruned with the same tables (the
+ *   skipped parts of the intermediate spectra are never written); the results
+ *   equal the unpruned chain's.  pmb_force / pmb_force_vjp run their chains
+ *   pruned whenever has_masks is set.
  * pmb_pmfft_timeouts: bounded copy waits in these passes that gave up.
  * pmb_pmfft_set_col_ctas(0, 1 or 2): resident CTAs per SM of the column
  *   passes, 0 = the default (one); a tuning knob, results are identical. */
@@ -284,6 +296,11 @@ int pmb_pmfft_z(int nx, int ny, int nz, int inverse, int batch, const void* in, 
 int pmb_pmfft_col(int nx, int ny, int nz, int mode, int nbatch, int ch_off, const void* in, void* out,
                   const float* tables, int has_masks, const float* transfer, const float* radial, int radial_len,
                   float post_scale, void* stream);
+int pmb_pmfft_z2(int nx, int ny, int nz, int inverse, int batch, const void* in, void* out, const float* tables,
+                 int has_masks, int prune, void* stream);
+int pmb_pmfft_col2(int nx, int ny, int nz, int mode, int nbatch, int ch_off, const void* in, void* out,
+                   const float* tables, int has_masks, const float* transfer, const float* radial, int radial_len,
+                   float post_scale, int prune, void* stream);
 int pmb_pmfft_timeouts(uint32_t* count);
 int pmb_pmfft_set_col_ctas(int ctas);
 

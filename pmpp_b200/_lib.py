@@ -47,6 +47,9 @@ _SIGS = {
     "pmb_pmfft_z": (c_int, [c_int, c_int, c_int, c_int, c_int, c_p, c_p, c_p]),
     "pmb_pmfft_col": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_int, c_p, c_p, c_int, c_f,
                               c_p]),
+    "pmb_pmfft_z2": (c_int, [c_int, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_int, c_int, c_p]),
+    "pmb_pmfft_col2": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_int, c_p, c_p, c_int, c_f,
+                               c_int, c_p]),
     "pmb_pmfft_timeouts": (c_int, [c_p]),
     "pmb_pmfft_set_col_ctas": (c_int, [c_int]),
     "pmb_rfft3": (c_int, [c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
@@ -197,7 +200,7 @@ _KERNELS = {
     "pmb_force64": 5, "pmb_deposit64": 1, "pmb_axpy64": 1, "pmb_sum64": 1, "pmb_force_vjp64": 4, "pmb_dot64": 1, "pmb_lpt64_ex": 4, "pmb_lpt_vjp64": 6,
     "pmb_scatter_vjp64": 1, "pmb_white_noise_nested64": 1,
     "pmb_linear_modes64": 1, "pmb_lpt64": 4, "pmb_pk_shells64": 1, "pmb_overdensity64": 1,
-    "pmb_pmfft_z": 1, "pmb_pmfft_col": 1,
+    "pmb_pmfft_z": 1, "pmb_pmfft_col": 1, "pmb_pmfft_z2": 1, "pmb_pmfft_col2": 1,
 }
 _pmfft = {"enabled": True}
 _launches = [0]

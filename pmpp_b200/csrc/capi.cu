@@ -431,6 +431,35 @@ int pmb_pmfft_col(int nx, int ny, int nz, int mode, int nbatch, int ch_off, cons
                    make_green(0, transfer, radial, radial_len, post_scale), S(stream));
 }
 
+int pmb_pmfft_z2(int nx, int ny, int nz, int inverse, int batch, const void* in, void* out, const float* tables,
+                 int has_masks, int prune, void* stream) {
+  Mesh3 m{nx, ny, nz};
+  PMB_REQUIRE(pmfft_supported(m), "pmb_pmfft_z2: mesh not supported (powers of two, 64..1024, nz >= 128)");
+  PMB_REQUIRE(batch >= 1, "pmb_pmfft_z2: batch must be positive");
+  PMB_REQUIRE(!prune || (tables != nullptr && has_masks), "pmb_pmfft_z2: pruning needs tables with masks");
+  SpecTables t{};
+  if (prune) t = make_tables(tables, m, 1);
+  if (inverse) return pmfft_z_pruned(m, 1, batch, nullptr, (const float2*)in, (float*)out, nullptr, t, S(stream));
+  return pmfft_z_pruned(m, 0, batch, (const float*)in, nullptr, nullptr, (float2*)out, t, S(stream));
+}
+
+int pmb_pmfft_col2(int nx, int ny, int nz, int mode, int nbatch, int ch_off, const void* in, void* out,
+                   const float* tables, int has_masks, const float* transfer, const float* radial, int radial_len,
+                   float post_scale, int prune, void* stream) {
+  Mesh3 m{nx, ny, nz};
+  PMB_REQUIRE(pmfft_supported(m), "pmb_pmfft_col2: mesh not supported (powers of two, 64..1024, nz >= 128)");
+  PMB_REQUIRE(mode >= 0 && mode <= 8, "pmb_pmfft_col2: mode must be 0..8");
+  PMB_REQUIRE(nbatch >= 1 && ch_off >= 0, "pmb_pmfft_col2: bad batch");
+  PMB_REQUIRE(tables != nullptr || mode == 0 || mode == 1 || mode == 4 || mode == 5,
+              "pmb_pmfft_col2: spectral tables required for the multiplier modes");
+  PMB_REQUIRE(!prune || (tables != nullptr && has_masks), "pmb_pmfft_col2: pruning needs tables with masks");
+  PMB_REQUIRE(!prune || (mode != 4 && mode != 5 && mode != 8), "pmb_pmfft_col2: modes 4, 5, 8 have no pruned form");
+  SpecTables t{};
+  if (tables != nullptr) t = make_tables(tables, m, has_masks);
+  return pmfft_col_pruned(m, mode, nbatch, ch_off, (const float2*)in, (float2*)out, t,
+                          make_green(0, transfer, radial, radial_len, post_scale), prune != 0, S(stream));
+}
+
 int pmb_pmfft_set_col_ctas(int ctas) { return pmfft_set_col_ctas(ctas); }
 
 int pmb_pmfft_timeouts(uint32_t* count) {

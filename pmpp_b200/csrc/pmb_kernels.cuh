@@ -106,6 +106,11 @@ int pmfft_col(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float
 int pmfft_col_batched(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t,
                       GreenParams g, const float* tab_base, int64_t tab_stride, int has_masks, int oofs, int ostride,
                       int cstride, cudaStream_t s);
+// one pass of a pruned force chain (prune_tables with masks; t.mx null: unpruned)
+int pmfft_z_pruned(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in_c, float* out_r, float2* out_c,
+                   SpecTables prune_tables, cudaStream_t s);
+int pmfft_col_pruned(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t,
+                     GreenParams g, bool prune, cudaStream_t s);
 int pmfft_force_batched(Mesh3 m, int count, const float* src, float* force_meshes, float2* work,
                         const float* tab_base, int64_t tab_stride, int has_masks, GreenParams g, cudaStream_t s);
 int pmfft_force(Mesh3 m, const float* src, float* force_meshes, float2* work, SpecTables t, GreenParams g,

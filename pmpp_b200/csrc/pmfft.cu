@@ -280,6 +280,11 @@ struct ColArgs {
   int has_masks;
   // output channel of (batch, channel c): oofs + batch * ostride + c * cstride
   int oofs, ostride, cstride;
+  // live-spectrum pruning inside a force chain (null: none): the masks of
+  // prune_count table arrays at prune_base + b * prune_stride
+  const float* prune_base;
+  int64_t prune_stride;
+  int prune_count;
 };
 
 // SpecTables of a table array [kx ky kz cx cy cz (mx my mz)] on the device
@@ -317,6 +322,77 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
 
 __device__ __forceinline__ bool kz_valid(int kz, int nz) { return kz <= nz / 2; }
 
+// Live part of the spectrum inside a force chain.  The Green multiplier
+// carries the particle-Nyquist masks (core/utils.py:15-37): on a mesh finer
+// than the particle grid they keep ky in [0, ylo) u [ny - yhi, ny) and
+// kz < zl (and the same box in kx), so on a mesh twice as fine 7/8 of the
+// half spectrum is zero after it.  The passes on either side of the
+// multiplier skip that part: the forward y pass runs only the kz < zs
+// columns and stores only live ky rows, the x pass runs only live (ky, kz)
+// columns, the inverse y pass runs only kz < zs and reads only live ky rows,
+// and the z C2R takes kz >= zs as zeros.  Nothing skipped is ever read, and
+// the values it would have carried are exact zeros, so the forward and
+// adjoint results are the full chain's (up to the sign of exact zeros).  The
+// z passes stay whole-row: they are bound by their transform work, and
+// storing or loading only the live columns measured slower at 1024^3.
+struct Live {
+  int ylo, yhi;  // live ky: [0, ylo) u [ny - yhi, ny)
+  int zs;        // kz columns kept: a multiple of KT, at most P
+};
+
+// Live extents of the masks of `count` table arrays (base + b * stride),
+// their union over the arrays; masks of any other shape (or base null) keep
+// the whole spectrum.  Block-wide: every thread calls it, every thread gets
+// the result.
+__device__ Live live_extents(const float* base, int64_t stride, int count, int nx, int ny, int nz) {
+  __shared__ int s_first, s_last, s_fz;
+  const int nzh = nz / 2 + 1, P = nz / 2 + 8;
+  Live L{ny, 0, P};
+  if (base == nullptr) return L;
+  int ylo = 0, yhi = 0, zl = 0;
+  bool bad = false;
+  for (int b = 0; b < count && !bad; ++b) {
+    const SpecTables T = tables_at(base + (int64_t)b * stride, nx, ny, nz, 1);
+    if (threadIdx.x == 0) {
+      s_first = ny;
+      s_last = -1;
+      s_fz = nzh;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < ny; i += blockDim.x)
+      if (T.my[i] == 0.f) {
+        atomicMin(&s_first, i);
+        atomicMax(&s_last, i);
+      }
+    for (int i = threadIdx.x; i < nzh; i += blockDim.x)
+      if (T.mz[i] == 0.f) atomicMin(&s_fz, i);
+    __syncthreads();
+    const int first = s_first, last = s_last, fz = s_fz;
+    // the dead ky must be one run [first, last], the dead kz a tail [fz, nzh)
+    int live_inside = 0;
+    for (int i = first + (int)threadIdx.x; i <= last; i += blockDim.x) live_inside |= T.my[i] != 0.f;
+    for (int i = fz + (int)threadIdx.x; i < nzh; i += blockDim.x) live_inside |= T.mz[i] != 0.f;
+    bad = __syncthreads_or(live_inside) != 0;  // also orders the reads before the next member's reset
+    if (last < 0) {
+      ylo = ny;  // no dead ky
+    } else {
+      ylo = max(ylo, first);
+      yhi = max(yhi, ny - 1 - last);
+    }
+    zl = max(zl, fz);
+  }
+  if (bad) return L;
+  if (ylo + yhi < ny) {
+    L.ylo = ylo;
+    L.yhi = yhi;
+  }
+  const int zs = (zl + KT - 1) / KT * KT;
+  L.zs = zs < P ? zs : P;
+  return L;
+}
+
+__device__ __forceinline__ bool ky_live(const Live& L, int ky, int ny) { return ky < L.ylo || ky >= ny - L.yhi; }
+
 // Green multiplier of the source value at (ix, iy, iz): phi = K(k) S, K =
 // post * mask * T * (-1/k^2), zero at k = 0 (pmb_spectral_device.cuh has the
 // reference citations).  kx2 / mx are the x-axis tables in shared memory; the
@@ -339,7 +415,7 @@ __device__ __forceinline__ float green_scalar(const ColArgs& a, const float* kx2
 
 // Persistent column pass: a ring of S stages, stage slot i holds input q =
 // i % NIN of tile i / NIN of this CTA.
-template <int R1, int R2, int S, int MODE, int CTAS>
+template <int R1, int R2, int S, int MODE, int CTAS, bool PR>
 __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
     col_pass_kernel(const __grid_constant__ CUtensorMap tin, const ColArgs a) {
   using G = ColGeom<R1, R2>;
@@ -353,10 +429,44 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
   uint64_t* bars = reinterpret_cast<uint64_t*>(tab + col_table_floats(MODE, L));
   const int t = threadIdx.x;
   const int c = t % KT;
-  const int tiles_mine = a.ntiles > (int)blockIdx.x ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-  const int slots = tiles_mine * NIN;
   if (t == 0)
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+  // live part of the spectrum (the whole of it outside a pruned chain):
+  // y passes run the column tiles kz < zs; x passes the live (ky, kz tile)
+  // columns; the forward y pass stores live ky rows only and the inverse y
+  // pass loads them only (PIN / POUT)
+  constexpr bool PIN = (MODE == kYInv || MODE == kYInvYZ);
+  constexpr bool POUT = (MODE == kYFwd || MODE == kYFwdYZ);
+  Live lv{a.ny, 0, a.P};
+  if constexpr (PR) lv = live_extents(a.prune_base, a.prune_stride, a.prune_count, a.nx, a.ny, a.nz);
+  const int nkt = lv.zs / KT;          // live kz tiles
+  const int nly = lv.ylo + lv.yhi;     // live ky
+  int ntiles = a.ntiles;
+  if constexpr (PR) ntiles = (YP ? nkt * a.nouter : nly * nkt) * (a.ntiles / (a.ncolt * a.nouter));
+  const int tiles_mine = ntiles > (int)blockIdx.x ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int slots = tiles_mine * NIN;
+  // tile -> (column tile, outer, batch)
+  auto decode = [&](int tile, int& ct, int& outer, int& batch) {
+    if constexpr (!PR) {
+      ct = tile % a.ncolt;
+      const int r = tile / a.ncolt;
+      outer = r % a.nouter;
+      batch = r / a.nouter;
+    } else if constexpr (YP) {
+      ct = tile % nkt;
+      const int r = tile / nkt;
+      outer = r % a.nouter;
+      batch = r / a.nouter;
+    } else {
+      const int kt = tile % nkt;
+      const int r = tile / nkt;
+      const int li = r % nly;
+      batch = r / nly;
+      const int iy = li < lv.ylo ? li : a.ny - nly + li;
+      outer = iy / BY;
+      ct = (iy % BY) * (a.P / KT) + kt;
+    }
+  };
   // tables of the current batch (the configuration's for unbatched passes)
   SpecTables T = a.t;
   int tab_batch = 0;
@@ -372,7 +482,12 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
     }
   };
   if (a.tab_base != nullptr && tiles_mine > 0) {
-    tab_batch = (int)(blockIdx.x / (a.ncolt * a.nouter));
+    if constexpr (PR) {
+      int ct0, outer0;
+      decode((int)blockIdx.x, ct0, outer0, tab_batch);
+    } else {
+      tab_batch = (int)(blockIdx.x / (a.ncolt * a.nouter));
+    }
     T = tables_at(a.tab_base + (int64_t)tab_batch * a.tab_stride, a.nx, a.ny, a.nz, a.has_masks);
   }
   for (int i = t; i < L; i += G::T) stw[i] = a.tw[i];
@@ -381,14 +496,12 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
   auto out_ch = [&](int batch, int chan) -> int64_t {
     return (int64_t)(a.oofs + batch * a.ostride + chan * a.cstride) * a.ch;
   };
+  // y blocks holding live ky rows (the inverse y pass loads only these)
+  auto yblock_live = [&](int b) { return b * BY < lv.ylo || (b + 1) * BY > a.ny - lv.yhi; };
+  int live_blocks = 0;
+  if constexpr (PIN && PR)
+    for (int b = 0; b < a.ny / BY; ++b) live_blocks += yblock_live(b);
 
-  // tile -> (column tile, outer, batch)
-  auto decode = [&](int tile, int& ct, int& outer, int& batch) {
-    ct = tile % a.ncolt;
-    const int r = tile / a.ncolt;
-    outer = r % a.nouter;
-    batch = r / a.nouter;
-  };
   auto issue = [&](int i) {
     if (i >= slots) return;
     const int tile = blockIdx.x + (i / NIN) * gridDim.x;
@@ -397,8 +510,16 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
     const int ch = a.ch_off + batch * NIN + i % NIN;
     const int s = i % S;
     float2* dst = smem + s * G::BUF;
-    mbar_expect_tx(&bars[s], L * KT * 8);
     const int nyb = a.ny / BY;
+    if constexpr (PIN && PR) {
+      // one y block per box (the tensor map of a pruned inverse y pass)
+      mbar_expect_tx(&bars[s], live_blocks * BY * KT * 8);
+#pragma unroll 1
+      for (int b = 0; b < nyb; ++b)
+        if (yblock_live(b)) tma_load_4d(dst + b * BY * KT, &tin, ct * KT, 0, outer, b + ch * nyb, &bars[s]);
+      return;
+    }
+    mbar_expect_tx(&bars[s], L * KT * 8);
 #pragma unroll 1
     for (int r = 0; r < L; r += G::BOX) {
       if (YP)
@@ -431,6 +552,13 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
     }
   };
 
+  // value of row r of this thread's column in a stage; a pruned inverse y
+  // pass reads dead ky rows as zeros (they were never written)
+  auto ld = [&](const float2* buf, int r) -> float2 {
+    if constexpr (PIN && PR)
+      if (!ky_live(lv, r, a.ny)) return make_float2(0.f, 0.f);
+    return buf[r * KT + c];
+  };
   const bool ja = t < R2 * KT;  // first-half jobs (n2 = t / KT)
   const bool jb = t < R1 * KT;  // second-half jobs (k1 = t / KT)
   const int q = t / KT;
@@ -444,7 +572,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
     float2 v[R1];
     if (ja) {
 #pragma unroll
-      for (int n1 = 0; n1 < R1; ++n1) v[n1] = buf[(R2 * n1 + q) * KT + c];
+      for (int n1 = 0; n1 < R1; ++n1) v[n1] = ld(buf, R2 * n1 + q);
     }
     __syncthreads();
     if (ja) four_step_a<R1, R2, INV>(v, buf, q, c, stw);
@@ -485,6 +613,8 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) {
           const int r = q + R1 * k2;
+          if constexpr (POUT && PR)
+            if (!ky_live(lv, r, a.ny)) continue;
           int64_t off;
           if (YP)
             off = ob + (int64_t)(r / BY) * a.sb + ((int64_t)outer * BY + r % BY) * a.P + ct * KT + c;
@@ -523,6 +653,8 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
             for (int k2 = 0; k2 < R2; ++k2) {
               const float2 r = kv ? cadd(acc[k2], i_times(-cz, u[k2])) : make_float2(0.f, 0.f);
               const int ky = q + R1 * k2;
+              if constexpr (PR)
+                if (!ky_live(lv, ky, a.ny)) continue;
               a.out[(int64_t)(ky / BY) * a.sb + ((int64_t)outer * BY + ky % BY) * a.P + kz] = r;
             }
           }
@@ -548,6 +680,8 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
             const float2 z = i_times(-cz, u[k2]);
             const float2 r = kv ? cadd(acc[k2], z) : make_float2(0.f, 0.f);
             const int ky = q + R1 * k2;
+            if constexpr (PR)
+              if (!ky_live(lv, ky, a.ny)) continue;
             a.out[(int64_t)(ky / BY) * a.sb + ((int64_t)outer * BY + ky % BY) * a.P + kz] = r;
           }
         }
@@ -567,7 +701,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
 #pragma unroll
           for (int n1 = 0; n1 < R1; ++n1) {
             if (ph == 0) {
-              keep[n1] = buf[(R2 * n1 + q) * KT + c];
+              keep[n1] = ld(buf, R2 * n1 + q);
               v[n1] = conjf2(i_times(tab[R2 * n1 + q], keep[n1]));
             } else {
               v[n1] = conjf2(keep[n1]);
@@ -596,7 +730,7 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
         if (ja) {
   #pragma unroll
           for (int n1 = 0; n1 < R1; ++n1) {
-            v[n1] = buf[(R2 * n1 + q) * KT + c];
+            v[n1] = ld(buf, R2 * n1 + q);
             vy[n1] = i_times(tab[R2 * n1 + q], v[n1]);
           }
         }
@@ -802,6 +936,11 @@ struct ZArgs {
   uint32_t polls;      // poll limit of the first wait on a stage (pmb_set_wait_limit)
   const float2* tw_m;  // W_M^k, k < M
   const float2* tw_n;  // W_nz^k, k < nz
+  // live-spectrum pruning inside a force chain (ColArgs): the C2R takes the
+  // columns kz >= zs of each row as zeros
+  const float* prune_base;
+  int64_t prune_stride;
+  int prune_count;
 };
 
 // spectral row offset of mesh row (x, y)
@@ -916,7 +1055,7 @@ __global__ void __launch_bounds__(256, 1) z_r2c_kernel(const ZArgs a) {
 }
 
 // Complex-to-real along z: KR rows of P complex -> KR rows of nz reals.
-template <int R1, int R2, int S>
+template <int R1, int R2, int S, bool PR>
 __global__ void __launch_bounds__(256, 1) z_c2r_kernel(const ZArgs a) {
   using G = ZGeom<R1, R2>;
   constexpr int M = G::M, P = G::P;
@@ -930,6 +1069,8 @@ __global__ void __launch_bounds__(256, 1) z_c2r_kernel(const ZArgs a) {
   if (t == 0)
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
   load_z_twiddles<M>(a, tw);
+  int zs = P;
+  if constexpr (PR) zs = live_extents(a.prune_base, a.prune_stride, a.prune_count, a.nx, a.ny, a.nz).zs;
   __syncthreads();
   auto issue = [&](int i) {
     if (i >= tiles_mine) return;
@@ -964,8 +1105,8 @@ __global__ void __launch_bounds__(256, 1) z_c2r_kernel(const ZArgs a) {
 #pragma unroll
       for (int n1 = 0; n1 < R1; ++n1) {
         const int k = R2 * n1 + n2;
-        float2 xk = st[rho * P + k];
-        float2 xm = st[rho * P + M - k];
+        float2 xk = k < zs ? st[rho * P + k] : make_float2(0.f, 0.f);
+        float2 xm = M - k < zs ? st[rho * P + M - k] : make_float2(0.f, 0.f);
         if (k == 0) {
           xk.y = 0.f;
           xm.y = 0.f;
@@ -1074,13 +1215,13 @@ constexpr int stages_for(int buf_bytes, int extra, int ctas) {
 // stages per CTA; 2: 128 registers and one or two stages each; 0: default).
 int g_col_ctas = 0;
 
-template <int R1, int R2, int MODE, int CTAS>
+template <int R1, int R2, int MODE, int CTAS, bool PR>
 int launch_col_ctas(const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
   using G = ColGeom<R1, R2>;
   constexpr int EXTRA = G::L * 8 + col_table_floats(MODE, G::L) * 4;
   constexpr int S = stages_for(G::BUF * 8, EXTRA, CTAS);
   const int smem = S * G::BUF * 8 + EXTRA + S * 8;
-  auto k = col_pass_kernel<R1, R2, S, MODE, CTAS>;
+  auto k = col_pass_kernel<R1, R2, S, MODE, CTAS, PR>;
   PMB_CUDA_CHECK(smem_optin((const void*)k, smem));
   const int grid = persistent_grid(k, G::T, smem, a.ntiles);
   k<<<grid, G::T, smem, s>>>(map, a);
@@ -1092,30 +1233,37 @@ int launch_col_ctas(const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
 // CTAs of 128 registers spill in the fused x passes; with the multiplier's
 // tables in shared memory one CTA is faster (1024^3 on B200: x + multiplier
 // 4.07 against 4.53 ms, adjoint 4.02 against 4.45 ms).
-template <int R1, int R2, int MODE>
+template <int R1, int R2, int MODE, bool PR>
 int launch_col(const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
-  return g_col_ctas == 2 ? launch_col_ctas<R1, R2, MODE, 2>(map, a, s) : launch_col_ctas<R1, R2, MODE, 1>(map, a, s);
+  return g_col_ctas == 2 ? launch_col_ctas<R1, R2, MODE, 2, PR>(map, a, s)
+                         : launch_col_ctas<R1, R2, MODE, 1, PR>(map, a, s);
 }
 
-template <int MODE>
+template <int MODE, bool PR = false>
 int launch_col_len(int L, const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
   switch (L) {
-    case 64: return launch_col<8, 8, MODE>(map, a, s);
-    case 128: return launch_col<16, 8, MODE>(map, a, s);
-    case 256: return launch_col<16, 16, MODE>(map, a, s);
-    case 512: return launch_col<32, 16, MODE>(map, a, s);
-    case 1024: return launch_col<32, 32, MODE>(map, a, s);
+    case 64: return launch_col<8, 8, MODE, PR>(map, a, s);
+    case 128: return launch_col<16, 8, MODE, PR>(map, a, s);
+    case 256: return launch_col<16, 16, MODE, PR>(map, a, s);
+    case 512: return launch_col<32, 16, MODE, PR>(map, a, s);
+    case 1024: return launch_col<32, 32, MODE, PR>(map, a, s);
     default: set_last_error("pmfft: unsupported transform length"); return kUnsupported;
   }
 }
 
-template <int R1, int R2, bool C2R>
+// the pruned instantiation of the modes a force chain runs pruned
+template <int MODE>
+int launch_col_len_pr(bool pr, int L, const CUtensorMap& map, const ColArgs& a, cudaStream_t s) {
+  return pr ? launch_col_len<MODE, true>(L, map, a, s) : launch_col_len<MODE, false>(L, map, a, s);
+}
+
+template <int R1, int R2, bool C2R, bool PR>
 int launch_z(const ZArgs& a, cudaStream_t s) {
   using G = ZGeom<R1, R2>;
   constexpr int stage = C2R ? KR * G::P * 8 : KR * G::M * 8;
   constexpr int S = 2;
   constexpr int smem = S * stage + G::XP * 8 + G::TW * 8 + S * 8;
-  auto k = C2R ? z_c2r_kernel<R1, R2, S> : z_r2c_kernel<R1, R2, S>;
+  auto k = C2R ? z_c2r_kernel<R1, R2, S, PR> : z_r2c_kernel<R1, R2, S>;
   PMB_CUDA_CHECK(smem_optin((const void*)k, smem));
   const int grid = persistent_grid(k, G::T, smem, a.ntiles);
   k<<<grid, G::T, smem, s>>>(a);
@@ -1123,13 +1271,13 @@ int launch_z(const ZArgs& a, cudaStream_t s) {
   return kOk;
 }
 
-template <bool C2R>
+template <bool C2R, bool PR>
 int launch_z_len(int M, const ZArgs& a, cudaStream_t s) {
   switch (M) {
-    case 64: return launch_z<8, 8, C2R>(a, s);
-    case 128: return launch_z<16, 8, C2R>(a, s);
-    case 256: return launch_z<16, 16, C2R>(a, s);
-    case 512: return launch_z<32, 16, C2R>(a, s);
+    case 64: return launch_z<8, 8, C2R, PR>(a, s);
+    case 128: return launch_z<16, 8, C2R, PR>(a, s);
+    case 256: return launch_z<16, 16, C2R, PR>(a, s);
+    case 512: return launch_z<32, 16, C2R, PR>(a, s);
     default: set_last_error("pmfft: unsupported z length"); return kUnsupported;
   }
 }
@@ -1162,8 +1310,35 @@ int pmfft_row_len(Mesh3 m) { return m.nz / 2 + 8; }
 
 int64_t pmfft_channel_elems(Mesh3 m) { return (int64_t)m.nx * m.ny * pmfft_row_len(m); }
 
+namespace {
+
+// Masks that prune a force chain's passes: count table arrays at base +
+// b * stride (base null: no pruning).
+struct PruneSrc {
+  const float* base;
+  int64_t stride;
+  int count;
+};
+
+PruneSrc prune_of(const SpecTables& t) { return PruneSrc{t.mx != nullptr ? t.kx : nullptr, 0, 1}; }
+
+int z_pass(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in_c, float* out_r, float2* out_c,
+           PruneSrc pr, cudaStream_t s);
+int col_pass(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t, GreenParams g,
+             const float* tab_base, int64_t tab_stride, int has_masks, int oofs, int ostride, int cstride, PruneSrc pr,
+             cudaStream_t s);
+
+}  // namespace
+
 int pmfft_z(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in_c, float* out_r, float2* out_c,
             cudaStream_t s) {
+  return z_pass(m, inverse, batch, in_r, in_c, out_r, out_c, PruneSrc{nullptr, 0, 0}, s);
+}
+
+namespace {
+
+int z_pass(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in_c, float* out_r, float2* out_c,
+           PruneSrc pr, cudaStream_t s) {
   if (!pmfft_supported(m) || batch < 1) {
     set_last_error("pmfft: unsupported mesh");
     return kUnsupported;
@@ -1183,21 +1358,22 @@ int pmfft_z(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in
   a.tiles_per_ch = (int)(m.rows() / KR);
   a.ntiles = a.tiles_per_ch * batch;
   a.polls = wait_polls();
+  a.prune_base = pr.base;
+  a.prune_stride = pr.stride;
+  a.prune_count = pr.count;
   int st = twiddle_table(M, &a.tw_m);
   if (st != kOk) return st;
   st = twiddle_table(m.nz, &a.tw_n);
   if (st != kOk) return st;
-  return inverse ? launch_z_len<true>(M, a, s) : launch_z_len<false>(M, a, s);
+  // only the inverse reads a pruned spectrum (the forward pass stores whole
+  // rows: storing the live columns alone measured slower)
+  if (inverse && pr.base != nullptr) return launch_z_len<true, true>(M, a, s);
+  return inverse ? launch_z_len<true, false>(M, a, s) : launch_z_len<false, false>(M, a, s);
 }
 
-int pmfft_col(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t, GreenParams g,
-              cudaStream_t s) {
-  return pmfft_col_batched(m, mode, nbatch, ch_off, in, out, t, g, nullptr, 0, 0, 0, 1, 1, s);
-}
-
-int pmfft_col_batched(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t,
-                      GreenParams g, const float* tab_base, int64_t tab_stride, int has_masks, int oofs, int ostride,
-                      int cstride, cudaStream_t s) {
+int col_pass(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t, GreenParams g,
+             const float* tab_base, int64_t tab_stride, int has_masks, int oofs, int ostride, int cstride, PruneSrc pr,
+             cudaStream_t s) {
   if (!pmfft_supported(m) || nbatch < 1 || mode < kYFwd || mode > kXFwdAdjK) {
     set_last_error("pmfft: unsupported mesh or mode");
     return kUnsupported;
@@ -1223,13 +1399,19 @@ int pmfft_col_batched(Mesh3 m, int mode, int nbatch, int ch_off, const float2* i
   a.oofs = oofs;
   a.ostride = ostride;
   a.cstride = cstride;
+  if (mode == kXFwd || mode == kXInv || mode == kXFwdAdjK) pr = PruneSrc{nullptr, 0, 0};
+  a.prune_base = pr.base;
+  a.prune_stride = pr.stride;
+  a.prune_count = pr.count;
   CUtensorMap map;
   int L, st;
   if (is_y(mode)) {
     L = m.ny;
     a.ncolt = P / KT;
     a.nouter = m.nx;
-    const int box_rows = L < 256 ? L : 256;
+    // a pruned inverse y pass loads live y blocks one box each
+    const bool pin = pr.base != nullptr && (mode == kYInv || mode == kYInvYZ);
+    const int box_rows = pin ? BY : (L < 256 ? L : 256);
     cuuint64_t dims[4] = {(cuuint64_t)P, (cuuint64_t)BY, (cuuint64_t)m.nx, (cuuint64_t)nyb * nch};
     cuuint64_t strides[3] = {(cuuint64_t)P * 8, (cuuint64_t)BY * P * 8, (cuuint64_t)a.sb * 8};
     cuuint32_t box[4] = {(cuuint32_t)KT, (cuuint32_t)BY, 1, (cuuint32_t)(box_rows / BY)};
@@ -1253,17 +1435,43 @@ int pmfft_col_batched(Mesh3 m, int mode, int nbatch, int ch_off, const float2* i
   a.ntiles = (int)ntiles;
   st = twiddle_table(L, &a.tw);
   if (st != kOk) return st;
+  const bool pr_on = pr.base != nullptr;
   switch (mode) {
-    case kYFwd: return launch_col_len<kYFwd>(L, map, a, s);
-    case kYInv: return launch_col_len<kYInv>(L, map, a, s);
-    case kYInvYZ: return launch_col_len<kYInvYZ>(L, map, a, s);
-    case kYFwdYZ: return launch_col_len<kYFwdYZ>(L, map, a, s);
+    case kYFwd: return launch_col_len_pr<kYFwd>(pr_on, L, map, a, s);
+    case kYInv: return launch_col_len_pr<kYInv>(pr_on, L, map, a, s);
+    case kYInvYZ: return launch_col_len_pr<kYInvYZ>(pr_on, L, map, a, s);
+    case kYFwdYZ: return launch_col_len_pr<kYFwdYZ>(pr_on, L, map, a, s);
     case kXFwd: return launch_col_len<kXFwd>(L, map, a, s);
     case kXInv: return launch_col_len<kXInv>(L, map, a, s);
-    case kXGreen: return launch_col_len<kXGreen>(L, map, a, s);
-    case kXGreenAdj: return launch_col_len<kXGreenAdj>(L, map, a, s);
+    case kXGreen: return launch_col_len_pr<kXGreen>(pr_on, L, map, a, s);
+    case kXGreenAdj: return launch_col_len_pr<kXGreenAdj>(pr_on, L, map, a, s);
     default: return launch_col_len<kXFwdAdjK>(L, map, a, s);
   }
+}
+
+}  // namespace
+
+int pmfft_col(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t, GreenParams g,
+              cudaStream_t s) {
+  return col_pass(m, mode, nbatch, ch_off, in, out, t, g, nullptr, 0, 0, 0, 1, 1, PruneSrc{nullptr, 0, 0}, s);
+}
+
+int pmfft_col_batched(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t,
+                      GreenParams g, const float* tab_base, int64_t tab_stride, int has_masks, int oofs, int ostride,
+                      int cstride, cudaStream_t s) {
+  return col_pass(m, mode, nbatch, ch_off, in, out, t, g, tab_base, tab_stride, has_masks, oofs, ostride, cstride,
+                  PruneSrc{nullptr, 0, 0}, s);
+}
+
+int pmfft_z_pruned(Mesh3 m, int inverse, int batch, const float* in_r, const float2* in_c, float* out_r, float2* out_c,
+                   SpecTables prune_tables, cudaStream_t s) {
+  return z_pass(m, inverse, batch, in_r, in_c, out_r, out_c, prune_of(prune_tables), s);
+}
+
+int pmfft_col_pruned(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2* out, SpecTables t,
+                     GreenParams g, bool prune, cudaStream_t s) {
+  return col_pass(m, mode, nbatch, ch_off, in, out, t, g, nullptr, 0, 0, 0, 1, 1,
+                  prune ? prune_of(t) : PruneSrc{nullptr, 0, 0}, s);
 }
 
 int pmfft_set_col_ctas(int ctas) {
@@ -1294,13 +1502,14 @@ int pmfft_force(Mesh3 m, const float* src, float* force_meshes, float2* work, Sp
   float2* aq = work;       // A, then W (channel 0) and Q (channel 1)
   float2* fp = work + 2 * C;  // B (channel 0), then F'_x, F'_y, F'_z
   GreenParams none = g;
-  int st = pmfft_z(m, 0, 1, src, nullptr, nullptr, aq, s);
+  const PruneSrc pr = prune_of(t);
+  int st = z_pass(m, 0, 1, src, nullptr, nullptr, aq, pr, s);
   if (st != kOk) return st;
-  if ((st = pmfft_col(m, kYFwd, 1, 0, aq, fp, t, none, s)) != kOk) return st;
-  if ((st = pmfft_col(m, kXGreen, 1, 0, fp, aq, t, g, s)) != kOk) return st;
-  if ((st = pmfft_col(m, kYInv, 1, 0, aq, fp, t, none, s)) != kOk) return st;
-  if ((st = pmfft_col(m, kYInvYZ, 1, 1, aq, fp + C, t, none, s)) != kOk) return st;
-  return pmfft_z(m, 1, 3, nullptr, fp, force_meshes, nullptr, s);
+  if ((st = col_pass(m, kYFwd, 1, 0, aq, fp, t, none, nullptr, 0, 0, 0, 1, 1, pr, s)) != kOk) return st;
+  if ((st = col_pass(m, kXGreen, 1, 0, fp, aq, t, g, nullptr, 0, 0, 0, 1, 1, pr, s)) != kOk) return st;
+  if ((st = col_pass(m, kYInv, 1, 0, aq, fp, t, none, nullptr, 0, 0, 0, 1, 1, pr, s)) != kOk) return st;
+  if ((st = col_pass(m, kYInvYZ, 1, 1, aq, fp + C, t, none, nullptr, 0, 0, 0, 1, 1, pr, s)) != kOk) return st;
+  return z_pass(m, 1, 3, nullptr, fp, force_meshes, nullptr, pr, s);
 }
 
 // The forward chain for `count` equal-shape meshes in one launch per pass
@@ -1315,17 +1524,17 @@ int pmfft_force_batched(Mesh3 m, int count, const float* src, float* force_meshe
   float2* fp = work + 2 * count * C;  // B (count), then F'_x, F'_y, F'_z per member
   GreenParams none = g;
   const SpecTables t0 = spec_tables_from(tab_base, m, has_masks);
-  int st = pmfft_z(m, 0, count, src, nullptr, nullptr, aq, s);
+  const PruneSrc pr{has_masks ? tab_base : nullptr, tab_stride, count};
+  int st = z_pass(m, 0, count, src, nullptr, nullptr, aq, pr, s);
   if (st != kOk) return st;
-  if ((st = pmfft_col_batched(m, kYFwd, count, 0, aq, fp, t0, none, nullptr, 0, 0, 0, 1, 1, s)) != kOk) return st;
-  if ((st = pmfft_col_batched(m, kXGreen, count, 0, fp, aq, t0, g, tab_base, tab_stride, has_masks, 0, 1, count, s)) !=
+  if ((st = col_pass(m, kYFwd, count, 0, aq, fp, t0, none, nullptr, 0, 0, 0, 1, 1, pr, s)) != kOk) return st;
+  if ((st = col_pass(m, kXGreen, count, 0, fp, aq, t0, g, tab_base, tab_stride, has_masks, 0, 1, count, pr, s)) != kOk)
+    return st;
+  if ((st = col_pass(m, kYInv, count, 0, aq, fp, t0, none, nullptr, 0, 0, 0, 3, 1, pr, s)) != kOk) return st;
+  if ((st = col_pass(m, kYInvYZ, count, count, aq, fp, t0, none, tab_base, tab_stride, has_masks, 1, 3, 1, pr, s)) !=
       kOk)
     return st;
-  if ((st = pmfft_col_batched(m, kYInv, count, 0, aq, fp, t0, none, nullptr, 0, 0, 0, 3, 1, s)) != kOk) return st;
-  if ((st = pmfft_col_batched(m, kYInvYZ, count, count, aq, fp, t0, none, tab_base, tab_stride, has_masks, 1, 3, 1,
-                              s)) != kOk)
-    return st;
-  return pmfft_z(m, 1, 3 * count, nullptr, fp, force_meshes, nullptr, s);
+  return z_pass(m, 1, 3 * count, nullptr, fp, force_meshes, nullptr, pr, s);
 }
 
 // Adjoint spectral chain: three mesh cotangents -> source cotangent.
@@ -1334,15 +1543,16 @@ int pmfft_force_adjoint(Mesh3 m, const float* mesh_cot, float* src_cot, float2* 
   const int64_t C = pmfft_channel_elems(m);
   float2* a3 = work;          // A_x, A_y, A_z; then S' (0) and S'' (1)
   float2* bb = work + 3 * C;  // B_x, b
-  int st = pmfft_z(m, 0, 3, mesh_cot, nullptr, nullptr, a3, s);
+  const PruneSrc pr = prune_of(t);
+  int st = z_pass(m, 0, 3, mesh_cot, nullptr, nullptr, a3, pr, s);
   if (st != kOk) return st;
-  if ((st = pmfft_col(m, kYFwd, 1, 0, a3, bb, t, g, s)) != kOk) return st;
-  if ((st = pmfft_col(m, kYFwdYZ, 1, 1, a3, bb + C, t, g, s)) != kOk) return st;
+  if ((st = col_pass(m, kYFwd, 1, 0, a3, bb, t, g, nullptr, 0, 0, 0, 1, 1, pr, s)) != kOk) return st;
+  if ((st = col_pass(m, kYFwdYZ, 1, 1, a3, bb + C, t, g, nullptr, 0, 0, 0, 1, 1, pr, s)) != kOk) return st;
   // fused x pass (4.45 ms at 1024^3) rather than the multiplier pass plus a
   // plain inverse x pass (3.45 + 1.49 ms)
-  if ((st = pmfft_col(m, kXGreenAdj, 1, 0, bb, a3, t, g, s)) != kOk) return st;
-  if ((st = pmfft_col(m, kYInv, 1, 0, a3, a3 + C, t, g, s)) != kOk) return st;
-  return pmfft_z(m, 1, 1, nullptr, a3 + C, src_cot, nullptr, s);
+  if ((st = col_pass(m, kXGreenAdj, 1, 0, bb, a3, t, g, nullptr, 0, 0, 0, 1, 1, pr, s)) != kOk) return st;
+  if ((st = col_pass(m, kYInv, 1, 0, a3, a3 + C, t, g, nullptr, 0, 0, 0, 1, 1, pr, s)) != kOk) return st;
+  return z_pass(m, 1, 1, nullptr, a3 + C, src_cot, nullptr, pr, s);
 }
 
 }  // namespace pmb

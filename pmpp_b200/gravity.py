@@ -360,18 +360,20 @@ def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F
         C8 = 8 * lib().pmb_pmfft_channel_elems(nx, ny, nz)
         pm = workspace(5 * C8, dev, "st_pm5")
         aq, fp = pm.data_ptr(), pm.data_ptr() + 2 * C8
-        call("pmb_pmfft_z", nx, ny, nz, 0, 1, real3.data_ptr(), aq, s)
+        # (pruned to the live spectrum when the particle-Nyquist masks apply)
+        tp = tables.data_ptr()
+        call("pmb_pmfft_z2", nx, ny, nz, 0, 1, real3.data_ptr(), aq, tp, masks, masks, s)
         t = timer.mark("fft_z_r2c", t)
-        call("pmb_pmfft_col", nx, ny, nz, 0, 1, 0, aq, fp, tables.data_ptr(), masks, None, None, 0, 1.0, s)
+        call("pmb_pmfft_col2", nx, ny, nz, 0, 1, 0, aq, fp, tp, masks, None, None, 0, 1.0, masks, s)
         t = timer.mark("fft_y", t)
-        call("pmb_pmfft_col", nx, ny, nz, 6, 1, 0, fp, aq, tables.data_ptr(), masks, ptr(transfer), ptr(radial), rl,
-             float(1.0 / conf.mesh_size), s)
+        call("pmb_pmfft_col2", nx, ny, nz, 6, 1, 0, fp, aq, tp, masks, ptr(transfer), ptr(radial), rl,
+             float(1.0 / conf.mesh_size), masks, s)
         t = timer.mark("fft_x_green", t)
-        call("pmb_pmfft_col", nx, ny, nz, 1, 1, 0, aq, fp, tables.data_ptr(), masks, None, None, 0, 1.0, s)
+        call("pmb_pmfft_col2", nx, ny, nz, 1, 1, 0, aq, fp, tp, masks, None, None, 0, 1.0, masks, s)
         t = timer.mark("fft_y_inv", t)
-        call("pmb_pmfft_col", nx, ny, nz, 2, 1, 1, aq, fp + C8, tables.data_ptr(), masks, None, None, 0, 1.0, s)
+        call("pmb_pmfft_col2", nx, ny, nz, 2, 1, 1, aq, fp + C8, tp, masks, None, None, 0, 1.0, masks, s)
         t = timer.mark("fft_y_inv_yz", t)
-        call("pmb_pmfft_z", nx, ny, nz, 1, 3, fp, F.data_ptr(), s)
+        call("pmb_pmfft_z2", nx, ny, nz, 1, 3, fp, F.data_ptr(), tp, masks, masks, s)
         t = timer.mark("fft_z_c2r3", t)
     else:
         spec3, spec1, work = _cufft_buffers(conf, dev)
@@ -424,18 +426,18 @@ def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, r
         C8 = 8 * lib().pmb_pmfft_channel_elems(nx, ny, nz)
         pm = workspace(5 * C8, dev, "st_pm5" + work_lane)
         a3, bb = pm.data_ptr(), pm.data_ptr() + 3 * C8
-        call("pmb_pmfft_z", nx, ny, nz, 0, 3, real3.data_ptr(), a3, s)
+        tp = tables.data_ptr()
+        call("pmb_pmfft_z2", nx, ny, nz, 0, 3, real3.data_ptr(), a3, tp, masks, masks, s)
         t = timer.mark("fft_z_r2c3", t)
-        call("pmb_pmfft_col", nx, ny, nz, 0, 1, 0, a3, bb, tables.data_ptr(), masks, None, None, 0, 1.0, s)
+        call("pmb_pmfft_col2", nx, ny, nz, 0, 1, 0, a3, bb, tp, masks, None, None, 0, 1.0, masks, s)
         t = timer.mark("fft_y", t)
-        call("pmb_pmfft_col", nx, ny, nz, 3, 1, 1, a3, bb + C8, tables.data_ptr(), masks, None, None, 0, 1.0, s)
+        call("pmb_pmfft_col2", nx, ny, nz, 3, 1, 1, a3, bb + C8, tp, masks, None, None, 0, 1.0, masks, s)
         t = timer.mark("fft_y_yz", t)
-        call("pmb_pmfft_col", nx, ny, nz, 7, 1, 0, bb, a3, tables.data_ptr(), masks, ptr(transfer), ptr(radial), rl,
-             post, s)
+        call("pmb_pmfft_col2", nx, ny, nz, 7, 1, 0, bb, a3, tp, masks, ptr(transfer), ptr(radial), rl, post, masks, s)
         t = timer.mark("fft_x_green_adj", t)
-        call("pmb_pmfft_col", nx, ny, nz, 1, 1, 0, a3, a3 + C8, tables.data_ptr(), masks, None, None, 0, 1.0, s)
+        call("pmb_pmfft_col2", nx, ny, nz, 1, 1, 0, a3, a3 + C8, tp, masks, None, None, 0, 1.0, masks, s)
         t = timer.mark("fft_y_inv", t)
-        call("pmb_pmfft_z", nx, ny, nz, 1, 1, a3 + C8, real3.data_ptr(), s)
+        call("pmb_pmfft_z2", nx, ny, nz, 1, 1, a3 + C8, real3.data_ptr(), tp, masks, masks, s)
         t = timer.mark("fft_z_c2r", t)
     else:
         spec3, spec1, work = _cufft_buffers(conf, dev)

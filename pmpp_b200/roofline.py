@@ -8,14 +8,38 @@ layout (pmid int16 x 3 + disp float32 x 3 = 18 B per particle); re-reads,
 halo redundancy, the pass chain's zero padding and cuFFT's extra passes are not
 counted, so a stage's
 achieved GB/s is directly comparable with the HBM copy bandwidth.
+
+live = (fy, fz): the pass chain pruned to the particle-Nyquist box (pmfft.cu,
+on meshes finer than the particle grid), fy the live fraction of ky and fz of
+kz (Mz/2+1 values).  Its passes then need only the live part: the forward y
+passes read fz of the spectrum and write fz*fy, the x passes read and write
+fy*fz, the inverse y passes read fz*fy and write fz, and the z passes need
+only the live fz of each spectral row (the kernels move whole rows, which
+measured faster; that surplus is not counted).
 """
 from __future__ import annotations
 
 
-def algorithmic_bytes(op, N, M, Mc=None, R=None, T=None):
+def algorithmic_bytes(op, N, M, Mc=None, R=None, T=None, live=None):
     Mc = M // 2 if Mc is None else Mc
     R = round(M ** (2 / 3)) if R is None else R
     T = min(M, 8 * N) if T is None else min(T, M)
+    if live is not None:
+        fy, fz = live
+        pruned = {
+            "fft_z_r2c": 4 * M + 8 * Mc * fz,
+            "fft_z_r2c3": 3 * (4 * M + 8 * Mc * fz),
+            "fft_y": 8 * Mc * fz * (1 + fy),
+            "fft_y_yz": 8 * Mc * fz * (2 + fy),
+            "fft_y_inv": 8 * Mc * fz * (fy + 1),
+            "fft_y_inv_yz": 8 * Mc * fz * (fy + 2),
+            "fft_x_green": 24 * Mc * fy * fz,
+            "fft_x_green_adj": 24 * Mc * fy * fz,
+            "fft_z_c2r": 8 * Mc * fz + 4 * M,
+            "fft_z_c2r3": 3 * (8 * Mc * fz + 4 * M),
+        }
+        if op in pruned:
+            return pruned[op]
     table = {
         # row sort: pmid+disp in, 16 B records + 4 B permutation out, row offsets
         "sort": 18 * N + 20 * N + 8 * R,

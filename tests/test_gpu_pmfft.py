@@ -197,3 +197,60 @@ def test_split_adjoint_x_pass_matches_fused():
     f = torch.view_as_real(fused).cpu().numpy()
     g = torch.view_as_real(split).cpu().numpy()
     assert rel_err(g, f) < 1e-5
+
+
+def _chain(L, nx, ny, nz, src, tab, masks, prune, s):
+    """Forward force chain through the per-pass entry points (pmfft_force's
+    order) and the adjoint chain (pmfft_force_adjoint's) on the force meshes."""
+    C = L.lib().pmb_pmfft_channel_elems(nx, ny, nz)
+    pm = torch.full((5 * C,), float("nan"), dtype=torch.complex64, device="cuda")  # garbage where never written
+    aq, fp = pm.data_ptr(), pm.data_ptr() + 16 * C
+    F = torch.empty((3, nx, ny, nz), dtype=torch.float32, device="cuda")
+    L.call("pmb_pmfft_z2", nx, ny, nz, 0, 1, src.data_ptr(), aq, tab, masks, prune, s)
+    L.call("pmb_pmfft_col2", nx, ny, nz, 0, 1, 0, aq, fp, tab, masks, None, None, 0, 1.0, prune, s)
+    L.call("pmb_pmfft_col2", nx, ny, nz, 6, 1, 0, fp, aq, tab, masks, None, None, 0, 0.7, prune, s)
+    L.call("pmb_pmfft_col2", nx, ny, nz, 1, 1, 0, aq, fp, tab, masks, None, None, 0, 1.0, prune, s)
+    L.call("pmb_pmfft_col2", nx, ny, nz, 2, 1, 1, aq, fp + 8 * C, tab, masks, None, None, 0, 1.0, prune, s)
+    L.call("pmb_pmfft_z2", nx, ny, nz, 1, 3, fp, F.data_ptr(), tab, masks, prune, s)
+    pm.fill_(float("nan"))
+    a3, bb = pm.data_ptr(), pm.data_ptr() + 24 * C
+    out = torch.empty((nx, ny, nz), dtype=torch.float32, device="cuda")
+    L.call("pmb_pmfft_z2", nx, ny, nz, 0, 3, F.data_ptr(), a3, tab, masks, prune, s)
+    L.call("pmb_pmfft_col2", nx, ny, nz, 0, 1, 0, a3, bb, tab, masks, None, None, 0, 1.0, prune, s)
+    L.call("pmb_pmfft_col2", nx, ny, nz, 3, 1, 1, a3, bb + 8 * C, tab, masks, None, None, 0, 1.0, prune, s)
+    L.call("pmb_pmfft_col2", nx, ny, nz, 7, 1, 0, bb, a3, tab, masks, None, None, 0, 0.7, prune, s)
+    L.call("pmb_pmfft_col2", nx, ny, nz, 1, 1, 0, a3, a3 + 8 * C, tab, masks, None, None, 0, 1.0, prune, s)
+    L.call("pmb_pmfft_z2", nx, ny, nz, 1, 1, a3 + 8 * C, out.data_ptr(), tab, masks, prune, s)
+    return F, out
+
+
+@pytest.mark.parametrize("ptcl,mesh", [((32, 64, 64), 2), ((32, 32, 32), 4), ((64, 32, 128), 2)])
+def test_pruned_chain_equals_full_chain(ptcl, mesh):
+    """The chain pruned to the particle-Nyquist box (intermediate buffers
+    filled with NaN, so a read of a skipped part would show) gives the full
+    chain's force meshes and adjoint bit for bit, and both match numpy."""
+    pb, co, conf = _confs(ptcl, mesh)
+    nx, ny, nz = conf.mesh_shape
+    L = _lib()
+    s = _stream()
+    assert conf.has_particle_nyquist_masks
+    tab = conf.spectral_tables("mesh", torch.device("cuda"), 0).data_ptr()
+    x = np.random.default_rng(8).normal(size=(nx, ny, nz)).astype(np.float32)
+    src = torch.from_numpy(x).cuda()
+    full = _chain(L, nx, ny, nz, src, tab, 1, 0, s)
+    pruned = _chain(L, nx, ny, nz, src, tab, 1, 1, s)
+    for f, p in zip(full, pruned):
+        assert torch.isfinite(p).all()
+        assert torch.equal(f, p)
+    # the live box is what the masks keep: numpy restatement of the forward chain
+    kx, ky, kz = (np.asarray(k, np.float64) for k in co.kvec)
+    m = opm.nyquist_filter(co).astype(np.float64)
+    k2 = kx[:, None, None] ** 2 + ky[None, :, None] ** 2 + kz[None, None, :] ** 2
+    with np.errstate(divide="ignore"):
+        K = np.where(k2 > 0, -0.7 * m / k2, 0.0)
+    phi = K * np.fft.rfftn(x.astype(np.float64))
+    cs = [np.asarray(c, np.float64) for c in co.neg_ik]
+    ref = np.stack([np.fft.irfftn(1j * c * phi, s=(nx, ny, nz)) * nx * ny * nz for c in
+                    (cs[0][:, None, None], cs[1][None, :, None], cs[2][None, None, :])])
+    assert rel_err(full[0].cpu().numpy(), ref) < 1e-5
+    assert _lib().pmfft_timeouts() == 0
