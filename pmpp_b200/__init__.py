@@ -18,7 +18,8 @@ from .gravity import gravity, gravity_vjp, gravity_streamed
 from .nbody import (nbody, nbody_adj, integrate, kick, drift, NBodyRun, kick_adj, drift_adj_from_output,
                     force_adj, integrate_adj, nbody_low_memory, nbody_scheduled, nbody_static_halo_scheduled,
                     nbody_init, nbody_step, nbody_collect, nbody_observe)
-from . import observers, checkpoint, corrections, meshcnn
+from . import observers, checkpoint, corrections, meshcnn, slab
+from .slab import SlabPM, LocalComm, ProcessGroupComm
 from .observers import density_projection_observer, nbody_kappa
 from .checkpoint import save_state, load_state
 
@@ -28,7 +29,7 @@ __all__ = [
     "drift", "NBodyRun", "kick_adj", "drift_adj_from_output", "force_adj", "integrate_adj", "gravity_streamed",
     "nbody_low_memory", "nbody_scheduled", "nbody_static_halo_scheduled", "nbody_init", "nbody_step",
     "nbody_collect", "nbody_observe", "observers", "checkpoint", "density_projection_observer", "nbody_kappa",
-    "save_state", "load_state", "corrections", "meshcnn"
+    "save_state", "load_state", "corrections", "meshcnn", "slab", "SlabPM", "LocalComm", "ProcessGroupComm"
 ]
 from . import modes, lpt, power_spectrum, pipeline  # noqa: E402
 from .modes import white_noise_nested, linear_modes  # noqa: E402
