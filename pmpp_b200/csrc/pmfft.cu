@@ -496,11 +496,12 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
   auto out_ch = [&](int batch, int chan) -> int64_t {
     return (int64_t)(a.oofs + batch * a.ostride + chan * a.cstride) * a.ch;
   };
-  // y blocks holding live ky rows (the inverse y pass loads only these)
-  auto yblock_live = [&](int b) { return b * BY < lv.ylo || (b + 1) * BY > a.ny - lv.yhi; };
-  int live_blocks = 0;
+  // TMA boxes (G::BOX rows) holding live ky rows: the pruned inverse y pass
+  // loads only these (fewer, larger copies measured faster than one per y block)
+  auto box_live = [&](int r0) { return r0 < lv.ylo || r0 + G::BOX > a.ny - lv.yhi; };
+  int live_boxes = 0;
   if constexpr (PIN && PR)
-    for (int b = 0; b < a.ny / BY; ++b) live_blocks += yblock_live(b);
+    for (int r0 = 0; r0 < L; r0 += G::BOX) live_boxes += box_live(r0);
 
   auto issue = [&](int i) {
     if (i >= slots) return;
@@ -511,17 +512,11 @@ __global__ void __launch_bounds__(ColGeom<R1, R2>::T, CTAS)
     const int s = i % S;
     float2* dst = smem + s * G::BUF;
     const int nyb = a.ny / BY;
-    if constexpr (PIN && PR) {
-      // one y block per box (the tensor map of a pruned inverse y pass)
-      mbar_expect_tx(&bars[s], live_blocks * BY * KT * 8);
-#pragma unroll 1
-      for (int b = 0; b < nyb; ++b)
-        if (yblock_live(b)) tma_load_4d(dst + b * BY * KT, &tin, ct * KT, 0, outer, b + ch * nyb, &bars[s]);
-      return;
-    }
-    mbar_expect_tx(&bars[s], L * KT * 8);
+    mbar_expect_tx(&bars[s], ((PIN && PR) ? live_boxes * G::BOX : L) * KT * 8);
 #pragma unroll 1
     for (int r = 0; r < L; r += G::BOX) {
+      if constexpr (PIN && PR)
+        if (!box_live(r)) continue;
       if (YP)
         tma_load_4d(dst + r * KT, &tin, ct * KT, r % BY, outer, r / BY + ch * nyb, &bars[s]);
       else
@@ -1409,9 +1404,7 @@ int col_pass(Mesh3 m, int mode, int nbatch, int ch_off, const float2* in, float2
     L = m.ny;
     a.ncolt = P / KT;
     a.nouter = m.nx;
-    // a pruned inverse y pass loads live y blocks one box each
-    const bool pin = pr.base != nullptr && (mode == kYInv || mode == kYInvYZ);
-    const int box_rows = pin ? BY : (L < 256 ? L : 256);
+    const int box_rows = L < 256 ? L : 256;
     cuuint64_t dims[4] = {(cuuint64_t)P, (cuuint64_t)BY, (cuuint64_t)m.nx, (cuuint64_t)nyb * nch};
     cuuint64_t strides[3] = {(cuuint64_t)P * 8, (cuuint64_t)BY * P * 8, (cuuint64_t)a.sb * 8};
     cuuint32_t box[4] = {(cuuint32_t)KT, (cuuint32_t)BY, 1, (cuuint32_t)(box_rows / BY)};

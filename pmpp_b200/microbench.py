@@ -182,12 +182,33 @@ def pmfft_stages(conf, reps, peak, only=None):
         "fft_z_c2r": lambda: call("pmb_pmfft_z", nx, ny, nz, 1, 1, a, real3b.data_ptr(), s),
         "fft_z_c2r3": lambda: call("pmb_pmfft_z", nx, ny, nz, 1, 3, a, real3b.data_ptr(), s),
     }
+    # the same passes as stages of a force chain pruned to the particle-Nyquist
+    # box (what pmb_force runs when the mesh is finer than the particle grid)
+    live = None
+    if masks:
+        my, mz = conf.particle_nyquist_masks()[1:]
+        live = (float((my != 0).sum()) / len(my), float((mz != 0).sum()) / len(mz))
+        col2 = lambda mode, ch_off, i, o, post=1.0: call("pmb_pmfft_col2", nx, ny, nz, mode, 1, ch_off, i, o, tables,
+                                                         masks, None, None, 0, post, 1, s)
+        stages.update({
+            "fft_y_pruned": lambda: col2(0, 0, a, b),
+            "fft_y_yz_pruned": lambda: col2(3, 1, a, b),
+            "fft_x_green_pruned": lambda: col2(6, 0, a, b, inv_m),
+            "fft_x_green_adj_pruned": lambda: col2(7, 0, a, b, inv_m),
+            "fft_y_inv_pruned": lambda: col2(1, 0, a, b),
+            "fft_y_inv_yz_pruned": lambda: col2(2, 0, a, b),
+            "fft_z_c2r_pruned": lambda: call("pmb_pmfft_z2", nx, ny, nz, 1, 1, a, real3b.data_ptr(), tables, masks, 1,
+                                             s),
+            "fft_z_c2r3_pruned": lambda: call("pmb_pmfft_z2", nx, ny, nz, 1, 3, a, real3b.data_ptr(), tables, masks,
+                                              1, s),
+        })
     out = {}
     for name, fn in stages.items():
-        if only and name not in only:
+        if only and name.replace("_pruned", "") not in only:
             continue
         ms = _time(fn, reps)
-        alg = algorithmic_bytes(name, 0, M, Mc=Mc, R=nx * ny)
+        base = name.replace("_pruned", "")
+        alg = algorithmic_bytes(base, 0, M, Mc=Mc, R=nx * ny, live=live if name.endswith("_pruned") else None)
         gbs = alg / (ms * 1e-3) / 1e9
         out[name] = {"ms": round(ms, 4), "algorithmic_bytes": alg, "GB/s": round(gbs, 1), "frac_hbm": round(gbs / peak, 4)}
     return out
