@@ -104,13 +104,30 @@ MEASURED_TRAFFIC_PER_PARTICLE = {
     "scatter3": (0.472 + 1.556) * 1e9 / 256**3,
     "scatter": (0.270 + 0.484) * 1e9 / 256**3,
     "scatter_adjoint": (1.075 + 0.189) * 1e9 / 256**3,
+    "fft_z_c2r3": (1.660984 + 1.565085) * 1e9 / 256**3,  # z_c2r_kernel, 3 channels, pruned chain
 }
 
 
 # Stages whose launches run in two variants, the second tagged by the stage timer (a gather that also
 # applies the folded kicks reads and writes the velocities): the dominant stage's algorithmic bytes and
 # traffic are the launch-weighted mean of its variants.
-STAGE_VARIANTS = {"gather": "gather_kick"}
+STAGE_VARIANTS = {"gather": ("gather_kick", "gather_kick_only")}
+
+
+def stage_mix(stage, counts, N, M, conf, live):
+    """(algorithmic bytes, measured traffic per particle or None, launch mix) of
+    one launch of a stage, weighted over the launch variants the timer counted."""
+    from pmpp_b200.roofline import algorithmic_bytes
+    nx, ny, nz = conf.mesh_shape
+    ab = lambda op: algorithmic_bytes(op, N, M, Mc=nx * ny * (nz // 2 + 1), R=nx * ny, live=live)
+    nd = counts[stage]
+    parts = {v: counts.get(v, 0) for v in STAGE_VARIANTS.get(stage, ()) if counts.get(v, 0)}
+    parts[stage] = nd - sum(parts.values())
+    alg = sum(n * ab(v) for v, n in parts.items()) / nd
+    traffic = None
+    if all(v in MEASURED_TRAFFIC_PER_PARTICLE for v, n in parts.items() if n):
+        traffic = sum(n * MEASURED_TRAFFIC_PER_PARTICLE[v] for v, n in parts.items() if n) / nd
+    return alg, traffic, (parts if len(parts) > 1 else None)
 
 
 def live_fractions(conf):
@@ -303,16 +320,7 @@ def run_ours(args):
     from pmpp_b200.roofline import algorithmic_bytes
     nx, ny, nz = conf.mesh_shape
     live = live_fractions(conf)
-    alg = algorithmic_bytes(dom, N, M, Mc=nx * ny * (nz // 2 + 1), R=nx * ny, live=live)
-    traffic_pp = MEASURED_TRAFFIC_PER_PARTICLE.get(dom)
-    mix = None
-    var = STAGE_VARIANTS.get(dom)
-    if var is not None and counts.get(var, 0):
-        nv, nd = counts[var], counts[dom]
-        alg = (nv * algorithmic_bytes(var, N, M, Mc=nx * ny * (nz // 2 + 1), R=nx * ny) + (nd - nv) * alg) / nd
-        if traffic_pp is not None and var in MEASURED_TRAFFIC_PER_PARTICLE:
-            traffic_pp = (nv * MEASURED_TRAFFIC_PER_PARTICLE[var] + (nd - nv) * traffic_pp) / nd
-        mix = {var: nv, dom: nd - nv}
+    alg, traffic_pp, mix = stage_mix(dom, counts, N, M, conf, live)
     achieved = alg / (per_launch_ms * 1e-3) / 1e9
     stages["other (kick/drift adjoints, LPT, P(k), host)"] = max(ms * args.steps - sum(stages.values()), 0.0)
     counts["other (kick/drift adjoints, LPT, P(k), host)"] = args.steps
@@ -320,13 +328,9 @@ def run_ours(args):
                  for k, v in sorted(stages.items(), key=lambda kv: -kv[1])}
     for k, b in breakdown.items():
         try:  # each stage's fraction of the HBM peak in its algorithmic bytes
-            ab = algorithmic_bytes(k, N, M, Mc=nx * ny * (nz // 2 + 1), R=nx * ny, live=live)
+            ab = stage_mix(k, counts, N, M, conf, live)[0]
         except KeyError:
             continue
-        if k in STAGE_VARIANTS and counts.get(STAGE_VARIANTS[k], 0):
-            nv = counts[STAGE_VARIANTS[k]]
-            ab = (nv * algorithmic_bytes(STAGE_VARIANTS[k], N, M, Mc=nx * ny * (nz // 2 + 1), R=nx * ny)
-                  + (counts[k] - nv) * ab) / counts[k]
         b["frac"] = round(ab / (b["ms_total"] / b["launches"] * 1e-3) / 1e9 / peak, 3)
     learned = None
     wpath = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pmpp_b200", "data", "learned_green_c3.npy")

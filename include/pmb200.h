@@ -103,7 +103,8 @@ int pmb_scatter_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int 
 int pmb_gather_rows(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh, float* out,
                     float* vel, float kick, void* stream);
 /* pmb_gather_rows with a second half-kick vel += out * kick2 after the first
- * (the next step's opening kick, same acceleration; kick2 = 0: none). */
+ * (the next step's opening kick, same acceleration; kick2 = 0: none).  With
+ * vel != NULL, out may be NULL: the kicks only, no gathered values stored. */
 int pmb_gather_rows2(const void* sorted, int64_t n, int nx, int ny, int nz, int C, const float* mesh, float* out,
                      float* vel, float kick, float kick2, void* stream);
 /* Position term of the CIC adjoints (cic/gather.py:495-502,
@@ -318,7 +319,9 @@ int pmb_force(const int16_t* pmid, float* disp, const float* drift_vel, float dr
               const float* transfer, const float* radial, int radial_len, float* force_meshes, float* acc,
               float* vel_kick, float kick, void* workspace, int64_t workspace_bytes, void* stream);
 /* pmb_force with a second fused half-kick vel_kick += acc * kick2 after the
- * first (the next KDK step's opening kick; kick2 = 0: none). */
+ * first (the next KDK step's opening kick; kick2 = 0: none).  With vel_kick
+ * != NULL, acc may be NULL: the kicks are applied and no acceleration is
+ * stored (a run whose next force overwrites it anyway). */
 int pmb_force2(const int16_t* pmid, float* disp, const float* drift_vel, float drift, int64_t n, int nx, int ny, int nz,
                float cell, float val_const, float src_mul, const float* tables, int has_masks, int green_kernel,
                const float* transfer, const float* radial, int radial_len, float* force_meshes, float* acc,

@@ -182,6 +182,7 @@ int pmb_gather_rows2(const void* sorted, int64_t n, int nx, int ny, int nz, int 
   PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_gather_rows: unsupported mesh shape");
   PMB_REQUIRE(n >= 0 && n < 4294967295ll, "pmb_gather_rows: particle count out of range");
   PMB_REQUIRE(C >= 1 && C <= 4, "pmb_gather_rows: 1..4 channels supported");
+  PMB_REQUIRE(out != nullptr || vel != nullptr, "pmb_gather_rows: out may be null only with vel");
   SortedView v = sorted_view((void*)sorted, n, m);
   return gather_sorted(v.rec, v.perm, v.offs, n, m, C, mesh, out, vel, kick, kick2, S(stream), v.status);
 }
@@ -505,6 +506,7 @@ int pmb_force2(const int16_t* pmid, float* disp, const float* drift_vel, float d
   PMB_REQUIRE(valid_mesh(nx, ny, nz), "pmb_force: unsupported mesh shape");
   PMB_REQUIRE(n >= 0 && n < 4294967295ll, "pmb_force: particle count out of range");
   PMB_REQUIRE(cell > 0.f, "pmb_force: cell size must be positive");
+  PMB_REQUIRE(acc != nullptr || vel_kick != nullptr, "pmb_force: acc may be null only with vel_kick");
   void *sorted, *bins, *scale16, *work;
   float* src;
   float2 *src_hat, *grad_hat;

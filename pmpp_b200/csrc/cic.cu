@@ -924,7 +924,7 @@ __global__ void __launch_bounds__(256) gather_staged_kernel(const Rec* __restric
         const float v = stage[((c * SX + k + bx) * SY + iy + by) * nz + (bz ? z1 : cz)];
         a = __fadd_rn(a, __fmul_rn(v, __fmul_rn(__fmul_rn(wx[bx], wy[by]), wz[bz])));
       }
-      out[(int64_t)src * C + c] = a;
+      if (out != nullptr) out[(int64_t)src * C + c] = a;
       if (vel != nullptr) vel[(int64_t)src * C + c] = kicked(vel[(int64_t)src * C + c], a, kick, kick2);
     }
   }
@@ -979,10 +979,10 @@ __global__ void __launch_bounds__(256) gather_kernel_x2(const Rec* __restrict__ 
       a0 = __fadd_rn(a0, __fmul_rn(v0[b], k0.w[b]));
       a1 = __fadd_rn(a1, __fmul_rn(v1[b], k1.w[b]));
     }
-    out[(int64_t)s0 * C + c] = mk0 ? 0.f : a0;
+    if (out != nullptr) out[(int64_t)s0 * C + c] = mk0 ? 0.f : a0;
     if (vel != nullptr && !mk0) vel[(int64_t)s0 * C + c] = kicked(u0[c], a0, kick, kick2);
     if (two) {
-      out[(int64_t)s1 * C + c] = mk1 ? 0.f : a1;
+      if (out != nullptr) out[(int64_t)s1 * C + c] = mk1 ? 0.f : a1;
       if (vel != nullptr && !mk1) vel[(int64_t)s1 * C + c] = kicked(u1[c], a1, kick, kick2);
     }
   }
@@ -998,7 +998,8 @@ __global__ void masked_tail_gather_kernel(const uint32_t* __restrict__ perm, con
   if (flagged(status)) return;
   for (int64_t i = (int64_t)*offs_end + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
-    for (int c = 0; c < C; ++c) out[(int64_t)perm[i] * C + c] = 0.f;
+    for (int c = 0; c < C; ++c)
+      if (out != nullptr) out[(int64_t)perm[i] * C + c] = 0.f;
 }
 
 __global__ void masked_tail_interp_kernel(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ offs_end,

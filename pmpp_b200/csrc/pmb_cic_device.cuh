@@ -283,7 +283,8 @@ __device__ __forceinline__ void gather_one(const Rec& r, uint32_t src, Mesh3 m, 
   if (r.key == kMaskedKey) {
     // masked particle: zero value, velocity untouched (a zero kick)
 #pragma unroll
-    for (int c = 0; c < C; ++c) out[(int64_t)src * C + c] = 0.f;
+    for (int c = 0; c < C; ++c)
+      if (out != nullptr) out[(int64_t)src * C + c] = 0.f;
     return;
   }
   Corners k;
@@ -301,7 +302,7 @@ __device__ __forceinline__ void gather_one(const Rec& r, uint32_t src, Mesh3 m, 
     float a = 0.f;
 #pragma unroll
     for (int b = 0; b < 8; ++b) a = __fadd_rn(a, __fmul_rn(__ldg(mc + k.idx[b]), k.w[b]));
-    out[(int64_t)src * C + c] = a;
+    if (out != nullptr) out[(int64_t)src * C + c] = a;
     if (vel != nullptr) vel[(int64_t)src * C + c] = kicked(u[c], a, kick, kick2);
   }
 }

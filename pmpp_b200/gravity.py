@@ -336,7 +336,7 @@ class _NoTimer:
 
 
 def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc, drift_vel, drift, vel_kick,
-                  kick, timer, src_hat_out=None, lane="", kick2=0.0):
+                  kick, timer, src_hat_out=None, lane="", kick2=0.0, keep_acc=True):
     """pmb_force as separate stage calls with a CUDA event after each stage.
 
     With src_hat_out (complex64, half spectrum) the rFFT of the Poisson source
@@ -386,11 +386,13 @@ def _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F
         t = timer.mark("green_gradient", t)
         call("pmb_irfft3", nx, ny, nz, 3, spec3.data_ptr(), F.data_ptr(), work.data_ptr(), s)
         t = timer.mark("fft_c2r", t)
-    call("pmb_gather_rows2", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), acc.data_ptr(), ptr(vel_kick),
+    out = acc if (keep_acc or vel_kick is None) else None
+    call("pmb_gather_rows2", sorted_buf.data_ptr(), n, nx, ny, nz, 3, F.data_ptr(), ptr(out), ptr(vel_kick),
          float(kick), float(kick2), s)
     timer.mark("gather", t)
     if vel_kick is not None:
-        timer.tag("gather_kick")  # this gather also read and wrote the velocities
+        # this gather also read and wrote the velocities (and stored no acc)
+        timer.tag("gather_kick" if out is not None else "gather_kick_only")
 
 
 def _force_vjp_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, F, acc_cot, disp_cot, timer,
@@ -476,7 +478,7 @@ def _tables(conf, dev, gk, correction):
 
 
 def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, force_meshes=None, acc=None,
-          drift_vel=None, drift=0.0, vel_kick=None, kick=0.0, kick2=0.0, src_hat_out=None, lane=""):
+          drift_vel=None, drift=0.0, vel_kick=None, kick=0.0, kick2=0.0, src_hat_out=None, lane="", keep_acc=True):
     """One PM force evaluation on device tensors.
 
     Returns (acc (N,3), force_meshes (3,Mx,My,Mz)).  With drift_vel the
@@ -484,6 +486,8 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
     half-kick vel_kick += acc * kick is fused into the gather, followed by
     vel_kick += acc * kick2 when kick2 != 0 (the next step's opening kick).
     lane selects the workspace that keeps the sorted records (see force_vjp).
+    keep_acc=False with vel_kick: apply the kicks without storing acc (the
+    plain route; returns acc None there).
     float64 displacements take the float64 build (x64.force; no correction,
     one folded kick)."""
     require_cuda(pmid, disp, drift_vel, vel_kick)
@@ -515,17 +519,18 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
         return acc, force_meshes
     if StageTimer.active is not None or src_hat_out is not None:
         _force_staged(pmid, disp, conf, omega_m, tables, gk, transfer, radial, rl, force_meshes, acc, drift_vel,
-                      drift, vel_kick, kick, StageTimer.active, src_hat_out, lane, kick2)
-        return acc, force_meshes
+                      drift, vel_kick, kick, StageTimer.active, src_hat_out, lane, kick2, keep_acc)
+        return (acc if (keep_acc or vel_kick is None) else None), force_meshes
     wb = lib().pmb_force_workspace_bytes(n, nx, ny, nz)
     if wb < 0:
         raise RuntimeError("pmb_force_workspace_bytes failed: " + lib().pmb_last_error().decode())
     ws = workspace(wb, dev, "force" + _lane_suffix(lane))
+    out = acc if (keep_acc or vel_kick is None) else None
     call("pmb_force2", pmid.data_ptr(), disp.data_ptr(), ptr(drift_vel), float(drift), n, nx, ny, nz,
          float(conf.cell_size), float(conf.mesh_size / conf.ptcl_num), 1.5 * _om32(omega_m), tables.data_ptr(),
          int(conf.has_particle_nyquist_masks), gk, ptr(transfer), ptr(radial), rl, force_meshes.data_ptr(),
-         acc.data_ptr(), ptr(vel_kick), float(kick), float(kick2), ws.data_ptr(), ws.numel(), stream_handle(dev))
-    return acc, force_meshes
+         ptr(out), ptr(vel_kick), float(kick), float(kick2), ws.data_ptr(), ws.numel(), stream_handle(dev))
+    return out, force_meshes
 
 
 def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *, a=None, cosmo=None,

@@ -225,14 +225,18 @@ class NBodyRun:
             kick_f = ks[0] if ks else 0.0
             kick2 = ks[1] if len(ks) == 2 else 0.0
             vk = vel if ks else None
+            # the acceleration is needed only if a later op reads it before the
+            # next force overwrites it (an unfolded kick, or the returned state)
+            j = i + 1 + len(ks)
+            keep = vk is None or j >= len(ops) or ops[j][0] != "drift"
             if st[0] == "init":
                 force(ptcl.pmid, disp, conf, cosmo.Omega_m, a=float(a[0]), cosmo=cosmo, correction=self.correction,
-                      force_meshes=F, acc=acc, vel_kick=vk, kick=kick_f, kick2=kick2, src_hat_out=S)
+                      force_meshes=F, acc=acc, vel_kick=vk, kick=kick_f, kick2=kick2, src_hat_out=S, keep_acc=keep)
             else:
                 D = _f32(cosmo.drift_factor(st[1], st[2], st[3]))
                 force(ptcl.pmid, disp, conf, cosmo.Omega_m, a=float(st[3]), cosmo=cosmo, correction=self.correction,
                       force_meshes=F, acc=acc, drift_vel=vel, drift=D, vel_kick=vk, kick=kick_f, kick2=kick2,
-                      src_hat_out=S)
+                      src_hat_out=S, keep_acc=keep)
             i += 1 + len(ks)
         self.final_meshes = F
         self.final_src_hat = S

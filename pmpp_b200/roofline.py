@@ -47,6 +47,7 @@ def algorithmic_bytes(op, N, M, Mc=None, R=None, T=None, live=None):
         "scatter3": 18 * N + 12 * N + 12 * M,          # gather adjoint: 3-channel values in, 3 meshes out
         "gather": 18 * N + 12 * N + 12 * T,             # 3 force meshes in, acc out
         "gather_kick": 18 * N + 12 * N + 12 * T + 24 * N,  # ... and the folded kick: vel in and out
+        "gather_kick_only": 18 * N + 12 * T + 24 * N,   # the folded kicks without storing acc
         "gather_adjoint": 18 * N + 12 * T + 12 * N + 24 * N,   # positions, meshes, acc cot, disp cot r/w
         "scatter_adjoint": 18 * N + 4 * T + 24 * N,     # positions, density cot, disp cot r/w
         "fft_r2c": 4 * M + 8 * Mc,

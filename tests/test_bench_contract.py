@@ -42,12 +42,20 @@ def test_roofline_byte_models():
     from pmpp_b200.roofline import algorithmic_bytes
     N, M = 256**3, 512**3
     assert algorithmic_bytes("gather_kick", N, M) - algorithmic_bytes("gather", N, M) == 24 * N
+    assert algorithmic_bytes("gather_kick", N, M) - algorithmic_bytes("gather_kick_only", N, M) == 12 * N
     b = _bench()
     # measured traffic per launch stays within a few percent of the algorithmic bytes
     for name in ("gather", "gather_kick"):
         ratio = b.MEASURED_TRAFFIC_PER_PARTICLE[name] * N / algorithmic_bytes(name, N, M)
         assert 0.95 < ratio < 1.05, (name, ratio)
-    assert b.STAGE_VARIANTS["gather"] == "gather_kick"
+    assert b.STAGE_VARIANTS["gather"] == ("gather_kick", "gather_kick_only")
+    # a stage's bytes are the launch-weighted mean over the variants the timer counted
+    conf = types.SimpleNamespace(mesh_shape=(512, 512, 512))
+    counts = {"gather": 10, "gather_kick": 3, "gather_kick_only": 5}
+    alg, _, mix = b.stage_mix("gather", counts, N, M, conf, None)
+    want = (3 * algorithmic_bytes("gather_kick", N, M) + 5 * algorithmic_bytes("gather_kick_only", N, M)
+            + 2 * algorithmic_bytes("gather", N, M)) / 10
+    assert abs(alg - want) < 1 and mix == {"gather_kick": 3, "gather_kick_only": 5, "gather": 2}
 
 
 def test_gpus_flag_self_launches_ranks():
