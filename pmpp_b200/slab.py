@@ -46,8 +46,8 @@ from .gravity import _om32
 from .nbody import _f32, _schedule
 from .runtime import stream_handle
 
-# bytes of one routed particle: pmid (3 x int16), disp and vel (3 x float32 each)
-_ROW = 6 + 12 + 12
+# per-particle fields routed with a particle after pmid (3 x int16): float32 x 3 each
+_FIELDS = ("disp", "vel", "acc", "disp_cot", "vel_cot", "acc_cot")
 
 
 class ProcessGroupComm:
@@ -82,6 +82,14 @@ class ProcessGroupComm:
         self.dist.all_to_all_single(recv, send, rcnt, scnt, group=self.group)
         return [recv]
 
+    def allreduce_sum(self, value):
+        """Sum of a float over the ranks (float64)."""
+        t = torch.tensor([float(value)], dtype=torch.float64)
+        if self.dist.get_backend(self.group) == "nccl":
+            t = t.cuda()
+        self.dist.all_reduce(t, group=self.group)
+        return float(t.item())
+
     def shift(self, tensors, offset):
         """Rank r receives the tensor of rank (r - offset) mod P."""
         t = tensors[0].contiguous()
@@ -113,6 +121,9 @@ class LocalComm:
         segs = [list(torch.split(sends[i].contiguous(), [int(v) for v in matrix[i]])) for i in range(P)]
         return [torch.cat([segs[i][j] for i in range(P)]) for j in range(P)]
 
+    def allreduce_sum(self, value):
+        return float(value)  # the local ranks' values are already summed by the caller
+
     def shift(self, tensors, offset):
         P = self.world
         return [tensors[(r - offset) % P].clone() for r in range(P)]
@@ -121,11 +132,15 @@ class LocalComm:
 @dataclass
 class SlabParticles:
     """The particles one rank owns: global lattice anchors pmid (int16 x 3),
-    displacements, velocities and accelerations (float32 x 3)."""
+    displacements, velocities and accelerations (float32 x 3), and in a
+    reverse sweep their cotangents."""
     pmid: torch.Tensor
     disp: torch.Tensor
     vel: torch.Tensor
     acc: torch.Tensor = None
+    disp_cot: torch.Tensor = None
+    vel_cot: torch.Tensor = None
+    acc_cot: torch.Tensor = None
 
 
 def _as_bytes(t):
@@ -179,27 +194,28 @@ class SlabPM:
         there.  Raises on every rank, before moving anything, when a rank's
         total would exceed the capacity."""
         P = self.P
+        # the fields every rank carries (the same on all ranks: a collective decision)
+        fields = [f for f in _FIELDS if getattr(states[0], f) is not None]
+        row = 6 + 12 * len(fields)
         sends, counts = [], []
         for st in states:
             dest = self.owner(st.pmid, st.disp)
             order = torch.argsort(dest, stable=True)
-            rows = torch.cat([_as_bytes(st.pmid), _as_bytes(st.disp), _as_bytes(st.vel)], dim=1)
+            rows = torch.cat([_as_bytes(st.pmid)] + [_as_bytes(getattr(st, f)) for f in fields], dim=1)
             sends.append(rows[order].reshape(-1))
-            counts.append((torch.bincount(dest, minlength=P) * _ROW).tolist())
+            counts.append((torch.bincount(dest, minlength=P) * row).tolist())
         matrix = self.comm.count_matrix(counts)
-        totals = matrix.sum(axis=0) // _ROW
+        totals = matrix.sum(axis=0) // row
         if self.capacity is not None and int(totals.max()) > self.capacity:
             worst = int(np.argmax(totals))
             raise RuntimeError(f"slab routing: rank {worst} would hold {int(totals[worst])} particles, "
                                f"over its capacity {self.capacity}")
         recvs = self.comm.alltoallv(sends, matrix)
         out = []
-        for st, rb in zip(states, recvs):
-            rows = rb.reshape(-1, _ROW)
-            pmid = rows[:, :6].contiguous().view(torch.int16)
-            disp = rows[:, 6:18].contiguous().view(torch.float32)
-            vel = rows[:, 18:].contiguous().view(torch.float32)
-            out.append(SlabParticles(pmid, disp, vel))
+        for rb in recvs:
+            rows = rb.reshape(-1, row)
+            vals = {f: rows[:, 6 + 12 * k:18 + 12 * k].contiguous().view(torch.float32) for k, f in enumerate(fields)}
+            out.append(SlabParticles(rows[:, :6].contiguous().view(torch.int16), **vals))
         return out
 
     # -- force ------------------------------------------------------------------
@@ -234,36 +250,65 @@ class SlabPM:
              stream_handle(spec.device))
         return out
 
+    def green_adjoint(self, r, spec3, post):
+        """Transpose of rank r's multiplier: three spectra (3, nx, ny/P, nz/2+1) -> one."""
+        nx, _, nz = self.conf.mesh_shape
+        out = torch.empty(tuple(spec3.shape[1:]), dtype=torch.complex64, device=spec3.device)
+        call("pmb_green_gradient_adjoint", spec3.data_ptr(), out.data_ptr(), nx, self.nyl, nz,
+             self.tables(r, spec3.device).data_ptr(), int(self.conf.has_particle_nyquist_masks), 0, None, None, 0,
+             float(post), stream_handle(spec3.device))
+        return out[None]
+
+    def _spectral(self, fields, mult, c_out):
+        """Distributed transform of real slabs (c_in, nx/P, ny, nz): rfft over
+        (y, z), all-to-all to ky slabs, fft over x, mult(r, spectra (c_in, nx,
+        ny/P, nz/2+1)) -> (c_out, ...), inverse fft over x, all-to-all back,
+        irfft over (y, z): real slabs (c_out, nx/P, ny, nz).  Unnormalised both
+        ways, like the single-GPU chain."""
+        nx, ny, nz = self.conf.mesh_shape
+        P, nxl, nyl, nzh = self.P, self.nxl, self.nyl, nz // 2 + 1
+        c_in = fields[0].shape[0]
+        sends = []
+        for f in fields:
+            A = torch.fft.rfft2(f, dim=(2, 3))  # (c_in, nxl, ny, nzh)
+            A = A.reshape(c_in, nxl, P, nyl, nzh).permute(2, 0, 1, 3, 4)  # ky slab j first
+            sends.append(torch.view_as_real(A.contiguous()).reshape(-1))
+        seg = c_in * nxl * nyl * nzh * 2
+        recvs = self.comm.alltoallv(sends, np.full((P, P), seg, dtype=np.int64))
+        backs = []
+        for r, rb in zip(self.comm.local, recvs):
+            B = torch.view_as_complex(rb.reshape(P, c_in, nxl, nyl, nzh, 2))  # rank order = x order
+            B = B.permute(1, 0, 2, 3, 4).reshape(c_in, nx, nyl, nzh)
+            G = mult(r, torch.fft.fft(B, dim=1).contiguous())
+            g = torch.fft.ifft(G, dim=1, norm="forward")  # (c_out, nx, nyl, nzh)
+            backs.append(torch.view_as_real(g.reshape(c_out, P, nxl, nyl, nzh).transpose(0, 1).contiguous()).reshape(-1))
+        recvs = self.comm.alltoallv(backs, np.full((P, P), c_out * seg // c_in, dtype=np.int64))
+        out = []
+        for rb in recvs:
+            g = torch.view_as_complex(rb.reshape(P, c_out, nxl, nyl, nzh, 2))  # rank order = ky order
+            g = g.permute(1, 2, 0, 3, 4).reshape(c_out, nxl, ny, nzh)
+            out.append(torch.fft.irfft2(g, s=(ny, nz), dim=(2, 3), norm="forward").contiguous())
+        return out
+
     def spectral_force(self, sources, green=None):
         """Force slabs (3, nx/P, ny, nz) from Poisson-source slabs (nx/P, ny, nz):
         distributed rfft, multiplier, inverse.  green(r, spec) is the multiplier
         (the kernel by default)."""
         green = self.green if green is None else green
-        nx, ny, nz = self.conf.mesh_shape
-        P, nxl, nyl, nzh = self.P, self.nxl, self.nyl, nz // 2 + 1
-        # (y, z) transforms of the x slab, then ky slabs to their ranks
-        sends = []
-        for src in sources:
-            A = torch.fft.rfft2(src, dim=(1, 2))  # (nxl, ny, nzh), unnormalised
-            sends.append(torch.view_as_real(A.reshape(nxl, P, nyl, nzh).transpose(0, 1).contiguous()).reshape(-1))
-        seg = nxl * nyl * nzh * 2
-        recvs = self.comm.alltoallv(sends, np.full((P, P), seg, dtype=np.int64))
-        backs = []
-        for r, rb in zip(self.comm.local, recvs):
-            B = torch.view_as_complex(rb.reshape(nx, nyl, nzh, 2))  # rank order = x order
-            G = green(r, torch.fft.fft(B, dim=0).contiguous())
-            g = torch.fft.ifft(G, dim=1, norm="forward")  # (3, nx, nyl, nzh), unnormalised
-            backs.append(torch.view_as_real(g.reshape(3, P, nxl, nyl, nzh).transpose(0, 1).contiguous()).reshape(-1))
-        recvs = self.comm.alltoallv(backs, np.full((P, P), 3 * seg, dtype=np.int64))
-        out = []
-        for rb in recvs:
-            g = torch.view_as_complex(rb.reshape(P, 3, nxl, nyl, nzh, 2))  # rank order = ky order
-            g = g.permute(1, 2, 0, 3, 4).reshape(3, nxl, ny, nzh)
-            out.append(torch.fft.irfft2(g, s=(ny, nz), dim=(2, 3), norm="forward").contiguous())
-        return out
+        mult = lambda r, spec: green(r, spec[0].contiguous())
+        return self._spectral([s[None] for s in sources], mult, 3)
 
     def force(self, states, omega_m):
         """Accelerations of every local rank's particles (in their order)."""
+        sorted_, exts = self._forward(states, omega_m)
+        acc = [sp.gather(ext) for sp, ext in zip(sorted_, exts)]
+        for st, a in zip(states, acc):
+            st.acc = a
+        return acc
+
+    def _forward(self, states, omega_m):
+        """Cell-sorted particles on the local meshes and the force meshes with
+        their halo plane (3, nx/P + 1, ny, nz) of every local rank."""
         conf = self.conf
         nx, ny, nz = conf.mesh_shape
         L = self.nxl + 1
@@ -279,13 +324,41 @@ class SlabPM:
             sources.append((rho - 1.0) * src_mul)
         F = self.spectral_force(sources)
         fh = self.comm.shift([f[:, 0] for f in F], -1)
-        acc = []
-        for sp, f, h in zip(sorted_, F, fh):
-            ext = torch.cat([f, h[:, None]], dim=1).contiguous()  # (3, nxl + 1, ny, nz)
-            acc.append(sp.gather(ext))
-        for st, a in zip(states, acc):
-            st.acc = a
-        return acc
+        exts = [torch.cat([f, h[:, None]], dim=1).contiguous() for f, h in zip(F, fh)]  # (3, nxl + 1, ny, nz)
+        return sorted_, exts
+
+    def force_vjp(self, states, acc_cots, omega_m):
+        """Displacement cotangents (d acc / d disp)^T acc_cot of every local
+        rank's particles, the force recomputed at their positions; also sets
+        each state's acc.  The transpose of force(): gather adjoint (position
+        term, and the 3-channel deposit of acc_cot on the local mesh), the force
+        halo plane back to the rank it came from, the distributed transform with
+        the transposed multiplier (into the density cotangent, the source scale
+        included), the density halo plane back, and the deposit's position term."""
+        conf = self.conf
+        nx, ny, nz = conf.mesh_shape
+        sorted_, exts = self._forward(states, omega_m)
+        dcs, mesh_cots = [], []
+        for st, sp, ext, ac in zip(states, sorted_, exts, acc_cots):
+            st.acc = sp.gather(ext)
+            cot_sorted = torch.empty_like(ac)
+            dc, _ = sp.interp_grad(ext, u=ac.contiguous(), u_sorted=cot_sorted)
+            dcs.append(dc)
+            mesh_cots.append(sp.scatter(val=cot_sorted, channels=3, mode=0, val_sorted=True))  # (3, L, ny, nz)
+        back = self.comm.shift([m[:, self.nxl] for m in mesh_cots], 1)
+        fields = []
+        for m, b in zip(mesh_cots, back):
+            g = m[:, : self.nxl].clone()
+            g[:, 0] += b
+            fields.append(g)
+        post = float(np.float32(1.5 * _om32(omega_m)) / conf.mesh_size)
+        rho_cots = self._spectral(fields, lambda r, spec: self.green_adjoint(r, spec, post), 1)
+        hb = self.comm.shift([rc[0, 0] for rc in rho_cots], -1)
+        vc = float(conf.mesh_size / conf.ptcl_num)
+        for sp, rc, h, dc in zip(sorted_, rho_cots, hb, dcs):
+            dens_cot = torch.cat([rc[0], h[None]], dim=0)[None].contiguous()  # (1, nxl + 1, ny, nz)
+            sp.interp_grad(dens_cot, u_const=vc, disp_cot=dc, accumulate=True)
+        return dcs
 
     # -- time integration -------------------------------------------------------
     def nbody(self, states, cosmo, a_nbody=None):
@@ -309,6 +382,56 @@ class SlabPM:
                         call("pmb_axpy", p.vel.data_ptr(), p.acc.data_ptr(), p.vel.numel(), K,
                              stream_handle(p.vel.device))
         return states
+
+    def nbody_adj(self, states, cosmo, a_nbody=None):
+        """Reverse sweep on the slabs from the final state.  states hold pmid,
+        disp, vel, acc at the last time and the cotangents disp_cot, vel_cot
+        (acc_cot: zero when None).  Runs the per-operation adjoints of
+        nbody.integrate_adj (kick adjoint, force adjoint, drift adjoint, force
+        recompute) with the particles and their cotangents routed after every
+        reverse drift, then the initial force's adjoint.  Returns the initial
+        states (with their cotangents) and the Omega_m cotangent, summed over
+        all ranks."""
+        conf = self.conf
+        a = conf.a_nbody if a_nbody is None else np.asarray(a_nbody)
+        om32 = _om32(cosmo.Omega_m)
+        for st in states:
+            for f in ("disp_cot", "vel_cot", "acc_cot"):
+                t = getattr(st, f)
+                setattr(st, f, torch.zeros_like(st.disp) if t is None else t.clone().float().contiguous())
+        om_local = 0.0
+
+        def force_adj(states):
+            dcs = self.force_vjp(states, [st.acc_cot for st in states], cosmo.Omega_m)
+            tot = 0.0
+            for st, dc in zip(states, dcs):
+                st.disp_cot += dc
+                tot += float((st.acc_cot.double() * st.acc.double()).sum())
+                st.acc_cot.zero_()
+            return tot / om32
+
+        for a_prev, a_next in list(zip(a[:-1], a[1:]))[::-1]:
+            for st in reversed(_schedule(a_prev, a_next, conf)):
+                if st[0] == "kick":
+                    K, dK = cosmo.kick_factor(st[1], st[2], st[3], with_grad=True)
+                    for p in states:
+                        dot = torch.zeros(1, dtype=torch.float64, device=p.vel.device)
+                        call("pmb_kick_adj", p.vel.data_ptr(), p.acc.data_ptr(), p.vel_cot.data_ptr(),
+                             p.acc_cot.data_ptr(), p.vel.numel(), _f32(K), dot.data_ptr(), stream_handle(p.vel.device))
+                        om_local += dK * float(dot.item())
+                    continue
+                _, a_vel, a_disp, a_disp_next, a_acc_in = st
+                om_local += force_adj(states)
+                D, dD = cosmo.drift_factor(a_vel, a_disp, a_disp_next, with_grad=True)
+                for p in states:
+                    dot = torch.zeros(1, dtype=torch.float64, device=p.disp.device)
+                    call("pmb_drift_adj", p.disp.data_ptr(), p.vel.data_ptr(), p.disp_cot.data_ptr(),
+                         p.vel_cot.data_ptr(), p.disp.numel(), _f32(D), dot.data_ptr(), stream_handle(p.disp.device))
+                    om_local += dD * float(dot.item())
+                states = self.migrate(states)
+                self.force(states, cosmo.Omega_m)
+        om_local += force_adj(states)
+        return states, self.comm.allreduce_sum(om_local)
 
     def collect(self, states):
         """Concatenate local ranks' particles and order them by anchor cell

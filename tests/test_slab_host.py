@@ -75,8 +75,9 @@ def _rank_main(rank, world, port, q):
         conf = _conf()
         slab = SlabPM(conf, ProcessGroupComm())
         states, F, planes = _work(slab, *_particles(conf))
+        total = slab.comm.allreduce_sum(rank + 0.5)
         q.put((rank, [tuple(t.numpy() for t in s) for s in states], [f.numpy() for f in F],
-               [p.numpy() for p in planes]))
+               [p.numpy() for p in planes], total))
     finally:
         dist.destroy_process_group()
 
@@ -97,8 +98,9 @@ def test_process_group_exchanges_match_local_comm():
         p.start()
     got = {}
     for _ in range(2):
-        r, st, F, planes = q.get(timeout=240)
+        r, st, F, planes, total = q.get(timeout=240)
         got[r] = (st, F, planes)
+        assert total == 2.0  # 0.5 + 1.5 summed over the two ranks
     for p in procs:
         p.join(timeout=120)
         assert p.exitcode == 0
