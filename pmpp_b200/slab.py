@@ -178,6 +178,15 @@ class SlabPM:
     def owner(self, pmid, disp):
         return self.cell_x(pmid, disp)[0] // self.nxl
 
+    def cell_key(self, pmid, disp):
+        """Raveled global lower-corner cell (x-major), binned as the sort bins it."""
+        nx, ny, nz = self.conf.mesh_shape
+        q = disp / np.float32(self.conf.cell_size)
+        q = torch.where(torch.isfinite(q), q, torch.zeros_like(q))
+        c = pmid.to(torch.int64) + torch.floor(q).to(torch.int64)
+        c = torch.remainder(c, torch.tensor([nx, ny, nz], device=c.device))
+        return (c[:, 0] * ny + c[:, 1]) * nz + c[:, 2]
+
     def distribute(self, pmid, disp, vel=None):
         """Each local rank's share of a particle set every process holds."""
         vel = torch.zeros_like(disp) if vel is None else vel
@@ -190,9 +199,10 @@ class SlabPM:
 
     def migrate(self, states):
         """Route every particle to the rank owning its cell (after a drift).
-        Received particles are ordered by source rank, then by their order
-        there.  Raises on every rank, before moving anything, when a rank's
-        total would exceed the capacity."""
+        Received particles are merged in stable cell-key order (ties: source
+        rank, then order there), as the reference's merge path keeps them.
+        Raises on every rank, before moving anything, when a rank's total would
+        exceed the capacity."""
         P = self.P
         # the fields every rank carries (the same on all ranks: a collective decision)
         fields = [f for f in _FIELDS if getattr(states[0], f) is not None]
@@ -214,6 +224,9 @@ class SlabPM:
         out = []
         for rb in recvs:
             rows = rb.reshape(-1, row)
+            pmid = rows[:, :6].contiguous().view(torch.int16)
+            disp = rows[:, 6:18].contiguous().view(torch.float32)
+            rows = rows[torch.argsort(self.cell_key(pmid, disp), stable=True)]
             vals = {f: rows[:, 6 + 12 * k:18 + 12 * k].contiguous().view(torch.float32) for k, f in enumerate(fields)}
             out.append(SlabParticles(rows[:, :6].contiguous().view(torch.int16), **vals))
         return out

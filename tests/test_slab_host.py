@@ -134,3 +134,5 @@ def test_process_group_exchanges_match_local_comm():
     assert total == 2000
     for r, s in enumerate(states):
         assert bool(((slab.owner(s[0], s[1])) == r).all())
+        keys = slab.cell_key(s[0], s[1])
+        assert bool((keys[1:] >= keys[:-1]).all())  # merged in cell-key order
