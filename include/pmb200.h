@@ -370,6 +370,13 @@ int pmb_kick_adj(float* vel, const float* acc, const float* vel_cot, float* acc_
 int pmb_kick_adj2(float* vel, const float* acc, const float* vel_cot, float* acc_cot, int64_t n, float kick_a,
                   float kick_b, int two, int zero_cot, double* dot_a, double* dot_b, double* dot_force,
                   void* stream);
+/* pmb_kick_adj2 preceded, in the same pass, by the cotangent half of the
+ * drift adjoint that comes before the kicks in a reverse sweep (disp_cot may
+ * be null: none): vel_cot += disp_cot * drift and dot_drift += sum disp_cot *
+ * vel (vel on entry); bit-identical to pmb_drift_cot_adj then pmb_kick_adj2. */
+int pmb_kick_adj3(float* vel, const float* acc, float* vel_cot, float* acc_cot, int64_t n, float kick_a, float kick_b,
+                  int two, int zero_cot, double* dot_a, double* dot_b, double* dot_force, const float* disp_cot,
+                  float drift, double* dot_drift, void* stream);
 /* Cotangent half of pmb_drift_adj (vel_cot += disp_cot * drift, dot += sum
  * disp_cot * vel); the position half is a drift by -drift, fused into the
  * next pmb_force's sort (bit-identical to pmb_drift_adj's position update). */

@@ -84,6 +84,7 @@ _SIGS = {
     "pmb_axpy": (c_int, [c_p, c_p, c_i64, c_f, c_p]),
     "pmb_kick_adj": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_p, c_p]),
     "pmb_kick_adj2": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_f, c_int, c_int, c_p, c_p, c_p, c_p]),
+    "pmb_kick_adj3": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_f, c_int, c_int, c_p, c_p, c_p, c_p, c_f, c_p, c_p]),
     "pmb_drift_cot_adj": (c_int, [c_p, c_p, c_p, c_i64, c_f, c_p, c_p]),
     "pmb_drift_adj": (c_int, [c_p, c_p, c_p, c_p, c_i64, c_f, c_p, c_p]),
     "pmb_dot": (c_int, [c_p, c_p, c_i64, c_p, c_p]),
@@ -192,7 +193,7 @@ _KERNELS = {
     "pmb_cnn_conv3d_wgrad": 1, "pmb_cnn_stem_input": 1, "pmb_cnn_residual": 1, "pmb_cnn_residual_adjoint": 1,
     "pmb_cnn_norm_adjoint": 1, "pmb_green_potential": 1, "pmb_gradient_spectra": 1, "pmb_gradient_adjoint_plain": 1,
     "pmb_green_gradient_adjoint": 1, "pmb_axpy": 1,
-    "pmb_kick_adj": 1, "pmb_kick_adj2": 1, "pmb_drift_cot_adj": 1, "pmb_drift_adj": 1, "pmb_dot": 1,
+    "pmb_kick_adj": 1, "pmb_kick_adj2": 1, "pmb_kick_adj3": 1, "pmb_drift_cot_adj": 1, "pmb_drift_adj": 1, "pmb_dot": 1,
     "pmb_force": 9, "pmb_force2": 9, "pmb_force_streamed": 14, "pmb_force_vjp": 11, "pmb_force_vjp_presorted": 6, "pmb_sum": 1,
     "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,
     "pmb_lpt": 4, "pmb_lpt_vjp": 6, "pmb_pk_shells": 1, "pmb_shell_stats": 1, "pmb_pk_shells_adjoint": 1,

@@ -720,8 +720,17 @@ int pmb_kick_adj2(float* vel, const float* acc, const float* vel_cot, float* acc
                   float kick_b, int two, int zero_cot, double* dot_a, double* dot_b, double* dot_force,
                   void* stream) {
   PMB_REQUIRE(dot_a != nullptr && (two == 0 || dot_b != nullptr), "pmb_kick_adj2: dot accumulators required");
+  return kick_adj2(vel, acc, const_cast<float*>(vel_cot), acc_cot, n, kick_a, kick_b, two != 0, zero_cot != 0, dot_a,
+                   dot_b, dot_force, nullptr, 0.f, nullptr, S(stream));
+}
+
+int pmb_kick_adj3(float* vel, const float* acc, float* vel_cot, float* acc_cot, int64_t n, float kick_a, float kick_b,
+                  int two, int zero_cot, double* dot_a, double* dot_b, double* dot_force, const float* disp_cot,
+                  float drift, double* dot_drift, void* stream) {
+  PMB_REQUIRE(dot_a != nullptr && (two == 0 || dot_b != nullptr), "pmb_kick_adj3: dot accumulators required");
+  PMB_REQUIRE(disp_cot == nullptr || dot_drift != nullptr, "pmb_kick_adj3: drift dot accumulator required");
   return kick_adj2(vel, acc, vel_cot, acc_cot, n, kick_a, kick_b, two != 0, zero_cot != 0, dot_a, dot_b, dot_force,
-                   S(stream));
+                   disp_cot, drift, dot_drift, S(stream));
 }
 
 int pmb_drift_cot_adj(const float* vel, const float* disp_cot, float* vel_cot, int64_t n, float drift, double* dot,

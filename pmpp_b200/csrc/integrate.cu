@@ -60,14 +60,26 @@ __global__ void kick_adj_kernel(float* __restrict__ vel, const float* __restrict
 // separate kernels would apply them, plus the force-slot dot sum(acc_cot * acc)
 // of the force adjoint that follows.  zero_cot: acc_cot is taken as zero
 // (the force adjoint before consumed it).
+// With disp_cot, the cotangent half of the drift adjoint that precedes the
+// kicks in the reverse sweep runs first, as drift_cot_adj_kernel would:
+// vel_cot += disp_cot * dd, dot_d += sum disp_cot * vel (vel before the kicks).
 __global__ void kick_adj2_kernel(float* __restrict__ vel, const float* __restrict__ acc,
-                                 const float* __restrict__ vel_cot, float* __restrict__ acc_cot, int64_t n, float ka,
+                                 float* __restrict__ vel_cot, float* __restrict__ acc_cot, int64_t n, float ka,
                                  float kb, int two, int zero_cot, double* __restrict__ dot_a,
-                                 double* __restrict__ dot_b, double* __restrict__ dot_f) {
-  double s = 0.0, sf = 0.0;
+                                 double* __restrict__ dot_b, double* __restrict__ dot_f,
+                                 const float* __restrict__ disp_cot, float dd, double* __restrict__ dot_d) {
+  double s = 0.0, sf = 0.0, sd = 0.0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const float a = acc[i], vc = vel_cot[i];
-    float v = __fsub_rn(vel[i], __fmul_rn(a, ka));
+    const float a = acc[i];
+    float vc = vel_cot[i];
+    float v = vel[i];
+    if (disp_cot != nullptr) {
+      const float dc = disp_cot[i];
+      vc = __fadd_rn(vc, __fmul_rn(dc, dd));
+      vel_cot[i] = vc;
+      sd += (double)dc * (double)v;
+    }
+    v = __fsub_rn(v, __fmul_rn(a, ka));
     float c = __fadd_rn(zero_cot ? 0.f : acc_cot[i], __fmul_rn(vc, ka));
     if (two) {
       v = __fsub_rn(v, __fmul_rn(a, kb));
@@ -81,6 +93,7 @@ __global__ void kick_adj2_kernel(float* __restrict__ vel, const float* __restric
   block_add(s, dot_a);
   if (two) block_add(s, dot_b);
   if (dot_f != nullptr) block_add(sf, dot_f);
+  if (disp_cot != nullptr) block_add(sd, dot_d);
 }
 
 // Cotangent half of the drift adjoint: vel_cot += disp_cot * d, dot += sum
@@ -139,11 +152,12 @@ int kick_adj(float* vel, const float* acc, const float* vel_cot, float* acc_cot,
   return kOk;
 }
 
-int kick_adj2(float* vel, const float* acc, const float* vel_cot, float* acc_cot, int64_t n, float ka, float kb,
-              int two, int zero_cot, double* dot_a, double* dot_b, double* dot_f, cudaStream_t s) {
+int kick_adj2(float* vel, const float* acc, float* vel_cot, float* acc_cot, int64_t n, float ka, float kb,
+              int two, int zero_cot, double* dot_a, double* dot_b, double* dot_f, const float* disp_cot, float dd,
+              double* dot_d, cudaStream_t s) {
   if (n > 0)
     kick_adj2_kernel<<<grid_n(n, 256), 256, 0, s>>>(vel, acc, vel_cot, acc_cot, n, ka, kb, two, zero_cot, dot_a, dot_b,
-                                                    dot_f);
+                                                    dot_f, disp_cot, dd, dot_d);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }

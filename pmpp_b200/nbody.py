@@ -324,6 +324,17 @@ class NBodyRun:
         side = torch.cuda.Stream(device=dev) if overlap else None
         ev_force = None  # side-stream force that main must see before touching vel / acc
         lane = 0  # lane holding the sorted records of the current positions
+        # the cotangent half of a drift adjoint waiting to run inside the next
+        # kick adjoints' pass (D, dot slot), or alone before a force adjoint
+        drift_pending = None
+
+        def flush_drift():
+            nonlocal drift_pending
+            if drift_pending is not None:
+                call("pmb_drift_cot_adj", vel.data_ptr(), dc.data_ptr(), vc.data_ptr(), disp.numel(), drift_pending[0],
+                     dots[drift_pending[1]:].data_ptr(), s)
+                drift_pending = None
+
         i = 0
         while i < len(ops):
             st = ops[i]
@@ -342,10 +353,13 @@ class NBodyRun:
                 sb = slot + 1 if two else None
                 sf = slot + len(ks) if force_next else None
                 slot += len(ks) + (1 if force_next else 0)
-                call("pmb_kick_adj2", vel.data_ptr(), acc.data_ptr(), vc.data_ptr(), ac.data_ptr(), n3,
+                dp = drift_pending
+                call("pmb_kick_adj3", vel.data_ptr(), acc.data_ptr(), vc.data_ptr(), ac.data_ptr(), n3,
                      _f32(Ks[0][0]), _f32(Ks[1][0]) if two else 0.0, int(two), int(zero_pending),
                      dots[sa:].data_ptr(), dots[sb:].data_ptr() if two else None,
-                     dots[sf:].data_ptr() if force_next else None, s)
+                     dots[sf:].data_ptr() if force_next else None, dc.data_ptr() if dp else None,
+                     dp[0] if dp else 0.0, dots[dp[1]:].data_ptr() if dp else None, s)
+                drift_pending = None
                 grads.append((Ks[0][1], sa))
                 if two:
                     grads.append((Ks[1][1], sb))
@@ -356,6 +370,7 @@ class NBodyRun:
                 i = j
                 continue
             # force adjoint at the post-drift positions (or the initial evaluation)
+            flush_drift()
             if zero_pending:
                 ac.zero_()
                 zero_pending = False
@@ -390,9 +405,9 @@ class NBodyRun:
                           force_meshes=F2, acc=acc, src_hat_out=S2, drift_vel=vel, drift=-D32,
                           lane=str(1 - lane))
                 ev_force = side.record_event()
-            # the drift's cotangent half: vel_cot += D disp_cot (after the force adjoint)
-            call("pmb_drift_cot_adj", vel.data_ptr(), dc.data_ptr(), vc.data_ptr(), disp.numel(), D32,
-                 dots[slot:].data_ptr(), s)
+            # the drift's cotangent half: vel_cot += D disp_cot (after the force
+            # adjoint), run inside the next kick adjoints' pass
+            drift_pending = (D32, slot)
             grads.append((dD, slot))
             slot += 1
             if not overlap:
@@ -404,6 +419,7 @@ class NBodyRun:
             S, S2 = S2, S
         if ev_force is not None:
             main.wait_event(ev_force)
+        flush_drift()
         if zero_pending:
             ac.zero_()
         d = dots.cpu().numpy()
