@@ -188,7 +188,9 @@ __global__ void __launch_bounds__(256) ens_scatter_kernel(EnsDev d) {
 
 // Flat loop over the half spectra of all members; local cell coordinates
 // from 32-bit index arithmetic (members have fewer than 2^31 half cells).
-__global__ void ens_green_kernel(EnsDev d) {
+// odd_only: skip the members whose class the vector class kernel serves
+// (half spectra of 4-divisible size at 4-aligned offsets).
+__global__ void ens_green_kernel(EnsDev d, int odd_only) {
   __shared__ int64_t ss[kEnsMaxSims + 1];
   load_starts(ss, d.spec_start, d.nsims);
   for (int64_t jg = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; jg < d.nspec;
@@ -196,6 +198,7 @@ __global__ void ens_green_kernel(EnsDev d) {
     const int s = find_sim(ss, d.nsims, jg);
     const EnsSim& sim = d.sims[s];
     if (sim.pm) continue;  // multiplier fused into the member's FFT pass chain
+    if (odd_only && sim.m.half_cells() % 4 == 0 && (ss[s] & 3) == 0) continue;
     GreenParams g;
     g.green_kernel = 0;
     g.cell = 0.f;
@@ -210,6 +213,52 @@ __global__ void ens_green_kernel(EnsDev d) {
     const uint32_t r = j / nzh, ix = r / ny;
     green_gradient_at(sim.rho_hat, sim.grad_hat, (int64_t)j, m.half_cells(), (int)ix, (int)(r - ix * ny),
                       (int)(j - r * nzh), m, t, g);
+  }
+}
+
+// The multiplier of one mesh-shape class on the cuFFT route: blockIdx.y is
+// the member (its own tables and post scale), the x blocks stride over its
+// half spectrum four cells per thread with 32-byte vector loads and stores
+// (members of one class have equal, 4-divisible half spectra, stored
+// back to back).  The same per-cell arithmetic as ens_green_kernel, without
+// its per-cell search over the members.
+__global__ void ens_green_class_kernel(const EnsSim* __restrict__ sims, int first) {
+  const EnsSim& sim = sims[first + blockIdx.y];
+  GreenParams g;
+  g.green_kernel = 0;
+  g.cell = 0.f;
+  g.transfer = nullptr;
+  g.radial = nullptr;
+  g.radial_len = 0;
+  g.post_scale = sim.post;
+  const Mesh3 m = sim.m;
+  const SpecTables t = sim.t;
+  const uint32_t nzh = (uint32_t)(m.nz / 2 + 1), ny = (uint32_t)m.ny;
+  const uint32_t total = (uint32_t)m.half_cells(), groups = total / 4;
+  const float4* s4 = reinterpret_cast<const float4*>(sim.rho_hat);
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+    const uint32_t j = 4 * q, r = j / nzh, x = r / ny;
+    int ix = (int)x, iy = (int)(r - x * ny), iz = (int)(j - r * nzh);
+    const float4 a = s4[2 * q], b = s4[2 * q + 1];
+    const float2 v[4] = {make_float2(a.x, a.y), make_float2(a.z, a.w), make_float2(b.x, b.y), make_float2(b.z, b.w)};
+    float2 o[4][3];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      green_gradient_value(v[e], (int64_t)j + e, ix, iy, iz, m, t, g, o[e]);
+      if (++iz == (int)nzh) {
+        iz = 0;
+        if (++iy == (int)ny) {
+          iy = 0;
+          ++ix;
+        }
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      float4* g4 = reinterpret_cast<float4*>(sim.grad_hat + (int64_t)d * total);
+      g4[2 * q] = make_float4(o[0][d].x, o[0][d].y, o[1][d].x, o[1][d].y);
+      g4[2 * q + 1] = make_float4(o[2][d].x, o[2][d].y, o[3][d].x, o[3][d].y);
+    }
   }
 }
 
@@ -440,8 +489,26 @@ int run_stage(Ensemble* e, int stage, int drift, int kick, cudaStream_t s) {
       }
       break;
     case kStGreen:
-      if (e->nspec > 0 && e->any_cufft)
-        ens_green_kernel<<<grid_of(e, kStGreen, e->nspec), e->threads[kStGreen], 0, s>>>(d);
+      if (e->nspec > 0 && e->any_cufft) {
+        // classes whose half spectra split into aligned groups of four run the
+        // class kernel; any other cuFFT member takes the flat kernel
+        bool flat = false;
+        for (const EnsClass& c : e->classes) {
+          if (e->sims[c.first].pm) continue;
+          const int64_t hc = c.m.half_cells();
+          if (hc % 4 != 0 || (e->spec_start[c.first] & 3) != 0) {
+            flat = true;
+            continue;
+          }
+          const int th = e->threads[kStGreen];
+          int64_t bx = (hc / 4 + th - 1) / th;
+          const int64_t cap = ((int64_t)e->nsm * e->ctas_per_sm[kStGreen] + c.count - 1) / c.count;
+          if (bx > cap) bx = cap;
+          ens_green_class_kernel<<<dim3((unsigned)(bx > 0 ? bx : 1), (unsigned)c.count), th, 0, s>>>(e->d_sims,
+                                                                                                  c.first);
+        }
+        if (flat) ens_green_kernel<<<grid_of(e, kStGreen, e->nspec), e->threads[kStGreen], 0, s>>>(d, 1);
+      }
       break;
     case kStC2R:
       for (const EnsClass& c : e->classes)
