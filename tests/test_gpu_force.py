@@ -144,6 +144,31 @@ def test_kick_adj2_matches_separate_kernels(two, zero):
     torch.testing.assert_close(d1, d2, rtol=1e-12, atol=1e-9)
 
 
+@pytest.mark.parametrize("two", [0, 1])
+def test_kick_adj3_matches_drift_cot_then_kick_adj2(two):
+    """The drift cotangent folded into the kick adjoints' pass gives the
+    separate pmb_drift_cot_adj + pmb_kick_adj2 results bit for bit (the dots to
+    summation-order rounding)."""
+    from pmpp_b200._lib import call
+    from pmpp_b200.runtime import stream_handle
+    g = torch.Generator().manual_seed(9)
+    n = 3 * 100003
+    vel, acc, vc, ac, dc = (torch.randn(n, generator=g).cuda() for _ in range(5))
+    s = stream_handle(vel.device)
+    ka, kb, dd = 0.37, -1.21, 0.83
+    v1, w1, c1 = vel.clone(), vc.clone(), ac.clone()
+    d1 = torch.zeros(4, dtype=torch.float64, device="cuda")
+    call("pmb_drift_cot_adj", v1.data_ptr(), dc.data_ptr(), w1.data_ptr(), n, dd, d1[3:].data_ptr(), s)
+    call("pmb_kick_adj2", v1.data_ptr(), acc.data_ptr(), w1.data_ptr(), c1.data_ptr(), n, ka, kb, two, 0,
+         d1[0:].data_ptr(), d1[1:].data_ptr(), d1[2:].data_ptr(), s)
+    v2, w2, c2 = vel.clone(), vc.clone(), ac.clone()
+    d2 = torch.zeros(4, dtype=torch.float64, device="cuda")
+    call("pmb_kick_adj3", v2.data_ptr(), acc.data_ptr(), w2.data_ptr(), c2.data_ptr(), n, ka, kb, two, 0,
+         d2[0:].data_ptr(), d2[1:].data_ptr(), d2[2:].data_ptr(), dc.data_ptr(), dd, d2[3:].data_ptr(), s)
+    assert torch.equal(v1, v2) and torch.equal(w1, w2) and torch.equal(c1, c2)
+    torch.testing.assert_close(d1, d2, rtol=1e-12, atol=1e-9)
+
+
 @pytest.mark.parametrize("staged", [False, True])
 def test_reverse_sweep_overlap_matches_sequential(staged):
     """The force recompute on a side stream gives the sequential sweep's result."""
