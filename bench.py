@@ -130,6 +130,25 @@ def stage_mix(stage, counts, N, M, conf, live):
     return alg, traffic, (parts if len(parts) > 1 else None)
 
 
+# CIC stage groups whose combined fraction of the HBM peak the line reports:
+# the forward pair (deposit + force gather) and the adjoint CIC stages.
+CIC_GROUPS = {"scatter+gather": ("scatter", "gather"),
+              "adjoint": ("gather_adjoint", "scatter3", "scatter_adjoint")}
+
+
+def cic_fractions(breakdown, counts, N, M, conf, live, peak):
+    """Combined fraction of the HBM peak of each CIC group: the group's
+    algorithmic bytes over the group's device time, per run."""
+    out = {}
+    for name, stages in CIC_GROUPS.items():
+        if not all(s in breakdown for s in stages):
+            continue
+        byts = sum(stage_mix(s, counts, N, M, conf, live)[0] * breakdown[s]["launches"] for s in stages)
+        ms = sum(breakdown[s]["ms_total"] for s in stages)
+        out[name] = round(byts / (ms * 1e-3) / 1e9 / peak, 3)
+    return out
+
+
 def live_fractions(conf):
     """(fy, fz): live fractions of ky and kz (nz/2+1 values) of the pass chain
     pruned to the particle-Nyquist box, or None when the chain is not pruned."""
@@ -332,6 +351,7 @@ def run_ours(args):
         except KeyError:
             continue
         b["frac"] = round(ab / (b["ms_total"] / b["launches"] * 1e-3) / 1e9 / peak, 3)
+    cic = cic_fractions(breakdown, counts, N, M, conf, live, peak)
     learned = None
     wpath = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pmpp_b200", "data", "learned_green_c3.npy")
     if world == 1 and not args.no_learned and os.path.exists(wpath):
@@ -355,6 +375,7 @@ def run_ours(args):
                      "traffic_source": "ncu captures at 256^3/512^3 (each launch variant) scaled by particles",
                      "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms, "launch_mix": mix},
         "breakdown": breakdown,
+        "cic_roofline": cic,
         "cpu_baseline": cpu,
         "e2e": {"value": world * N * args.nsteps / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},

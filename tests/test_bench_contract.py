@@ -56,6 +56,28 @@ def test_roofline_byte_models():
     want = (3 * algorithmic_bytes("gather_kick", N, M) + 5 * algorithmic_bytes("gather_kick_only", N, M)
             + 2 * algorithmic_bytes("gather", N, M)) / 10
     assert abs(alg - want) < 1 and mix == {"gather_kick": 3, "gather_kick_only": 5, "gather": 2}
+    # combined fraction of a CIC group: total bytes over total time
+    bd = {"scatter": {"ms_total": 2.0, "launches": 2}, "gather": {"ms_total": 5.0, "launches": 10}}
+    peak = 1000.0
+    fr = b.cic_fractions(bd, dict(counts, scatter=2), N, M, conf, None, peak)
+    tot = 2 * algorithmic_bytes("scatter", N, M) + 10 * want
+    assert abs(fr["scatter+gather"] - round(tot / 7e-3 / 1e9 / peak, 3)) < 1e-9 and "adjoint" not in fr
+
+
+def test_pruned_byte_models():
+    """Live fractions of the 512^3 / 1024^3 chain and the pruned pass bytes."""
+    import pmpp_b200 as pb
+    from pmpp_b200.roofline import algorithmic_bytes
+    b = _bench()
+    conf = pb.Configuration(2.0, (512,) * 3, 2, device="cpu")
+    fy, fz = b.live_fractions(conf)
+    assert fy == 513 / 1024 and fz == 257 / 513
+    M, Mc = 1024 ** 3, 1024 * 1024 * 513
+    full = algorithmic_bytes("fft_x_green", 0, M, Mc=Mc)
+    assert algorithmic_bytes("fft_x_green", 0, M, Mc=Mc, live=(fy, fz)) == full * fy * fz
+    assert algorithmic_bytes("fft_y", 0, M, Mc=Mc, live=(fy, fz)) == 8 * Mc * fz * (1 + fy)
+    assert algorithmic_bytes("gather", 512 ** 3, M, live=(fy, fz)) == algorithmic_bytes("gather", 512 ** 3, M)
+    assert b.live_fractions(pb.Configuration(2.0, (64,) * 3, 1, device="cpu")) is None
 
 
 def test_gpus_flag_self_launches_ranks():
