@@ -136,3 +136,45 @@ def test_process_group_exchanges_match_local_comm():
         assert bool(((slab.owner(s[0], s[1])) == r).all())
         keys = slab.cell_key(s[0], s[1])
         assert bool((keys[1:] >= keys[:-1]).all())  # merged in cell-key order
+
+
+def _rank_capacity(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from pmpp_b200.slab import ProcessGroupComm, SlabPM
+        conf = _conf()
+        slab = SlabPM(conf, ProcessGroupComm(), capacity=600)
+        states = slab.distribute(*_particles(conf))
+        for s in states:  # most particles move to the other rank
+            s.disp = s.disp + torch.tensor([slab.nxl * slab.conf.cell_size * 0.9, 0.0, 0.0])
+        try:
+            slab.migrate(states)
+            q.put((rank, "moved"))
+        except RuntimeError as e:
+            q.put((rank, str(e)))
+        # the group still works after the refusal: no rank was left inside a collective
+        q.put((rank, slab.comm.allreduce_sum(1.0)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_process_group_routing_fails_closed_on_every_rank():
+    """A capacity below a rank's incoming share makes every rank raise the same
+    error before any particle moves, and the process group stays usable."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_capacity, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=240) for _ in range(4)]
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    msgs = [m for _, m in got if isinstance(m, str)]
+    sums = [m for _, m in got if not isinstance(m, str)]
+    assert len(msgs) == 2 and all("capacity" in m for m in msgs) and msgs[0] == msgs[1]
+    assert sums == [2.0, 2.0]
