@@ -1,8 +1,9 @@
 """Slab decomposition's exchanges over real process groups (gloo, world size
 2, CPU): particle routing, the mesh halo shifts and the distributed rFFT
 transposes give what the one-process LocalComm gives, and the distributed
-transform with a plain multiplier equals the full numpy transform.  The
-device kernels (deposit, gather, Green multiplier) are covered on the GPU by
+transform with a plain multiplier equals the full numpy transform; a routing
+over capacity raises the same error on every rank and leaves the group
+usable.  The device kernels (deposit, gather, Green multiplier) are covered on the GPU by
 tests/test_gpu_slab.py; here the multiplier is a torch restatement.
 """
 import os
