@@ -556,6 +556,10 @@ int pmb_scatter_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx
                       double val, const double* mesh_cot, double* disp_cot, void* stream);
 int pmb_pk_shells64(const void* spec, int nx, int ny, int nz, const double* sinc_tab, int mas_power, int num_shells,
                     double* sums, void* stream);
+/* float64 form of pmb_pk_shells_adjoint (power_spectrum.py:120-143 transposed):
+ * out = 2 spec W^-2p wshell[shell] * post, complex128 half spectra. */
+int pmb_pk_shells_adjoint64(const void* spec, int nx, int ny, int nz, const double* sinc_tab, int mas_power,
+                            int num_shells, const double* wshell, double post, void* out, void* stream);
 int pmb_overdensity64(const double* rho, double* delta, int64_t n, const double* total, void* stream);
 
 /* ---------------- ensembles of independent simulations --------------------

@@ -138,6 +138,7 @@ _SIGS = {
     "pmb_lpt64": (c_int, [c_p, c_int, c_int, c_int, c_d, c_d, c_p, c_int, c_d, c_d, c_d, c_d, c_p, c_p, c_p, c_i64, c_d,
                           c_p, c_p, c_i64, c_p]),
     "pmb_pk_shells64": (c_int, [c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_p]),
+    "pmb_pk_shells_adjoint64": (c_int, [c_p, c_int, c_int, c_int, c_p, c_int, c_int, c_p, c_d, c_p, c_p]),
     "pmb_overdensity64": (c_int, [c_p, c_p, c_i64, c_p, c_p]),
     "pmb_ens_create": (c_int, [c_int, c_p, c_p, c_p, c_p, c_p, c_p, c_int, c_p]),
     "pmb_ens_destroy": (c_int, [c_p]),
@@ -200,7 +201,7 @@ _KERNELS = {
     "pmb_overdensity": 1, "pmb_ens_force": 7, "pmb_ens_step": 9, "pmb_ens_set_step": 1,
     "pmb_force64": 5, "pmb_deposit64": 1, "pmb_axpy64": 1, "pmb_sum64": 1, "pmb_force_vjp64": 4, "pmb_dot64": 1, "pmb_lpt64_ex": 4, "pmb_lpt_vjp64": 6,
     "pmb_scatter_vjp64": 1, "pmb_white_noise_nested64": 1,
-    "pmb_linear_modes64": 1, "pmb_lpt64": 4, "pmb_pk_shells64": 1, "pmb_overdensity64": 1,
+    "pmb_linear_modes64": 1, "pmb_lpt64": 4, "pmb_pk_shells64": 1, "pmb_pk_shells_adjoint64": 1, "pmb_overdensity64": 1,
     "pmb_pmfft_z": 1, "pmb_pmfft_col": 1, "pmb_pmfft_z2": 1, "pmb_pmfft_col2": 1,
 }
 _pmfft = {"enabled": True}

@@ -633,6 +633,14 @@ int pmb_pk_shells64(const void* spec, int nx, int ny, int nz, const double* sinc
   return pk_shells64((const double2*)spec, Mesh3{nx, ny, nz}, sinc_tab, mas_power, num_shells, sums, s);
 }
 
+int pmb_pk_shells_adjoint64(const void* spec, int nx, int ny, int nz, const double* sinc_tab, int mas_power,
+                            int num_shells, const double* wshell, double post, void* out, void* stream) {
+  F64_REQUIRE(valid64(nx, ny, nz) && num_shells > 0, "pmb_pk_shells_adjoint64: bad arguments");
+  F64_REQUIRE(spec && sinc_tab && wshell && out, "pmb_pk_shells_adjoint64: null buffer");
+  return pk_shells_adjoint64((const double2*)spec, Mesh3{nx, ny, nz}, sinc_tab, mas_power, num_shells, wshell, post,
+                             (double2*)out, S(stream));
+}
+
 int pmb_overdensity64(const double* rho, double* delta, int64_t n, const double* total, void* stream) {
   return overdensity64(rho, delta, n, total, S(stream));
 }

@@ -641,12 +641,16 @@ int pk_shells64(const double2* spec, Mesh3 m, const double* sinc_tab, int mas_po
 // times the normalisation), out = 2 * spec * deconv * w_shell * (1/mult) so
 // that M * irfftn(out) is the real-field cotangent (rfftn^T for the
 // Hermitian-consistent spectrum).
-__global__ void pk_shells_adjoint_kernel(const float2* __restrict__ spec, Mesh3 m, const float* __restrict__ sinc_tab,
-                                         int mas_power, int num_shells, const double* __restrict__ wshell,
-                                         float post, float2* __restrict__ out) {
-  const float* sx = sinc_tab;
-  const float* sy = sx + m.nx;
-  const float* sz = sy + m.ny;
+// T = double: the float64 build's form, with the same operations in double.
+template <class T>
+__global__ void pk_shells_adjoint_kernel(const typename Real<T>::T2* __restrict__ spec, Mesh3 m,
+                                         const T* __restrict__ sinc_tab, int mas_power, int num_shells,
+                                         const double* __restrict__ wshell, T post,
+                                         typename Real<T>::T2* __restrict__ out) {
+  using R = Real<T>;
+  const T* sx = sinc_tab;
+  const T* sy = sx + m.nx;
+  const T* sz = sy + m.ny;
   const int64_t total = m.half_cells();
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
     const Idx3 q = unravel_half(j, m);
@@ -654,22 +658,30 @@ __global__ void pk_shells_adjoint_kernel(const float2* __restrict__ spec, Mesh3 
     const long long n2 = mx * mx + my * my + mz * mz;
     int shell = (int)floor(sqrt((double)n2) + 1e-9);
     if (shell > num_shells - 1) shell = num_shells - 1;
-    float deconv = 1.0f;
+    T deconv = (T)1;
     if (mas_power > 0) {
-      const float w = __fmul_rn(__fmul_rn(sx[q.ix], sy[q.iy]), sz[q.iz]);
-      deconv = powf(w, (float)(-2 * mas_power));
+      const T w = R::mul(R::mul(sx[q.ix], sy[q.iy]), sz[q.iz]);
+      deconv = R::pow_(w, (T)(-2 * mas_power));
     }
     // the multiplicity cancels against the 1/mult of the rFFT transpose
-    const float f = __fmul_rn(__fmul_rn(2.0f * (float)wshell[shell], deconv), post);
-    const float2 a = spec[j];
-    out[j] = make_float2(__fmul_rn(a.x, f), __fmul_rn(a.y, f));
+    const T f = R::mul(R::mul((T)2 * (T)wshell[shell], deconv), post);
+    const typename R::T2 a = spec[j];
+    out[j] = R::make2(R::mul(a.x, f), R::mul(a.y, f));
   }
 }
 
 int pk_shells_adjoint(const float2* spec, Mesh3 m, const float* sinc_tab, int mas_power, int num_shells,
                       const double* wshell, float post, float2* out, cudaStream_t s) {
-  pk_shells_adjoint_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(spec, m, sinc_tab, mas_power, num_shells,
-                                                                         wshell, post, out);
+  pk_shells_adjoint_kernel<float><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(spec, m, sinc_tab, mas_power,
+                                                                                num_shells, wshell, post, out);
+  PMB_CUDA_CHECK(cudaGetLastError());
+  return kOk;
+}
+
+int pk_shells_adjoint64(const double2* spec, Mesh3 m, const double* sinc_tab, int mas_power, int num_shells,
+                        const double* wshell, double post, double2* out, cudaStream_t s) {
+  pk_shells_adjoint_kernel<double><<<grid_for(m.half_cells(), 256), 256, 0, s>>>(spec, m, sinc_tab, mas_power,
+                                                                                 num_shells, wshell, post, out);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
 }

@@ -60,6 +60,8 @@ int lpt_modes_adjoint64(const double2* F1, const double2* FS, const double* amp,
                         const double* tab, double scale, cudaStream_t s);
 int pk_shells64(const double2* spec, Mesh3 m, const double* sinc_tab, int mas_power, int num_shells, double* sums,
                 cudaStream_t s);
+int pk_shells_adjoint64(const double2* spec, Mesh3 m, const double* sinc_tab, int mas_power, int num_shells,
+                        const double* wshell, double post, double2* out, cudaStream_t s);
 int overdensity64(const double* rho, double* delta, int64_t n, const double* total, cudaStream_t s);
 
 }  // namespace pmb

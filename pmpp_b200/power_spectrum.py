@@ -179,7 +179,11 @@ def pk_loss(ptcl, conf, pk_target, mas="CIC", grad=True, kmax=None):
 
     Forward: scatter -> delta = rho/mean - 1 -> rFFT -> FP64 shell sums.
     Backward: shell-power adjoint -> C2R -> overdensity adjoint (including the
-    mean) -> scatter adjoint (cic/scatter.py:386-437)."""
+    mean) -> scatter adjoint (cic/scatter.py:386-437).  float64 particles take
+    the float64 build (x64.pk_loss)."""
+    if ptcl.disp.dtype == torch.float64:
+        from . import x64
+        return x64.pk_loss(ptcl, conf, pk_target, mas_power=_mas(mas), grad=grad, kmax=kmax)
     nx, ny, nz = conf.mesh_shape
     dev = ptcl.disp.device
     s = stream_handle(dev)

@@ -317,3 +317,52 @@ def density_to_pk(rho, conf, mas_power=2):
 
 def particles_to_pk(ptcl, conf, mas_power=2):
     return density_to_pk(scatter(ptcl, conf), conf, mas_power)
+
+
+def pk_loss(ptcl, conf, pk_target, mas_power=2, grad=True, kmax=None):
+    """The P(k) loss of power_spectrum.pk_loss in float64 (deposit, overdensity,
+    D2Z, shell sums) and its displacement cotangent through the transposed
+    stages: shell-power adjoint, Z2D, the overdensity's adjoint (the mean
+    included) and the deposit's position term (cic/scatter.py:386-437)."""
+    from .power_spectrum import _finalize, num_shells
+    nx, ny, nz = conf.mesh_shape
+    dev = ptcl.disp.device
+    s = stream_handle(dev)
+    rho = scatter(ptcl, conf)
+    tot = torch.zeros(1, dtype=torch.float64, device=dev)
+    call("pmb_sum64", rho.data_ptr(), rho.numel(), tot.data_ptr(), s)
+    delta = torch.empty_like(rho)
+    call("pmb_overdensity64", rho.data_ptr(), delta.data_ptr(), rho.numel(), tot.data_ptr(), s)
+    spec = torch.empty((nx, ny, nz // 2 + 1), dtype=torch.complex128, device=dev)
+    w = workspace(lib().pmb_fft64_work_bytes(nx, ny, nz, 1), dev, "fft64")
+    call("pmb_rfft3_64", nx, ny, nz, 1, delta.data_ptr(), spec.data_ptr(), w.data_ptr(), s)
+    ns = num_shells(conf)
+    sinc = _sinc_tables64(conf, dev)
+    sums = torch.empty(ns, dtype=torch.float64, device=dev)
+    call("pmb_pk_shells64", spec.data_ptr(), nx, ny, nz, sinc.data_ptr(), mas_power, ns, sums.data_ptr(), s)
+    k, pk, nmodes = _finalize(sums, conf)
+    tgt = np.asarray(pk_target, dtype=np.float64)
+    valid = (nmodes > 0) & (pk > 0) & (tgt > 0)
+    if kmax is not None:
+        valid &= k <= kmax
+    lr = np.where(valid, np.log(np.where(valid, pk, 1.0) / np.where(valid, tgt, 1.0)), 0.0)
+    nv = max(int(valid.sum()), 1)
+    loss = float((lr**2).sum() / nv)
+    if not grad:
+        return loss, None
+    norm = conf.cell_size**3 / conf.mesh_size
+    wsh = np.zeros(ns)
+    wsh[1:] = np.where(valid, 2 * lr / nv / np.where(valid, pk, 1.0), 0.0) * norm / np.maximum(nmodes, 1)
+    wd = torch.from_numpy(wsh).to(dev)
+    gspec = torch.empty_like(spec)
+    call("pmb_pk_shells_adjoint64", spec.data_ptr(), nx, ny, nz, sinc.data_ptr(), mas_power, ns, wd.data_ptr(), 1.0,
+         gspec.data_ptr(), s)
+    dcot = torch.empty((nx, ny, nz), dtype=torch.float64, device=dev)
+    call("pmb_irfft3_64", nx, ny, nz, 1, gspec.data_ptr(), dcot.data_ptr(), w.data_ptr(), s)
+    # delta = rho / m - 1 with m = sum(rho)/M:  rho_cot = dcot/m - sum(dcot*rho)/(m^2 M)
+    dd = torch.zeros(1, dtype=torch.float64, device=dev)
+    call("pmb_dot64", dcot.data_ptr(), rho.data_ptr(), rho.numel(), dd.data_ptr(), s)
+    m = float(tot.item()) / rho.numel()
+    rho_cot = dcot.mul_(1.0 / m).sub_(float(dd.item()) / (m * m * rho.numel()))
+    disp_cot, _ = scatter_vjp(ptcl, conf, rho_cot)
+    return loss, disp_cot

@@ -185,3 +185,55 @@ def test_density_loss_gradient_float64_finite_differences():
     u = torch.from_numpy(rng.normal(size=omega.shape) + 1j * rng.normal(size=omega.shape)).cuda()
     fd = _mode_fd(L, omega, u, 1e-4)
     np.testing.assert_allclose(_cdot(g, u), fd, rtol=1e-6)
+
+
+def test_pk_loss_gradient_float64_finite_differences():
+    """The float64 P(k) loss (deposit, overdensity, D2Z, shell sums) and its
+    displacement cotangent (shell-power adjoint, Z2D, overdensity and deposit
+    adjoints) against fourth-order differences (1e-6)."""
+    import pmpp_b200 as pb
+    from pmpp_b200.power_spectrum import pk_loss
+    pb_, co, conf = _confs(16, 2)
+    pmid, disp, vel, ptcl = _state(co, conf, pb, 3, 1.5, 0.0)
+    k, pk, _ = pb.particles_to_pk(ptcl, conf)
+    rng = np.random.default_rng(11)
+    target = np.asarray(pk) * rng.uniform(0.5, 1.5, size=len(pk))
+    loss, dc = pk_loss(ptcl, conf, target)
+    assert dc.dtype == torch.float64 and loss > 0
+    u = rng.normal(size=disp.shape)
+    u /= np.linalg.norm(u)
+
+    def L(d):
+        p = pb.Particles(conf, ptcl.pmid, torch.from_numpy(d).cuda())
+        return pk_loss(p, conf, target, grad=False)[0]
+
+    eps = 1e-5
+    fd = (-L(disp + 2 * eps * u) + 8 * L(disp + eps * u) - 8 * L(disp - eps * u) + L(disp - 2 * eps * u)) / (12 * eps)
+    np.testing.assert_allclose(float((dc.cpu().numpy() * u).sum()), fd, rtol=1e-6)
+
+
+def test_pk_loss_modes_gradient_float64_finite_differences():
+    """The float64 forward model's P(k)-loss gradient w.r.t. the white-noise
+    modes (ForwardModel.loss + backward: 2LPT, two KDK steps, the P(k) loss)
+    against differences (1e-6)."""
+    import pmpp_b200 as pb
+    from pmpp_b200 import pipeline
+    a = np.linspace(0.1, 0.5, 3)
+    conf = pb.Configuration(8.0, (8, 8, 8), 2, a_start=0.1, a_custom=a, float_dtype="float64", device="cuda")
+    cos = pb.boltzmann(pb.SimpleLCDM(conf))
+    omega = pb.white_noise_nested(4, conf)
+    model = pipeline.ForwardModel(conf, cos)
+    model.forward(omega)
+    _, pk0, _ = pb.particles_to_pk(model.final, conf)
+    rng = np.random.default_rng(12)
+    target = np.asarray(pk0) * rng.uniform(0.6, 1.4, size=len(pk0))
+    loss, dc = model.loss(target)
+    g = model.backward(dc)["modes"]
+
+    def L(w):
+        model.forward(w)
+        return model.loss(target, grad=False)[0]
+
+    u = torch.from_numpy(rng.normal(size=omega.shape) + 1j * rng.normal(size=omega.shape)).cuda()
+    # step 1e-5: at 1e-4 the difference's own truncation error is about 2e-4 relative
+    np.testing.assert_allclose(_cdot(g, u), _mode_fd(L, omega, u, 1e-5), rtol=1e-6)
