@@ -118,6 +118,11 @@ def linear_modes_param_cotangents(omega, modes_cot, cosmo, conf, a=None, h=1e-6)
     A_s enters as sqrt(A_s) (exact); Omega_m through the transfer function and
     the explicit 1/Omega_m: the modes are re-evaluated with the transfer table
     differentiated in FP64 (central difference of the analytic fit)."""
+    if conf.float_dtype == torch.float64:
+        if a is not None:
+            raise NotImplementedError("the float64 build takes the linear modes at a = 1")
+        from . import x64
+        return x64.linear_modes_param_cotangents(omega, modes_cot, cosmo, conf, h=h)
     dev = omega.device
     s = stream_handle(dev)
     lin = torch.empty_like(omega)

@@ -56,11 +56,10 @@ class ForwardModel:
         mc_lin, om_lpt = _lpt.lpt_vjp(self.lpt, c0.disp, c0.vel, cosmo, conf)
         mc_noise = mc_lin * self.amp
         if conf.float_dtype == torch.float64:
-            # float64 build: the modes gradient; the linear modes' cosmology
-            # cotangents exist in float32 only
-            return {"modes": mc_noise, "Omega_m": None, "A_s_1e9": None,
-                    "Omega_m_parts": (om_nbody, om_lpt, None)}
-        dAs, om_lin = _modes.linear_modes_param_cotangents(self.omega, mc_lin, cosmo, conf)
+            from . import x64
+            dAs, om_lin = x64.linear_modes_param_cotangents(self.omega, mc_lin, cosmo, conf)
+        else:
+            dAs, om_lin = _modes.linear_modes_param_cotangents(self.omega, mc_lin, cosmo, conf)
         return {"modes": mc_noise, "Omega_m": om_nbody + om_lpt + om_lin, "A_s_1e9": dAs,
                 "Omega_m_parts": (om_nbody, om_lpt, om_lin)}
 

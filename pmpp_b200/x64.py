@@ -6,9 +6,9 @@ With ``Configuration(..., float_dtype="float64")`` the public functions
 operations as the float32 kernels, evaluated in double precision on the
 device (cuFFT D2Z / Z2D, double-precision CIC deposit and gather), for parity
 with the reference's float64 results.  The adjoints of the N-body run, the
-force, the LPT displacements and the deposit exist here too (``nbody_adj``,
-``force_vjp``, ``lpt_vjp``, ``scatter_vjp``); the P(k) loss adjoint and the
-cosmology cotangents of the linear modes are float32 only.
+force, the LPT displacements, the deposit, the P(k) loss and the linear
+modes' cosmology parameters exist here too (``nbody_adj``, ``force_vjp``,
+``lpt_vjp``, ``scatter_vjp``, ``pk_loss``, ``linear_modes_param_cotangents``).
 """
 from __future__ import annotations
 
@@ -34,17 +34,50 @@ def white_noise_nested(seed, conf, device=None):
 
 def linear_modes(modes, cosmo, conf):
     """delta(k) = omega(k) sqrt(V P_lin(|k|)) at a = 1 (modes.py:397-454)."""
+    return _linear_with(modes.to(torch.complex128).contiguous(), cosmo, conf, cosmo.transfer)
+
+
+def _linear_with(modes, cosmo, conf, transfer):
     dev = modes.device
     gx, gy, gz = conf.ptcl_grid_shape
-    modes = modes.to(torch.complex128).contiguous()
     out = torch.empty_like(modes)
     k = torch.from_numpy(np.concatenate(conf.kvec_spacing).astype(np.float64)).to(dev)
     tk = torch.from_numpy(np.ascontiguousarray(conf.transfer_k, dtype=np.float64)).to(dev)
-    tt = torch.from_numpy(np.ascontiguousarray(cosmo.transfer, dtype=np.float64)).to(dev)
+    tt = torch.from_numpy(np.ascontiguousarray(transfer, dtype=np.float64)).to(dev)
     call("pmb_linear_modes64", modes.data_ptr(), out.data_ptr(), gx, gy, gz, k.data_ptr(), tk.data_ptr(),
          tt.data_ptr(), int(tk.numel()), float(cosmo.A_s), float(cosmo.n_s), float(cosmo.Omega_m),
          float(cosmo.k_pivot), 1.0, float(conf.box_vol), stream_handle(dev))
     return out
+
+
+def linear_modes_param_cotangents(omega, modes_cot, cosmo, conf, h=1e-6):
+    """(dL/dA_s_1e9, dL/dOmega_m) of the float64 linear modes at a = 1 given
+    their cotangent (modes.py:397-454 differentiated).
+
+    The modes scale as sqrt(A_s), so dL/dA_s = <cot, lin> / (2 A_s).  They are
+    linear in the interpolated transfer function T and carry an explicit
+    1/Omega_m, so dL/dOmega_m = <cot, lin(T + e dT) - lin(T - e dT)> / (2e)
+    - <cot, lin> / Omega_m with dT = dT/dOmega_m, a central difference of the
+    host's FP64 transfer fit; e keeps T - e dT positive, where the kernel's
+    sqrt(T^2) is linear."""
+    from .cosmology import transfer_fit
+    omega = omega.to(torch.complex128).contiguous()
+    mc = torch.view_as_real(modes_cot.to(torch.complex128).contiguous())
+    s = stream_handle(omega.device)
+    n2 = 2 * omega.numel()
+    dots = torch.zeros(3, dtype=torch.float64, device=omega.device)
+    T = np.asarray(cosmo.transfer, np.float64)
+    Tp = transfer_fit(conf.transfer_k, cosmo.replace(Omega_m=cosmo.Omega_m + h), conf)
+    Tm = transfer_fit(conf.transfer_k, cosmo.replace(Omega_m=cosmo.Omega_m - h), conf)
+    dT = (np.asarray(Tp, np.float64) - np.asarray(Tm, np.float64)) / (2 * h)
+    eps = 1e-2
+    while np.any(T[1:] - eps * np.abs(dT[1:]) <= 0):
+        eps *= 0.5
+    for i, tab in enumerate((T, T + eps * dT, T - eps * dT)):
+        lin = torch.view_as_real(_linear_with(omega, cosmo, conf, tab))
+        call("pmb_dot64", mc.data_ptr(), lin.data_ptr(), n2, dots[i:].data_ptr(), s)
+    d = dots.cpu().numpy()
+    return float(d[0] / (2 * cosmo.A_s_1e9)), float((d[1] - d[2]) / (2 * eps) - d[0] / cosmo.Omega_m)
 
 
 def linear_amplitude(cosmo, conf, device=None):

@@ -237,3 +237,39 @@ def test_pk_loss_modes_gradient_float64_finite_differences():
     u = torch.from_numpy(rng.normal(size=omega.shape) + 1j * rng.normal(size=omega.shape)).cuda()
     # step 1e-5: at 1e-4 the difference's own truncation error is about 2e-4 relative
     np.testing.assert_allclose(_cdot(g, u), _mode_fd(L, omega, u, 1e-5), rtol=1e-6)
+
+
+def test_cosmology_gradients_float64_finite_differences():
+    """The float64 forward model's P(k)-loss gradients w.r.t. Omega_m (at fixed
+    A_s; growth factors, LPT, force and the linear modes' transfer function) and
+    A_s_1e9 against fourth-order differences of the same float64 model with the
+    cosmology tables rebuilt at each shifted parameter."""
+    import pmpp_b200 as pb
+    from pmpp_b200 import pipeline
+    a = np.linspace(0.1, 0.5, 3)
+    conf = pb.Configuration(8.0, (8, 8, 8), 2, a_start=0.1, a_custom=a, float_dtype="float64", device="cuda")
+    cos = pb.boltzmann(pb.SimpleLCDM(conf))
+    omega = pb.white_noise_nested(4, conf)
+    model = pipeline.ForwardModel(conf, cos)
+    model.forward(omega)
+    _, pk0, _ = pb.particles_to_pk(model.final, conf)
+    rng = np.random.default_rng(13)
+    target = np.asarray(pk0) * rng.uniform(0.6, 1.4, size=len(pk0))
+    _, dc = model.loss(target)
+    g = model.backward(dc)
+
+    def L(**kw):
+        m = pipeline.ForwardModel(conf, pb.boltzmann(cos.replace(**kw)))
+        m.forward(omega)
+        return m.loss(target, grad=False)[0]
+
+    def fd(name, x, h):
+        return (-L(**{name: x + 2 * h}) + 8 * L(**{name: x + h}) - 8 * L(**{name: x - h})
+                + L(**{name: x - 2 * h})) / (12 * h)
+
+    # A_s enters as sqrt(A_s) only: measured 1e-12 apart
+    np.testing.assert_allclose(g["A_s_1e9"], fd("A_s_1e9", cos.A_s_1e9, 1e-4), rtol=1e-8)
+    # Omega_m: measured 1.2e-6 apart at step 1e-4; the adaptive growth solver's
+    # tolerance bounds the difference's own accuracy (1e-5 at step 1e-5, 2e-3
+    # truncation at step 1e-3)
+    np.testing.assert_allclose(g["Omega_m"], fd("Omega_m", cos.Omega_m, 1e-4), rtol=1e-5)
