@@ -492,7 +492,10 @@ int pmb_linear_power(const double* k, int64_t nk, const double* tk, const double
  * optimised path: the deposit uses double atomics without a sort.
  * pmb_force64: optional drift disp += drift_vel * drift, CIC deposit of val,
  * source (rho - 1) * src_mul, D2Z, Green x gradient (tables: float64
- * [kx ky kz cx cy cz (mx my mz)]), 3 x Z2D into force_meshes (3, nx, ny, nz),
+ * [kx ky kz cx cy cz (mx my mz)], the discrete-Laplacian k and FastPM's
+ * derivative when a correction asks for them; transfer: the correction's
+ * float64 multiplier per half-spectrum cell, or NULL, corrections/core.py:
+ * 333-334), 3 x Z2D into force_meshes (3, nx, ny, nz),
  * gather into acc with optional vel_kick += acc * kick (nbody/gravity.py:
  * 786-814, nbody/integrator.py:202-238, 512-538).  pmb_deposit64: the density
  * alone (cic/scatter.py:315-338).  pmb_lpt64 / pmb_linear_modes64 /
@@ -501,8 +504,8 @@ int pmb_linear_power(const double* k, int64_t nk, const double* tk, const double
 int64_t pmb_force64_workspace_bytes(int nx, int ny, int nz);
 int pmb_force64(const int16_t* pmid, double* disp, const double* drift_vel, double drift, int64_t n, int nx, int ny,
                 int nz, double cell, double val, double src_mul, const double* tables, int has_masks,
-                double* force_meshes, double* acc, double* vel_kick, double kick, void* workspace,
-                int64_t workspace_bytes, void* stream);
+                const double* transfer, double* force_meshes, double* acc, double* vel_kick, double kick,
+                void* workspace, int64_t workspace_bytes, void* stream);
 int pmb_deposit64(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz, double cell, double val,
                   double* rho, void* stream);
 int pmb_axpy64(double* y, const double* x, int64_t n, double f, void* stream);
@@ -517,8 +520,9 @@ int pmb_sum64(const double* a, int64_t n, double* out, void* stream);
  * positions. */
 int64_t pmb_force_vjp64_workspace_bytes(int nx, int ny, int nz);
 int pmb_force_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz, double cell,
-                    double val, double src_mul, const double* tables, int has_masks, const double* force_meshes,
-                    const double* acc_cot, double* disp_cot, void* workspace, int64_t workspace_bytes, void* stream);
+                    double val, double src_mul, const double* tables, int has_masks, const double* transfer,
+                    const double* force_meshes, const double* acc_cot, double* disp_cot, void* workspace,
+                    int64_t workspace_bytes, void* stream);
 /* *out += sum a[i] b[i] in float64 (the Omega_m cotangent dots of the float64
  * reverse sweep, nbody/integrator.py:173-199). */
 int pmb_dot64(const double* a, const double* b, int64_t n, double* out, void* stream);

@@ -859,10 +859,13 @@ def nbody_adj(pmid, disp, vel, acc, disp_cot, vel_cot, acc_cot, conf, cosmo, ker
 
     Returns (disp, vel, disp_cot, vel_cot, Omega_m_cot) at the initial time;
     om_terms (a list) receives every term of the Omega_m cotangent's sum (the
-    sum can cancel to far below its terms)."""
+    sum can cancel to far below its terms).  A callable kernel is evaluated
+    at the scale factor of the positions each force sees, as force_adj(a, ...)
+    does (integrator.py:620-686)."""
     om_terms = [] if om_terms is None else om_terms
     ft = conf.float_dtype
     a = conf.a_nbody
+    K = kernel if callable(kernel) else (lambda _a: kernel)
     disp, vel, acc = disp.astype(ft).copy(), vel.astype(ft).copy(), acc.astype(ft).copy()
     dc = disp_cot.astype(np.float64).copy()
     vc = vel_cot.astype(np.float64).copy()
@@ -880,7 +883,7 @@ def nbody_adj(pmid, disp, vel, acc, disp_cot, vel_cot, acc_cot, conf, cosmo, ker
                     om_cot += om_terms[-1]
                 continue
             _, a_vel, a_dp, a_dn, a_acc_in = st
-            g, oc = gravity_vjp(pmid, disp, conf, cosmo.Omega_m, ac, kernel, interlacing=interlacing)
+            g, oc = gravity_vjp(pmid, disp, conf, cosmo.Omega_m, ac, K(a_dn), interlacing=interlacing)
             dc = dc + g
             om_cot += oc
             om_terms.append(oc)
@@ -892,8 +895,8 @@ def nbody_adj(pmid, disp, vel, acc, disp_cot, vel_cot, acc_cot, conf, cosmo, ker
             if om_grads:
                 om_terms.append(_factor_dOm(drift_factor, (a_vel, a_dp, a_dn), cosmo, conf) * float((dc * vel).sum()))
                 om_cot += om_terms[-1]
-            acc = gravity(pmid, disp, conf, cosmo.Omega_m, kernel, interlacing=interlacing).astype(ft)
-    g, oc = gravity_vjp(pmid, disp, conf, cosmo.Omega_m, ac, kernel, interlacing=interlacing)
+            acc = gravity(pmid, disp, conf, cosmo.Omega_m, K(a_dp), interlacing=interlacing).astype(ft)
+    g, oc = gravity_vjp(pmid, disp, conf, cosmo.Omega_m, ac, K(a[0]), interlacing=interlacing)
     dc = dc + g
     om_cot += oc
     om_terms.append(oc)

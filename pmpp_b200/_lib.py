@@ -114,13 +114,13 @@ _SIGS = {
     "pmb_linear_power": (c_int, [c_p, c_i64, c_p, c_p, c_int, c_d, c_d, c_d, c_d, c_d, c_p]),
     "pmb_force64_workspace_bytes": (c_i64, [c_int, c_int, c_int]),
     "pmb_force64": (c_int, [c_p, c_p, c_p, c_d, c_i64, c_int, c_int, c_int, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p,
-                            c_d, c_p, c_i64, c_p]),
+                            c_p, c_d, c_p, c_i64, c_p]),
     "pmb_deposit64": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_d, c_d, c_p, c_p]),
     "pmb_axpy64": (c_int, [c_p, c_p, c_i64, c_d, c_p]),
     "pmb_sum64": (c_int, [c_p, c_i64, c_p, c_p]),
     "pmb_force_vjp64_workspace_bytes": (c_i64, [c_int, c_int, c_int]),
     "pmb_force_vjp64": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p,
-                                c_i64, c_p]),
+                                c_p, c_i64, c_p]),
     "pmb_dot64": (c_int, [c_p, c_p, c_i64, c_p, c_p]),
     "pmb_lpt64_ex": (c_int, [c_p, c_int, c_int, c_int, c_d, c_d, c_p, c_int, c_d, c_d, c_d, c_d, c_p, c_p, c_p, c_i64,
                              c_d, c_p, c_p, c_p, c_i64, c_p]),

@@ -54,14 +54,16 @@ class PMWindowCompensation:
         self._cache = {}
 
     def transfer_tables(self, a, cosmo, conf):
+        """Gain per half-spectrum cell in the configuration's float dtype."""
         if self.alpha == 0:
             return None, None  # gain W^0 = 1 everywhere: no transfer
         dev = conf.device
-        key = (conf.mesh_shape, conf.cell_size, conf.ptcl_spacing, str(dev))
+        key = (conf.mesh_shape, conf.cell_size, conf.ptcl_spacing, str(dev), str(conf.float_dtype))
         if key not in self._cache:
-            kx, ky, kz = [torch.from_numpy(k.astype(np.float32)).to(dev) for k in conf.kvec]
-            c = np.float32(conf.cell_size)
-            two_pi = np.float32(2 * np.pi)
+            f = conf.np_dtype.type
+            kx, ky, kz = [torch.from_numpy(k.astype(conf.np_dtype)).to(dev) for k in conf.kvec]
+            c = f(conf.cell_size)
+            two_pi = f(2 * np.pi)
             sinc = lambda x: torch.where(x == 0, torch.ones_like(x), torch.sin(np.pi * x) / (np.pi * x))
             sx = sinc(kx * c / two_pi)[:, None, None]
             sy = sinc(ky * c / two_pi)[None, :, None]
@@ -71,12 +73,12 @@ class PMWindowCompensation:
             if self.max_gain is not None and self.max_gain > 0:
                 gain = torch.clamp(gain, max=float(self.max_gain))
             if self.taper_stop > self.taper_start:
-                kn = np.float32(np.pi / conf.ptcl_spacing)
+                kn = f(np.pi / conf.ptcl_spacing)
                 q = torch.maximum(torch.maximum(kx.abs()[:, None, None], ky.abs()[None, :, None]),
                                   kz.abs()[None, None, :]) / kn
                 t = torch.clamp((q - self.taper_start) / (self.taper_stop - self.taper_start), 0.0, 1.0)
                 gain = 1.0 + (gain - 1.0) * (1.0 - t * t * (3.0 - 2.0 * t))
-            self._cache[key] = gain.to(torch.float32).contiguous()
+            self._cache[key] = gain.to(conf.float_dtype).contiguous()
         return self._cache[key], None
 
 
@@ -93,23 +95,25 @@ class PGDPotentialCorrection:
         self.alpha0, self.A, self.B, self.kl, self.ks = alpha0, A, B, kl, ks
         self._cache = {}
 
-    def alpha(self, a):
-        f = np.float32
+    def alpha(self, a, f=np.float32):
         return f(self.alpha0) * (f(10.0)**(f(self.A) * f(a)**2 - f(self.B) * f(a)))
 
     def transfer_tables(self, a, cosmo, conf):
+        """Transfer per half-spectrum cell at scale factor a, in the
+        configuration's float dtype."""
         a = 1.0 if a is None else float(a)
-        key = (a, conf.mesh_shape, conf.cell_size, str(conf.device))
+        key = (a, conf.mesh_shape, conf.cell_size, str(conf.device), str(conf.float_dtype))
         if key not in self._cache:
             if len(self._cache) > 64:
                 self._cache.clear()
             dev = conf.device
-            kx, ky, kz = [torch.from_numpy(k.astype(np.float32)).to(dev) for k in conf.kvec]
+            f = conf.np_dtype.type
+            kx, ky, kz = [torch.from_numpy(k.astype(conf.np_dtype)).to(dev) for k in conf.kvec]
             k2 = (kx[:, None, None]**2 + ky[None, :, None]**2) + kz[None, None, :]**2
             safe = torch.where(k2 > 0, k2, torch.ones_like(k2))
-            band = torch.exp(-np.float32(self.kl)**2 / safe - safe**2 / np.float32(self.ks)**4)
+            band = torch.exp(-f(self.kl)**2 / safe - safe**2 / f(self.ks)**4)
             band = torch.where(k2 > 0, band, torch.zeros_like(band))
-            self._cache[key] = (1.0 - float(self.alpha(a)) * band).to(torch.float32).contiguous()
+            self._cache[key] = (1.0 - float(self.alpha(a, f)) * band).to(conf.float_dtype).contiguous()
         return self._cache[key], None
 
 
@@ -128,16 +132,17 @@ class HighKSofteningCorrection:
         self._cache = {}
 
     def transfer_tables(self, a, cosmo, conf):
-        key = (conf.mesh_shape, conf.cell_size, conf.ptcl_spacing, str(conf.device))
+        """Transfer per half-spectrum cell in the configuration's float dtype."""
+        key = (conf.mesh_shape, conf.cell_size, conf.ptcl_spacing, str(conf.device), str(conf.float_dtype))
         if key not in self._cache:
             dev = conf.device
-            kx, ky, kz = [torch.from_numpy(k.astype(np.float32)).to(dev).abs() for k in conf.kvec]
-            kn = np.float32(np.pi / conf.ptcl_spacing)
+            f = conf.np_dtype.type
+            kx, ky, kz = [torch.from_numpy(k.astype(conf.np_dtype)).to(dev).abs() for k in conf.kvec]
+            kn = f(np.pi / conf.ptcl_spacing)
             q = torch.maximum(torch.maximum(kx[:, None, None] / kn, ky[None, :, None] / kn), kz[None, None, :] / kn)
-            t = torch.clamp((q - np.float32(self.start)) / max(np.float32(self.stop - self.start), np.float32(1e-6)),
-                            0.0, 1.0)
+            t = torch.clamp((q - f(self.start)) / max(f(self.stop - self.start), f(1e-6)), 0.0, 1.0)
             taper = t * t * (3.0 - 2.0 * t) if self.mode == "smoothstep" else t
-            self._cache[key] = torch.clamp(1.0 - np.float32(self.strength) * taper, min=0.0).to(torch.float32)
+            self._cache[key] = torch.clamp(1.0 - f(self.strength) * taper, min=0.0).to(conf.float_dtype)
         return self._cache[key], None
 
 

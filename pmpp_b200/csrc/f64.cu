@@ -82,9 +82,11 @@ struct Tables64 {
   const double *kx, *ky, *kz, *cx, *cy, *cz, *mx, *my, *mz;
 };
 
-// Green x gradient in float64: phi = -(S mask) / k^2, grad_d = (i c_d) phi, 1/M folded in.
+// Green x gradient in float64: phi = -(S mask) / k^2 * T, grad_d = (i c_d) phi,
+// 1/M folded in; T the correction's transfer per half-spectrum cell
+// (corrections/core.py:333-334), none when transfer is null.
 __global__ void green64_kernel(const double2* __restrict__ src, double2* __restrict__ grad, Mesh3 m, Tables64 t,
-                               double post) {
+                               double post, const double* __restrict__ transfer) {
   const int nzh = m.nz / 2 + 1;
   const int64_t total = m.half_cells();
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
@@ -103,6 +105,10 @@ __global__ void green64_kernel(const double2* __restrict__ src, double2* __restr
     if (k2 != 0.0) {
       pr = RD::div(-v.x, k2);
       pi = RD::div(-v.y, k2);
+      if (transfer != nullptr) {
+        pr = RD::mul(pr, transfer[j]);
+        pi = RD::mul(pi, transfer[j]);
+      }
     }
     const double c[3] = {t.cx[ix], t.cy[iy], t.cz[iz]};
 #pragma unroll
@@ -213,9 +219,9 @@ __global__ void deposit64v_kernel(const int16_t* __restrict__ pmid, const double
 }
 
 // Transpose of green64_kernel (gravity.py:226-260, 290-321):
-// src_cot = post * mask * (-1/k^2) * sum_d conj(i c_d) A_d, zero at k = 0.
+// src_cot = post * mask * (-1/k^2) * T * sum_d conj(i c_d) A_d, zero at k = 0.
 __global__ void green64_adjoint_kernel(const double2* __restrict__ gc, double2* __restrict__ out, Mesh3 m, Tables64 t,
-                                       double post) {
+                                       double post, const double* __restrict__ transfer) {
   const int nzh = m.nz / 2 + 1;
   const int64_t total = m.half_cells();
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
@@ -234,6 +240,10 @@ __global__ void green64_adjoint_kernel(const double2* __restrict__ gc, double2* 
                               RD::mul(t.kz[iz], t.kz[iz]));
     double pr = 0.0, pi = 0.0;
     if (k2 != 0.0) {
+      if (transfer != nullptr) {
+        sr = RD::mul(sr, transfer[j]);
+        si = RD::mul(si, transfer[j]);
+      }
       pr = RD::div(-sr, k2);
       pi = RD::div(-si, k2);
     }
@@ -386,8 +396,8 @@ int64_t pmb_force64_workspace_bytes(int nx, int ny, int nz) {
 
 int pmb_force64(const int16_t* pmid, double* disp, const double* drift_vel, double drift, int64_t n, int nx, int ny,
                 int nz, double cell, double val, double src_mul, const double* tables, int has_masks,
-                double* force_meshes, double* acc, double* vel_kick, double kick, void* workspace,
-                int64_t workspace_bytes, void* stream) {
+                const double* transfer, double* force_meshes, double* acc, double* vel_kick, double kick,
+                void* workspace, int64_t workspace_bytes, void* stream) {
   Mesh3 m{nx, ny, nz};
   F64_REQUIRE(valid64(nx, ny, nz), "pmb_force64: unsupported mesh shape");
   F64_REQUIRE(n >= 0 && cell > 0.0, "pmb_force64: bad particle count or cell size");
@@ -407,7 +417,7 @@ int pmb_force64(const int16_t* pmid, double* disp, const double* drift_vel, doub
   PMB_CUDA_CHECK(cudaGetLastError());
   F64_TRY(fft_d2z(m, 1, rho, rho_hat, work, s));
   green64_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(rho_hat, grad_hat, m, tables64(tables, m, has_masks),
-                                                               1.0 / (double)m.cells());
+                                                               1.0 / (double)m.cells(), transfer);
   PMB_CUDA_CHECK(cudaGetLastError());
   F64_TRY(fft_z2d(m, 3, grad_hat, force_meshes, work, s));
   if (n > 0) gather64_kernel<<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, n, m, cell, force_meshes, acc, vel_kick, kick);
@@ -423,8 +433,9 @@ int64_t pmb_force_vjp64_workspace_bytes(int nx, int ny, int nz) {
 }
 
 int pmb_force_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz, double cell,
-                    double val, double src_mul, const double* tables, int has_masks, const double* force_meshes,
-                    const double* acc_cot, double* disp_cot, void* workspace, int64_t workspace_bytes, void* stream) {
+                    double val, double src_mul, const double* tables, int has_masks, const double* transfer,
+                    const double* force_meshes, const double* acc_cot, double* disp_cot, void* workspace,
+                    int64_t workspace_bytes, void* stream) {
   Mesh3 m{nx, ny, nz};
   F64_REQUIRE(valid64(nx, ny, nz), "pmb_force_vjp64: unsupported mesh shape");
   F64_REQUIRE(n >= 0 && n < 4294967296ll && cell > 0.0, "pmb_force_vjp64: bad particle count or cell size");
@@ -448,7 +459,7 @@ int pmb_force_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx, 
   PMB_CUDA_CHECK(cudaGetLastError());
   F64_TRY(fft_d2z(m, 3, mesh3, spec3, work, s));
   green64_adjoint_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(spec3, spec1, m, tables64(tables, m, has_masks),
-                                                                       src_mul / (double)m.cells());
+                                                                       src_mul / (double)m.cells(), transfer);
   PMB_CUDA_CHECK(cudaGetLastError());
   F64_TRY(fft_z2d(m, 1, spec1, mesh3, work, s));
   if (n > 0)  // scatter adjoint, position term (scatter.py:366-370)

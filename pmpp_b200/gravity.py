@@ -488,15 +488,15 @@ def force(pmid, disp, conf, omega_m, *, a=None, cosmo=None, correction=None, for
     lane selects the workspace that keeps the sorted records (see force_vjp).
     keep_acc=False with vel_kick: apply the kicks without storing acc (the
     plain route; returns acc None there).
-    float64 displacements take the float64 build (x64.force; no correction,
-    one folded kick)."""
+    float64 displacements take the float64 build (x64.force: the analytic
+    corrections, one folded kick)."""
     require_cuda(pmid, disp, drift_vel, vel_kick)
     if disp.dtype == torch.float64:
-        if correction is not None or kick2 != 0.0 or src_hat_out is not None:
-            raise NotImplementedError("the float64 force takes no correction, one folded kick and no spectrum")
+        if kick2 != 0.0 or src_hat_out is not None:
+            raise NotImplementedError("the float64 force takes one folded kick and no spectrum")
         from . import x64
         return x64.force(pmid, disp, conf, omega_m, acc=acc, force_meshes=force_meshes, drift_vel=drift_vel,
-                         drift=drift, vel_kick=vel_kick, kick=kick)
+                         drift=drift, vel_kick=vel_kick, kick=kick, correction=correction, a=a, cosmo=cosmo)
     n = pmid.shape[0]
     nx, ny, nz = conf.mesh_shape
     dev = disp.device
@@ -547,10 +547,11 @@ def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, *
     where it is not sum(acc_cot acc) / Omega_m (the mesh-CNN correction)."""
     require_cuda(pmid, disp, force_meshes, acc_cot, disp_cot)
     if disp.dtype == torch.float64:
-        if correction is not None or transfer_cot_out is not None:
-            raise NotImplementedError("the float64 force adjoint takes no correction")
+        if transfer_cot_out is not None or src_hat is not None:
+            raise NotImplementedError("the float64 force adjoint trains no correction")
         from . import x64
-        return x64.force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot)
+        return x64.force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot, correction=correction, a=a,
+                             cosmo=cosmo)
     n = pmid.shape[0]
     nx, ny, nz = conf.mesh_shape
     dev = disp.device

@@ -193,10 +193,8 @@ class NBodyRun:
     def forward(self, ptcl, a_nbody=None):
         conf, cosmo = self.conf, self.cosmo
         if conf.float_dtype == torch.float64:
-            if self.correction is not None:
-                raise NotImplementedError("corrections run in the float32 build")
             from . import x64
-            return x64.nbody(ptcl, cosmo, conf, a_nbody)
+            return x64.nbody(ptcl, cosmo, conf, a_nbody, correction=self.correction)
         a = conf.a_nbody if a_nbody is None else np.asarray(a_nbody)
         disp = ptcl.disp.clone()
         vel = ptcl.vel.clone() if ptcl.vel is not None else torch.zeros_like(disp)
@@ -279,10 +277,8 @@ class NBodyRun:
         conf, cosmo, corr = self.conf, self.cosmo, self.correction
         a = conf.a_nbody if a_nbody is None else np.asarray(a_nbody)
         if conf.float_dtype == torch.float64:
-            if corr is not None:
-                raise NotImplementedError("corrections run in the float32 build")
             from . import x64
-            return x64.nbody_adj(ptcl, ptcl_cot, cosmo, conf, a, force_meshes)
+            return x64.nbody_adj(ptcl, ptcl_cot, cosmo, conf, a, force_meshes, correction=corr)
         dev = ptcl.disp.device
         s = stream_handle(dev)
         pmid = ptcl.pmid

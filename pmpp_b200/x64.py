@@ -8,7 +8,8 @@ device (cuFFT D2Z / Z2D, double-precision CIC deposit and gather), for parity
 with the reference's float64 results.  The adjoints of the N-body run, the
 force, the LPT displacements, the deposit, the P(k) loss and the linear
 modes' cosmology parameters exist here too (``nbody_adj``, ``force_vjp``,
-``lpt_vjp``, ``scatter_vjp``, ``pk_loss``, ``linear_modes_param_cotangents``).
+``lpt_vjp``, ``scatter_vjp``, ``pk_loss``, ``linear_modes_param_cotangents``),
+and the force takes the analytic corrections (``correction_tables``).
 """
 from __future__ import annotations
 
@@ -171,9 +172,32 @@ def lpt(modes, cosmo, conf):
     return ptcl
 
 
-def force(pmid, disp, conf, omega_m, acc=None, force_meshes=None, drift_vel=None, drift=0.0, vel_kick=None, kick=0.0):
+def correction_tables(conf, dev, correction=None, a=None, cosmo=None):
+    """Spectral tables and float64 transfer of the force for a correction: the
+    analytic ones (window compensation, FastPM's Green's functions and 4-point
+    gradient, PGD, high-k softening and their products, corrections/core.py:
+    40-151, 333-334, 396-422).  Interlacing, the mesh CNN and the learned
+    radial transfer are float32 only."""
+    if correction is None:
+        return conf.spectral_tables("mesh", dev), None
+    from .gravity import _correction_args, _tables, mesh_cnn_of, uses_interlacing
+    if uses_interlacing(correction) or mesh_cnn_of(correction) is not None:
+        raise NotImplementedError("the float64 build takes the analytic corrections without interlacing")
+    gk, transfer, radial, _ = _correction_args(correction, a, cosmo, conf)
+    if radial is not None:
+        raise NotImplementedError("the float64 build takes no learned radial transfer")
+    if transfer is not None:
+        if transfer.dtype != torch.float64:
+            raise TypeError("the float64 force needs a float64 transfer table")
+        transfer = transfer.to(dev).contiguous()
+    return _tables(conf, dev, gk, correction), transfer
+
+
+def force(pmid, disp, conf, omega_m, acc=None, force_meshes=None, drift_vel=None, drift=0.0, vel_kick=None, kick=0.0,
+          correction=None, a=None, cosmo=None):
     """PM accelerations (gravity.py:786-814) in float64; with drift_vel the
-    drift is applied first, with vel_kick the closing half-kick is fused."""
+    drift is applied first, with vel_kick the closing half-kick is fused; an
+    analytic correction at scale factor a (correction_tables)."""
     nx, ny, nz = conf.mesh_shape
     dev = disp.device
     n = pmid.shape[0]
@@ -181,29 +205,32 @@ def force(pmid, disp, conf, omega_m, acc=None, force_meshes=None, drift_vel=None
         acc = torch.empty((n, 3), dtype=torch.float64, device=dev)
     if force_meshes is None:
         force_meshes = torch.empty((3, nx, ny, nz), dtype=torch.float64, device=dev)
+    tables, transfer = correction_tables(conf, dev, correction, a, cosmo)
     ws = workspace(lib().pmb_force64_workspace_bytes(nx, ny, nz), dev, "force64")
     call("pmb_force64", pmid.data_ptr(), disp.data_ptr(), None if drift_vel is None else drift_vel.data_ptr(),
          float(drift), n, nx, ny, nz, float(conf.cell_size), float(conf.mesh_size / conf.ptcl_num), 1.5 * float(omega_m),
-         conf.spectral_tables("mesh", dev).data_ptr(), int(conf.has_particle_nyquist_masks), force_meshes.data_ptr(),
-         acc.data_ptr(), None if vel_kick is None else vel_kick.data_ptr(), float(kick), ws.data_ptr(), ws.numel(),
-         stream_handle(dev))
+         tables.data_ptr(), int(conf.has_particle_nyquist_masks), None if transfer is None else transfer.data_ptr(),
+         force_meshes.data_ptr(), acc.data_ptr(), None if vel_kick is None else vel_kick.data_ptr(), float(kick),
+         ws.data_ptr(), ws.numel(), stream_handle(dev))
     return acc, force_meshes
 
 
-def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None):
+def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, correction=None, a=None, cosmo=None):
     """disp_cot (+)= (d acc / d disp)^T acc_cot in float64 (pmb_force_vjp64),
-    force_meshes being force()'s at these positions."""
+    force_meshes being force()'s at these positions (same correction and a)."""
     nx, ny, nz = conf.mesh_shape
     dev = disp.device
     n = pmid.shape[0]
     if disp_cot is None:
         disp_cot = torch.zeros((n, 3), dtype=torch.float64, device=dev)
     acc_cot = acc_cot.to(torch.float64).contiguous()
+    tables, transfer = correction_tables(conf, dev, correction, a, cosmo)
     ws = workspace(lib().pmb_force_vjp64_workspace_bytes(nx, ny, nz), dev, "force_vjp64")
     call("pmb_force_vjp64", pmid.data_ptr(), disp.data_ptr(), n, nx, ny, nz, float(conf.cell_size),
-         float(conf.mesh_size / conf.ptcl_num), 1.5 * float(omega_m), conf.spectral_tables("mesh", dev).data_ptr(),
-         int(conf.has_particle_nyquist_masks), force_meshes.data_ptr(), acc_cot.data_ptr(), disp_cot.data_ptr(),
-         ws.data_ptr(), ws.numel(), stream_handle(dev))
+         float(conf.mesh_size / conf.ptcl_num), 1.5 * float(omega_m), tables.data_ptr(),
+         int(conf.has_particle_nyquist_masks), None if transfer is None else transfer.data_ptr(),
+         force_meshes.data_ptr(), acc_cot.data_ptr(), disp_cot.data_ptr(), ws.data_ptr(), ws.numel(),
+         stream_handle(dev))
     return disp_cot
 
 
@@ -217,7 +244,7 @@ def axpy(y, x, f):
     call("pmb_axpy64", y.data_ptr(), x.data_ptr(), y.numel(), float(f), stream_handle(y.device))
 
 
-def nbody_adj(ptcl, ptcl_cot, cosmo, conf, a_nbody=None, force_meshes=None):
+def nbody_adj(ptcl, ptcl_cot, cosmo, conf, a_nbody=None, force_meshes=None, correction=None):
     """Reverse sweep in float64 (nbody/solver.py:385-444; integrator.py:429-509,
     541-582, 620-686, 781-837), stage by stage: a kick adjoint restores vel
     and moves vel_cot into acc_cot; a drift stage takes the force adjoint at
@@ -225,8 +252,9 @@ def nbody_adj(ptcl, ptcl_cot, cosmo, conf, a_nbody=None, force_meshes=None):
     recomputes the acceleration there.  The Omega_m cotangent sums the time
     factors' derivatives times their dots and, per force, sum(acc_cot acc) /
     Omega_m (the force is linear in Omega_m).  force_meshes: force()'s meshes
-    at ptcl's positions (recomputed when None).  Returns (ptcl_in,
-    ptcl_cot_in, Omega_m_cot)."""
+    at ptcl's positions (recomputed when None).  An analytic correction
+    enters every force at its positions' scale factor (correction_tables).
+    Returns (ptcl_in, ptcl_cot_in, Omega_m_cot)."""
     from .nbody import _schedule
     a = conf.a_nbody if a_nbody is None else np.asarray(a_nbody)
     f64 = lambda t: t.to(torch.float64).clone().contiguous()
@@ -237,8 +265,9 @@ def nbody_adj(ptcl, ptcl_cot, cosmo, conf, a_nbody=None, force_meshes=None):
     dc = f64(ptcl_cot.disp) if ptcl_cot.disp is not None else z.clone()
     vc = f64(ptcl_cot.vel) if ptcl_cot.vel is not None else z.clone()
     ac = f64(ptcl_cot.acc) if ptcl_cot.acc is not None else z.clone()
+    kw = dict(correction=correction, cosmo=cosmo)
     if force_meshes is None or ptcl.acc is None:
-        acc, F = force(pmid, disp, conf, cosmo.Omega_m)
+        acc, F = force(pmid, disp, conf, cosmo.Omega_m, a=float(a[-1]), **kw)
     else:
         acc, F = f64(ptcl.acc), force_meshes
     stages = []
@@ -259,7 +288,7 @@ def nbody_adj(ptcl, ptcl_cot, cosmo, conf, a_nbody=None, force_meshes=None):
         dot(ac, acc, dots, slot)
         force_slots.append(slot)
         slot += 1
-        force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc)
+        force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=float(a_dn), **kw)
         ac.zero_()
         D, dD = cosmo.drift_factor(a_vel, a_dp, a_dn, with_grad=True)
         axpy(disp, vel, -D)
@@ -267,10 +296,10 @@ def nbody_adj(ptcl, ptcl_cot, cosmo, conf, a_nbody=None, force_meshes=None):
         dot(dc, vel, dots, slot)
         grads.append((dD, slot))
         slot += 1
-        acc, F = force(pmid, disp, conf, cosmo.Omega_m, acc=acc, force_meshes=F)
+        acc, F = force(pmid, disp, conf, cosmo.Omega_m, acc=acc, force_meshes=F, a=float(a_dp), **kw)
     dot(ac, acc, dots, slot)
     force_slots.append(slot)
-    force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc)
+    force_vjp(pmid, disp, conf, cosmo.Omega_m, F, ac, dc, a=float(a[0]), **kw)
     ac.zero_()
     d = dots.cpu().numpy()
     om = sum(g * d[k] for g, k in grads) + sum(d[k] for k in force_slots) / float(cosmo.Omega_m)
@@ -278,14 +307,16 @@ def nbody_adj(ptcl, ptcl_cot, cosmo, conf, a_nbody=None, force_meshes=None):
     return (ptcl.replace(disp=disp, vel=vel, acc=acc), Particles(conf, pmid, dc, vc, ac), float(om))
 
 
-def nbody(ptcl, cosmo, conf, a_nbody=None):
+def nbody(ptcl, cosmo, conf, a_nbody=None, correction=None):
     """Kick-drift-kick run (solver.py:253-273) in float64: initial force, then
-    per step kick, drift + force, closing kick (fused into the gather)."""
+    per step kick, drift + force, closing kick (fused into the gather); an
+    analytic correction at each force's scale factor."""
     from .nbody import _schedule
     a = conf.a_nbody if a_nbody is None else np.asarray(a_nbody)
     disp = ptcl.disp.to(torch.float64).clone()
     vel = ptcl.vel.to(torch.float64).clone() if ptcl.vel is not None else torch.zeros_like(disp)
-    acc, F = force(ptcl.pmid, disp, conf, cosmo.Omega_m)
+    kw = dict(correction=correction, cosmo=cosmo)
+    acc, F = force(ptcl.pmid, disp, conf, cosmo.Omega_m, a=float(a[0]), **kw)
     s = stream_handle(disp.device)
     for a_prev, a_next in zip(a[:-1], a[1:]):
         stages = _schedule(a_prev, a_next, conf)
@@ -304,7 +335,7 @@ def nbody(ptcl, cosmo, conf, a_nbody=None):
                 kick_f, vk = float(cosmo.kick_factor(kst[1], kst[2], kst[3])), vel
                 i += 1
             force(ptcl.pmid, disp, conf, cosmo.Omega_m, acc=acc, force_meshes=F, drift_vel=vel, drift=D, vel_kick=vk,
-                  kick=kick_f)
+                  kick=kick_f, a=float(st[3]), **kw)
             i += 1
     return ptcl.replace(disp=disp, vel=vel, acc=acc)
 

@@ -5,6 +5,7 @@ corrections/softening.py:49-80) and the combined correction's kernel selection
 runs them on the GPU in tests/test_gpu_force.py."""
 import numpy as np
 import pytest
+import torch
 
 from oracle import pm as opm
 
@@ -153,3 +154,19 @@ def test_oracle_mesh_cnn_reference_properties():
     disp = disp + rng.normal(0, 1.0, disp.shape)
     np.testing.assert_allclose(opm.gravity_cnn(pmid, disp, co, 0.3, P, 1.0, 0.8, depth=2),
                                opm.gravity(pmid, disp, co, 0.3), rtol=1e-12, atol=1e-14)
+
+
+def test_float64_transfers_match_oracle():
+    """The float64 build's window, PGD and softening tables are float64 and
+    match the oracle's float64 restatements to rounding."""
+    import pmpp_b200 as pb
+    from pmpp_b200.corrections import init_potential_correction
+    conf = pb.Configuration(4.0, (16, 16, 16), 2, float_dtype="float64", device="cpu")
+    co = opm.Conf(4.0, (16, 16, 16), mesh_shape=2, float_dtype=np.float64)
+    pgd = dict(alpha0=0.3, A=0.4, B=0.1, kl=0.1, ks=1.0)
+    cases = [("pm_window", opm.window_gain(co)), ("pgd", opm.pgd_transfer(co, 0.5, **pgd)),
+             ("softening", opm.softening_transfer(co, 0.6, 0.5, 1.0))]
+    for model, ref in cases:
+        T, R = init_potential_correction(model, strength=0.6, start=0.5, **pgd).transfer_tables(0.5, None, conf)
+        assert R is None and T.dtype == torch.float64, model
+        np.testing.assert_allclose(T.numpy(), ref, rtol=1e-13, atol=1e-15, err_msg=model)
