@@ -523,6 +523,23 @@ int pmb_force_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx, 
                     double val, double src_mul, const double* tables, int has_masks, const double* transfer,
                     const double* force_meshes, const double* acc_cot, double* disp_cot, void* workspace,
                     int64_t workspace_bytes, void* stream);
+/* Interlaced forms of pmb_force64 / pmb_force_vjp64 (nbody/gravity.py:440-463,
+ * 809-811): a second deposit on the mesh shifted by half a cell, one batched
+ * D2Z, the average (S + S_shift P) / 2 with P = exp(-i (kx + ky + kz) cell / 2)
+ * as the source spectrum, then the same multiplier, Z2D and gather at the
+ * regular origin; the adjoint splits the source cotangent back with conj(P)
+ * / 2 and / 2 and takes both deposits' adjoints.  Same arguments; the
+ * workspaces hold the second mesh and spectrum. */
+int64_t pmb_force64_interlaced_workspace_bytes(int nx, int ny, int nz);
+int pmb_force64_interlaced(const int16_t* pmid, double* disp, const double* drift_vel, double drift, int64_t n, int nx,
+                           int ny, int nz, double cell, double val, double src_mul, const double* tables,
+                           int has_masks, const double* transfer, double* force_meshes, double* acc, double* vel_kick,
+                           double kick, void* workspace, int64_t workspace_bytes, void* stream);
+int64_t pmb_force_vjp64_interlaced_workspace_bytes(int nx, int ny, int nz);
+int pmb_force_vjp64_interlaced(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz,
+                               double cell, double val, double src_mul, const double* tables, int has_masks,
+                               const double* transfer, const double* force_meshes, const double* acc_cot,
+                               double* disp_cot, void* workspace, int64_t workspace_bytes, void* stream);
 /* *out += sum a[i] b[i] in float64 (the Omega_m cotangent dots of the float64
  * reverse sweep, nbody/integrator.py:173-199). */
 int pmb_dot64(const double* a, const double* b, int64_t n, double* out, void* stream);

@@ -121,6 +121,12 @@ _SIGS = {
     "pmb_force_vjp64_workspace_bytes": (c_i64, [c_int, c_int, c_int]),
     "pmb_force_vjp64": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_d, c_d, c_d, c_p, c_int, c_p, c_p, c_p, c_p,
                                 c_p, c_i64, c_p]),
+    "pmb_force64_interlaced_workspace_bytes": (c_i64, [c_int, c_int, c_int]),
+    "pmb_force64_interlaced": (c_int, [c_p, c_p, c_p, c_d, c_i64, c_int, c_int, c_int, c_d, c_d, c_d, c_p, c_int,
+                                       c_p, c_p, c_p, c_p, c_d, c_p, c_i64, c_p]),
+    "pmb_force_vjp64_interlaced_workspace_bytes": (c_i64, [c_int, c_int, c_int]),
+    "pmb_force_vjp64_interlaced": (c_int, [c_p, c_p, c_i64, c_int, c_int, c_int, c_d, c_d, c_d, c_p, c_int, c_p,
+                                           c_p, c_p, c_p, c_p, c_i64, c_p]),
     "pmb_dot64": (c_int, [c_p, c_p, c_i64, c_p, c_p]),
     "pmb_lpt64_ex": (c_int, [c_p, c_int, c_int, c_int, c_d, c_d, c_p, c_int, c_d, c_d, c_d, c_d, c_p, c_p, c_p, c_i64,
                              c_d, c_p, c_p, c_p, c_i64, c_p]),
@@ -199,7 +205,7 @@ _KERNELS = {
     "pmb_white_noise_nested": 1, "pmb_linear_modes": 1,
     "pmb_lpt": 4, "pmb_lpt_vjp": 6, "pmb_pk_shells": 1, "pmb_shell_stats": 1, "pmb_pk_shells_adjoint": 1,
     "pmb_overdensity": 1, "pmb_ens_force": 7, "pmb_ens_step": 9, "pmb_ens_set_step": 1,
-    "pmb_force64": 5, "pmb_deposit64": 1, "pmb_axpy64": 1, "pmb_sum64": 1, "pmb_force_vjp64": 4, "pmb_dot64": 1, "pmb_lpt64_ex": 4, "pmb_lpt_vjp64": 6,
+    "pmb_force64": 5, "pmb_force64_interlaced": 7, "pmb_force_vjp64_interlaced": 6, "pmb_deposit64": 1, "pmb_axpy64": 1, "pmb_sum64": 1, "pmb_force_vjp64": 4, "pmb_dot64": 1, "pmb_lpt64_ex": 4, "pmb_lpt_vjp64": 6,
     "pmb_scatter_vjp64": 1, "pmb_white_noise_nested64": 1,
     "pmb_linear_modes64": 1, "pmb_lpt64": 4, "pmb_pk_shells64": 1, "pmb_pk_shells_adjoint64": 1, "pmb_overdensity64": 1,
     "pmb_pmfft_z": 1, "pmb_pmfft_col": 1, "pmb_pmfft_z2": 1, "pmb_pmfft_col2": 1,

@@ -33,14 +33,16 @@ struct Cell64 {
   double f[3];
 };
 
-// Lower corner and fractions in float64 (enmesh.py:139-147).
+// Lower corner and fractions in float64 (enmesh.py:139-147); org is the mesh
+// origin's offset within a cell (the interlaced deposit's cell / 2,
+// cic/enmesh.py:128-147), subtracted before the division.
 __device__ __forceinline__ Cell64 bin64(const int16_t* __restrict__ pmid, const double* __restrict__ disp, int64_t i,
-                                       Mesh3 m, double cell) {
+                                       Mesh3 m, double cell, double org = 0.0) {
   Cell64 r;
   const int dims[3] = {m.nx, m.ny, m.nz};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const double q = RD::div(disp[3 * i + a], cell);
+    const double q = RD::div(org != 0.0 ? RD::sub(disp[3 * i + a], org) : disp[3 * i + a], cell);
     const double l = floor(q);
     r.f[a] = RD::sub(q, l);
     r.c[a] = pmod((int)pmid[3 * i + a] + (int)l, dims[a]);
@@ -53,13 +55,13 @@ __device__ __forceinline__ double w64(double f, int b) { return RD::sub(1.0, fab
 // Optional drift disp += vel * D, then the CIC deposit of val per particle.
 __global__ void deposit64_kernel(const int16_t* __restrict__ pmid, double* __restrict__ disp,
                                  const double* __restrict__ vel, double drift, int64_t n, Mesh3 m, double cell,
-                                 double val, double* __restrict__ rho) {
+                                 double val, double* __restrict__ rho, double org = 0.0) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     if (vel != nullptr) {
 #pragma unroll
       for (int a = 0; a < 3; ++a) disp[3 * i + a] = RD::add(disp[3 * i + a], RD::mul(vel[3 * i + a], drift));
     }
-    const Cell64 b = bin64(pmid, disp, i, m, cell);
+    const Cell64 b = bin64(pmid, disp, i, m, cell, org);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int bx = k & 1, by = (k >> 1) & 1, bz = (k >> 2) & 1;
@@ -158,10 +160,11 @@ __device__ __forceinline__ double sign64(double f, int b) {
 template <int C>
 __global__ void interp_grad64_kernel(const int16_t* __restrict__ pmid, const double* __restrict__ disp, int64_t n,
                                      Mesh3 m, double cell, const double* __restrict__ mesh,
-                                     const double* __restrict__ u, double u_const, double* __restrict__ disp_cot) {
+                                     const double* __restrict__ u, double u_const, double* __restrict__ disp_cot,
+                                     double org = 0.0) {
   const int64_t cells = m.cells();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const Cell64 b = bin64(pmid, disp, i, m, cell);
+    const Cell64 b = bin64(pmid, disp, i, m, cell, org);
     double uu[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) uu[c] = u ? u[i * C + c] : u_const;
@@ -256,6 +259,35 @@ __global__ void green64_adjoint_kernel(const double2* __restrict__ gc, double2* 
   }
 }
 
+// Interlaced source spectrum (gravity.py:440-463): mode 0 s0 = (s0 + s1 P) / 2
+// with P = exp(-i (kx + ky + kz) cell / 2) = exp(-i pi (nx/Nx + ny/Ny + nz/Nz))
+// over the signed mode numbers of the half spectrum; mode 1 its transpose from
+// the cotangent c held in s0: s1 = conj(P) c / 2, s0 = c / 2.
+__global__ void interlace64_kernel(double2* __restrict__ s0, double2* __restrict__ s1, Mesh3 m, int mode) {
+  const int nzh = m.nz / 2 + 1;
+  const int64_t total = m.half_cells();
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (int64_t)gridDim.x * blockDim.x) {
+    const int iz = (int)(j % nzh);
+    const int64_t r = j / nzh;
+    const int iy = (int)(r % m.ny), ix = (int)(r / m.ny);
+    const int kx = ix < (m.nx + 1) / 2 ? ix : ix - m.nx, ky = iy < (m.ny + 1) / 2 ? iy : iy - m.ny;
+    const double t = RD::add(RD::add(RD::div((double)kx, (double)m.nx), RD::div((double)ky, (double)m.ny)),
+                             RD::div((double)iz, (double)m.nz));
+    double sn, cs;
+    sincospi(t, &sn, &cs);
+    if (mode == 0) {
+      const double2 a = s0[j], b = s1[j];
+      const double pr = RD::add(RD::mul(b.x, cs), RD::mul(b.y, sn)), pim = RD::sub(RD::mul(b.y, cs), RD::mul(b.x, sn));
+      s0[j] = make_double2(RD::mul(0.5, RD::add(a.x, pr)), RD::mul(0.5, RD::add(a.y, pim)));
+    } else {
+      const double2 c = s0[j];
+      s1[j] = make_double2(RD::mul(0.5, RD::sub(RD::mul(c.x, cs), RD::mul(c.y, sn))),
+                           RD::mul(0.5, RD::add(RD::mul(c.y, cs), RD::mul(c.x, sn))));
+      s0[j] = make_double2(RD::mul(0.5, c.x), RD::mul(0.5, c.y));
+    }
+  }
+}
+
 __global__ void dot64_kernel(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
                              double* __restrict__ out) {
   double s = 0.0;
@@ -289,25 +321,31 @@ struct Carve64 {
   }
 };
 
-int64_t force64_layout(Mesh3 m, void* ws, double** rho, double2** rho_hat, double2** grad_hat, void** work) {
+// Interlaced forms (il) hold two source meshes and spectra: the regular and
+// the half-cell-shifted deposit's.
+int64_t force64_layout(Mesh3 m, void* ws, double** rho, double2** rho_hat, double2** grad_hat, void** work,
+                       bool il = false) {
   Carve64 c(ws);
-  *rho = (double*)c.take(8 * m.cells());
-  *rho_hat = (double2*)c.take(16 * m.half_cells());
+  const int ns = il ? 2 : 1;
+  *rho = (double*)c.take(8 * ns * m.cells());
+  *rho_hat = (double2*)c.take(16 * ns * m.half_cells());
   *grad_hat = (double2*)c.take(48 * m.half_cells());
-  const int64_t w3 = fft_work_bytes64(m, 3), w1 = fft_work_bytes64(m, 1);
-  if (w3 < 0 || w1 < 0) return -1;
-  *work = c.take(w3 > w1 ? w3 : w1);
+  const int64_t w3 = fft_work_bytes64(m, 3), ws_ = fft_work_bytes64(m, ns);
+  if (w3 < 0 || ws_ < 0) return -1;
+  *work = c.take(w3 > ws_ ? w3 : ws_);
   return c.off;
 }
 
-int64_t force_vjp64_layout(Mesh3 m, void* ws, double** mesh3, double2** spec3, double2** spec1, void** work) {
+int64_t force_vjp64_layout(Mesh3 m, void* ws, double** mesh3, double2** spec3, double2** spec1, void** work,
+                           bool il = false) {
   Carve64 c(ws);
+  const int ns = il ? 2 : 1;
   *mesh3 = (double*)c.take(24 * m.cells());
   *spec3 = (double2*)c.take(48 * m.half_cells());
-  *spec1 = (double2*)c.take(16 * m.half_cells());
-  const int64_t w3 = fft_work_bytes64(m, 3), w1 = fft_work_bytes64(m, 1);
-  if (w3 < 0 || w1 < 0) return -1;
-  *work = c.take(w3 > w1 ? w3 : w1);
+  *spec1 = (double2*)c.take(16 * ns * m.half_cells());
+  const int64_t w3 = fft_work_bytes64(m, 3), ws_ = fft_work_bytes64(m, ns);
+  if (w3 < 0 || ws_ < 0) return -1;
+  *work = c.take(w3 > ws_ ? w3 : ws_);
   return c.off;
 }
 
@@ -394,28 +432,33 @@ int64_t pmb_force64_workspace_bytes(int nx, int ny, int nz) {
   return force64_layout(Mesh3{nx, ny, nz}, nullptr, &r, &rh, &gh, &w);
 }
 
-int pmb_force64(const int16_t* pmid, double* disp, const double* drift_vel, double drift, int64_t n, int nx, int ny,
-                int nz, double cell, double val, double src_mul, const double* tables, int has_masks,
-                const double* transfer, double* force_meshes, double* acc, double* vel_kick, double kick,
-                void* workspace, int64_t workspace_bytes, void* stream) {
+static int force64_impl(const int16_t* pmid, double* disp, const double* drift_vel, double drift, int64_t n, int nx,
+                        int ny, int nz, double cell, double val, double src_mul, const double* tables, int has_masks,
+                        const double* transfer, double* force_meshes, double* acc, double* vel_kick, double kick,
+                        void* workspace, int64_t workspace_bytes, void* stream, bool il) {
   Mesh3 m{nx, ny, nz};
   F64_REQUIRE(valid64(nx, ny, nz), "pmb_force64: unsupported mesh shape");
   F64_REQUIRE(n >= 0 && cell > 0.0, "pmb_force64: bad particle count or cell size");
   double* rho;
   double2 *rho_hat, *grad_hat;
   void* work;
-  const int64_t need = force64_layout(m, workspace, &rho, &rho_hat, &grad_hat, &work);
+  const int64_t need = force64_layout(m, workspace, &rho, &rho_hat, &grad_hat, &work, il);
   F64_REQUIRE(need >= 0, "pmb_force64: cuFFT plan creation failed");
   if (need > workspace_bytes) {
     set_last_error("pmb_force64: workspace too small");
     return kScratchTooSmall;
   }
   cudaStream_t s = S(stream);
-  PMB_CUDA_CHECK(cudaMemsetAsync(rho, 0, 8 * m.cells(), s));
+  const int ns = il ? 2 : 1;
+  PMB_CUDA_CHECK(cudaMemsetAsync(rho, 0, 8 * ns * m.cells(), s));
   if (n > 0) deposit64_kernel<<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, drift_vel, drift, n, m, cell, val, rho);
-  source64_kernel<<<grid_for(m.cells(), 256), 256, 0, s>>>(rho, m.cells(), src_mul);
+  if (n > 0 && il)  // the deposit on the mesh shifted by half a cell (gravity.py:446-463), drifted positions
+    deposit64_kernel<<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, nullptr, 0.0, n, m, cell, val, rho + m.cells(),
+                                                      0.5 * cell);
+  source64_kernel<<<grid_for(ns * m.cells(), 256), 256, 0, s>>>(rho, ns * m.cells(), src_mul);
   PMB_CUDA_CHECK(cudaGetLastError());
-  F64_TRY(fft_d2z(m, 1, rho, rho_hat, work, s));
+  F64_TRY(fft_d2z(m, ns, rho, rho_hat, work, s));
+  if (il) interlace64_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(rho_hat, rho_hat + m.half_cells(), m, 0);
   green64_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(rho_hat, grad_hat, m, tables64(tables, m, has_masks),
                                                                1.0 / (double)m.cells(), transfer);
   PMB_CUDA_CHECK(cudaGetLastError());
@@ -425,6 +468,29 @@ int pmb_force64(const int16_t* pmid, double* disp, const double* drift_vel, doub
   return kOk;
 }
 
+int pmb_force64(const int16_t* pmid, double* disp, const double* drift_vel, double drift, int64_t n, int nx, int ny,
+                int nz, double cell, double val, double src_mul, const double* tables, int has_masks,
+                const double* transfer, double* force_meshes, double* acc, double* vel_kick, double kick,
+                void* workspace, int64_t workspace_bytes, void* stream) {
+  return force64_impl(pmid, disp, drift_vel, drift, n, nx, ny, nz, cell, val, src_mul, tables, has_masks, transfer,
+                      force_meshes, acc, vel_kick, kick, workspace, workspace_bytes, stream, false);
+}
+
+int64_t pmb_force64_interlaced_workspace_bytes(int nx, int ny, int nz) {
+  double* r;
+  double2 *rh, *gh;
+  void* w;
+  return force64_layout(Mesh3{nx, ny, nz}, nullptr, &r, &rh, &gh, &w, true);
+}
+
+int pmb_force64_interlaced(const int16_t* pmid, double* disp, const double* drift_vel, double drift, int64_t n, int nx,
+                           int ny, int nz, double cell, double val, double src_mul, const double* tables,
+                           int has_masks, const double* transfer, double* force_meshes, double* acc, double* vel_kick,
+                           double kick, void* workspace, int64_t workspace_bytes, void* stream) {
+  return force64_impl(pmid, disp, drift_vel, drift, n, nx, ny, nz, cell, val, src_mul, tables, has_masks, transfer,
+                      force_meshes, acc, vel_kick, kick, workspace, workspace_bytes, stream, true);
+}
+
 int64_t pmb_force_vjp64_workspace_bytes(int nx, int ny, int nz) {
   double* m3;
   double2 *s3, *s1;
@@ -432,10 +498,10 @@ int64_t pmb_force_vjp64_workspace_bytes(int nx, int ny, int nz) {
   return force_vjp64_layout(Mesh3{nx, ny, nz}, nullptr, &m3, &s3, &s1, &w);
 }
 
-int pmb_force_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz, double cell,
-                    double val, double src_mul, const double* tables, int has_masks, const double* transfer,
-                    const double* force_meshes, const double* acc_cot, double* disp_cot, void* workspace,
-                    int64_t workspace_bytes, void* stream) {
+static int force_vjp64_impl(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz, double cell,
+                            double val, double src_mul, const double* tables, int has_masks, const double* transfer,
+                            const double* force_meshes, const double* acc_cot, double* disp_cot, void* workspace,
+                            int64_t workspace_bytes, void* stream, bool il) {
   Mesh3 m{nx, ny, nz};
   F64_REQUIRE(valid64(nx, ny, nz), "pmb_force_vjp64: unsupported mesh shape");
   F64_REQUIRE(n >= 0 && n < 4294967296ll && cell > 0.0, "pmb_force_vjp64: bad particle count or cell size");
@@ -443,7 +509,7 @@ int pmb_force_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx, 
   double* mesh3;
   double2 *spec3, *spec1;
   void* work;
-  const int64_t need = force_vjp64_layout(m, workspace, &mesh3, &spec3, &spec1, &work);
+  const int64_t need = force_vjp64_layout(m, workspace, &mesh3, &spec3, &spec1, &work, il);
   F64_REQUIRE(need >= 0, "pmb_force_vjp64: cuFFT plan creation failed");
   if (need > workspace_bytes) {
     set_last_error("pmb_force_vjp64: workspace too small");
@@ -460,12 +526,40 @@ int pmb_force_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx, 
   F64_TRY(fft_d2z(m, 3, mesh3, spec3, work, s));
   green64_adjoint_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(spec3, spec1, m, tables64(tables, m, has_masks),
                                                                        src_mul / (double)m.cells(), transfer);
+  // interlaced: split the source cotangent between the two deposits
+  if (il) interlace64_kernel<<<grid_for(m.half_cells(), 256), 256, 0, s>>>(spec1, spec1 + m.half_cells(), m, 1);
   PMB_CUDA_CHECK(cudaGetLastError());
-  F64_TRY(fft_z2d(m, 1, spec1, mesh3, work, s));
+  F64_TRY(fft_z2d(m, il ? 2 : 1, spec1, mesh3, work, s));
   if (n > 0)  // scatter adjoint, position term (scatter.py:366-370)
     interp_grad64_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, n, m, cell, mesh3, nullptr, val, disp_cot);
+  if (n > 0 && il)  // the shifted deposit's adjoint on its own mesh
+    interp_grad64_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(pmid, disp, n, m, cell, mesh3 + m.cells(), nullptr, val,
+                                                             disp_cot, 0.5 * cell);
   PMB_CUDA_CHECK(cudaGetLastError());
   return kOk;
+}
+
+int pmb_force_vjp64(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz, double cell,
+                    double val, double src_mul, const double* tables, int has_masks, const double* transfer,
+                    const double* force_meshes, const double* acc_cot, double* disp_cot, void* workspace,
+                    int64_t workspace_bytes, void* stream) {
+  return force_vjp64_impl(pmid, disp, n, nx, ny, nz, cell, val, src_mul, tables, has_masks, transfer, force_meshes,
+                          acc_cot, disp_cot, workspace, workspace_bytes, stream, false);
+}
+
+int64_t pmb_force_vjp64_interlaced_workspace_bytes(int nx, int ny, int nz) {
+  double* m3;
+  double2 *s3, *s1;
+  void* w;
+  return force_vjp64_layout(Mesh3{nx, ny, nz}, nullptr, &m3, &s3, &s1, &w, true);
+}
+
+int pmb_force_vjp64_interlaced(const int16_t* pmid, const double* disp, int64_t n, int nx, int ny, int nz,
+                               double cell, double val, double src_mul, const double* tables, int has_masks,
+                               const double* transfer, const double* force_meshes, const double* acc_cot,
+                               double* disp_cot, void* workspace, int64_t workspace_bytes, void* stream) {
+  return force_vjp64_impl(pmid, disp, n, nx, ny, nz, cell, val, src_mul, tables, has_masks, transfer, force_meshes,
+                          acc_cot, disp_cot, workspace, workspace_bytes, stream, true);
 }
 
 int pmb_dot64(const double* a, const double* b, int64_t n, double* out, void* stream) {

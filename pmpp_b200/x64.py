@@ -9,7 +9,8 @@ with the reference's float64 results.  The adjoints of the N-body run, the
 force, the LPT displacements, the deposit, the P(k) loss and the linear
 modes' cosmology parameters exist here too (``nbody_adj``, ``force_vjp``,
 ``lpt_vjp``, ``scatter_vjp``, ``pk_loss``, ``linear_modes_param_cotangents``),
-and the force takes the analytic corrections (``correction_tables``).
+and the force takes the analytic corrections, interlaced or not
+(``correction_tables``).
 """
 from __future__ import annotations
 
@@ -173,16 +174,17 @@ def lpt(modes, cosmo, conf):
 
 
 def correction_tables(conf, dev, correction=None, a=None, cosmo=None):
-    """Spectral tables and float64 transfer of the force for a correction: the
-    analytic ones (window compensation, FastPM's Green's functions and 4-point
-    gradient, PGD, high-k softening and their products, corrections/core.py:
-    40-151, 333-334, 396-422).  Interlacing, the mesh CNN and the learned
-    radial transfer are float32 only."""
+    """(spectral tables, float64 transfer or None, interlaced) of the force for
+    a correction: the analytic ones (window compensation, FastPM's Green's
+    functions and 4-point gradient, PGD, high-k softening and their products,
+    corrections/core.py:40-151, 333-334, 396-422), interlaced when the
+    correction asks for it (corrections/core.py:381-393).  The mesh CNN and
+    the learned radial transfer are float32 only."""
     if correction is None:
-        return conf.spectral_tables("mesh", dev), None
+        return conf.spectral_tables("mesh", dev), None, False
     from .gravity import _correction_args, _tables, mesh_cnn_of, uses_interlacing
-    if uses_interlacing(correction) or mesh_cnn_of(correction) is not None:
-        raise NotImplementedError("the float64 build takes the analytic corrections without interlacing")
+    if mesh_cnn_of(correction) is not None:
+        raise NotImplementedError("the float64 build takes no mesh-CNN correction")
     gk, transfer, radial, _ = _correction_args(correction, a, cosmo, conf)
     if radial is not None:
         raise NotImplementedError("the float64 build takes no learned radial transfer")
@@ -190,7 +192,7 @@ def correction_tables(conf, dev, correction=None, a=None, cosmo=None):
         if transfer.dtype != torch.float64:
             raise TypeError("the float64 force needs a float64 transfer table")
         transfer = transfer.to(dev).contiguous()
-    return _tables(conf, dev, gk, correction), transfer
+    return _tables(conf, dev, gk, correction), transfer, bool(uses_interlacing(correction))
 
 
 def force(pmid, disp, conf, omega_m, acc=None, force_meshes=None, drift_vel=None, drift=0.0, vel_kick=None, kick=0.0,
@@ -205,9 +207,10 @@ def force(pmid, disp, conf, omega_m, acc=None, force_meshes=None, drift_vel=None
         acc = torch.empty((n, 3), dtype=torch.float64, device=dev)
     if force_meshes is None:
         force_meshes = torch.empty((3, nx, ny, nz), dtype=torch.float64, device=dev)
-    tables, transfer = correction_tables(conf, dev, correction, a, cosmo)
-    ws = workspace(lib().pmb_force64_workspace_bytes(nx, ny, nz), dev, "force64")
-    call("pmb_force64", pmid.data_ptr(), disp.data_ptr(), None if drift_vel is None else drift_vel.data_ptr(),
+    tables, transfer, il = correction_tables(conf, dev, correction, a, cosmo)
+    entry = "pmb_force64_interlaced" if il else "pmb_force64"
+    ws = workspace(getattr(lib(), entry + "_workspace_bytes")(nx, ny, nz), dev, "force64")
+    call(entry, pmid.data_ptr(), disp.data_ptr(), None if drift_vel is None else drift_vel.data_ptr(),
          float(drift), n, nx, ny, nz, float(conf.cell_size), float(conf.mesh_size / conf.ptcl_num), 1.5 * float(omega_m),
          tables.data_ptr(), int(conf.has_particle_nyquist_masks), None if transfer is None else transfer.data_ptr(),
          force_meshes.data_ptr(), acc.data_ptr(), None if vel_kick is None else vel_kick.data_ptr(), float(kick),
@@ -224,9 +227,10 @@ def force_vjp(pmid, disp, conf, omega_m, force_meshes, acc_cot, disp_cot=None, c
     if disp_cot is None:
         disp_cot = torch.zeros((n, 3), dtype=torch.float64, device=dev)
     acc_cot = acc_cot.to(torch.float64).contiguous()
-    tables, transfer = correction_tables(conf, dev, correction, a, cosmo)
-    ws = workspace(lib().pmb_force_vjp64_workspace_bytes(nx, ny, nz), dev, "force_vjp64")
-    call("pmb_force_vjp64", pmid.data_ptr(), disp.data_ptr(), n, nx, ny, nz, float(conf.cell_size),
+    tables, transfer, il = correction_tables(conf, dev, correction, a, cosmo)
+    entry = "pmb_force_vjp64_interlaced" if il else "pmb_force_vjp64"
+    ws = workspace(getattr(lib(), entry + "_workspace_bytes")(nx, ny, nz), dev, "force_vjp64")
+    call(entry, pmid.data_ptr(), disp.data_ptr(), n, nx, ny, nz, float(conf.cell_size),
          float(conf.mesh_size / conf.ptcl_num), 1.5 * float(omega_m), tables.data_ptr(),
          int(conf.has_particle_nyquist_masks), None if transfer is None else transfer.data_ptr(),
          force_meshes.data_ptr(), acc_cot.data_ptr(), disp_cot.data_ptr(), ws.data_ptr(), ws.numel(),

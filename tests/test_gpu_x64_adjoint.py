@@ -291,25 +291,28 @@ def _oracle_kernel(model, corr, co, a):
 
 
 @pytest.mark.parametrize("model", ["pm_window", "fastpm_1_4", "fastpm_3_4", "pgd", "softening", "windowed_pgd",
-                                   "pm_window+softening"])
+                                   "pm_window+softening", "pm_window:interlaced", "windowed_pgd:interlaced"])
 def test_force_with_analytic_corrections_float64(model):
     """The analytic corrections in the float64 force and its adjoint: the
     window compensation (corrections/window.py:229-265), the discrete
     Laplacian (gravity.py:122-171), FastPM's 4-point gradient
     (gravity.py:355-391), PGD at a = 0.5 (corrections/pgd.py:154-237), high-k
-    softening (corrections/softening.py:49-80) and their products, within
-    1e-12 of the float64 oracle (float64 transfer tables, cuFFT D2Z / Z2D)."""
+    softening (corrections/softening.py:49-80), their products and the
+    interlaced deposit (gravity.py:440-463), within 1e-12 of the float64
+    oracle (float64 transfer tables, cuFFT D2Z / Z2D)."""
     from pmpp_b200.corrections import init_potential_correction
     pb, co, conf = _confs(16, 2)
     pmid, disp, _, ptcl = _state(co, conf, pb, 5, 1.0)
     cos = pb.boltzmann(pb.SimpleLCDM(conf))
     a = 0.5
-    corr = init_potential_correction(model, strength=0.6, start=0.5, **_PGD)
+    il = model.endswith(":interlaced")
+    model = model.replace(":interlaced", "")
+    corr = init_potential_correction(model, strength=0.6, start=0.5, interlacing=il, **_PGD)
     kernel = _oracle_kernel(model, corr, co, a)
     grad = corr.gradient_kernel
-    ref = opm.gravity(pmid, disp, co, cos.Omega_m, kernel=kernel, gradient=grad)
+    ref = opm.gravity(pmid, disp, co, cos.Omega_m, kernel=kernel, gradient=grad, interlacing=il)
     ac = np.random.default_rng(6).normal(size=disp.shape)
-    rdc, rom = opm.gravity_vjp(pmid, disp, co, cos.Omega_m, ac, kernel=kernel, gradient=grad)
+    rdc, rom = opm.gravity_vjp(pmid, disp, co, cos.Omega_m, ac, kernel=kernel, gradient=grad, interlacing=il)
     acc = pb.gravity(a, ptcl, cos, conf, correction=corr)
     dc, om = pb.gravity_vjp(a, ptcl, cos, conf, torch.from_numpy(ac).cuda(), correction=corr)
     assert acc.dtype == torch.float64 and dc.dtype == torch.float64
@@ -317,25 +320,28 @@ def test_force_with_analytic_corrections_float64(model):
     assert _rel(dc.cpu().numpy(), rdc) < 1e-12
     np.testing.assert_allclose(om, rom, rtol=1e-12)
     assert _rel(acc.cpu().numpy(), opm.gravity(pmid, disp, co, cos.Omega_m)) > 1e-6  # not the plain force
+    if il:  # nor the same correction without interlacing
+        assert _rel(acc.cpu().numpy(), opm.gravity(pmid, disp, co, cos.Omega_m, kernel=kernel, gradient=grad)) > 1e-6
 
 
-def test_pgd_windowed_reverse_sweep_float64_matches_oracle():
+@pytest.mark.parametrize("il", [False, True])
+def test_pgd_windowed_reverse_sweep_float64_matches_oracle(il):
     """Three KDK steps and the reverse sweep with the window compensation times
     the scale-factor dependent PGD transfer, each force at its positions'
-    scale factor, against the float64 oracle: positions and cotangents within
-    1e-10, the final acceleration within 1e-9, the Omega_m cotangent within
-    1e-5 (as the plain sweep)."""
+    scale factor, plain and interlaced, against the float64 oracle: positions
+    and cotangents within 1e-10, the final acceleration within 1e-9, the
+    Omega_m cotangent within 1e-5 (as the plain sweep)."""
     from pmpp_b200.corrections import init_potential_correction
     a = np.linspace(0.1, 1.0, 4)
     pb, co, conf = _confs(16, 2, a)
     cos = pb.boltzmann(pb.SimpleLCDM(conf))
     oc = opm.boltzmann(ocos.Cosmo(), co)
     pmid, disp, vel, ptcl = _state(co, conf, pb, 3, 1.0)
-    corr = init_potential_correction("windowed_pgd", **_PGD)
+    corr = init_potential_correction("windowed_pgd", interlacing=il, **_PGD)
     K = lambda s: _oracle_kernel("windowed_pgd", corr, co, s)
     run = pb.NBodyRun(conf, cos, corr)
     out = run.forward(ptcl)
-    rd, rv, ra = opm.nbody(pmid, disp, vel, co, oc, K)
+    rd, rv, ra = opm.nbody(pmid, disp, vel, co, oc, K, interlacing=il)
     assert _rel(out.disp.cpu().numpy(), rd) < 1e-10
     # the force at the final positions amplifies their rounding (measured 1.2e-10)
     assert _rel(out.acc.cpu().numpy(), ra) < 1e-9
@@ -344,7 +350,8 @@ def test_pgd_windowed_reverse_sweep_float64_matches_oracle():
     cot = pb.Particles(conf, ptcl.pmid, torch.from_numpy(dcot).cuda(), torch.from_numpy(vcot).cuda(),
                        torch.zeros_like(out.disp))
     _, c0, om = run.adjoint(out, cot)
-    _, _, rdc, rvc, rom = opm.nbody_adj(pmid, rd, rv, ra, dcot, vcot, np.zeros_like(dcot), co, oc, K)
+    _, _, rdc, rvc, rom = opm.nbody_adj(pmid, rd, rv, ra, dcot, vcot, np.zeros_like(dcot), co, oc, K,
+                                        interlacing=il)
     assert _rel(c0.disp.cpu().numpy(), rdc) < 1e-10
     assert _rel(c0.vel.cpu().numpy(), rvc) < 1e-10
     np.testing.assert_allclose(om, rom, rtol=1e-5)
