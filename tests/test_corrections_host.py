@@ -170,3 +170,41 @@ def test_float64_transfers_match_oracle():
         T, R = init_potential_correction(model, strength=0.6, start=0.5, **pgd).transfer_tables(0.5, None, conf)
         assert R is None and T.dtype == torch.float64, model
         np.testing.assert_allclose(T.numpy(), ref, rtol=1e-13, atol=1e-15, err_msg=model)
+
+
+def test_float64_correction_tables_route_and_refuse():
+    """x64.correction_tables: float64 spectral tables (the discrete-Laplacian
+    wavenumbers and FastPM's derivative when asked for), the float64 transfer
+    and the interlacing flag; the mesh CNN, a learned radial transfer and a
+    float32 transfer are refused."""
+    import pmpp_b200 as pb
+    from pmpp_b200 import x64
+    from pmpp_b200.corrections import init_potential_correction
+    conf = pb.Configuration(4.0, (8, 8, 8), 2, float_dtype="float64", device="cpu")
+    t0, T0, il0 = x64.correction_tables(conf, "cpu")
+    assert t0.dtype == torch.float64 and T0 is None and not il0
+    t, T, il = x64.correction_tables(conf, "cpu", init_potential_correction("fastpm_3_4"), 0.5)
+    assert T is None and not il and t.dtype == torch.float64
+    assert torch.equal(t, conf.spectral_tables("mesh", "cpu", 1, 1)) and not torch.equal(t, t0)
+    t, T, il = x64.correction_tables(conf, "cpu", init_potential_correction("windowed_pgd", interlacing=True), 0.5)
+    assert il and T.dtype == torch.float64 and T.shape == (16, 16, 9)
+
+    class Radial:
+        green_kernel = 0
+
+        def transfer_tables(self, a, cosmo, conf):
+            return None, torch.ones(10, dtype=torch.float32)
+
+    class Float32Transfer(Radial):
+        def transfer_tables(self, a, cosmo, conf):
+            return torch.ones((16, 16, 9), dtype=torch.float32), None
+
+    class Cnn(Radial):
+        mesh_cnn = True
+
+    with pytest.raises(NotImplementedError):
+        x64.correction_tables(conf, "cpu", Radial(), 0.5)
+    with pytest.raises(NotImplementedError):
+        x64.correction_tables(conf, "cpu", Cnn(), 0.5)
+    with pytest.raises(TypeError):
+        x64.correction_tables(conf, "cpu", Float32Transfer(), 0.5)
