@@ -310,6 +310,39 @@ def test_windowed_nbody_forward_and_adjoint_match_oracle(il):
     assert abs(om - rom) < 1e-4 * sum(abs(t) for t in terms)
 
 
+def test_pgd_windowed_nbody_forward_and_adjoint_match_oracle():
+    """Two KDK steps and the reverse sweep with the window compensation times
+    the scale-factor dependent PGD transfer: every force, its adjoint and each
+    recomputed force take their positions' scale factor (integrator.py:
+    620-686), as the oracle's run and sweep with a kernel per scale factor."""
+    from pmpp_b200.corrections import init_potential_correction
+    a = np.linspace(0.1, 1.0, 3)
+    pb, co, conf = _confs(a_custom=a)
+    cos = pb.boltzmann(pb.SimpleLCDM(conf))
+    oc = opm.boltzmann(ocos.Cosmo(), co)
+    corr = init_potential_correction("windowed_pgd", **_PGD)
+    kern = lambda s: opm.potential_kernel(co, "discrete_laplacian", opm.window_gain(co) * opm.pgd_transfer(co, s, **_PGD))
+    pmid, disp, vel, ptcl = _nbody_inputs(co, conf, pb, seed=35)
+    run = pb.NBodyRun(conf, cos, corr)
+    out = run.forward(ptcl)
+    rd, rv, ra = opm.nbody(pmid, disp, vel, co, oc, kern)
+    assert rel_err(out.disp.cpu().numpy(), rd) < 1e-4
+    assert rel_err(out.vel.cpu().numpy(), rv) < 1e-4
+    assert rel_err(out.acc.cpu().numpy(), ra) < 1e-4
+    rng = np.random.default_rng(6)
+    dcot = rng.normal(size=disp.shape).astype(np.float32)
+    vcot = rng.normal(size=disp.shape).astype(np.float32)
+    cot = pb.Particles(conf, ptcl.pmid, torch.from_numpy(dcot).cuda(), torch.from_numpy(vcot).cuda(),
+                       torch.zeros_like(out.disp))
+    _, c0, om = run.adjoint(out, cot)
+    terms = []
+    _, _, rdc, rvc, rom = opm.nbody_adj(pmid, rd, rv, ra, dcot, vcot, np.zeros_like(dcot), co, oc, kern,
+                                        om_terms=terms)
+    assert rel_err(c0.disp.cpu().numpy(), rdc) < 1e-3
+    assert rel_err(c0.vel.cpu().numpy(), rvc) < 1e-3
+    assert abs(om - rom) < 1e-4 * sum(abs(t) for t in terms)
+
+
 def test_per_operation_adjoints_match_the_fused_reverse_sweep():
     """kick_adj / drift_adj_from_output / force_adj / integrate_adj
     (integrator.py:429-837) stepped by hand from the final state reproduce the
